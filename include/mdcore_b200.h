@@ -1,0 +1,356 @@
+/*
+ * mdcore_b200.h -- C ABI of the B200-native mdcore nonbonded engine.
+ *
+ * A driver written against the reference mdcore engine API compiles against this header
+ * and links against libmdcore_b200.so instead of libmdcore_single.  Every declaration below
+ * cites the reference declaration it stands in for (file:line in the mdcore sources).
+ * Semantics follow the reference: functions return 0 (or a non-negative id/count) on
+ * success and a negative error code on failure, after pushing an entry on the error stack
+ * (errs_dump prints and clears it).
+ *
+ * Precision model: positions are single precision relative to their cell's origin, as in
+ * the reference FPTYPE_SINGLE build.  Pair forces are computed in FP32 and accumulated on
+ * the device in 64-bit fixed point (scale 2^24 per kJ/mol/nm); energies and virials are
+ * accumulated in FP64.  Nonbonded forces are therefore independent of the order in which
+ * cell-pair tasks run.
+ *
+ * Exclusions are honoured inside the pair sweep (excluded pairs are skipped) instead of
+ * being subtracted afterwards as src/exclusion.c:81-295 does; the total potential energy
+ * s.epot is the same quantity, s.epot_exclusion stays 0 and s.epot_nonbond already holds
+ * the net nonbonded energy.
+ */
+#ifndef MDCORE_B200_H
+#define MDCORE_B200_H
+
+#include <stdio.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- error stack
+ * Replaces src/errs.h:21-41 (errs_register / errs_dump / errs_clear). */
+#define errs_maxstack 100
+int errs_register(int id, const char *msg, int line, const char *func, const char *file);
+int errs_dump(FILE *out);
+void errs_clear(void);
+
+/* ---------------------------------------------------------------- error codes
+ * Same values as src/engine.h:22-52, src/potential.h:21-27, src/space.h:21-30. */
+#define engine_err_ok          0
+#define engine_err_null       -1
+#define engine_err_malloc     -2
+#define engine_err_space      -3
+#define engine_err_pthread    -4
+#define engine_err_runner     -5
+#define engine_err_range      -6
+#define engine_err_cell       -7
+#define engine_err_domain     -8
+#define engine_err_nompi      -9
+#define engine_err_mpi       -10
+#define engine_err_bond      -11
+#define engine_err_angle     -12
+#define engine_err_reader    -13
+#define engine_err_psf       -14
+#define engine_err_pdb       -15
+#define engine_err_cpf       -16
+#define engine_err_potential -17
+#define engine_err_exclusion -18
+#define engine_err_sets      -19
+#define engine_err_dihedral  -20
+#define engine_err_cuda      -21
+#define engine_err_nocuda    -22
+#define engine_err_cudasp    -23
+#define engine_err_maxparts  -24
+#define engine_err_queue     -25
+#define engine_err_rigid     -26
+#define engine_err_cutoff    -27
+#define engine_err_nometis   -28
+#define engine_err_deps      -29
+#define engine_err_nyi       -30
+
+#define potential_err_ok        0
+#define potential_err_null     -1
+#define potential_err_malloc   -2
+#define potential_err_bounds   -3
+#define potential_err_nyi      -4
+#define potential_err_ivalsmax -5
+
+#define space_err_ok        0
+#define space_err_null     -1
+#define space_err_malloc   -2
+#define space_err_cell     -3
+#define space_err_pthread  -4
+#define space_err_range    -5
+#define space_err_maxpairs -6
+#define space_err_nrtasks  -7
+#define space_err_task     -8
+
+extern int engine_err;     /* src/engine.h:117 */
+extern int potential_err;  /* src/potential.h:48 */
+extern int space_err;      /* src/space.h:60 */
+
+/* ---------------------------------------------------------------- engine flags
+ * Same bits as src/engine.h:56-72.  Honoured: none, cuda, unsorted (sweep without the
+ * projection cut), verlet_pseudo/verlet/verlet_pairwise (accepted; sorts are redone every
+ * step), affinity (ignored), shake.  Others make engine_init fail with engine_err_nyi. */
+#define engine_flag_none             0
+#define engine_flag_static           1
+#define engine_flag_localparts       2
+#define engine_flag_cuda             4
+#define engine_flag_explepot         8
+#define engine_flag_verlet          16
+#define engine_flag_verlet_pairwise 32
+#define engine_flag_affinity        64
+#define engine_flag_prefetch       128
+#define engine_flag_verlet_pseudo  256
+#define engine_flag_unsorted       512
+#define engine_flag_shake         1024
+#define engine_flag_mpi           2048
+#define engine_flag_parbonded     4096
+#define engine_flag_async         8192
+#define engine_flag_dpd          16384
+#define engine_flag_nullpart     32768
+
+/* Periodicity bits, src/space.h:33-42. */
+#define space_periodic_none  0
+#define space_periodic_x     1
+#define space_periodic_y     2
+#define space_periodic_z     4
+#define space_periodic_full  7
+
+/* ---------------------------------------------------------------- particles
+ * Same 64-byte layout as struct part, src/part.h:46-69 (FPTYPE = float). */
+#define part_flag_none   0
+#define part_flag_frozen 1
+#define part_flag_ghost  2
+
+struct part {
+    float x[4] __attribute__((aligned(16)));
+    float v[4] __attribute__((aligned(16)));
+    float f[4] __attribute__((aligned(16)));
+    float q;
+    int id, vid;
+    short int type;
+    unsigned short int flags;
+} __attribute__((aligned(64)));
+
+/* src/part.h:73-88 */
+struct part_type {
+    int id;
+    double mass, imass, charge;
+    double eps, rmin;
+    char name[64], name2[64];
+};
+
+/* ---------------------------------------------------------------- potentials
+ * struct potential and constants as in src/potential.h:30-74: a piecewise quintic
+ * interpolant on n intervals; interval 0 is a linear continuation for r < a.  The table
+ * holds (n+1) chunks of 8 floats {centre, 1/halfwidth, c5, c4, c3, c2, c1, c0}. */
+#define potential_degree   5
+#define potential_chunk    (potential_degree + 3)
+#define potential_ivalsa   1
+#define potential_ivalsb   10
+#define potential_N        100
+#define potential_align    64
+#define potential_ivalsmax 320
+#define potential_escale   (0.079577471545947667882)
+
+#define potential_flag_none    0
+#define potential_flag_LJ126   1
+#define potential_flag_Ewald   2
+#define potential_flag_Coulomb 4
+
+struct potential {
+    float alpha[4];
+    float *c;
+    double a, b;
+    unsigned int flags;
+    int n;
+};
+
+/* Table construction, src/potential.c:963-1194 (potential_init) and the creators at
+ * src/potential.c:517-914.  Tables are bit-identical to the reference single-precision
+ * build compiled without FMA contraction. */
+int potential_init(struct potential *p, double (*f)(double), double (*fp)(double),
+                   double (*f6p)(double), float a, float b, float tol);
+double potential_getalpha(double (*f6p)(double), double a, double b);
+struct potential *potential_create_LJ126(double a, double b, double A, double B, double tol);
+struct potential *potential_create_LJ126_switch(double a, double b, double A, double B, double s, double tol);
+struct potential *potential_create_LJ126_Ewald(double a, double b, double A, double B, double q, double kappa, double tol);
+struct potential *potential_create_LJ126_Coulomb(double a, double b, double A, double B, double q, double tol);
+struct potential *potential_create_Ewald(double a, double b, double q, double kappa, double tol);
+struct potential *potential_create_Coulomb(double a, double b, double q, double tol);
+void potential_clear(struct potential *p);
+/* Scalar host evaluation, src/potential_eval.h:67-104. */
+void potential_eval(struct potential *p, float r2, float *e, float *f);
+
+/* ---------------------------------------------------------------- cells, tasks, space
+ * src/cell.h:58-118, src/task.h:47-88, src/space.h:65-142 (the fields drivers read). */
+struct cell {
+    unsigned int flags;
+    int id;
+    int loc[3];
+    double origin[3];
+    double dim[3];
+    int size, count;
+    struct part *parts;
+    double epot;
+    unsigned int sortmask;   /* sort directions this cell's pair tasks need */
+};
+
+enum { task_type_none = 0, task_type_self, task_type_pair, task_type_sort };
+
+struct task {
+    short int type, subtype;
+    int flags;               /* sort direction (sid) of a pair task */
+    int i, j;                /* cell indices, already flipped as by space_getsid */
+};
+
+struct space {
+    double dim[3];
+    double origin[3];
+    int cdim[3];
+    int span[3];
+    double h[3], ih[3];
+    double cutoff, cutoff2;
+    unsigned int period;
+    int nr_cells;
+    struct cell *cells;
+    int nr_tasks, tasks_size;
+    struct task *tasks;
+    struct part **partlist;
+    struct cell **celllist;
+    int nr_parts, size_parts;
+    int verlet_rebuild;
+    float maxdx;
+    double epot, epot_nonbond, epot_bond, epot_angle, epot_dihedral, epot_exclusion;
+    double ekin;
+};
+
+/* src/space.c:530-783 and src/space.c:80-114. */
+int space_init(struct space *s, const double *origin, const double *dim, double *L,
+               double cutoff, unsigned int period);
+int space_getsid(struct space *s, struct cell **ci, struct cell **cj, float *shift);
+int space_addpart(struct space *s, struct part *p, double *x);
+
+/* ---------------------------------------------------------------- exclusions, rigids
+ * src/exclusion.h:34-41 and src/rigid.h:31-52. */
+struct exclusion { int i, j; };
+#define rigid_maxparts  10
+#define rigid_maxconstr (3 * rigid_maxparts)
+struct rigid {
+    int nr_parts, nr_constr;
+    int parts[rigid_maxparts];
+    struct { int i, j; double d2; } constr[rigid_maxconstr];
+};
+
+/* ---------------------------------------------------------------- the engine
+ * Field-compatible prefix of struct engine, src/engine.h:169-302: drivers may read and
+ * write flags, s, time, dt, max_type, nr_types, types, p, nr_exclusions, tol_rigid. */
+struct nb_stats {
+    int64_t pairs;          /* unordered pairs with r2 <= rc^2, potential set, not excluded */
+    int64_t excluded;       /* excluded pairs that would otherwise have been counted */
+    int64_t candidates;     /* pairs examined by the sorted sweep (inside the projection cut) */
+    double epot;            /* FP64 nonbonded energy of the last force evaluation */
+    double virial;          /* FP64 sum over pairs of r_ij . F_ij */
+    int status;             /* device status word of the last launch (0 = ok) */
+    float ms_kernels;       /* device time of the last force evaluation (CUDA events) */
+};
+
+struct engine {
+    unsigned int flags;
+    struct space s;
+    int time;
+    double dt;
+    int max_type;
+    int nr_types;
+    struct part_type *types;
+    struct potential **p;
+    struct exclusion *exclusions;
+    int nr_exclusions, exclusions_size;
+    struct rigid *rigids;
+    int *part2rigid;
+    int nr_rigids, rigids_size, nr_constr;
+    double tol_rigid;
+    int nr_runners;
+    int device;
+    void *cuda;             /* device state, owned by the engine */
+    struct nb_stats stats;
+};
+
+/* src/engine.c:2439-2591 */
+int engine_init(struct engine *e, const double *origin, const double *dim, double *L,
+                double cutoff, unsigned int period, int max_type, unsigned int flags);
+/* src/engine.c:1543-1567 */
+int engine_addtype(struct engine *e, double mass, double charge, char *name, char *name2);
+/* src/engine.c:1584-1600 */
+int engine_addpot(struct engine *e, struct potential *p, int i, int j);
+/* src/engine.c:1345-1392 */
+int engine_load(struct engine *e, double *x, double *v, int *type, int *pid, int *vid,
+                double *q, unsigned int *flags, int N);
+/* src/engine.c:1076-1145 */
+int engine_unload(struct engine *e, double *x, double *v, int *type, int *pid, int *vid,
+                  double *q, unsigned int *flags, double *epot, int N);
+/* src/engine_bonded.c:1400-1440 and :1301-1390 */
+int engine_exclusion_add(struct engine *e, int i, int j);
+int engine_exclusion_shrink(struct engine *e);
+/* src/engine_rigid.c:78-229 */
+int engine_rigid_add(struct engine *e, int pid, int pjd, double d);
+/* src/engine.c:1674-1826 */
+int engine_start(struct engine *e, int nr_runners, int nr_queues);
+/* src/engine.c:2070-2240 */
+int engine_step(struct engine *e);
+/* src/engine.c:1945-2052 */
+int engine_advance(struct engine *e);
+/* src/engine.c:2338-2430 */
+int engine_finalize(struct engine *e);
+
+/* ---------------------------------------------------------------- GPU entry points
+ * The two functions src/engine.c calls when engine_flag_cuda is set, plus the device
+ * selection and particle load/unload helpers of src/runner_cuda.cu / src/engine_cuda.cu. */
+/* src/runner_cuda.cu:2931-3545: upload tables, cell geometry, task list. */
+int engine_cuda_load(struct engine *e);
+/* src/runner_cuda.cu:2287-2628: one nonbonded force evaluation; packs the cells' particles,
+ * copies them to the device, sorts, sweeps, and copies forces and energy back into
+ * the cells (f += nonbonded force; cell epot and s.epot_nonbond updated). */
+int engine_nonbond_cuda(struct engine *e);
+/* src/runner_cuda.cu:2641-2825 */
+int engine_cuda_load_parts(struct engine *e);
+int engine_cuda_unload_parts(struct engine *e);
+/* src/engine_cuda.cu:109-167 */
+int engine_cuda_setdevice(struct engine *e, int id);
+int engine_cuda_setdevices(struct engine *e, int nr_devices, int *ids);
+
+/* ---------------------------------------------------------------- extensions
+ * No counterpart in the reference. */
+
+/* sizeof(struct engine), for foreign-function callers that allocate it themselves. */
+size_t engine_sizeof(void);
+/* Forces by particle id (N x 3 doubles), as accumulated by the last step. */
+int engine_getforces(struct engine *e, double *f, int N);
+/* Cell index of each particle by id. */
+int engine_getcells(struct engine *e, int *cell, int N);
+/* Counters and FP64 sums of the last nonbonded evaluation. */
+int engine_nonbond_stats(struct engine *e, struct nb_stats *out);
+/* The sorted key lists the device built in the last evaluation for cell cid
+ * (13 x count entries, sid-major, same key format as src/runner_dosort.c:148-149). */
+int engine_cuda_getsort(struct engine *e, int cid, unsigned int *keys, int size);
+/* Device-resident force evaluation: positions already on the device (uploaded by
+ * engine_cuda_load_parts), forces left on the device.  Used to time the kernels alone. */
+int engine_nonbond_cuda_resident(struct engine *e);
+/* Sets the time step (the field e->dt of a C driver). */
+int engine_set_dt(struct engine *e, double dt);
+/* Zeroes forces and energies ahead of a stand-alone engine_nonbond_cuda call. */
+int engine_zero_forces(struct engine *e);
+/* Makes later launches use this cudaStream_t (e.g. the caller framework's stream). */
+int engine_cuda_setstream(struct engine *e, void *stream);
+/* Sweep kernel launch parameters (warps per block, i-chunks per warp); 0 = autotuned. */
+int engine_cuda_settune(struct engine *e, int warps, int unroll);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

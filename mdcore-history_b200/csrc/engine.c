@@ -1,0 +1,365 @@
+/* Engine API (host side): set-up, particle load/unload, exclusions, the time step.
+ *
+ * Stands in for the parts of src/engine.c, src/engine_bonded.c and src/engine_rigid.c that
+ * the nonbonded path needs.  All force evaluation runs on the GPU through
+ * engine_nonbond_cuda (nonbond.cu); there is no CPU force path.
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include "mdcore_b200.h"
+#include "internal.h"
+
+int engine_err = engine_err_ok;
+
+static const char *engine_msg[] = {
+    "Nothing bad happened.",
+    "An unexpected NULL pointer was encountered.",
+    "A call to malloc failed, probably due to insufficient memory.",
+    "An error occured when calling a space function.",
+    "A call to a pthread routine failed.",
+    "An error occured when calling a runner function.",
+    "One or more values were outside of the allowed range.",
+    "An error occured while calling a cell function.",
+    "The computational domain is too small for the requested operation.",
+    "mdcore was not compiled with MPI.",
+    "An error occured while calling an MPI function.",
+    "An error occured when calling a bond function.",
+    "An error occured when calling an angle function.",
+    "An error occured when calling a reader function.",
+    "An error occured while interpreting the PSF file.",
+    "An error occured while interpreting the PDB file.",
+    "An error occured while interpreting the CPF file.",
+    "An error occured when calling a potential function.",
+    "An error occured when calling an exclusion function.",
+    "An error occured while computing the bonded sets.",
+    "An error occured when calling a dihedral funtion.",
+    "An error occured when calling a CUDA funtion.",
+    "mdcore was not compiled with CUDA support.",
+    "CUDA support is only available in single-precision.",
+    "Max. number of parts per cell exceeded.",
+    "An error occured when calling a queue funtion.",
+    "An error occured when evaluating a rigid constraint.",
+    "Cell cutoff size doesn't work with METIS",
+    "METIS library undefined",
+    "Dependencies could not be computed.",
+    "Not yet implemented."
+};
+#define engine_error(id) (engine_err = errs_register((id), engine_msg[-(id)], __LINE__, __func__, __FILE__))
+
+/* Flags this engine implements (others are refused with engine_err_nyi). */
+#define ENGINE_FLAGS_SUPPORTED                                                                 \
+    (engine_flag_static | engine_flag_localparts | engine_flag_cuda | engine_flag_verlet |     \
+     engine_flag_verlet_pairwise | engine_flag_affinity | engine_flag_prefetch |               \
+     engine_flag_verlet_pseudo | engine_flag_unsorted | engine_flag_shake | engine_flag_nullpart)
+
+size_t engine_sizeof(void) { return sizeof(struct engine); }
+
+int engine_init(struct engine *e, const double *origin, const double *dim, double *L,
+                double cutoff, unsigned int period, int max_type, unsigned int flags) {
+    if (e == NULL || origin == NULL || dim == NULL || L == NULL) return engine_error(engine_err_null);
+    if (flags & ~ENGINE_FLAGS_SUPPORTED) return engine_error(engine_err_nyi);
+    memset(e, 0, sizeof(struct engine));
+    if (space_init(&e->s, origin, dim, L, cutoff, period) < 0) return engine_error(engine_err_space);
+    /* Flag implications of src/engine.c:2458-2463. */
+    if (flags & engine_flag_verlet_pseudo) flags |= engine_flag_verlet_pairwise;
+    if (flags & engine_flag_verlet_pairwise) flags |= engine_flag_verlet;
+    e->flags = flags;
+    e->time = 0;
+    e->dt = 0.0;
+    e->device = 0;
+    if (flags & engine_flag_nullpart) max_type += 1;
+    e->max_type = max_type;
+    e->nr_types = 0;
+    e->types = calloc(max_type, sizeof(struct part_type));
+    e->p = calloc((size_t)max_type * max_type, sizeof(struct potential *));
+    e->exclusions_size = 100;
+    e->exclusions = malloc(sizeof(struct exclusion) * e->exclusions_size);
+    e->rigids_size = 100;
+    e->rigids = malloc(sizeof(struct rigid) * e->rigids_size);
+    if (e->types == NULL || e->p == NULL || e->exclusions == NULL || e->rigids == NULL)
+        return engine_error(engine_err_malloc);
+    e->tol_rigid = 1e-6;
+    if (flags & engine_flag_nullpart) {
+        /* Type 0 is the interaction-free NULL type (src/engine.c:2517-2533). */
+        strcpy(e->types[0].name, "NULL");
+        strcpy(e->types[0].name2, "NULL");
+        e->nr_types = 1;
+    }
+    return engine_err_ok;
+}
+
+int engine_addtype(struct engine *e, double mass, double charge, char *name, char *name2) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (e->nr_types >= e->max_type) return engine_error(engine_err_range);
+    struct part_type *t = &e->types[e->nr_types];
+    t->id = e->nr_types;
+    t->mass = mass;
+    t->imass = 1.0 / mass;
+    t->charge = charge;
+    strncpy(t->name, name ? name : "X", sizeof(t->name) - 1);
+    strncpy(t->name2, name2 ? name2 : "X", sizeof(t->name2) - 1);
+    return e->nr_types++;
+}
+
+int engine_addpot(struct engine *e, struct potential *p, int i, int j) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (i < 0 || i >= e->max_type || j < 0 || j >= e->max_type) return engine_error(engine_err_range);
+    e->p[i * e->max_type + j] = p;
+    if (i != j) e->p[j * e->max_type + i] = p;
+    return engine_err_ok;
+}
+
+int engine_load(struct engine *e, double *x, double *v, int *type, int *pid, int *vid,
+                double *q, unsigned int *flags, int N) {
+    struct part p;
+    if (e == NULL || x == NULL || type == NULL) return engine_error(engine_err_null);
+    memset(&p, 0, sizeof(p));
+    for (int j = 0; j < N; j++) {
+        if (type[j] < 0 || type[j] >= e->max_type) return engine_error(engine_err_range);
+        p.type = type[j];
+        p.id = pid ? pid[j] : j;
+        p.vid = vid ? vid[j] : 0;
+        p.flags = flags ? flags[j] : part_flag_none;
+        for (int k = 0; k < 3; k++) {
+            p.v[k] = v ? v[3 * j + k] : 0.0;
+            p.f[k] = 0.0f;
+        }
+        p.q = q ? q[j] : 0.0;
+        if (space_addpart(&e->s, &p, &x[3 * j]) < 0) return engine_error(engine_err_space);
+    }
+    return engine_err_ok;
+}
+
+int engine_unload(struct engine *e, double *x, double *v, int *type, int *pid, int *vid,
+                  double *q, unsigned int *flags, double *epot, int N) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    int total = 0;
+    for (int c = 0; c < s->nr_cells; c++) total += s->cells[c].count;
+    if (total > N) return engine_error(engine_err_range);
+    int count = 0;
+    double ep = 0.0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell *cl = &s->cells[c];
+        ep += cl->epot;
+        for (int k = 0; k < cl->count; k++, count++) {
+            struct part *p = &cl->parts[k];
+            if (x)
+                for (int j = 0; j < 3; j++) x[3 * count + j] = cl->origin[j] + p->x[j];
+            if (v)
+                for (int j = 0; j < 3; j++) v[3 * count + j] = p->v[j];
+            if (type) type[count] = p->type;
+            if (pid) pid[count] = p->id;
+            if (vid) vid[count] = p->vid;
+            if (q) q[count] = p->q;
+            if (flags) flags[count] = p->flags;
+        }
+    }
+    if (epot) *epot += ep;
+    return count;
+}
+
+int engine_getforces(struct engine *e, double *f, int N) {
+    if (e == NULL || f == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    for (int id = 0; id < N; id++) {
+        if (id >= s->size_parts || s->partlist[id] == NULL) {
+            f[3 * id] = f[3 * id + 1] = f[3 * id + 2] = 0.0;
+            continue;
+        }
+        for (int k = 0; k < 3; k++) f[3 * id + k] = s->partlist[id]->f[k];
+    }
+    return engine_err_ok;
+}
+
+int engine_getcells(struct engine *e, int *cell, int N) {
+    if (e == NULL || cell == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    for (int id = 0; id < N; id++)
+        cell[id] = (id < s->size_parts && s->celllist[id]) ? (int)(s->celllist[id] - s->cells) : -1;
+    return engine_err_ok;
+}
+
+int engine_nonbond_stats(struct engine *e, struct nb_stats *out) {
+    if (e == NULL || out == NULL) return engine_error(engine_err_null);
+    *out = e->stats;
+    return engine_err_ok;
+}
+
+/* ---------------------------------------------------------------- exclusions */
+
+int engine_exclusion_add(struct engine *e, int i, int j) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (e->nr_exclusions == e->exclusions_size) {
+        int nsize = e->exclusions_size * 2;
+        struct exclusion *ne = realloc(e->exclusions, sizeof(struct exclusion) * nsize);
+        if (ne == NULL) return engine_error(engine_err_malloc);
+        e->exclusions = ne;
+        e->exclusions_size = nsize;
+    }
+    struct exclusion *x = &e->exclusions[e->nr_exclusions++];
+    x->i = i < j ? i : j;
+    x->j = i < j ? j : i;
+    return engine_err_ok;
+}
+
+static int excl_cmp(const void *a, const void *b) {
+    const struct exclusion *x = a, *y = b;
+    if (x->i != y->i) return x->i < y->i ? -1 : 1;
+    if (x->j != y->j) return x->j < y->j ? -1 : 1;
+    return 0;
+}
+
+/* Sort by (i, j) and drop duplicates, as src/engine_bonded.c:1301-1390. */
+int engine_exclusion_shrink(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (e->nr_exclusions == 0) return engine_err_ok;
+    qsort(e->exclusions, e->nr_exclusions, sizeof(struct exclusion), excl_cmp);
+    int j = 0;
+    for (int k = 1; k < e->nr_exclusions; k++)
+        if (e->exclusions[k].i != e->exclusions[j].i || e->exclusions[k].j != e->exclusions[j].j)
+            e->exclusions[++j] = e->exclusions[k];
+    e->nr_exclusions = j + 1;
+    return engine_err_ok;
+}
+
+/* ---------------------------------------------------------------- rigid constraints */
+
+int engine_rigid_add(struct engine *e, int pid, int pjd, double d) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (pid < 0 || pjd < 0 || pid == pjd) return engine_error(engine_err_range);
+    int need = (pid > pjd ? pid : pjd) + 1;
+    if (e->part2rigid == NULL || need > e->s.size_parts) {
+        int nsize = need > e->s.size_parts ? need : e->s.size_parts;
+        int *np = realloc(e->part2rigid, sizeof(int) * nsize);
+        if (np == NULL) return engine_error(engine_err_malloc);
+        /* Only entries past what was there before need initialising. */
+        static int known = 0;
+        if (e->part2rigid == NULL) known = 0;
+        for (int k = known; k < nsize; k++) np[k] = -1;
+        known = nsize;
+        e->part2rigid = np;
+    }
+    int ri = e->part2rigid[pid], rj = e->part2rigid[pjd];
+    struct rigid *r;
+    if (ri < 0 && rj < 0) {
+        if (e->nr_rigids == e->rigids_size) {
+            int nsize = e->rigids_size * 2;
+            struct rigid *nr = realloc(e->rigids, sizeof(struct rigid) * nsize);
+            if (nr == NULL) return engine_error(engine_err_malloc);
+            e->rigids = nr;
+            e->rigids_size = nsize;
+        }
+        r = &e->rigids[e->nr_rigids];
+        memset(r, 0, sizeof(*r));
+        e->part2rigid[pid] = e->part2rigid[pjd] = e->nr_rigids++;
+        r->parts[r->nr_parts++] = pid;
+        r->parts[r->nr_parts++] = pjd;
+    } else if (ri >= 0 && rj >= 0 && ri != rj) {
+        return engine_error(engine_err_nyi);   /* merging two rigid groups */
+    } else {
+        int g = ri >= 0 ? ri : rj;
+        r = &e->rigids[g];
+        int add = ri >= 0 ? pjd : pid;
+        if (e->part2rigid[add] < 0) {
+            if (r->nr_parts >= rigid_maxparts) return engine_error(engine_err_range);
+            r->parts[r->nr_parts++] = add;
+            e->part2rigid[add] = g;
+        }
+    }
+    if (r->nr_constr >= rigid_maxconstr) return engine_error(engine_err_range);
+    r->constr[r->nr_constr].i = pid;
+    r->constr[r->nr_constr].j = pjd;
+    r->constr[r->nr_constr].d2 = d * d;
+    r->nr_constr++;
+    e->nr_constr++;
+    return engine_err_ok;
+}
+
+/* ---------------------------------------------------------------- running */
+
+int engine_start(struct engine *e, int nr_runners, int nr_queues) {
+    (void)nr_queues;
+    if (e == NULL) return engine_error(engine_err_null);
+    e->nr_runners = nr_runners;
+    if (engine_cuda_load(e) < 0) return engine_error(engine_err_cuda);
+    return engine_err_ok;
+}
+
+/* Symplectic Euler update v += f/m dt, x += v dt, as src/engine.c:1945-2052; particles
+ * that leave their cell are moved at the start of the next step. */
+int engine_advance(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    float dt = e->dt;
+    double epot = 0.0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell *cl = &s->cells[c];
+        epot += cl->epot;
+        for (int k = 0; k < cl->count; k++) {
+            struct part *p = &cl->parts[k];
+            float w = dt * e->types[p->type].imass;
+            for (int j = 0; j < 3; j++) {
+                p->v[j] += p->f[j] * w;
+                p->x[j] += dt * p->v[j];
+            }
+        }
+    }
+    (void)epot;
+    return engine_err_ok;
+}
+
+int engine_step(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    e->time += 1;
+    if (space_shuffle(s) < 0) return engine_error(engine_err_space);
+    s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell *cl = &s->cells[c];
+        cl->epot = 0.0;
+        for (int k = 0; k < cl->count; k++) cl->parts[k].f[0] = cl->parts[k].f[1] = cl->parts[k].f[2] = 0.0f;
+    }
+    if (engine_nonbond_cuda(e) < 0) return engine_error(engine_err_cuda);
+    s->epot += s->epot_nonbond;
+    if (engine_advance(e) < 0) return engine_error(engine_err);
+    return engine_err_ok;
+}
+
+int engine_finalize(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    nb_device_free(e);
+    for (int c = 0; c < e->s.nr_cells; c++) free(e->s.cells[c].parts);
+    free(e->s.cells);
+    free(e->s.tasks);
+    free(e->s.partlist);
+    free(e->s.celllist);
+    free(e->types);
+    free(e->p);
+    free(e->exclusions);
+    free(e->rigids);
+    free(e->part2rigid);
+    memset(e, 0, sizeof(struct engine));
+    return engine_err_ok;
+}
+
+int engine_set_dt(struct engine *e, double dt) {
+    if (e == NULL) return engine_error(engine_err_null);
+    e->dt = dt;
+    return engine_err_ok;
+}
+
+/* Zeroes forces and energies before a stand-alone force evaluation (what space_prepare,
+ * src/space.c:186-219, does at the start of a step). */
+int engine_zero_forces(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell *cl = &s->cells[c];
+        cl->epot = 0.0;
+        for (int k = 0; k < cl->count; k++) cl->parts[k].f[0] = cl->parts[k].f[1] = cl->parts[k].f[2] = 0.0f;
+    }
+    return engine_err_ok;
+}

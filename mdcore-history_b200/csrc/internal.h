@@ -1,0 +1,30 @@
+/* Declarations shared by the host sources of libmdcore_b200 (not part of the public ABI). */
+#ifndef MDCORE_B200_INTERNAL_H
+#define MDCORE_B200_INTERNAL_H
+
+#include "mdcore_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define space_cellid(s, i, j, k) ((((i) * (s)->cdim[1] + (j)) * (s)->cdim[2]) + (k))
+
+/* Unit vector of sort direction sid (the values of cell_shift, src/cell.c:84-98). */
+void sort_axis(int sid, float n[3]);
+struct part *cell_add(struct cell *c, const struct part *p);
+void space_relink(struct space *s, struct cell *c);
+int space_shuffle(struct space *s);
+
+void nb_sweep_scales(const struct space *s, float *bias, float *dscale, int *dmaxdist);
+int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dnshift, int *ci_out,
+                  int *cj_out);
+
+/* Device side (nonbond.cu). */
+int nb_device_free(struct engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

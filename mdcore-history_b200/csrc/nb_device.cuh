@@ -1,0 +1,129 @@
+// Device-side data layout and small PTX helpers of the nonbonded engine (sm_100a).
+//
+// Particle data in HBM is cell-major: cell c owns the slots [start[c], start[c]+count[c])
+// of every per-particle array, with start[c] a multiple of 4 so that every cell's block
+// of 4-byte and 16-byte records starts on a 16-byte boundary and can be moved into shared
+// memory with one cp.async.bulk (TMA bulk copy) per array.
+//
+//   xq[slot]    float4  {x, y, z} relative to the cell origin (the reference's FPTYPE
+//                       cell-local coordinates, src/space.c:421-423) and w = type (int bits)
+//   pid[slot]   int     global particle id
+//   keys[13*start[c] + sid*cpad[c] + k]   uint32 sort keys of cell c along direction sid,
+//                       (k_local << 16) | projected distance (src/runner_dosort.c:148-149),
+//                       sorted by descending distance; cpad[c] = count rounded up to 4.
+//   force[3*slot+k]  int64 fixed-point force, 2^24 units per kJ/mol/nm.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nb {
+
+constexpr float kForceScale = 16777216.0f;          // 2^24
+constexpr double kEnergyScale = 4294967296.0;       // 2^32
+constexpr int kMaxPartsPerCell = 1024;
+constexpr int kSpinLimit = 1 << 22;                 // bounded waits
+
+// Status bits of the device status word.
+enum : unsigned {
+    kStatusOk = 0,
+    kStatusCopyTimeout = 1u,
+    kStatusCellOverflow = 2u,
+    kStatusTableIndex = 4u,
+    kStatusForceOverflow = 8u,
+};
+
+// Accumulator slots (unsigned long long each).
+enum { kAccEpot = 0, kAccVirial, kAccPairs, kAccExcl, kAccCand, kAccStatus, kAccCount = 8 };
+
+struct TaskRec {        // one cell pair (or self) task
+    int ci, cj, sid, dnshift;     // sid = -1 for self tasks
+};
+
+struct Params {
+    const float4* xq;
+    const int* pid;
+    const unsigned* keys;
+    const int* cstart;
+    const int* ccount;
+    unsigned long long* force;
+    unsigned long long* acc;
+    unsigned long long* cell_epot;  // per-cell fixed-point energy (2^32 units per kJ/mol)
+    const TaskRec* tasks;
+    const float4* tshift;       // per-task shift of cell j relative to cell i
+    int ntasks;
+    const float* coef;          // concatenated tables, (n+1)*8 floats each
+    const float4* potinfo;      // {alpha0, alpha1, alpha2, int_bits(offset of chunk 0)}
+    const int* potn;            // n of each table (largest valid chunk index)
+    const int* potidx;          // max_type*max_type -> table index or -1
+    int max_type, npots, ncoef;
+    const unsigned* emask;      // by particle id: excluded partners at id offsets +-1..16
+    const int* exoff;           // by particle id: CSR of the other excluded partners
+    const int* exlist;
+    float cutoff2;              // pair tasks: float(cutoff)^2 in float (src/runner_dopair.c:578-579)
+    float cutoff2s;             // self tasks: float(cutoff^2) (src/runner_dopair.c:896)
+    int dmaxdist;
+    int unsorted;               // 1: sweep every candidate (engine_flag_unsorted)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// One-dimensional TMA bulk copy global -> shared, completion counted on `bar`.
+// dst and src must be 16-byte aligned and bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for phase `parity` of `bar` to complete, at most kSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < kSpinLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Float -> 64-bit fixed point, flagging values outside the representable range.
+__device__ __forceinline__ long long to_fixed(float v, unsigned& status) {
+    float s = v * kForceScale;
+    if (!(fabsf(s) < 9.0e18f)) status |= kStatusForceOverflow;
+    return __float2ll_rn(s);
+}
+
+__device__ __forceinline__ void atomic_add_fixed(unsigned long long* p, long long v) {
+    if (v != 0) atomicAdd(p, static_cast<unsigned long long>(v));
+}
+
+}  // namespace nb

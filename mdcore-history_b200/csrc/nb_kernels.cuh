@@ -1,0 +1,388 @@
+// Sort and sorted-sweep kernels of the nonbonded engine (sm_100a).
+//
+// sort_cells   : runner_dosort (src/runner_dosort.c:97-161) -- one CTA per cell builds the
+//                13 projected-distance key lists the cell's pair tasks need and orders
+//                them by descending distance (a stable rank sort: ties keep storage order).
+// sweep_tasks  : runner_dopair_vec / runner_doself_vec (src/runner_dopair.c:540-741,
+//                858-1029) with potential_eval (src/potential_eval.h:67-104) -- one CTA per
+//                cell-pair task; the two cells' particle blocks and sort keys are moved
+//                into shared memory with TMA bulk copies, each warp sweeps 32 consecutive
+//                sorted i particles against the j list in ascending projected distance,
+//                stopping at the reference's projection bound, and Newton's third law is
+//                applied inside the CTA: the j force of every pair is summed over the warp
+//                by shuffles and over the warps in a fixed order, so every task produces
+//                the same FP32 partial forces whatever order the tasks run in; partials are
+//                converted once per particle and task to 64-bit fixed point and added with
+//                integer atomics.
+#pragma once
+#include "nb_device.cuh"
+
+namespace nb {
+
+__constant__ float c_axes[13][3];
+
+// ---------------------------------------------------------------- sort
+__global__ void __launch_bounds__(256) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+                                                  const int* __restrict__ ccount, const unsigned* __restrict__ cmask,
+                                                  unsigned* __restrict__ keys, float dscale, float bias,
+                                                  unsigned long long* acc) {
+    extern __shared__ unsigned skey[];
+    const int c = blockIdx.x;
+    const int n = ccount[c];
+    if (n <= 0) return;
+    if (n > kMaxPartsPerCell) {
+        if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
+        return;
+    }
+    const int start = cstart[c];
+    const int pad = (n + 3) & ~3;
+    const unsigned mask = cmask[c];
+    for (int sid = 0; sid < 13; ++sid) {
+        if (!((mask >> sid) & 1u)) continue;
+        const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const float4 x = xq[start + k];
+            // dscale * (bias + x.n), evaluated left to right without contraction.
+            float d = __fadd_rn(bias, __fmul_rn(x.x, nx));
+            d = __fadd_rn(d, __fmul_rn(x.y, ny));
+            d = __fadd_rn(d, __fmul_rn(x.z, nz));
+            d = __fmul_rn(dscale, d);
+            skey[k] = ((unsigned)k << 16) | __float2uint_rz(d);
+        }
+        __syncthreads();
+        unsigned* out = keys + 13 * (size_t)start + (size_t)sid * pad;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const unsigned mine = skey[k];
+            const unsigned md = mine & 0xffffu;
+            int rank = 0;
+            for (int m = 0; m < n; ++m) {
+                const unsigned od = skey[m] & 0xffffu;
+                rank += (od > md) | ((od == md) & (m < k));
+            }
+            out[rank] = mine;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- potential evaluation
+// Interval index as the reference computes it (no contraction, so it matches the host
+// table construction), Horner recurrences with fused multiply-adds.
+__device__ __forceinline__ void eval_table(const float* __restrict__ coef, float4 info, int nmax, float r2,
+                                           float& e, float& f, unsigned& status) {
+    const float r = __fsqrt_rn(r2);
+    float t = __fadd_rn(info.x, __fmul_rn(r, __fadd_rn(info.y, __fmul_rn(r, info.z))));
+    int ind = __float2int_rz(fmaxf(0.0f, t));
+    if (ind > nmax) {
+        status |= kStatusTableIndex;
+        ind = nmax;
+    }
+    const float4* c = reinterpret_cast<const float4*>(coef + __float_as_int(info.w) + 8 * ind);
+    const float4 c0 = c[0], c1 = c[1];
+    const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
+    float ee = fmaf(c0.z, x, c0.w);
+    float eff = c0.z;
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.x);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.y);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.z);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.w);
+    e = ee;
+    f = __fdiv_rn(eff * c0.y, r);
+}
+
+__device__ __forceinline__ bool excluded_pair(int pi, int pj, unsigned emask, int exlo, int exhi,
+                                              const int* __restrict__ exlist) {
+    const int d = pj - pi;
+    if (d >= -16 && d <= 16) {
+        if (d == 0) return false;
+        const int bit = (d < 0) ? d + 16 : d + 15;
+        return (emask >> bit) & 1u;
+    }
+    for (int k = exlo; k < exhi; ++k)
+        if (exlist[k] == pj) return true;
+    return false;
+}
+
+// Shared-memory carve-up of one sweep CTA; cap = largest cell (multiple of 4).
+struct SweepSmem {
+    uint64_t* bar;
+    float4 *xi, *xj, *js, *fj, *fi;
+    int *pidi, *pidj, *jd, *jid, *jloc, *potidx, *potn;
+    unsigned *keyi, *keyj;
+    float* coef;
+    float4* potinfo;
+    double* wred;
+    unsigned long long* cred;
+};
+
+__host__ __device__ inline size_t sweep_smem_bytes(int cap, int nw, int ncoef, int npots, int mt) {
+    size_t b = 16;                                  // mbarrier
+    b += (size_t)cap * 16 * 4;                      // xi, xj, js, fi
+    b += (size_t)nw * cap * 16;                     // per-warp j partial forces
+    b += (size_t)cap * 4 * 7;                       // pidi, pidj, keyi, keyj, jd, jid, jloc
+    b += (size_t)npots * 16;                        // potinfo
+    b += (size_t)((ncoef + 3) & ~3) * 4;            // coef
+    b += (size_t)((npots + 3) & ~3) * 4;            // potn
+    b += (size_t)((mt * mt + 3) & ~3) * 4;          // potidx
+    b += (size_t)nw * 16 + (size_t)nw * 32;         // reductions
+    return b;
+}
+
+__device__ inline SweepSmem carve(unsigned char* base, int cap, int nw, int ncoef, int npots, int mt) {
+    SweepSmem s;
+    unsigned char* p = base;
+    s.bar = reinterpret_cast<uint64_t*>(p); p += 16;
+    s.xi = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
+    s.xj = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
+    s.js = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
+    s.fi = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
+    s.fj = reinterpret_cast<float4*>(p); p += (size_t)nw * cap * 16;
+    s.potinfo = reinterpret_cast<float4*>(p); p += (size_t)npots * 16;
+    s.pidi = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
+    s.pidj = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
+    s.keyi = reinterpret_cast<unsigned*>(p); p += (size_t)cap * 4;
+    s.keyj = reinterpret_cast<unsigned*>(p); p += (size_t)cap * 4;
+    s.jd = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
+    s.jid = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
+    s.jloc = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
+    s.coef = reinterpret_cast<float*>(p); p += (size_t)((ncoef + 3) & ~3) * 4;
+    s.potn = reinterpret_cast<int*>(p); p += (size_t)((npots + 3) & ~3) * 4;
+    s.potidx = reinterpret_cast<int*>(p); p += (size_t)((mt * mt + 3) & ~3) * 4;
+    s.wred = reinterpret_cast<double*>(p); p += (size_t)nw * 16;
+    s.cred = reinterpret_cast<unsigned long long*>(p);
+    return s;
+}
+
+// ---------------------------------------------------------------- sweep
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr unsigned FULL = 0xffffffffu;
+    const int t = blockIdx.x;
+    const TaskRec tr = P.tasks[t];
+    const bool self = tr.sid < 0;
+    const int ci = tr.ci, cj = tr.cj;
+    const int ni = P.ccount[ci], nj = P.ccount[cj];
+    if (ni == 0 || nj == 0 || (self && ni < 2)) return;
+    if (ni > cap || nj > cap) {
+        if (threadIdx.x == 0) atomicOr(&P.acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
+        return;
+    }
+    const int si = P.cstart[ci], sj = P.cstart[cj];
+    const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
+    const int mt = P.max_type;
+    SweepSmem S = carve(smem_raw, cap, NW, P.ncoef, P.npots, mt);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // Stage the cells with TMA bulk copies; the tables with ordinary loads meanwhile.
+    if (tid == 0) {
+        mbar_init(S.bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = self ? (uint32_t)padj * 20u : (uint32_t)(padi + padj) * 24u;
+        mbar_arrive_expect_tx(S.bar, bytes);
+        bulk_g2s(S.xj, P.xq + sj, padj * 16, S.bar);
+        bulk_g2s(S.pidj, P.pid + sj, padj * 4, S.bar);
+        if (!self) {
+            bulk_g2s(S.keyj, P.keys + 13 * (size_t)sj + (size_t)tr.sid * padj, padj * 4, S.bar);
+            bulk_g2s(S.xi, P.xq + si, padi * 16, S.bar);
+            bulk_g2s(S.pidi, P.pid + si, padi * 4, S.bar);
+            bulk_g2s(S.keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, S.bar);
+        }
+    }
+    for (int k = tid; k < P.ncoef; k += NW * 32) S.coef[k] = P.coef[k];
+    for (int k = tid; k < P.npots; k += NW * 32) {
+        S.potinfo[k] = P.potinfo[k];
+        S.potn[k] = P.potn[k];
+    }
+    for (int k = tid; k < mt * mt; k += NW * 32) S.potidx[k] = P.potidx[k];
+    for (int k = tid; k < NW * cap; k += NW * 32) S.fj[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool arrived = mbar_wait_bounded(S.bar, 0);
+    if (__syncthreads_or(!arrived)) {
+        if (tid == 0) atomicOr(&P.acc[kAccStatus], (unsigned long long)kStatusCopyTimeout);
+        mbar_wait_bounded(S.bar, 0);  // give copies still in flight a second bounded chance
+        return;
+    }
+
+    // j list in ascending projected distance from cell i (the reference walks its
+    // descending list from the far end, src/runner_dopair.c:616-618).
+    if (!self) {
+        for (int k = tid; k < nj; k += NW * 32) {
+            const unsigned key = S.keyj[nj - 1 - k];
+            const int loc = key >> 16;
+            S.js[k] = S.xj[loc];
+            S.jd[k] = key & 0xffff;
+            S.jid[k] = S.pidj[loc];
+            S.jloc[k] = loc;
+        }
+    }
+    __syncthreads();
+
+    const float4* __restrict__ jpos = self ? S.xj : S.js;
+    const int* __restrict__ jids = self ? S.pidj : S.jid;
+    const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
+    const int dnshift = tr.dnshift;
+    const float cut2 = self ? P.cutoff2s : P.cutoff2;
+    float4* myfj = S.fj + warp * cap;
+    double epot = 0.0, vir = 0.0;
+    unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
+
+    const int nchunks = (ni + 31) >> 5;
+    for (int ch = warp; ch < nchunks; ch += NW) {
+        const int ii = ch * 32 + lane;
+        bool valid = ii < ni;
+        int loc = ii, di = 0;
+        if (!self) {
+            const unsigned key = valid ? S.keyi[ii] : 0u;
+            loc = key >> 16;
+            di = key & 0xffff;
+            // Quit-early test of the reference i loop (src/runner_dopair.c:600-602).
+            if (!P.unsorted) valid = valid && (S.jd[0] + dnshift - di <= P.dmaxdist);
+            if (!__any_sync(FULL, valid)) break;   // later chunks lie farther from cell j
+        }
+        float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+        int pidi = -1;
+        unsigned emask = 0u;
+        int exlo = 0, exhi = 0;
+        if (valid) {
+            xi = self ? S.xj[loc] : S.xi[loc];
+            pidi = self ? S.pidj[loc] : S.pidi[loc];
+            emask = P.emask[pidi];
+            exlo = P.exoff[pidi];
+            exhi = P.exoff[pidi + 1];
+        }
+        const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
+        const int prow = __float_as_int(xi.w) * mt;
+        const int lim = P.dmaxdist - dnshift + di;
+        const int kend = self ? min(ch * 32 + 32, ni) - 1 : nj;
+        float fix = 0.f, fiy = 0.f, fiz = 0.f;
+        for (int k = 0; k < kend; ++k) {
+            bool act;
+            if (self) {
+                act = valid && (k < ii);
+            } else {
+                act = valid && (P.unsorted || S.jd[k] < lim);
+                if (!__any_sync(FULL, act)) break;
+            }
+            const float4 xj = jpos[k];
+            const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
+            const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            const int pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
+            bool acc = act && pot >= 0 && r2 <= cut2;
+            ncand += act;
+            if (acc && excluded_pair(pidi, jids[k], emask, exlo, exhi, P.exlist)) {
+                acc = false;
+                ++nexcl;
+            }
+            if (__any_sync(FULL, acc)) {
+                float wx = 0.f, wy = 0.f, wz = 0.f;
+                if (acc) {
+                    float e, f;
+                    eval_table(S.coef, S.potinfo[pot], S.potn[pot], r2, e, f, status);
+                    wx = f * dx; wy = f * dy; wz = f * dz;
+                    fix -= wx; fiy -= wy; fiz -= wz;
+                    epot += (double)e;
+                    vir += (double)(f * r2);
+                    ++npairs;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    wx += __shfl_xor_sync(FULL, wx, o);
+                    wy += __shfl_xor_sync(FULL, wy, o);
+                    wz += __shfl_xor_sync(FULL, wz, o);
+                }
+                if (lane == 0) {
+                    float4 a = myfj[k];
+                    a.x += wx; a.y += wy; a.z += wz;
+                    myfj[k] = a;
+                }
+            }
+        }
+        if (valid) {
+            if (self) {
+                S.fi[loc] = make_float4(fix, fiy, fiz, 0.f);
+            } else {
+                unsigned long long* fp = P.force + 3 * (size_t)(si + loc);
+                atomic_add_fixed(fp + 0, to_fixed(fix, status));
+                atomic_add_fixed(fp + 1, to_fixed(fiy, status));
+                atomic_add_fixed(fp + 2, to_fixed(fiz, status));
+            }
+        }
+    }
+    __syncwarp();
+
+    // Energy, virial and counters: warp sums, then warps in a fixed order.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        epot += __shfl_xor_sync(FULL, epot, o);
+        vir += __shfl_xor_sync(FULL, vir, o);
+        npairs += __shfl_xor_sync(FULL, npairs, o);
+        nexcl += __shfl_xor_sync(FULL, nexcl, o);
+        ncand += __shfl_xor_sync(FULL, ncand, o);
+        status |= __shfl_xor_sync(FULL, status, o);
+    }
+    if (lane == 0) {
+        S.wred[2 * warp] = epot;
+        S.wred[2 * warp + 1] = vir;
+        S.cred[4 * warp] = npairs;
+        S.cred[4 * warp + 1] = nexcl;
+        S.cred[4 * warp + 2] = ncand;
+        S.cred[4 * warp + 3] = status;
+    }
+    __syncthreads();
+
+    // j forces (and, for self tasks, i forces) summed over warps in order.
+    if (self) {
+        for (int k = tid; k < ni; k += NW * 32) {
+            float4 a = S.fi[k];
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                const float4 b = S.fj[w * cap + k];
+                a.x += b.x; a.y += b.y; a.z += b.z;
+            }
+            unsigned st = 0;
+            unsigned long long* fp = P.force + 3 * (size_t)(si + k);
+            atomic_add_fixed(fp + 0, to_fixed(a.x, st));
+            atomic_add_fixed(fp + 1, to_fixed(a.y, st));
+            atomic_add_fixed(fp + 2, to_fixed(a.z, st));
+            if (st) atomicOr(&P.acc[kAccStatus], (unsigned long long)st);
+        }
+    } else {
+        for (int k = tid; k < nj; k += NW * 32) {
+            float4 a = S.fj[k];
+#pragma unroll
+            for (int w = 1; w < NW; ++w) {
+                const float4 b = S.fj[w * cap + k];
+                a.x += b.x; a.y += b.y; a.z += b.z;
+            }
+            unsigned st = 0;
+            unsigned long long* fp = P.force + 3 * (size_t)(sj + S.jloc[k]);
+            atomic_add_fixed(fp + 0, to_fixed(a.x, st));
+            atomic_add_fixed(fp + 1, to_fixed(a.y, st));
+            atomic_add_fixed(fp + 2, to_fixed(a.z, st));
+            if (st) atomicOr(&P.acc[kAccStatus], (unsigned long long)st);
+        }
+    }
+    if (tid == 0) {
+        double e = 0.0, v = 0.0;
+        unsigned long long np = 0, ne = 0, nc = 0, st = 0;
+        for (int w = 0; w < NW; ++w) {
+            e += S.wred[2 * w];
+            v += S.wred[2 * w + 1];
+            np += S.cred[4 * w];
+            ne += S.cred[4 * w + 1];
+            nc += S.cred[4 * w + 2];
+            st |= S.cred[4 * w + 3];
+        }
+        atomicAdd(&P.cell_epot[ci], (unsigned long long)__double2ll_rn(e * kEnergyScale));
+        atomicAdd(&P.acc[kAccVirial], (unsigned long long)__double2ll_rn(v * kEnergyScale));
+        if (np) atomicAdd(&P.acc[kAccPairs], np);
+        if (ne) atomicAdd(&P.acc[kAccExcl], ne);
+        if (nc) atomicAdd(&P.acc[kAccCand], nc);
+        if (st) atomicOr(&P.acc[kAccStatus], st);
+    }
+}
+
+}  // namespace nb

@@ -1,0 +1,522 @@
+// GPU entry points of the engine: engine_cuda_load (src/runner_cuda.cu:2931-3545) and
+// engine_nonbond_cuda (src/runner_cuda.cu:2287-2628), plus device selection and the
+// device-resident evaluation used to time the kernels alone.
+//
+// Per evaluation: pack the cells' particles (cell-relative float positions + type, id)
+// into pinned host buffers, one host->device copy each, zero the fixed-point force and
+// energy accumulators, sort_cells, sweep_tasks, one device->host copy of forces and
+// per-cell energies, unpack into the cells.  All launches go to one stream; CUDA events
+// around the kernels give the device time.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <cmath>
+#include <cuda_runtime.h>
+#include "mdcore_b200.h"
+#include "internal.h"
+#include "nb_kernels.cuh"
+
+using namespace nb;
+
+namespace {
+
+struct NbState {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // geometry
+    int ncells = 0, ntasks = 0, ncap = 0, nid = 0;
+    float bias = 0.f, dscale = 0.f;
+    int dmaxdist = 0;
+    int maxcount = 0;
+    // tables
+    int npots = 0, ncoef = 0, max_type = 0;
+    // tuning
+    int warps = 4;
+    // device buffers
+    float4* d_xq = nullptr;
+    int* d_pid = nullptr;
+    unsigned* d_keys = nullptr;
+    unsigned long long* d_force = nullptr;
+    int* d_cstart = nullptr;
+    int* d_ccount = nullptr;
+    unsigned* d_cmask = nullptr;
+    unsigned long long* d_acc = nullptr;
+    unsigned long long* d_cell_epot = nullptr;
+    TaskRec* d_tasks = nullptr;
+    float4* d_tshift = nullptr;
+    float* d_coef = nullptr;
+    float4* d_potinfo = nullptr;
+    int* d_potn = nullptr;
+    int* d_potidx = nullptr;
+    unsigned* d_emask = nullptr;
+    int* d_exoff = nullptr;
+    int* d_exlist = nullptr;
+    // pinned host buffers
+    float4* h_xq = nullptr;
+    int* h_pid = nullptr;
+    int* h_cstart = nullptr;    // ncells+1 followed by ncells counts
+    unsigned long long* h_force = nullptr;
+    unsigned long long* h_cell_epot = nullptr;
+    unsigned long long* h_acc = nullptr;
+    bool resident_valid = false;
+};
+
+int cuda_fail(cudaError_t err, int line, const char* func) {
+    errs_register(engine_err_cuda, cudaGetErrorString(err), line, func, __FILE__);
+    engine_err = engine_err_cuda;
+    return engine_err_cuda;
+}
+
+#define CU(call)                                                           \
+    do {                                                                   \
+        cudaError_t err_ = (call);                                         \
+        if (err_ != cudaSuccess) return cuda_fail(err_, __LINE__, __func__); \
+    } while (0)
+
+NbState* state(struct engine* e) { return static_cast<NbState*>(e->cuda); }
+
+float bits_as_float(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof(f));
+    return f;
+}
+
+template <typename T>
+int dev_alloc(T** p, size_t n) {
+    CU(cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 16));
+    return 0;
+}
+
+// (Re)allocates the per-particle buffers for `ncap` slots.
+int alloc_particles(NbState* st, int ncap) {
+    if (ncap <= st->ncap) return 0;
+    ncap = ncap + ncap / 8 + 64;
+    cudaFree(st->d_xq); cudaFree(st->d_pid); cudaFree(st->d_keys); cudaFree(st->d_force);
+    cudaFreeHost(st->h_xq); cudaFreeHost(st->h_pid); cudaFreeHost(st->h_force);
+    if (dev_alloc(&st->d_xq, ncap) || dev_alloc(&st->d_pid, ncap) || dev_alloc(&st->d_keys, 13 * (size_t)ncap) ||
+        dev_alloc(&st->d_force, 3 * (size_t)ncap))
+        return engine_err_cuda;
+    CU(cudaMallocHost(&st->h_xq, sizeof(float4) * ncap));
+    CU(cudaMallocHost(&st->h_pid, sizeof(int) * ncap));
+    CU(cudaMallocHost(&st->h_force, sizeof(unsigned long long) * 3 * ncap));
+    CU(cudaMemset(st->d_xq, 0, sizeof(float4) * ncap));
+    CU(cudaMemset(st->d_pid, 0, sizeof(int) * ncap));
+    st->ncap = ncap;
+    return 0;
+}
+
+// Packs the cells into the pinned staging buffers; returns the number of slots used.
+int pack_cells(struct engine* e, NbState* st) {
+    struct space* s = &e->s;
+    int total = 0, maxc = 0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        int n = s->cells[c].count;
+        total += (n + 3) & ~3;
+        if (n > maxc) maxc = n;
+    }
+    if (maxc > kMaxPartsPerCell) {
+        errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    if (alloc_particles(st, total + 4) < 0) return engine_err_cuda;
+    int* cstart = st->h_cstart;
+    int* ccount = st->h_cstart + s->nr_cells + 1;
+    int slot = 0;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell* cl = &s->cells[c];
+        cstart[c] = slot;
+        ccount[c] = cl->count;
+        for (int k = 0; k < cl->count; k++) {
+            const struct part* p = &cl->parts[k];
+            float4 v;
+            v.x = p->x[0]; v.y = p->x[1]; v.z = p->x[2];
+            v.w = bits_as_float((int)p->type);
+            st->h_xq[slot + k] = v;
+            st->h_pid[slot + k] = p->id;
+        }
+        int pad = (cl->count + 3) & ~3;
+        for (int k = cl->count; k < pad; k++) {
+            st->h_xq[slot + k] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
+            st->h_pid[slot + k] = 0;
+        }
+        slot += pad;
+    }
+    cstart[s->nr_cells] = slot;
+    st->maxcount = maxc;
+    return slot;
+}
+
+int launch_kernels(struct engine* e, NbState* st) {
+    struct space* s = &e->s;
+    CU(cudaMemsetAsync(st->d_force, 0, sizeof(unsigned long long) * 3 * (size_t)st->h_cstart[s->nr_cells],
+                       st->stream));
+    CU(cudaMemsetAsync(st->d_acc, 0, sizeof(unsigned long long) * kAccCount, st->stream));
+    CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * st->ncells, st->stream));
+    const int cap = (st->maxcount + 3) & ~3;
+    if (cap == 0) return 0;
+    sort_cells<<<st->ncells, 128, sizeof(unsigned) * cap, st->stream>>>(
+        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->dscale, st->bias, st->d_acc);
+    CU(cudaGetLastError());
+
+    Params P;
+    P.xq = st->d_xq;
+    P.pid = st->d_pid;
+    P.keys = st->d_keys;
+    P.cstart = st->d_cstart;
+    P.ccount = st->d_ccount;
+    P.force = st->d_force;
+    P.acc = st->d_acc;
+    P.cell_epot = st->d_cell_epot;
+    P.tasks = st->d_tasks;
+    P.tshift = st->d_tshift;
+    P.ntasks = st->ntasks;
+    P.coef = st->d_coef;
+    P.potinfo = st->d_potinfo;
+    P.potn = st->d_potn;
+    P.potidx = st->d_potidx;
+    P.max_type = st->max_type;
+    P.npots = st->npots;
+    P.ncoef = st->ncoef;
+    P.emask = st->d_emask;
+    P.exoff = st->d_exoff;
+    P.exlist = st->d_exlist;
+    const float cutf = (float)s->cutoff;
+    P.cutoff2 = cutf * cutf;
+    P.cutoff2s = (float)s->cutoff2;
+    P.dmaxdist = st->dmaxdist;
+    P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
+
+    int nw = st->warps;
+    size_t smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    while (smem > 200 * 1024 && nw > 1) {
+        nw /= 2;
+        smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    }
+    if (smem > 220 * 1024) {
+        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    switch (nw) {
+        case 1:
+            CU(cudaFuncSetAttribute(sweep_tasks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sweep_tasks<1><<<st->ntasks, 32, smem, st->stream>>>(P, cap);
+            break;
+        case 2:
+            CU(cudaFuncSetAttribute(sweep_tasks<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sweep_tasks<2><<<st->ntasks, 64, smem, st->stream>>>(P, cap);
+            break;
+        case 8:
+            CU(cudaFuncSetAttribute(sweep_tasks<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sweep_tasks<8><<<st->ntasks, 256, smem, st->stream>>>(P, cap);
+            break;
+        default:
+            CU(cudaFuncSetAttribute(sweep_tasks<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sweep_tasks<4><<<st->ntasks, 128, smem, st->stream>>>(P, cap);
+            break;
+    }
+    CU(cudaGetLastError());
+    return 0;
+}
+
+// Reads back accumulators, stores stats and the per-cell energies.
+int finish_stats(struct engine* e, NbState* st) {
+    struct space* s = &e->s;
+    const unsigned long long* a = st->h_acc;
+    double epot = 0.0;
+    long long esum = 0;
+    for (int c = 0; c < st->ncells; c++) {
+        long long v = (long long)st->h_cell_epot[c];
+        esum += v;
+        s->cells[c].epot = (double)v / kEnergyScale;
+    }
+    epot = (double)esum / kEnergyScale;
+    e->stats.epot = epot;
+    e->stats.virial = -(double)(long long)a[kAccVirial] / kEnergyScale;
+    e->stats.pairs = (int64_t)a[kAccPairs];
+    e->stats.excluded = (int64_t)a[kAccExcl];
+    e->stats.candidates = (int64_t)a[kAccCand];
+    e->stats.status = (int)a[kAccStatus];
+    s->epot_nonbond += epot;
+    if (a[kAccStatus] != 0) {
+        const char* msg = (a[kAccStatus] & kStatusCellOverflow)   ? "Max. number of parts per cell exceeded."
+                          : (a[kAccStatus] & kStatusCopyTimeout)  ? "Bulk copy into shared memory timed out."
+                          : (a[kAccStatus] & kStatusTableIndex)   ? "Pair distance beyond the potential table."
+                                                                   : "Fixed-point force overflow.";
+        int code = (a[kAccStatus] & kStatusCellOverflow) ? engine_err_maxparts : engine_err_cuda;
+        errs_register(code, msg, __LINE__, __func__, __FILE__);
+        return engine_err = code;
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int nb_device_free(struct engine* e) {
+    NbState* st = state(e);
+    if (st == nullptr) return 0;
+    cudaSetDevice(st->device);
+    void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
+                   st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
+                   st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist};
+    for (void* p : dev) cudaFree(p);
+    void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
+    for (void* p : host) cudaFreeHost(p);
+    if (st->ev0) cudaEventDestroy(st->ev0);
+    if (st->ev1) cudaEventDestroy(st->ev1);
+    if (st->stream) cudaStreamDestroy(st->stream);
+    delete st;
+    e->cuda = nullptr;
+    return 0;
+}
+
+extern "C" int engine_cuda_setdevice(struct engine* e, int id) {
+    if (e == nullptr) return engine_err_null;
+    int n = 0;
+    CU(cudaGetDeviceCount(&n));
+    if (id < 0 || id >= n) {
+        errs_register(engine_err_range, "No such CUDA device.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_range;
+    }
+    e->device = id;
+    return 0;
+}
+
+extern "C" int engine_cuda_setdevices(struct engine* e, int nr_devices, int* ids) {
+    if (e == nullptr || ids == nullptr) return engine_err_null;
+    if (nr_devices != 1) {
+        errs_register(engine_err_nyi, "Only one device per engine.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_nyi;
+    }
+    return engine_cuda_setdevice(e, ids[0]);
+}
+
+extern "C" int engine_cuda_settune(struct engine* e, int warps, int unroll) {
+    (void)unroll;
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8) return engine_err_range;
+    state(e)->warps = warps ? warps : 4;
+    return 0;
+}
+
+extern "C" int engine_cuda_load(struct engine* e) {
+    if (e == nullptr) return engine_err_null;
+    struct space* s = &e->s;
+    if (e->cuda) nb_device_free(e);
+    NbState* st = new NbState();
+    e->cuda = st;
+    st->device = e->device;
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&st->ev0));
+    CU(cudaEventCreate(&st->ev1));
+    st->ncells = s->nr_cells;
+    nb_sweep_scales(s, &st->bias, &st->dscale, &st->dmaxdist);
+
+    float axes[13][3];
+    for (int sid = 0; sid < 13; sid++) sort_axis(sid, axes[sid]);
+    CU(cudaMemcpyToSymbol(c_axes, axes, sizeof(axes)));
+
+    // Potential tables: one copy of every distinct table, type pair -> table index.
+    const int mt = e->max_type;
+    std::vector<struct potential*> uniq;
+    std::vector<int> potidx((size_t)mt * mt, -1);
+    for (int i = 0; i < mt; i++)
+        for (int j = 0; j < mt; j++) {
+            struct potential* p = e->p[i * mt + j];
+            if (p == nullptr) continue;
+            int k = 0;
+            while (k < (int)uniq.size() && uniq[k] != p) k++;
+            if (k == (int)uniq.size()) uniq.push_back(p);
+            potidx[i * mt + j] = k;
+        }
+    std::vector<float> coef;
+    std::vector<float4> potinfo;
+    std::vector<int> potn;
+    for (struct potential* p : uniq) {
+        int off = (int)coef.size();
+        coef.insert(coef.end(), p->c, p->c + (size_t)(p->n + 1) * potential_chunk);
+        potinfo.push_back(make_float4(p->alpha[0], p->alpha[1], p->alpha[2], bits_as_float(off)));
+        potn.push_back(p->n);
+    }
+    st->npots = (int)uniq.size();
+    st->ncoef = (int)coef.size();
+    st->max_type = mt;
+    if (coef.empty()) coef.push_back(0.f);
+    if (potinfo.empty()) { potinfo.push_back(make_float4(0, 0, 0, 0)); potn.push_back(0); }
+    if (dev_alloc(&st->d_coef, coef.size()) || dev_alloc(&st->d_potinfo, potinfo.size()) ||
+        dev_alloc(&st->d_potn, potn.size()) || dev_alloc(&st->d_potidx, potidx.size()))
+        return engine_err_cuda;
+    CU(cudaMemcpy(st->d_coef, coef.data(), coef.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_potinfo, potinfo.data(), potinfo.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_potn, potn.data(), potn.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_potidx, potidx.data(), potidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+
+    // Task list with the reference's per-pair shift and discretised shift norm.
+    st->ntasks = s->nr_tasks;
+    std::vector<TaskRec> tasks(st->ntasks > 0 ? st->ntasks : 1);
+    std::vector<float4> tshift(tasks.size(), make_float4(0, 0, 0, 0));
+    for (int t = 0; t < s->nr_tasks; t++) {
+        const struct task* tk = &s->tasks[t];
+        if (tk->type == task_type_self) {
+            tasks[t] = TaskRec{tk->i, tk->i, -1, 0};
+        } else {
+            float sh[3];
+            int dn, ci, cj;
+            int sid = nb_task_shift(s, t, st->dscale, sh, &dn, &ci, &cj);
+            tasks[t] = TaskRec{ci, cj, sid, dn};
+            tshift[t] = make_float4(sh[0], sh[1], sh[2], 0.f);
+        }
+    }
+    if (dev_alloc(&st->d_tasks, tasks.size()) || dev_alloc(&st->d_tshift, tshift.size())) return engine_err_cuda;
+    CU(cudaMemcpy(st->d_tasks, tasks.data(), tasks.size() * sizeof(TaskRec), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_tshift, tshift.data(), tshift.size() * sizeof(float4), cudaMemcpyHostToDevice));
+
+    // Cells: sort-direction masks and the offset/count staging.
+    std::vector<unsigned> cmask(st->ncells);
+    for (int c = 0; c < st->ncells; c++) cmask[c] = s->cells[c].sortmask;
+    if (dev_alloc(&st->d_cmask, st->ncells) || dev_alloc(&st->d_cstart, st->ncells + 1) ||
+        dev_alloc(&st->d_ccount, st->ncells) || dev_alloc(&st->d_cell_epot, st->ncells) ||
+        dev_alloc(&st->d_acc, kAccCount))
+        return engine_err_cuda;
+    CU(cudaMemcpy(st->d_cmask, cmask.data(), cmask.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    CU(cudaMallocHost(&st->h_cstart, sizeof(int) * (2 * st->ncells + 2)));
+    CU(cudaMallocHost(&st->h_cell_epot, sizeof(unsigned long long) * (st->ncells + 1)));
+    CU(cudaMallocHost(&st->h_acc, sizeof(unsigned long long) * kAccCount));
+
+    // Exclusions by particle id: a bit mask for partners at id offsets -16..16, a CSR
+    // list for the rest.  Each exclusion is recorded on both particles.
+    const int nid = s->size_parts > 0 ? s->size_parts : 1;
+    st->nid = nid;
+    std::vector<unsigned> emask(nid, 0u);
+    std::vector<int> cnt(nid + 1, 0);
+    for (int k = 0; k < e->nr_exclusions; k++) {
+        int a = e->exclusions[k].i, b = e->exclusions[k].j;
+        if (a < 0 || b < 0 || a >= nid || b >= nid || a == b) continue;
+        int d = b - a;
+        if (d >= -16 && d <= 16) {
+            emask[a] |= 1u << ((d < 0) ? d + 16 : d + 15);
+            emask[b] |= 1u << ((-d < 0) ? -d + 16 : -d + 15);
+        } else {
+            cnt[a + 1]++;
+            cnt[b + 1]++;
+        }
+    }
+    for (int k = 0; k < nid; k++) cnt[k + 1] += cnt[k];
+    std::vector<int> exlist(cnt[nid] > 0 ? cnt[nid] : 1), fill(cnt.begin(), cnt.end() - 1);
+    for (int k = 0; k < e->nr_exclusions; k++) {
+        int a = e->exclusions[k].i, b = e->exclusions[k].j;
+        if (a < 0 || b < 0 || a >= nid || b >= nid || a == b) continue;
+        int d = b - a;
+        if (d >= -16 && d <= 16) continue;
+        exlist[fill[a]++] = b;
+        exlist[fill[b]++] = a;
+    }
+    if (dev_alloc(&st->d_emask, nid) || dev_alloc(&st->d_exoff, nid + 1) || dev_alloc(&st->d_exlist, exlist.size()))
+        return engine_err_cuda;
+    CU(cudaMemcpy(st->d_emask, emask.data(), nid * sizeof(unsigned), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_exoff, cnt.data(), (nid + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_exlist, exlist.data(), exlist.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+extern "C" int engine_cuda_load_parts(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    int slots = pack_cells(e, st);
+    if (slots < 0) return slots;
+    CU(cudaMemcpyAsync(st->d_xq, st->h_xq, sizeof(float4) * slots, cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemcpyAsync(st->d_pid, st->h_pid, sizeof(int) * slots, cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemcpyAsync(st->d_cstart, st->h_cstart, sizeof(int) * (st->ncells + 1), cudaMemcpyHostToDevice,
+                       st->stream));
+    CU(cudaMemcpyAsync(st->d_ccount, st->h_cstart + st->ncells + 1, sizeof(int) * st->ncells,
+                       cudaMemcpyHostToDevice, st->stream));
+    st->resident_valid = true;
+    return 0;
+}
+
+// Copies forces and energies of the last evaluation back into the cells.
+extern "C" int engine_cuda_unload_parts(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    struct space* s = &e->s;
+    const int slots = st->h_cstart[s->nr_cells];
+    CU(cudaMemcpyAsync(st->h_force, st->d_force, sizeof(unsigned long long) * 3 * (size_t)slots,
+                       cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * st->ncells,
+                       cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
+                       st->stream));
+    CU(cudaStreamSynchronize(st->stream));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, st->ev0, st->ev1) == cudaSuccess) e->stats.ms_kernels = ms;
+    int rc = finish_stats(e, st);
+    const double inv = 1.0 / (double)kForceScale;
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell* cl = &s->cells[c];
+        const unsigned long long* f = st->h_force + 3 * (size_t)st->h_cstart[c];
+        for (int k = 0; k < cl->count; k++)
+            for (int j = 0; j < 3; j++) cl->parts[k].f[j] += (float)((double)(long long)f[3 * k + j] * inv);
+    }
+    return rc;
+}
+
+extern "C" int engine_nonbond_cuda(struct engine* e) {
+    if (e == nullptr) return engine_err_null;
+    if (e->cuda == nullptr && engine_cuda_load(e) < 0) return engine_err_cuda;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    int rc = engine_cuda_load_parts(e);
+    if (rc < 0) return rc;
+    CU(cudaEventRecord(st->ev0, st->stream));
+    rc = launch_kernels(e, st);
+    if (rc < 0) return rc;
+    CU(cudaEventRecord(st->ev1, st->stream));
+    return engine_cuda_unload_parts(e);
+}
+
+// Sort + sweep on the particles already resident on the device (no host copies, no
+// synchronisation); results stay on the device until engine_cuda_unload_parts.
+extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    if (!st->resident_valid) {
+        errs_register(engine_err_cuda, "No particles resident on the device.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
+    CU(cudaSetDevice(st->device));
+    CU(cudaEventRecord(st->ev0, st->stream));
+    int rc = launch_kernels(e, st);
+    if (rc < 0) return rc;
+    CU(cudaEventRecord(st->ev1, st->stream));
+    return 0;
+}
+
+// Runs further launches on a caller-provided stream (e.g. the framework's current stream).
+extern "C" int engine_cuda_setstream(struct engine* e, void* stream) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    st->stream = static_cast<cudaStream_t>(stream);
+    return 0;
+}
+
+extern "C" int engine_cuda_getsort(struct engine* e, int cid, unsigned int* keys, int size) {
+    if (e == nullptr || e->cuda == nullptr || keys == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    struct space* s = &e->s;
+    if (cid < 0 || cid >= s->nr_cells) return engine_err_range;
+    int n = s->cells[cid].count, pad = (n + 3) & ~3;
+    if (size < 13 * n) return engine_err_range;
+    std::vector<unsigned> buf(13 * (size_t)pad + 1);
+    CU(cudaStreamSynchronize(st->stream));
+    CU(cudaMemcpy(buf.data(), st->d_keys + 13 * (size_t)st->h_cstart[cid], sizeof(unsigned) * 13 * (size_t)pad,
+                  cudaMemcpyDeviceToHost));
+    for (int sid = 0; sid < 13; sid++)
+        for (int k = 0; k < n; k++) keys[sid * n + k] = buf[(size_t)sid * pad + k];
+    return 0;
+}

@@ -1,0 +1,253 @@
+"""ctypes binding of libmdcore_b200.so (the C engine API declared in include/mdcore_b200.h).
+
+The calls mirror a reference mdcore driver (examples/argon/argon.c): engine_init,
+engine_addtype, potential_create_*, engine_addpot, engine_load, engine_exclusion_add,
+engine_start, engine_step.  The library runs every force evaluation on the GPU and fails
+loudly when it cannot: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmdcore_b200.so")
+
+engine_flag_none = 0
+engine_flag_cuda = 4
+engine_flag_unsorted = 512
+space_periodic_full = 7
+
+
+class Potential(C.Structure):
+    """struct potential (src/potential.h:57-74)."""
+    _fields_ = [("alpha", C.c_float * 4), ("c", C.POINTER(C.c_float)), ("a", C.c_double),
+                ("b", C.c_double), ("flags", C.c_uint), ("n", C.c_int)]
+
+    def table(self):
+        n = self.n
+        c = np.ctypeslib.as_array(self.c, shape=((n + 1) * 8,)).copy()
+        return n, np.array(self.alpha[:], dtype=np.float32), c
+
+
+class NbStats(C.Structure):
+    _fields_ = [("pairs", C.c_int64), ("excluded", C.c_int64), ("candidates", C.c_int64),
+                ("epot", C.c_double), ("virial", C.c_double), ("status", C.c_int),
+                ("ms_kernels", C.c_float)]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Loads the library (once); raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C mdcore-history_b200`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    dp, ip, vp = P(C.c_double), P(C.c_int), C.c_void_p
+    sig = {
+        "engine_sizeof": (C.c_size_t, []),
+        "engine_init": (C.c_int, [vp, dp, dp, dp, C.c_double, C.c_uint, C.c_int, C.c_uint]),
+        "engine_addtype": (C.c_int, [vp, C.c_double, C.c_double, C.c_char_p, C.c_char_p]),
+        "engine_addpot": (C.c_int, [vp, P(Potential), C.c_int, C.c_int]),
+        "engine_load": (C.c_int, [vp, dp, dp, ip, ip, ip, dp, P(C.c_uint), C.c_int]),
+        "engine_unload": (C.c_int, [vp, dp, dp, ip, ip, ip, dp, P(C.c_uint), dp, C.c_int]),
+        "engine_exclusion_add": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_exclusion_shrink": (C.c_int, [vp]),
+        "engine_rigid_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]),
+        "engine_start": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_step": (C.c_int, [vp]),
+        "engine_finalize": (C.c_int, [vp]),
+        "engine_cuda_setdevice": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_load": (C.c_int, [vp]),
+        "engine_nonbond_cuda": (C.c_int, [vp]),
+        "engine_cuda_load_parts": (C.c_int, [vp]),
+        "engine_cuda_unload_parts": (C.c_int, [vp]),
+        "engine_nonbond_cuda_resident": (C.c_int, [vp]),
+        "engine_cuda_setstream": (C.c_int, [vp, vp]),
+        "engine_cuda_settune": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_cuda_getsort": (C.c_int, [vp, C.c_int, P(C.c_uint), C.c_int]),
+        "engine_getforces": (C.c_int, [vp, dp, C.c_int]),
+        "engine_getcells": (C.c_int, [vp, ip, C.c_int]),
+        "engine_nonbond_stats": (C.c_int, [vp, P(NbStats)]),
+        "engine_set_dt": (C.c_int, [vp, C.c_double]),
+        "engine_zero_forces": (C.c_int, [vp]),
+        "potential_create_LJ126": (P(Potential), [C.c_double] * 5),
+        "potential_create_LJ126_Coulomb": (P(Potential), [C.c_double] * 6),
+        "potential_create_Coulomb": (P(Potential), [C.c_double] * 4),
+        "potential_create_Ewald": (P(Potential), [C.c_double] * 5),
+        "potential_create_LJ126_Ewald": (P(Potential), [C.c_double] * 7),
+        "errs_dump": (C.c_int, [vp]),
+        "errs_clear": (None, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class MdcoreError(RuntimeError):
+    pass
+
+
+def _check(rc: int, what: str):
+    if rc is not None and rc < 0:
+        import io, tempfile
+        libc = C.CDLL(None)
+        msg = ""
+        with tempfile.TemporaryFile(mode="w+") as tf:
+            fp = libc.fdopen(os.dup(tf.fileno()), b"w")
+            lib().errs_dump(fp)
+            libc.fflush(fp)
+            libc.fclose(fp)
+            tf.seek(0)
+            msg = tf.read()
+        raise MdcoreError(f"{what} failed with {rc}: {msg.strip()}")
+    return rc
+
+
+def create_potential(spec):
+    """Builds a table with the library's potential_create_* (spec: workloads.PotSpec)."""
+    L = lib()
+    k, a, b, tol, p = spec.kind, spec.a, spec.b, spec.tol, spec.p
+    if k == 1:
+        ptr = L.potential_create_LJ126(a, b, p[0], p[1], tol)
+    elif k == 2:
+        ptr = L.potential_create_LJ126_Coulomb(a, b, p[0], p[1], p[2], tol)
+    elif k == 3:
+        ptr = L.potential_create_Coulomb(a, b, p[0], tol)
+    elif k == 4:
+        ptr = L.potential_create_Ewald(a, b, p[0], p[1], tol)
+    elif k == 5:
+        ptr = L.potential_create_LJ126_Ewald(a, b, p[0], p[1], p[2], p[3], tol)
+    else:
+        raise ValueError(f"potential kind {k} has no library constructor")
+    if not ptr:
+        _check(-17, f"potential_create kind {k}")
+    return ptr
+
+
+class Engine:
+    """Owns one struct engine allocated in Python memory, as a C driver would on its stack."""
+
+    def __init__(self, origin, dim, L, cutoff, period=space_periodic_full, max_type=1, flags=engine_flag_cuda):
+        self.lib = lib()
+        size = self.lib.engine_sizeof()
+        self._buf = C.create_string_buffer(size + 64)
+        addr = C.addressof(self._buf)
+        self.ptr = C.c_void_p((addr + 63) & ~63)
+        o = np.ascontiguousarray(origin, np.float64)
+        d = np.ascontiguousarray(dim, np.float64)
+        l = np.ascontiguousarray(L, np.float64)
+        _check(self.lib.engine_init(self.ptr, _dptr(o), _dptr(d), _dptr(l), float(cutoff), period, max_type, flags),
+               "engine_init")
+        self.pots = []
+        self.n = 0
+        self.closed = False
+
+    @classmethod
+    def from_system(cls, sysm, flags=engine_flag_cuda, device=0, start=True):
+        e = cls(sysm.origin, sysm.dim, sysm.L, sysm.cutoff, sysm.period, len(sysm.masses), flags)
+        for m, q in zip(sysm.masses, sysm.charges):
+            _check(e.lib.engine_addtype(e.ptr, m, q, None, None), "engine_addtype")
+        for spec in sysm.pots:
+            ptr = create_potential(spec)
+            e.pots.append(ptr)
+            _check(e.lib.engine_addpot(e.ptr, ptr, spec.ti, spec.tj), "engine_addpot")
+        x = np.ascontiguousarray(sysm.x, np.float64)
+        t = np.ascontiguousarray(sysm.type, np.int32)
+        _check(e.lib.engine_load(e.ptr, _dptr(x), None, _iptr(t), None, None, None, None, sysm.n), "engine_load")
+        e.n = sysm.n
+        for i, j in np.asarray(sysm.excl).reshape(-1, 2):
+            _check(e.lib.engine_exclusion_add(e.ptr, int(i), int(j)), "engine_exclusion_add")
+        if len(sysm.excl):
+            _check(e.lib.engine_exclusion_shrink(e.ptr), "engine_exclusion_shrink")
+        _check(e.lib.engine_set_dt(e.ptr, sysm.dt), "engine_set_dt")
+        if start:
+            _check(e.lib.engine_cuda_setdevice(e.ptr, device), "engine_cuda_setdevice")
+            _check(e.lib.engine_start(e.ptr, 1, 1), "engine_start")
+        return e
+
+    # -- force evaluation ----------------------------------------------------------
+    def nonbond(self):
+        """One force evaluation at the current positions (host buffers in and out)."""
+        _check(self.lib.engine_zero_forces(self.ptr), "engine_zero_forces")
+        _check(self.lib.engine_nonbond_cuda(self.ptr), "engine_nonbond_cuda")
+        return self
+
+    def step(self):
+        _check(self.lib.engine_step(self.ptr), "engine_step")
+        return self
+
+    def load_parts(self):
+        _check(self.lib.engine_cuda_load_parts(self.ptr), "engine_cuda_load_parts")
+
+    def resident(self):
+        _check(self.lib.engine_nonbond_cuda_resident(self.ptr), "engine_nonbond_cuda_resident")
+
+    def unload_parts(self):
+        _check(self.lib.engine_zero_forces(self.ptr), "engine_zero_forces")
+        _check(self.lib.engine_cuda_unload_parts(self.ptr), "engine_cuda_unload_parts")
+
+    def set_stream(self, stream_ptr: int):
+        _check(self.lib.engine_cuda_setstream(self.ptr, C.c_void_p(stream_ptr)), "engine_cuda_setstream")
+
+    def tune(self, warps: int):
+        _check(self.lib.engine_cuda_settune(self.ptr, warps, 0), "engine_cuda_settune")
+
+    # -- readback --------------------------------------------------------------------
+    def forces(self) -> np.ndarray:
+        f = np.zeros((self.n, 3), np.float64)
+        _check(self.lib.engine_getforces(self.ptr, _dptr(f), self.n), "engine_getforces")
+        return f
+
+    def cells(self) -> np.ndarray:
+        c = np.zeros(self.n, np.int32)
+        _check(self.lib.engine_getcells(self.ptr, _iptr(c), self.n), "engine_getcells")
+        return c
+
+    def stats(self) -> NbStats:
+        s = NbStats()
+        _check(self.lib.engine_nonbond_stats(self.ptr, C.byref(s)), "engine_nonbond_stats")
+        return s
+
+    def sortkeys(self, cid: int, count: int) -> np.ndarray:
+        buf = np.zeros(13 * max(count, 1), np.uint32)
+        _check(self.lib.engine_cuda_getsort(self.ptr, cid, buf.ctypes.data_as(C.POINTER(C.c_uint)), buf.size),
+               "engine_cuda_getsort")
+        return buf[:13 * count].reshape(13, count)
+
+    def unload(self):
+        x = np.zeros((self.n, 3)); t = np.zeros(self.n, np.int32); pid = np.zeros(self.n, np.int32)
+        epot = np.zeros(1)
+        _check(self.lib.engine_unload(self.ptr, _dptr(x), None, _iptr(t), _iptr(pid), None, None, None,
+                                      _dptr(epot), self.n), "engine_unload")
+        return x, t, pid, float(epot[0])
+
+    def close(self):
+        if not self.closed:
+            self.lib.engine_finalize(self.ptr)
+            self.closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,206 @@
+"""Seeded synthetic workloads of the shapes the mdcore nonbonded path is measured on.
+
+Each generator returns a ``System``: box, cutoff, particle types, per-type-pair potential
+specifications (arguments of the reference's ``potential_create_*`` calls,
+src/potential.c:517-914), positions in id order and exclusion pairs.  The same ``System``
+drives this package's engine (``mdcore_b200.Engine.from_system``) and, serialised with
+``write_sysfile``, the reference CPU driver used as oracle and baseline.
+
+No public benchmark data is involved: these generators are the benchmark inputs.
+
+Units: nm, kJ/mol, amu, ps.  The reference's Coulomb prefactor is 1/(4 pi)
+(src/potential.h:40), so charges products are passed as q_i q_j * 4 pi * 138.935458
+to obtain kJ/mol.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import struct
+from typing import List, Optional
+
+import numpy as np
+
+COULOMB_K = 138.935458                     # kJ mol^-1 nm e^-2
+Q_SCALE = 4.0 * math.pi * COULOMB_K        # undoes potential_escale = 1/(4 pi)
+
+# Potential kinds shared with oracle/sysfile.h.
+KIND_LJ126, KIND_LJ126_COULOMB, KIND_COULOMB, KIND_EWALD, KIND_LJ126_EWALD, KIND_COUNTER = 1, 2, 3, 4, 5, 6
+
+
+@dataclasses.dataclass
+class PotSpec:
+    kind: int
+    ti: int
+    tj: int
+    a: float
+    b: float
+    tol: float
+    p: tuple = (0.0, 0.0, 0.0, 0.0)
+
+
+@dataclasses.dataclass
+class System:
+    name: str
+    origin: np.ndarray            # (3,)
+    dim: np.ndarray               # (3,)
+    L: np.ndarray                 # (3,) requested cell edge
+    cutoff: float
+    masses: List[float]
+    charges: List[float]
+    pots: List[PotSpec]
+    x: np.ndarray                 # (N,3) float64, inside [origin, origin+dim)
+    type: np.ndarray              # (N,) int32
+    excl: np.ndarray              # (M,2) int32
+    dt: float = 0.002
+    flags: int = 0
+    period: int = 7
+
+    @property
+    def n(self) -> int:
+        return int(self.x.shape[0])
+
+    def counting(self) -> "System":
+        """Copy whose potentials are all pair counters (energy 1 per accepted pair)."""
+        pots = [PotSpec(KIND_COUNTER, p.ti, p.tj, 0.0, 1.0, 1.0) for p in self.pots]
+        return dataclasses.replace(self, pots=pots, name=self.name + "-count")
+
+
+def lj_AB(eps: float, sigma: float):
+    """A = 4 eps sigma^12, B = 4 eps sigma^6 for U = A/r^12 - B/r^6."""
+    return 4.0 * eps * sigma ** 12, 4.0 * eps * sigma ** 6
+
+
+def _wrap(x: np.ndarray, dim: np.ndarray) -> np.ndarray:
+    x = np.mod(x, dim)
+    # np.mod can return dim itself for tiny negative inputs; keep strictly inside.
+    hi = np.nextafter(dim, 0.0)
+    return np.minimum(x, hi)
+
+
+def argon_fcc(ncell: int = 20, seed: int = 0, density: float = 21.0, jitter: float = 0.01,
+              tol: float = 1e-4, cutoff: float = 1.0) -> System:
+    """Plain LJ argon: 4*ncell^3 atoms on a jittered FCC lattice at `density` atoms/nm^3.
+
+    ncell=20 gives the 32,000-atom system in an 11.5074 nm box (11^3 cells)."""
+    n = 4 * ncell ** 3
+    L = (n / density) ** (1.0 / 3.0)
+    a = L / ncell
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]], dtype=np.float64)
+    g = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell), indexing="ij"), -1)
+    g = g.reshape(-1, 1, 3).astype(np.float64)
+    x = ((g + basis[None, :, :]) * a + 0.25 * a).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    x = x + rng.normal(0.0, jitter, size=x.shape)
+    dim = np.full(3, L)
+    x = _wrap(x, dim)
+    A, B = lj_AB(0.996, 0.3405)
+    return System(
+        name=f"argon-fcc-{n}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
+        masses=[39.948], charges=[0.0],
+        pots=[PotSpec(KIND_LJ126, 0, 0, 0.25, cutoff, tol, (A, B, 0.0, 0.0))],
+        x=x, type=np.zeros(n, np.int32), excl=np.zeros((0, 2), np.int32), dt=0.005)
+
+
+def _random_rotations(rng, m: int) -> np.ndarray:
+    """m uniformly distributed rotation matrices (random unit quaternions)."""
+    q = rng.normal(size=(m, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.empty((m, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z); R[:, 0, 1] = 2 * (x * y - z * w); R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w); R[:, 1, 1] = 1 - 2 * (x * x + z * z); R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w); R[:, 2, 1] = 2 * (y * z + x * w); R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def water_spce(nside: int = 32, seed: int = 0, density: float = 33.4, jitter: float = 0.01,
+               tol: float = 1e-4, cutoff: float = 1.0, coul_a: float = 0.05) -> System:
+    """Rigid SPC/E water: nside^3 molecules on a jittered cubic grid, random orientations.
+
+    nside=32 gives 32,768 molecules (98,304 atoms) in a 9.9365 nm box (9^3 cells).
+    Particle ids are 3k (O), 3k+1, 3k+2 (H); the three intramolecular pairs are excluded.
+    O-O: LJ (sigma 0.3166, eps 0.650) + shifted Coulomb; O-H, H-H: shifted Coulomb.
+
+    The O-H and H-H tables start at coul_a = 0.05 nm, below the 0.1 nm O-H bond: the
+    reference's table continuation below r = a drops the degree-5 term of the first
+    interval (src/potential.c:1167-1185), so its tables jump by |c5| at r = a, and a bond
+    sitting exactly at a lands on either side depending on how r^2 was rounded."""
+    nmol = nside ** 3
+    L = (nmol / density) ** (1.0 / 3.0)
+    gsp = L / nside
+    g = np.stack(np.meshgrid(np.arange(nside), np.arange(nside), np.arange(nside), indexing="ij"), -1)
+    o = (g.reshape(-1, 3).astype(np.float64) + 0.5) * gsp
+    rng = np.random.default_rng(seed)
+    o = o + rng.normal(0.0, jitter, size=o.shape)
+    theta = math.radians(109.47)
+    d = 0.1
+    local = np.array([[d, 0.0, 0.0], [d * math.cos(theta), d * math.sin(theta), 0.0]])
+    R = _random_rotations(rng, nmol)
+    h = o[:, None, :] + np.einsum("mij,hj->mhi", R, local)
+    x = np.concatenate([o[:, None, :], h], axis=1).reshape(-1, 3)
+    dim = np.full(3, L)
+    x = _wrap(x, dim)
+    typ = np.tile(np.array([0, 1, 1], np.int32), nmol)
+    k = np.arange(nmol, dtype=np.int32) * 3
+    excl = np.stack([np.stack([k, k + 1], 1), np.stack([k, k + 2], 1), np.stack([k + 1, k + 2], 1)], 1)
+    excl = excl.reshape(-1, 2).astype(np.int32)
+    qO, qH = -0.8476, 0.4238
+    A, B = lj_AB(0.650, 0.3166)
+    pots = [
+        PotSpec(KIND_LJ126_COULOMB, 0, 0, 0.25, cutoff, tol, (A, B, qO * qO * Q_SCALE, 0.0)),
+        PotSpec(KIND_COULOMB, 0, 1, coul_a, cutoff, tol, (qO * qH * Q_SCALE, 0.0, 0.0, 0.0)),
+        PotSpec(KIND_COULOMB, 1, 1, coul_a, cutoff, tol, (qH * qH * Q_SCALE, 0.0, 0.0, 0.0)),
+    ]
+    return System(
+        name=f"water-spce-{3 * nmol}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
+        masses=[15.9994, 1.00794], charges=[qO, qH], pots=pots, x=x, type=typ, excl=excl, dt=0.002)
+
+
+def write_sysfile(sysm: System, path: str) -> None:
+    """Serialise in the format of oracle/sysfile.h."""
+    with open(path, "wb") as f:
+        f.write(b"MDB2SYS1")
+        f.write(struct.pack("<6i", sysm.n, len(sysm.masses), len(sysm.pots), len(sysm.excl),
+                            sysm.flags, sysm.period))
+        f.write(np.concatenate([sysm.origin, sysm.dim, sysm.L, [sysm.cutoff]]).astype("<f8").tobytes())
+        for m, q in zip(sysm.masses, sysm.charges):
+            f.write(struct.pack("<2d", m, q))
+        for p in sysm.pots:
+            f.write(struct.pack("<4i7d", p.kind, p.ti, p.tj, 0, p.a, p.b, p.tol, *p.p))
+        f.write(np.ascontiguousarray(sysm.x, dtype="<f8").tobytes())
+        f.write(np.ascontiguousarray(sysm.type, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(sysm.excl, dtype="<i4").tobytes())
+
+
+def read_refout(path: str, sysm: System):
+    """Parse the output of `ref_driver forces` (oracle/ref_driver.c)."""
+    buf = open(path, "rb").read()
+    off = 0
+
+    def take(dtype, count):
+        nonlocal off
+        a = np.frombuffer(buf, dtype=dtype, count=count, offset=off)
+        off += a.nbytes
+        return a
+
+    N, npots, ncells, nexcl = take("<i4", 4)
+    epot, epot_nb, epot_ex = take("<f8", 3)
+    f = take("<f8", 3 * N).reshape(N, 3)
+    xr = take("<f4", 3 * N).reshape(N, 3)
+    cell = take("<i4", N)
+    cells = []
+    for _ in range(ncells):
+        cnt, flags = take("<i4", 2)
+        ids = take("<i4", cnt)
+        keys = take("<u4", 13 * cnt).reshape(13, cnt)
+        cells.append((int(flags), ids.copy(), keys.copy()))
+    tables = []
+    for _ in range(npots):
+        (n,) = take("<i4", 1)
+        alpha = take("<f4", 4)
+        c = take("<f4", (n + 1) * 8)
+        tables.append((int(n), alpha.copy(), c.copy()))
+    return dict(N=int(N), nexcl=int(nexcl), epot=float(epot), epot_nonbond=float(epot_nb),
+                epot_exclusion=float(epot_ex), f=f.copy(), xrel=xr.copy(), cell=cell.copy(),
+                cells=cells, tables=tables)

@@ -1,0 +1,240 @@
+/* ORACLE -- test infrastructure only.  Nothing in the product links against, loads or calls
+ * this file; tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it as the
+ * checker.
+ *
+ * A CPU restatement of the reference mdcore nonbonded evaluation, in plain C, on the same
+ * single-precision inputs the reference and the GPU engine see (cell-local float
+ * coordinates, float potential tables):
+ *
+ *   - cell grid and task list: src/space.c:530-783 (space_init) with the shift/flip rule of
+ *     src/space.c:80-114 (space_getsid);
+ *   - pair set: every (i, j) of a pair task and every j < i of a self task whose float r2,
+ *     computed as src/runner_dopair.c:625-631 does (pix = x_i - shift, dx = pix - x_j,
+ *     r2 = (dx0^2 + dx1^2) + dx2^2), is <= cutoff^2 with a potential for the two types
+ *     (src/runner_dopair.c:640-642, 954-955).  The cut is the float cutoff squared in float
+ *     for pair tasks (src/runner_dopair.c:578-579) and the float of the double square for
+ *     self tasks (src/runner_dopair.c:896).  The sorted sweep of the reference is a pruned
+ *     walk over exactly this set, so the oracle enumerates it by brute force;
+ *   - exclusions: excluded pairs are removed from the set (src/exclusion.c:81-295 subtracts
+ *     them after the sweep, which is the same sum) and counted;
+ *   - potential evaluation: the interval index is computed in float exactly as
+ *     src/potential_eval.h:67-81 does, so the same chunk of the float table is used; the
+ *     polynomial, the distance, the force and all sums are then evaluated in double
+ *     (src/potential_eval.h:84-103 restated in FP64);
+ *   - sort keys: src/runner_dosort.c:140-153, ordered by descending distance with ties in
+ *     storage order.
+ *
+ * Compile with -ffp-contract=off: the float steps must round like the reference build.
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+
+#define CELLID(cd, i, j, k) ((((i) * (cd)[1] + (j)) * (cd)[2]) + (k))
+
+struct ocell {
+    double origin[3];
+    int start, count;
+};
+
+/* Shift and flip of src/space.c:80-114: returns the sort direction, swaps *a/*b when the
+ * shift points into the negative half-space. */
+static int getsid(const double dim[3], const struct ocell *cells, int *a, int *b, float shift[3]) {
+    int idx = 0;
+    for (int k = 0; k < 3; k++) {
+        shift[k] = cells[*b].origin[k] - cells[*a].origin[k];
+        if (shift[k] * 2 > dim[k])
+            shift[k] -= dim[k];
+        else if (shift[k] * 2 < -dim[k])
+            shift[k] += dim[k];
+    }
+    for (int k = 0; k < 3; k++) idx = 3 * idx + ((shift[k] < 0) ? 0 : ((shift[k] > 0) ? 2 : 1));
+    if (idx < 13) {
+        int t = *a; *a = *b; *b = t;
+        for (int k = 0; k < 3; k++) shift[k] = -shift[k];
+        return idx;
+    }
+    return 26 - idx;
+}
+
+static int excl_cmp(const void *x, const void *y) {
+    const long long a = *(const long long *)x, b = *(const long long *)y;
+    return (a > b) - (a < b);
+}
+
+static int is_excluded(const long long *keys, int n, int i, int j) {
+    long long key = (i < j) ? ((long long)i << 32) | (unsigned)j : ((long long)j << 32) | (unsigned)i;
+    return bsearch(&key, keys, n, sizeof(long long), excl_cmp) != NULL;
+}
+
+/* Interval index in float (src/potential_eval.h:74-78), polynomial in double. */
+static void eval_fp64(const float *coef, const float *alpha, int nmax, float r2f, double r, double *e, double *f) {
+    float rf = sqrtf(r2f);
+    int ind = (int)fmaxf(0.0f, alpha[0] + rf * (alpha[1] + rf * alpha[2]));
+    if (ind > nmax) ind = nmax;
+    const float *c = &coef[8 * ind];
+    double x = (r - (double)c[0]) * (double)c[1];
+    double ee = (double)c[2] * x + (double)c[3];
+    double eff = (double)c[2];
+    for (int k = 4; k < 8; k++) {
+        eff = eff * x + ee;
+        ee = ee * x + (double)c[k];
+    }
+    *e = ee;
+    *f = eff * (double)c[1] / r;
+}
+
+/* Nonbonded forces (by particle id, FP64), energy, virial and counts.
+ *   xrel[3N] float cell-local positions, cell[N] cell index, type[N]
+ *   coef: tables concatenated; alpha[4*npots]; coff[npots] float offset of each table;
+ *   potn[npots]; potidx[mt*mt] table index or -1.
+ * Returns 0, or -1 on bad input. */
+int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
+                   const double *origin, const double *dim, const int *cdim, double cutoff,
+                   unsigned period, int mt, const int *potidx, const float *coef, const float *alpha,
+                   const int *coff, const int *potn, int nexcl, const int *excl,
+                   double *f_out, double *epot_out, double *virial_out, long long *npairs_out,
+                   long long *nexcl_out) {
+    const int ncells = cdim[0] * cdim[1] * cdim[2];
+    double h[3];
+    int span[3];
+    for (int k = 0; k < 3; k++) {
+        h[k] = dim[k] / cdim[k];
+        span[k] = ceil(cutoff * (1.0 / h[k]));
+    }
+    struct ocell *cells = calloc(ncells, sizeof(struct ocell));
+    int *order = malloc(sizeof(int) * (N + 1));
+    long long *ekeys = malloc(sizeof(long long) * (nexcl + 1));
+    if (!cells || !order || !ekeys) return -1;
+    for (int i = 0; i < cdim[0]; i++)
+        for (int j = 0; j < cdim[1]; j++)
+            for (int k = 0; k < cdim[2]; k++) {
+                struct ocell *c = &cells[CELLID(cdim, i, j, k)];
+                c->origin[0] = origin[0] + i * h[0];
+                c->origin[1] = origin[1] + j * h[1];
+                c->origin[2] = origin[2] + k * h[2];
+            }
+    for (int p = 0; p < N; p++) {
+        if (cell[p] < 0 || cell[p] >= ncells) return -1;
+        cells[cell[p]].count++;
+    }
+    for (int c = 0, s = 0; c < ncells; c++) { cells[c].start = s; s += cells[c].count; cells[c].count = 0; }
+    for (int p = 0; p < N; p++) { struct ocell *c = &cells[cell[p]]; order[c->start + c->count++] = p; }
+    for (int k = 0; k < nexcl; k++) {
+        int a = excl[2 * k], b = excl[2 * k + 1];
+        ekeys[k] = (a < b) ? ((long long)a << 32) | (unsigned)b : ((long long)b << 32) | (unsigned)a;
+    }
+    qsort(ekeys, nexcl, sizeof(long long), excl_cmp);
+
+    const float cutf = (float)cutoff;
+    const float cut2_pair = cutf * cutf;
+    const float cut2_self = (float)(cutoff * cutoff);
+    double epot = 0.0, vir = 0.0;
+    long long npairs = 0, nex = 0;
+    memset(f_out, 0, sizeof(double) * 3 * N);
+
+    for (int i = 0; i < cdim[0]; i++)
+        for (int j = 0; j < cdim[1]; j++)
+            for (int k = 0; k < cdim[2]; k++) {
+                int id1 = CELLID(cdim, i, j, k), d[3], nb[3];
+                for (d[0] = -span[0]; d[0] <= span[0]; d[0]++) {
+                    nb[0] = i + d[0];
+                    if (nb[0] < 0 || nb[0] >= cdim[0]) {
+                        if (!(period & 1)) continue;
+                        nb[0] = (nb[0] + cdim[0]) % cdim[0];
+                    }
+                    for (d[1] = -span[1]; d[1] <= span[1]; d[1]++) {
+                        nb[1] = j + d[1];
+                        if (nb[1] < 0 || nb[1] >= cdim[1]) {
+                            if (!(period & 2)) continue;
+                            nb[1] = (nb[1] + cdim[1]) % cdim[1];
+                        }
+                        for (d[2] = -span[2]; d[2] <= span[2]; d[2]++) {
+                            double lh[3];
+                            for (int q = 0; q < 3; q++) lh[q] = h[q] * fmax(abs(d[q]) - 1, 0);
+                            if (lh[0] * lh[0] + lh[1] * lh[1] + lh[2] * lh[2] > cutoff * cutoff) continue;
+                            nb[2] = k + d[2];
+                            if (nb[2] < 0 || nb[2] >= cdim[2]) {
+                                if (!(period & 4)) continue;
+                                nb[2] = (nb[2] + cdim[2]) % cdim[2];
+                            }
+                            int id2 = CELLID(cdim, nb[0], nb[1], nb[2]);
+                            int self = (id1 == id2);
+                            if (!(id1 < id2 || (self && d[0] == 0 && d[1] == 0 && d[2] == 0))) continue;
+                            int a = id1, b = id2;
+                            float shift[3];
+                            getsid(dim, cells, &a, &b, shift);
+                            if (self) shift[0] = shift[1] = shift[2] = 0.0f;
+                            const struct ocell *ca = &cells[a], *cb = &cells[b];
+                            const float cut2 = self ? cut2_self : cut2_pair;
+                            for (int ii = 0; ii < ca->count; ii++) {
+                                int pi = order[ca->start + ii];
+                                const float *xi = &xrel[3 * pi];
+                                float pix[3] = {xi[0] - shift[0], xi[1] - shift[1], xi[2] - shift[2]};
+                                int jend = self ? ii : cb->count;
+                                for (int jj = 0; jj < jend; jj++) {
+                                    int pj = order[cb->start + jj];
+                                    const float *xj = &xrel[3 * pj];
+                                    float dxf[3] = {pix[0] - xj[0], pix[1] - xj[1], pix[2] - xj[2]};
+                                    float r2f = dxf[0] * dxf[0] + dxf[1] * dxf[1] + dxf[2] * dxf[2];
+                                    int pot = potidx[type[pi] * mt + type[pj]];
+                                    if (pot < 0 || r2f > cut2) continue;
+                                    if (nexcl > 0 && is_excluded(ekeys, nexcl, pi, pj)) { nex++; continue; }
+                                    double dx[3], r2 = 0.0;
+                                    for (int q = 0; q < 3; q++) {
+                                        dx[q] = ((double)xi[q] - (double)shift[q]) - (double)xj[q];
+                                        r2 += dx[q] * dx[q];
+                                    }
+                                    double r = sqrt(r2), e, fs;
+                                    eval_fp64(coef + coff[pot], alpha + 4 * pot, potn[pot], r2f, r, &e, &fs);
+                                    for (int q = 0; q < 3; q++) {
+                                        double w = fs * dx[q];
+                                        f_out[3 * pi + q] -= w;
+                                        f_out[3 * pj + q] += w;
+                                    }
+                                    epot += e;
+                                    vir += fs * r2;
+                                    npairs++;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+    *epot_out = epot;
+    *virial_out = -vir;
+    *npairs_out = npairs;
+    *nexcl_out = nex;
+    free(cells);
+    free(order);
+    free(ekeys);
+    return 0;
+}
+
+/* Sort keys of one cell along direction sid (src/runner_dosort.c:118-153): key =
+ * (k << 16) | (unsigned)(dscale*(bias + x.n)), dscale = 32767/(2 bias), bias = |h|; ordered
+ * by descending distance, ties in storage order. */
+int oracle_sortkeys(int count, const float *xrel, const double *h, int sid, unsigned *keys) {
+    int idx = 26 - sid;
+    int dv[3] = {idx / 9 - 1, (idx / 3) % 3 - 1, idx % 3 - 1};
+    double len = sqrt((double)(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]));
+    float n[3];
+    for (int k = 0; k < 3; k++) n[k] = (float)(dv[k] / len);
+    float bias = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    float dscale = (float)32767 / (2 * bias);
+    for (int k = 0; k < count; k++) {
+        const float *x = &xrel[3 * k];
+        keys[k] = ((unsigned)k << 16) | (unsigned)(dscale * (bias + x[0] * n[0] + x[1] * n[1] + x[2] * n[2]));
+    }
+    /* insertion sort, descending by distance, stable */
+    for (int a = 1; a < count; a++) {
+        unsigned v = keys[a];
+        int b = a - 1;
+        while (b >= 0 && (keys[b] & 0xffff) < (v & 0xffff)) {
+            keys[b + 1] = keys[b];
+            b--;
+        }
+        keys[b + 1] = v;
+    }
+    return 0;
+}

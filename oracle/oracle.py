@@ -1,0 +1,126 @@
+"""ORACLE -- test infrastructure only (checker for tests/, smoke() and bench.py's
+cpu_baseline leg; the product never imports it).
+
+ctypes front end of oracle/liboracle.so (oracle.c, a CPU FP64 restatement of the
+reference nonbonded evaluation) plus the reference's particle binning
+(src/space.c:403-423: cell index by truncating (x - origin) * (1/h) in double, position
+stored relative to the cell origin in float).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "liboracle.so")
+REF_DIR = os.path.join(_HERE, "_ref")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            subprocess.run(["make", "-C", _HERE, "liboracle.so"], check=True, capture_output=True)
+        L = C.CDLL(LIB)
+        P = C.POINTER
+        L.oracle_nonbond.restype = C.c_int
+        L.oracle_nonbond.argtypes = [C.c_int, P(C.c_float), P(C.c_int), P(C.c_int), P(C.c_double), P(C.c_double),
+                                     P(C.c_int), C.c_double, C.c_uint, C.c_int, P(C.c_int), P(C.c_float),
+                                     P(C.c_float), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int), P(C.c_double),
+                                     P(C.c_double), P(C.c_double), P(C.c_longlong), P(C.c_longlong)]
+        L.oracle_sortkeys.restype = C.c_int
+        L.oracle_sortkeys.argtypes = [C.c_int, P(C.c_float), P(C.c_double), C.c_int, P(C.c_uint)]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def bin_system(sysm):
+    """Cell grid and the reference's cell assignment / cell-local float positions."""
+    cdim = np.floor(sysm.dim / sysm.L).astype(np.int32)
+    h = sysm.dim / cdim
+    ih = 1.0 / h
+    ind = ((sysm.x - sysm.origin) * ih).astype(np.int64)      # truncation, values >= 0
+    cell = ((ind[:, 0] * cdim[1] + ind[:, 1]) * cdim[2] + ind[:, 2]).astype(np.int32)
+    corigin = sysm.origin + ind * h
+    xrel = (sysm.x - corigin).astype(np.float32)
+    return dict(cdim=cdim, h=h, cell=cell, xrel=xrel)
+
+
+def pack_tables(sysm, tables):
+    """tables[k] = (n, alpha[4] float32, coef[(n+1)*8] float32) for sysm.pots[k]."""
+    mt = len(sysm.masses)
+    potidx = -np.ones((mt, mt), np.int32)
+    coef, alpha, coff, potn = [], [], [], []
+    off = 0
+    for k, (spec, (n, a, c)) in enumerate(zip(sysm.pots, tables)):
+        potidx[spec.ti, spec.tj] = k
+        potidx[spec.tj, spec.ti] = k
+        coef.append(np.asarray(c, np.float32))
+        alpha.append(np.asarray(a, np.float32)[:4])
+        coff.append(off)
+        potn.append(n)
+        off += len(c)
+    return dict(potidx=potidx.reshape(-1), coef=np.concatenate(coef).astype(np.float32),
+                alpha=np.concatenate(alpha).astype(np.float32), coff=np.array(coff, np.int32),
+                potn=np.array(potn, np.int32))
+
+
+def nonbond(sysm, tables, binned=None):
+    """FP64 forces (by id), energy, virial, pair and excluded-pair counts."""
+    b = binned or bin_system(sysm)
+    t = pack_tables(sysm, tables)
+    N = sysm.n
+    f = np.zeros((N, 3), np.float64)
+    epot, vir = C.c_double(), C.c_double()
+    npairs, nex = C.c_longlong(), C.c_longlong()
+    xrel = np.ascontiguousarray(b["xrel"], np.float32)
+    cell = np.ascontiguousarray(b["cell"], np.int32)
+    typ = np.ascontiguousarray(sysm.type, np.int32)
+    org = np.ascontiguousarray(sysm.origin, np.float64)
+    dim = np.ascontiguousarray(sysm.dim, np.float64)
+    cdim = np.ascontiguousarray(b["cdim"], np.int32)
+    excl = np.ascontiguousarray(sysm.excl, np.int32).reshape(-1)
+    rc = lib().oracle_nonbond(N, _p(xrel, C.c_float), _p(cell, C.c_int), _p(typ, C.c_int), _p(org, C.c_double),
+                              _p(dim, C.c_double), _p(cdim, C.c_int), float(sysm.cutoff), sysm.period,
+                              len(sysm.masses), _p(t["potidx"], C.c_int), _p(t["coef"], C.c_float),
+                              _p(t["alpha"], C.c_float), _p(t["coff"], C.c_int), _p(t["potn"], C.c_int),
+                              len(sysm.excl), _p(excl, C.c_int) if excl.size else None, _p(f, C.c_double),
+                              C.byref(epot), C.byref(vir), C.byref(npairs), C.byref(nex))
+    if rc != 0:
+        raise RuntimeError("oracle_nonbond failed")
+    return dict(f=f, epot=epot.value, virial=vir.value, pairs=npairs.value, excluded=nex.value)
+
+
+def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:
+    n = len(xrel_cell)
+    keys = np.zeros(max(n, 1), np.uint32)
+    x = np.ascontiguousarray(xrel_cell, np.float32)
+    hh = np.ascontiguousarray(h, np.float64)
+    lib().oracle_sortkeys(n, _p(x, C.c_float), _p(hh, C.c_double), sid, _p(keys, C.c_uint))
+    return keys[:n]
+
+
+def ref_available(strict: bool = True) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "ref_driver_strict" if strict else "ref_driver"))
+
+
+def run_ref_forces(sysm, workdir, runners=4, strict=True):
+    """Runs the compiled reference (oracle/_ref) on `sysm`; returns workloads.read_refout()."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(_HERE), "mdcore-history_b200"))
+    import workloads as W
+    sysf = os.path.join(workdir, sysm.name + ".sys")
+    outf = os.path.join(workdir, sysm.name + ".out")
+    W.write_sysfile(sysm, sysf)
+    exe = os.path.join(REF_DIR, "ref_driver_strict" if strict else "ref_driver")
+    subprocess.run([exe, "forces", sysf, outf, str(runners)], check=True, capture_output=True)
+    return W.read_refout(outf, sysm)

@@ -1,0 +1,183 @@
+/* Test/bench infrastructure (not product code).
+ *
+ * Driver for the reference mdcore CPU library (built by oracle/Makefile.ref into
+ * oracle/_ref/).  It only uses the reference's public engine API, the way the reference's
+ * own example drivers do (examples/argon/argon.c, examples/bulk/bulk.c):
+ * engine_init, engine_addtype, potential_create_*, engine_addpot, engine_load,
+ * engine_exclusion_add/_shrink, engine_start, engine_step.
+ *
+ *   ref_driver forces <sysfile> <outfile> <nr_runners>
+ *       One engine_step with dt = 0 (positions do not move, src/engine.c:1975-1979), then
+ *       dumps forces, energies, cell assignment, sort lists and the float potential tables.
+ *   ref_driver bench <sysfile> <nr_runners> <warmup> <steps>
+ *       Times engine_step (dt = 0: sort + pair/self sweep + exclusion subtraction +
+ *       bookkeeping, src/engine.c:2070-2240) with clock_gettime and prints one JSON line.
+ *
+ * The pair-counter potential (sysfile kind 6) is a hand-made one-interval table:
+ * alpha = {1,0,0} selects interval 1 for every r, its coefficients are all zero except the
+ * constant term 1.0f, so potential_eval (src/potential_eval.h:67-104) returns e = 1.0f and
+ * f = 0 exactly and the nonbonded energy sums to the number of accepted pairs.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <float.h>
+#include <time.h>
+#include <pthread.h>
+#include <omp.h>
+#include "cycle.h"
+#include "mdcore.h"
+#include "sysfile.h"
+
+static struct potential *make_counter(void) {
+    struct potential *p = NULL;
+    float *c = NULL;
+    if (posix_memalign((void **)&p, 16, sizeof(struct potential)) != 0) return NULL;
+    if (posix_memalign((void **)&c, 64, sizeof(float) * 2 * potential_chunk) != 0) return NULL;
+    memset(c, 0, sizeof(float) * 2 * potential_chunk);
+    c[potential_chunk + 1] = 1.0f;                  /* x = r */
+    c[2 * potential_chunk - 1] = 1.0f;              /* constant term */
+    p->alpha[0] = 1.0f; p->alpha[1] = 0.0f; p->alpha[2] = 0.0f; p->alpha[3] = 0.0f;
+    p->c = c; p->a = 0.0; p->b = DBL_MAX; p->flags = potential_flag_none; p->n = 1;
+    return p;
+}
+
+static struct potential *make_pot(const struct sys_pot *sp) {
+    switch (sp->kind) {
+        case 1: return potential_create_LJ126(sp->a, sp->b, sp->p[0], sp->p[1], sp->tol);
+        case 2: return potential_create_LJ126_Coulomb(sp->a, sp->b, sp->p[0], sp->p[1], sp->p[2], sp->tol);
+        case 3: return potential_create_Coulomb(sp->a, sp->b, sp->p[0], sp->tol);
+        case 4: return potential_create_Ewald(sp->a, sp->b, sp->p[0], sp->p[1], sp->tol);
+        case 5: return potential_create_LJ126_Ewald(sp->a, sp->b, sp->p[0], sp->p[1], sp->p[2], sp->p[3], sp->tol);
+        case 6: return make_counter();
+    }
+    return NULL;
+}
+
+static int build(struct engine *e, struct sys_desc *sd, struct potential ***pots_out, int runners) {
+    int k;
+    struct potential **pots = malloc(sizeof(struct potential *) * (sd->npots + 1));
+    if (engine_init(e, sd->origin, sd->dim, sd->L, sd->cutoff, sd->period, sd->ntypes,
+                    sd->flags) != 0) {
+        fprintf(stderr, "ref_driver: engine_init failed (%i)\n", engine_err);
+        errs_dump(stderr);
+        return -1;
+    }
+    for (k = 0; k < sd->ntypes; k++)
+        if (engine_addtype(e, sd->mass[k], sd->charge[k], NULL, NULL) < 0) { errs_dump(stderr); return -1; }
+    for (k = 0; k < sd->npots; k++) {
+        if ((pots[k] = make_pot(&sd->pots[k])) == NULL) {
+            fprintf(stderr, "ref_driver: potential %i (kind %i) failed (%i)\n", k, sd->pots[k].kind, potential_err);
+            errs_dump(stderr);
+            return -1;
+        }
+        if (engine_addpot(e, pots[k], sd->pots[k].ti, sd->pots[k].tj) < 0) { errs_dump(stderr); return -1; }
+    }
+    if (engine_load(e, sd->x, NULL, sd->type, NULL, NULL, NULL, NULL, sd->N) < 0) {
+        fprintf(stderr, "ref_driver: engine_load failed (%i)\n", engine_err);
+        errs_dump(stderr);
+        return -1;
+    }
+    for (k = 0; k < sd->nexcl; k++)
+        if (engine_exclusion_add(e, sd->excl[2 * k], sd->excl[2 * k + 1]) < 0) { errs_dump(stderr); return -1; }
+    if (sd->nexcl > 0 && engine_exclusion_shrink(e) < 0) { errs_dump(stderr); return -1; }
+    e->time = 0;
+    e->dt = 0.0;
+    if (engine_start(e, runners, runners) < 0) {
+        fprintf(stderr, "ref_driver: engine_start failed (%i)\n", engine_err);
+        errs_dump(stderr);
+        return -1;
+    }
+    *pots_out = pots;
+    return 0;
+}
+
+static int do_forces(const char *sysf, const char *outf, int runners) {
+    struct sys_desc sd;
+    static struct engine e;
+    struct potential **pots;
+    int k, id, cid, hdr[4];
+    double en[3];
+    FILE *out;
+    if (sys_read(sysf, &sd) != 0) { fprintf(stderr, "ref_driver: bad system file %s\n", sysf); return 1; }
+    if (build(&e, &sd, &pots, runners) != 0) return 1;
+    if (engine_step(&e) != 0) { errs_dump(stderr); return 1; }
+    out = fopen(outf, "wb");
+    if (out == NULL) return 1;
+    hdr[0] = sd.N; hdr[1] = sd.npots; hdr[2] = e.s.nr_cells; hdr[3] = e.nr_exclusions;
+    fwrite(hdr, sizeof(int), 4, out);
+    en[0] = e.s.epot; en[1] = e.s.epot_nonbond; en[2] = e.s.epot_exclusion;
+    fwrite(en, sizeof(double), 3, out);
+    /* Forces, cell-relative float positions and cell index, by particle id. */
+    for (id = 0; id < sd.N; id++) {
+        double f[3];
+        struct part *p = e.s.partlist[id];
+        for (k = 0; k < 3; k++) f[k] = p->f[k];
+        fwrite(f, sizeof(double), 3, out);
+    }
+    for (id = 0; id < sd.N; id++) fwrite(e.s.partlist[id]->x, sizeof(float), 3, out);
+    for (id = 0; id < sd.N; id++) {
+        int c = (int)(e.s.celllist[id] - e.s.cells);
+        fwrite(&c, sizeof(int), 1, out);
+    }
+    /* Per cell: count, sort-task flags, particle ids in cell order, 13*count sort keys. */
+    for (cid = 0; cid < e.s.nr_cells; cid++) {
+        struct cell *c = &e.s.cells[cid];
+        int cf[2];
+        cf[0] = c->count; cf[1] = c->sort ? (int)c->sort->flags : 0;
+        fwrite(cf, sizeof(int), 2, out);
+        for (k = 0; k < c->count; k++) fwrite(&c->parts[k].id, sizeof(int), 1, out);
+        fwrite(c->sortlist, sizeof(unsigned int), 13 * (size_t)c->count, out);
+    }
+    /* Float tables. */
+    for (k = 0; k < sd.npots; k++) {
+        struct potential *p = pots[k];
+        int n = p->n;
+        fwrite(&n, sizeof(int), 1, out);
+        fwrite(p->alpha, sizeof(float), 4, out);
+        fwrite(p->c, sizeof(float), (size_t)(n + 1) * potential_chunk, out);
+    }
+    fclose(out);
+    return 0;
+}
+
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+static int do_bench(const char *sysf, int runners, int warmup, int steps) {
+    struct sys_desc sd;
+    static struct engine e;
+    struct potential **pots;
+    int k;
+    double t0, t1, tmin = 1e30;
+    if (sys_read(sysf, &sd) != 0) { fprintf(stderr, "ref_driver: bad system file %s\n", sysf); return 1; }
+    omp_set_num_threads(runners);
+    if (build(&e, &sd, &pots, runners) != 0) return 1;
+    for (k = 0; k < warmup; k++)
+        if (engine_step(&e) != 0) { errs_dump(stderr); return 1; }
+    t0 = now_s();
+    for (k = 0; k < steps; k++) {
+        double ts = now_s();
+        if (engine_step(&e) != 0) { errs_dump(stderr); return 1; }
+        ts = now_s() - ts;
+        if (ts < tmin) tmin = ts;
+    }
+    t1 = now_s();
+    printf("{\"ms_per_step\": %.6f, \"ms_min\": %.6f, \"steps\": %i, \"runners\": %i, "
+           "\"epot\": %.17g, \"nr_tasks\": %i, \"nr_cells\": %i}\n",
+           1e3 * (t1 - t0) / steps, 1e3 * tmin, steps, runners, e.s.epot, e.s.nr_tasks, e.s.nr_cells);
+    return 0;
+}
+
+int main(int argc, char *argv[]) {
+    if (argc >= 5 && strcmp(argv[1], "forces") == 0)
+        return do_forces(argv[2], argv[3], atoi(argv[4]));
+    if (argc >= 6 && strcmp(argv[1], "bench") == 0)
+        return do_bench(argv[2], atoi(argv[3]), atoi(argv[4]), atoi(argv[5]));
+    fprintf(stderr, "usage: ref_driver forces <sys> <out> <runners> | bench <sys> <runners> <warmup> <steps>\n");
+    return 2;
+}
