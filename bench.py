@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Benchmark of the nonbonded hot path: pair interactions per second on rigid SPC/E water
+(98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions per molecule).
+
+One step = one nonbonded force evaluation of the whole system: sort every cell along the
+13 pair directions, sweep all 10,206 cell-pair/self tasks, fixed-point force accumulation,
+FP64 energy and virial.
+
+  value   device-resident: positions already in HBM, kernels only (CUDA events around each
+          step on the launching stream; L2 flushed with a 256 MiB write before every step,
+          outside the events).
+  e2e     the C-ABI call engine_nonbond_cuda with host buffers: packing the cells, one
+          host->device copy of positions/ids/cell offsets, sort + sweep, one device->host
+          copy of forces and energies, unpacking.
+
+Multi-GPU: the path is not partitioned here ("replicas only"): each rank evaluates its own
+copy of the system and value = ranks * pairs / max-over-ranks time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mdcore-history_b200"))
+
+METRIC = "pair interactions/s + ns/day, 1 B200: tuned vs plain at ≤1e-5 rel force err"
+UNIT = "pair interactions/s"
+FLOPS_PER_PAIR = 45          # per accepted pair, FMA = 2 (roofline)
+DT_FS = 2.0
+WORKLOAD = "rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, " \
+           "9x9x9 cells, cutoff 1.0 nm, 98,304 exclusions, seeded"
+
+
+def ns_per_day(ms_per_step):
+    return DT_FS * 1e-6 * 86400.0 / (ms_per_step * 1e-3)
+
+
+def build_system():
+    import workloads as W
+    return W.water_spce(32)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) >= 9:
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_reference_driver(sysm, threads, warmup, steps):
+    import workloads as W
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as tmp:
+        sysf = os.path.join(tmp, "water.sys")
+        W.write_sysfile(sysm, sysf)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
+        r = subprocess.run([exe, "bench", sysf, str(threads), str(warmup), str(steps)], capture_output=True,
+                           text=True, env=env, check=True)
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+    return json.loads(line)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank):
+    """The reference's own pthreads CPU runner (oracle/_ref, built from the reference
+    sources) on the same workload, all host threads."""
+    if rank != 0:
+        return
+    sysm = build_system()
+    threads = host_threads()
+    pairs = pair_count(sysm)
+    try:
+        r = run_reference_driver(sysm, threads, max(1, min(args.warmup, 3)), max(1, min(args.steps, 20)))
+    except (FileNotFoundError, subprocess.CalledProcessError) as exc:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {exc}"}))
+        return
+    ms = r["ms_per_step"]
+    v = pairs / (ms * 1e-3)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": r["steps"], "warmup": max(1, min(args.warmup, 3)), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "ns_per_day": ns_per_day(ms),
+        "config": {"workload": WORKLOAD, "pairs_per_step": pairs, "parallelism": "pthreads runners"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{r['steps']} engine_step calls (dt=0) of the full system, "
+                                   f"{threads} runners"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+_PAIRS = {}
+
+
+def pair_count(sysm):
+    """Pairs per step of the workload (the reference's pair set, counted by the oracle)."""
+    if sysm.name not in _PAIRS:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import mdcore_b200 as M
+        import oracle as O
+        tables = [M.create_potential(p).contents.table() for p in sysm.pots]
+        _PAIRS[sysm.name] = O.nonbond(sysm, tables)["pairs"]
+    return _PAIRS[sysm.name]
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    import mdcore_b200 as M
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    sysm = build_system()
+    e = M.Engine.from_system(sysm, device=local_rank)
+    stream = torch.cuda.current_stream()
+    e.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    N = sysm.n
+
+    # warm-up (host-buffer path, which also uploads the particles)
+    for _ in range(args.warmup):
+        e.nonbond()
+    st = e.stats()
+    if st.status != 0:
+        raise SystemExit(f"bench.py: device status {st.status}")
+    pairs = int(st.pairs)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+
+    # ---- device-resident timed region
+    e.load_parts()
+    for _ in range(2):
+        e.resident()
+    barrier()
+    tot_ms, sweep_ms = 0.0, 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.resident()
+        ev1.record(stream)
+        ev1.synchronize()
+        tot_ms += ev0.elapsed_time(ev1)
+        sweep_ms += e.kernel_times()[1]
+    barrier()
+    e.unload_parts()
+    if e.stats().status != 0:
+        raise SystemExit("bench.py: device status after timed region")
+
+    # ---- end-to-end timed region (host buffers through the C ABI)
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.nonbond()
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_ms += ev0.elapsed_time(ev1)
+    barrier()
+    clk = clocks.stop()
+
+    ms = tot_ms / args.steps
+    ms_e2e = e2e_ms / args.steps
+    ms_sweep = sweep_ms / args.steps
+    if dist is not None:
+        t = torch.tensor([ms, ms_e2e, ms_sweep], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e, ms_sweep = [float(v) for v in t.tolist()]
+    if rank == 0:
+        import numpy as np
+        counts = np.bincount(e.cells(), minlength=1)
+        ncells = len(counts)
+        slots_used = int((((counts + 3) // 4) * 4).sum())
+        h2d = 20 * slots_used + 4 * (2 * ncells + 1)          # xq + pid, cell offsets + counts
+        d2h = 24 * slots_used + 8 * ncells + 64               # fixed-point forces, cell energies, counters
+        peak = M.fp32_peak_tflops(local_rank)
+        achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+        if os.path.exists(prof):
+            traffic = json.load(open(prof)).get("bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ns_per_day": ns_per_day(ms),
+            "config": {"workload": WORKLOAD, "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
+                       "tasks": 10206, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB write before every timed step (outside the timed events)"},
+            "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "sweep_tasks", "kernel_ms": ms_sweep,
+                         "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
+                                        "MEASURED_PEAKS.json has no FP32 figure"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk,
+        }
+        if world == 1:
+            try:
+                threads = host_threads()
+                r = run_reference_driver(sysm, threads, 1, 5)
+                cv = pairs / (r["ms_per_step"] * 1e-3)
+                line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "reference",
+                                        "sample": f"5 engine_step calls (dt=0) of the full system on "
+                                                  f"{threads} pthreads runners, reference build in oracle/_ref"}
+            except (FileNotFoundError, subprocess.CalledProcessError) as exc:
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                        "sample": f"unavailable: {exc}"}
+        print(json.dumps(line))
+    e.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

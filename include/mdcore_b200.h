@@ -346,6 +346,10 @@ int engine_set_dt(struct engine *e, double dt);
 int engine_zero_forces(struct engine *e);
 /* Makes later launches use this cudaStream_t (e.g. the caller framework's stream). */
 int engine_cuda_setstream(struct engine *e, void *stream);
+/* Device time (ms) of the last evaluation: sort + sweep, and the sweep kernel alone. */
+int engine_cuda_kernel_times(struct engine *e, float *total_ms, float *sweep_ms);
+/* Measured FP32 FMA throughput of a device in TFLOP/s (a register-only FMA loop). */
+int engine_cuda_fp32_peak(int device, float *tflops);
 /* Sweep kernel launch parameters (warps per block, i-chunks per warp); 0 = autotuned. */
 int engine_cuda_settune(struct engine *e, int warps, int unroll);
 

@@ -23,8 +23,10 @@ namespace {
 
 struct NbState {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream = nullptr;         // launch stream (own_stream unless the caller set one)
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;       // around sort + sweep
+    cudaEvent_t evs0 = nullptr, evs1 = nullptr;     // around the sweep kernel alone
     // geometry
     int ncells = 0, ntasks = 0, ncap = 0, nid = 0;
     float bias = 0.f, dscale = 0.f;
@@ -188,6 +190,7 @@ int launch_kernels(struct engine* e, NbState* st) {
     P.dmaxdist = st->dmaxdist;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
 
+    CU(cudaEventRecord(st->evs0, st->stream));
     int nw = st->warps;
     size_t smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
     while (smem > 200 * 1024 && nw > 1) {
@@ -218,6 +221,7 @@ int launch_kernels(struct engine* e, NbState* st) {
             break;
     }
     CU(cudaGetLastError());
+    CU(cudaEventRecord(st->evs1, st->stream));
     return 0;
 }
 
@@ -266,7 +270,9 @@ extern "C" int nb_device_free(struct engine* e) {
     for (void* p : host) cudaFreeHost(p);
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
-    if (st->stream) cudaStreamDestroy(st->stream);
+    if (st->evs0) cudaEventDestroy(st->evs0);
+    if (st->evs1) cudaEventDestroy(st->evs1);
+    if (st->own_stream) cudaStreamDestroy(st->own_stream);
     delete st;
     e->cuda = nullptr;
     return 0;
@@ -309,9 +315,12 @@ extern "C" int engine_cuda_load(struct engine* e) {
     e->cuda = st;
     st->device = e->device;
     CU(cudaSetDevice(st->device));
-    CU(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&st->own_stream, cudaStreamNonBlocking));
+    st->stream = st->own_stream;
     CU(cudaEventCreate(&st->ev0));
     CU(cudaEventCreate(&st->ev1));
+    CU(cudaEventCreate(&st->evs0));
+    CU(cudaEventCreate(&st->evs1));
     st->ncells = s->nr_cells;
     nb_sweep_scales(s, &st->bias, &st->dscale, &st->dmaxdist);
 
@@ -501,7 +510,7 @@ extern "C" int engine_cuda_setstream(struct engine* e, void* stream) {
     NbState* st = state(e);
     CU(cudaSetDevice(st->device));
     CU(cudaStreamSynchronize(st->stream));
-    st->stream = static_cast<cudaStream_t>(stream);
+    st->stream = stream ? static_cast<cudaStream_t>(stream) : st->own_stream;
     return 0;
 }
 
@@ -518,5 +527,69 @@ extern "C" int engine_cuda_getsort(struct engine* e, int cid, unsigned int* keys
                   cudaMemcpyDeviceToHost));
     for (int sid = 0; sid < 13; sid++)
         for (int k = 0; k < n; k++) keys[sid * n + k] = buf[(size_t)sid * pad + k];
+    return 0;
+}
+
+// Device times of the last evaluation: sort + sweep, and the sweep kernel alone (waits for
+// the launching stream).
+extern "C" int engine_cuda_kernel_times(struct engine* e, float* total_ms, float* sweep_ms) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    float a = 0.f, b = 0.f;
+    CU(cudaEventElapsedTime(&a, st->ev0, st->ev1));
+    CU(cudaEventElapsedTime(&b, st->evs0, st->evs1));
+    if (total_ms) *total_ms = a;
+    if (sweep_ms) *sweep_ms = b;
+    return 0;
+}
+
+namespace {
+// Independent FMA chains: 2 flops per lane per FMA, no memory traffic in the loop.
+__global__ void __launch_bounds__(256) fma_probe(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    const float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+}  // namespace
+
+// Measured FP32 FMA throughput of the current device (TFLOP/s), for roofline fractions.
+extern "C" int engine_cuda_fp32_peak(int device, float* tflops) {
+    if (tflops == nullptr) return engine_err_null;
+    CU(cudaSetDevice(device));
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    float* out = nullptr;
+    CU(cudaMalloc(&out, sizeof(float) * blocks * threads));
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    fma_probe<<<blocks, threads>>>(out, 64, 0.999f, 1e-4f);
+    float best = 0.f;
+    for (int rep = 0; rep < 5; ++rep) {
+        CU(cudaEventRecord(e0));
+        fma_probe<<<blocks, threads>>>(out, iters, 0.999f, 1e-4f);
+        CU(cudaEventRecord(e1));
+        CU(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+        const float tf = (float)(flops / (ms * 1e-3) / 1e12);
+        if (tf > best) best = tf;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = best;
     return 0;
 }

@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
         "engine_getcells": (C.c_int, [vp, ip, C.c_int]),
         "engine_nonbond_stats": (C.c_int, [vp, P(NbStats)]),
         "engine_set_dt": (C.c_int, [vp, C.c_double]),
+        "engine_cuda_kernel_times": (C.c_int, [vp, P(C.c_float), P(C.c_float)]),
+        "engine_cuda_fp32_peak": (C.c_int, [C.c_int, P(C.c_float)]),
         "engine_zero_forces": (C.c_int, [vp]),
         "potential_create_LJ126": (P(Potential), [C.c_double] * 5),
         "potential_create_LJ126_Coulomb": (P(Potential), [C.c_double] * 6),
@@ -209,6 +211,11 @@ class Engine:
     def set_stream(self, stream_ptr: int):
         _check(self.lib.engine_cuda_setstream(self.ptr, C.c_void_p(stream_ptr)), "engine_cuda_setstream")
 
+    def kernel_times(self):
+        a, b = C.c_float(), C.c_float()
+        _check(self.lib.engine_cuda_kernel_times(self.ptr, C.byref(a), C.byref(b)), "engine_cuda_kernel_times")
+        return a.value, b.value
+
     def tune(self, warps: int):
         _check(self.lib.engine_cuda_settune(self.ptr, warps, 0), "engine_cuda_settune")
 
@@ -251,3 +258,9 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def fp32_peak_tflops(device: int = 0) -> float:
+    v = C.c_float()
+    _check(lib().engine_cuda_fp32_peak(device, C.byref(v)), "engine_cuda_fp32_peak")
+    return v.value

@@ -1,0 +1,45 @@
+"""Shared test helpers: golden fixtures as workloads.System objects, error metrics."""
+import os
+
+import numpy as np
+
+import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load_golden(fname):
+    """Returns (System, dict of reference outputs) for a fixture written by make_golden.py."""
+    z = np.load(os.path.join(GOLDEN, fname))
+    pots = [W.PotSpec(int(r[0]), int(r[1]), int(r[2]), float(r[3]), float(r[4]), float(r[5]),
+                      tuple(float(v) for v in r[6:10])) for r in z["pots"]]
+    sysm = W.System(name=str(z["name"]), origin=z["origin"], dim=z["dim"], L=z["L"], cutoff=float(z["cutoff"]),
+                    masses=list(z["masses"]), charges=list(z["charges"]), pots=pots, x=z["x"],
+                    type=z["type"].astype(np.int32), excl=z["excl"].astype(np.int32).reshape(-1, 2),
+                    dt=float(z["dt"]))
+    ref = {k: z[k] for k in z.files}
+    ref["tables"] = [(int(z[f"tab{k}_n"]), z[f"tab{k}_alpha"], z[f"tab{k}_c"]) for k in range(int(z["npots"]))]
+    return sysm, ref
+
+
+def force_errors(f, f_ref):
+    """Error metrics of forces f against f_ref (both N x 3, by particle id)."""
+    d = np.linalg.norm(f - f_ref, axis=1)
+    fn = np.linalg.norm(f_ref, axis=1)
+    frms = np.sqrt((f_ref ** 2).sum(1).mean())
+    rel = d / np.maximum(fn, 1e-30)
+    return dict(global_rel=float(np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref)),
+                max_over_frms=float(d.max() / frms), rel_max=float(rel.max()),
+                rel_p99=float(np.percentile(rel, 99)), rel_median=float(np.median(rel)),
+                frac_over_1e5=float((rel > 1e-5).mean()))
+
+
+def sort_cells_of(ref):
+    """Yields (cell id, sort mask, particle ids, keys[13, count]) of a fixture."""
+    off_i = off_k = 0
+    for cid, (mask, cnt) in enumerate(zip(ref["sort_mask"], ref["sort_count"])):
+        ids = ref["sort_ids"][off_i:off_i + cnt]
+        keys = ref["sort_keys"][off_k:off_k + 13 * cnt].reshape(13, cnt)
+        off_i += cnt
+        off_k += 13 * cnt
+        yield cid, int(mask), ids, keys
