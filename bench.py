@@ -168,7 +168,8 @@ def ours(args, rank, world, local_rank):
 
     sysm = build_system()
     e = M.Engine.from_system(sysm, device=local_rank)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     e.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     N = sysm.n
@@ -209,6 +210,25 @@ def ours(args, rank, world, local_rank):
     e.unload_parts()
     if e.stats().status != 0:
         raise SystemExit("bench.py: device status after timed region")
+
+    # ---- the plain form (one CTA per task, IEEE sqrt/div), same protocol, for tuned-vs-plain
+    e.tune(0, plain=True)
+    e.load_parts()
+    e.resident()
+    barrier()
+    plain_ms, plain_sweep = 0.0, 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.resident()
+        ev1.record(stream)
+        ev1.synchronize()
+        plain_ms += ev0.elapsed_time(ev1)
+        plain_sweep += e.kernel_times()[1]
+    barrier()
+    e.tune(0, plain=False)
 
     # ---- end-to-end timed region (host buffers through the C ABI)
     barrier()
@@ -261,10 +281,13 @@ def ours(args, rank, world, local_rank):
                          "kernel": "sweep_tasks", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
+            "plain": {"value": world * pairs / (plain_ms / args.steps * 1e-3), "ms_per_step": plain_ms / args.steps,
+                      "sweep_ms": plain_sweep / args.steps,
+                      "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
             "gpu_launches": 2 * args.steps,
             "clocks": clk,
         }
-        if world == 1:
+        if world == 1 and not args.no_cpu_baseline:
             try:
                 threads = host_threads()
                 r = run_reference_driver(sysm, threads, 1, 5)
@@ -287,6 +310,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

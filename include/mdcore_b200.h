@@ -350,8 +350,16 @@ int engine_cuda_setstream(struct engine *e, void *stream);
 int engine_cuda_kernel_times(struct engine *e, float *total_ms, float *sweep_ms);
 /* Measured FP32 FMA throughput of a device in TFLOP/s (a register-only FMA loop). */
 int engine_cuda_fp32_peak(int device, float *tflops);
-/* Sweep kernel launch parameters (warps per block, i-chunks per warp); 0 = autotuned. */
-int engine_cuda_settune(struct engine *e, int warps, int unroll);
+/* Sweep kernel launch parameters: warps per block (0 = default) and plain = 1 for the
+ * plain form (one block per task, IEEE sqrt/div) instead of the persistent queue. */
+int engine_cuda_settune(struct engine *e, int warps, int plain);
+/* Replaces the device task-queue order (a permutation of 0..ntasks-1). */
+int engine_cuda_setorder(struct engine *e, const int *order, int n);
+/* Per-task clock64 records of the persistent sweep: enable/disable, and read the last
+ * launch's (start, end) pairs and SM ids when clocks/sms are non-NULL. */
+int engine_cuda_taskclocks(struct engine *e, int enable, long long *clocks, int *sms, int n);
+/* Number of device tasks (self + pair). */
+int engine_cuda_ntasks(struct engine *e);
 
 #ifdef __cplusplus
 }

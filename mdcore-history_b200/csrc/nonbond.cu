@@ -11,11 +11,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+#include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cuda_runtime.h>
 #include "mdcore_b200.h"
 #include "internal.h"
-#include "nb_kernels.cuh"
+#include "nb_tuned.cuh"
 
 using namespace nb;
 
@@ -36,6 +38,14 @@ struct NbState {
     int npots = 0, ncoef = 0, max_type = 0;
     // tuning
     int warps = 4;
+    bool has_excl = false;
+    int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
+    int* d_order = nullptr;        // task queue order
+    int* d_counter = nullptr;      // queue head
+    long long* d_task_clock = nullptr;
+    int* d_task_sm = nullptr;
+    int record_clock = 0;
+    int sm_count = 0;
     // device buffers
     float4* d_xq = nullptr;
     int* d_pid = nullptr;
@@ -150,6 +160,76 @@ int pack_cells(struct engine* e, NbState* st) {
     return slot;
 }
 
+template <int NW>
+int launch_plain_nw(NbState* st, const Params& P, int cap, size_t smem) {
+    CU(cudaFuncSetAttribute(sweep_tasks<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sweep_tasks<NW><<<st->ntasks, NW * 32, smem, st->stream>>>(P, cap);
+    CU(cudaGetLastError());
+    return 0;
+}
+
+int launch_plain(NbState* st, const Params& P, int cap) {
+    int nw = st->warps;
+    size_t smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    while (smem > 200 * 1024 && nw > 1) {
+        nw /= 2;
+        smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    }
+    if (smem > 220 * 1024) {
+        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    switch (nw) {
+        case 1: return launch_plain_nw<1>(st, P, cap, smem);
+        case 2: return launch_plain_nw<2>(st, P, cap, smem);
+        case 8: return launch_plain_nw<8>(st, P, cap, smem);
+        default: return launch_plain_nw<4>(st, P, cap, smem);
+    }
+}
+
+template <int NW, bool EX>
+int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
+    CU(cudaFuncSetAttribute(sweep_tuned<NW, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_tuned<NW, EX>, NW * 32, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int grid = st->sm_count * per_sm;
+    sweep_tuned<NW, EX><<<grid, NW * 32, smem, st->stream>>>(T, cap);
+    CU(cudaGetLastError());
+    return 0;
+}
+
+int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
+    (void)e;
+    const int cap = cap4 + 8;
+    TunedParams T;
+    T.p = P;
+    T.order = st->d_order;
+    T.counter = st->d_counter;
+    T.task_clock = st->record_clock ? st->d_task_clock : nullptr;
+    T.task_sm = st->record_clock ? st->d_task_sm : nullptr;
+    CU(cudaMemsetAsync(st->d_counter, 0, sizeof(int), st->stream));
+    int nw = st->warps;
+    size_t smem = tuned_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    while (smem > 200 * 1024 && nw > 1) {
+        nw /= 2;
+        smem = tuned_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    }
+    if (smem > 220 * 1024) {
+        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    const bool ex = st->has_excl;
+    switch (nw) {
+        case 1: return ex ? launch_tuned_nw<1, true>(st, T, cap, smem) : launch_tuned_nw<1, false>(st, T, cap, smem);
+        case 2: return ex ? launch_tuned_nw<2, true>(st, T, cap, smem) : launch_tuned_nw<2, false>(st, T, cap, smem);
+        case 8: return ex ? launch_tuned_nw<8, true>(st, T, cap, smem) : launch_tuned_nw<8, false>(st, T, cap, smem);
+        default: return ex ? launch_tuned_nw<4, true>(st, T, cap, smem) : launch_tuned_nw<4, false>(st, T, cap, smem);
+    }
+}
+
 int launch_kernels(struct engine* e, NbState* st) {
     struct space* s = &e->s;
     CU(cudaMemsetAsync(st->d_force, 0, sizeof(unsigned long long) * 3 * (size_t)st->h_cstart[s->nr_cells],
@@ -191,36 +271,8 @@ int launch_kernels(struct engine* e, NbState* st) {
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
 
     CU(cudaEventRecord(st->evs0, st->stream));
-    int nw = st->warps;
-    size_t smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
-    while (smem > 200 * 1024 && nw > 1) {
-        nw /= 2;
-        smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
-    }
-    if (smem > 220 * 1024) {
-        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
-                      __func__, __FILE__);
-        return engine_err = engine_err_maxparts;
-    }
-    switch (nw) {
-        case 1:
-            CU(cudaFuncSetAttribute(sweep_tasks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sweep_tasks<1><<<st->ntasks, 32, smem, st->stream>>>(P, cap);
-            break;
-        case 2:
-            CU(cudaFuncSetAttribute(sweep_tasks<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sweep_tasks<2><<<st->ntasks, 64, smem, st->stream>>>(P, cap);
-            break;
-        case 8:
-            CU(cudaFuncSetAttribute(sweep_tasks<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sweep_tasks<8><<<st->ntasks, 256, smem, st->stream>>>(P, cap);
-            break;
-        default:
-            CU(cudaFuncSetAttribute(sweep_tasks<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sweep_tasks<4><<<st->ntasks, 128, smem, st->stream>>>(P, cap);
-            break;
-    }
-    CU(cudaGetLastError());
+    int rc = st->plain ? launch_plain(st, P, cap) : launch_tuned(e, st, P, cap);
+    if (rc < 0) return rc;
     CU(cudaEventRecord(st->evs1, st->stream));
     return 0;
 }
@@ -264,7 +316,8 @@ extern "C" int nb_device_free(struct engine* e) {
     cudaSetDevice(st->device);
     void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
                    st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
-                   st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist};
+                   st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
+                   st->d_counter, st->d_task_clock, st->d_task_sm};
     for (void* p : dev) cudaFree(p);
     void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
     for (void* p : host) cudaFreeHost(p);
@@ -299,11 +352,11 @@ extern "C" int engine_cuda_setdevices(struct engine* e, int nr_devices, int* ids
     return engine_cuda_setdevice(e, ids[0]);
 }
 
-extern "C" int engine_cuda_settune(struct engine* e, int warps, int unroll) {
-    (void)unroll;
+extern "C" int engine_cuda_settune(struct engine* e, int warps, int plain) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8) return engine_err_range;
     state(e)->warps = warps ? warps : 4;
+    state(e)->plain = plain ? 1 : 0;
     return 0;
 }
 
@@ -383,6 +436,27 @@ extern "C" int engine_cuda_load(struct engine* e) {
     CU(cudaMemcpy(st->d_tasks, tasks.data(), tasks.size() * sizeof(TaskRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->d_tshift, tshift.data(), tshift.size() * sizeof(float4), cudaMemcpyHostToDevice));
 
+    // Task queue: initial order by decreasing particle-count product (self: n(n-1)/2), the
+    // load-balancing weight of the reference's task ranking (src/engine.c:574-699).
+    CU(cudaDeviceGetAttribute(&st->sm_count, cudaDevAttrMultiProcessorCount, st->device));
+    {
+        std::vector<std::pair<double, int>> w(st->ntasks);
+        for (int t = 0; t < st->ntasks; t++) {
+            const TaskRec& r = tasks[t];
+            double ni = s->cells[r.ci].count, nj = s->cells[r.cj].count;
+            w[t] = {r.sid < 0 ? 0.5 * ni * (ni - 1) : ni * nj, t};
+        }
+        std::stable_sort(w.begin(), w.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+            return a.first > b.first;
+        });
+        std::vector<int> order(st->ntasks > 0 ? st->ntasks : 1, 0);
+        for (int t = 0; t < st->ntasks; t++) order[t] = w[t].second;
+        if (dev_alloc(&st->d_order, order.size()) || dev_alloc(&st->d_counter, 1) ||
+            dev_alloc(&st->d_task_clock, 2 * order.size()) || dev_alloc(&st->d_task_sm, order.size()))
+            return engine_err_cuda;
+        CU(cudaMemcpy(st->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+
     // Cells: sort-direction masks and the offset/count staging.
     std::vector<unsigned> cmask(st->ncells);
     for (int c = 0; c < st->ncells; c++) cmask[c] = s->cells[c].sortmask;
@@ -399,6 +473,7 @@ extern "C" int engine_cuda_load(struct engine* e) {
     // list for the rest.  Each exclusion is recorded on both particles.
     const int nid = s->size_parts > 0 ? s->size_parts : 1;
     st->nid = nid;
+    st->has_excl = e->nr_exclusions > 0;
     std::vector<unsigned> emask(nid, 0u);
     std::vector<int> cnt(nid + 1, 0);
     for (int k = 0; k < e->nr_exclusions; k++) {
@@ -592,4 +667,41 @@ extern "C" int engine_cuda_fp32_peak(int device, float* tflops) {
     cudaFree(out);
     *tflops = best;
     return 0;
+}
+
+// Replaces the task queue order (a permutation of 0..nr_tasks-1).
+extern "C" int engine_cuda_setorder(struct engine* e, const int* order, int n) {
+    if (e == nullptr || e->cuda == nullptr || order == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    if (n != st->ntasks) return engine_err_range;
+    std::vector<char> seen(n, 0);
+    for (int k = 0; k < n; k++) {
+        if (order[k] < 0 || order[k] >= n || seen[order[k]]) return engine_err_range;
+        seen[order[k]] = 1;
+    }
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    CU(cudaMemcpy(st->d_order, order, sizeof(int) * n, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// Switches per-task clock64 recording on or off; reads the last launch's records
+// (start, end, SM of every task) when the output pointers are given.
+extern "C" int engine_cuda_taskclocks(struct engine* e, int enable, long long* clocks, int* sms, int n) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    if (clocks != nullptr || sms != nullptr) {
+        if (n != st->ntasks) return engine_err_range;
+        if (clocks) CU(cudaMemcpy(clocks, st->d_task_clock, sizeof(long long) * 2 * n, cudaMemcpyDeviceToHost));
+        if (sms) CU(cudaMemcpy(sms, st->d_task_sm, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    st->record_clock = enable ? 1 : 0;
+    return 0;
+}
+
+extern "C" int engine_cuda_ntasks(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return state(e)->ntasks;
 }

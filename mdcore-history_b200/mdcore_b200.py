@@ -79,6 +79,9 @@ def lib() -> C.CDLL:
         "engine_nonbond_stats": (C.c_int, [vp, P(NbStats)]),
         "engine_set_dt": (C.c_int, [vp, C.c_double]),
         "engine_cuda_kernel_times": (C.c_int, [vp, P(C.c_float), P(C.c_float)]),
+        "engine_cuda_setorder": (C.c_int, [vp, ip, C.c_int]),
+        "engine_cuda_taskclocks": (C.c_int, [vp, C.c_int, P(C.c_longlong), ip, C.c_int]),
+        "engine_cuda_ntasks": (C.c_int, [vp]),
         "engine_cuda_fp32_peak": (C.c_int, [C.c_int, P(C.c_float)]),
         "engine_zero_forces": (C.c_int, [vp]),
         "potential_create_LJ126": (P(Potential), [C.c_double] * 5),
@@ -216,8 +219,29 @@ class Engine:
         _check(self.lib.engine_cuda_kernel_times(self.ptr, C.byref(a), C.byref(b)), "engine_cuda_kernel_times")
         return a.value, b.value
 
-    def tune(self, warps: int):
-        _check(self.lib.engine_cuda_settune(self.ptr, warps, 0), "engine_cuda_settune")
+    def tune(self, warps: int = 0, plain: bool = False):
+        """warps per block (0 = default); plain=True selects the one-block-per-task form."""
+        _check(self.lib.engine_cuda_settune(self.ptr, warps, 1 if plain else 0), "engine_cuda_settune")
+
+    def ntasks(self) -> int:
+        return _check(self.lib.engine_cuda_ntasks(self.ptr), "engine_cuda_ntasks")
+
+    def set_order(self, order):
+        o = np.ascontiguousarray(order, np.int32)
+        _check(self.lib.engine_cuda_setorder(self.ptr, _iptr(o), len(o)), "engine_cuda_setorder")
+
+    def task_clocks(self, enable: bool = True, read: bool = False):
+        """Enables per-task clock64 records; with read=True returns (clocks[n,2], sm[n]) of
+        the last launch."""
+        if not read:
+            _check(self.lib.engine_cuda_taskclocks(self.ptr, int(enable), None, None, 0), "engine_cuda_taskclocks")
+            return None
+        n = self.ntasks()
+        clk = np.zeros((n, 2), np.int64)
+        sm = np.zeros(n, np.int32)
+        _check(self.lib.engine_cuda_taskclocks(self.ptr, int(enable), clk.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                               _iptr(sm), n), "engine_cuda_taskclocks")
+        return clk, sm
 
     # -- readback --------------------------------------------------------------------
     def forces(self) -> np.ndarray:

@@ -23,10 +23,10 @@ pytestmark = pytest.mark.gpu
 SYSTEMS = ["argon_1372.npz", "water_3000.npz"]
 
 
-def evaluate(sysm, flags=M.engine_flag_cuda, warps=0):
+def evaluate(sysm, flags=M.engine_flag_cuda, warps=0, plain=False):
     e = M.Engine.from_system(sysm, flags=flags)
-    if warps:
-        e.tune(warps)
+    if warps or plain:
+        e.tune(warps, plain)
     e.nonbond()
     return e, e.forces(), e.stats()
 
@@ -46,10 +46,11 @@ def check_against_oracle(sysm, tables, f, st, label):
     return o, err
 
 
+@pytest.mark.parametrize("plain", [False, True], ids=["tuned", "plain"])
 @pytest.mark.parametrize("fname", SYSTEMS)
-def test_forces_energy_counts_vs_oracle(fname):
+def test_forces_energy_counts_vs_oracle(fname, plain):
     sysm, ref = load_golden(fname)
-    e, f, st = evaluate(sysm)
+    e, f, st = evaluate(sysm, plain=plain)
     check_against_oracle(sysm, ref["tables"], f, st, fname)
     # The reference's own FP32 forces (golden) agree with ours to its precision.
     err = force_errors(f, ref["f"])
@@ -76,12 +77,43 @@ def test_sort_keys_bit_exact(fname):
     e.close()
 
 
+@pytest.mark.parametrize("plain", [False, True], ids=["tuned", "plain"])
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
-def test_launch_shapes_agree(warps):
+def test_launch_shapes_agree(warps, plain):
     """Every block size gives the same pair set and forces within FP32 rounding."""
     sysm, ref = load_golden("water_3000.npz")
-    e, f, st = evaluate(sysm, warps=warps)
-    check_against_oracle(sysm, ref["tables"], f, st, f"warps={warps}")
+    e, f, st = evaluate(sysm, warps=warps, plain=plain)
+    check_against_oracle(sysm, ref["tables"], f, st, f"warps={warps} plain={plain}")
+    e.close()
+
+
+@pytest.mark.parametrize("fname", SYSTEMS)
+def test_forces_independent_of_task_order(fname):
+    """Fixed-point accumulation: any queue order gives bit-identical forces and energy."""
+    sysm, _ = load_golden(fname)
+    e = M.Engine.from_system(sysm)
+    e.nonbond()
+    f1, s1 = e.forces(), e.stats()
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        e.set_order(rng.permutation(e.ntasks()))
+        e.nonbond()
+        f2, s2 = e.forces(), e.stats()
+        assert np.array_equal(f1, f2)
+        assert s1.epot == s2.epot and s1.virial == s2.virial and s1.pairs == s2.pairs
+    e.close()
+
+
+def test_task_clocks_recorded():
+    sysm, _ = load_golden("water_3000.npz")
+    e = M.Engine.from_system(sysm)
+    e.task_clocks(True)
+    e.nonbond()
+    clk, sm = e.task_clocks(False, read=True)
+    nonempty = clk[:, 1] > 0
+    assert nonempty.sum() == e.ntasks()
+    assert (clk[nonempty, 1] >= clk[nonempty, 0]).all()
+    assert (sm >= 0).all()
     e.close()
 
 
