@@ -278,7 +278,7 @@ def ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "sweep_tasks", "kernel_ms": ms_sweep,
+                         "kernel": "sweep_tuned", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
             "plain": {"value": world * pairs / (plain_ms / args.steps * 1e-3), "ms_per_step": plain_ms / args.steps,

@@ -22,11 +22,23 @@ namespace nb {
 __constant__ float c_axes[13][3];
 
 // ---------------------------------------------------------------- sort
-__global__ void __launch_bounds__(256) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+// Keys of one sort direction are ranked by a counting sort on the top 8 bits of the 16-bit
+// distance (256 buckets in shared memory) followed by an exact rank inside the bucket:
+// position = (keys in farther buckets) + (keys of the same bucket with a larger distance,
+// or an equal distance and a smaller storage index).  The result is the stable
+// descending order, independent of the order in which threads reach the atomics.
+constexpr int kSortBuckets = 256;
+
+__global__ void __launch_bounds__(128) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
                                                   const int* __restrict__ ccount, const unsigned* __restrict__ cmask,
                                                   unsigned* __restrict__ keys, float dscale, float bias,
                                                   unsigned long long* acc) {
-    extern __shared__ unsigned skey[];
+    extern __shared__ unsigned sort_smem[];
+    unsigned* skey = sort_smem;                          // n keys
+    unsigned short* members = reinterpret_cast<unsigned short*>(sort_smem + kMaxPartsPerCell);  // bucket-major
+    int* bcount = reinterpret_cast<int*>(sort_smem + kMaxPartsPerCell + kMaxPartsPerCell / 2);
+    int* bstart = bcount + kSortBuckets;
+    int* bfill = bstart + kSortBuckets + 1;
     const int c = blockIdx.x;
     const int n = ccount[c];
     if (n <= 0) return;
@@ -40,6 +52,8 @@ __global__ void __launch_bounds__(256) sort_cells(const float4* __restrict__ xq,
     for (int sid = 0; sid < 13; ++sid) {
         if (!((mask >> sid) & 1u)) continue;
         const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
+        for (int b = threadIdx.x; b < kSortBuckets; b += blockDim.x) { bcount[b] = 0; bfill[b] = 0; }
+        __syncthreads();
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
             const float4 x = xq[start + k];
             // dscale * (bias + x.n), evaluated left to right without contraction.
@@ -47,22 +61,53 @@ __global__ void __launch_bounds__(256) sort_cells(const float4* __restrict__ xq,
             d = __fadd_rn(d, __fmul_rn(x.y, ny));
             d = __fadd_rn(d, __fmul_rn(x.z, nz));
             d = __fmul_rn(dscale, d);
-            skey[k] = ((unsigned)k << 16) | __float2uint_rz(d);
+            const unsigned key = ((unsigned)k << 16) | __float2uint_rz(d);
+            skey[k] = key;
+            atomicAdd(&bcount[min((int)((key & 0xffffu) >> 7), kSortBuckets - 1)], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {          // bucket starts in descending bucket order (warp scan)
+            const int lane = threadIdx.x;
+            int run = 0;
+            for (int base = 0; base < kSortBuckets; base += 32) {
+                const int b = kSortBuckets - 1 - (base + lane);
+                const int v = bcount[b];
+                int incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                bstart[b] = run + incl - v;
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int b = min((int)((skey[k] & 0xffffu) >> 7), kSortBuckets - 1);
+            members[bstart[b] + atomicAdd(&bfill[b], 1)] = (unsigned short)k;
         }
         __syncthreads();
         unsigned* out = keys + 13 * (size_t)start + (size_t)sid * pad;
         for (int k = threadIdx.x; k < n; k += blockDim.x) {
             const unsigned mine = skey[k];
             const unsigned md = mine & 0xffffu;
-            int rank = 0;
-            for (int m = 0; m < n; ++m) {
-                const unsigned od = skey[m] & 0xffffu;
-                rank += (od > md) | ((od == md) & (m < k));
+            const int b = min((int)(md >> 7), kSortBuckets - 1);
+            const int b0 = bstart[b], nb = bcount[b];
+            int rank = b0;
+            for (int m = 0; m < nb; ++m) {
+                const int o = members[b0 + m];
+                const unsigned od = skey[o] & 0xffffu;
+                rank += (od > md) | ((od == md) & (o < k));
             }
             out[rank] = mine;
         }
         __syncthreads();
     }
+}
+
+__host__ inline size_t sort_smem_bytes() {
+    return (size_t)kMaxPartsPerCell * 4 + (size_t)kMaxPartsPerCell * 2 + (size_t)(3 * kSortBuckets + 1) * 4;
 }
 
 // ---------------------------------------------------------------- potential evaluation

@@ -6,18 +6,26 @@
 //    queue, e.g. longest task first); the tables are staged into shared memory once per CTA;
 //  * two shared-memory stages: while a CTA sweeps one task, the TMA bulk copies of the next
 //    task's cells are already in flight;
-//  * r = r2 * rsqrt(r2), f = U'(r) * (1/halfwidth) * rsqrt(r2): one MUFU op instead of an
-//    IEEE square root and division (the cutoff test still uses the exactly rounded r2);
+//  * f = U'(r) * (1/halfwidth) * rsqrt(r2) with one Newton step instead of an IEEE
+//    division (r itself stays correctly rounded, and the cutoff test uses the exactly
+//    rounded r2);
 //  * Newton's third law through a register reduce-scatter: each lane keeps its j
 //    contributions of 8 consecutive sweep steps and the warp sums them with 9 shuffles per
 //    component (xor 1, 2, 4 exchange halves; xor 8, 16 add), after which lane m holds the
 //    warp total for step m.  The order of additions is fixed, so task partials stay
 //    independent of scheduling;
 //  * the j record carries its sort distance and type in one 16-byte shared-memory word;
-//  * energy and virial are summed in float over an 8-step window and in double beyond;
+//  * energy and virial are summed per pair in double (float partial sums of cancelling
+//    Coulomb terms would cost ~1e-6 of the total);
 //  * optional per-task clock64 records (start, end, SM) for the learned scheduler.
 #pragma once
 #include "nb_kernels.cuh"
+
+// Resident threads per SM the register allocation of sweep_tuned is sized for (launch
+// bounds): 640 threads = 20 warps leaves ~100 registers per thread.
+#ifndef MDB_TUNED_THREADS_PER_SM
+#define MDB_TUNED_THREADS_PER_SM 640
+#endif
 
 namespace nb {
 
@@ -48,7 +56,7 @@ __host__ __device__ inline size_t tuned_smem_bytes(int cap, int nw, int ncoef, i
     size_t b = 64;                                   // 2 mbarriers + queue slots
     b += 2 * tuned_stage_bytes(cap);                 // double-buffered raw cells
     b += (size_t)cap * 16 * 2;                       // js (sorted j, dist|type in w), fi
-    b += (size_t)cap * 4 * 2;                        // jid, jloc
+    b += (size_t)cap * 4 * 3;                        // jid, jloc, jdist
     b += (size_t)nw * cap * 16;                      // per-warp j partial forces
     b += (size_t)npots * 16;
     b += (size_t)((ncoef + 3) & ~3) * 4;
@@ -98,12 +106,13 @@ __device__ __forceinline__ void issue_task(const Params& P, int t, const Stage& 
     }
 }
 
-// Fast table evaluation: index as the reference computes it (rounded ops), r from rsqrt.
+// Table evaluation with fused multiply-adds (interval index included: a different
+// rounding can only move r to the neighbouring interval at a node, where the two pieces
+// agree), 1/r supplied by the caller.
 __device__ __forceinline__ void eval_table_fast(const float* __restrict__ coef, float4 info, int nmax, float r,
                                                 float rinv, float& e, float& f) {
-    float t = __fadd_rn(info.x, __fmul_rn(r, __fadd_rn(info.y, __fmul_rn(r, info.z))));
-    int ind = __float2int_rz(fmaxf(0.0f, t));
-    ind = min(ind, nmax);
+    const float t = fmaf(r, fmaf(r, info.z, info.y), info.x);
+    const int ind = min(__float2int_rz(fmaxf(0.0f, t)), nmax);
     const float4* c = reinterpret_cast<const float4*>(coef + __float_as_int(info.w) + 8 * ind);
     const float4 c0 = c[0], c1 = c[1];
     const float x = (r - c0.x) * c0.y;
@@ -115,6 +124,27 @@ __device__ __forceinline__ void eval_table_fast(const float* __restrict__ coef, 
     eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.w);
     e = ee;
     f = eff * c0.y * rinv;
+}
+
+// Warp reduce-scatter of 4 values per lane: afterwards lane l holds the sum over the warp
+// of v[l & 3] (lanes l, l+4, ..., l+28 hold the same total).  Six shuffles.
+__device__ __forceinline__ float reduce_scatter4(const float (&v)[4], int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool b0 = lane & 1, b1 = lane & 2;
+    float a[2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const float send = b0 ? v[2 * m] : v[2 * m + 1];
+        const float keep = b0 ? v[2 * m + 1] : v[2 * m];
+        a[m] = keep + __shfl_xor_sync(FULL, send, 1);
+    }
+    const float send = b1 ? a[0] : a[1];
+    const float keep = b1 ? a[1] : a[0];
+    float d = keep + __shfl_xor_sync(FULL, send, 2);
+    d += __shfl_xor_sync(FULL, d, 4);
+    d += __shfl_xor_sync(FULL, d, 8);
+    d += __shfl_xor_sync(FULL, d, 16);
+    return d;
 }
 
 // Warp reduce-scatter of 8 values per lane: afterwards lane l holds sum over the warp of
@@ -145,205 +175,249 @@ __device__ __forceinline__ float reduce_scatter8(const float (&v)[8], int lane) 
     return d;
 }
 
-template <int NW, bool HAS_EXCL>
-__global__ void __launch_bounds__(NW * 32) sweep_tuned(TunedParams T, int cap) {
+// Shared memory of one worker warp (cap = largest cell rounded up to 4, plus 8 spare rows
+// that the 4-step sweep windows may read past the end of the j list).
+__host__ __device__ inline size_t warp_slice_bytes(int cap) { return 16 + (size_t)cap * 56; }
+
+__host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, int npots, int mt) {
+    size_t b = (size_t)nw * warp_slice_bytes(cap);
+    b += (size_t)npots * 16;
+    b += (size_t)((ncoef + 3) & ~3) * 4;
+    b += (size_t)((npots + 3) & ~3) * 4;
+    b += (size_t)((mt * mt + 3) & ~3) * 4;
+    return b;
+}
+
+// Persistent worker warps: every warp pops whole tasks from the device queue, stages the
+// j cell (positions, ids, sort keys) and the i cell's sort keys in its own shared-memory
+// slice with TMA bulk copies, sweeps all i chunks of the task itself and writes the
+// task's forces and energy.  Warps never wait for each other.
+template <int NW, bool HAS_EXCL, bool ONE_POT>
+__global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const Params& P = T.p;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mt = P.max_type;
 
-    // ---- shared memory carve-up
-    unsigned char* sp = smem_raw;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sp);
-    int* qslot = reinterpret_cast<int*>(sp + 16);
-    sp += 64;
-    unsigned char* const stage_base = sp;
-    sp += 2 * tuned_stage_bytes(cap);
-    float4* js = reinterpret_cast<float4*>(sp); sp += (size_t)cap * 16;     // cap includes 8 spare rows
-    float4* fis = reinterpret_cast<float4*>(sp); sp += (size_t)cap * 16;
-    int* jid = reinterpret_cast<int*>(sp); sp += (size_t)cap * 4;
-    int* jloc = reinterpret_cast<int*>(sp); sp += (size_t)cap * 4;
-    float4* fj = reinterpret_cast<float4*>(sp); sp += (size_t)NW * cap * 16;
+    // ---- shared tables (once per block), then the warp's slice
+    unsigned char* sp = smem_raw + (size_t)NW * warp_slice_bytes(cap);
     float4* potinfo = reinterpret_cast<float4*>(sp); sp += (size_t)P.npots * 16;
     float* coef = reinterpret_cast<float*>(sp); sp += (size_t)((P.ncoef + 3) & ~3) * 4;
     int* potn = reinterpret_cast<int*>(sp); sp += (size_t)((P.npots + 3) & ~3) * 4;
-    int* potidx = reinterpret_cast<int*>(sp); sp += (size_t)((mt * mt + 3) & ~3) * 4;
-    double* wred = reinterpret_cast<double*>(sp); sp += (size_t)NW * 16;
-    unsigned long long* cred = reinterpret_cast<unsigned long long*>(sp);
-
+    int* potidx = reinterpret_cast<int*>(sp);
     for (int k = tid; k < P.ncoef; k += NW * 32) coef[k] = P.coef[k];
     for (int k = tid; k < P.npots; k += NW * 32) { potinfo[k] = P.potinfo[k]; potn[k] = P.potn[k]; }
     for (int k = tid; k < mt * mt; k += NW * 32) potidx[k] = P.potidx[k];
-    if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+
+    unsigned char* wp = smem_raw + (size_t)warp * warp_slice_bytes(cap);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wp); wp += 16;
+    float4* xraw = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;   // j cell as copied
+    float4* js = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;     // j cell, sweep order
+    float4* fj = xraw;            // j (and self) forces, once js has been built from xraw
+    int* pidraw = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    unsigned* keyj = reinterpret_cast<unsigned*>(wp); wp += (size_t)cap * 4;
+    unsigned* keyi = reinterpret_cast<unsigned*>(wp); wp += (size_t)cap * 4;
+    int* jid = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    int* jloc = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    int* jdist = reinterpret_cast<int*>(wp);
+    if (lane == 0) {
+        mbar_init(bar, 1);
         mbar_fence_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        const int q0 = atomicAdd(T.counter, 1);
-        qslot[0] = q0;
-        if (q0 < P.ntasks) issue_task(P, T.order[q0], stage_at(stage_base, cap, 0), &bars[0]);
     }
     __syncthreads();
 
     unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
-    for (int it = 0;; ++it) {
-        const int s = it & 1;
-        const int q = qslot[s];
+    unsigned phase = 0;                   // completed phases of this warp's mbarrier
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(T.counter, 1);
+        q = __shfl_sync(FULL, q, 0);
         if (q >= P.ntasks) break;
         const int t = T.order[q];
-        if (tid == 0) {                       // prefetch the next task into the other stage
-            const int q1 = atomicAdd(T.counter, 1);
-            qslot[s ^ 1] = q1;
-            if (q1 < P.ntasks) issue_task(P, T.order[q1], stage_at(stage_base, cap, s ^ 1), &bars[s ^ 1]);
-        }
         const TaskRec tr = P.tasks[t];
         const bool self = tr.sid < 0;
         const int ni = P.ccount[tr.ci], nj = P.ccount[tr.cj];
+        if (ni == 0 || nj == 0 || (self && ni < 2)) continue;
+        if (ni + 8 > cap || nj + 8 > cap) { status |= kStatusCellOverflow; continue; }
         const int si = P.cstart[tr.ci], sj = P.cstart[tr.cj];
-        const bool ok = mbar_wait_bounded(&bars[s], (it >> 1) & 1);
-        if (__syncthreads_or(!ok)) {
+        const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
+        long long t_start = 0;
+        __syncwarp();
+        if (lane == 0) {
+            if (T.task_clock) t_start = clock64();
+            fence_proxy_async();
+            mbar_arrive_expect_tx(bar, self ? (uint32_t)padj * 20u : (uint32_t)padj * 24u + (uint32_t)padi * 4u);
+            bulk_g2s(xraw, P.xq + sj, padj * 16, bar);
+            bulk_g2s(pidraw, P.pid + sj, padj * 4, bar);
+            if (!self) {
+                bulk_g2s(keyj, P.keys + 13 * (size_t)sj + (size_t)tr.sid * padj, padj * 4, bar);
+                bulk_g2s(keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, bar);
+            }
+        }
+        const int nout = self ? ni : nj;
+        if (!__all_sync(FULL, mbar_wait_bounded(bar, phase & 1))) {
             status |= kStatusCopyTimeout;
-            if (tid == 0) mbar_wait_bounded(&bars[s ^ 1], ((it + 1) >> 1) & 1);
+            mbar_wait_bounded(bar, phase & 1);   // second bounded chance for copies in flight
             break;
         }
-        if (ni == 0 || nj == 0 || (self && ni < 2)) {
-            __syncthreads();
-            continue;
-        }
-        if (ni + 8 > cap || nj + 8 > cap) {   // host sizes cap; guard anyway
-            status |= kStatusCellOverflow;
-            __syncthreads();
-            continue;
-        }
-        long long t_start = 0;
-        if (tid == 0 && T.task_clock) t_start = clock64();
-        const Stage S = stage_at(stage_base, cap, s);
-
-        // j records in ascending projected distance: xyz, w = type | dist << 16.
+        ++phase;
         if (!self) {
-            for (int k = tid; k < nj; k += NW * 32) {
-                const unsigned key = S.keyj[nj - 1 - k];
+            for (int k = lane; k < nj; k += 32) {
+                const unsigned key = keyj[nj - 1 - k];
                 const int loc = key >> 16;
-                float4 x = S.xj[loc];
-                x.w = __int_as_float((__float_as_int(x.w) & 0xffff) | (int)((key & 0xffffu) << 16));
-                js[k] = x;
-                jid[k] = S.pidj[loc];
+                js[k] = xraw[loc];
+                jid[k] = pidraw[loc];
                 jloc[k] = loc;
+                jdist[k] = key & 0xffff;
             }
         } else {
-            for (int k = tid; k < nj; k += NW * 32) {
-                js[k] = S.xj[k];
-                jid[k] = S.pidj[k];
-            }
+            for (int k = lane; k < nj; k += 32) js[k] = xraw[k];
         }
-        for (int k = tid; k < NW * nj; k += NW * 32) {
-            const int w = k / nj, kk = k - w * nj;
-            fj[w * cap + kk] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        __syncthreads();
+        __syncwarp();
+        for (int k = lane; k < nout; k += 32) fj[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+        const float4* __restrict__ jpos = js;
+        const int* __restrict__ jids = self ? pidraw : jid;
 
         const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
         const int dnshift = tr.dnshift;
-        float4* myfj = fj + warp * cap;
         double e_task = 0.0, v_task = 0.0;
         const int nchunks = (ni + 31) >> 5;
-        const int jd0 = self ? 0 : (int)((unsigned)__float_as_int(js[0].w) >> 16);
+        const int jd0 = self ? 0 : jdist[0];
 
-        for (int ch = warp; ch < nchunks; ch += NW) {
+        for (int ch = 0; ch < nchunks; ++ch) {
             const int ii = ch * 32 + lane;
             bool valid = ii < ni;
-            int loc = ii, di = 0;
-            if (!self) {
-                const unsigned key = valid ? S.keyi[ii] : 0u;
+            int loc = ii, len = 0;
+            if (self) {
+                len = valid ? ii : 0;                       // pairs j < i
+            } else {
+                const unsigned key = valid ? keyi[ii] : 0u;
                 loc = key >> 16;
-                di = key & 0xffff;
+                const int di = key & 0xffff;
                 if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= P.dmaxdist);
-                if (!__any_sync(FULL, valid)) break;
+                if (!__any_sync(FULL, valid)) break;        // later chunks lie farther from cell j
+                if (valid) {
+                    if (P.unsorted) {
+                        len = nj;
+                    } else {                                // j with dist < lim form a prefix
+                        const int lim = P.dmaxdist - dnshift + di;
+                        int lo = 0, hi = nj;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (jdist[mid] < lim) lo = mid + 1; else hi = mid;
+                        }
+                        len = lo;
+                    }
+                }
             }
+            const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-            int pidi = -1, exlo = 0, exhi = 0;
+            int pidi = 0, exlo = 0, exhi = 0;
             unsigned emask = 0u;
             if (valid) {
-                xi = self ? S.xj[loc] : S.xi[loc];
+                xi = self ? js[loc] : P.xq[si + loc];
                 if (HAS_EXCL) {
-                    pidi = self ? S.pidj[loc] : S.pidi[loc];
+                    pidi = self ? pidraw[loc] : P.pid[si + loc];
                     emask = P.emask[pidi];
                     exlo = P.exoff[pidi];
                     exhi = P.exoff[pidi + 1];
                 }
             }
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
-            const int prow = (__float_as_int(xi.w) & 0xffff) * mt;
-            const int lim = P.dmaxdist - dnshift + di;
-            const int kend = self ? min(ch * 32 + 32, ni) - 1 : nj;
+            const int prow = __float_as_int(xi.w) * mt;
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
-            for (int k0 = 0; k0 < kend; k0 += 8) {
-                if (!self && !P.unsorted) {
-                    const int dk = (int)((unsigned)__float_as_int(js[k0].w) >> 16);
-                    if (!__any_sync(FULL, valid && dk < lim)) break;   // distances only grow with k
-                }
-                float vx[8], vy[8], vz[8];
-                float ew = 0.f, vw = 0.f;
+            float e_hi = 0.f, e_lo = 0.f;                   // Kahan-compensated energy
+            for (int k0 = 0; k0 < kmax; k0 += 4) {
+                float vx[4], vy[4], vz[4];
                 bool any_acc = false;
 #pragma unroll
-                for (int m = 0; m < 8; ++m) {
+                for (int m = 0; m < 4; ++m) {
                     const int k = k0 + m;
-                    const float4 xj = js[k];
-                    const int wbits = __float_as_int(xj.w);
-                    const int dk = (int)((unsigned)wbits >> 16);
-                    const bool act = valid && k < kend && (self ? (k < ii) : (P.unsorted || dk < lim));
+                    const float4 xj = jpos[k];
+                    const bool act = k < len;
                     const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
                     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                    const int pot = act ? potidx[prow + (wbits & 0xffff)] : -1;
+                    int pot = 0;
+                    if (!ONE_POT) pot = act ? potidx[prow + __float_as_int(xj.w)] : -1;
                     bool acc = act && pot >= 0 && r2 <= cut2;
                     ncand += act;
-                    if (HAS_EXCL && acc && excluded_pair(pidi, jid[k], emask, exlo, exhi, P.exlist)) {
-                        acc = false;
-                        ++nexcl;
+                    if (HAS_EXCL && acc) {
+                        const int d = jids[k] - pidi;
+                        bool ex;
+                        if ((unsigned)(d + 16) <= 32u)
+                            ex = (emask >> (d + 16 - (d > 0))) & (d != 0);
+                        else {
+                            ex = false;
+                            for (int qx = exlo; qx < exhi; ++qx) ex |= (P.exlist[qx] == pidi + d);
+                        }
+                        if (ex) { acc = false; ++nexcl; }
                     }
                     float wx = 0.f, wy = 0.f, wz = 0.f;
                     if (__any_sync(FULL, acc)) {
                         any_acc = true;
                         if (acc) {
-                            const float rinv = rsqrtf(r2);
+                            // 1/r: rsqrt plus one Newton step; r: r2/r corrected by one
+                            // residual step, which gives the correctly rounded square root
+                            // (the water energy is ~250x smaller than the sum of |pair
+                            // energies|, so unbiased 1-ulp errors in r would show at 1e-6).
+                            float rinv = rsqrtf(r2);
+                            rinv = fmaf(-0.5f * rinv, fmaf(r2 * rinv, rinv, -1.0f), rinv);
+                            float r = r2 * rinv;
+                            r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
                             float e, f;
-                            eval_table_fast(coef, potinfo[pot], potn[pot], r2 * rinv, rinv, e, f);
+                            eval_table_fast(coef, potinfo[pot], potn[pot], r, rinv, e, f);
                             wx = f * dx; wy = f * dy; wz = f * dz;
                             fix -= wx; fiy -= wy; fiz -= wz;
-                            ew += e;
-                            vw = fmaf(f, r2, vw);
+                            const float y = e - e_lo;
+                            const float tsum = e_hi + y;
+                            e_lo = (tsum - e_hi) - y;
+                            e_hi = tsum;
                             ++npairs;
                         }
                     }
                     vx[m] = wx; vy[m] = wy; vz[m] = wz;
                 }
                 if (any_acc) {
-                    const float tx = reduce_scatter8(vx, lane);
-                    const float ty = reduce_scatter8(vy, lane);
-                    const float tz = reduce_scatter8(vz, lane);
-                    if (lane < 8 && k0 + lane < kend) {
-                        float4 a = myfj[k0 + lane];
+                    const float tx = reduce_scatter4(vx, lane);
+                    const float ty = reduce_scatter4(vy, lane);
+                    const float tz = reduce_scatter4(vz, lane);
+                    if (lane < 4 && k0 + lane < kmax) {
+                        float4 a = fj[k0 + lane];
                         a.x += tx; a.y += ty; a.z += tz;
-                        myfj[k0 + lane] = a;
+                        fj[k0 + lane] = a;
                     }
-                    e_task += (double)ew;
-                    v_task += (double)vw;
                 }
             }
+            e_task += (double)e_hi - (double)e_lo;
+            __syncwarp();
             if (valid) {
                 if (self) {
-                    fis[loc] = make_float4(fix, fiy, fiz, 0.f);
+                    float4 a = fj[loc];
+                    a.x += fix; a.y += fiy; a.z += fiz;
+                    fj[loc] = a;
                 } else {
+                    // virial, i side: sum over pairs of r_ij.F_ij = sum_i (x_i - shift).F_i + sum_j x_j.F_j
+                    v_task += (double)pix * fix + (double)piy * fiy + (double)piz * fiz;
                     unsigned long long* fp = P.force + 3 * (size_t)(si + loc);
                     atomic_add_fixed(fp + 0, to_fixed(fix, status));
                     atomic_add_fixed(fp + 1, to_fixed(fiy, status));
                     atomic_add_fixed(fp + 2, to_fixed(fiz, status));
                 }
             }
+            __syncwarp();
+        }
+
+        for (int k = lane; k < nout; k += 32) {
+            const float4 a = fj[k];
+            const float4 xk = jpos[k];
+            v_task += (double)xk.x * a.x + (double)xk.y * a.y + (double)xk.z * a.z;
+            unsigned long long* fp = P.force + 3 * (size_t)(self ? (si + k) : (sj + jloc[k]));
+            atomic_add_fixed(fp + 0, to_fixed(a.x, status));
+            atomic_add_fixed(fp + 1, to_fixed(a.y, status));
+            atomic_add_fixed(fp + 2, to_fixed(a.z, status));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -351,36 +425,14 @@ __global__ void __launch_bounds__(NW * 32) sweep_tuned(TunedParams T, int cap) {
             v_task += __shfl_xor_sync(FULL, v_task, o);
         }
         if (lane == 0) {
-            wred[2 * warp] = e_task;
-            wred[2 * warp + 1] = v_task;
-        }
-        __syncthreads();
-
-        const int nout = self ? ni : nj;
-        for (int k = tid; k < nout; k += NW * 32) {
-            float4 a = self ? fis[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                const float4 b = fj[w * cap + k];
-                a.x += b.x; a.y += b.y; a.z += b.z;
-            }
-            unsigned long long* fp = P.force + 3 * (size_t)(self ? (si + k) : (sj + jloc[k]));
-            atomic_add_fixed(fp + 0, to_fixed(a.x, status));
-            atomic_add_fixed(fp + 1, to_fixed(a.y, status));
-            atomic_add_fixed(fp + 2, to_fixed(a.z, status));
-        }
-        if (tid == 0) {
-            double e = 0.0, v = 0.0;
-            for (int w = 0; w < NW; ++w) { e += wred[2 * w]; v += wred[2 * w + 1]; }
-            atomicAdd(&P.cell_epot[tr.ci], (unsigned long long)__double2ll_rn(e * kEnergyScale));
-            atomicAdd(&P.acc[kAccVirial], (unsigned long long)__double2ll_rn(v * kEnergyScale));
+            atomicAdd(&P.cell_epot[tr.ci], (unsigned long long)__double2ll_rn(e_task * kEnergyScale));
+            atomicAdd(&P.acc[kAccVirial], (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
             if (T.task_clock) {
                 T.task_clock[2 * t] = t_start;
                 T.task_clock[2 * t + 1] = clock64();
                 T.task_sm[t] = (int)smid();
             }
         }
-        __syncthreads();
     }
 
     // Counters: warp sums, one atomic per warp.

@@ -39,6 +39,7 @@ struct NbState {
     // tuning
     int warps = 4;
     bool has_excl = false;
+    bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
     int* d_order = nullptr;        // task queue order
     int* d_counter = nullptr;      // queue head
@@ -188,16 +189,25 @@ int launch_plain(NbState* st, const Params& P, int cap) {
     }
 }
 
-template <int NW, bool EX>
+template <int NW, bool EX, bool ONE>
 int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    CU(cudaFuncSetAttribute(sweep_tuned<NW, EX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = sweep_tuned<NW, EX, ONE>;
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_tuned<NW, EX>, NW * 32, smem));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
     if (per_sm < 1) per_sm = 1;
     const int grid = st->sm_count * per_sm;
-    sweep_tuned<NW, EX><<<grid, NW * 32, smem, st->stream>>>(T, cap);
+    kern<<<grid, NW * 32, smem, st->stream>>>(T, cap);
     CU(cudaGetLastError());
     return 0;
+}
+
+template <int NW>
+int launch_tuned_w(NbState* st, const TunedParams& T, int cap, size_t smem) {
+    const bool one = st->one_pot;
+    if (st->has_excl)
+        return one ? launch_tuned_nw<NW, true, true>(st, T, cap, smem) : launch_tuned_nw<NW, true, false>(st, T, cap, smem);
+    return one ? launch_tuned_nw<NW, false, true>(st, T, cap, smem) : launch_tuned_nw<NW, false, false>(st, T, cap, smem);
 }
 
 int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
@@ -211,22 +221,21 @@ int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
     T.task_sm = st->record_clock ? st->d_task_sm : nullptr;
     CU(cudaMemsetAsync(st->d_counter, 0, sizeof(int), st->stream));
     int nw = st->warps;
-    size_t smem = tuned_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    size_t smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
     while (smem > 200 * 1024 && nw > 1) {
         nw /= 2;
-        smem = tuned_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+        smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
     }
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
                       __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
-    const bool ex = st->has_excl;
     switch (nw) {
-        case 1: return ex ? launch_tuned_nw<1, true>(st, T, cap, smem) : launch_tuned_nw<1, false>(st, T, cap, smem);
-        case 2: return ex ? launch_tuned_nw<2, true>(st, T, cap, smem) : launch_tuned_nw<2, false>(st, T, cap, smem);
-        case 8: return ex ? launch_tuned_nw<8, true>(st, T, cap, smem) : launch_tuned_nw<8, false>(st, T, cap, smem);
-        default: return ex ? launch_tuned_nw<4, true>(st, T, cap, smem) : launch_tuned_nw<4, false>(st, T, cap, smem);
+        case 1: return launch_tuned_w<1>(st, T, cap, smem);
+        case 2: return launch_tuned_w<2>(st, T, cap, smem);
+        case 8: return launch_tuned_w<8>(st, T, cap, smem);
+        default: return launch_tuned_w<4>(st, T, cap, smem);
     }
 }
 
@@ -238,7 +247,7 @@ int launch_kernels(struct engine* e, NbState* st) {
     CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * st->ncells, st->stream));
     const int cap = (st->maxcount + 3) & ~3;
     if (cap == 0) return 0;
-    sort_cells<<<st->ncells, 128, sizeof(unsigned) * cap, st->stream>>>(
+    sort_cells<<<st->ncells, 128, sort_smem_bytes(), st->stream>>>(
         st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->dscale, st->bias, st->d_acc);
     CU(cudaGetLastError());
 
@@ -404,6 +413,7 @@ extern "C" int engine_cuda_load(struct engine* e) {
         potn.push_back(p->n);
     }
     st->npots = (int)uniq.size();
+    st->one_pot = (uniq.size() == 1) && std::all_of(potidx.begin(), potidx.end(), [](int v) { return v == 0; });
     st->ncoef = (int)coef.size();
     st->max_type = mt;
     if (coef.empty()) coef.push_back(0.f);
