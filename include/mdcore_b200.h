@@ -350,6 +350,22 @@ int engine_cuda_setstream(struct engine *e, void *stream);
 int engine_cuda_kernel_times(struct engine *e, float *total_ms, float *sweep_ms);
 /* Measured FP32 FMA throughput of a device in TFLOP/s (a register-only FMA loop). */
 int engine_cuda_fp32_peak(int device, float *tflops);
+/* Allocation-free force evaluation.  No counterpart in the reference.  For callers that
+ * cannot allocate device memory when they need forces (a fixed, pre-reserved device
+ * budget; code between set-up and a stream capture): sort + persistent sweep on
+ * caller-provided device buffers, with the only scratch (sort keys, queue head) in a
+ * static device array of at most 65,536 particle slots, shared by all calls; calls that
+ * overlap on the GPU race on it.  The first call on a device looks up that array's
+ * address and should come before any stream capture.  Inputs use the device layout of
+ * engine_cuda_load_parts (cell-major slots, cell starts multiples of 4): xq = float4
+ * {x, y, z cell-local, type bits}, pid, cstart[ncells+1], ccount[ncells]; maxcount = the
+ * largest cell count.  Outputs (zeroed by the call): force[3*nslots] int64 fixed point
+ * 2^24/(kJ/mol/nm), cell_epot[ncells] int64 2^32/(kJ/mol), acc[8] {unused, virial*2^32
+ * (negated), pairs, excluded, candidates, status}.  stream may be NULL (engine stream).
+ * Tables, tasks and exclusions come from engine_cuda_load. */
+int engine_nonbond_cuda_noalloc(struct engine *e, const void *xq, const int *pid, const int *cstart,
+                                const int *ccount, int nslots, int maxcount, unsigned long long *force,
+                                unsigned long long *cell_epot, unsigned long long *acc, void *stream);
 /* Sweep kernel launch parameters: warps per block (0 = default) and plain = 1 for the
  * plain form (one block per task, IEEE sqrt/div) instead of the persistent queue. */
 int engine_cuda_settune(struct engine *e, int warps, int plain);

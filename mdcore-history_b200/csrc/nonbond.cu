@@ -715,3 +715,117 @@ extern "C" int engine_cuda_ntasks(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     return state(e)->ntasks;
 }
+
+// ---------------------------------------------------------------- allocation-free variant
+//
+// Some callers cannot allocate device memory at the time they need forces: a host
+// program that hands this engine a fixed device-memory budget (every byte pre-reserved by
+// its own allocator), a caller inside a region where a cudaMalloc would synchronise the
+// device or is forbidden (real-time loops, code running between the engine's set-up and a
+// stream capture), or a plugin that must not grow the process's footprint.  For them,
+// engine_nonbond_cuda_noalloc runs the same sort + persistent sweep on caller-provided
+// device buffers and keeps its only scratch -- the sort key lists and the task-queue head
+// -- in the file-scope array below, sized for at most kNoAllocMaxSlots particle slots.
+// Every GPU that loads this library holds the array until the process exits.
+//
+// The array's name is a host-side stand-in, not a device address; the first call on each
+// device (with that device current) looks the address up with cudaGetSymbolAddress.  That
+// first call should therefore come before any stream capture.  All calls share the one
+// array and it keeps the last call's contents: the queue head is cleared on every call,
+// and calls that overlap on the GPU (other streams, other host threads) race on it.
+
+namespace {
+constexpr int kNoAllocMaxSlots = 65536;
+constexpr size_t kNoAllocKeyBytes = (size_t)13 * kNoAllocMaxSlots * sizeof(unsigned);
+static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocKeyBytes + 256];
+
+constexpr int kMaxDevices = 64;
+unsigned char* noalloc_addr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, const int* pid, const int* cstart,
+                                           const int* ccount, int nslots, int maxcount,
+                                           unsigned long long* force, unsigned long long* cell_epot,
+                                           unsigned long long* acc, void* stream) {
+    if (e == nullptr || e->cuda == nullptr || xq == nullptr || pid == nullptr || cstart == nullptr ||
+        ccount == nullptr || force == nullptr || cell_epot == nullptr || acc == nullptr) {
+        errs_register(engine_err_null, "engine_nonbond_cuda_noalloc: NULL argument.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_null;
+    }
+    NbState* st = state(e);
+    if (nslots < 0 || nslots > kNoAllocMaxSlots) {
+        errs_register(engine_err_range, "engine_nonbond_cuda_noalloc: more particle slots than its 65536-slot scratch.",
+                      __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_range;
+    }
+    if (maxcount < 0 || maxcount > kMaxPartsPerCell) {
+        errs_register(engine_err_maxparts, "engine_nonbond_cuda_noalloc: cell larger than 1024 particles.",
+                      __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    CU(cudaSetDevice(st->device));
+    if (st->device < 0 || st->device >= kMaxDevices) return engine_err_range;
+    if (noalloc_addr[st->device] == nullptr) {
+        void* p = nullptr;
+        CU(cudaGetSymbolAddress(&p, noalloc_scratch));
+        noalloc_addr[st->device] = static_cast<unsigned char*>(p);
+    }
+    unsigned* keys = reinterpret_cast<unsigned*>(noalloc_addr[st->device]);
+    int* counter = reinterpret_cast<int*>(noalloc_addr[st->device] + kNoAllocKeyBytes);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : st->stream;
+
+    CU(cudaMemsetAsync(force, 0, sizeof(unsigned long long) * 3 * (size_t)nslots, s));
+    CU(cudaMemsetAsync(cell_epot, 0, sizeof(unsigned long long) * st->ncells, s));
+    CU(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * kAccCount, s));
+    CU(cudaMemsetAsync(counter, 0, sizeof(int), s));
+    const int cap4 = (maxcount + 3) & ~3;
+    if (cap4 == 0) return 0;
+    sort_cells<<<st->ncells, 128, sort_smem_bytes(), s>>>(static_cast<const float4*>(xq), cstart, ccount,
+                                                           st->d_cmask, keys, st->dscale, st->bias, acc);
+    CU(cudaGetLastError());
+
+    TunedParams T;
+    Params& P = T.p;
+    P.xq = static_cast<const float4*>(xq);
+    P.pid = pid;
+    P.keys = keys;
+    P.cstart = cstart;
+    P.ccount = ccount;
+    P.force = force;
+    P.acc = acc;
+    P.cell_epot = cell_epot;
+    P.tasks = st->d_tasks;
+    P.tshift = st->d_tshift;
+    P.ntasks = st->ntasks;
+    P.coef = st->d_coef;
+    P.potinfo = st->d_potinfo;
+    P.potn = st->d_potn;
+    P.potidx = st->d_potidx;
+    P.max_type = st->max_type;
+    P.npots = st->npots;
+    P.ncoef = st->ncoef;
+    P.emask = st->d_emask;
+    P.exoff = st->d_exoff;
+    P.exlist = st->d_exlist;
+    const float cutf = (float)e->s.cutoff;
+    P.cutoff2 = cutf * cutf;
+    P.cutoff2s = (float)e->s.cutoff2;
+    P.dmaxdist = st->dmaxdist;
+    P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
+    T.order = st->d_order;
+    T.counter = counter;
+    T.task_clock = nullptr;
+    T.task_sm = nullptr;
+    const int cap = cap4 + 8;
+    const size_t smem = warps_smem_bytes(cap, 4, st->ncoef, st->npots, st->max_type);
+    if (smem > 220 * 1024) {
+        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    cudaStream_t saved = st->stream;
+    st->stream = s;
+    const int rc = launch_tuned_w<4>(st, T, cap, smem);
+    st->stream = saved;
+    return rc;
+}
