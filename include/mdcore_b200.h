@@ -257,6 +257,9 @@ struct nb_stats {
     double virial;          /* FP64 sum over pairs of r_ij . F_ij */
     int status;             /* device status word of the last launch (0 = ok) */
     float ms_kernels;       /* device time of the last force evaluation (CUDA events) */
+    float ms_pack;          /* host: packing the cells into the staging buffers */
+    float ms_device;        /* host wall time from the first copy to the last copy's completion */
+    float ms_unpack;        /* host: adding the forces into the cells */
 };
 
 struct engine {

@@ -22,23 +22,34 @@ namespace nb {
 __constant__ float c_axes[13][3];
 
 // ---------------------------------------------------------------- sort
-// Keys of one sort direction are ranked by a counting sort on the top 8 bits of the 16-bit
-// distance (256 buckets in shared memory) followed by an exact rank inside the bucket:
+// One CTA per cell, one warp per sort direction (directions w, w+4, ... for warp w).  Keys
+// of a direction are ranked by a counting sort on the top bits of the 16-bit distance
+// (64 buckets in the warp's shared memory) and an exact rank inside the bucket:
 // position = (keys in farther buckets) + (keys of the same bucket with a larger distance,
-// or an equal distance and a smaller storage index).  The result is the stable
-// descending order, independent of the order in which threads reach the atomics.
-constexpr int kSortBuckets = 256;
+// or an equal distance and a smaller storage index).  The result is the stable descending
+// order, independent of the order in which lanes reach the atomics.
+constexpr int kSortBuckets = 64;
+constexpr int kSortWarps = 4;
 
-__global__ void __launch_bounds__(128) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
-                                                  const int* __restrict__ ccount, const unsigned* __restrict__ cmask,
-                                                  unsigned* __restrict__ keys, float dscale, float bias,
-                                                  unsigned long long* acc) {
-    extern __shared__ unsigned sort_smem[];
-    unsigned* skey = sort_smem;                          // n keys
-    unsigned short* members = reinterpret_cast<unsigned short*>(sort_smem + kMaxPartsPerCell);  // bucket-major
-    int* bcount = reinterpret_cast<int*>(sort_smem + kMaxPartsPerCell + kMaxPartsPerCell / 2);
+__host__ __device__ inline size_t sort_warp_bytes() {
+    return (size_t)kMaxPartsPerCell * 4 + (size_t)kMaxPartsPerCell * 2 + (size_t)3 * kSortBuckets * 4;
+}
+__host__ inline size_t sort_smem_bytes() { return kSortWarps * sort_warp_bytes(); }
+
+__global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+                                                              const int* __restrict__ ccount,
+                                                              const unsigned* __restrict__ cmask,
+                                                              unsigned* __restrict__ keys, float dscale, float bias,
+                                                              unsigned long long* acc) {
+    extern __shared__ __align__(16) unsigned char sort_smem[];
+    constexpr unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wp = sort_smem + (size_t)warp * sort_warp_bytes();
+    unsigned* skey = reinterpret_cast<unsigned*>(wp);
+    unsigned short* members = reinterpret_cast<unsigned short*>(wp + (size_t)kMaxPartsPerCell * 4);
+    int* bcount = reinterpret_cast<int*>(wp + (size_t)kMaxPartsPerCell * 6);
     int* bstart = bcount + kSortBuckets;
-    int* bfill = bstart + kSortBuckets + 1;
+    int* bfill = bstart + kSortBuckets;
     const int c = blockIdx.x;
     const int n = ccount[c];
     if (n <= 0) return;
@@ -49,12 +60,12 @@ __global__ void __launch_bounds__(128) sort_cells(const float4* __restrict__ xq,
     const int start = cstart[c];
     const int pad = (n + 3) & ~3;
     const unsigned mask = cmask[c];
-    for (int sid = 0; sid < 13; ++sid) {
+    for (int sid = warp; sid < 13; sid += kSortWarps) {
         if (!((mask >> sid) & 1u)) continue;
         const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
-        for (int b = threadIdx.x; b < kSortBuckets; b += blockDim.x) { bcount[b] = 0; bfill[b] = 0; }
-        __syncthreads();
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        for (int b = lane; b < kSortBuckets; b += 32) { bcount[b] = 0; bfill[b] = 0; }
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
             const float4 x = xq[start + k];
             // dscale * (bias + x.n), evaluated left to right without contraction.
             float d = __fadd_rn(bias, __fmul_rn(x.x, nx));
@@ -63,36 +74,33 @@ __global__ void __launch_bounds__(128) sort_cells(const float4* __restrict__ xq,
             d = __fmul_rn(dscale, d);
             const unsigned key = ((unsigned)k << 16) | __float2uint_rz(d);
             skey[k] = key;
-            atomicAdd(&bcount[min((int)((key & 0xffffu) >> 7), kSortBuckets - 1)], 1);
+            atomicAdd(&bcount[min((int)((key & 0xffffu) >> 9), kSortBuckets - 1)], 1);
         }
-        __syncthreads();
-        if (threadIdx.x < 32) {          // bucket starts in descending bucket order (warp scan)
-            const int lane = threadIdx.x;
-            int run = 0;
-            for (int base = 0; base < kSortBuckets; base += 32) {
-                const int b = kSortBuckets - 1 - (base + lane);
-                const int v = bcount[b];
-                int incl = v;
+        __syncwarp();
+        {   // bucket starts in descending bucket order: lane l owns buckets 63-2l, 62-2l
+            const int bh = kSortBuckets - 1 - 2 * lane, bl = bh - 1;
+            const int ch = bcount[bh], cl = bcount[bl];
+            int incl = ch + cl;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                bstart[b] = run + incl - v;
-                run += __shfl_sync(0xffffffffu, incl, 31);
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
             }
+            const int excl = incl - ch - cl;
+            bstart[bh] = excl;
+            bstart[bl] = excl + ch;
         }
-        __syncthreads();
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const int b = min((int)((skey[k] & 0xffffu) >> 7), kSortBuckets - 1);
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+            const int b = min((int)((skey[k] & 0xffffu) >> 9), kSortBuckets - 1);
             members[bstart[b] + atomicAdd(&bfill[b], 1)] = (unsigned short)k;
         }
-        __syncthreads();
+        __syncwarp();
         unsigned* out = keys + 13 * (size_t)start + (size_t)sid * pad;
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        for (int k = lane; k < n; k += 32) {
             const unsigned mine = skey[k];
             const unsigned md = mine & 0xffffu;
-            const int b = min((int)(md >> 7), kSortBuckets - 1);
+            const int b = min((int)(md >> 9), kSortBuckets - 1);
             const int b0 = bstart[b], nb = bcount[b];
             int rank = b0;
             for (int m = 0; m < nb; ++m) {
@@ -102,12 +110,8 @@ __global__ void __launch_bounds__(128) sort_cells(const float4* __restrict__ xq,
             }
             out[rank] = mine;
         }
-        __syncthreads();
+        __syncwarp();
     }
-}
-
-__host__ inline size_t sort_smem_bytes() {
-    return (size_t)kMaxPartsPerCell * 4 + (size_t)kMaxPartsPerCell * 2 + (size_t)(3 * kSortBuckets + 1) * 4;
 }
 
 // ---------------------------------------------------------------- potential evaluation
@@ -122,7 +126,7 @@ __device__ __forceinline__ void eval_table(const float* __restrict__ coef, float
         status |= kStatusTableIndex;
         ind = nmax;
     }
-    const float4* c = reinterpret_cast<const float4*>(coef + __float_as_int(info.w) + 8 * ind);
+    const float4* c = reinterpret_cast<const float4*>(coef + (__float_as_int(info.w) & 0xfffff) + 8 * ind);
     const float4 c0 = c[0], c1 = c[1];
     const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
     float ee = fmaf(c0.z, x, c0.w);

@@ -15,8 +15,9 @@
 //    warp total for step m.  The order of additions is fixed, so task partials stay
 //    independent of scheduling;
 //  * the j record carries its sort distance and type in one 16-byte shared-memory word;
-//  * energy and virial are summed per pair in double (float partial sums of cancelling
-//    Coulomb terms would cost ~1e-6 of the total);
+//  * energy is summed per pair in double (float partial sums of cancelling Coulomb terms
+//    would cost ~1e-6 of the total); the virial per particle and task from the partial
+//    forces: sum over pairs of r_ij.F_ij = sum_i (x_i - shift).F_i + sum_j x_j.F_j;
 //  * optional per-task clock64 records (start, end, SM) for the learned scheduler.
 #pragma once
 #include "nb_kernels.cuh"
@@ -113,7 +114,7 @@ __device__ __forceinline__ void eval_table_fast(const float* __restrict__ coef, 
                                                 float rinv, float& e, float& f) {
     const float t = fmaf(r, fmaf(r, info.z, info.y), info.x);
     const int ind = min(__float2int_rz(fmaxf(0.0f, t)), nmax);
-    const float4* c = reinterpret_cast<const float4*>(coef + __float_as_int(info.w) + 8 * ind);
+    const float4* c = reinterpret_cast<const float4*>(coef + (__float_as_int(info.w) & 0xfffff) + 8 * ind);
     const float4 c0 = c[0], c1 = c[1];
     const float x = (r - c0.x) * c0.y;
     float ee = fmaf(c0.z, x, c0.w);
@@ -329,7 +330,6 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
-            float e_hi = 0.f, e_lo = 0.f;                   // Kahan-compensated energy
             for (int k0 = 0; k0 < kmax; k0 += 4) {
                 float vx[4], vy[4], vz[4];
                 bool any_acc = false;
@@ -368,13 +368,11 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
                             float r = r2 * rinv;
                             r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
                             float e, f;
-                            eval_table_fast(coef, potinfo[pot], potn[pot], r, rinv, e, f);
+                            const float4 info = potinfo[pot];
+                            eval_table_fast(coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
                             wx = f * dx; wy = f * dy; wz = f * dz;
                             fix -= wx; fiy -= wy; fiz -= wz;
-                            const float y = e - e_lo;
-                            const float tsum = e_hi + y;
-                            e_lo = (tsum - e_hi) - y;
-                            e_hi = tsum;
+                            e_task += (double)e;
                             ++npairs;
                         }
                     }
@@ -391,7 +389,6 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
                     }
                 }
             }
-            e_task += (double)e_hi - (double)e_lo;
             __syncwarp();
             if (valid) {
                 if (self) {

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <utility>
 #include <cmath>
+#include <ctime>
 #include <cuda_runtime.h>
 #include "mdcore_b200.h"
 #include "internal.h"
@@ -70,7 +71,8 @@ struct NbState {
     float4* h_xq = nullptr;
     int* h_pid = nullptr;
     int* h_cstart = nullptr;    // ncells+1 followed by ncells counts
-    unsigned long long* h_force = nullptr;
+    unsigned long long* h_force = nullptr;   // pinned; holds float forces (3 per slot)
+    float* d_forcef = nullptr;
     unsigned long long* h_cell_epot = nullptr;
     unsigned long long* h_acc = nullptr;
     bool resident_valid = false;
@@ -90,6 +92,15 @@ int cuda_fail(cudaError_t err, int line, const char* func) {
 
 NbState* state(struct engine* e) { return static_cast<NbState*>(e->cuda); }
 
+// Estimated cost of a task (the reference's METIS cell-pair weights).
+double task_weight(int sid, double ni, double nj) {
+    if (sid < 0) return ni * ni - ni;
+    const int idx = 26 - sid;                         // direction index, see sort_axis
+    const int nz = (idx / 9 != 1) + ((idx / 3) % 3 != 1) + (idx % 3 != 1);
+    const double w = nz == 1 ? 0.50004 : (nz == 2 ? 0.16176 : 0.036213);
+    return ni * nj * w;
+}
+
 float bits_as_float(int v) {
     float f;
     std::memcpy(&f, &v, sizeof(f));
@@ -107,6 +118,7 @@ int alloc_particles(NbState* st, int ncap) {
     if (ncap <= st->ncap) return 0;
     ncap = ncap + ncap / 8 + 64;
     cudaFree(st->d_xq); cudaFree(st->d_pid); cudaFree(st->d_keys); cudaFree(st->d_force);
+    st->d_xq = nullptr; st->d_pid = nullptr; st->d_keys = nullptr; st->d_force = nullptr;
     cudaFreeHost(st->h_xq); cudaFreeHost(st->h_pid); cudaFreeHost(st->h_force);
     if (dev_alloc(&st->d_xq, ncap) || dev_alloc(&st->d_pid, ncap) || dev_alloc(&st->d_keys, 13 * (size_t)ncap) ||
         dev_alloc(&st->d_force, 3 * (size_t)ncap))
@@ -114,10 +126,24 @@ int alloc_particles(NbState* st, int ncap) {
     CU(cudaMallocHost(&st->h_xq, sizeof(float4) * ncap));
     CU(cudaMallocHost(&st->h_pid, sizeof(int) * ncap));
     CU(cudaMallocHost(&st->h_force, sizeof(unsigned long long) * 3 * ncap));
+    cudaFree(st->d_forcef);
+    if (dev_alloc(&st->d_forcef, 3 * (size_t)ncap)) return engine_err_cuda;
     CU(cudaMemset(st->d_xq, 0, sizeof(float4) * ncap));
     CU(cudaMemset(st->d_pid, 0, sizeof(int) * ncap));
     st->ncap = ncap;
     return 0;
+}
+
+// Fixed-point forces (int64, 2^24 units) to float, for the copy back to the host.
+__global__ void fixed_to_float(const unsigned long long* __restrict__ f, float* __restrict__ out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)((double)(long long)f[i] * (1.0 / (double)kForceScale));
+}
+
+double now_ms() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
 // Packs the cells into the pinned staging buffers; returns the number of slots used.
@@ -138,9 +164,13 @@ int pack_cells(struct engine* e, NbState* st) {
     int* ccount = st->h_cstart + s->nr_cells + 1;
     int slot = 0;
     for (int c = 0; c < s->nr_cells; c++) {
-        struct cell* cl = &s->cells[c];
         cstart[c] = slot;
-        ccount[c] = cl->count;
+        ccount[c] = s->cells[c].count;
+        slot += (s->cells[c].count + 3) & ~3;
+    }
+    for (int c = 0; c < s->nr_cells; c++) {
+        struct cell* cl = &s->cells[c];
+        const int slot = cstart[c];
         for (int k = 0; k < cl->count; k++) {
             const struct part* p = &cl->parts[k];
             float4 v;
@@ -154,7 +184,6 @@ int pack_cells(struct engine* e, NbState* st) {
             st->h_xq[slot + k] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
             st->h_pid[slot + k] = 0;
         }
-        slot += pad;
     }
     cstart[s->nr_cells] = slot;
     st->maxcount = maxc;
@@ -247,7 +276,7 @@ int launch_kernels(struct engine* e, NbState* st) {
     CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * st->ncells, st->stream));
     const int cap = (st->maxcount + 3) & ~3;
     if (cap == 0) return 0;
-    sort_cells<<<st->ncells, 128, sort_smem_bytes(), st->stream>>>(
+    sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
         st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->dscale, st->bias, st->d_acc);
     CU(cudaGetLastError());
 
@@ -326,7 +355,7 @@ extern "C" int nb_device_free(struct engine* e) {
     void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
                    st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
-                   st->d_counter, st->d_task_clock, st->d_task_sm};
+                   st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef};
     for (void* p : dev) cudaFree(p);
     void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
     for (void* p : host) cudaFreeHost(p);
@@ -409,8 +438,13 @@ extern "C" int engine_cuda_load(struct engine* e) {
     for (struct potential* p : uniq) {
         int off = (int)coef.size();
         coef.insert(coef.end(), p->c, p->c + (size_t)(p->n + 1) * potential_chunk);
-        potinfo.push_back(make_float4(p->alpha[0], p->alpha[1], p->alpha[2], bits_as_float(off)));
+        // w: offset of the table's chunk 0 (low 20 bits) and its last chunk index n (high 12)
+        potinfo.push_back(make_float4(p->alpha[0], p->alpha[1], p->alpha[2], bits_as_float(off | (p->n << 20))));
         potn.push_back(p->n);
+    }
+    if (coef.size() >= (1u << 20)) {
+        errs_register(engine_err_potential, "Potential tables exceed 2^20 floats.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_potential;
     }
     st->npots = (int)uniq.size();
     st->one_pot = (uniq.size() == 1) && std::all_of(potidx.begin(), potidx.end(), [](int v) { return v == 0; });
@@ -446,15 +480,16 @@ extern "C" int engine_cuda_load(struct engine* e) {
     CU(cudaMemcpy(st->d_tasks, tasks.data(), tasks.size() * sizeof(TaskRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->d_tshift, tshift.data(), tshift.size() * sizeof(float4), cudaMemcpyHostToDevice));
 
-    // Task queue: initial order by decreasing particle-count product (self: n(n-1)/2), the
-    // load-balancing weight of the reference's task ranking (src/engine.c:574-699).
+    // Task queue: initial order by decreasing estimated cost, the reference's cell-pair
+    // weight (src/engine.c:574-576, 643-699): count_i*count_j times 0.50004 (face),
+    // 0.16176 (edge) or 0.036213 (corner) neighbours, n^2 - n for a cell with itself.
     CU(cudaDeviceGetAttribute(&st->sm_count, cudaDevAttrMultiProcessorCount, st->device));
     {
         std::vector<std::pair<double, int>> w(st->ntasks);
         for (int t = 0; t < st->ntasks; t++) {
             const TaskRec& r = tasks[t];
             double ni = s->cells[r.ci].count, nj = s->cells[r.cj].count;
-            w[t] = {r.sid < 0 ? 0.5 * ni * (ni - 1) : ni * nj, t};
+            w[t] = {task_weight(r.sid, ni, nj), t};
         }
         std::stable_sort(w.begin(), w.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
             return a.first > b.first;
@@ -520,8 +555,12 @@ extern "C" int engine_cuda_load_parts(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     NbState* st = state(e);
     CU(cudaSetDevice(st->device));
+    const double t0 = now_ms();
     int slots = pack_cells(e, st);
     if (slots < 0) return slots;
+    const double t1 = now_ms();
+    e->stats.ms_pack = (float)(t1 - t0);
+    e->stats.ms_device = 0.f;
     CU(cudaMemcpyAsync(st->d_xq, st->h_xq, sizeof(float4) * slots, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->d_pid, st->h_pid, sizeof(int) * slots, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->d_cstart, st->h_cstart, sizeof(int) * (st->ncells + 1), cudaMemcpyHostToDevice,
@@ -538,23 +577,33 @@ extern "C" int engine_cuda_unload_parts(struct engine* e) {
     NbState* st = state(e);
     struct space* s = &e->s;
     const int slots = st->h_cstart[s->nr_cells];
-    CU(cudaMemcpyAsync(st->h_force, st->d_force, sizeof(unsigned long long) * 3 * (size_t)slots,
-                       cudaMemcpyDeviceToHost, st->stream));
+    const double t0 = now_ms();
+    if (slots > 0) {
+        fixed_to_float<<<(3 * slots + 255) / 256, 256, 0, st->stream>>>(st->d_force, st->d_forcef, 3 * slots);
+        CU(cudaGetLastError());
+    }
+    float* hf = reinterpret_cast<float*>(st->h_force);
+    CU(cudaMemcpyAsync(hf, st->d_forcef, sizeof(float) * 3 * (size_t)slots, cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
     CU(cudaStreamSynchronize(st->stream));
+    const double t1 = now_ms();
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, st->ev0, st->ev1) == cudaSuccess) e->stats.ms_kernels = ms;
     int rc = finish_stats(e, st);
-    const double inv = 1.0 / (double)kForceScale;
     for (int c = 0; c < s->nr_cells; c++) {
         struct cell* cl = &s->cells[c];
-        const unsigned long long* f = st->h_force + 3 * (size_t)st->h_cstart[c];
-        for (int k = 0; k < cl->count; k++)
-            for (int j = 0; j < 3; j++) cl->parts[k].f[j] += (float)((double)(long long)f[3 * k + j] * inv);
+        const float* f = hf + 3 * (size_t)st->h_cstart[c];
+        for (int k = 0; k < cl->count; k++) {
+            cl->parts[k].f[0] += f[3 * k];
+            cl->parts[k].f[1] += f[3 * k + 1];
+            cl->parts[k].f[2] += f[3 * k + 2];
+        }
     }
+    e->stats.ms_device += (float)(t1 - t0);
+    e->stats.ms_unpack = (float)(now_ms() - t1);
     return rc;
 }
 
@@ -780,7 +829,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     CU(cudaMemsetAsync(counter, 0, sizeof(int), s));
     const int cap4 = (maxcount + 3) & ~3;
     if (cap4 == 0) return 0;
-    sort_cells<<<st->ncells, 128, sort_smem_bytes(), s>>>(static_cast<const float4*>(xq), cstart, ccount,
+    sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), s>>>(static_cast<const float4*>(xq), cstart, ccount,
                                                            st->d_cmask, keys, st->dscale, st->bias, acc);
     CU(cudaGetLastError());
 

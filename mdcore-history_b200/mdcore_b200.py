@@ -36,7 +36,8 @@ class Potential(C.Structure):
 class NbStats(C.Structure):
     _fields_ = [("pairs", C.c_int64), ("excluded", C.c_int64), ("candidates", C.c_int64),
                 ("epot", C.c_double), ("virial", C.c_double), ("status", C.c_int),
-                ("ms_kernels", C.c_float)]
+                ("ms_kernels", C.c_float), ("ms_pack", C.c_float), ("ms_device", C.c_float),
+                ("ms_unpack", C.c_float)]
 
 
 _lib: Optional[C.CDLL] = None
