@@ -268,9 +268,11 @@ def ours(args, rank, world, local_rank):
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "sweep_traffic.json")
-        if os.path.exists(prof):
-            traffic = json.load(open(prof)).get("bytes_per_launch")
+        prof = os.path.join(ROOT, "profiles", "sweep_tuned_water98k_traffic.txt")
+        if os.path.exists(prof):       # dram read + write bytes of one sweep launch, from ncu
+            for ln in open(prof):
+                if ln.startswith("dram_bytes_per_launch"):
+                    traffic = int(ln.split()[1])
         line = {
             "metric": METRIC, "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
