@@ -35,17 +35,26 @@ METRIC = "pair interactions/s + ns/day, 1 B200: tuned vs plain at ≤1e-5 rel fo
 UNIT = "pair interactions/s"
 FLOPS_PER_PAIR = 45          # per accepted pair, FMA = 2 (roofline)
 DT_FS = 2.0
-WORKLOAD = "rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, " \
-           "9x9x9 cells, cutoff 1.0 nm, 98,304 exclusions, seeded"
 
 
 def ns_per_day(ms_per_step):
     return DT_FS * 1e-6 * 86400.0 / (ms_per_step * 1e-3)
 
 
+WORKLOADS = {
+    "water": ("rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, 9x9x9 cells, "
+              "cutoff 1.0 nm, 98,304 exclusions, seeded", lambda W: W.water_spce(32)),
+    "slab": ("LJ liquid slab in vapour, 1,048,576 atoms (80/20 two types) in a 40x40x160 nm box, 40x40x160 cells, "
+             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab()),
+    "argon": ("LJ argon, 32,000 atoms on a jittered FCC lattice in an 11.5074 nm box, 11^3 cells, cutoff 1.0 nm, "
+              "seeded", lambda W: W.argon_fcc(20)),
+}
+SELECTED = "water"
+
+
 def build_system():
     import workloads as W
-    return W.water_spce(32)
+    return WORKLOADS[SELECTED][1](W)
 
 
 class ClockSampler:
@@ -131,7 +140,7 @@ def reference_arm(args, rank):
         "steps": r["steps"], "warmup": max(1, min(args.warmup, 3)), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "ns_per_day": ns_per_day(ms),
-        "config": {"workload": WORKLOAD, "pairs_per_step": pairs, "parallelism": "pthreads runners"},
+        "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "parallelism": "pthreads runners"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{r['steps']} engine_step calls (dt=0) of the full system, "
                                    f"{threads} runners"},
@@ -278,8 +287,8 @@ def ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "ns_per_day": ns_per_day(ms),
-            "config": {"workload": WORKLOAD, "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
-                       "tasks": 10206, "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
+                       "tasks": e.ntasks(), "parallelism": f"replicas x{world}",
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
             "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -319,7 +328,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
+    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
+                    help="water (default: the headline configuration) or another seeded system")
     args = ap.parse_args()
+    global SELECTED
+    SELECTED = args.workload
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))

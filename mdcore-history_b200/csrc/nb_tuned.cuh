@@ -33,6 +33,7 @@ namespace nb {
 struct TunedParams {
     Params p;
     const int* order;            // queue: task indices in scheduling order
+    const int* qcount;           // number of queue entries (device), or nullptr: p.ntasks
     int* counter;                // queue head (zeroed before each launch)
     long long* task_clock;       // 2 * ntasks: start, end (clock64) or nullptr
     int* task_sm;                // SM id per task or nullptr
@@ -176,6 +177,100 @@ __device__ __forceinline__ float reduce_scatter8(const float (&v)[8], int lane) 
     return d;
 }
 
+// ---------------------------------------------------------------- queue compaction
+// Each step the queue is rebuilt from the scheduling order, keeping (in order) only tasks
+// whose cells are both non-empty: a block-wise flag count, a one-block scan of the block
+// totals, and a scatter.  Deterministic and stable.
+constexpr int kQueueBlock = 1024;
+
+__device__ __forceinline__ bool task_live(const TaskRec& r, const int* __restrict__ ccount) {
+    const int ni = ccount[r.ci], nj = ccount[r.cj];
+    return r.sid < 0 ? ni >= 2 : (ni > 0 && nj > 0);
+}
+
+// Exclusive scan of one flag per thread over the block; returns the block total.
+__device__ __forceinline__ int block_scan_flag(int flag, int& excl, int* warp_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned ball = __ballot_sync(0xffffffffu, flag);
+    const int in_warp = __popc(ball & ((1u << lane) - 1u));
+    if (lane == 0) warp_tot[warp] = __popc(ball);
+    __syncthreads();
+    if (warp == 0) {
+        const int v = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        warp_tot[lane] = incl - v;          // exclusive prefix of warps
+        if (lane == 31) warp_tot[32] = incl;
+    }
+    __syncthreads();
+    excl = warp_tot[warp] + in_warp;
+    const int total = warp_tot[32];
+    __syncthreads();
+    return total;
+}
+
+__global__ void __launch_bounds__(kQueueBlock) queue_count(const int* __restrict__ order, const TaskRec* __restrict__ tasks,
+                                                           const int* __restrict__ ccount, int ntasks, int* __restrict__ bsum) {
+    __shared__ int warp_tot[33];
+    const int q = blockIdx.x * kQueueBlock + threadIdx.x;
+    const int flag = q < ntasks ? task_live(tasks[order[q]], ccount) : 0;
+    int excl;
+    const int total = block_scan_flag(flag, excl, warp_tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kQueueBlock) queue_offsets(int* __restrict__ bsum, int nblocks, int* __restrict__ qcount) {
+    __shared__ int warp_tot[33];
+    int run = 0;
+    for (int base = 0; base < nblocks; base += kQueueBlock) {
+        const int b = base + threadIdx.x;
+        const int v = b < nblocks ? bsum[b] : 0;
+        // inclusive-of-others exclusive scan via the flag scan applied to counts: do it in
+        // two steps: warp scan of values, then warps
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int wv = warp_tot[lane];
+            int wi = wv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            warp_tot[lane] = wi - wv;
+            if (lane == 31) warp_tot[32] = wi;
+        }
+        __syncthreads();
+        if (b < nblocks) bsum[b] = run + warp_tot[warp] + incl - v;
+        run += warp_tot[32];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *qcount = run;
+}
+
+__global__ void __launch_bounds__(kQueueBlock) queue_scatter(const int* __restrict__ order, const TaskRec* __restrict__ tasks,
+                                                             const int* __restrict__ ccount, int ntasks,
+                                                             const int* __restrict__ bsum, int* __restrict__ queue) {
+    __shared__ int warp_tot[33];
+    const int q = blockIdx.x * kQueueBlock + threadIdx.x;
+    const int t = q < ntasks ? order[q] : 0;
+    const int flag = q < ntasks ? task_live(tasks[t], ccount) : 0;
+    int excl;
+    block_scan_flag(flag, excl, warp_tot);
+    if (flag) queue[bsum[blockIdx.x] + excl] = t;
+}
+
 // Shared memory of one worker warp (cap = largest cell rounded up to 4, plus 8 spare rows
 // that the 4-step sweep windows may read past the end of the j list).
 __host__ __device__ inline size_t warp_slice_bytes(int cap) { return 16 + (size_t)cap * 56; }
@@ -230,12 +325,22 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
 
     unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
     unsigned phase = 0;                   // completed phases of this warp's mbarrier
+    const int nq = T.qcount ? *T.qcount : P.ntasks;
+    // Queue entries are taken `batch` at a time: one when there are few tasks per worker
+    // (load balance), up to 16 on systems with millions of small tasks (the queue head is
+    // a single atomic counter).
+    const int workers = gridDim.x * NW;
+    const int batch = max(1, min(16, nq / (8 * workers)));
+    int q = 0, qend = 0;
     for (;;) {
-        int q = 0;
-        if (lane == 0) q = atomicAdd(T.counter, 1);
-        q = __shfl_sync(FULL, q, 0);
-        if (q >= P.ntasks) break;
-        const int t = T.order[q];
+        if (q >= qend) {
+            int q0 = 0;
+            if (lane == 0) q0 = atomicAdd(T.counter, batch);
+            q = __shfl_sync(FULL, q0, 0);
+            qend = min(q + batch, nq);
+            if (q >= nq) break;
+        }
+        const int t = T.order[q++];
         const TaskRec tr = P.tasks[t];
         const bool self = tr.sid < 0;
         const int ni = P.ccount[tr.ci], nj = P.ccount[tr.cj];

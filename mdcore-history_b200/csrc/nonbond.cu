@@ -42,7 +42,11 @@ struct NbState {
     bool has_excl = false;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
-    int* d_order = nullptr;        // task queue order
+    int* d_order = nullptr;        // task queue order (scheduling order of all tasks)
+    int* d_queue = nullptr;        // compacted queue of the current step
+    int* d_qcount = nullptr;
+    int* d_bsum = nullptr;
+    bool compact = false;          // rebuild the queue each step without empty tasks
     int* d_counter = nullptr;      // queue head
     long long* d_task_clock = nullptr;
     int* d_task_sm = nullptr;
@@ -245,6 +249,17 @@ int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
     TunedParams T;
     T.p = P;
     T.order = st->d_order;
+    T.qcount = nullptr;
+    if (st->compact && st->ntasks > 0) {
+        const int nb = (st->ntasks + kQueueBlock - 1) / kQueueBlock;
+        queue_count<<<nb, kQueueBlock, 0, st->stream>>>(st->d_order, st->d_tasks, P.ccount, st->ntasks, st->d_bsum);
+        queue_offsets<<<1, kQueueBlock, 0, st->stream>>>(st->d_bsum, nb, st->d_qcount);
+        queue_scatter<<<nb, kQueueBlock, 0, st->stream>>>(st->d_order, st->d_tasks, P.ccount, st->ntasks, st->d_bsum,
+                                                          st->d_queue);
+        CU(cudaGetLastError());
+        T.order = st->d_queue;
+        T.qcount = st->d_qcount;
+    }
     T.counter = st->d_counter;
     T.task_clock = st->record_clock ? st->d_task_clock : nullptr;
     T.task_sm = st->record_clock ? st->d_task_sm : nullptr;
@@ -355,7 +370,8 @@ extern "C" int nb_device_free(struct engine* e) {
     void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
                    st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
-                   st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef};
+                   st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef, st->d_queue,
+                   st->d_qcount, st->d_bsum};
     for (void* p : dev) cudaFree(p);
     void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
     for (void* p : host) cudaFreeHost(p);
@@ -496,6 +512,12 @@ extern "C" int engine_cuda_load(struct engine* e) {
         });
         std::vector<int> order(st->ntasks > 0 ? st->ntasks : 1, 0);
         for (int t = 0; t < st->ntasks; t++) order[t] = w[t].second;
+        const int nb = (st->ntasks + kQueueBlock - 1) / kQueueBlock + 1;
+        if (dev_alloc(&st->d_queue, order.size()) || dev_alloc(&st->d_qcount, 1) || dev_alloc(&st->d_bsum, nb))
+            return engine_err_cuda;
+        int empty = 0;
+        for (int c = 0; c < s->nr_cells; c++) empty += s->cells[c].count == 0;
+        st->compact = empty > 0;
         if (dev_alloc(&st->d_order, order.size()) || dev_alloc(&st->d_counter, 1) ||
             dev_alloc(&st->d_task_clock, 2 * order.size()) || dev_alloc(&st->d_task_sm, order.size()))
             return engine_err_cuda;
@@ -862,6 +884,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     P.dmaxdist = st->dmaxdist;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
     T.order = st->d_order;
+    T.qcount = nullptr;
     T.counter = counter;
     T.task_clock = nullptr;
     T.task_sm = nullptr;

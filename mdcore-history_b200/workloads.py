@@ -157,6 +157,46 @@ def water_spce(nside: int = 32, seed: int = 0, density: float = 33.4, jitter: fl
         masses=[15.9994, 1.00794], charges=[qO, qH], pots=pots, x=x, type=typ, excl=excl, dt=0.002)
 
 
+def lb_mix(eps_i, sig_i, eps_j, sig_j):
+    """Lorentz-Berthelot: sigma arithmetic mean, epsilon geometric mean."""
+    return math.sqrt(eps_i * eps_j), 0.5 * (sig_i + sig_j)
+
+
+def lj_slab(nx: int = 110, nz: int = 77, n_total: int = 1 << 20, seed: int = 0, box=(40.0, 40.0, 160.0),
+            slab: float = 28.07, jitter: float = 0.02, frac_a: float = 0.8, tol: float = 1e-4,
+            cutoff: float = 1.0) -> System:
+    """Inhomogeneous LJ slab: a liquid slab of thickness `slab` at the box centre along z
+    (jittered simple-cubic lattice, nx*nx*nz sites, ~21 atoms/nm^3 for the defaults) and a
+    uniform vapour filling the rest of the box with the remaining n_total - nx*nx*nz atoms
+    (~0.55 atoms/nm^3).  Two types mixed 80/20 at random (sigma 0.3405/0.30 nm,
+    eps 0.996/0.80 kJ/mol, Lorentz-Berthelot cross term).  Defaults: 2^20 atoms in a
+    40 x 40 x 160 nm box, 40 x 40 x 160 cells."""
+    rng = np.random.default_rng(seed)
+    Lx, Ly, Lz = box
+    dx, dy, dz = Lx / nx, Ly / nx, slab / nz
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(nx), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    z0 = 0.5 * (Lz - slab)
+    liq = (g + 0.5) * np.array([dx, dy, dz]) + np.array([0.0, 0.0, z0])
+    liq = liq + rng.normal(0.0, jitter, size=liq.shape)
+    nv = n_total - len(liq)
+    vz = rng.uniform(0.0, Lz - slab, size=nv)
+    vz = np.where(vz < z0, vz, vz + slab)
+    vap = np.stack([rng.uniform(0.0, Lx, nv), rng.uniform(0.0, Ly, nv), vz], 1)
+    x = np.concatenate([liq, vap])
+    dim = np.array(box, dtype=np.float64)
+    x = _wrap(x, dim)
+    typ = (rng.uniform(size=n_total) >= frac_a).astype(np.int32)
+    eps, sig = (0.996, 0.80), (0.3405, 0.30)
+    pots = []
+    for i in range(2):
+        for j in range(i, 2):
+            e_ij, s_ij = lb_mix(eps[i], sig[i], eps[j], sig[j])
+            pots.append(PotSpec(KIND_LJ126, i, j, 0.25, cutoff, tol, (*lj_AB(e_ij, s_ij), 0.0, 0.0)))
+    return System(name=f"lj-slab-{n_total}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
+                  masses=[39.948, 39.948], charges=[0.0, 0.0], pots=pots, x=x, type=typ,
+                  excl=np.zeros((0, 2), np.int32), dt=0.005)
+
+
 def write_sysfile(sysm: System, path: str) -> None:
     """Serialise in the format of oracle/sysfile.h."""
     with open(path, "wb") as f:

@@ -151,8 +151,8 @@ def test_resident_path_matches_host_path():
     e.close()
 
 
-@pytest.mark.parametrize("make", [lambda: W.argon_fcc(20), lambda: W.water_spce(32)],
-                         ids=["argon-32000", "water-98304"])
+@pytest.mark.parametrize("make", [lambda: W.argon_fcc(20), lambda: W.water_spce(32), lambda: W.lj_slab()],
+                         ids=["argon-32000", "water-98304", "slab-1048576"])
 def test_full_size_vs_oracle(make):
     """The benchmark systems at full size: counts bit-exact, energies and forces to FP32."""
     sysm = make()
