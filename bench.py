@@ -321,6 +321,56 @@ def ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def sched_ab(args, local_rank):
+    """Makespan of the sweep with the count-product order, the learned order and a random
+    order (same workload, device-resident, CUDA events, L2 flushed before every step)."""
+    import numpy as np
+    import torch
+    import mdcore_b200 as M
+    torch.cuda.set_device(local_rank)
+    sysm = build_system()
+    e = M.Engine.from_system(sysm, device=local_rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    e.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        e.nonbond()
+    e.load_parts()
+    t0 = time.time()
+    e.sched_record(args.record)
+    X = e.sched_features()
+    y = e.sched_targets()
+    loss = e.sched_train(epochs=args.epochs, batch=512, lr=3e-3, seed=1)
+    train_s = time.time() - t0
+    pred = e.sched_predict()
+
+    def timed(order_name):
+        e.resident()
+        torch.cuda.synchronize()
+        sweeps = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e.resident()
+            sweeps.append(e.kernel_times()[1])
+        return float(np.median(sweeps))
+
+    res = {}
+    e.sched_apply(False)
+    res["count_product"] = timed("heuristic")
+    e.sched_apply(True)
+    res["learned"] = timed("mlp")
+    e.set_order(np.random.default_rng(0).permutation(e.ntasks()))
+    res["random"] = timed("random")
+    e.tune(0, plain=True)
+    res["plain_form"] = timed("plain")
+    nz = y > 0
+    print(json.dumps({"sched_ab": WORKLOADS[SELECTED][0], "sweep_ms_median": res, "tasks": e.ntasks(),
+                      "record_steps": args.record, "epochs": args.epochs, "train_s": round(train_s, 3),
+                      "train_mse": loss, "corr_pred_target": float(np.corrcoef(pred[nz], y[nz])[0, 1])}))
+    e.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,9 +380,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
                     help="water (default: the headline configuration) or another seeded system")
+    ap.add_argument("--sched-ab", action="store_true",
+                    help="train the task-cost model and compare sweep makespans of the queue orders")
+    ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")
+    ap.add_argument("--epochs", type=int, default=150, help="--sched-ab: training epochs")
     args = ap.parse_args()
     global SELECTED
     SELECTED = args.workload
+    if args.sched_ab:
+        sched_ab(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))

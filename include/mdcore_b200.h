@@ -369,6 +369,32 @@ int engine_cuda_fp32_peak(int device, float *tflops);
 int engine_nonbond_cuda_noalloc(struct engine *e, const void *xq, const int *pid, const int *cstart,
                                 const int *ccount, int nslots, int maxcount, unsigned long long *force,
                                 unsigned long long *cell_epot, unsigned long long *acc, void *stream);
+/* ---- learned task-cost scheduler (no counterpart in the reference) ----
+ * A small MLP (NB_MLP_IN -> 32 -> 32 -> 1) predicts each task's cost from the two cells'
+ * particle counts, the fraction of i particles within the sort-axis reach of cell j, the
+ * type mix and the neighbour class; it is trained on the GPU on clock64 task durations the
+ * sweep records, and orders the device queue longest-first.  Forces do not depend on the
+ * order (fixed-point accumulation). */
+#define NB_MLP_IN 10
+#define NB_MLP_HIDDEN 32
+#define NB_MLP_NPARAM (NB_MLP_HIDDEN * NB_MLP_IN + NB_MLP_HIDDEN + NB_MLP_HIDDEN * NB_MLP_HIDDEN + \
+                       NB_MLP_HIDDEN + NB_MLP_HIDDEN + 1)
+/* Device kernels on caller buffers (X: n x NB_MLP_IN floats; weights: NB_MLP_NPARAM bf16). */
+int nb_mlp_predict(const float *X, int n, const void *w_bf16, float *out, void *stream);
+int nb_mlp_grad(const float *X, const float *target, const int *idx, int n, const void *w_bf16,
+                float *grad, float *loss, void *stream);
+int nb_mlp_adam(float *w_master, void *w_bf16, const float *grad, float *m, float *v, float lr,
+                float beta1, float beta2, float eps, int step, void *stream);
+int nb_mlp_round(const float *w_master, void *w_bf16, void *stream);
+/* Engine-level use: record per-task durations over nsteps device-resident evaluations,
+ * compute features, train, and apply an order (use_mlp = 0 restores the count-product
+ * heuristic order). */
+int engine_sched_record(struct engine *e, int nsteps);
+int engine_sched_features(struct engine *e, float *features_out, int n);
+int engine_sched_targets(struct engine *e, float *targets_out, int n);
+int engine_sched_train(struct engine *e, int epochs, int batch, float lr, unsigned seed, float *loss_out);
+int engine_sched_predict(struct engine *e, float *pred_out, int n);
+int engine_sched_apply(struct engine *e, int use_mlp);
 /* Sweep kernel launch parameters: warps per block (0 = default) and plain = 1 for the
  * plain form (one block per task, IEEE sqrt/div) instead of the persistent queue. */
 int engine_cuda_settune(struct engine *e, int warps, int plain);

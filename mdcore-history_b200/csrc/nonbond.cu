@@ -80,7 +80,11 @@ struct NbState {
     unsigned long long* h_cell_epot = nullptr;
     unsigned long long* h_acc = nullptr;
     bool resident_valid = false;
+    void* sched = nullptr;             // learned-scheduler state (SchedState)
+    std::vector<int> heur_order;       // count-product order built at load
 };
+
+void sched_free(void* p);
 
 int cuda_fail(cudaError_t err, int line, const char* func) {
     errs_register(engine_err_cuda, cudaGetErrorString(err), line, func, __FILE__);
@@ -380,6 +384,7 @@ extern "C" int nb_device_free(struct engine* e) {
     if (st->evs0) cudaEventDestroy(st->evs0);
     if (st->evs1) cudaEventDestroy(st->evs1);
     if (st->own_stream) cudaStreamDestroy(st->own_stream);
+    sched_free(st->sched);
     delete st;
     e->cuda = nullptr;
     return 0;
@@ -512,6 +517,7 @@ extern "C" int engine_cuda_load(struct engine* e) {
         });
         std::vector<int> order(st->ntasks > 0 ? st->ntasks : 1, 0);
         for (int t = 0; t < st->ntasks; t++) order[t] = w[t].second;
+        st->heur_order.assign(order.begin(), order.begin() + st->ntasks);
         const int nb = (st->ntasks + kQueueBlock - 1) / kQueueBlock + 1;
         if (dev_alloc(&st->d_queue, order.size()) || dev_alloc(&st->d_qcount, 1) || dev_alloc(&st->d_bsum, nb))
             return engine_err_cuda;
@@ -900,4 +906,290 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const int rc = launch_tuned_w<4>(st, T, cap, smem);
     st->stream = saved;
     return rc;
+}
+
+// ---------------------------------------------------------------- learned scheduler
+namespace {
+
+// Per-cell count of type-0 particles (the type mix feature).
+__global__ void cell_type0(const float4* __restrict__ xq, const int* __restrict__ cstart,
+                           const int* __restrict__ ccount, int ncells, int* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int n0 = 0;
+    for (int k = 0; k < ccount[c]; k++) n0 += __float_as_int(xq[cstart[c] + k].w) == 0;
+    out[c] = n0;
+}
+
+// Features of every task (NB_MLP_IN floats): counts, reach fraction, pair volume, type mix,
+// neighbour class one-hot (face, edge, corner, self).
+__global__ void task_features(const TaskRec* __restrict__ tasks, int ntasks, const int* __restrict__ ccount,
+                              const int* __restrict__ cstart, const unsigned* __restrict__ keys,
+                              const int* __restrict__ ctype0, int dmaxdist, float inv_scale,
+                              float* __restrict__ X) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const TaskRec r = tasks[t];
+    const int ni = ccount[r.ci], nj = ccount[r.cj];
+    float reach = 1.f;
+    int cls = 3;
+    if (r.sid >= 0) {
+        const int idx = 26 - r.sid;
+        cls = (idx / 9 != 1) + ((idx / 3) % 3 != 1) + (idx % 3 != 1) - 1;
+        if (ni > 0 && nj > 0) {
+            const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
+            const unsigned* ki = keys + 13 * (size_t)cstart[r.ci] + (size_t)r.sid * padi;
+            const unsigned* kj = keys + 13 * (size_t)cstart[r.cj] + (size_t)r.sid * padj;
+            const int thr = (int)(kj[nj - 1] & 0xffffu) + r.dnshift - dmaxdist;   // i needs dist >= thr
+            int lo = 0, hi = ni;                                                   // descending list
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((int)(ki[mid] & 0xffffu) >= thr) lo = mid + 1; else hi = mid;
+            }
+            reach = (float)lo / (float)ni;
+        } else {
+            reach = 0.f;
+        }
+    }
+    float* x = X + (size_t)t * NB_MLP_IN;
+    x[0] = ni * inv_scale;
+    x[1] = nj * inv_scale;
+    x[2] = reach;
+    x[3] = (float)ni * (float)nj * reach * inv_scale * inv_scale;
+    x[4] = ni > 0 ? (float)ctype0[r.ci] / ni : 0.f;
+    x[5] = nj > 0 ? (float)ctype0[r.cj] / nj : 0.f;
+    for (int k = 0; k < 4; k++) x[6 + k] = (k == cls) ? 1.f : 0.f;
+}
+
+// Adds this launch's task durations (clock64 cycles) into the running sums.
+__global__ void accumulate_durations(const long long* __restrict__ clk, int ntasks, double* __restrict__ dur,
+                                     int* __restrict__ nrec) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const long long a = clk[2 * t], b = clk[2 * t + 1];
+    if (b > a && a > 0) {
+        dur[t] += (double)(b - a);
+        nrec[t] += 1;
+    }
+}
+
+struct SchedState {
+    float* d_feat = nullptr;
+    double* d_dur = nullptr;
+    int* d_nrec = nullptr;
+    int* d_ctype0 = nullptr;
+    float* d_target = nullptr;
+    float* d_pred = nullptr;
+    int* d_idx = nullptr;
+    float *d_wm = nullptr, *d_m = nullptr, *d_v = nullptr, *d_grad = nullptr, *d_loss = nullptr;
+    void* d_wb = nullptr;
+    int step = 0;
+    bool trained = false;
+    std::vector<int> heuristic;   // count-product order
+};
+
+SchedState* sched(struct engine* e, NbState* st);
+
+}  // namespace
+
+#include <random>
+
+extern "C" int nb_mlp_predict(const float* X, int n, const void* w_bf16, float* out, void* stream);
+extern "C" int nb_mlp_grad(const float* X, const float* target, const int* idx, int n, const void* w_bf16,
+                           float* grad, float* loss, void* stream);
+extern "C" int nb_mlp_adam(float* w_master, void* w_bf16, const float* grad, float* m, float* v, float lr,
+                           float beta1, float beta2, float eps, int step, void* stream);
+extern "C" int nb_mlp_round(const float* w_master, void* w_bf16, void* stream);
+
+namespace {
+
+void sched_free(void* p) {
+    SchedState* ss = static_cast<SchedState*>(p);
+    if (ss == nullptr) return;
+    void* bufs[] = {ss->d_feat, ss->d_dur, ss->d_nrec, ss->d_ctype0, ss->d_target, ss->d_pred, ss->d_idx,
+                    ss->d_wm, ss->d_m, ss->d_v, ss->d_grad, ss->d_loss, ss->d_wb};
+    for (void* b : bufs) cudaFree(b);
+    delete ss;
+}
+
+SchedState* sched(struct engine* e, NbState* st) {
+    (void)e;
+    if (st->sched) return static_cast<SchedState*>(st->sched);
+    SchedState* ss = new SchedState();
+    st->sched = ss;
+    const int n = st->ntasks > 0 ? st->ntasks : 1;
+    bool bad = dev_alloc(&ss->d_feat, (size_t)n * NB_MLP_IN) || dev_alloc(&ss->d_dur, n) ||
+               dev_alloc(&ss->d_nrec, n) || dev_alloc(&ss->d_ctype0, st->ncells) || dev_alloc(&ss->d_target, n) ||
+               dev_alloc(&ss->d_pred, n) || dev_alloc(&ss->d_idx, n) || dev_alloc(&ss->d_wm, NB_MLP_NPARAM) ||
+               dev_alloc(&ss->d_m, NB_MLP_NPARAM) || dev_alloc(&ss->d_v, NB_MLP_NPARAM) ||
+               dev_alloc(&ss->d_grad, NB_MLP_NPARAM) || dev_alloc(&ss->d_loss, 1);
+    if (!bad) bad = cudaMalloc(&ss->d_wb, sizeof(uint16_t) * NB_MLP_NPARAM) != cudaSuccess;
+    if (bad) return nullptr;
+    cudaMemset(ss->d_dur, 0, sizeof(double) * n);
+    cudaMemset(ss->d_nrec, 0, sizeof(int) * n);
+    return ss;
+}
+
+}  // namespace
+
+// Runs nsteps device-resident evaluations with per-task clock64 records and adds each
+// task's duration into a running sum (the training targets).
+extern "C" int engine_sched_record(struct engine* e, int nsteps) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    SchedState* ss = sched(e, st);
+    if (ss == nullptr) return engine_err_cuda;
+    if (!st->resident_valid) {
+        int rc = engine_cuda_load_parts(e);
+        if (rc < 0) return rc;
+    }
+    const int prev = st->record_clock;
+    st->record_clock = 1;
+    for (int k = 0; k < nsteps; k++) {
+        CU(cudaMemsetAsync(st->d_task_clock, 0, sizeof(long long) * 2 * st->ntasks, st->stream));
+        int rc = launch_kernels(e, st);
+        if (rc < 0) return rc;
+        accumulate_durations<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_task_clock, st->ntasks,
+                                                                             ss->d_dur, ss->d_nrec);
+        CU(cudaGetLastError());
+    }
+    st->record_clock = prev;
+    CU(cudaStreamSynchronize(st->stream));
+    return 0;
+}
+
+// Features of the current configuration (needs the sort keys of the last launch).
+extern "C" int engine_sched_features(struct engine* e, float* features_out, int n) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    SchedState* ss = sched(e, st);
+    if (ss == nullptr) return engine_err_cuda;
+    cell_type0<<<(st->ncells + 255) / 256, 256, 0, st->stream>>>(st->d_xq, st->d_cstart, st->d_ccount, st->ncells,
+                                                                 ss->d_ctype0);
+    task_features<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_tasks, st->ntasks, st->d_ccount,
+                                                                    st->d_cstart, st->d_keys, ss->d_ctype0,
+                                                                    st->dmaxdist, 1.0f / 32.0f, ss->d_feat);
+    CU(cudaGetLastError());
+    if (features_out != nullptr) {
+        if (n != st->ntasks) return engine_err_range;
+        CU(cudaMemcpyAsync(features_out, ss->d_feat, sizeof(float) * NB_MLP_IN * (size_t)n, cudaMemcpyDeviceToHost,
+                           st->stream));
+    }
+    CU(cudaStreamSynchronize(st->stream));
+    return 0;
+}
+
+// Mean recorded duration per task normalised by the mean over recorded tasks (0 for tasks
+// that never ran, e.g. with an empty cell); uploads them as training targets.
+extern "C" int engine_sched_targets(struct engine* e, float* targets_out, int n) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    SchedState* ss = sched(e, st);
+    if (ss == nullptr) return engine_err_cuda;
+    std::vector<double> dur(st->ntasks);
+    std::vector<int> nrec(st->ntasks);
+    CU(cudaMemcpy(dur.data(), ss->d_dur, sizeof(double) * st->ntasks, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(nrec.data(), ss->d_nrec, sizeof(int) * st->ntasks, cudaMemcpyDeviceToHost));
+    double sum = 0.0;
+    int cnt = 0;
+    for (int t = 0; t < st->ntasks; t++)
+        if (nrec[t] > 0) { sum += dur[t] / nrec[t]; cnt++; }
+    const double mean = cnt ? sum / cnt : 1.0;
+    std::vector<float> tg(st->ntasks);
+    for (int t = 0; t < st->ntasks; t++) tg[t] = nrec[t] > 0 ? (float)(dur[t] / nrec[t] / mean) : 0.f;
+    CU(cudaMemcpy(ss->d_target, tg.data(), sizeof(float) * st->ntasks, cudaMemcpyHostToDevice));
+    if (targets_out != nullptr) {
+        if (n != st->ntasks) return engine_err_range;
+        std::copy(tg.begin(), tg.end(), targets_out);
+    }
+    return 0;
+}
+
+// Adam on mini-batches of the recorded tasks (at most 2^18 samples per epoch), weights
+// initialised on the first call (He-normal, seeded).
+extern "C" int engine_sched_train(struct engine* e, int epochs, int batch, float lr, unsigned seed, float* loss_out) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    SchedState* ss = sched(e, st);
+    if (ss == nullptr) return engine_err_cuda;
+    std::mt19937 rng(seed);
+    if (!ss->trained && ss->step == 0) {
+        std::vector<float> w(NB_MLP_NPARAM, 0.f);
+        auto fill = [&](int off, int nout, int nin) {
+            std::normal_distribution<float> nd(0.f, std::sqrt(2.f / nin));
+            for (int k = 0; k < nout * nin; k++) w[off + k] = nd(rng);
+        };
+        const int H = NB_MLP_HIDDEN, I = NB_MLP_IN;
+        fill(0, H, I);
+        fill(H * I + H, H, H);
+        fill(H * I + H + H * H + H, 1, H);
+        w[NB_MLP_NPARAM - 1] = 1.0f;                   // targets are normalised to mean 1
+        CU(cudaMemcpy(ss->d_wm, w.data(), sizeof(float) * NB_MLP_NPARAM, cudaMemcpyHostToDevice));
+        CU(cudaMemset(ss->d_m, 0, sizeof(float) * NB_MLP_NPARAM));
+        CU(cudaMemset(ss->d_v, 0, sizeof(float) * NB_MLP_NPARAM));
+        if (nb_mlp_round(ss->d_wm, ss->d_wb, st->stream) < 0) return engine_err_cuda;
+    }
+    const int n = st->ntasks;
+    std::vector<int> perm(n);
+    for (int k = 0; k < n; k++) perm[k] = k;
+    const int per_epoch = std::min(n, 1 << 18);
+    if (batch <= 0) batch = 1024;
+    for (int ep = 0; ep < epochs; ep++) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        CU(cudaMemcpyAsync(ss->d_idx, perm.data(), sizeof(int) * per_epoch, cudaMemcpyHostToDevice, st->stream));
+        CU(cudaStreamSynchronize(st->stream));
+        for (int b0 = 0; b0 < per_epoch; b0 += batch) {
+            const int nb = std::min(batch, per_epoch - b0);
+            if (nb_mlp_grad(ss->d_feat, ss->d_target, ss->d_idx + b0, nb, ss->d_wb, ss->d_grad, ss->d_loss,
+                            st->stream) < 0)
+                return engine_err_cuda;
+            if (nb_mlp_adam(ss->d_wm, ss->d_wb, ss->d_grad, ss->d_m, ss->d_v, lr, 0.9f, 0.999f, 1e-8f, ++ss->step,
+                            st->stream) < 0)
+                return engine_err_cuda;
+        }
+    }
+    ss->trained = true;
+    if (loss_out != nullptr) {
+        // mean squared error over every task
+        if (nb_mlp_grad(ss->d_feat, ss->d_target, nullptr, n, ss->d_wb, ss->d_grad, ss->d_loss, st->stream) < 0)
+            return engine_err_cuda;
+        CU(cudaMemcpyAsync(loss_out, ss->d_loss, sizeof(float), cudaMemcpyDeviceToHost, st->stream));
+    }
+    CU(cudaStreamSynchronize(st->stream));
+    return 0;
+}
+
+extern "C" int engine_sched_predict(struct engine* e, float* pred_out, int n) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    SchedState* ss = sched(e, st);
+    if (ss == nullptr || !ss->trained) return engine_err_range;
+    if (nb_mlp_predict(ss->d_feat, st->ntasks, ss->d_wb, ss->d_pred, st->stream) < 0) return engine_err_cuda;
+    if (pred_out != nullptr) {
+        if (n != st->ntasks) return engine_err_range;
+        CU(cudaMemcpyAsync(pred_out, ss->d_pred, sizeof(float) * n, cudaMemcpyDeviceToHost, st->stream));
+    }
+    CU(cudaStreamSynchronize(st->stream));
+    return 0;
+}
+
+// Orders the queue by decreasing predicted cost (use_mlp) or restores the count-product
+// heuristic order.
+extern "C" int engine_sched_apply(struct engine* e, int use_mlp) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    if (!use_mlp) return engine_cuda_setorder(e, st->heur_order.data(), st->ntasks);
+    std::vector<float> pred(st->ntasks);
+    int rc = engine_sched_predict(e, pred.data(), st->ntasks);
+    if (rc < 0) return rc;
+    std::vector<int> order(st->ntasks);
+    for (int t = 0; t < st->ntasks; t++) order[t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pred[a] > pred[b]; });
+    return engine_cuda_setorder(e, order.data(), st->ntasks);
 }

@@ -16,6 +16,12 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmdcore_b200.so")
 
+MLP_IN = 10
+MLP_HIDDEN = 32
+MLP_NPARAM = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
+# count-product heuristic weights of the reference's partitioner (src/engine.c:574-576)
+CLASS_WEIGHT = (0.50004, 0.16176, 0.036213)
+
 engine_flag_none = 0
 engine_flag_cuda = 4
 engine_flag_unsorted = 512
@@ -85,6 +91,15 @@ def lib() -> C.CDLL:
         "engine_cuda_ntasks": (C.c_int, [vp]),
         "engine_cuda_fp32_peak": (C.c_int, [C.c_int, P(C.c_float)]),
         "engine_zero_forces": (C.c_int, [vp]),
+        "engine_sched_record": (C.c_int, [vp, C.c_int]),
+        "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
+        "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
+        "engine_sched_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint, P(C.c_float)]),
+        "engine_sched_predict": (C.c_int, [vp, P(C.c_float), C.c_int]),
+        "engine_sched_apply": (C.c_int, [vp, C.c_int]),
+        "nb_mlp_predict": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+        "nb_mlp_grad": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
+        "nb_mlp_adam": (C.c_int, [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, vp]),
         "potential_create_LJ126": (P(Potential), [C.c_double] * 5),
         "potential_create_LJ126_Coulomb": (P(Potential), [C.c_double] * 6),
         "potential_create_Coulomb": (P(Potential), [C.c_double] * 4),
@@ -219,6 +234,39 @@ class Engine:
         a, b = C.c_float(), C.c_float()
         _check(self.lib.engine_cuda_kernel_times(self.ptr, C.byref(a), C.byref(b)), "engine_cuda_kernel_times")
         return a.value, b.value
+
+    # -- learned scheduler ----------------------------------------------------------
+    def sched_record(self, nsteps: int):
+        _check(self.lib.engine_sched_record(self.ptr, nsteps), "engine_sched_record")
+
+    def sched_features(self) -> np.ndarray:
+        n = self.ntasks()
+        X = np.zeros((n, MLP_IN), np.float32)
+        _check(self.lib.engine_sched_features(self.ptr, X.ctypes.data_as(C.POINTER(C.c_float)), n),
+               "engine_sched_features")
+        return X
+
+    def sched_targets(self) -> np.ndarray:
+        n = self.ntasks()
+        y = np.zeros(n, np.float32)
+        _check(self.lib.engine_sched_targets(self.ptr, y.ctypes.data_as(C.POINTER(C.c_float)), n),
+               "engine_sched_targets")
+        return y
+
+    def sched_train(self, epochs: int = 100, batch: int = 1024, lr: float = 3e-3, seed: int = 0) -> float:
+        loss = C.c_float()
+        _check(self.lib.engine_sched_train(self.ptr, epochs, batch, lr, seed, C.byref(loss)), "engine_sched_train")
+        return loss.value
+
+    def sched_predict(self) -> np.ndarray:
+        n = self.ntasks()
+        p = np.zeros(n, np.float32)
+        _check(self.lib.engine_sched_predict(self.ptr, p.ctypes.data_as(C.POINTER(C.c_float)), n),
+               "engine_sched_predict")
+        return p
+
+    def sched_apply(self, use_mlp: bool):
+        _check(self.lib.engine_sched_apply(self.ptr, int(use_mlp)), "engine_sched_apply")
 
     def tune(self, warps: int = 0, plain: bool = False):
         """warps per block (0 = default); plain=True selects the one-block-per-task form."""
