@@ -1,22 +1,27 @@
 #!/usr/bin/env python
 """Benchmark of the nonbonded hot path: pair interactions per second on rigid SPC/E water
-(98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions per molecule).
+(98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions per molecule) by default; also LJ
+argon (32,000 atoms), the 1,048,576-atom LJ slab and the 512-replica argon ensemble
+(--workload argon|slab|replicas).
 
-One step = one nonbonded force evaluation of the whole system: sort every cell along the
-13 pair directions, sweep all 10,206 cell-pair/self tasks, fixed-point force accumulation,
-FP64 energy and virial.
+One step = one nonbonded force evaluation of the whole system (of every replica): sort every
+cell along the 13 pair directions, sweep all cell-pair/self tasks, fixed-point force
+accumulation, FP64 energy and virial.  The launch shape comes from the autotuner and every
+evaluation replays a CUDA graph of its launches.
 
   value   device-resident: positions already in HBM, kernels only (CUDA events around each
           step on the launching stream; L2 flushed with a 256 MiB write before every step,
           outside the events).
-  e2e     the C-ABI call engine_nonbond_cuda with host buffers: packing the cells, one
-          host->device copy of positions/ids/cell offsets, sort + sweep, one device->host
-          copy of forces and energies, unpacking.
+  e2e     the C-ABI call engine_nonbond_cuda (engine_batch_nonbond for the replicas) with
+          host buffers: packing the cells, one host->device copy of positions/ids/cell
+          offsets, sort + sweep, one device->host copy of forces and energies, unpacking.
+  plain   the plain form (one block per task) on the same protocol; for the replicas also
+          the ensemble evaluated as 512 sequential single-engine plain runs.
 
 Multi-GPU: the path is not partitioned here ("replicas only"): each rank evaluates its own
-copy of the system and value = ranks * pairs / max-over-ranks time.
+copy of the workload and value = ranks * pairs / max-over-ranks time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 """
 import argparse
 import json
@@ -43,11 +48,15 @@ def ns_per_day(ms_per_step):
 
 WORKLOADS = {
     "water": ("rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, 9x9x9 cells, "
-              "cutoff 1.0 nm, 98,304 exclusions, seeded", lambda W: W.water_spce(32)),
+              "cutoff 1.0 nm, 98,304 exclusions, seeded", lambda W: W.water_spce(32),
+              "sweep_tuned_water98k_traffic.txt"),
     "slab": ("LJ liquid slab in vapour, 1,048,576 atoms (80/20 two types) in a 40x40x160 nm box, 40x40x160 cells, "
-             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab()),
+             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab(), "sweep_tuned_slab1m_traffic.txt"),
     "argon": ("LJ argon, 32,000 atoms on a jittered FCC lattice in an 11.5074 nm box, 11^3 cells, cutoff 1.0 nm, "
-              "seeded", lambda W: W.argon_fcc(20)),
+              "seeded", lambda W: W.argon_fcc(20), "sweep_tuned_argon32k_traffic.txt"),
+    "replicas": ("512 LJ argon replicas, N log-uniform 500-8,000 (1,451,403 atoms in all), density 18-24 "
+                 "atoms/nm^3, cubic periodic boxes, cutoff 1.0 nm, seeded; one batch", lambda W: W.argon_replicas(),
+                 "sweep_tuned_replicas512_traffic.txt"),
 }
 SELECTED = "water"
 
@@ -104,7 +113,7 @@ def run_reference_driver(sysm, threads, warmup, steps):
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     with tempfile.TemporaryDirectory() as tmp:
-        sysf = os.path.join(tmp, "water.sys")
+        sysf = os.path.join(tmp, "system.sys")
         W.write_sysfile(sysm, sysf)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
         r = subprocess.run([exe, "bench", sysf, str(threads), str(warmup), str(steps)], capture_output=True,
@@ -120,30 +129,49 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+def cpu_sample(systems, threads, steps=5, every=16):
+    """The reference's pthreads CPU runner on a bounded sample of the workload: the whole
+    system, or every `every`-th replica of an ensemble; pairs per second over the sample."""
+    sample = systems if len(systems) == 1 else systems[::every]
+    try:
+        ms = pairs = 0.0
+        for s in sample:
+            r = run_reference_driver(s, threads, 1, steps)
+            ms += r["ms_per_step"]
+            pairs += pair_count(s)
+    except (FileNotFoundError, subprocess.CalledProcessError) as exc:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    what = ("the full system" if len(systems) == 1 else
+            f"{len(sample)} of the {len(systems)} replicas (every {every}th, {int(sum(s.n for s in sample))} atoms)")
+    return {"value": pairs / (ms * 1e-3), "unit": UNIT, "cores": threads, "kind": "reference",
+            "ms_per_step": ms, "sample": f"{steps} engine_step calls (dt=0) of {what} on {threads} pthreads runners, "
+                                        f"reference build in oracle/_ref"}
+
+
 def reference_arm(args, rank):
     """The reference's own pthreads CPU runner (oracle/_ref, built from the reference
     sources) on the same workload, all host threads."""
     if rank != 0:
         return
-    sysm = build_system()
+    built = build_system()
+    systems = built if isinstance(built, list) else [built]
     threads = host_threads()
-    pairs = pair_count(sysm)
-    try:
-        r = run_reference_driver(sysm, threads, max(1, min(args.warmup, 3)), max(1, min(args.steps, 20)))
-    except (FileNotFoundError, subprocess.CalledProcessError) as exc:
-        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {exc}"}))
+    steps = max(1, min(args.steps, 20 if len(systems) == 1 else 3))
+    cb = cpu_sample(systems, threads, steps=steps)
+    if cb["value"] is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {cb['sample']}"}))
         return
-    ms = r["ms_per_step"]
-    v = pairs / (ms * 1e-3)
+    ms = cb.pop("ms_per_step")
+    v = cb["value"]
+    pairs = sum(pair_count(s) for s in systems)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": r["steps"], "warmup": max(1, min(args.warmup, 3)), "ms_per_step": ms,
+        "steps": steps, "warmup": 1, "ms_per_step": pairs / v * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "ns_per_day": ns_per_day(ms),
-        "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "parallelism": "pthreads runners"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{r['steps']} engine_step calls (dt=0) of the full system, "
-                                   f"{threads} runners"},
+        "data": "synthetic", "ns_per_day": ns_per_day(pairs / v * 1e3),
+        "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "parallelism": "pthreads runners",
+                   "sample_ms_per_step": ms},
+        "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -162,7 +190,45 @@ def pair_count(sysm):
     return _PAIRS[sysm.name]
 
 
+def cell_counts(sysm, e):
+    """Particles per cell of one engine (cells as space_init lays them out)."""
+    import numpy as np
+    cdim = np.floor(np.asarray(sysm.dim) / np.asarray(sysm.L)).astype(int)
+    return np.bincount(e.cells(), minlength=int(np.prod(cdim)))
+
+
+def transfer_bytes(systems, engines):
+    """Bytes copied per host-buffer evaluation: positions+types and ids per padded slot and
+    the cell offsets/counts up; float forces per slot, cell energies and virials and the
+    counters down."""
+    slots = ncells = 0
+    for s, e in zip(systems, engines):
+        c = cell_counts(s, e)
+        slots += int((((c + 3) // 4) * 4).sum())
+        ncells += len(c)
+    return 20 * slots + 4 * (2 * ncells + 1), 12 * slots + 16 * ncells + 64, ncells, \
+        any((cell_counts(s, e) == 0).any() for s, e in zip(systems, engines))
+
+
+def timed_resident(tgt, stream, flush, steps, torch):
+    """Mean device time (ms) of `steps` device-resident evaluations, L2 flushed before
+    each (outside the events), and the mean sweep-kernel time."""
+    tot = sweep = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        tgt.resident()
+        ev1.record(stream)
+        ev1.synchronize()
+        tot += ev0.elapsed_time(ev1)
+        sweep += tgt.kernel_times()[1]
+    return tot / steps, sweep / steps
+
+
 def ours(args, rank, world, local_rank):
+    import numpy as np
     import torch
     import mdcore_b200 as M
 
@@ -175,18 +241,24 @@ def ours(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    sysm = build_system()
-    e = M.Engine.from_system(sysm, device=local_rank)
+    built = build_system()
+    replicas = isinstance(built, list)
+    systems = built if replicas else [built]
+    if replicas:
+        engines = [M.Engine.from_system(s, start=False) for s in systems]
+        tgt = M.Batch(engines, device=local_rank)
+    else:
+        engines = [M.Engine.from_system(built, device=local_rank)]
+        tgt = engines[0]
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    e.set_stream(stream.cuda_stream)
+    tgt.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    N = sysm.n
 
     # warm-up (host-buffer path, which also uploads the particles)
     for _ in range(args.warmup):
-        e.nonbond()
-    st = e.stats()
+        tgt.nonbond()
+    st = tgt.stats()
     if st.status != 0:
         raise SystemExit(f"bench.py: device status {st.status}")
     pairs = int(st.pairs)
@@ -196,50 +268,25 @@ def ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # ---- launch shape by the autotuner, then CUDA-graph replay of every evaluation
+    tgt.load_parts()
+    warps, window, tune_ms = tgt.autotune(reps=3)
+    tgt.graph(True)
+    for _ in range(3):                   # direct launch, capture, first replay
+        tgt.resident()
+
     clocks = ClockSampler(local_rank)
     clocks.start()
 
     # ---- device-resident timed region
-    e.load_parts()
-    for _ in range(2):
-        e.resident()
     barrier()
-    tot_ms, sweep_ms = 0.0, 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        e.resident()
-        ev1.record(stream)
-        ev1.synchronize()
-        tot_ms += ev0.elapsed_time(ev1)
-        sweep_ms += e.kernel_times()[1]
+    ms, ms_sweep = timed_resident(tgt, stream, flush, args.steps, torch)
     barrier()
-    e.unload_parts()
-    if e.stats().status != 0:
+    tgt.unload_parts()
+    if tgt.stats().status != 0:
         raise SystemExit("bench.py: device status after timed region")
 
-    # ---- the plain form (one CTA per task, IEEE sqrt/div), same protocol, for tuned-vs-plain
-    e.tune(0, plain=True)
-    e.load_parts()
-    e.resident()
-    barrier()
-    plain_ms, plain_sweep = 0.0, 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        e.resident()
-        ev1.record(stream)
-        ev1.synchronize()
-        plain_ms += ev0.elapsed_time(ev1)
-        plain_sweep += e.kernel_times()[1]
-    barrier()
-    e.tune(0, plain=False)
-
-    # ---- end-to-end timed region (host buffers through the C ABI)
+    # ---- end-to-end timed region (host buffers through the C ABI, graph replay)
     barrier()
     e2e_ms = 0.0
     host = {"pack": 0.0, "device": 0.0, "unpack": 0.0}
@@ -249,35 +296,69 @@ def ours(args, rank, world, local_rank):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        e.nonbond()
+        tgt.nonbond()
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms += ev0.elapsed_time(ev1)
-        hs = e.stats()
+        hs = tgt.stats()
         host["pack"] += hs.ms_pack / args.steps
         host["device"] += hs.ms_device / args.steps
         host["unpack"] += hs.ms_unpack / args.steps
     barrier()
     clk = clocks.stop()
+    if tgt.stats().status != 0:
+        raise SystemExit("bench.py: device status after e2e region")
 
-    ms = tot_ms / args.steps
-    ms_e2e = e2e_ms / args.steps
-    ms_sweep = sweep_ms / args.steps
+    # ---- the plain form (one CTA per task, IEEE sqrt/div, no graph), same protocol
+    tgt.graph(False)
+    tgt.tune(0, plain=True)
+    tgt.load_parts()
+    tgt.resident()
+    barrier()
+    plain_ms, plain_sweep = timed_resident(tgt, stream, flush, args.steps, torch)
+    barrier()
+    tgt.tune(warps, plain=False)
+
+    # ---- replicas: the same ensemble as sequential single-engine runs of the plain form
+    seq = None
+    if replicas:
+        singles = [M.Engine.from_system(s, device=local_rank) for s in systems]
+        for e in singles:
+            e.set_stream(stream.cuda_stream)
+            e.tune(0, plain=True)
+            e.load_parts()
+            e.resident()
+        barrier()
+        seq_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for e in singles:
+                e.resident()
+            ev1.record(stream)
+            ev1.synchronize()
+            seq_ms += ev0.elapsed_time(ev1)
+        barrier()
+        seq_ms /= args.steps
+        seq = {"value": world * pairs / (seq_ms * 1e-3), "ms_per_step": seq_ms,
+               "what": f"{len(singles)} sequential single-engine evaluations of the plain form, device-resident"}
+        for e in singles:
+            e.close()
+
     if dist is not None:
-        t = torch.tensor([ms, ms_e2e, ms_sweep], device="cuda", dtype=torch.float64)
+        t = torch.tensor([ms, e2e_ms / args.steps, ms_sweep], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_e2e, ms_sweep = [float(v) for v in t.tolist()]
+    else:
+        ms_e2e = e2e_ms / args.steps
     if rank == 0:
-        import numpy as np
-        counts = np.bincount(e.cells(), minlength=1)
-        ncells = len(counts)
-        slots_used = int((((counts + 3) // 4) * 4).sum())
-        h2d = 20 * slots_used + 4 * (2 * ncells + 1)          # xq + pid, cell offsets + counts
-        d2h = 12 * slots_used + 8 * ncells + 64               # float forces, cell energies, counters
+        h2d, d2h, ncells, compact = transfer_bytes(systems, engines)
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "sweep_tuned_water98k_traffic.txt")
+        prof = os.path.join(ROOT, "profiles", WORKLOADS[SELECTED][2])
         if os.path.exists(prof):       # dram read + write bytes of one sweep launch, from ncu
             for ln in open(prof):
                 if ln.startswith("dram_bytes_per_launch"):
@@ -287,8 +368,11 @@ def ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "ns_per_day": ns_per_day(ms),
-            "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
-                       "tasks": e.ntasks(), "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
+                       "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
+                       "tasks": tgt.ntasks(), "cells": ncells, "parallelism": f"replicas x{world}",
+                       "launch": {"warps_per_block": warps, "window": window, "autotune_ms": tune_ms,
+                                  "cuda_graph": True},
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
             "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -298,25 +382,20 @@ def ours(args, rank, world, local_rank):
                          "kernel": "sweep_tuned", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain": {"value": world * pairs / (plain_ms / args.steps * 1e-3), "ms_per_step": plain_ms / args.steps,
-                      "sweep_ms": plain_sweep / args.steps,
+            "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                      "sweep_ms": plain_sweep,
                       "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": (2 + 3 * int(compact)) * args.steps,
             "clocks": clk,
         }
+        if seq is not None:
+            line["sequential_plain"] = seq
         if world == 1 and not args.no_cpu_baseline:
-            try:
-                threads = host_threads()
-                r = run_reference_driver(sysm, threads, 1, 5)
-                cv = pairs / (r["ms_per_step"] * 1e-3)
-                line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "reference",
-                                        "sample": f"5 engine_step calls (dt=0) of the full system on "
-                                                  f"{threads} pthreads runners, reference build in oracle/_ref"}
-            except (FileNotFoundError, subprocess.CalledProcessError) as exc:
-                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                                        "sample": f"unavailable: {exc}"}
+            line["cpu_baseline"] = cpu_sample(systems, host_threads())
         print(json.dumps(line))
-    e.close()
+    tgt.close()
+    for e in engines:
+        e.close()
     if dist is not None:
         dist.destroy_process_group()
 
@@ -329,6 +408,8 @@ def sched_ab(args, local_rank):
     import mdcore_b200 as M
     torch.cuda.set_device(local_rank)
     sysm = build_system()
+    if isinstance(sysm, list):
+        raise SystemExit("bench.py: --sched-ab takes a single system (water, argon or slab)")
     e = M.Engine.from_system(sysm, device=local_rank)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -379,7 +460,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
-                    help="water (default: the headline configuration) or another seeded system")
+                    help="water (default: the headline configuration), argon, slab or replicas")
     ap.add_argument("--sched-ab", action="store_true",
                     help="train the task-cost model and compare sweep makespans of the queue orders")
     ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")

@@ -405,6 +405,44 @@ int engine_cuda_setorder(struct engine *e, const int *order, int n);
 int engine_cuda_taskclocks(struct engine *e, int enable, long long *clocks, int *sms, int n);
 /* Number of device tasks (self + pair). */
 int engine_cuda_ntasks(struct engine *e);
+/* Sweep steps each lane holds before the warp reduce-scatter of the persistent sweep: 4
+ * (default) or 8.  Forces are identical either way. */
+int engine_cuda_setwindow(struct engine *e, int window);
+/* CUDA-graph replay of each evaluation's launches (zeroing, sort, queue compaction,
+ * sweep): enable = 1 captures the launches on the second evaluation of a launch
+ * configuration and replays the graph from then on; a new configuration (other slot
+ * count, largest cell, buffers, launch shape) is captured anew. */
+int engine_cuda_graph(struct engine *e, int enable);
+/* Times every persistent launch shape (2, 4, 8 worker warps per block x window 4, 8) on
+ * the resident particles (uploaded first if none are) and keeps the fastest; returns the
+ * chosen shape and its median device time (sort + sweep).  Results stay resident. */
+int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *window, float *ms);
+
+/* ---- batches of engines (no counterpart in the reference) ----
+ * One device state for many independent engines (replicas: the same potentials, cutoff
+ * and flags; their own particles, boxes and cell sizes).  Each evaluation sorts every
+ * engine's cells in one launch and sweeps the concatenated task list with one persistent
+ * launch; forces, per-cell energies, energies and virials go back to each engine (its
+ * cells and stats; pair counts of each engine's stats are -1), totals to
+ * engine_batch_stats.  The engines keep their host data and must outlive the batch; they
+ * need no device state of their own (engine_start is not required). */
+struct engine_batch;
+int engine_batch_create(struct engine **engines, int n, struct engine_batch **out);
+int engine_batch_free(struct engine_batch *b);
+/* engine_nonbond_cuda for every engine: upload, sort + sweep, download. */
+int engine_batch_nonbond(struct engine_batch *b);
+/* engine_step for every engine with the forces of one batch evaluation. */
+int engine_batch_step(struct engine_batch *b);
+int engine_batch_load_parts(struct engine_batch *b);
+int engine_batch_resident(struct engine_batch *b);
+int engine_batch_unload_parts(struct engine_batch *b);
+int engine_batch_stats(struct engine_batch *b, struct nb_stats *out);
+int engine_batch_setstream(struct engine_batch *b, void *stream);
+int engine_batch_kernel_times(struct engine_batch *b, float *total_ms, float *sweep_ms);
+int engine_batch_settune(struct engine_batch *b, int warps, int plain);
+int engine_batch_graph(struct engine_batch *b, int enable);
+int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *window, float *ms);
+int engine_batch_ntasks(struct engine_batch *b);
 
 #ifdef __cplusplus
 }

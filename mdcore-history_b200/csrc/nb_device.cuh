@@ -36,8 +36,15 @@ enum : unsigned {
 enum { kAccEpot = 0, kAccVirial, kAccPairs, kAccExcl, kAccCand, kAccStatus, kAccCount = 8 };
 
 struct TaskRec {        // one cell pair (or self) task
-    int ci, cj, sid, dnshift;     // sid = -1 for self tasks
+    int ci, cj, sid;              // sid = -1 for self tasks
+    int dbits;                    // discretised shift norm | sweep bound << 16 (pair tasks)
 };
+
+// The reference's discretised |shift| (src/runner_dopair.c:593-597) and projection bound
+// dmaxdist (src/runner_dopair.c:583), per task because replicas of a batch have their own
+// cell sizes.
+__host__ __device__ __forceinline__ int task_dnshift(const TaskRec& r) { return r.dbits & 0xffff; }
+__host__ __device__ __forceinline__ int task_dmax(const TaskRec& r) { return (int)((unsigned)r.dbits >> 16); }
 
 struct Params {
     const float4* xq;
@@ -48,6 +55,7 @@ struct Params {
     unsigned long long* force;
     unsigned long long* acc;
     unsigned long long* cell_epot;  // per-cell fixed-point energy (2^32 units per kJ/mol)
+    unsigned long long* cell_vir;   // per-cell fixed-point virial, or nullptr: summed in acc
     const TaskRec* tasks;
     const float4* tshift;       // per-task shift of cell j relative to cell i
     int ntasks;
@@ -61,7 +69,6 @@ struct Params {
     const int* exlist;
     float cutoff2;              // pair tasks: float(cutoff)^2 in float (src/runner_dopair.c:578-579)
     float cutoff2s;             // self tasks: float(cutoff^2) (src/runner_dopair.c:896)
-    int dmaxdist;
     int unsorted;               // 1: sweep every candidate (engine_flag_unsorted)
 };
 

@@ -39,7 +39,8 @@ __host__ inline size_t sort_smem_bytes() { return kSortWarps * sort_warp_bytes()
 __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
                                                               const int* __restrict__ ccount,
                                                               const unsigned* __restrict__ cmask,
-                                                              unsigned* __restrict__ keys, float dscale, float bias,
+                                                              unsigned* __restrict__ keys,
+                                                              const float2* __restrict__ cscale,
                                                               unsigned long long* acc) {
     extern __shared__ __align__(16) unsigned char sort_smem[];
     constexpr unsigned FULL = 0xffffffffu;
@@ -60,6 +61,7 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
     const int start = cstart[c];
     const int pad = (n + 3) & ~3;
     const unsigned mask = cmask[c];
+    const float dscale = cscale[c].x, bias = cscale[c].y;     // 32767/(2|h|), |h| of the cell's box
     for (int sid = warp; sid < 13; sid += kSortWarps) {
         if (!((mask >> sid) & 1u)) continue;
         const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
@@ -272,7 +274,8 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     const float4* __restrict__ jpos = self ? S.xj : S.js;
     const int* __restrict__ jids = self ? S.pidj : S.jid;
     const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
-    const int dnshift = tr.dnshift;
+    const int dnshift = task_dnshift(tr);
+    const int dmaxdist = task_dmax(tr);
     const float cut2 = self ? P.cutoff2s : P.cutoff2;
     float4* myfj = S.fj + warp * cap;
     double epot = 0.0, vir = 0.0;
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             loc = key >> 16;
             di = key & 0xffff;
             // Quit-early test of the reference i loop (src/runner_dopair.c:600-602).
-            if (!P.unsorted) valid = valid && (S.jd[0] + dnshift - di <= P.dmaxdist);
+            if (!P.unsorted) valid = valid && (S.jd[0] + dnshift - di <= dmaxdist);
             if (!__any_sync(FULL, valid)) break;   // later chunks lie farther from cell j
         }
         float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
         }
         const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
         const int prow = __float_as_int(xi.w) * mt;
-        const int lim = P.dmaxdist - dnshift + di;
+        const int lim = dmaxdist - dnshift + di;
         const int kend = self ? min(ch * 32 + 32, ni) - 1 : nj;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         for (int k = 0; k < kend; ++k) {
@@ -426,7 +429,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             st |= S.cred[4 * w + 3];
         }
         atomicAdd(&P.cell_epot[ci], (unsigned long long)__double2ll_rn(e * kEnergyScale));
-        atomicAdd(&P.acc[kAccVirial], (unsigned long long)__double2ll_rn(v * kEnergyScale));
+        atomicAdd(P.cell_vir ? &P.cell_vir[ci] : &P.acc[kAccVirial], (unsigned long long)__double2ll_rn(v * kEnergyScale));
         if (np) atomicAdd(&P.acc[kAccPairs], np);
         if (ne) atomicAdd(&P.acc[kAccExcl], ne);
         if (nc) atomicAdd(&P.acc[kAccCand], nc);

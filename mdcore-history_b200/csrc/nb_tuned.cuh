@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kQueueBlock) queue_scatter(const int* __restri
 }
 
 // Shared memory of one worker warp (cap = largest cell rounded up to 4, plus 8 spare rows
-// that the 4-step sweep windows may read past the end of the j list).
+// that the 4- or 8-step sweep windows may read past the end of the j list).
 __host__ __device__ inline size_t warp_slice_bytes(int cap) { return 16 + (size_t)cap * 56; }
 
 __host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, int npots, int mt) {
@@ -288,8 +288,13 @@ __host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, i
 // j cell (positions, ids, sort keys) and the i cell's sort keys in its own shared-memory
 // slice with TMA bulk copies, sweeps all i chunks of the task itself and writes the
 // task's forces and energy.  Warps never wait for each other.
-template <int NW, bool HAS_EXCL, bool ONE_POT>
+//
+// WIN (4 or 8) is the number of consecutive sweep steps whose j contributions a lane keeps
+// in registers before the warp reduce-scatter: 8 halves the shuffles per step but holds
+// twice the registers.
+template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN>
 __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
+    static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const Params& P = T.p;
@@ -388,7 +393,8 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
 
         const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
-        const int dnshift = tr.dnshift;
+        const int dnshift = task_dnshift(tr);
+        const int dmaxdist = task_dmax(tr);
         double e_task = 0.0, v_task = 0.0;
         const int nchunks = (ni + 31) >> 5;
         const int jd0 = self ? 0 : jdist[0];
@@ -403,13 +409,13 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
                 const unsigned key = valid ? keyi[ii] : 0u;
                 loc = key >> 16;
                 const int di = key & 0xffff;
-                if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= P.dmaxdist);
+                if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
                 if (!__any_sync(FULL, valid)) break;        // later chunks lie farther from cell j
                 if (valid) {
                     if (P.unsorted) {
                         len = nj;
                     } else {                                // j with dist < lim form a prefix
-                        const int lim = P.dmaxdist - dnshift + di;
+                        const int lim = dmaxdist - dnshift + di;
                         int lo = 0, hi = nj;
                         while (lo < hi) {
                             const int mid = (lo + hi) >> 1;
@@ -435,11 +441,11 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
-            for (int k0 = 0; k0 < kmax; k0 += 4) {
-                float vx[4], vy[4], vz[4];
+            for (int k0 = 0; k0 < kmax; k0 += WIN) {
+                float vx[WIN], vy[WIN], vz[WIN];
                 bool any_acc = false;
 #pragma unroll
-                for (int m = 0; m < 4; ++m) {
+                for (int m = 0; m < WIN; ++m) {
                     const int k = k0 + m;
                     const float4 xj = jpos[k];
                     const bool act = k < len;
@@ -484,10 +490,17 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
                     vx[m] = wx; vy[m] = wy; vz[m] = wz;
                 }
                 if (any_acc) {
-                    const float tx = reduce_scatter4(vx, lane);
-                    const float ty = reduce_scatter4(vy, lane);
-                    const float tz = reduce_scatter4(vz, lane);
-                    if (lane < 4 && k0 + lane < kmax) {
+                    float tx, ty, tz;
+                    if constexpr (WIN == 8) {
+                        tx = reduce_scatter8(vx, lane);
+                        ty = reduce_scatter8(vy, lane);
+                        tz = reduce_scatter8(vz, lane);
+                    } else {
+                        tx = reduce_scatter4(vx, lane);
+                        ty = reduce_scatter4(vy, lane);
+                        tz = reduce_scatter4(vz, lane);
+                    }
+                    if (lane < WIN && k0 + lane < kmax) {
                         float4 a = fj[k0 + lane];
                         a.x += tx; a.y += ty; a.z += tz;
                         fj[k0 + lane] = a;
@@ -528,7 +541,8 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
         }
         if (lane == 0) {
             atomicAdd(&P.cell_epot[tr.ci], (unsigned long long)__double2ll_rn(e_task * kEnergyScale));
-            atomicAdd(&P.acc[kAccVirial], (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
+            atomicAdd(P.cell_vir ? &P.cell_vir[tr.ci] : &P.acc[kAccVirial],
+                      (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
             if (T.task_clock) {
                 T.task_clock[2 * t] = t_start;
                 T.task_clock[2 * t + 1] = clock64();

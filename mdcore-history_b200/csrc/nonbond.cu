@@ -1,12 +1,21 @@
 // GPU entry points of the engine: engine_cuda_load (src/runner_cuda.cu:2931-3545) and
-// engine_nonbond_cuda (src/runner_cuda.cu:2287-2628), plus device selection and the
-// device-resident evaluation used to time the kernels alone.
+// engine_nonbond_cuda (src/runner_cuda.cu:2287-2628), plus device selection, the
+// device-resident evaluation used to time the kernels alone, CUDA-graph replay, the launch
+// autotuner and batches of independent engines (replicas) evaluated by one launch.
 //
 // Per evaluation: pack the cells' particles (cell-relative float positions + type, id)
 // into pinned host buffers, one host->device copy each, zero the fixed-point force and
-// energy accumulators, sort_cells, sweep_tasks, one device->host copy of forces and
-// per-cell energies, unpack into the cells.  All launches go to one stream; CUDA events
-// around the kernels give the device time.
+// energy accumulators, sort_cells, sweep, one device->host copy of forces and per-cell
+// energies, unpack into the cells.  All launches go to one stream; CUDA events around the
+// kernels give the device time.
+//
+// One device state (NbState) serves a list of engines: a single engine (engine_cuda_load)
+// or a batch of replicas (engine_batch_create).  The engines' cells are concatenated
+// (engine k's cell c is global cell cell_off[k] + c), their particle ids offset by
+// id_off[k], and their tasks concatenated into one task list and one queue; each task
+// carries its own sort-distance bound and shift norm and each cell its own sort scale, so
+// replicas may have different boxes and cell sizes.  They must share the potential tables,
+// the cutoff and the flags.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -30,15 +39,22 @@ struct NbState {
     cudaStream_t own_stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;       // around sort + sweep
     cudaEvent_t evs0 = nullptr, evs1 = nullptr;     // around the sweep kernel alone
+    // engines served by this state and their offsets in the global cell / id numbering
+    std::vector<struct engine*> engines;
+    std::vector<int> cell_off, id_off;
+    struct nb_stats bstats = {};           // totals of the last evaluation over all engines
     // geometry
     int ncells = 0, ntasks = 0, ncap = 0, nid = 0;
-    float bias = 0.f, dscale = 0.f;
+    float bias = 0.f, dscale = 0.f;        // of engine 0 (used by the no-alloc entry point)
     int dmaxdist = 0;
     int maxcount = 0;
+    float cut2p = 0.f, cut2s = 0.f;        // pair and self cutoff^2 (src/runner_dopair.c:577, 896)
+    int unsorted = 0;
     // tables
     int npots = 0, ncoef = 0, max_type = 0;
     // tuning
     int warps = 4;
+    int window = 4;                // sweep steps per register reduce-scatter (4 or 8)
     bool has_excl = false;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
@@ -52,6 +68,14 @@ struct NbState {
     int* d_task_sm = nullptr;
     int record_clock = 0;
     int sm_count = 0;
+    // CUDA graph of one evaluation's launches (memsets, sort, queue, sweep)
+    bool use_graph = false;
+    bool capturing = false;
+    int last_grid = 0;             // grid of the last direct persistent launch
+    int buf_gen = 0;               // bumped whenever device buffers move
+    long long graph_key = -1, prepared_key = -1;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
     // device buffers
     float4* d_xq = nullptr;
     int* d_pid = nullptr;
@@ -60,8 +84,9 @@ struct NbState {
     int* d_cstart = nullptr;
     int* d_ccount = nullptr;
     unsigned* d_cmask = nullptr;
+    float2* d_cscale = nullptr;    // per cell: sort scale 32767/(2|h|) and bias |h|
     unsigned long long* d_acc = nullptr;
-    unsigned long long* d_cell_epot = nullptr;
+    unsigned long long* d_cell_epot = nullptr;   // 2 * ncells: energies, then virials
     TaskRec* d_tasks = nullptr;
     float4* d_tshift = nullptr;
     float* d_coef = nullptr;
@@ -77,7 +102,7 @@ struct NbState {
     int* h_cstart = nullptr;    // ncells+1 followed by ncells counts
     unsigned long long* h_force = nullptr;   // pinned; holds float forces (3 per slot)
     float* d_forcef = nullptr;
-    unsigned long long* h_cell_epot = nullptr;
+    unsigned long long* h_cell_epot = nullptr;   // 2 * ncells
     unsigned long long* h_acc = nullptr;
     bool resident_valid = false;
     void* sched = nullptr;             // learned-scheduler state (SchedState)
@@ -128,6 +153,8 @@ int alloc_particles(NbState* st, int ncap) {
     cudaFree(st->d_xq); cudaFree(st->d_pid); cudaFree(st->d_keys); cudaFree(st->d_force);
     st->d_xq = nullptr; st->d_pid = nullptr; st->d_keys = nullptr; st->d_force = nullptr;
     cudaFreeHost(st->h_xq); cudaFreeHost(st->h_pid); cudaFreeHost(st->h_force);
+    st->h_xq = nullptr; st->h_pid = nullptr; st->h_force = nullptr;
+    ++st->buf_gen;
     if (dev_alloc(&st->d_xq, ncap) || dev_alloc(&st->d_pid, ncap) || dev_alloc(&st->d_keys, 13 * (size_t)ncap) ||
         dev_alloc(&st->d_force, 3 * (size_t)ncap))
         return engine_err_cuda;
@@ -154,53 +181,52 @@ double now_ms() {
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
-// Packs the cells into the pinned staging buffers; returns the number of slots used.
-int pack_cells(struct engine* e, NbState* st) {
-    struct space* s = &e->s;
+// Packs every engine's cells into the pinned staging buffers; returns the number of slots.
+int pack_cells(NbState* st) {
     int total = 0, maxc = 0;
-    for (int c = 0; c < s->nr_cells; c++) {
-        int n = s->cells[c].count;
-        total += (n + 3) & ~3;
-        if (n > maxc) maxc = n;
-    }
+    for (struct engine* e : st->engines)
+        for (int c = 0; c < e->s.nr_cells; c++) {
+            const int n = e->s.cells[c].count;
+            total += (n + 3) & ~3;
+            if (n > maxc) maxc = n;
+        }
     if (maxc > kMaxPartsPerCell) {
         errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
     if (alloc_particles(st, total + 4) < 0) return engine_err_cuda;
     int* cstart = st->h_cstart;
-    int* ccount = st->h_cstart + s->nr_cells + 1;
+    int* ccount = st->h_cstart + st->ncells + 1;
     int slot = 0;
-    for (int c = 0; c < s->nr_cells; c++) {
-        cstart[c] = slot;
-        ccount[c] = s->cells[c].count;
-        slot += (s->cells[c].count + 3) & ~3;
-    }
-    for (int c = 0; c < s->nr_cells; c++) {
-        struct cell* cl = &s->cells[c];
-        const int slot = cstart[c];
-        for (int k = 0; k < cl->count; k++) {
-            const struct part* p = &cl->parts[k];
-            float4 v;
-            v.x = p->x[0]; v.y = p->x[1]; v.z = p->x[2];
-            v.w = bits_as_float((int)p->type);
-            st->h_xq[slot + k] = v;
-            st->h_pid[slot + k] = p->id;
-        }
-        int pad = (cl->count + 3) & ~3;
-        for (int k = cl->count; k < pad; k++) {
-            st->h_xq[slot + k] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
-            st->h_pid[slot + k] = 0;
+    for (size_t k = 0; k < st->engines.size(); k++) {
+        struct space* s = &st->engines[k]->s;
+        const int c0 = st->cell_off[k], id0 = st->id_off[k];
+        for (int c = 0; c < s->nr_cells; c++) {
+            struct cell* cl = &s->cells[c];
+            cstart[c0 + c] = slot;
+            ccount[c0 + c] = cl->count;
+            for (int q = 0; q < cl->count; q++) {
+                const struct part* p = &cl->parts[q];
+                st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
+                st->h_pid[slot + q] = id0 + p->id;
+            }
+            const int pad = (cl->count + 3) & ~3;
+            for (int q = cl->count; q < pad; q++) {
+                st->h_xq[slot + q] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
+                st->h_pid[slot + q] = 0;
+            }
+            slot += pad;
         }
     }
-    cstart[s->nr_cells] = slot;
+    cstart[st->ncells] = slot;
     st->maxcount = maxc;
     return slot;
 }
 
 template <int NW>
 int launch_plain_nw(NbState* st, const Params& P, int cap, size_t smem) {
-    CU(cudaFuncSetAttribute(sweep_tasks<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!st->capturing)
+        CU(cudaFuncSetAttribute(sweep_tasks<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     sweep_tasks<NW><<<st->ntasks, NW * 32, smem, st->stream>>>(P, cap);
     CU(cudaGetLastError());
     return 0;
@@ -226,29 +252,47 @@ int launch_plain(NbState* st, const Params& P, int cap) {
     }
 }
 
-template <int NW, bool EX, bool ONE>
+// Persistent launch: as many CTAs as fit on every SM at once.  Under stream capture the
+// function attribute and occupancy query are skipped and the grid of the preceding direct
+// launch of the same configuration is reused.
+template <int NW, bool EX, bool ONE, int WIN>
 int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    auto kern = sweep_tuned<NW, EX, ONE>;
-    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
-    if (per_sm < 1) per_sm = 1;
-    const int grid = st->sm_count * per_sm;
+    auto kern = sweep_tuned<NW, EX, ONE, WIN>;
+    int grid = st->last_grid;
+    if (!st->capturing) {
+        CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
+        if (per_sm < 1) per_sm = 1;
+        grid = st->sm_count * per_sm;
+        st->last_grid = grid;
+    }
     kern<<<grid, NW * 32, smem, st->stream>>>(T, cap);
     CU(cudaGetLastError());
     return 0;
 }
 
-template <int NW>
+template <int NW, int WIN>
 int launch_tuned_w(NbState* st, const TunedParams& T, int cap, size_t smem) {
     const bool one = st->one_pot;
     if (st->has_excl)
-        return one ? launch_tuned_nw<NW, true, true>(st, T, cap, smem) : launch_tuned_nw<NW, true, false>(st, T, cap, smem);
-    return one ? launch_tuned_nw<NW, false, true>(st, T, cap, smem) : launch_tuned_nw<NW, false, false>(st, T, cap, smem);
+        return one ? launch_tuned_nw<NW, true, true, WIN>(st, T, cap, smem)
+                   : launch_tuned_nw<NW, true, false, WIN>(st, T, cap, smem);
+    return one ? launch_tuned_nw<NW, false, true, WIN>(st, T, cap, smem)
+               : launch_tuned_nw<NW, false, false, WIN>(st, T, cap, smem);
 }
 
-int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
-    (void)e;
+template <int WIN>
+int launch_tuned_win(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
+    switch (nw) {
+        case 1: return launch_tuned_w<1, WIN>(st, T, cap, smem);
+        case 2: return launch_tuned_w<2, WIN>(st, T, cap, smem);
+        case 8: return launch_tuned_w<8, WIN>(st, T, cap, smem);
+        default: return launch_tuned_w<4, WIN>(st, T, cap, smem);
+    }
+}
+
+int launch_tuned(NbState* st, const Params& P, int cap4) {
     const int cap = cap4 + 8;
     TunedParams T;
     T.p = P;
@@ -279,24 +323,29 @@ int launch_tuned(struct engine* e, NbState* st, const Params& P, int cap4) {
                       __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
-    switch (nw) {
-        case 1: return launch_tuned_w<1>(st, T, cap, smem);
-        case 2: return launch_tuned_w<2>(st, T, cap, smem);
-        case 8: return launch_tuned_w<8>(st, T, cap, smem);
-        default: return launch_tuned_w<4>(st, T, cap, smem);
-    }
+    return st->window == 8 ? launch_tuned_win<8>(st, T, cap, smem, nw) : launch_tuned_win<4>(st, T, cap, smem, nw);
 }
 
-int launch_kernels(struct engine* e, NbState* st) {
-    struct space* s = &e->s;
-    CU(cudaMemsetAsync(st->d_force, 0, sizeof(unsigned long long) * 3 * (size_t)st->h_cstart[s->nr_cells],
+// Records an event; inside a stream capture as an external record node, so that replaying
+// the graph records it again (a plain record would stay internal to the graph).
+int record_event(NbState* st, cudaEvent_t ev) {
+    if (st->capturing)
+        CU(cudaEventRecordWithFlags(ev, st->stream, cudaEventRecordExternal));
+    else
+        CU(cudaEventRecord(ev, st->stream));
+    return 0;
+}
+
+// The launches of one evaluation: zero the accumulators, sort, (compact the queue,) sweep.
+int issue_kernels(NbState* st) {
+    CU(cudaMemsetAsync(st->d_force, 0, sizeof(unsigned long long) * 3 * (size_t)st->h_cstart[st->ncells],
                        st->stream));
     CU(cudaMemsetAsync(st->d_acc, 0, sizeof(unsigned long long) * kAccCount, st->stream));
-    CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * st->ncells, st->stream));
+    CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * 2 * st->ncells, st->stream));
     const int cap = (st->maxcount + 3) & ~3;
     if (cap == 0) return 0;
     sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
-        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->dscale, st->bias, st->d_acc);
+        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->d_cscale, st->d_acc);
     CU(cudaGetLastError());
 
     Params P;
@@ -308,6 +357,7 @@ int launch_kernels(struct engine* e, NbState* st) {
     P.force = st->d_force;
     P.acc = st->d_acc;
     P.cell_epot = st->d_cell_epot;
+    P.cell_vir = st->d_cell_epot + st->ncells;
     P.tasks = st->d_tasks;
     P.tshift = st->d_tshift;
     P.ntasks = st->ntasks;
@@ -321,38 +371,107 @@ int launch_kernels(struct engine* e, NbState* st) {
     P.emask = st->d_emask;
     P.exoff = st->d_exoff;
     P.exlist = st->d_exlist;
-    const float cutf = (float)s->cutoff;
-    P.cutoff2 = cutf * cutf;
-    P.cutoff2s = (float)s->cutoff2;
-    P.dmaxdist = st->dmaxdist;
-    P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
+    P.cutoff2 = st->cut2p;
+    P.cutoff2s = st->cut2s;
+    P.unsorted = st->unsorted;
 
-    CU(cudaEventRecord(st->evs0, st->stream));
-    int rc = st->plain ? launch_plain(st, P, cap) : launch_tuned(e, st, P, cap);
+    int rc = record_event(st, st->evs0);
     if (rc < 0) return rc;
-    CU(cudaEventRecord(st->evs1, st->stream));
+    rc = st->plain ? launch_plain(st, P, cap) : launch_tuned(st, P, cap);
+    if (rc < 0) return rc;
+    return record_event(st, st->evs1);
+}
+
+void drop_graph(NbState* st) {
+    if (st->graph_exec) cudaGraphExecDestroy(st->graph_exec);
+    if (st->graph) cudaGraphDestroy(st->graph);
+    st->graph_exec = nullptr;
+    st->graph = nullptr;
+    st->graph_key = -1;
+}
+
+// Everything the captured launches depend on besides the device buffers' contents.
+long long launch_key(const NbState* st) {
+    long long k = st->h_cstart[st->ncells];                    // slots
+    k = k * 1031 + st->maxcount;
+    k = k * 131 + st->buf_gen;
+    k = k * 17 + st->warps;
+    k = k * 17 + st->window;
+    k = k * 3 + st->plain;
+    k = k * 3 + st->record_clock;
+    return k;
+}
+
+// One evaluation on the device.  With graphs enabled, the first evaluation of a launch
+// configuration runs directly (it sets the kernels' attributes and sizes the grid), the
+// second captures the launches into a graph, and later ones replay it.
+int launch_kernels(NbState* st) {
+    if (!st->use_graph) return issue_kernels(st);
+    const long long key = launch_key(st);
+    if (st->graph_exec != nullptr && st->graph_key == key) {
+        CU(cudaGraphLaunch(st->graph_exec, st->stream));
+        return 0;
+    }
+    if (st->prepared_key != key) {
+        drop_graph(st);
+        st->prepared_key = key;
+        return issue_kernels(st);
+    }
+    drop_graph(st);
+    CU(cudaStreamBeginCapture(st->stream, cudaStreamCaptureModeThreadLocal));
+    st->capturing = true;
+    int rc = issue_kernels(st);
+    st->capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(st->stream, &g);
+    if (rc < 0) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CU(end);
+    st->graph = g;
+    CU(cudaGraphInstantiate(&st->graph_exec, g, 0));
+    st->graph_key = key;
+    CU(cudaGraphLaunch(st->graph_exec, st->stream));
     return 0;
 }
 
-// Reads back accumulators, stores stats and the per-cell energies.
-int finish_stats(struct engine* e, NbState* st) {
-    struct space* s = &e->s;
+// Reads back the accumulators: per-engine energies and virials into each engine's stats
+// and cells, totals into st->bstats.
+int finish_stats(NbState* st) {
     const unsigned long long* a = st->h_acc;
-    double epot = 0.0;
-    long long esum = 0;
-    for (int c = 0; c < st->ncells; c++) {
-        long long v = (long long)st->h_cell_epot[c];
-        esum += v;
-        s->cells[c].epot = (double)v / kEnergyScale;
+    const unsigned long long* cvir = st->h_cell_epot + st->ncells;
+    long long etot = 0, vtot = 0;
+    for (size_t k = 0; k < st->engines.size(); k++) {
+        struct engine* e = st->engines[k];
+        struct space* s = &e->s;
+        long long esum = 0, vsum = 0;
+        for (int c = 0; c < s->nr_cells; c++) {
+            const long long v = (long long)st->h_cell_epot[st->cell_off[k] + c];
+            esum += v;
+            vsum += (long long)cvir[st->cell_off[k] + c];
+            s->cells[c].epot = (double)v / kEnergyScale;
+        }
+        etot += esum;
+        vtot += vsum;
+        e->stats.epot = (double)esum / kEnergyScale;
+        e->stats.virial = -(double)vsum / kEnergyScale;
+        e->stats.status = (int)a[kAccStatus];
+        s->epot_nonbond += e->stats.epot;
+        if (st->engines.size() == 1) {
+            e->stats.pairs = (int64_t)a[kAccPairs];
+            e->stats.excluded = (int64_t)a[kAccExcl];
+            e->stats.candidates = (int64_t)a[kAccCand];
+        } else {                               // counts are kept for the batch only
+            e->stats.pairs = e->stats.excluded = e->stats.candidates = -1;
+        }
     }
-    epot = (double)esum / kEnergyScale;
-    e->stats.epot = epot;
-    e->stats.virial = -(double)(long long)a[kAccVirial] / kEnergyScale;
-    e->stats.pairs = (int64_t)a[kAccPairs];
-    e->stats.excluded = (int64_t)a[kAccExcl];
-    e->stats.candidates = (int64_t)a[kAccCand];
-    e->stats.status = (int)a[kAccStatus];
-    s->epot_nonbond += epot;
+    st->bstats.epot = (double)etot / kEnergyScale;
+    st->bstats.virial = -(double)vtot / kEnergyScale;
+    st->bstats.pairs = (int64_t)a[kAccPairs];
+    st->bstats.excluded = (int64_t)a[kAccExcl];
+    st->bstats.candidates = (int64_t)a[kAccCand];
+    st->bstats.status = (int)a[kAccStatus];
     if (a[kAccStatus] != 0) {
         const char* msg = (a[kAccStatus] & kStatusCellOverflow)   ? "Max. number of parts per cell exceeded."
                           : (a[kAccStatus] & kStatusCopyTimeout)  ? "Bulk copy into shared memory timed out."
@@ -365,14 +484,12 @@ int finish_stats(struct engine* e, NbState* st) {
     return 0;
 }
 
-}  // namespace
-
-extern "C" int nb_device_free(struct engine* e) {
-    NbState* st = state(e);
-    if (st == nullptr) return 0;
+void state_free(NbState* st) {
+    if (st == nullptr) return;
     cudaSetDevice(st->device);
+    drop_graph(st);
     void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
-                   st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
+                   st->d_cscale, st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
                    st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef, st->d_queue,
                    st->d_qcount, st->d_bsum};
@@ -386,46 +503,42 @@ extern "C" int nb_device_free(struct engine* e) {
     if (st->own_stream) cudaStreamDestroy(st->own_stream);
     sched_free(st->sched);
     delete st;
-    e->cuda = nullptr;
-    return 0;
 }
 
-extern "C" int engine_cuda_setdevice(struct engine* e, int id) {
-    if (e == nullptr) return engine_err_null;
-    int n = 0;
-    CU(cudaGetDeviceCount(&n));
-    if (id < 0 || id >= n) {
-        errs_register(engine_err_range, "No such CUDA device.", __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_range;
+// Same table contents (the batch evaluates every engine with engine 0's tables).
+bool same_table(const struct potential* p, const struct potential* q) {
+    if (p == q) return true;
+    if (p == nullptr || q == nullptr) return false;
+    if (p->n != q->n || std::memcmp(p->alpha, q->alpha, sizeof(p->alpha)) != 0) return false;
+    return std::memcmp(p->c, q->c, sizeof(float) * (size_t)(p->n + 1) * potential_chunk) == 0;
+}
+
+// Builds the device state of st->engines: tables, tasks, queue order, cell data, exclusions.
+int load_state(NbState* st) {
+    struct engine* e0 = st->engines[0];
+    const size_t ne = st->engines.size();
+    const int mt = e0->max_type;
+    st->cell_off.assign(ne + 1, 0);
+    st->id_off.assign(ne + 1, 0);
+    for (size_t k = 0; k < ne; k++) {                 // checked before any device call
+        struct engine* e = st->engines[k];
+        if (e->device != e0->device || e->max_type != mt || e->s.cutoff != e0->s.cutoff ||
+            (e->flags & engine_flag_unsorted) != (e0->flags & engine_flag_unsorted)) {
+            errs_register(engine_err_range, "Engines of a batch differ in device, types, cutoff or flags.", __LINE__,
+                          __func__, __FILE__);
+            return engine_err = engine_err_range;
+        }
+        for (int ij = 0; ij < mt * mt; ij++)
+            if (!same_table(e->p[ij], e0->p[ij])) {
+                errs_register(engine_err_potential, "Engines of a batch differ in their potentials.", __LINE__,
+                              __func__, __FILE__);
+                return engine_err = engine_err_potential;
+            }
+        st->cell_off[k + 1] = st->cell_off[k] + e->s.nr_cells;
+        st->id_off[k + 1] = st->id_off[k] + (e->s.size_parts > 0 ? e->s.size_parts : 1);
     }
-    e->device = id;
-    return 0;
-}
-
-extern "C" int engine_cuda_setdevices(struct engine* e, int nr_devices, int* ids) {
-    if (e == nullptr || ids == nullptr) return engine_err_null;
-    if (nr_devices != 1) {
-        errs_register(engine_err_nyi, "Only one device per engine.", __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_nyi;
-    }
-    return engine_cuda_setdevice(e, ids[0]);
-}
-
-extern "C" int engine_cuda_settune(struct engine* e, int warps, int plain) {
-    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8) return engine_err_range;
-    state(e)->warps = warps ? warps : 4;
-    state(e)->plain = plain ? 1 : 0;
-    return 0;
-}
-
-extern "C" int engine_cuda_load(struct engine* e) {
-    if (e == nullptr) return engine_err_null;
-    struct space* s = &e->s;
-    if (e->cuda) nb_device_free(e);
-    NbState* st = new NbState();
-    e->cuda = st;
-    st->device = e->device;
+    st->ncells = st->cell_off[ne];
+    st->device = e0->device;
     CU(cudaSetDevice(st->device));
     CU(cudaStreamCreateWithFlags(&st->own_stream, cudaStreamNonBlocking));
     st->stream = st->own_stream;
@@ -433,20 +546,23 @@ extern "C" int engine_cuda_load(struct engine* e) {
     CU(cudaEventCreate(&st->ev1));
     CU(cudaEventCreate(&st->evs0));
     CU(cudaEventCreate(&st->evs1));
-    st->ncells = s->nr_cells;
-    nb_sweep_scales(s, &st->bias, &st->dscale, &st->dmaxdist);
+    CU(cudaDeviceGetAttribute(&st->sm_count, cudaDevAttrMultiProcessorCount, st->device));
+    nb_sweep_scales(&e0->s, &st->bias, &st->dscale, &st->dmaxdist);
+    const float cutf = (float)e0->s.cutoff;
+    st->cut2p = cutf * cutf;
+    st->cut2s = (float)e0->s.cutoff2;
+    st->unsorted = (e0->flags & engine_flag_unsorted) ? 1 : 0;
 
     float axes[13][3];
     for (int sid = 0; sid < 13; sid++) sort_axis(sid, axes[sid]);
     CU(cudaMemcpyToSymbol(c_axes, axes, sizeof(axes)));
 
     // Potential tables: one copy of every distinct table, type pair -> table index.
-    const int mt = e->max_type;
     std::vector<struct potential*> uniq;
     std::vector<int> potidx((size_t)mt * mt, -1);
     for (int i = 0; i < mt; i++)
         for (int j = 0; j < mt; j++) {
-            struct potential* p = e->p[i * mt + j];
+            struct potential* p = e0->p[i * mt + j];
             if (p == nullptr) continue;
             int k = 0;
             while (k < (int)uniq.size() && uniq[k] != p) k++;
@@ -481,78 +597,95 @@ extern "C" int engine_cuda_load(struct engine* e) {
     CU(cudaMemcpy(st->d_potn, potn.data(), potn.size() * sizeof(int), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->d_potidx, potidx.data(), potidx.size() * sizeof(int), cudaMemcpyHostToDevice));
 
-    // Task list with the reference's per-pair shift and discretised shift norm.
-    st->ntasks = s->nr_tasks;
-    std::vector<TaskRec> tasks(st->ntasks > 0 ? st->ntasks : 1);
+    // Task list with the reference's per-pair shift, discretised shift norm and sweep
+    // bound; cells: sort-direction masks and sort scales.
+    int ntasks = 0;
+    for (struct engine* e : st->engines) ntasks += e->s.nr_tasks;
+    st->ntasks = ntasks;
+    std::vector<TaskRec> tasks(ntasks > 0 ? ntasks : 1, TaskRec{0, 0, -1, 0});
     std::vector<float4> tshift(tasks.size(), make_float4(0, 0, 0, 0));
-    for (int t = 0; t < s->nr_tasks; t++) {
-        const struct task* tk = &s->tasks[t];
-        if (tk->type == task_type_self) {
-            tasks[t] = TaskRec{tk->i, tk->i, -1, 0};
-        } else {
-            float sh[3];
-            int dn, ci, cj;
-            int sid = nb_task_shift(s, t, st->dscale, sh, &dn, &ci, &cj);
-            tasks[t] = TaskRec{ci, cj, sid, dn};
-            tshift[t] = make_float4(sh[0], sh[1], sh[2], 0.f);
+    std::vector<unsigned> cmask(st->ncells > 0 ? st->ncells : 1, 0u);
+    std::vector<float2> cscale(cmask.size(), make_float2(0.f, 0.f));
+    std::vector<double> cost(tasks.size(), 0.0);
+    int empty = 0;
+    for (size_t k = 0, t0 = 0; k < ne; k++) {
+        struct space* s = &st->engines[k]->s;
+        const int c0 = st->cell_off[k];
+        float bias, dscale;
+        int dmax;
+        nb_sweep_scales(s, &bias, &dscale, &dmax);
+        for (int c = 0; c < s->nr_cells; c++) {
+            cmask[c0 + c] = s->cells[c].sortmask;
+            cscale[c0 + c] = make_float2(dscale, bias);
+            empty += s->cells[c].count == 0;
         }
+        for (int t = 0; t < s->nr_tasks; t++) {
+            const struct task* tk = &s->tasks[t];
+            TaskRec r;
+            if (tk->type == task_type_self) {
+                r = TaskRec{c0 + tk->i, c0 + tk->i, -1, dmax << 16};
+            } else {
+                float sh[3];
+                int dn, ci, cj;
+                const int sid = nb_task_shift(s, t, dscale, sh, &dn, &ci, &cj);
+                r = TaskRec{c0 + ci, c0 + cj, sid, dn | (dmax << 16)};
+                tshift[t0 + t] = make_float4(sh[0], sh[1], sh[2], 0.f);
+            }
+            tasks[t0 + t] = r;
+            // Initial queue order by decreasing estimated cost, the reference's cell-pair
+            // weight (src/engine.c:574-576, 643-699): count_i*count_j times 0.50004 (face),
+            // 0.16176 (edge) or 0.036213 (corner) neighbours, n^2 - n for a cell with itself.
+            cost[t0 + t] = task_weight(r.sid, s->cells[r.ci - c0].count, s->cells[r.cj - c0].count);
+        }
+        t0 += s->nr_tasks;
     }
     if (dev_alloc(&st->d_tasks, tasks.size()) || dev_alloc(&st->d_tshift, tshift.size())) return engine_err_cuda;
     CU(cudaMemcpy(st->d_tasks, tasks.data(), tasks.size() * sizeof(TaskRec), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->d_tshift, tshift.data(), tshift.size() * sizeof(float4), cudaMemcpyHostToDevice));
-
-    // Task queue: initial order by decreasing estimated cost, the reference's cell-pair
-    // weight (src/engine.c:574-576, 643-699): count_i*count_j times 0.50004 (face),
-    // 0.16176 (edge) or 0.036213 (corner) neighbours, n^2 - n for a cell with itself.
-    CU(cudaDeviceGetAttribute(&st->sm_count, cudaDevAttrMultiProcessorCount, st->device));
     {
-        std::vector<std::pair<double, int>> w(st->ntasks);
-        for (int t = 0; t < st->ntasks; t++) {
-            const TaskRec& r = tasks[t];
-            double ni = s->cells[r.ci].count, nj = s->cells[r.cj].count;
-            w[t] = {task_weight(r.sid, ni, nj), t};
-        }
-        std::stable_sort(w.begin(), w.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
-            return a.first > b.first;
-        });
-        std::vector<int> order(st->ntasks > 0 ? st->ntasks : 1, 0);
-        for (int t = 0; t < st->ntasks; t++) order[t] = w[t].second;
-        st->heur_order.assign(order.begin(), order.begin() + st->ntasks);
-        const int nb = (st->ntasks + kQueueBlock - 1) / kQueueBlock + 1;
+        std::vector<int> order(tasks.size(), 0);
+        for (int t = 0; t < ntasks; t++) order[t] = t;
+        std::stable_sort(order.begin(), order.begin() + ntasks, [&](int a, int b) { return cost[a] > cost[b]; });
+        st->heur_order.assign(order.begin(), order.begin() + ntasks);
+        const int nb = (ntasks + kQueueBlock - 1) / kQueueBlock + 1;
         if (dev_alloc(&st->d_queue, order.size()) || dev_alloc(&st->d_qcount, 1) || dev_alloc(&st->d_bsum, nb))
             return engine_err_cuda;
-        int empty = 0;
-        for (int c = 0; c < s->nr_cells; c++) empty += s->cells[c].count == 0;
         st->compact = empty > 0;
         if (dev_alloc(&st->d_order, order.size()) || dev_alloc(&st->d_counter, 1) ||
             dev_alloc(&st->d_task_clock, 2 * order.size()) || dev_alloc(&st->d_task_sm, order.size()))
             return engine_err_cuda;
         CU(cudaMemcpy(st->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
-
-    // Cells: sort-direction masks and the offset/count staging.
-    std::vector<unsigned> cmask(st->ncells);
-    for (int c = 0; c < st->ncells; c++) cmask[c] = s->cells[c].sortmask;
-    if (dev_alloc(&st->d_cmask, st->ncells) || dev_alloc(&st->d_cstart, st->ncells + 1) ||
-        dev_alloc(&st->d_ccount, st->ncells) || dev_alloc(&st->d_cell_epot, st->ncells) ||
-        dev_alloc(&st->d_acc, kAccCount))
+    if (dev_alloc(&st->d_cmask, cmask.size()) || dev_alloc(&st->d_cscale, cscale.size()) ||
+        dev_alloc(&st->d_cstart, st->ncells + 1) || dev_alloc(&st->d_ccount, cmask.size()) ||
+        dev_alloc(&st->d_cell_epot, 2 * cmask.size()) || dev_alloc(&st->d_acc, kAccCount))
         return engine_err_cuda;
     CU(cudaMemcpy(st->d_cmask, cmask.data(), cmask.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->d_cscale, cscale.data(), cscale.size() * sizeof(float2), cudaMemcpyHostToDevice));
     CU(cudaMallocHost(&st->h_cstart, sizeof(int) * (2 * st->ncells + 2)));
-    CU(cudaMallocHost(&st->h_cell_epot, sizeof(unsigned long long) * (st->ncells + 1)));
+    CU(cudaMallocHost(&st->h_cell_epot, sizeof(unsigned long long) * (2 * st->ncells + 2)));
     CU(cudaMallocHost(&st->h_acc, sizeof(unsigned long long) * kAccCount));
+    std::memset(st->h_cstart, 0, sizeof(int) * (2 * st->ncells + 2));
 
-    // Exclusions by particle id: a bit mask for partners at id offsets -16..16, a CSR
-    // list for the rest.  Each exclusion is recorded on both particles.
-    const int nid = s->size_parts > 0 ? s->size_parts : 1;
+    // Exclusions by global particle id: a bit mask for partners at id offsets -16..16, a
+    // CSR list for the rest.  Each exclusion is recorded on both particles.
+    const int nid = st->id_off[ne];
     st->nid = nid;
-    st->has_excl = e->nr_exclusions > 0;
+    std::vector<std::pair<int, int>> ex;          // global ids, in range, distinct
+    for (size_t k = 0; k < ne; k++) {
+        struct engine* e = st->engines[k];
+        const int lo = st->id_off[k], n = st->id_off[k + 1] - lo;
+        for (int x = 0; x < e->nr_exclusions; x++) {
+            const int a = e->exclusions[x].i, b = e->exclusions[x].j;
+            if (a < 0 || b < 0 || a >= n || b >= n || a == b) continue;
+            ex.emplace_back(lo + a, lo + b);
+        }
+    }
+    st->has_excl = !ex.empty();
     std::vector<unsigned> emask(nid, 0u);
     std::vector<int> cnt(nid + 1, 0);
-    for (int k = 0; k < e->nr_exclusions; k++) {
-        int a = e->exclusions[k].i, b = e->exclusions[k].j;
-        if (a < 0 || b < 0 || a >= nid || b >= nid || a == b) continue;
-        int d = b - a;
+    for (const auto& ab : ex) {
+        const int a = ab.first, b = ab.second, d = b - a;
         if (d >= -16 && d <= 16) {
             emask[a] |= 1u << ((d < 0) ? d + 16 : d + 15);
             emask[b] |= 1u << ((-d < 0) ? -d + 16 : -d + 15);
@@ -561,12 +694,10 @@ extern "C" int engine_cuda_load(struct engine* e) {
             cnt[b + 1]++;
         }
     }
-    for (int k = 0; k < nid; k++) cnt[k + 1] += cnt[k];
+    for (int q = 0; q < nid; q++) cnt[q + 1] += cnt[q];
     std::vector<int> exlist(cnt[nid] > 0 ? cnt[nid] : 1), fill(cnt.begin(), cnt.end() - 1);
-    for (int k = 0; k < e->nr_exclusions; k++) {
-        int a = e->exclusions[k].i, b = e->exclusions[k].j;
-        if (a < 0 || b < 0 || a >= nid || b >= nid || a == b) continue;
-        int d = b - a;
+    for (const auto& ab : ex) {
+        const int a = ab.first, b = ab.second, d = b - a;
         if (d >= -16 && d <= 16) continue;
         exlist[fill[a]++] = b;
         exlist[fill[b]++] = a;
@@ -579,16 +710,24 @@ extern "C" int engine_cuda_load(struct engine* e) {
     return 0;
 }
 
-extern "C" int engine_cuda_load_parts(struct engine* e) {
-    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    NbState* st = state(e);
+// Copies of the timing fields of the last evaluation into every engine's stats.
+void share_times(NbState* st) {
+    for (struct engine* e : st->engines) {
+        e->stats.ms_kernels = st->bstats.ms_kernels;
+        e->stats.ms_pack = st->bstats.ms_pack;
+        e->stats.ms_device = st->bstats.ms_device;
+        e->stats.ms_unpack = st->bstats.ms_unpack;
+    }
+}
+
+int st_load_parts(NbState* st) {
     CU(cudaSetDevice(st->device));
     const double t0 = now_ms();
-    int slots = pack_cells(e, st);
+    const int slots = pack_cells(st);
     if (slots < 0) return slots;
     const double t1 = now_ms();
-    e->stats.ms_pack = (float)(t1 - t0);
-    e->stats.ms_device = 0.f;
+    st->bstats.ms_pack = (float)(t1 - t0);
+    st->bstats.ms_device = 0.f;
     CU(cudaMemcpyAsync(st->d_xq, st->h_xq, sizeof(float4) * slots, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->d_pid, st->h_pid, sizeof(int) * slots, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->d_cstart, st->h_cstart, sizeof(int) * (st->ncells + 1), cudaMemcpyHostToDevice,
@@ -596,15 +735,14 @@ extern "C" int engine_cuda_load_parts(struct engine* e) {
     CU(cudaMemcpyAsync(st->d_ccount, st->h_cstart + st->ncells + 1, sizeof(int) * st->ncells,
                        cudaMemcpyHostToDevice, st->stream));
     st->resident_valid = true;
+    share_times(st);
     return 0;
 }
 
-// Copies forces and energies of the last evaluation back into the cells.
-extern "C" int engine_cuda_unload_parts(struct engine* e) {
-    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    NbState* st = state(e);
-    struct space* s = &e->s;
-    const int slots = st->h_cstart[s->nr_cells];
+// Copies forces and energies of the last evaluation back into the engines' cells.
+int st_unload_parts(NbState* st) {
+    CU(cudaSetDevice(st->device));
+    const int slots = st->h_cstart[st->ncells];
     const double t0 = now_ms();
     if (slots > 0) {
         fixed_to_float<<<(3 * slots + 255) / 256, 256, 0, st->stream>>>(st->d_force, st->d_forcef, 3 * slots);
@@ -612,68 +750,230 @@ extern "C" int engine_cuda_unload_parts(struct engine* e) {
     }
     float* hf = reinterpret_cast<float*>(st->h_force);
     CU(cudaMemcpyAsync(hf, st->d_forcef, sizeof(float) * 3 * (size_t)slots, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * st->ncells,
+    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
     CU(cudaStreamSynchronize(st->stream));
     const double t1 = now_ms();
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, st->ev0, st->ev1) == cudaSuccess) e->stats.ms_kernels = ms;
-    int rc = finish_stats(e, st);
-    for (int c = 0; c < s->nr_cells; c++) {
-        struct cell* cl = &s->cells[c];
-        const float* f = hf + 3 * (size_t)st->h_cstart[c];
-        for (int k = 0; k < cl->count; k++) {
-            cl->parts[k].f[0] += f[3 * k];
-            cl->parts[k].f[1] += f[3 * k + 1];
-            cl->parts[k].f[2] += f[3 * k + 2];
+    // The events are unset when no evaluation ran since the last load; that error is
+    // cleared here so that it does not surface at the next launch check.
+    if (cudaEventElapsedTime(&ms, st->ev0, st->ev1) == cudaSuccess)
+        st->bstats.ms_kernels = ms;
+    else
+        cudaGetLastError();
+    const int rc = finish_stats(st);
+    for (size_t k = 0; k < st->engines.size(); k++) {
+        struct space* s = &st->engines[k]->s;
+        for (int c = 0; c < s->nr_cells; c++) {
+            struct cell* cl = &s->cells[c];
+            const float* f = hf + 3 * (size_t)st->h_cstart[st->cell_off[k] + c];
+            for (int q = 0; q < cl->count; q++) {
+                cl->parts[q].f[0] += f[3 * q];
+                cl->parts[q].f[1] += f[3 * q + 1];
+                cl->parts[q].f[2] += f[3 * q + 2];
+            }
         }
     }
-    e->stats.ms_device += (float)(t1 - t0);
-    e->stats.ms_unpack = (float)(now_ms() - t1);
+    st->bstats.ms_device += (float)(t1 - t0);
+    st->bstats.ms_unpack = (float)(now_ms() - t1);
+    share_times(st);
     return rc;
 }
 
-extern "C" int engine_nonbond_cuda(struct engine* e) {
-    if (e == nullptr) return engine_err_null;
-    if (e->cuda == nullptr && engine_cuda_load(e) < 0) return engine_err_cuda;
-    NbState* st = state(e);
-    CU(cudaSetDevice(st->device));
-    int rc = engine_cuda_load_parts(e);
-    if (rc < 0) return rc;
-    CU(cudaEventRecord(st->ev0, st->stream));
-    rc = launch_kernels(e, st);
-    if (rc < 0) return rc;
-    CU(cudaEventRecord(st->ev1, st->stream));
-    return engine_cuda_unload_parts(e);
-}
-
-// Sort + sweep on the particles already resident on the device (no host copies, no
-// synchronisation); results stay on the device until engine_cuda_unload_parts.
-extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
-    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    NbState* st = state(e);
+// Sort + sweep on the particles already resident on the device.
+int st_resident(NbState* st) {
     if (!st->resident_valid) {
         errs_register(engine_err_cuda, "No particles resident on the device.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_cuda;
     }
     CU(cudaSetDevice(st->device));
     CU(cudaEventRecord(st->ev0, st->stream));
-    int rc = launch_kernels(e, st);
+    const int rc = launch_kernels(st);
     if (rc < 0) return rc;
     CU(cudaEventRecord(st->ev1, st->stream));
     return 0;
 }
 
+int st_nonbond(NbState* st) {
+    int rc = st_load_parts(st);
+    if (rc < 0) return rc;
+    rc = st_resident(st);
+    if (rc < 0) return rc;
+    return st_unload_parts(st);
+}
+
+int st_setstream(NbState* st, void* stream) {
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : st->own_stream;
+    if (s != st->stream) drop_graph(st);
+    st->stream = s;
+    return 0;
+}
+
+int st_kernel_times(NbState* st, float* total_ms, float* sweep_ms) {
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    float a = 0.f, b = 0.f;
+    CU(cudaEventElapsedTime(&a, st->ev0, st->ev1));
+    CU(cudaEventElapsedTime(&b, st->evs0, st->evs1));
+    if (total_ms) *total_ms = a;
+    if (sweep_ms) *sweep_ms = b;
+    return 0;
+}
+
+int st_settune(NbState* st, int warps, int plain) {
+    if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8) return engine_err_range;
+    st->warps = warps ? warps : 4;
+    st->plain = plain ? 1 : 0;
+    return 0;
+}
+
+// Times every persistent launch shape (worker warps per CTA x sweep window) on the
+// resident particles, `reps` evaluations each after one warm-up, and keeps the fastest
+// (median device time of sort + sweep).  Every shape computes the same forces.
+int st_autotune(NbState* st, int reps, int* warps_out, int* window_out, float* ms_out) {
+    if (!st->resident_valid) {
+        const int rc = st_load_parts(st);
+        if (rc < 0) return rc;
+    }
+    CU(cudaSetDevice(st->device));
+    if (reps < 1) reps = 1;
+    const bool graph = st->use_graph;
+    st->use_graph = false;
+    st->plain = 0;
+    static const int shapes[][2] = {{2, 4}, {2, 8}, {4, 4}, {4, 8}, {8, 4}, {8, 8}};
+    int best = -1;
+    float best_ms = 0.f;
+    for (int k = 0; k < 6; k++) {
+        st->warps = shapes[k][0];
+        st->window = shapes[k][1];
+        std::vector<float> t;
+        for (int r = 0; r <= reps; r++) {
+            int rc = st_resident(st);
+            if (rc < 0) {
+                st->use_graph = graph;
+                return rc;
+            }
+            CU(cudaEventSynchronize(st->ev1));
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, st->ev0, st->ev1));
+            if (r > 0) t.push_back(ms);
+        }
+        std::sort(t.begin(), t.end());
+        const float med = t[t.size() / 2];
+        if (best < 0 || med < best_ms) {
+            best = k;
+            best_ms = med;
+        }
+    }
+    st->warps = shapes[best][0];
+    st->window = shapes[best][1];
+    st->use_graph = graph;
+    const int rc = st_resident(st);           // leave the chosen shape's results resident
+    if (rc < 0) return rc;
+    if (warps_out) *warps_out = st->warps;
+    if (window_out) *window_out = st->window;
+    if (ms_out) *ms_out = best_ms;
+    return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- single engine
+
+extern "C" int nb_device_free(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return 0;
+    state_free(state(e));
+    e->cuda = nullptr;
+    return 0;
+}
+
+extern "C" int engine_cuda_setdevice(struct engine* e, int id) {
+    if (e == nullptr) return engine_err_null;
+    int n = 0;
+    CU(cudaGetDeviceCount(&n));
+    if (id < 0 || id >= n) {
+        errs_register(engine_err_range, "No such CUDA device.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_range;
+    }
+    e->device = id;
+    return 0;
+}
+
+extern "C" int engine_cuda_setdevices(struct engine* e, int nr_devices, int* ids) {
+    if (e == nullptr || ids == nullptr) return engine_err_null;
+    if (nr_devices != 1) {
+        errs_register(engine_err_nyi, "Only one device per engine.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_nyi;
+    }
+    return engine_cuda_setdevice(e, ids[0]);
+}
+
+extern "C" int engine_cuda_settune(struct engine* e, int warps, int plain) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_settune(state(e), warps, plain);
+}
+
+extern "C" int engine_cuda_setwindow(struct engine* e, int window) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (window != 4 && window != 8) return engine_err_range;
+    state(e)->window = window;
+    return 0;
+}
+
+extern "C" int engine_cuda_graph(struct engine* e, int enable) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    st->use_graph = enable != 0;
+    if (!st->use_graph) drop_graph(st);
+    st->prepared_key = -1;
+    return 0;
+}
+
+extern "C" int engine_cuda_autotune(struct engine* e, int reps, int* warps, int* window, float* ms) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_autotune(state(e), reps, warps, window, ms);
+}
+
+extern "C" int engine_cuda_load(struct engine* e) {
+    if (e == nullptr) return engine_err_null;
+    if (e->cuda) nb_device_free(e);
+    NbState* st = new NbState();
+    e->cuda = st;
+    st->engines.assign(1, e);
+    return load_state(st);
+}
+
+extern "C" int engine_cuda_load_parts(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_load_parts(state(e));
+}
+
+extern "C" int engine_cuda_unload_parts(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_unload_parts(state(e));
+}
+
+extern "C" int engine_nonbond_cuda(struct engine* e) {
+    if (e == nullptr) return engine_err_null;
+    if (e->cuda == nullptr && engine_cuda_load(e) < 0) return engine_err_cuda;
+    return st_nonbond(state(e));
+}
+
+// Sort + sweep on the particles already resident on the device (no host copies, no
+// synchronisation); results stay on the device until engine_cuda_unload_parts.
+extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident(state(e));
+}
+
 // Runs further launches on a caller-provided stream (e.g. the framework's current stream).
 extern "C" int engine_cuda_setstream(struct engine* e, void* stream) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    NbState* st = state(e);
-    CU(cudaSetDevice(st->device));
-    CU(cudaStreamSynchronize(st->stream));
-    st->stream = stream ? static_cast<cudaStream_t>(stream) : st->own_stream;
-    return 0;
+    return st_setstream(state(e), stream);
 }
 
 extern "C" int engine_cuda_getsort(struct engine* e, int cid, unsigned int* keys, int size) {
@@ -696,15 +996,119 @@ extern "C" int engine_cuda_getsort(struct engine* e, int cid, unsigned int* keys
 // the launching stream).
 extern "C" int engine_cuda_kernel_times(struct engine* e, float* total_ms, float* sweep_ms) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    NbState* st = state(e);
-    CU(cudaSetDevice(st->device));
-    CU(cudaStreamSynchronize(st->stream));
-    float a = 0.f, b = 0.f;
-    CU(cudaEventElapsedTime(&a, st->ev0, st->ev1));
-    CU(cudaEventElapsedTime(&b, st->evs0, st->evs1));
-    if (total_ms) *total_ms = a;
-    if (sweep_ms) *sweep_ms = b;
+    return st_kernel_times(state(e), total_ms, sweep_ms);
+}
+
+// ---------------------------------------------------------------- batches of engines
+//
+// A batch evaluates the nonbonded forces of many independent engines (replicas: same
+// force field, own particles and box) with one sort launch and one persistent sweep over
+// the concatenated task list, so that systems of a few thousand particles -- too small to
+// fill a B200 alone -- share the GPU.  The engines keep their own host data; the batch owns
+// the device state.  Energies and virials are kept per engine; pair counts for the batch.
+
+namespace {
+NbState* bstate(struct engine_batch* b) { return reinterpret_cast<NbState*>(b); }
+}  // namespace
+
+extern "C" int engine_batch_create(struct engine** engines, int n, struct engine_batch** out) {
+    if (engines == nullptr || out == nullptr || n < 1) return engine_err_null;
+    for (int k = 0; k < n; k++)
+        if (engines[k] == nullptr) return engine_err_null;
+    NbState* st = new NbState();
+    st->engines.assign(engines, engines + n);
+    const int rc = load_state(st);
+    if (rc < 0) {
+        state_free(st);
+        return rc;
+    }
+    *out = reinterpret_cast<struct engine_batch*>(st);
     return 0;
+}
+
+extern "C" int engine_batch_free(struct engine_batch* b) {
+    if (b == nullptr) return 0;
+    state_free(bstate(b));
+    return 0;
+}
+
+extern "C" int engine_batch_load_parts(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_load_parts(bstate(b));
+}
+
+extern "C" int engine_batch_resident(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_resident(bstate(b));
+}
+
+extern "C" int engine_batch_unload_parts(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_unload_parts(bstate(b));
+}
+
+extern "C" int engine_batch_nonbond(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_nonbond(bstate(b));
+}
+
+// One time step of every engine: re-binning, force evaluation in one batch, symplectic
+// Euler update (engine_step for each engine, with the forces computed together).
+extern "C" int engine_batch_step(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    NbState* st = bstate(b);
+    for (struct engine* e : st->engines) {
+        e->time += 1;
+        if (space_shuffle(&e->s) < 0) return engine_err = engine_err_space;
+        engine_zero_forces(e);
+    }
+    const int rc = st_nonbond(st);
+    if (rc < 0) return rc;
+    for (struct engine* e : st->engines) {
+        e->s.epot += e->s.epot_nonbond;
+        if (engine_advance(e) < 0) return engine_err;
+    }
+    return 0;
+}
+
+extern "C" int engine_batch_stats(struct engine_batch* b, struct nb_stats* out) {
+    if (b == nullptr || out == nullptr) return engine_err_null;
+    *out = bstate(b)->bstats;
+    return 0;
+}
+
+extern "C" int engine_batch_setstream(struct engine_batch* b, void* stream) {
+    if (b == nullptr) return engine_err_null;
+    return st_setstream(bstate(b), stream);
+}
+
+extern "C" int engine_batch_kernel_times(struct engine_batch* b, float* total_ms, float* sweep_ms) {
+    if (b == nullptr) return engine_err_null;
+    return st_kernel_times(bstate(b), total_ms, sweep_ms);
+}
+
+extern "C" int engine_batch_settune(struct engine_batch* b, int warps, int plain) {
+    if (b == nullptr) return engine_err_null;
+    return st_settune(bstate(b), warps, plain);
+}
+
+extern "C" int engine_batch_graph(struct engine_batch* b, int enable) {
+    if (b == nullptr) return engine_err_null;
+    NbState* st = bstate(b);
+    st->use_graph = enable != 0;
+    if (!st->use_graph) drop_graph(st);
+    st->prepared_key = -1;
+    return 0;
+}
+
+extern "C" int engine_batch_autotune(struct engine_batch* b, int reps, int* warps, int* window, float* ms) {
+    if (b == nullptr) return engine_err_null;
+    return st_autotune(bstate(b), reps, warps, window, ms);
+}
+
+extern "C" int engine_batch_ntasks(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return bstate(b)->ntasks;
 }
 
 namespace {
@@ -858,7 +1262,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const int cap4 = (maxcount + 3) & ~3;
     if (cap4 == 0) return 0;
     sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), s>>>(static_cast<const float4*>(xq), cstart, ccount,
-                                                           st->d_cmask, keys, st->dscale, st->bias, acc);
+                                                                      st->d_cmask, keys, st->d_cscale, acc);
     CU(cudaGetLastError());
 
     TunedParams T;
@@ -871,6 +1275,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     P.force = force;
     P.acc = acc;
     P.cell_epot = cell_epot;
+    P.cell_vir = nullptr;
     P.tasks = st->d_tasks;
     P.tshift = st->d_tshift;
     P.ntasks = st->ntasks;
@@ -887,7 +1292,6 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const float cutf = (float)e->s.cutoff;
     P.cutoff2 = cutf * cutf;
     P.cutoff2s = (float)e->s.cutoff2;
-    P.dmaxdist = st->dmaxdist;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
     T.order = st->d_order;
     T.qcount = nullptr;
@@ -902,9 +1306,12 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
         return engine_err = engine_err_maxparts;
     }
     cudaStream_t saved = st->stream;
+    const bool cap_saved = st->capturing;
     st->stream = s;
-    const int rc = launch_tuned_w<4>(st, T, cap, smem);
+    st->capturing = false;
+    const int rc = launch_tuned_w<4, 4>(st, T, cap, smem);
     st->stream = saved;
+    st->capturing = cap_saved;
     return rc;
 }
 
@@ -925,7 +1332,7 @@ __global__ void cell_type0(const float4* __restrict__ xq, const int* __restrict_
 // neighbour class one-hot (face, edge, corner, self).
 __global__ void task_features(const TaskRec* __restrict__ tasks, int ntasks, const int* __restrict__ ccount,
                               const int* __restrict__ cstart, const unsigned* __restrict__ keys,
-                              const int* __restrict__ ctype0, int dmaxdist, float inv_scale,
+                              const int* __restrict__ ctype0, float inv_scale,
                               float* __restrict__ X) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntasks) return;
@@ -940,7 +1347,7 @@ __global__ void task_features(const TaskRec* __restrict__ tasks, int ntasks, con
             const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
             const unsigned* ki = keys + 13 * (size_t)cstart[r.ci] + (size_t)r.sid * padi;
             const unsigned* kj = keys + 13 * (size_t)cstart[r.cj] + (size_t)r.sid * padj;
-            const int thr = (int)(kj[nj - 1] & 0xffffu) + r.dnshift - dmaxdist;   // i needs dist >= thr
+            const int thr = (int)(kj[nj - 1] & 0xffffu) + task_dnshift(r) - task_dmax(r);   // i needs dist >= thr
             int lo = 0, hi = ni;                                                   // descending list
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
@@ -1048,7 +1455,7 @@ extern "C" int engine_sched_record(struct engine* e, int nsteps) {
     st->record_clock = 1;
     for (int k = 0; k < nsteps; k++) {
         CU(cudaMemsetAsync(st->d_task_clock, 0, sizeof(long long) * 2 * st->ntasks, st->stream));
-        int rc = launch_kernels(e, st);
+        int rc = launch_kernels(st);
         if (rc < 0) return rc;
         accumulate_durations<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_task_clock, st->ntasks,
                                                                              ss->d_dur, ss->d_nrec);
@@ -1070,7 +1477,7 @@ extern "C" int engine_sched_features(struct engine* e, float* features_out, int 
                                                                  ss->d_ctype0);
     task_features<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_tasks, st->ntasks, st->d_ccount,
                                                                     st->d_cstart, st->d_keys, ss->d_ctype0,
-                                                                    st->dmaxdist, 1.0f / 32.0f, ss->d_feat);
+                                                                    1.0f / 32.0f, ss->d_feat);
     CU(cudaGetLastError());
     if (features_out != nullptr) {
         if (n != st->ntasks) return engine_err_range;

@@ -91,6 +91,23 @@ def lib() -> C.CDLL:
         "engine_cuda_ntasks": (C.c_int, [vp]),
         "engine_cuda_fp32_peak": (C.c_int, [C.c_int, P(C.c_float)]),
         "engine_zero_forces": (C.c_int, [vp]),
+        "engine_cuda_setwindow": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_graph": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_autotune": (C.c_int, [vp, C.c_int, ip, ip, P(C.c_float)]),
+        "engine_batch_create": (C.c_int, [P(vp), C.c_int, P(vp)]),
+        "engine_batch_free": (C.c_int, [vp]),
+        "engine_batch_nonbond": (C.c_int, [vp]),
+        "engine_batch_step": (C.c_int, [vp]),
+        "engine_batch_load_parts": (C.c_int, [vp]),
+        "engine_batch_resident": (C.c_int, [vp]),
+        "engine_batch_unload_parts": (C.c_int, [vp]),
+        "engine_batch_stats": (C.c_int, [vp, P(NbStats)]),
+        "engine_batch_setstream": (C.c_int, [vp, vp]),
+        "engine_batch_kernel_times": (C.c_int, [vp, P(C.c_float), P(C.c_float)]),
+        "engine_batch_settune": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_batch_graph": (C.c_int, [vp, C.c_int]),
+        "engine_batch_autotune": (C.c_int, [vp, C.c_int, ip, ip, P(C.c_float)]),
+        "engine_batch_ntasks": (C.c_int, [vp]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -272,6 +289,21 @@ class Engine:
         """warps per block (0 = default); plain=True selects the one-block-per-task form."""
         _check(self.lib.engine_cuda_settune(self.ptr, warps, 1 if plain else 0), "engine_cuda_settune")
 
+    def set_window(self, window: int):
+        """Sweep steps per register reduce-scatter of the persistent sweep (4 or 8)."""
+        _check(self.lib.engine_cuda_setwindow(self.ptr, window), "engine_cuda_setwindow")
+
+    def graph(self, enable: bool = True):
+        """CUDA-graph replay of each evaluation's launches."""
+        _check(self.lib.engine_cuda_graph(self.ptr, int(enable)), "engine_cuda_graph")
+
+    def autotune(self, reps: int = 5):
+        """Keeps the fastest persistent launch shape; returns (warps, window, ms)."""
+        w, win, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.engine_cuda_autotune(self.ptr, reps, C.byref(w), C.byref(win), C.byref(ms)),
+               "engine_cuda_autotune")
+        return w.value, win.value, ms.value
+
     def ntasks(self) -> int:
         return _check(self.lib.engine_cuda_ntasks(self.ptr), "engine_cuda_ntasks")
 
@@ -337,3 +369,85 @@ def fp32_peak_tflops(device: int = 0) -> float:
     v = C.c_float()
     _check(lib().engine_cuda_fp32_peak(device, C.byref(v)), "engine_cuda_fp32_peak")
     return v.value
+
+
+class Batch:
+    """Many engines (replicas) evaluated together: one sort and one persistent sweep
+    launch over all of them (engine_batch_*).  The engines need no device state of their
+    own (Engine.from_system(..., start=False)) and must stay open while the batch is."""
+
+    def __init__(self, engines, device: Optional[int] = None):
+        self.lib = lib()
+        self.engines = list(engines)
+        self.closed = True
+        if device is not None:
+            for e in self.engines:
+                _check(self.lib.engine_cuda_setdevice(e.ptr, device), "engine_cuda_setdevice")
+        self._arr = (C.c_void_p * len(self.engines))(*[e.ptr.value for e in self.engines])
+        h = C.c_void_p()
+        _check(self.lib.engine_batch_create(self._arr, len(self.engines), C.byref(h)), "engine_batch_create")
+        self.ptr = h
+        self.closed = False
+
+    def _zero(self):
+        for e in self.engines:
+            _check(self.lib.engine_zero_forces(e.ptr), "engine_zero_forces")
+
+    def nonbond(self):
+        """One force evaluation of every engine (host buffers in and out)."""
+        self._zero()
+        _check(self.lib.engine_batch_nonbond(self.ptr), "engine_batch_nonbond")
+        return self
+
+    def step(self):
+        _check(self.lib.engine_batch_step(self.ptr), "engine_batch_step")
+        return self
+
+    def load_parts(self):
+        _check(self.lib.engine_batch_load_parts(self.ptr), "engine_batch_load_parts")
+
+    def resident(self):
+        _check(self.lib.engine_batch_resident(self.ptr), "engine_batch_resident")
+
+    def unload_parts(self):
+        self._zero()
+        _check(self.lib.engine_batch_unload_parts(self.ptr), "engine_batch_unload_parts")
+
+    def stats(self) -> NbStats:
+        s = NbStats()
+        _check(self.lib.engine_batch_stats(self.ptr, C.byref(s)), "engine_batch_stats")
+        return s
+
+    def set_stream(self, stream_ptr: int):
+        _check(self.lib.engine_batch_setstream(self.ptr, C.c_void_p(stream_ptr)), "engine_batch_setstream")
+
+    def kernel_times(self):
+        a, b = C.c_float(), C.c_float()
+        _check(self.lib.engine_batch_kernel_times(self.ptr, C.byref(a), C.byref(b)), "engine_batch_kernel_times")
+        return a.value, b.value
+
+    def tune(self, warps: int = 0, plain: bool = False):
+        _check(self.lib.engine_batch_settune(self.ptr, warps, 1 if plain else 0), "engine_batch_settune")
+
+    def graph(self, enable: bool = True):
+        _check(self.lib.engine_batch_graph(self.ptr, int(enable)), "engine_batch_graph")
+
+    def autotune(self, reps: int = 5):
+        w, win, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.engine_batch_autotune(self.ptr, reps, C.byref(w), C.byref(win), C.byref(ms)),
+               "engine_batch_autotune")
+        return w.value, win.value, ms.value
+
+    def ntasks(self) -> int:
+        return _check(self.lib.engine_batch_ntasks(self.ptr), "engine_batch_ntasks")
+
+    def close(self):
+        if not self.closed:
+            self.lib.engine_batch_free(self.ptr)
+            self.closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

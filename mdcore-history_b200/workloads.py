@@ -197,6 +197,34 @@ def lj_slab(nx: int = 110, nz: int = 77, n_total: int = 1 << 20, seed: int = 0, 
                   excl=np.zeros((0, 2), np.int32), dt=0.005)
 
 
+def argon_replicas(nrep: int = 512, seed: int = 0, nmin: int = 500, nmax: int = 8000, rho=(18.0, 24.0),
+                   jitter: float = 0.01, tol: float = 1e-4, cutoff: float = 1.0) -> List[System]:
+    """An ensemble of independent LJ argon replicas of different sizes and densities, the
+    workload of a replica batch: N log-uniform in [nmin, nmax], density uniform in `rho`
+    atoms/nm^3, cubic box of edge (N/density)^(1/3) (drawn again if below three cutoffs),
+    atoms on a random subset of a simple-cubic lattice, jittered.  Every replica carries
+    the same LJ potential (argon, table from 0.25 nm to the cutoff)."""
+    rng = np.random.default_rng(seed)
+    A, B = lj_AB(0.996, 0.3405)
+    out = []
+    while len(out) < nrep:
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        dens = rng.uniform(*rho)
+        L = (n / dens) ** (1.0 / 3.0)
+        if L < 3.0 * cutoff:
+            continue
+        m = int(math.ceil(n ** (1.0 / 3.0)))
+        sites = rng.choice(m ** 3, size=n, replace=False)
+        g = np.stack(np.unravel_index(sites, (m, m, m)), 1).astype(np.float64)
+        x = (g + 0.5) * (L / m) + rng.normal(0.0, jitter, size=(n, 3))
+        dim = np.full(3, L)
+        out.append(System(
+            name=f"argon-replica-{len(out)}-{n}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
+            masses=[39.948], charges=[0.0], pots=[PotSpec(KIND_LJ126, 0, 0, 0.25, cutoff, tol, (A, B, 0.0, 0.0))],
+            x=_wrap(x, dim), type=np.zeros(n, np.int32), excl=np.zeros((0, 2), np.int32), dt=0.005))
+    return out
+
+
 def write_sysfile(sysm: System, path: str) -> None:
     """Serialise in the format of oracle/sysfile.h."""
     with open(path, "wb") as f:

@@ -84,7 +84,9 @@ static void eval_fp64(const float *coef, const float *alpha, int nmax, float r2f
     *f = eff * (double)c[1] / r;
 }
 
-/* Nonbonded forces (by particle id, FP64), energy, virial and counts.
+/* Nonbonded forces (by particle id, FP64), energy, virial, sum over pairs of |r_ij . F_ij|
+ * (the scale of the virial's rounding error: the net virial may cancel to far less) and
+ * counts.
  *   xrel[3N] float cell-local positions, cell[N] cell index, type[N]
  *   coef: tables concatenated; alpha[4*npots]; coff[npots] float offset of each table;
  *   potn[npots]; potidx[mt*mt] table index or -1.
@@ -93,8 +95,8 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                    const double *origin, const double *dim, const int *cdim, double cutoff,
                    unsigned period, int mt, const int *potidx, const float *coef, const float *alpha,
                    const int *coff, const int *potn, int nexcl, const int *excl,
-                   double *f_out, double *epot_out, double *virial_out, long long *npairs_out,
-                   long long *nexcl_out) {
+                   double *f_out, double *epot_out, double *virial_out, double *virial_abs_out,
+                   long long *npairs_out, long long *nexcl_out) {
     const int ncells = cdim[0] * cdim[1] * cdim[2];
     double h[3];
     int span[3];
@@ -129,7 +131,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
     const float cutf = (float)cutoff;
     const float cut2_pair = cutf * cutf;
     const float cut2_self = (float)(cutoff * cutoff);
-    double epot = 0.0, vir = 0.0;
+    double epot = 0.0, vir = 0.0, vir_abs = 0.0;
     long long npairs = 0, nex = 0;
     memset(f_out, 0, sizeof(double) * 3 * N);
 
@@ -194,6 +196,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                                     }
                                     epot += e;
                                     vir += fs * r2;
+                                    vir_abs += fabs(fs * r2);
                                     npairs++;
                                 }
                             }
@@ -203,6 +206,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
             }
     *epot_out = epot;
     *virial_out = -vir;
+    if (virial_abs_out) *virial_abs_out = vir_abs;
     *npairs_out = npairs;
     *nexcl_out = nex;
     free(cells);

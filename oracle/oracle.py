@@ -32,7 +32,8 @@ def lib():
         L.oracle_nonbond.argtypes = [C.c_int, P(C.c_float), P(C.c_int), P(C.c_int), P(C.c_double), P(C.c_double),
                                      P(C.c_int), C.c_double, C.c_uint, C.c_int, P(C.c_int), P(C.c_float),
                                      P(C.c_float), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int), P(C.c_double),
-                                     P(C.c_double), P(C.c_double), P(C.c_longlong), P(C.c_longlong)]
+                                     P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_longlong),
+                                     P(C.c_longlong)]
         L.oracle_sortkeys.restype = C.c_int
         L.oracle_sortkeys.argtypes = [C.c_int, P(C.c_float), P(C.c_double), C.c_int, P(C.c_uint)]
         _lib = L
@@ -75,12 +76,13 @@ def pack_tables(sysm, tables):
 
 
 def nonbond(sysm, tables, binned=None):
-    """FP64 forces (by id), energy, virial, pair and excluded-pair counts."""
+    """FP64 forces (by id), energy, virial, sum over pairs of |r.F| (virial_abs), pair and
+    excluded-pair counts."""
     b = binned or bin_system(sysm)
     t = pack_tables(sysm, tables)
     N = sysm.n
     f = np.zeros((N, 3), np.float64)
-    epot, vir = C.c_double(), C.c_double()
+    epot, vir, vabs = C.c_double(), C.c_double(), C.c_double()
     npairs, nex = C.c_longlong(), C.c_longlong()
     xrel = np.ascontiguousarray(b["xrel"], np.float32)
     cell = np.ascontiguousarray(b["cell"], np.int32)
@@ -94,10 +96,11 @@ def nonbond(sysm, tables, binned=None):
                               len(sysm.masses), _p(t["potidx"], C.c_int), _p(t["coef"], C.c_float),
                               _p(t["alpha"], C.c_float), _p(t["coff"], C.c_int), _p(t["potn"], C.c_int),
                               len(sysm.excl), _p(excl, C.c_int) if excl.size else None, _p(f, C.c_double),
-                              C.byref(epot), C.byref(vir), C.byref(npairs), C.byref(nex))
+                              C.byref(epot), C.byref(vir), C.byref(vabs), C.byref(npairs), C.byref(nex))
     if rc != 0:
         raise RuntimeError("oracle_nonbond failed")
-    return dict(f=f, epot=epot.value, virial=vir.value, pairs=npairs.value, excluded=nex.value)
+    return dict(f=f, epot=epot.value, virial=vir.value, virial_abs=vabs.value, pairs=npairs.value,
+                excluded=nex.value)
 
 
 def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:

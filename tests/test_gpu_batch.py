@@ -1,0 +1,159 @@
+"""GPU tests of replica batches (engine_batch_*): many independent engines evaluated by one
+sort launch and one persistent sweep over their concatenated task lists.
+
+Each replica's forces, energy and virial must equal those of the same engine evaluated
+alone, bit for bit (fixed-point accumulation, and every task computes the same float
+partials whichever engine list it belongs to), and match the oracle within the parity
+tolerances of the single-engine tests; the batch's pair and exclusion counts are the sums
+over the replicas.
+"""
+import numpy as np
+import pytest
+
+import mdcore_b200 as M
+import oracle as O
+import workloads as W
+from helpers import force_errors, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def engines_of(systems, start=False):
+    return [M.Engine.from_system(s, start=start) for s in systems]
+
+
+def check_replica_vs_oracle(sysm, tables, f, st):
+    o = O.nonbond(sysm, tables)
+    err = force_errors(f, o["f"])
+    assert abs(st.epot - o["epot"]) <= 1e-6 * abs(o["epot"]), (sysm.name, st.epot, o["epot"])
+    # The net virial of a replica near zero pressure is a small remainder of cancelling
+    # pair terms: its FP32 rounding error is bounded against the sum of |r.F| instead.
+    assert abs(st.virial - o["virial"]) <= 1e-6 * o["virial_abs"], (sysm.name, st.virial, o["virial"])
+    assert err["global_rel"] <= 2e-6, (sysm.name, err)
+    assert err["max_over_frms"] <= 2e-5, (sysm.name, err)
+    return o
+
+
+@pytest.mark.parametrize("plain", [False, True], ids=["tuned", "plain"])
+def test_batch_equals_single_engines(plain):
+    systems = W.argon_replicas(nrep=12, seed=3)
+    tables = [M.create_potential(p).contents.table() for p in systems[0].pots]
+    singles = []
+    for s in systems:
+        e = M.Engine.from_system(s)
+        if plain:
+            e.tune(0, True)
+        e.nonbond()
+        singles.append((e.forces(), e.stats()))
+        e.close()
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    if plain:
+        b.tune(0, True)
+    b.nonbond()
+    bs = b.stats()
+    assert bs.status == 0
+    pairs = excluded = 0
+    for s, e, (f1, s1) in zip(systems, engines, singles):
+        f2, s2 = e.forces(), e.stats()
+        assert np.array_equal(f1, f2), s.name
+        assert s1.epot == s2.epot and s1.virial == s2.virial, s.name
+        pairs += s1.pairs
+        excluded += s1.excluded
+        o = check_replica_vs_oracle(s, tables, f2, s2)
+        assert o["pairs"] == s1.pairs
+    assert bs.pairs == pairs and bs.excluded == excluded
+    assert abs(bs.epot - sum(e.stats().epot for e in engines)) <= 1e-9 * abs(bs.epot)
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_batch_of_water_and_exclusions():
+    """Replicas with exclusions: particle ids of replica k are offset in the batch, so each
+    replica's exclusions must still remove exactly its own pairs."""
+    sysm, ref = load_golden("water_3000.npz")
+    e1 = M.Engine.from_system(sysm)
+    e1.nonbond()
+    f1, s1 = e1.forces(), e1.stats()
+    e1.close()
+    engines = engines_of([sysm, sysm, sysm])
+    b = M.Batch(engines)
+    b.nonbond()
+    bs = b.stats()
+    assert bs.status == 0
+    for e in engines:
+        assert np.array_equal(e.forces(), f1)
+        assert e.stats().epot == s1.epot
+    assert bs.pairs == 3 * s1.pairs and bs.excluded == 3 * s1.excluded
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_full_replica_ensemble_vs_oracle():
+    """The 512-replica benchmark ensemble (1.45 M atoms): every replica against the oracle,
+    batch pair count equal to the oracle's total."""
+    systems = W.argon_replicas()
+    tables = [M.create_potential(p).contents.table() for p in systems[0].pots]
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    b.nonbond()
+    bs = b.stats()
+    assert bs.status == 0
+    pairs = 0
+    for s, e in zip(systems, engines):
+        o = check_replica_vs_oracle(s, tables, e.forces(), e.stats())
+        pairs += o["pairs"]
+    assert bs.pairs == pairs
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_batch_steps_equal_single_steps():
+    """engine_batch_step: re-binning, one batch force evaluation, integration -- the same
+    trajectories as engine_step on each engine alone."""
+    systems = W.argon_replicas(nrep=6, seed=5)
+    single = []
+    for s in systems:
+        e = M.Engine.from_system(s)
+        for _ in range(5):
+            e.step()
+        single.append(e.unload())
+        e.close()
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    for _ in range(5):
+        b.step()
+        assert b.stats().status == 0
+    for e, (x1, t1, p1, ep1) in zip(engines, single):
+        x2, t2, p2, ep2 = e.unload()
+        o1, o2 = np.argsort(p1), np.argsort(p2)
+        assert np.array_equal(p1[o1], p2[o2])
+        assert np.array_equal(x1[o1], x2[o2])
+        assert ep1 == ep2
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_batch_graph_and_autotune_keep_results():
+    systems = W.argon_replicas(nrep=16, seed=7)
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    b.nonbond()
+    ref = [e.forces() for e in engines]
+    e_ref = [e.stats().epot for e in engines]
+    warps, window, ms = b.autotune(reps=2)
+    assert warps in (2, 4, 8) and window in (4, 8) and ms > 0
+    b.graph(True)
+    for _ in range(4):                 # direct, capture, replay, replay
+        b.nonbond()
+        assert b.stats().status == 0
+        for e, f, ep in zip(engines, ref, e_ref):
+            assert np.array_equal(e.forces(), f)
+            assert e.stats().epot == ep
+    b.close()
+    for e in engines:
+        e.close()

@@ -80,3 +80,31 @@ def test_potential_range_errors():
     p = lib.potential_create_LJ126(0.1, 1.0, *W.lj_AB(0.996, 0.3405), 1e-13)
     assert not p
     lib.errs_clear()
+
+
+def test_batch_refuses_engines_with_other_potentials():
+    """A batch evaluates every replica with one set of tables: engines with other types or
+    potentials are refused before any device call."""
+    a, _ = load_golden("argon_1372.npz")
+    w, _ = load_golden("water_3000.npz")
+    ea, ew = M.Engine.from_system(a, start=False), M.Engine.from_system(w, start=False)
+    with pytest.raises(M.MdcoreError, match="differ"):
+        M.Batch([ea, ew])
+    b = W.argon_fcc(7)
+    b.pots = [W.PotSpec(p.kind, p.ti, p.tj, p.a, p.b, 1e-3, p.p) for p in b.pots]
+    eb = M.Engine.from_system(b, start=False)
+    with pytest.raises(M.MdcoreError, match="potentials"):
+        M.Batch([ea, eb])
+    M.lib().errs_clear()
+    for e in (ea, ew, eb):
+        e.close()
+
+
+def test_replica_ensemble_shapes():
+    systems = W.argon_replicas(nrep=64, seed=1)
+    assert len(systems) == 64
+    for s in systems:
+        assert 500 <= s.n <= 8000
+        assert (s.dim >= 3 * s.cutoff).all()
+        assert (s.x >= 0).all() and (s.x < s.dim).all()
+        assert len(np.unique(np.round(s.x / 1e-4))) > 0
