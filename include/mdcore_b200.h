@@ -238,12 +238,23 @@ int space_addpart(struct space *s, struct part *p, double *x);
 /* ---------------------------------------------------------------- exclusions, rigids
  * src/exclusion.h:34-41 and src/rigid.h:31-52. */
 struct exclusion { int i, j; };
-#define rigid_maxparts  10
-#define rigid_maxconstr (3 * rigid_maxparts)
+/* Rigid groups, src/rigid.h:27-59 (same fields in the same order): up to rigid_maxparts
+ * particles (by id) and rigid_maxconstr distance constraints between group-local indices
+ * i, j with squared length d2; a is the P-SHAKE constraint mixing matrix (identity when a
+ * constraint is added, refined on the device during the first engine_pshake_steps steps
+ * and whenever a group needs more than rigid_pshake_refine iterations). */
+#define rigid_maxparts        10
+#define rigid_maxconstr       (3 * rigid_maxparts)
+#define rigid_maxiter         100
+#define rigid_pshake_refine   10
+#define rigid_pshake_maxalpha 0.1f
+#define engine_pshake_steps   20
 struct rigid {
-    int nr_parts, nr_constr;
+    int nr_parts;
     int parts[rigid_maxparts];
+    int nr_constr;
     struct { int i, j; double d2; } constr[rigid_maxconstr];
+    float a[rigid_maxconstr * rigid_maxconstr];
 };
 
 /* ---------------------------------------------------------------- the engine
@@ -281,6 +292,9 @@ struct engine {
     int device;
     void *cuda;             /* device state, owned by the engine */
     struct nb_stats stats;
+    void *cuda_rigid;       /* device state of the rigid groups, owned by the engine */
+    int part2rigid_size;    /* entries of part2rigid */
+    int rigids_gen;         /* bumped by every engine_rigid_add */
 };
 
 /* src/engine.c:2439-2591 */
@@ -405,6 +419,25 @@ int engine_cuda_setorder(struct engine *e, const int *order, int n);
 int engine_cuda_taskclocks(struct engine *e, int enable, long long *clocks, int *sms, int n);
 /* Number of device tasks (self + pair). */
 int engine_cuda_ntasks(struct engine *e);
+
+/* ---- rigid constraints on the device ----
+ * src/engine_rigid.c:352-583: resolves every rigid group after the position update of a
+ * step, SHAKE (src/rigid.c:81-277) when engine_flag_shake is set, P-SHAKE
+ * (src/rigid.c:279-523) otherwise; engine_step calls it when the engine has rigid groups.
+ * The iterations run on the GPU in FP64, one thread per group; positions, velocities (and
+ * for P-SHAKE the constraint forces) of the cells are corrected as in the reference.  The
+ * P-SHAKE matrices live on the device once the first evaluation has uploaded them. */
+int engine_rigid_eval(struct engine *e);
+/* Largest iteration count of any group in the last engine_rigid_eval and the number of
+ * groups that did not converge within rigid_maxiter iterations. */
+int engine_rigid_stats(struct engine *e, int *max_iter, int *unconverged);
+/* Copies the device's P-SHAKE matrices back into e->rigids[].a. */
+int engine_rigid_getmatrices(struct engine *e);
+/* Copies rigid group g into *out; returns the number of groups (out may be NULL). */
+int engine_rigid_get(struct engine *e, int g, struct rigid *out);
+/* Particle state by id: cell-relative float positions, velocities and forces (3 floats
+ * each) and cell index; any pointer may be NULL. */
+int engine_getparts(struct engine *e, float *x, float *v, float *f, int *cell, int N);
 /* Sweep steps each lane holds before the warp reduce-scatter of the persistent sweep: 4
  * (default) or 8.  Forces are identical either way. */
 int engine_cuda_setwindow(struct engine *e, int window);

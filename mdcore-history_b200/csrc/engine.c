@@ -226,54 +226,129 @@ int engine_exclusion_shrink(struct engine *e) {
 
 /* ---------------------------------------------------------------- rigid constraints */
 
+/* Sets the P-SHAKE matrix of group r to the identity (src/engine_rigid.c:212-215). */
+static void rigid_reset_matrix(struct rigid *r) {
+    memset(r->a, 0, sizeof(float) * r->nr_constr * r->nr_constr);
+    for (int k = 0; k < r->nr_constr; k++) r->a[k + k * r->nr_constr] = 1.0f;
+}
+
+/* src/engine_rigid.c:78-229: a distance constraint between particles pid and pjd joins
+ * them into one rigid group -- a new group, an existing group of either particle, or the
+ * merger of two groups.  Constraint ends are group-local indices. */
 int engine_rigid_add(struct engine *e, int pid, int pjd, double d) {
     if (e == NULL) return engine_error(engine_err_null);
     if (pid < 0 || pjd < 0 || pid == pjd) return engine_error(engine_err_range);
     int need = (pid > pjd ? pid : pjd) + 1;
-    if (e->part2rigid == NULL || need > e->s.size_parts) {
-        int nsize = need > e->s.size_parts ? need : e->s.size_parts;
-        int *np = realloc(e->part2rigid, sizeof(int) * nsize);
+    if (need < e->s.size_parts) need = e->s.size_parts;
+    if (e->part2rigid == NULL || need > e->part2rigid_size) {
+        int *np = realloc(e->part2rigid, sizeof(int) * need);
         if (np == NULL) return engine_error(engine_err_malloc);
-        /* Only entries past what was there before need initialising. */
-        static int known = 0;
-        if (e->part2rigid == NULL) known = 0;
-        for (int k = known; k < nsize; k++) np[k] = -1;
-        known = nsize;
+        for (int k = e->part2rigid ? e->part2rigid_size : 0; k < need; k++) np[k] = -1;
         e->part2rigid = np;
+        e->part2rigid_size = need;
     }
-    int ri = e->part2rigid[pid], rj = e->part2rigid[pjd];
+    int rid = e->part2rigid[pid], rjd = e->part2rigid[pjd];
     struct rigid *r;
-    if (ri < 0 && rj < 0) {
+    if (rid < 0 && rjd < 0) {
         if (e->nr_rigids == e->rigids_size) {
-            int nsize = e->rigids_size * 2;
+            int nsize = e->rigids_size + e->rigids_size / 2 + 1;
             struct rigid *nr = realloc(e->rigids, sizeof(struct rigid) * nsize);
             if (nr == NULL) return engine_error(engine_err_malloc);
             e->rigids = nr;
             e->rigids_size = nsize;
         }
         r = &e->rigids[e->nr_rigids];
-        memset(r, 0, sizeof(*r));
+        r->nr_parts = 2;
+        r->nr_constr = 1;
+        r->parts[0] = pid;
+        r->parts[1] = pjd;
+        r->constr[0].i = 0;
+        r->constr[0].j = 1;
+        r->constr[0].d2 = d * d;
         e->part2rigid[pid] = e->part2rigid[pjd] = e->nr_rigids++;
-        r->parts[r->nr_parts++] = pid;
-        r->parts[r->nr_parts++] = pjd;
-    } else if (ri >= 0 && rj >= 0 && ri != rj) {
-        return engine_error(engine_err_nyi);   /* merging two rigid groups */
-    } else {
-        int g = ri >= 0 ? ri : rj;
-        r = &e->rigids[g];
-        int add = ri >= 0 ? pjd : pid;
-        if (e->part2rigid[add] < 0) {
-            if (r->nr_parts >= rigid_maxparts) return engine_error(engine_err_range);
-            r->parts[r->nr_parts++] = add;
-            e->part2rigid[add] = g;
+    } else if (rid >= 0 && rjd >= 0 && rid != rjd) {
+        /* Merge group rjd into rid, then add the constraint between the two. */
+        r = &e->rigids[rid];
+        struct rigid *o = &e->rigids[rjd];
+        if (r->nr_parts + o->nr_parts > rigid_maxparts || r->nr_constr + o->nr_constr + 1 > rigid_maxconstr)
+            return engine_error(engine_err_range);
+        int ind = 0, jnd = 0;
+        while (r->parts[ind] != pid) ind++;
+        while (o->parts[jnd] != pjd) jnd++;
+        for (int k = 0; k < o->nr_constr; k++) {
+            r->constr[r->nr_constr + k] = o->constr[k];
+            r->constr[r->nr_constr + k].i += r->nr_parts;
+            r->constr[r->nr_constr + k].j += r->nr_parts;
         }
+        for (int k = 0; k < o->nr_parts; k++) {
+            r->parts[r->nr_parts + k] = o->parts[k];
+            e->part2rigid[o->parts[k]] = rid;
+        }
+        r->nr_constr += o->nr_constr;
+        jnd += r->nr_parts;
+        r->nr_parts += o->nr_parts;
+        r->constr[r->nr_constr].i = ind;
+        r->constr[r->nr_constr].j = jnd;
+        r->constr[r->nr_constr].d2 = d * d;
+        r->nr_constr++;
+        /* The last group takes the place of the merged one. */
+        e->nr_rigids--;
+        if (rjd < e->nr_rigids) {
+            e->rigids[rjd] = e->rigids[e->nr_rigids];
+            for (int k = 0; k < e->rigids[rjd].nr_parts; k++) e->part2rigid[e->rigids[rjd].parts[k]] = rjd;
+            if (rid == e->nr_rigids) r = &e->rigids[rjd];
+        }
+    } else {
+        /* One or both particles already in the same group. */
+        r = &e->rigids[rid >= 0 ? rid : rjd];
+        const int g = (int)(r - e->rigids);
+        int ind = -1, jnd = -1;
+        for (int k = 0; k < r->nr_parts; k++) {
+            if (r->parts[k] == pid) ind = k;
+            else if (r->parts[k] == pjd) jnd = k;
+        }
+        if (r->nr_constr >= rigid_maxconstr || ((ind < 0 || jnd < 0) && r->nr_parts >= rigid_maxparts))
+            return engine_error(engine_err_range);
+        if (ind < 0) {
+            ind = r->nr_parts++;
+            r->parts[ind] = pid;
+            e->part2rigid[pid] = g;
+        } else if (jnd < 0) {
+            jnd = r->nr_parts++;
+            r->parts[jnd] = pjd;
+            e->part2rigid[pjd] = g;
+        }
+        r->constr[r->nr_constr].i = ind;
+        r->constr[r->nr_constr].j = jnd;
+        r->constr[r->nr_constr].d2 = d * d;
+        r->nr_constr++;
     }
-    if (r->nr_constr >= rigid_maxconstr) return engine_error(engine_err_range);
-    r->constr[r->nr_constr].i = pid;
-    r->constr[r->nr_constr].j = pjd;
-    r->constr[r->nr_constr].d2 = d * d;
-    r->nr_constr++;
+    rigid_reset_matrix(r);
     e->nr_constr++;
+    e->rigids_gen++;
+    return engine_err_ok;
+}
+
+int engine_rigid_get(struct engine *e, int g, struct rigid *out) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (out == NULL) return e->nr_rigids;
+    if (g < 0 || g >= e->nr_rigids) return engine_error(engine_err_range);
+    *out = e->rigids[g];
+    return e->nr_rigids;
+}
+
+int engine_getparts(struct engine *e, float *x, float *v, float *f, int *cell, int N) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    for (int id = 0; id < N; id++) {
+        const struct part *p = (id < s->size_parts) ? s->partlist[id] : NULL;
+        for (int k = 0; k < 3; k++) {
+            if (x) x[3 * id + k] = p ? p->x[k] : 0.0f;
+            if (v) v[3 * id + k] = p ? p->v[k] : 0.0f;
+            if (f) f[3 * id + k] = p ? p->f[k] : 0.0f;
+        }
+        if (cell) cell[id] = p ? (int)(s->celllist[id] - s->cells) : -1;
+    }
     return engine_err_ok;
 }
 
@@ -324,12 +399,15 @@ int engine_step(struct engine *e) {
     if (engine_nonbond_cuda(e) < 0) return engine_error(engine_err_cuda);
     s->epot += s->epot_nonbond;
     if (engine_advance(e) < 0) return engine_error(engine_err);
+    /* Resolve the rigid constraints (src/engine.c:2196-2231). */
+    if (e->nr_rigids > 0 && engine_rigid_eval(e) < 0) return engine_error(engine_err_rigid);
     return engine_err_ok;
 }
 
 int engine_finalize(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
     nb_device_free(e);
+    rigid_device_free(e);
     for (int c = 0; c < e->s.nr_cells; c++) free(e->s.cells[c].parts);
     free(e->s.cells);
     free(e->s.tasks);

@@ -20,8 +20,11 @@ void nb_sweep_scales(const struct space *s, float *bias, float *dscale, int *dma
 int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dnshift, int *ci_out,
                   int *cj_out);
 
-/* Device side (nonbond.cu). */
+/* Device side (nonbond.cu, rigid.cu). */
 int nb_device_free(struct engine *e);
+int rigid_device_free(struct engine *e);
+/* Launch stream of the engine's device state (NULL before engine_cuda_load). */
+void *nb_engine_stream(struct engine *e);
 
 #ifdef __cplusplus
 }

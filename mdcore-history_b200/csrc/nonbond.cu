@@ -884,6 +884,10 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* window_out, float* m
 
 // ---------------------------------------------------------------- single engine
 
+extern "C" void* nb_engine_stream(struct engine* e) {
+    return (e != nullptr && e->cuda != nullptr) ? static_cast<void*>(state(e)->stream) : nullptr;
+}
+
 extern "C" int nb_device_free(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return 0;
     state_free(state(e));
@@ -1067,6 +1071,7 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
     for (struct engine* e : st->engines) {
         e->s.epot += e->s.epot_nonbond;
         if (engine_advance(e) < 0) return engine_err;
+        if (e->nr_rigids > 0 && engine_rigid_eval(e) < 0) return engine_err = engine_err_rigid;
     }
     return 0;
 }

@@ -25,6 +25,7 @@ CLASS_WEIGHT = (0.50004, 0.16176, 0.036213)
 engine_flag_none = 0
 engine_flag_cuda = 4
 engine_flag_unsorted = 512
+engine_flag_shake = 1024
 space_periodic_full = 7
 
 
@@ -37,6 +38,24 @@ class Potential(C.Structure):
         n = self.n
         c = np.ctypeslib.as_array(self.c, shape=((n + 1) * 8,)).copy()
         return n, np.array(self.alpha[:], dtype=np.float32), c
+
+
+class RigidConstr(C.Structure):
+    _fields_ = [("i", C.c_int), ("j", C.c_int), ("d2", C.c_double)]
+
+
+class Rigid(C.Structure):
+    """struct rigid (src/rigid.h:39-59)."""
+    _fields_ = [("nr_parts", C.c_int), ("parts", C.c_int * 10), ("nr_constr", C.c_int),
+                ("constr", RigidConstr * 30), ("a", C.c_float * 900)]
+
+    def constraints(self):
+        """(i, j, d2) of every constraint, group-local indices."""
+        return [(self.constr[k].i, self.constr[k].j, self.constr[k].d2) for k in range(self.nr_constr)]
+
+    def matrix(self) -> np.ndarray:
+        n = self.nr_constr
+        return np.array(self.a[:n * n], np.float32).reshape(n, n)
 
 
 class NbStats(C.Structure):
@@ -92,6 +111,11 @@ def lib() -> C.CDLL:
         "engine_cuda_fp32_peak": (C.c_int, [C.c_int, P(C.c_float)]),
         "engine_zero_forces": (C.c_int, [vp]),
         "engine_cuda_setwindow": (C.c_int, [vp, C.c_int]),
+        "engine_rigid_eval": (C.c_int, [vp]),
+        "engine_rigid_stats": (C.c_int, [vp, ip, ip]),
+        "engine_rigid_getmatrices": (C.c_int, [vp]),
+        "engine_rigid_get": (C.c_int, [vp, C.c_int, vp]),
+        "engine_getparts": (C.c_int, [vp, vp, vp, vp, vp, C.c_int]),
         "engine_cuda_graph": (C.c_int, [vp, C.c_int]),
         "engine_cuda_autotune": (C.c_int, [vp, C.c_int, ip, ip, P(C.c_float)]),
         "engine_batch_create": (C.c_int, [P(vp), C.c_int, P(vp)]),
@@ -211,8 +235,13 @@ class Engine:
             _check(e.lib.engine_addpot(e.ptr, ptr, spec.ti, spec.tj), "engine_addpot")
         x = np.ascontiguousarray(sysm.x, np.float64)
         t = np.ascontiguousarray(sysm.type, np.int32)
-        _check(e.lib.engine_load(e.ptr, _dptr(x), None, _iptr(t), None, None, None, None, sysm.n), "engine_load")
+        v = None if sysm.v is None else np.ascontiguousarray(sysm.v, np.float64)
+        _check(e.lib.engine_load(e.ptr, _dptr(x), None if v is None else _dptr(v), _iptr(t), None, None, None, None,
+                                 sysm.n), "engine_load")
         e.n = sysm.n
+        if sysm.rigid is not None:
+            for i, j, d in np.asarray(sysm.rigid):
+                _check(e.lib.engine_rigid_add(e.ptr, int(i), int(j), float(d)), "engine_rigid_add")
         for i, j in np.asarray(sysm.excl).reshape(-1, 2):
             _check(e.lib.engine_exclusion_add(e.ptr, int(i), int(j)), "engine_exclusion_add")
         if len(sysm.excl):
@@ -323,6 +352,36 @@ class Engine:
         _check(self.lib.engine_cuda_taskclocks(self.ptr, int(enable), clk.ctypes.data_as(C.POINTER(C.c_longlong)),
                                                _iptr(sm), n), "engine_cuda_taskclocks")
         return clk, sm
+
+    # -- rigid constraints -----------------------------------------------------------
+    def rigid_eval(self):
+        """engine_rigid_eval: SHAKE or P-SHAKE of every rigid group on the device."""
+        _check(self.lib.engine_rigid_eval(self.ptr), "engine_rigid_eval")
+
+    def rigid_stats(self):
+        """(largest iteration count, unconverged groups) of the last evaluation."""
+        a, b = C.c_int(), C.c_int()
+        _check(self.lib.engine_rigid_stats(self.ptr, C.byref(a), C.byref(b)), "engine_rigid_stats")
+        return a.value, b.value
+
+    def rigid_groups(self):
+        """Every rigid group as a Rigid structure, P-SHAKE matrices synced from the device."""
+        _check(self.lib.engine_rigid_getmatrices(self.ptr), "engine_rigid_getmatrices")
+        n = _check(self.lib.engine_rigid_get(self.ptr, 0, None), "engine_rigid_get")
+        out = []
+        for g in range(n):
+            r = Rigid()
+            _check(self.lib.engine_rigid_get(self.ptr, g, C.byref(r)), "engine_rigid_get")
+            out.append(r)
+        return out
+
+    def parts(self):
+        """Cell-relative float positions, velocities, forces (N x 3 each) and cells by id."""
+        x = np.zeros((self.n, 3), np.float32); v = np.zeros((self.n, 3), np.float32)
+        f = np.zeros((self.n, 3), np.float32); c = np.zeros(self.n, np.int32)
+        _check(self.lib.engine_getparts(self.ptr, x.ctypes.data, v.ctypes.data, f.ctypes.data, c.ctypes.data,
+                                        self.n), "engine_getparts")
+        return x, v, f, c
 
     # -- readback --------------------------------------------------------------------
     def forces(self) -> np.ndarray:

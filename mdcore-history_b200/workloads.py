@@ -55,6 +55,8 @@ class System:
     dt: float = 0.002
     flags: int = 0
     period: int = 7
+    v: Optional[np.ndarray] = None          # (N,3) velocities, nm/ps (None: at rest)
+    rigid: Optional[np.ndarray] = None      # (M,3) rigid constraints: id i, id j, length d (nm)
 
     @property
     def n(self) -> int:
@@ -76,6 +78,11 @@ def _wrap(x: np.ndarray, dim: np.ndarray) -> np.ndarray:
     # np.mod can return dim itself for tiny negative inputs; keep strictly inside.
     hi = np.nextafter(dim, 0.0)
     return np.minimum(x, hi)
+
+
+def wrap_positions(x: np.ndarray, dim: np.ndarray) -> np.ndarray:
+    """Positions wrapped into the periodic box [0, dim)."""
+    return _wrap(np.asarray(x, np.float64), np.asarray(dim, np.float64))
 
 
 def argon_fcc(ncell: int = 20, seed: int = 0, density: float = 21.0, jitter: float = 0.01,
@@ -155,6 +162,45 @@ def water_spce(nside: int = 32, seed: int = 0, density: float = 33.4, jitter: fl
     return System(
         name=f"water-spce-{3 * nmol}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
         masses=[15.9994, 1.00794], charges=[qO, qH], pots=pots, x=x, type=typ, excl=excl, dt=0.002)
+
+
+KB = 0.0083144626                         # kJ mol^-1 K^-1
+
+
+def maxwell_velocities(sysm: System, temperature: float, seed: int = 1) -> np.ndarray:
+    """Velocities (nm/ps) drawn from the Maxwell-Boltzmann distribution at `temperature`
+    for every particle's mass, net momentum removed."""
+    rng = np.random.default_rng(seed)
+    m = np.asarray(sysm.masses, np.float64)[sysm.type]
+    v = rng.normal(size=(sysm.n, 3)) * np.sqrt(KB * temperature / m)[:, None]
+    v -= (m[:, None] * v).sum(0) / m.sum()
+    return v
+
+
+def with_rigid_water(sysm: System, temperature: float = 300.0, seed: int = 1) -> System:
+    """The SPC/E system with its three distance constraints per molecule (O-H 0.1 nm twice,
+    H-H 0.163298 nm, the geometry examples/bulk/bulk.c:308-310 holds with SHAKE), added in
+    the order O-H1, O-H2, H1-H2, and Maxwell-Boltzmann velocities."""
+    nmol = sysm.n // 3
+    k = np.arange(nmol) * 3
+    hh = 2.0 * 0.1 * math.sin(math.radians(109.47) / 2.0)
+    rig = np.stack([np.stack([k, k + 1, np.full(nmol, 0.1)], 1), np.stack([k, k + 2, np.full(nmol, 0.1)], 1),
+                    np.stack([k + 1, k + 2, np.full(nmol, hh)], 1)], 1).reshape(-1, 3)
+    return dataclasses.replace(sysm, rigid=rig, v=maxwell_velocities(sysm, temperature, seed),
+                               name=sysm.name + "-rigid")
+
+
+def write_rigidfile(sysm: System, path: str, shake: bool) -> None:
+    """Velocities and rigid constraints for the reference driver's rigid mode."""
+    rig = np.zeros((0, 3)) if sysm.rigid is None else np.asarray(sysm.rigid)
+    v = np.zeros((sysm.n, 3)) if sysm.v is None else np.asarray(sysm.v, np.float64)
+    with open(path, "wb") as f:
+        f.write(b"MDB2RIG1")
+        f.write(struct.pack("<iii", len(rig), int(shake), 0))
+        f.write(struct.pack("<d", sysm.dt))
+        f.write(np.ascontiguousarray(v, "<f8").tobytes())
+        for i, j, d in rig:
+            f.write(struct.pack("<iid", int(i), int(j), float(d)))
 
 
 def lb_mix(eps_i, sig_i, eps_j, sig_j):

@@ -37,7 +37,7 @@ struct ocell {
     int start, count;
 };
 
-/* Shift and flip of src/space.c:80-114: returns the sort direction, swaps *a/*b when the
+/* Shift and flip of src/space.c:80-114: returns the sort direction, swaps *a and *b when the
  * shift points into the negative half-space. */
 static int getsid(const double dim[3], const struct ocell *cells, int *a, int *b, float shift[3]) {
     int idx = 0;
@@ -84,9 +84,9 @@ static void eval_fp64(const float *coef, const float *alpha, int nmax, float r2f
     *f = eff * (double)c[1] / r;
 }
 
-/* Nonbonded forces (by particle id, FP64), energy, virial, sum over pairs of |r_ij . F_ij|
- * (the scale of the virial's rounding error: the net virial may cancel to far less) and
- * counts.
+/* Nonbonded forces (by particle id, FP64), energy, virial, the sums over pairs of |e_ij|
+ * and |r_ij . F_ij| (the scales of the rounding errors of energy and virial: the net values
+ * may cancel to far less) and counts.
  *   xrel[3N] float cell-local positions, cell[N] cell index, type[N]
  *   coef: tables concatenated; alpha[4*npots]; coff[npots] float offset of each table;
  *   potn[npots]; potidx[mt*mt] table index or -1.
@@ -95,8 +95,8 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                    const double *origin, const double *dim, const int *cdim, double cutoff,
                    unsigned period, int mt, const int *potidx, const float *coef, const float *alpha,
                    const int *coff, const int *potn, int nexcl, const int *excl,
-                   double *f_out, double *epot_out, double *virial_out, double *virial_abs_out,
-                   long long *npairs_out, long long *nexcl_out) {
+                   double *f_out, double *epot_out, double *epot_abs_out, double *virial_out,
+                   double *virial_abs_out, long long *npairs_out, long long *nexcl_out) {
     const int ncells = cdim[0] * cdim[1] * cdim[2];
     double h[3];
     int span[3];
@@ -131,7 +131,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
     const float cutf = (float)cutoff;
     const float cut2_pair = cutf * cutf;
     const float cut2_self = (float)(cutoff * cutoff);
-    double epot = 0.0, vir = 0.0, vir_abs = 0.0;
+    double epot = 0.0, epot_abs = 0.0, vir = 0.0, vir_abs = 0.0;
     long long npairs = 0, nex = 0;
     memset(f_out, 0, sizeof(double) * 3 * N);
 
@@ -195,6 +195,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                                         f_out[3 * pj + q] += w;
                                     }
                                     epot += e;
+                                    epot_abs += fabs(e);
                                     vir += fs * r2;
                                     vir_abs += fabs(fs * r2);
                                     npairs++;
@@ -205,6 +206,7 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                 }
             }
     *epot_out = epot;
+    if (epot_abs_out) *epot_abs_out = epot_abs;
     *virial_out = -vir;
     if (virial_abs_out) *virial_abs_out = vir_abs;
     *npairs_out = npairs;
@@ -239,6 +241,154 @@ int oracle_sortkeys(int count, const float *xrel, const double *h, int sid, unsi
             b--;
         }
         keys[b + 1] = v;
+    }
+    return 0;
+}
+
+/* Rigid constraints of one evaluation (src/engine_rigid.c:352-583), FP64: SHAKE
+ * (src/rigid.c:81-277) when pshake == 0, P-SHAKE (src/rigid.c:279-523) otherwise.
+ *   Particles by id: x[3N], v[3N], f[3N] cell-relative float state (updated in place),
+ *   cell[N] cell index, loc[3*ncells] cell grid coordinates, h[3] cell edge, mass[N].
+ *   Groups: roff[ng+1] into parts[] (particle ids), coff[ng+1] into ci/cj (group-local
+ *   indices) and d2; a[] the float P-SHAKE matrices (nc*nc per group, in group order),
+ *   refined in place when pshake and (a_update or more than 10 iterations).
+ *   iters[ng] receives each group's iteration count.
+ * Mixed precision follows the reference's P-SHAKE exactly (double iterations, float
+ * matrices); SHAKE is restated entirely in double (the reference's single build keeps
+ * lambda, the gradients and the tolerance in float). */
+#define O_MAXP 10
+#define O_MAXC 30
+#define O_MAXITER 100
+
+static int oshift(const int *loc, int c, int c0, int j) {
+    int s = loc[3 * c + j] - loc[3 * c0 + j];
+    if (s > 1) s = -1;
+    else if (s < -1) s = 1;
+    return s;
+}
+
+int oracle_rigid(int ng, const int *roff, const int *parts, const int *coff, const int *ci, const int *cj,
+                 const double *d2, float *a, const int *cell, const int *loc, const double *h,
+                 const double *mass, float *x, float *v, float *f, double dt, double tol, int pshake,
+                 int a_update, int *iters) {
+    double idt = 1.0 / dt;
+    int aoff = 0;
+    for (int g = 0; g < ng; g++) {
+        int np = roff[g + 1] - roff[g], nc = coff[g + 1] - coff[g];
+        const int *pid = parts + roff[g];
+        const int *gi = ci + coff[g], *gj = cj + coff[g];
+        const double *gd2 = d2 + coff[g];
+        float *ga = a + aoff;
+        aoff += nc * nc;
+        if (np > O_MAXP || nc > O_MAXC) return -1;
+        double xp[3 * O_MAXP], xo[3 * O_MAXP], m[O_MAXP];
+        int c0 = cell[pid[0]], iter;
+        for (int k = 0; k < np; k++) {
+            int id = pid[k];
+            for (int j = 0; j < 3; j++) {
+                xp[3 * k + j] = (double)x[3 * id + j] + h[j] * (double)oshift(loc, cell[id], c0, j);
+                xo[3 * k + j] = xp[3 * k + j] - dt * (double)v[3 * id + j];
+            }
+            m[k] = mass[id];
+        }
+        if (!pshake) {
+            double vc[3 * O_MAXC], wvc[3 * O_MAXC], res[O_MAXC];
+            for (int k = 0; k < nc; k++)
+                for (int j = 0; j < 3; j++) {
+                    vc[3 * k + j] = xo[3 * gi[k] + j] - xo[3 * gj[k] + j];
+                    wvc[3 * k + j] = 1.0 / (m[gi[k]] + m[gj[k]]) * vc[3 * k + j];
+                }
+            for (iter = 0; iter < O_MAXITER; iter++) {
+                double max_res = 0.0;
+                for (int k = 0; k < nc; k++) {
+                    res[k] = gd2[k];
+                    for (int j = 0; j < 3; j++)
+                        res[k] -= (xp[3 * gi[k] + j] - xp[3 * gj[k] + j]) * (xp[3 * gi[k] + j] - xp[3 * gj[k] + j]);
+                    if (fabs(res[k]) > max_res) max_res = fabs(res[k]);
+                }
+                if (max_res < tol) break;
+                for (int k = 0; k < nc; k++) {
+                    int p = gi[k], q = gj[k];
+                    double lambda = 0.5 * res[k] / ((xp[3 * p] - xp[3 * q]) * vc[3 * k] +
+                                                    (xp[3 * p + 1] - xp[3 * q + 1]) * vc[3 * k + 1] +
+                                                    (xp[3 * p + 2] - xp[3 * q + 2]) * vc[3 * k + 2]);
+                    for (int j = 0; j < 3; j++) {
+                        double w = lambda * wvc[3 * k + j];
+                        xp[3 * p + j] += w * m[q];
+                        xp[3 * q + j] -= w * m[p];
+                    }
+                }
+            }
+        } else {
+            static double vc[3 * O_MAXC * O_MAXP];
+            int row = 3 * np;
+            memset(vc, 0, sizeof(double) * nc * row);
+            for (int k = 0; k < nc; k++) {
+                int p = gi[k], q = gj[k];
+                double dv[3];
+                for (int j = 0; j < 3; j++) dv[j] = (xo[3 * p + j] - xo[3 * q + j]) / (m[p] + m[q]);
+                for (int i = 0; i < nc; i++)
+                    if (ga[k * nc + i] != 0.0f)
+                        for (int j = 0; j < 3; j++) {
+                            vc[i * row + p * 3 + j] += ga[k * nc + i] * dv[j] * m[q];
+                            vc[i * row + q * 3 + j] += -ga[k * nc + i] * dv[j] * m[p];
+                        }
+            }
+            for (iter = 0; iter < O_MAXITER; iter++) {
+                double max_res = 0.0;
+                for (int k = 0; k < nc; k++) {
+                    int p = gi[k], q = gj[k];
+                    const double *vk = vc + k * row;
+                    double res = gd2[k];
+                    for (int j = 0; j < 3; j++) res -= (xp[3 * p + j] - xp[3 * q + j]) * (xp[3 * p + j] - xp[3 * q + j]);
+                    if (fabs(res) > max_res) max_res = fabs(res);
+                    double lambda = 0.5 * res / ((xp[3 * p] - xp[3 * q]) * (vk[3 * p] - vk[3 * q]) +
+                                                 (xp[3 * p + 1] - xp[3 * q + 1]) * (vk[3 * p + 1] - vk[3 * q + 1]) +
+                                                 (xp[3 * p + 2] - xp[3 * q + 2]) * (vk[3 * p + 2] - vk[3 * q + 2]));
+                    for (int j = 0; j < row; j++) xp[j] += lambda * vk[j];
+                }
+                if (max_res < tol) break;
+            }
+            if (nc > 1 && (a_update || iter > 10)) {
+                float an[O_MAXC * O_MAXC], tmp[O_MAXC * O_MAXC], maxa = 0.0f;
+                for (int i = 0; i < nc; i++) {
+                    int p = gi[i], q = gj[i];
+                    const double *vi = vc + i * row;
+                    float dx[3];
+                    for (int j = 0; j < 3; j++) dx[j] = (float)(xp[3 * p + j] - xp[3 * q + j]);
+                    float w = -1.0 / (dx[0] * (vi[3 * p] - vi[3 * q]) + dx[1] * (vi[3 * p + 1] - vi[3 * q + 1]) +
+                                      dx[2] * (vi[3 * p + 2] - vi[3 * q + 2]));
+                    for (int j = i + 1; j < nc; j++) {
+                        const double *vj = vc + j * row;
+                        an[i + j * nc] = w * (dx[0] * (vj[3 * p] - vj[3 * q]) + dx[1] * (vj[3 * p + 1] - vj[3 * q + 1]) +
+                                              dx[2] * (vj[3 * p + 2] - vj[3 * q + 2]));
+                        an[j + i * nc] = an[i + j * nc];
+                        maxa = fmaxf(maxa, fabsf(an[i + j * nc]));
+                    }
+                    an[i + i * nc] = 1.0f;
+                }
+                if (maxa > 0.1f) {
+                    float w = 0.1 / maxa;
+                    for (int i = 0; i < nc * nc; i++) an[i] *= w;
+                    for (int i = 0; i < nc; i++) an[i * nc + i] = 1.0f;
+                }
+                memset(tmp, 0, sizeof(float) * nc * nc);
+                for (int j = 0; j < nc; j++)
+                    for (int k = 0; k < nc; k++)
+                        for (int i = 0; i < nc; i++) tmp[j * nc + i] += ga[k * nc + i] * an[j * nc + k];
+                memcpy(ga, tmp, sizeof(float) * nc * nc);
+            }
+        }
+        iters[g] = iter;
+        for (int k = 0; k < np; k++) {
+            int id = pid[k];
+            for (int j = 0; j < 3; j++) {
+                double xn = xp[3 * k + j] - h[j] * oshift(loc, cell[id], c0, j);
+                if (pshake) f[3 * id + j] += idt * idt * (xn - x[3 * id + j]) * m[k];
+                v[3 * id + j] += idt * (xn - x[3 * id + j]);
+                x[3 * id + j] = xn;
+            }
+        }
     }
     return 0;
 }

@@ -32,8 +32,11 @@ def lib():
         L.oracle_nonbond.argtypes = [C.c_int, P(C.c_float), P(C.c_int), P(C.c_int), P(C.c_double), P(C.c_double),
                                      P(C.c_int), C.c_double, C.c_uint, C.c_int, P(C.c_int), P(C.c_float),
                                      P(C.c_float), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int), P(C.c_double),
-                                     P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_longlong),
+                                     P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_longlong),
                                      P(C.c_longlong)]
+        L.oracle_rigid.restype = C.c_int
+        L.oracle_rigid.argtypes = [C.c_int] + [C.c_void_p] * 14 + [C.c_double, C.c_double, C.c_int, C.c_int,
+                                                                    C.c_void_p]
         L.oracle_sortkeys.restype = C.c_int
         L.oracle_sortkeys.argtypes = [C.c_int, P(C.c_float), P(C.c_double), C.c_int, P(C.c_uint)]
         _lib = L
@@ -76,13 +79,13 @@ def pack_tables(sysm, tables):
 
 
 def nonbond(sysm, tables, binned=None):
-    """FP64 forces (by id), energy, virial, sum over pairs of |r.F| (virial_abs), pair and
-    excluded-pair counts."""
+    """FP64 forces (by id), energy, virial, the sums over pairs of |e| (epot_abs) and |r.F|
+    (virial_abs), pair and excluded-pair counts."""
     b = binned or bin_system(sysm)
     t = pack_tables(sysm, tables)
     N = sysm.n
     f = np.zeros((N, 3), np.float64)
-    epot, vir, vabs = C.c_double(), C.c_double(), C.c_double()
+    epot, eabs, vir, vabs = C.c_double(), C.c_double(), C.c_double(), C.c_double()
     npairs, nex = C.c_longlong(), C.c_longlong()
     xrel = np.ascontiguousarray(b["xrel"], np.float32)
     cell = np.ascontiguousarray(b["cell"], np.int32)
@@ -96,11 +99,12 @@ def nonbond(sysm, tables, binned=None):
                               len(sysm.masses), _p(t["potidx"], C.c_int), _p(t["coef"], C.c_float),
                               _p(t["alpha"], C.c_float), _p(t["coff"], C.c_int), _p(t["potn"], C.c_int),
                               len(sysm.excl), _p(excl, C.c_int) if excl.size else None, _p(f, C.c_double),
-                              C.byref(epot), C.byref(vir), C.byref(vabs), C.byref(npairs), C.byref(nex))
+                              C.byref(epot), C.byref(eabs), C.byref(vir), C.byref(vabs), C.byref(npairs),
+                              C.byref(nex))
     if rc != 0:
         raise RuntimeError("oracle_nonbond failed")
-    return dict(f=f, epot=epot.value, virial=vir.value, virial_abs=vabs.value, pairs=npairs.value,
-                excluded=nex.value)
+    return dict(f=f, epot=epot.value, epot_abs=eabs.value, virial=vir.value, virial_abs=vabs.value,
+                pairs=npairs.value, excluded=nex.value)
 
 
 def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:
@@ -110,6 +114,44 @@ def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:
     hh = np.ascontiguousarray(h, np.float64)
     lib().oracle_sortkeys(n, _p(x, C.c_float), _p(hh, C.c_double), sid, _p(keys, C.c_uint))
     return keys[:n]
+
+
+def rigid(groups, x, v, f, cell, cdim, h, mass, dt, tol, pshake, a_update):
+    """One rigid-constraint evaluation (oracle_rigid) on particle state by id.
+
+    groups: list of (parts: list of ids, constraints: list of (i, j, d2), a: nc x nc float32).
+    x, v, f: (N, 3) float32 cell-relative positions, velocities, forces; cell: (N,) cell
+    index; cdim: cell grid; h: cell edge; mass: (N,) per-particle mass.
+    Returns (x, v, f, [a], iters) after the evaluation (inputs are not modified)."""
+    roff = np.cumsum([0] + [len(g[0]) for g in groups]).astype(np.int32)
+    coff = np.cumsum([0] + [len(g[1]) for g in groups]).astype(np.int32)
+    parts = np.array([i for g in groups for i in g[0]], np.int32)
+    con = np.array([c for g in groups for c in g[1]], np.float64).reshape(-1, 3)
+    ci = np.ascontiguousarray(con[:, 0], np.int32)
+    cj = np.ascontiguousarray(con[:, 1], np.int32)
+    d2 = np.ascontiguousarray(con[:, 2], np.float64)
+    a = np.concatenate([np.asarray(g[2], np.float32).reshape(-1) for g in groups]).astype(np.float32)
+    cdim = np.asarray(cdim, np.int64)
+    ncells = int(np.prod(cdim))
+    cid = np.arange(ncells)
+    loc = np.stack([cid // (cdim[1] * cdim[2]), (cid // cdim[2]) % cdim[1], cid % cdim[2]], 1).astype(np.int32)
+    xo, vo, fo = (np.ascontiguousarray(t, np.float32).copy() for t in (x, v, f))
+    cell = np.ascontiguousarray(cell, np.int32)
+    hh = np.ascontiguousarray(h, np.float64)
+    m = np.ascontiguousarray(mass, np.float64)
+    iters = np.zeros(len(groups), np.int32)
+    rc = lib().oracle_rigid(len(groups), roff.ctypes.data, parts.ctypes.data, coff.ctypes.data, ci.ctypes.data,
+                            cj.ctypes.data, d2.ctypes.data, a.ctypes.data, cell.ctypes.data, loc.ctypes.data,
+                            hh.ctypes.data, m.ctypes.data, xo.ctypes.data, vo.ctypes.data, fo.ctypes.data,
+                            float(dt), float(tol), int(pshake), int(a_update), iters.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("oracle_rigid failed")
+    mats, off = [], 0
+    for g in groups:
+        n = len(g[1])
+        mats.append(a[off:off + n * n].reshape(n, n).copy())
+        off += n * n
+    return xo, vo, fo, mats, iters
 
 
 def ref_available(strict: bool = True) -> bool:

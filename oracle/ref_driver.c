@@ -9,6 +9,13 @@
  *   ref_driver forces <sysfile> <outfile> <nr_runners>
  *       One engine_step with dt = 0 (positions do not move, src/engine.c:1975-1979), then
  *       dumps forces, energies, cell assignment, sort lists and the float potential tables.
+ *   ref_driver rigid <sysfile> <rigidfile> <outfile> <nevals>
+ *       Loads the system with velocities, adds the rigid constraints (engine_rigid_add),
+ *       sets dt, then calls engine_rigid_eval nevals times (src/engine_rigid.c:352-583:
+ *       SHAKE with engine_flag_shake, P-SHAKE otherwise) and dumps, after each call, the
+ *       cell-relative positions, velocities and forces by particle id and every group's
+ *       P-SHAKE matrix.  Rigid file (little-endian): "MDB2RIG1", int32 ncon, shake, pad,
+ *       double dt, double v[3N], ncon x {int32 i, j; double d}.
  *   ref_driver bench <sysfile> <nr_runners> <warmup> <steps>
  *       Times engine_step (dt = 0: sort + pair/self sweep + exclusion subtraction +
  *       bookkeeping, src/engine.c:2070-2240) with clock_gettime and prints one JSON line.
@@ -55,11 +62,12 @@ static struct potential *make_pot(const struct sys_pot *sp) {
     return NULL;
 }
 
-static int build(struct engine *e, struct sys_desc *sd, struct potential ***pots_out, int runners) {
+static int build_v(struct engine *e, struct sys_desc *sd, struct potential ***pots_out, int runners, double *v,
+                   unsigned int extra_flags, int start) {
     int k;
     struct potential **pots = malloc(sizeof(struct potential *) * (sd->npots + 1));
     if (engine_init(e, sd->origin, sd->dim, sd->L, sd->cutoff, sd->period, sd->ntypes,
-                    sd->flags) != 0) {
+                    sd->flags | extra_flags) != 0) {
         fprintf(stderr, "ref_driver: engine_init failed (%i)\n", engine_err);
         errs_dump(stderr);
         return -1;
@@ -74,7 +82,7 @@ static int build(struct engine *e, struct sys_desc *sd, struct potential ***pots
         }
         if (engine_addpot(e, pots[k], sd->pots[k].ti, sd->pots[k].tj) < 0) { errs_dump(stderr); return -1; }
     }
-    if (engine_load(e, sd->x, NULL, sd->type, NULL, NULL, NULL, NULL, sd->N) < 0) {
+    if (engine_load(e, sd->x, v, sd->type, NULL, NULL, NULL, NULL, sd->N) < 0) {
         fprintf(stderr, "ref_driver: engine_load failed (%i)\n", engine_err);
         errs_dump(stderr);
         return -1;
@@ -84,12 +92,74 @@ static int build(struct engine *e, struct sys_desc *sd, struct potential ***pots
     if (sd->nexcl > 0 && engine_exclusion_shrink(e) < 0) { errs_dump(stderr); return -1; }
     e->time = 0;
     e->dt = 0.0;
-    if (engine_start(e, runners, runners) < 0) {
+    if (start && engine_start(e, runners, runners) < 0) {
         fprintf(stderr, "ref_driver: engine_start failed (%i)\n", engine_err);
         errs_dump(stderr);
         return -1;
     }
     *pots_out = pots;
+    return 0;
+}
+
+static int build(struct engine *e, struct sys_desc *sd, struct potential ***pots_out, int runners) {
+    return build_v(e, sd, pots_out, runners, NULL, 0, 1);
+}
+
+static int do_rigid(const char *sysf, const char *rigf, const char *outf, int nevals) {
+    struct sys_desc sd;
+    static struct engine e;
+    struct potential **pots;
+    char magic[8];
+    int hdr[3], k, id, ev;
+    double dt;
+    FILE *f, *out;
+    if (sys_read(sysf, &sd) != 0) { fprintf(stderr, "ref_driver: bad system file %s\n", sysf); return 1; }
+    f = fopen(rigf, "rb");
+    if (f == NULL || fread(magic, 1, 8, f) != 8 || memcmp(magic, "MDB2RIG1", 8) != 0 ||
+        fread(hdr, sizeof(int), 3, f) != 3 || fread(&dt, sizeof(double), 1, f) != 1) {
+        fprintf(stderr, "ref_driver: bad rigid file %s\n", rigf);
+        return 1;
+    }
+    double *v = malloc(sizeof(double) * 3 * sd.N);
+    if (fread(v, sizeof(double), 3 * (size_t)sd.N, f) != 3 * (size_t)sd.N) return 1;
+    if (build_v(&e, &sd, &pots, 1, v, hdr[1] ? engine_flag_shake : 0, 0) != 0) return 1;
+    for (k = 0; k < hdr[0]; k++) {
+        int ij[2];
+        double d;
+        if (fread(ij, sizeof(int), 2, f) != 2 || fread(&d, sizeof(double), 1, f) != 1) return 1;
+        if (engine_rigid_add(&e, ij[0], ij[1], d) < 0) { errs_dump(stderr); return 1; }
+    }
+    fclose(f);
+    e.dt = dt;
+    e.time = 0;
+    out = fopen(outf, "wb");
+    if (out == NULL) return 1;
+    fwrite(&sd.N, sizeof(int), 1, out);
+    fwrite(&e.nr_rigids, sizeof(int), 1, out);
+    fwrite(&nevals, sizeof(int), 1, out);
+    for (ev = 0; ev < nevals; ev++) {
+        if (engine_rigid_eval(&e) != 0) { errs_dump(stderr); return 1; }
+        for (id = 0; id < sd.N; id++) fwrite(e.s.partlist[id]->x, sizeof(float), 3, out);
+        for (id = 0; id < sd.N; id++) fwrite(e.s.partlist[id]->v, sizeof(float), 3, out);
+        for (id = 0; id < sd.N; id++) fwrite(e.s.partlist[id]->f, sizeof(float), 3, out);
+        for (k = 0; k < e.nr_rigids; k++) {
+            struct rigid *r = &e.rigids[k];
+            fwrite(&r->nr_parts, sizeof(int), 1, out);
+            fwrite(r->parts, sizeof(int), r->nr_parts, out);
+            fwrite(&r->nr_constr, sizeof(int), 1, out);
+            for (int c = 0; c < r->nr_constr; c++) {
+                fwrite(&r->constr[c].i, sizeof(int), 1, out);
+                fwrite(&r->constr[c].j, sizeof(int), 1, out);
+                fwrite(&r->constr[c].d2, sizeof(double), 1, out);
+            }
+            fwrite(r->a, sizeof(float), (size_t)r->nr_constr * r->nr_constr, out);
+        }
+    }
+    for (id = 0; id < sd.N; id++) {
+        int c = (int)(e.s.celllist[id] - e.s.cells);
+        fwrite(&c, sizeof(int), 1, out);
+    }
+    fclose(out);
     return 0;
 }
 
@@ -176,6 +246,8 @@ static int do_bench(const char *sysf, int runners, int warmup, int steps) {
 int main(int argc, char *argv[]) {
     if (argc >= 5 && strcmp(argv[1], "forces") == 0)
         return do_forces(argv[2], argv[3], atoi(argv[4]));
+    if (argc >= 6 && strcmp(argv[1], "rigid") == 0)
+        return do_rigid(argv[2], argv[3], argv[4], atoi(argv[5]));
     if (argc >= 6 && strcmp(argv[1], "bench") == 0)
         return do_bench(argv[2], atoi(argv[3]), atoi(argv[4]), atoi(argv[5]));
     fprintf(stderr, "usage: ref_driver forces <sys> <out> <runners> | bench <sys> <runners> <warmup> <steps>\n");

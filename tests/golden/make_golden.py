@@ -12,6 +12,11 @@ Fixtures
   argon_1372.npz   jittered FCC LJ argon, 1,372 atoms, 4^3 cells, table tol 1e-4
   water_3000.npz   rigid SPC/E water, 1,000 molecules, 3^3 cells, 3,000 exclusions
   tables.npz       float tables of potential_create_* for a parameter sweep
+  water_rigid.npz  the water_3000 system with its 3,000 distance constraints (O-H, O-H, H-H)
+                   and Maxwell-Boltzmann velocities at 300 K: the reference's
+                   engine_rigid_eval, P-SHAKE three times in a row (matrix refinement on)
+                   and SHAKE (engine_flag_shake) once, positions/velocities/forces after
+                   each call, the rigid groups and their P-SHAKE matrices
 For each system: reference forces (FP32, by id), energies (total, sweep, exclusion
 subtraction), the pair count of the reference sweep (one-interval counter tables),
 cell assignment, cell-local float positions, the reference's sort key lists and tables.
@@ -83,6 +88,70 @@ TABLE_CASES = [
 ]
 
 
+def read_rigidout(path, n):
+    """Parses the output of `ref_driver rigid`."""
+    raw = open(path, "rb").read()
+    off = 0
+
+    def take(dtype, count):
+        nonlocal off
+        a = np.frombuffer(raw, dtype, count, off)
+        off += a.nbytes
+        return a
+
+    N, nrig, nev = take("<i4", 3)
+    assert N == n
+    evals = []
+    groups = None
+    for _ in range(nev):
+        x = take("<f4", 3 * N).reshape(N, 3)
+        v = take("<f4", 3 * N).reshape(N, 3)
+        f = take("<f4", 3 * N).reshape(N, 3)
+        gs, mats = [], []
+        for _ in range(nrig):
+            np_ = int(take("<i4", 1)[0])
+            parts = take("<i4", np_).copy()
+            nc = int(take("<i4", 1)[0])
+            con = []
+            for _ in range(nc):
+                i, j = take("<i4", 2)
+                d2 = float(take("<f8", 1)[0])
+                con.append((int(i), int(j), d2))
+            mats.append(take("<f4", nc * nc).copy())
+            gs.append((parts, con))
+        groups = gs
+        evals.append((x.copy(), v.copy(), f.copy(), np.concatenate(mats)))
+    cell = take("<i4", N).copy()
+    return groups, evals, cell
+
+
+def rigid_fixture(tmp):
+    sysm = W.with_rigid_water(W.water_spce(10), 300.0, seed=1)
+    # Positions one free step ahead (x + dt v, as after the position update of a step):
+    # the constraints are violated by ~dt |v| and the positions before the step
+    # (x - dt v, which SHAKE reconstructs) satisfy them.
+    sysm.x = W.wrap_positions(sysm.x + sysm.dt * sysm.v, sysm.dim)
+    sysf = os.path.join(tmp, "w.sys")
+    W.write_sysfile(sysm, sysf)
+    out = {"x": sysm.x, "v": sysm.v, "rigid": sysm.rigid, "dt": sysm.dt}
+    for shake, nev, tag in ((0, 3, "p"), (1, 1, "s")):
+        rigf, outf = os.path.join(tmp, "w.rig"), os.path.join(tmp, "w.rout")
+        W.write_rigidfile(sysm, rigf, shake=bool(shake))
+        subprocess.run([DRIVER, "rigid", sysf, rigf, outf, str(nev)], check=True)
+        groups, evals, cell = read_rigidout(outf, sysm.n)
+        out[f"{tag}x"] = np.stack([e[0] for e in evals])
+        out[f"{tag}v"] = np.stack([e[1] for e in evals])
+        out[f"{tag}f"] = np.stack([e[2] for e in evals])
+        out[f"{tag}a"] = np.stack([e[3] for e in evals])
+        out["cell"] = cell
+    out["roff"] = np.cumsum([0] + [len(g[0]) for g in groups]).astype(np.int32)
+    out["parts"] = np.concatenate([g[0] for g in groups]).astype(np.int32)
+    out["coff"] = np.cumsum([0] + [len(g[1]) for g in groups]).astype(np.int32)
+    out["constr"] = np.array([c for g in groups for c in g[1]], np.float64)
+    np.savez_compressed(os.path.join(HERE, "water_rigid.npz"), **out)
+    print("rigid", len(groups), "groups; P-SHAKE x3, SHAKE x1")
+
+
 def table_fixture(tmp):
     out = {}
     for k, (kind, a, b, tol, p0, p1, p2, p3) in enumerate(TABLE_CASES):
@@ -109,3 +178,4 @@ if __name__ == "__main__":
         system_fixture(W.argon_fcc(7), "argon_1372.npz", tmp)
         system_fixture(W.water_spce(10), "water_3000.npz", tmp)
         table_fixture(tmp)
+        rigid_fixture(tmp)

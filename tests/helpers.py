@@ -43,3 +43,36 @@ def sort_cells_of(ref):
         off_i += cnt
         off_k += 13 * cnt
         yield cid, int(mask), ids, keys
+
+
+def load_rigid_golden():
+    """The rigid-water fixture: (System with positions one free step ahead, velocities and
+    constraints; fixture arrays; the reference's groups as oracle input with identity
+    P-SHAKE matrices)."""
+    import dataclasses
+    sysm, _ = load_golden("water_3000.npz")
+    z = np.load(os.path.join(GOLDEN, "water_rigid.npz"))
+    sysm = dataclasses.replace(sysm, x=z["x"], v=z["v"], rigid=z["rigid"], dt=float(z["dt"]))
+    roff, parts, coff, con = z["roff"], z["parts"], z["coff"], z["constr"]
+    groups = []
+    for g in range(len(roff) - 1):
+        nc = int(coff[g + 1] - coff[g])
+        groups.append(([int(p) for p in parts[roff[g]:roff[g + 1]]],
+                       [(int(c[0]), int(c[1]), float(c[2])) for c in con[coff[g]:coff[g + 1]]],
+                       np.eye(nc, dtype=np.float32)))
+    return sysm, z, groups
+
+
+def rigid_oracle_steps(sysm, groups, x, v, f, pshake, nevals, time0=0, tol=1e-6):
+    """nevals oracle rigid evaluations from cell-relative state (x, v, f by id); returns the
+    state after each evaluation and the final matrices."""
+    import oracle as O
+    b = O.bin_system(sysm)
+    mass = np.asarray(sysm.masses, np.float64)[sysm.type]
+    out = []
+    for k in range(nevals):
+        x, v, f, mats, it = O.rigid(groups, x, v, f, b["cell"], b["cdim"], b["h"], mass, sysm.dt, tol, pshake,
+                                    (time0 + k) < 20)
+        groups = [(g[0], g[1], m) for g, m in zip(groups, mats)]
+        out.append((x, v, f, np.concatenate([m.reshape(-1) for m in mats]), it))
+    return out
