@@ -270,7 +270,7 @@ def ours(args, rank, world, local_rank):
 
     # ---- launch shape by the autotuner, then CUDA-graph replay of every evaluation
     tgt.load_parts()
-    warps, window, tune_ms = tgt.autotune(reps=3)
+    warps, layout, stages, tune_ms = tgt.autotune(reps=3)
     tgt.graph(True)
     for _ in range(3):                   # direct launch, capture, first replay
         tgt.resident()
@@ -371,8 +371,8 @@ def ours(args, rank, world, local_rank):
             "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
                        "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
                        "tasks": tgt.ntasks(), "cells": ncells, "parallelism": f"replicas x{world}",
-                       "launch": {"warps_per_block": warps, "window": window, "autotune_ms": tune_ms,
-                                  "cuda_graph": True},
+                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
+                                  "staging_buffers": stages, "autotune_ms": tune_ms, "cuda_graph": True},
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
             "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -446,10 +446,16 @@ int engine_cuda_setwindow(struct engine *e, int window);
  * configuration and replays the graph from then on; a new configuration (other slot
  * count, largest cell, buffers, launch shape) is captured anew. */
 int engine_cuda_graph(struct engine *e, int enable);
-/* Times every persistent launch shape (2, 4, 8 worker warps per block x window 4, 8) on
- * the resident particles (uploaded first if none are) and keeps the fastest; returns the
- * chosen shape and its median device time (sort + sweep).  Results stay resident. */
-int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *window, float *ms);
+/* Persistent sweep shape: lane layout 0 = one i particle per lane (32 per warp, the
+ * default), 1 = a tile of 8 i particles x 4 j columns per warp; stages = 1 or 2 staging
+ * buffers per worker warp (2: the next task's bulk copies land while the warp sweeps the
+ * current one).  Same pair set. */
+int engine_cuda_setlayout(struct engine *e, int layout, int stages);
+/* Times every persistent launch shape (2, 4, 8 worker warps per block x lane layout x
+ * staging buffers, window 4) on the resident particles (uploaded first if none are) and
+ * keeps the fastest; returns the chosen shape and its median device time (sort + sweep).
+ * Results stay resident. */
+int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, int *stages, float *ms);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff
@@ -474,7 +480,8 @@ int engine_batch_setstream(struct engine_batch *b, void *stream);
 int engine_batch_kernel_times(struct engine_batch *b, float *total_ms, float *sweep_ms);
 int engine_batch_settune(struct engine_batch *b, int warps, int plain);
 int engine_batch_graph(struct engine_batch *b, int enable);
-int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *window, float *ms);
+int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *layout, int *stages, float *ms);
+int engine_batch_setlayout(struct engine_batch *b, int layout, int stages, int window);
 int engine_batch_ntasks(struct engine_batch *b);
 
 #ifdef __cplusplus

@@ -1,20 +1,20 @@
-// Tuned sweep: persistent CTAs over a device task queue (sm_100a).
+// Persistent sweeps over a device task queue (sm_100a): sweep_tuned (one i particle per
+// lane, 32 per warp) and sweep_tiled (8 i x 4 j lanes per warp).
 //
 // Differences from the plain sweep (nb_kernels.cuh), none of which changes the pair set:
-//  * persistent CTAs (a multiple of the SM count) pull task indices from a device queue
-//    (an atomic counter over a permutation of the task list, so a scheduler can order the
-//    queue, e.g. longest task first); the tables are staged into shared memory once per CTA;
-//  * two shared-memory stages: while a CTA sweeps one task, the TMA bulk copies of the next
-//    task's cells are already in flight;
+//  * persistent blocks (as many as fit on every SM) of independent worker warps: every
+//    warp pops whole tasks from a device queue (an atomic counter over a permutation of the
+//    task list, so a scheduler can order it, e.g. longest task first), stages the j cell
+//    (positions, ids, sort keys) and the i cell's sort keys in its own shared-memory slice
+//    with TMA bulk copies completed on an mbarrier (bounded waits), sweeps the task and
+//    writes its forces; the tables are staged into shared memory once per block;
 //  * f = U'(r) * (1/halfwidth) * rsqrt(r2) with one Newton step instead of an IEEE
 //    division (r itself stays correctly rounded, and the cutoff test uses the exactly
 //    rounded r2);
 //  * Newton's third law through a register reduce-scatter: each lane keeps its j
-//    contributions of 8 consecutive sweep steps and the warp sums them with 9 shuffles per
-//    component (xor 1, 2, 4 exchange halves; xor 8, 16 add), after which lane m holds the
-//    warp total for step m.  The order of additions is fixed, so task partials stay
-//    independent of scheduling;
-//  * the j record carries its sort distance and type in one 16-byte shared-memory word;
+//    contributions of 4 or 8 consecutive sweep steps and one reduce-scatter across the warp
+//    sums them, after which distinct lanes hold the totals of distinct j.  The order of
+//    additions is fixed, so task partials stay independent of scheduling;
 //  * energy is summed per pair in double (float partial sums of cancelling Coulomb terms
 //    would cost ~1e-6 of the total); the virial per particle and task from the partial
 //    forces: sum over pairs of r_ij.F_ij = sum_i (x_i - shift).F_i + sum_j x_j.F_j;
@@ -43,69 +43,6 @@ __device__ __forceinline__ unsigned smid() {
     unsigned r;
     asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
     return r;
-}
-
-// Shared-memory layout of one stage (raw copies of the two cells of a task).
-struct Stage {
-    float4 *xi, *xj;
-    int *pidi, *pidj;
-    unsigned *keyi, *keyj;
-};
-
-__host__ __device__ inline size_t tuned_stage_bytes(int cap) { return (size_t)cap * 48; }
-
-__host__ __device__ inline size_t tuned_smem_bytes(int cap, int nw, int ncoef, int npots, int mt) {
-    size_t b = 64;                                   // 2 mbarriers + queue slots
-    b += 2 * tuned_stage_bytes(cap);                 // double-buffered raw cells
-    b += (size_t)cap * 16 * 2;                       // js (sorted j, dist|type in w), fi
-    b += (size_t)cap * 4 * 3;                        // jid, jloc, jdist
-    b += (size_t)nw * cap * 16;                      // per-warp j partial forces
-    b += (size_t)npots * 16;
-    b += (size_t)((ncoef + 3) & ~3) * 4;
-    b += (size_t)((npots + 3) & ~3) * 4;
-    b += (size_t)((mt * mt + 3) & ~3) * 4;
-    b += (size_t)nw * 16 + (size_t)nw * 32;
-    return b;
-}
-
-__device__ __forceinline__ Stage stage_at(unsigned char* base, int cap, int s) {
-    unsigned char* p = base + (size_t)s * tuned_stage_bytes(cap);
-    Stage st;
-    st.xi = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
-    st.xj = reinterpret_cast<float4*>(p); p += (size_t)cap * 16;
-    st.pidi = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
-    st.pidj = reinterpret_cast<int*>(p); p += (size_t)cap * 4;
-    st.keyi = reinterpret_cast<unsigned*>(p); p += (size_t)cap * 4;
-    st.keyj = reinterpret_cast<unsigned*>(p);
-    return st;
-}
-
-template <bool SELF>
-__device__ __forceinline__ uint32_t stage_bytes(int padi, int padj) {
-    return SELF ? (uint32_t)padj * 20u : (uint32_t)(padi + padj) * 24u;
-}
-
-// Thread 0: issue the bulk copies of task t into stage st.
-__device__ __forceinline__ void issue_task(const Params& P, int t, const Stage& st, uint64_t* bar) {
-    const TaskRec tr = P.tasks[t];
-    const int ni = P.ccount[tr.ci], nj = P.ccount[tr.cj];
-    const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
-    const int si = P.cstart[tr.ci], sj = P.cstart[tr.cj];
-    const bool self = tr.sid < 0;
-    fence_proxy_async();
-    if (ni == 0 || nj == 0) {          // nothing to copy; complete the phase by arrival alone
-        mbar_arrive_expect_tx(bar, 0);
-        return;
-    }
-    mbar_arrive_expect_tx(bar, self ? stage_bytes<true>(padi, padj) : stage_bytes<false>(padi, padj));
-    bulk_g2s(st.xj, P.xq + sj, padj * 16, bar);
-    bulk_g2s(st.pidj, P.pid + sj, padj * 4, bar);
-    if (!self) {
-        bulk_g2s(st.keyj, P.keys + 13 * (size_t)sj + (size_t)tr.sid * padj, padj * 4, bar);
-        bulk_g2s(st.xi, P.xq + si, padi * 16, bar);
-        bulk_g2s(st.pidi, P.pid + si, padi * 4, bar);
-        bulk_g2s(st.keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, bar);
-    }
 }
 
 // Table evaluation with fused multiply-adds (interval index included: a different
@@ -272,11 +209,16 @@ __global__ void __launch_bounds__(kQueueBlock) queue_scatter(const int* __restri
 }
 
 // Shared memory of one worker warp (cap = largest cell rounded up to 4, plus 8 spare rows
-// that the 4- or 8-step sweep windows may read past the end of the j list).
-__host__ __device__ inline size_t warp_slice_bytes(int cap) { return 16 + (size_t)cap * 56; }
+// that the sweep windows may read past the end of the j list): two mbarriers, the j list
+// in sweep order (js, jid, jloc, jdist: 28 B per row) and STAGES staging buffers for the
+// raw bulk copies of a task (xraw, pidraw, keyj, keyi: 28 B per row).  With two stages the
+// copies of the next task land while the warp sweeps the current one.
+__host__ __device__ inline size_t warp_slice_bytes(int cap, int stages) {
+    return 16 + (size_t)cap * 28 * (size_t)(stages + 1);
+}
 
-__host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, int npots, int mt) {
-    size_t b = (size_t)nw * warp_slice_bytes(cap);
+__host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, int npots, int mt, int stages) {
+    size_t b = (size_t)nw * warp_slice_bytes(cap, stages);
     b += (size_t)npots * 16;
     b += (size_t)((ncoef + 3) & ~3) * 4;
     b += (size_t)((npots + 3) & ~3) * 4;
@@ -284,120 +226,431 @@ __host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, i
     return b;
 }
 
-// Persistent worker warps: every warp pops whole tasks from the device queue, stages the
-// j cell (positions, ids, sort keys) and the i cell's sort keys in its own shared-memory
-// slice with TMA bulk copies, sweeps all i chunks of the task itself and writes the
-// task's forces and energy.  Warps never wait for each other.
+// Shared tables (one copy per block, after the warp slices).
+struct SharedTables {
+    float4* potinfo;
+    float* coef;
+    int* potn;
+    int* potidx;
+};
+
+template <int NW, int STAGES>
+__device__ __forceinline__ SharedTables stage_tables(const Params& P, unsigned char* smem_raw, int cap) {
+    SharedTables S;
+    unsigned char* sp = smem_raw + (size_t)NW * warp_slice_bytes(cap, STAGES);
+    S.potinfo = reinterpret_cast<float4*>(sp); sp += (size_t)P.npots * 16;
+    S.coef = reinterpret_cast<float*>(sp); sp += (size_t)((P.ncoef + 3) & ~3) * 4;
+    S.potn = reinterpret_cast<int*>(sp); sp += (size_t)((P.npots + 3) & ~3) * 4;
+    S.potidx = reinterpret_cast<int*>(sp);
+    const int tid = threadIdx.x;
+    for (int k = tid; k < P.ncoef; k += NW * 32) S.coef[k] = P.coef[k];
+    for (int k = tid; k < P.npots; k += NW * 32) { S.potinfo[k] = P.potinfo[k]; S.potn[k] = P.potn[k]; }
+    for (int k = tid; k < P.max_type * P.max_type; k += NW * 32) S.potidx[k] = P.potidx[k];
+    return S;
+}
+
+// One worker warp's shared-memory slice, viewed through staging buffer `stage`.
+struct WarpSlice {
+    uint64_t* bar;      // mbarrier of this stage
+    float4* xraw;       // j cell as copied
+    float4* js;         // j cell in sweep order (w: type bits)
+    float4* fj;         // j (and self) partial forces; aliases xraw once js is built
+    int* pidraw;
+    unsigned* keyj;
+    unsigned* keyi;
+    int* jid;
+    int* jloc;
+    int* jdist;
+};
+
+__device__ __forceinline__ WarpSlice warp_slice(unsigned char* smem_raw, int cap, int warp, int stages, int stage) {
+    unsigned char* wp = smem_raw + (size_t)warp * warp_slice_bytes(cap, stages);
+    WarpSlice W;
+    W.bar = reinterpret_cast<uint64_t*>(wp) + stage;
+    wp += 16;
+    W.js = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;
+    W.jid = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    W.jloc = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    W.jdist = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    wp += (size_t)stage * cap * 28;
+    W.xraw = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;
+    W.fj = W.xraw;
+    W.pidraw = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
+    W.keyj = reinterpret_cast<unsigned*>(wp); wp += (size_t)cap * 4;
+    W.keyi = reinterpret_cast<unsigned*>(wp);
+    return W;
+}
+
+// Pops the next task index of this warp from the device queue (`batch` entries at a time);
+// returns -1 when the queue is drained.
+struct QueueCursor {
+    int q = 0, qend = 0;
+};
+
+__device__ __forceinline__ int pop_task(const TunedParams& T, QueueCursor& c, int nq, int batch, int lane) {
+    if (c.q >= c.qend) {
+        int q0 = 0;
+        if (lane == 0) q0 = atomicAdd(T.counter, batch);
+        c.q = __shfl_sync(0xffffffffu, q0, 0);
+        c.qend = min(c.q + batch, nq);
+        if (c.q >= nq) return -1;
+    }
+    return T.order[c.q++];
+}
+
+// A task as the warp sees it.
+struct TaskDesc {
+    int t;                  // task index, -1 when the queue is drained
+    TaskRec tr;
+    int ni, nj, si, sj;     // particle counts and first slots of cells i and j
+};
+
+// Pops the next task and starts loading its description, spread over the lanes (lane k
+// holds field k: t, ci, cj, sid, dbits, ni, nj, si, sj), so that the dependent loads stay
+// in flight while the warp works on the current task.
+__device__ __forceinline__ int desc_fetch(const Params& P, const TunedParams& T, QueueCursor& c, int nq, int batch,
+                                          int lane) {
+    const int t = pop_task(T, c, nq, batch, lane);
+    if (t < 0) return -1;
+    if (lane == 0) return t;
+    if (lane <= 4) return reinterpret_cast<const int*>(P.tasks + t)[lane - 1];
+    if (lane <= 8) {
+        const int cell = (lane & 1) ? P.tasks[t].ci : P.tasks[t].cj;    // lanes 5, 7: ci; 6, 8: cj
+        return lane <= 6 ? P.ccount[cell] : P.cstart[cell];
+    }
+    return 0;
+}
+
+__device__ __forceinline__ TaskDesc desc_get(int f) {
+    constexpr unsigned FULL = 0xffffffffu;
+    TaskDesc d;
+    d.t = __shfl_sync(FULL, f, 0);
+    d.tr.ci = __shfl_sync(FULL, f, 1);
+    d.tr.cj = __shfl_sync(FULL, f, 2);
+    d.tr.sid = __shfl_sync(FULL, f, 3);
+    d.tr.dbits = __shfl_sync(FULL, f, 4);
+    d.ni = __shfl_sync(FULL, f, 5);
+    d.nj = __shfl_sync(FULL, f, 6);
+    d.si = __shfl_sync(FULL, f, 7);
+    d.sj = __shfl_sync(FULL, f, 8);
+    return d;
+}
+
+// A task with pairs to sweep that fits the slice.
+__device__ __forceinline__ bool desc_runnable(const TaskDesc& d, int cap) {
+    const bool self = d.tr.sid < 0;
+    return d.ni > 0 && d.nj > 0 && !(self && d.ni < 2) && d.ni + 8 <= cap && d.nj + 8 <= cap;
+}
+
+__device__ __forceinline__ bool desc_oversized(const TaskDesc& d, int cap) {
+    return d.ni + 8 > cap || d.nj + 8 > cap;
+}
+
+// Lane 0 issues the bulk copies of task d into the staging buffer of W: the j cell's
+// positions and ids, and for pair tasks the sort keys of both cells along the task's axis.
+__device__ __forceinline__ void issue_copies(const Params& P, const TaskDesc& d, const WarpSlice& W, int lane) {
+    __syncwarp();                      // earlier generic accesses of the buffer are done
+    if (lane == 0) {
+        const bool self = d.tr.sid < 0;
+        const int padi = (d.ni + 3) & ~3, padj = (d.nj + 3) & ~3;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(W.bar, self ? (uint32_t)padj * 20u : (uint32_t)padj * 24u + (uint32_t)padi * 4u);
+        bulk_g2s(W.xraw, P.xq + d.sj, padj * 16, W.bar);
+        bulk_g2s(W.pidraw, P.pid + d.sj, padj * 4, W.bar);
+        if (!self) {
+            bulk_g2s(W.keyj, P.keys + 13 * (size_t)d.sj + (size_t)d.tr.sid * padj, padj * 4, W.bar);
+            bulk_g2s(W.keyi, P.keys + 13 * (size_t)d.si + (size_t)d.tr.sid * padi, padi * 4, W.bar);
+        }
+    }
+}
+
+// After the copies of d landed in W: the j list in sweep order (ascending sort distance
+// for pair tasks, storage order for self tasks) and zeroed j partial forces.
+__device__ __forceinline__ void build_jlist(const TaskDesc& d, const WarpSlice& W, int lane) {
+    const bool self = d.tr.sid < 0;
+    const int nj = d.nj;
+    if (!self) {
+        for (int k = lane; k < nj; k += 32) {
+            const unsigned key = W.keyj[nj - 1 - k];
+            const int loc = key >> 16;
+            W.js[k] = W.xraw[loc];
+            W.jid[k] = W.pidraw[loc];
+            W.jloc[k] = loc;
+            W.jdist[k] = key & 0xffff;
+        }
+    } else {
+        for (int k = lane; k < nj; k += 32) W.js[k] = W.xraw[k];
+    }
+    __syncwarp();
+    const int nout = self ? d.ni : nj;
+    for (int k = lane; k < nout; k += 32) W.fj[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+}
+
+// The task loop of a worker warp: pops tasks, stages them (STAGES = 2: the next task's
+// copies are issued before the current task is swept) and calls
+// sweep(task, slice, t_start) for every task with pairs to sweep.  Returns when the queue
+// is drained or a bulk copy timed out (status set).
 //
-// WIN (4 or 8) is the number of consecutive sweep steps whose j contributions a lane keeps
-// in registers before the warp reduce-scatter: 8 halves the shuffles per step but holds
-// twice the registers.
-template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN>
+// With many tasks per worker warp (at least 16), or two stages, the next task is popped
+// and its description loaded while the current one is swept.  With few, large tasks the
+// warp pops only when it is done: a task reserved early would wait behind the current one
+// while other warps run dry at the end of the queue.
+template <int STAGES, typename Sweep>
+__device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T, unsigned char* smem_raw, int cap,
+                                          int nw, unsigned& status, Sweep&& sweep) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nq = T.qcount ? *T.qcount : P.ntasks;
+    const int workers = (int)gridDim.x * nw;
+    const int batch = max(1, min(16, nq / (8 * workers)));
+    const bool early = STAGES == 2 || nq >= 16 * workers;     // warp-uniform
+    QueueCursor cur;
+    unsigned phases = 0;               // bit s: parity of completed phases of stage s
+    int s = 0;
+    TaskDesc d = desc_get(desc_fetch(P, T, cur, nq, batch, lane));
+    bool issued = d.t >= 0 && desc_runnable(d, cap);
+    if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
+    while (d.t >= 0) {
+        long long t_start = 0;
+        if (T.task_clock && lane == 0) t_start = clock64();
+        int fnext = early ? desc_fetch(P, T, cur, nq, batch, lane) : 0;
+        if (!issued) {                 // empty, single-particle or oversized task
+            if (!early) fnext = desc_fetch(P, T, cur, nq, batch, lane);
+            if (desc_oversized(d, cap)) status |= kStatusCellOverflow;
+            d = desc_get(fnext);
+            issued = d.t >= 0 && desc_runnable(d, cap);
+            if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
+            continue;
+        }
+        const WarpSlice W = warp_slice(smem_raw, cap, warp, STAGES, s);
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(W.bar, (phases >> s) & 1))) {
+            status |= kStatusCopyTimeout;
+            mbar_wait_bounded(W.bar, (phases >> s) & 1);   // second bounded chance for copies in flight
+            return;
+        }
+        phases ^= 1u << s;
+        build_jlist(d, W, lane);
+        bool n_issued = false;
+        if (STAGES == 2) {
+            const TaskDesc n = desc_get(fnext);
+            if (n.t >= 0 && desc_runnable(n, cap)) {
+                issue_copies(P, n, warp_slice(smem_raw, cap, warp, STAGES, s ^ 1), lane);
+                n_issued = true;
+            }
+        }
+        // Only the lane-spread description of the next task (one register) stays live
+        // through the sweep.
+        sweep(d, W, t_start);
+        if (!early) fnext = desc_fetch(P, T, cur, nq, batch, lane);
+        d = desc_get(fnext);
+        if (STAGES == 2) {
+            s ^= 1;
+            issued = n_issued;
+        } else {
+            issued = d.t >= 0 && desc_runnable(d, cap);
+            if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
+        }
+    }
+}
+
+// Length of the sorted j prefix lane's particle i (sort distance di) interacts with: j
+// whose distance is below dmaxdist - dnshift + di (src/runner_dopair.c:606-612).
+__device__ __forceinline__ int sorted_prefix(const int* __restrict__ jdist, int nj, int lim) {
+    int lo = 0, hi = nj;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (jdist[mid] < lim) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// The pair interaction of lane's particle i with j at sweep position k: cutoff test on the
+// exactly rounded r^2, potential lookup, exclusion test, table evaluation.  Returns the
+// force contribution on j (w) and adds -w to the i force; counts candidates, pairs and
+// excluded pairs.
+template <bool HAS_EXCL, bool ONE_POT>
+__device__ __forceinline__ void pair_force(const Params& P, const SharedTables& S, const float4 xj,
+                                           const int* __restrict__ jids, int k, bool act,
+                                           float pix, float piy, float piz, int prow, int pidi, unsigned emask,
+                                           int exlo, int exhi, float cut2, float& fix, float& fiy, float& fiz,
+                                           float& wx, float& wy, float& wz, double& e_task, unsigned& npairs,
+                                           unsigned& nexcl, unsigned& ncand, bool& any_acc) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
+    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    int pot = 0;
+    if (!ONE_POT) pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
+    bool acc = act && pot >= 0 && r2 <= cut2;
+    ncand += act;
+    if (HAS_EXCL && acc) {
+        const int d = jids[k] - pidi;
+        bool ex;
+        if ((unsigned)(d + 16) <= 32u)
+            ex = (emask >> (d + 16 - (d > 0))) & (d != 0);
+        else {
+            ex = false;
+            for (int qx = exlo; qx < exhi; ++qx) ex |= (P.exlist[qx] == pidi + d);
+        }
+        if (ex) { acc = false; ++nexcl; }
+    }
+    wx = 0.f; wy = 0.f; wz = 0.f;
+    if (__any_sync(FULL, acc)) {
+        any_acc = true;
+        if (acc) {
+            // 1/r: rsqrt plus one Newton step; r: r2/r corrected by one residual step,
+            // which gives the correctly rounded square root (the water energy is ~250x
+            // smaller than the sum of |pair energies|, so unbiased 1-ulp errors in r would
+            // show at 1e-6).
+            float rinv = rsqrtf(r2);
+            rinv = fmaf(-0.5f * rinv, fmaf(r2 * rinv, rinv, -1.0f), rinv);
+            float r = r2 * rinv;
+            r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
+            float e, f;
+            const float4 info = S.potinfo[pot];
+            eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
+            wx = f * dx; wy = f * dy; wz = f * dz;
+            fix -= wx; fiy -= wy; fiz -= wz;
+            e_task += (double)e;
+            ++npairs;
+        }
+    }
+}
+
+// End of a task: the j partial forces (and, for self tasks, the i forces) go to the
+// fixed-point accumulators, the j side of the virial is added, the warp sums energy and
+// virial in a fixed order and lane 0 adds them to the i cell (per-task clock64 record).
+__device__ __forceinline__ void finish_task(const Params& P, const TunedParams& T, const WarpSlice& W,
+                                            const TaskDesc& d, double e_task, double v_task, long long t_start,
+                                            unsigned& status, int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool self = d.tr.sid < 0;
+    const int nout = self ? d.ni : d.nj;
+    __syncwarp();
+    for (int k = lane; k < nout; k += 32) {
+        const float4 a = W.fj[k];
+        const float4 xk = W.js[k];
+        v_task += (double)xk.x * a.x + (double)xk.y * a.y + (double)xk.z * a.z;
+        unsigned long long* fp = P.force + 3 * (size_t)(self ? (d.si + k) : (d.sj + W.jloc[k]));
+        atomic_add_fixed(fp + 0, to_fixed(a.x, status));
+        atomic_add_fixed(fp + 1, to_fixed(a.y, status));
+        atomic_add_fixed(fp + 2, to_fixed(a.z, status));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        e_task += __shfl_xor_sync(FULL, e_task, o);
+        v_task += __shfl_xor_sync(FULL, v_task, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&P.cell_epot[d.tr.ci], (unsigned long long)__double2ll_rn(e_task * kEnergyScale));
+        atomicAdd(P.cell_vir ? &P.cell_vir[d.tr.ci] : &P.acc[kAccVirial],
+                  (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
+        if (T.task_clock) {
+            T.task_clock[2 * d.t] = t_start;
+            T.task_clock[2 * d.t + 1] = clock64();
+            T.task_sm[d.t] = (int)smid();
+        }
+    }
+    __syncwarp();
+}
+
+// Warp totals of the counters, one atomic per warp.
+__device__ __forceinline__ void flush_counters(const Params& P, unsigned npairs, unsigned nexcl, unsigned ncand,
+                                               unsigned status, int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        npairs += __shfl_xor_sync(FULL, npairs, o);
+        nexcl += __shfl_xor_sync(FULL, nexcl, o);
+        ncand += __shfl_xor_sync(FULL, ncand, o);
+        status |= __shfl_xor_sync(FULL, status, o);
+    }
+    if (lane == 0) {
+        if (npairs) atomicAdd(&P.acc[kAccPairs], (unsigned long long)npairs);
+        if (nexcl) atomicAdd(&P.acc[kAccExcl], (unsigned long long)nexcl);
+        if (ncand) atomicAdd(&P.acc[kAccCand], (unsigned long long)ncand);
+        if (status) atomicOr(&P.acc[kAccStatus], (unsigned long long)status);
+    }
+}
+
+
+
+
+// Warp reduce-scatter over the 8 i rows of the 8 x 4 lane tile (lane = 4 * row + column):
+// each lane holds WIN values (window steps m); afterwards the lane of row q holds, for its
+// column, the sum over the 8 rows of step m = q (WIN = 8) or m = q & 3 (WIN = 4).  Fixed
+// order of additions.
+template <int WIN>
+__device__ __forceinline__ float reduce_scatter_rows(const float (&v)[WIN], int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool b2 = lane & 4, b3 = lane & 8, b4 = lane & 16;
+    if constexpr (WIN == 8) {
+        float a[4], c[2];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const float send = b2 ? v[2 * m] : v[2 * m + 1];
+            const float keep = b2 ? v[2 * m + 1] : v[2 * m];
+            a[m] = keep + __shfl_xor_sync(FULL, send, 4);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const float send = b3 ? a[2 * m] : a[2 * m + 1];
+            const float keep = b3 ? a[2 * m + 1] : a[2 * m];
+            c[m] = keep + __shfl_xor_sync(FULL, send, 8);
+        }
+        const float send = b4 ? c[0] : c[1];
+        const float keep = b4 ? c[1] : c[0];
+        return keep + __shfl_xor_sync(FULL, send, 16);
+    } else {
+        float a[2];
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const float send = b2 ? v[2 * m] : v[2 * m + 1];
+            const float keep = b2 ? v[2 * m + 1] : v[2 * m];
+            a[m] = keep + __shfl_xor_sync(FULL, send, 4);
+        }
+        const float send = b3 ? a[0] : a[1];
+        const float keep = b3 ? a[1] : a[0];
+        float c = keep + __shfl_xor_sync(FULL, send, 8);
+        c += __shfl_xor_sync(FULL, c, 16);
+        return c;
+    }
+}
+
+// Persistent worker warps, one i particle per lane: every warp pops whole tasks from the
+// device queue, stages them in its own shared-memory slice and sweeps the i particles in
+// chunks of 32; the j contributions of WIN consecutive sweep steps are kept per lane and
+// summed across the warp by one reduce-scatter.  Warps never wait for each other.
+//
+// WIN (4 or 8): sweep steps per reduce-scatter; 8 halves the shuffles per step but holds
+// twice the registers.  STAGES (1 or 2): staging buffers per warp.
+template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES>
 __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const Params& P = T.p;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = P.max_type;
-
-    // ---- shared tables (once per block), then the warp's slice
-    unsigned char* sp = smem_raw + (size_t)NW * warp_slice_bytes(cap);
-    float4* potinfo = reinterpret_cast<float4*>(sp); sp += (size_t)P.npots * 16;
-    float* coef = reinterpret_cast<float*>(sp); sp += (size_t)((P.ncoef + 3) & ~3) * 4;
-    int* potn = reinterpret_cast<int*>(sp); sp += (size_t)((P.npots + 3) & ~3) * 4;
-    int* potidx = reinterpret_cast<int*>(sp);
-    for (int k = tid; k < P.ncoef; k += NW * 32) coef[k] = P.coef[k];
-    for (int k = tid; k < P.npots; k += NW * 32) { potinfo[k] = P.potinfo[k]; potn[k] = P.potn[k]; }
-    for (int k = tid; k < mt * mt; k += NW * 32) potidx[k] = P.potidx[k];
-
-    unsigned char* wp = smem_raw + (size_t)warp * warp_slice_bytes(cap);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(wp); wp += 16;
-    float4* xraw = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;   // j cell as copied
-    float4* js = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;     // j cell, sweep order
-    float4* fj = xraw;            // j (and self) forces, once js has been built from xraw
-    int* pidraw = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
-    unsigned* keyj = reinterpret_cast<unsigned*>(wp); wp += (size_t)cap * 4;
-    unsigned* keyi = reinterpret_cast<unsigned*>(wp); wp += (size_t)cap * 4;
-    int* jid = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
-    int* jloc = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
-    int* jdist = reinterpret_cast<int*>(wp);
-    if (lane == 0) {
-        mbar_init(bar, 1);
+    const SharedTables S = stage_tables<NW, STAGES>(P, smem_raw, cap);
+    if (lane < STAGES) {
+        mbar_init(warp_slice(smem_raw, cap, warp, STAGES, lane).bar, 1);
         mbar_fence_init();
     }
     __syncthreads();
 
     unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
-    unsigned phase = 0;                   // completed phases of this warp's mbarrier
-    const int nq = T.qcount ? *T.qcount : P.ntasks;
-    // Queue entries are taken `batch` at a time: one when there are few tasks per worker
-    // (load balance), up to 16 on systems with millions of small tasks (the queue head is
-    // a single atomic counter).
-    const int workers = gridDim.x * NW;
-    const int batch = max(1, min(16, nq / (8 * workers)));
-    int q = 0, qend = 0;
-    for (;;) {
-        if (q >= qend) {
-            int q0 = 0;
-            if (lane == 0) q0 = atomicAdd(T.counter, batch);
-            q = __shfl_sync(FULL, q0, 0);
-            qend = min(q + batch, nq);
-            if (q >= nq) break;
-        }
-        const int t = T.order[q++];
-        const TaskRec tr = P.tasks[t];
-        const bool self = tr.sid < 0;
-        const int ni = P.ccount[tr.ci], nj = P.ccount[tr.cj];
-        if (ni == 0 || nj == 0 || (self && ni < 2)) continue;
-        if (ni + 8 > cap || nj + 8 > cap) { status |= kStatusCellOverflow; continue; }
-        const int si = P.cstart[tr.ci], sj = P.cstart[tr.cj];
-        const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
-        long long t_start = 0;
-        __syncwarp();
-        if (lane == 0) {
-            if (T.task_clock) t_start = clock64();
-            fence_proxy_async();
-            mbar_arrive_expect_tx(bar, self ? (uint32_t)padj * 20u : (uint32_t)padj * 24u + (uint32_t)padi * 4u);
-            bulk_g2s(xraw, P.xq + sj, padj * 16, bar);
-            bulk_g2s(pidraw, P.pid + sj, padj * 4, bar);
-            if (!self) {
-                bulk_g2s(keyj, P.keys + 13 * (size_t)sj + (size_t)tr.sid * padj, padj * 4, bar);
-                bulk_g2s(keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, bar);
-            }
-        }
-        const int nout = self ? ni : nj;
-        if (!__all_sync(FULL, mbar_wait_bounded(bar, phase & 1))) {
-            status |= kStatusCopyTimeout;
-            mbar_wait_bounded(bar, phase & 1);   // second bounded chance for copies in flight
-            break;
-        }
-        ++phase;
-        if (!self) {
-            for (int k = lane; k < nj; k += 32) {
-                const unsigned key = keyj[nj - 1 - k];
-                const int loc = key >> 16;
-                js[k] = xraw[loc];
-                jid[k] = pidraw[loc];
-                jloc[k] = loc;
-                jdist[k] = key & 0xffff;
-            }
-        } else {
-            for (int k = lane; k < nj; k += 32) js[k] = xraw[k];
-        }
-        __syncwarp();
-        for (int k = lane; k < nout; k += 32) fj[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncwarp();
-        const float4* __restrict__ jpos = js;
-        const int* __restrict__ jids = self ? pidraw : jid;
-
-        const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
+    run_tasks<STAGES>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+        const bool self = d.tr.sid < 0;
+        const int ni = d.ni, nj = d.nj, si = d.si;
+        const float4* __restrict__ jpos = W.js;
+        const int* __restrict__ jids = self ? W.pidraw : W.jid;
+        const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
-        const int dnshift = task_dnshift(tr);
-        const int dmaxdist = task_dmax(tr);
+        const int dnshift = task_dnshift(d.tr);
+        const int dmaxdist = task_dmax(d.tr);
         double e_task = 0.0, v_task = 0.0;
         const int nchunks = (ni + 31) >> 5;
-        const int jd0 = self ? 0 : jdist[0];
+        const int jd0 = self ? 0 : W.jdist[0];
 
         for (int ch = 0; ch < nchunks; ++ch) {
             const int ii = ch * 32 + lane;
@@ -406,33 +659,21 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
             if (self) {
                 len = valid ? ii : 0;                       // pairs j < i
             } else {
-                const unsigned key = valid ? keyi[ii] : 0u;
+                const unsigned key = valid ? W.keyi[ii] : 0u;
                 loc = key >> 16;
                 const int di = key & 0xffff;
                 if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
                 if (!__any_sync(FULL, valid)) break;        // later chunks lie farther from cell j
-                if (valid) {
-                    if (P.unsorted) {
-                        len = nj;
-                    } else {                                // j with dist < lim form a prefix
-                        const int lim = dmaxdist - dnshift + di;
-                        int lo = 0, hi = nj;
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (jdist[mid] < lim) lo = mid + 1; else hi = mid;
-                        }
-                        len = lo;
-                    }
-                }
+                if (valid) len = P.unsorted ? nj : sorted_prefix(W.jdist, nj, dmaxdist - dnshift + di);
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
             int pidi = 0, exlo = 0, exhi = 0;
             unsigned emask = 0u;
             if (valid) {
-                xi = self ? js[loc] : P.xq[si + loc];
+                xi = self ? W.js[loc] : P.xq[si + loc];
                 if (HAS_EXCL) {
-                    pidi = self ? pidraw[loc] : P.pid[si + loc];
+                    pidi = self ? W.pidraw[loc] : P.pid[si + loc];
                     emask = P.emask[pidi];
                     exlo = P.exoff[pidi];
                     exhi = P.exoff[pidi + 1];
@@ -447,47 +688,9 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
 #pragma unroll
                 for (int m = 0; m < WIN; ++m) {
                     const int k = k0 + m;
-                    const float4 xj = jpos[k];
-                    const bool act = k < len;
-                    const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
-                    const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                    int pot = 0;
-                    if (!ONE_POT) pot = act ? potidx[prow + __float_as_int(xj.w)] : -1;
-                    bool acc = act && pot >= 0 && r2 <= cut2;
-                    ncand += act;
-                    if (HAS_EXCL && acc) {
-                        const int d = jids[k] - pidi;
-                        bool ex;
-                        if ((unsigned)(d + 16) <= 32u)
-                            ex = (emask >> (d + 16 - (d > 0))) & (d != 0);
-                        else {
-                            ex = false;
-                            for (int qx = exlo; qx < exhi; ++qx) ex |= (P.exlist[qx] == pidi + d);
-                        }
-                        if (ex) { acc = false; ++nexcl; }
-                    }
-                    float wx = 0.f, wy = 0.f, wz = 0.f;
-                    if (__any_sync(FULL, acc)) {
-                        any_acc = true;
-                        if (acc) {
-                            // 1/r: rsqrt plus one Newton step; r: r2/r corrected by one
-                            // residual step, which gives the correctly rounded square root
-                            // (the water energy is ~250x smaller than the sum of |pair
-                            // energies|, so unbiased 1-ulp errors in r would show at 1e-6).
-                            float rinv = rsqrtf(r2);
-                            rinv = fmaf(-0.5f * rinv, fmaf(r2 * rinv, rinv, -1.0f), rinv);
-                            float r = r2 * rinv;
-                            r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
-                            float e, f;
-                            const float4 info = potinfo[pot];
-                            eval_table_fast(coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
-                            wx = f * dx; wy = f * dy; wz = f * dz;
-                            fix -= wx; fiy -= wy; fiz -= wz;
-                            e_task += (double)e;
-                            ++npairs;
-                        }
-                    }
-                    vx[m] = wx; vy[m] = wy; vz[m] = wz;
+                    pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, pidi, emask,
+                                                  exlo, exhi, cut2, fix, fiy, fiz, vx[m], vy[m], vz[m], e_task,
+                                                  npairs, nexcl, ncand, any_acc);
                 }
                 if (any_acc) {
                     float tx, ty, tz;
@@ -501,18 +704,18 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
                         tz = reduce_scatter4(vz, lane);
                     }
                     if (lane < WIN && k0 + lane < kmax) {
-                        float4 a = fj[k0 + lane];
+                        float4 a = W.fj[k0 + lane];
                         a.x += tx; a.y += ty; a.z += tz;
-                        fj[k0 + lane] = a;
+                        W.fj[k0 + lane] = a;
                     }
                 }
             }
             __syncwarp();
             if (valid) {
                 if (self) {
-                    float4 a = fj[loc];
+                    float4 a = W.fj[loc];
                     a.x += fix; a.y += fiy; a.z += fiz;
-                    fj[loc] = a;
+                    W.fj[loc] = a;
                 } else {
                     // virial, i side: sum over pairs of r_ij.F_ij = sum_i (x_i - shift).F_i + sum_j x_j.F_j
                     v_task += (double)pix * fix + (double)piy * fiy + (double)piz * fiz;
@@ -524,47 +727,131 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
             }
             __syncwarp();
         }
+        finish_task(P, T, W, d, e_task, v_task, t_start, status, lane);
+    });
+    flush_counters(P, npairs, nexcl, ncand, status, lane);
+}
 
-        for (int k = lane; k < nout; k += 32) {
-            const float4 a = fj[k];
-            const float4 xk = jpos[k];
-            v_task += (double)xk.x * a.x + (double)xk.y * a.y + (double)xk.z * a.z;
-            unsigned long long* fp = P.force + 3 * (size_t)(self ? (si + k) : (sj + jloc[k]));
-            atomic_add_fixed(fp + 0, to_fixed(a.x, status));
-            atomic_add_fixed(fp + 1, to_fixed(a.y, status));
-            atomic_add_fixed(fp + 2, to_fixed(a.z, status));
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            e_task += __shfl_xor_sync(FULL, e_task, o);
-            v_task += __shfl_xor_sync(FULL, v_task, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&P.cell_epot[tr.ci], (unsigned long long)__double2ll_rn(e_task * kEnergyScale));
-            atomicAdd(P.cell_vir ? &P.cell_vir[tr.ci] : &P.acc[kAccVirial],
-                      (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
-            if (T.task_clock) {
-                T.task_clock[2 * t] = t_start;
-                T.task_clock[2 * t + 1] = clock64();
-                T.task_sm[t] = (int)smid();
+// Persistent worker warps on an 8 x 4 lane tile: lane 4 q + c sweeps i particle q of a
+// strip of 8 consecutive i (in sort order) against the j of its column c, j = k0 + 4 m + c.
+// Eight i of neighbouring sort distance have similar sorted-prefix lengths, so far fewer
+// lane slots fall outside a particle's prefix than with 32 i per warp (on ~20-particle
+// cells about 0.6 of the lane slots carry a candidate instead of ~0.25).  The j
+// contributions of WIN steps (4 WIN consecutive j) are summed over the 8 rows by one
+// reduce-scatter, after which the 32 (or 16) lanes write distinct j; the i forces are
+// summed over the 4 columns at the end of the strip.
+template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES>
+__global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tiled(TunedParams T, int cap) {
+    static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr unsigned FULL = 0xffffffffu;
+    const Params& P = T.p;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = lane >> 2, col = lane & 3;
+    const int mt = P.max_type;
+    const SharedTables S = stage_tables<NW, STAGES>(P, smem_raw, cap);
+    if (lane < STAGES) {
+        mbar_init(warp_slice(smem_raw, cap, warp, STAGES, lane).bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
+    run_tasks<STAGES>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+        const bool self = d.tr.sid < 0;
+        const int ni = d.ni, nj = d.nj, si = d.si;
+        const float4* __restrict__ jpos = W.js;
+        const int* __restrict__ jids = self ? W.pidraw : W.jid;
+        const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
+        const float cut2 = self ? P.cutoff2s : P.cutoff2;
+        const int dnshift = task_dnshift(d.tr);
+        const int dmaxdist = task_dmax(d.tr);
+        double e_task = 0.0, v_task = 0.0;
+        const int nstrips = (ni + 7) >> 3;
+        const int jd0 = self ? 0 : W.jdist[0];
+
+        for (int st = 0; st < nstrips; ++st) {
+            const int ii = st * 8 + row;
+            bool valid = ii < ni;
+            int loc = ii, len = 0;
+            if (self) {
+                len = valid ? ii : 0;                       // pairs j < i
+            } else {
+                const unsigned key = valid ? W.keyi[ii] : 0u;
+                loc = key >> 16;
+                const int di = key & 0xffff;
+                if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
+                if (!__any_sync(FULL, valid)) break;        // later strips lie farther from cell j
+                if (valid) len = P.unsorted ? nj : sorted_prefix(W.jdist, nj, dmaxdist - dnshift + di);
             }
-        }
-    }
-
-    // Counters: warp sums, one atomic per warp.
+            const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
+            float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+            int pidi = 0, exlo = 0, exhi = 0;
+            unsigned emask = 0u;
+            if (valid) {
+                xi = self ? W.js[loc] : P.xq[si + loc];
+                if (HAS_EXCL) {
+                    pidi = self ? W.pidraw[loc] : P.pid[si + loc];
+                    emask = P.emask[pidi];
+                    exlo = P.exoff[pidi];
+                    exhi = P.exoff[pidi + 1];
+                }
+            }
+            const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
+            const int prow = __float_as_int(xi.w) * mt;
+            float fix = 0.f, fiy = 0.f, fiz = 0.f;
+            for (int k0 = 0; k0 < kmax; k0 += 4 * WIN) {
+                float vx[WIN], vy[WIN], vz[WIN];
+                bool any_acc = false;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        npairs += __shfl_xor_sync(FULL, npairs, o);
-        nexcl += __shfl_xor_sync(FULL, nexcl, o);
-        ncand += __shfl_xor_sync(FULL, ncand, o);
-        status |= __shfl_xor_sync(FULL, status, o);
-    }
-    if (lane == 0) {
-        if (npairs) atomicAdd(&P.acc[kAccPairs], (unsigned long long)npairs);
-        if (nexcl) atomicAdd(&P.acc[kAccExcl], (unsigned long long)nexcl);
-        if (ncand) atomicAdd(&P.acc[kAccCand], (unsigned long long)ncand);
-        if (status) atomicOr(&P.acc[kAccStatus], (unsigned long long)status);
-    }
+                for (int m = 0; m < WIN; ++m) {
+                    if (k0 + 4 * m < kmax) {                 // warp-uniform
+                        const int k = k0 + 4 * m + col;
+                        pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, pidi,
+                                                      emask, exlo, exhi, cut2, fix, fiy, fiz, vx[m], vy[m], vz[m],
+                                                      e_task, npairs, nexcl, ncand, any_acc);
+                    } else {
+                        vx[m] = 0.f; vy[m] = 0.f; vz[m] = 0.f;
+                    }
+                }
+                if (any_acc) {
+                    const float tx = reduce_scatter_rows<WIN>(vx, lane);
+                    const float ty = reduce_scatter_rows<WIN>(vy, lane);
+                    const float tz = reduce_scatter_rows<WIN>(vz, lane);
+                    const int k = k0 + 4 * (WIN == 8 ? row : (row & 3)) + col;
+                    if ((WIN == 8 || row < 4) && k < kmax) {
+                        float4 a = W.fj[k];
+                        a.x += tx; a.y += ty; a.z += tz;
+                        W.fj[k] = a;
+                    }
+                }
+            }
+            // i force: sum over the 4 columns
+            fix += __shfl_xor_sync(FULL, fix, 1);
+            fiy += __shfl_xor_sync(FULL, fiy, 1);
+            fiz += __shfl_xor_sync(FULL, fiz, 1);
+            fix += __shfl_xor_sync(FULL, fix, 2);
+            fiy += __shfl_xor_sync(FULL, fiy, 2);
+            fiz += __shfl_xor_sync(FULL, fiz, 2);
+            __syncwarp();
+            if (valid && col == 0) {
+                if (self) {
+                    float4 a = W.fj[loc];
+                    a.x += fix; a.y += fiy; a.z += fiz;
+                    W.fj[loc] = a;
+                } else {
+                    v_task += (double)pix * fix + (double)piy * fiy + (double)piz * fiz;
+                    unsigned long long* fp = P.force + 3 * (size_t)(si + loc);
+                    atomic_add_fixed(fp + 0, to_fixed(fix, status));
+                    atomic_add_fixed(fp + 1, to_fixed(fiy, status));
+                    atomic_add_fixed(fp + 2, to_fixed(fiz, status));
+                }
+            }
+            __syncwarp();
+        }
+        finish_task(P, T, W, d, e_task, v_task, t_start, status, lane);
+    });
+    flush_counters(P, npairs, nexcl, ncand, status, lane);
 }
 
 }  // namespace nb

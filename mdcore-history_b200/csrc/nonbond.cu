@@ -55,6 +55,8 @@ struct NbState {
     // tuning
     int warps = 4;
     int window = 4;                // sweep steps per register reduce-scatter (4 or 8)
+    int layout = 0;                // persistent sweep: 0 = 32 i per warp, 1 = 8 i x 4 j tile
+    int stages = 1;                // staging buffers per worker warp (2: next task's copies in flight)
     bool has_excl = false;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
@@ -255,9 +257,9 @@ int launch_plain(NbState* st, const Params& P, int cap) {
 // Persistent launch: as many CTAs as fit on every SM at once.  Under stream capture the
 // function attribute and occupancy query are skipped and the grid of the preceding direct
 // launch of the same configuration is reused.
-template <int NW, bool EX, bool ONE, int WIN>
+template <int NW, bool EX, bool ONE, int WIN, int LAY, int STG>
 int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    auto kern = sweep_tuned<NW, EX, ONE, WIN>;
+    auto kern = LAY ? sweep_tiled<NW, EX, ONE, WIN, STG> : sweep_tuned<NW, EX, ONE, WIN, STG>;
     int grid = st->last_grid;
     if (!st->capturing) {
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -272,24 +274,33 @@ int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
     return 0;
 }
 
-template <int NW, int WIN>
+template <int NW, int WIN, int LAY, int STG>
 int launch_tuned_w(NbState* st, const TunedParams& T, int cap, size_t smem) {
     const bool one = st->one_pot;
     if (st->has_excl)
-        return one ? launch_tuned_nw<NW, true, true, WIN>(st, T, cap, smem)
-                   : launch_tuned_nw<NW, true, false, WIN>(st, T, cap, smem);
-    return one ? launch_tuned_nw<NW, false, true, WIN>(st, T, cap, smem)
-               : launch_tuned_nw<NW, false, false, WIN>(st, T, cap, smem);
+        return one ? launch_tuned_nw<NW, true, true, WIN, LAY, STG>(st, T, cap, smem)
+                   : launch_tuned_nw<NW, true, false, WIN, LAY, STG>(st, T, cap, smem);
+    return one ? launch_tuned_nw<NW, false, true, WIN, LAY, STG>(st, T, cap, smem)
+               : launch_tuned_nw<NW, false, false, WIN, LAY, STG>(st, T, cap, smem);
 }
 
-template <int WIN>
+// Worker warps per block: 2, 4 or 8 (two warps fit even the largest cells).
+template <int WIN, int LAY, int STG>
 int launch_tuned_win(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
     switch (nw) {
-        case 1: return launch_tuned_w<1, WIN>(st, T, cap, smem);
-        case 2: return launch_tuned_w<2, WIN>(st, T, cap, smem);
-        case 8: return launch_tuned_w<8, WIN>(st, T, cap, smem);
-        default: return launch_tuned_w<4, WIN>(st, T, cap, smem);
+        case 2: return launch_tuned_w<2, WIN, LAY, STG>(st, T, cap, smem);
+        case 8: return launch_tuned_w<8, WIN, LAY, STG>(st, T, cap, smem);
+        default: return launch_tuned_w<4, WIN, LAY, STG>(st, T, cap, smem);
     }
+}
+
+template <int STG>
+int launch_tuned_stg(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
+    if (st->layout)
+        return st->window == 8 ? launch_tuned_win<8, 1, STG>(st, T, cap, smem, nw)
+                               : launch_tuned_win<4, 1, STG>(st, T, cap, smem, nw);
+    return st->window == 8 ? launch_tuned_win<8, 0, STG>(st, T, cap, smem, nw)
+                           : launch_tuned_win<4, 0, STG>(st, T, cap, smem, nw);
 }
 
 int launch_tuned(NbState* st, const Params& P, int cap4) {
@@ -312,18 +323,18 @@ int launch_tuned(NbState* st, const Params& P, int cap4) {
     T.task_clock = st->record_clock ? st->d_task_clock : nullptr;
     T.task_sm = st->record_clock ? st->d_task_sm : nullptr;
     CU(cudaMemsetAsync(st->d_counter, 0, sizeof(int), st->stream));
-    int nw = st->warps;
-    size_t smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
-    while (smem > 200 * 1024 && nw > 1) {
+    int nw = st->warps < 2 ? 2 : st->warps;
+    size_t smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type, st->stages);
+    while (smem > 200 * 1024 && nw > 2) {
         nw /= 2;
-        smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+        smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type, st->stages);
     }
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
                       __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
-    return st->window == 8 ? launch_tuned_win<8>(st, T, cap, smem, nw) : launch_tuned_win<4>(st, T, cap, smem, nw);
+    return st->stages == 2 ? launch_tuned_stg<2>(st, T, cap, smem, nw) : launch_tuned_stg<1>(st, T, cap, smem, nw);
 }
 
 // Records an event; inside a stream capture as an external record node, so that replaying
@@ -397,6 +408,8 @@ long long launch_key(const NbState* st) {
     k = k * 131 + st->buf_gen;
     k = k * 17 + st->warps;
     k = k * 17 + st->window;
+    k = k * 3 + st->layout;
+    k = k * 3 + st->stages;
     k = k * 3 + st->plain;
     k = k * 3 + st->record_clock;
     return k;
@@ -831,10 +844,11 @@ int st_settune(NbState* st, int warps, int plain) {
     return 0;
 }
 
-// Times every persistent launch shape (worker warps per CTA x sweep window) on the
-// resident particles, `reps` evaluations each after one warm-up, and keeps the fastest
-// (median device time of sort + sweep).  Every shape computes the same forces.
-int st_autotune(NbState* st, int reps, int* warps_out, int* window_out, float* ms_out) {
+// Times every persistent launch shape (worker warps per block x lane layout x staging
+// buffers per warp) on the resident particles, `reps` evaluations each after one warm-up,
+// and keeps the fastest (median device time of sort + sweep).  Every shape computes the
+// same pair set and forces within FP32 rounding.
+int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* stages_out, float* ms_out) {
     if (!st->resident_valid) {
         const int rc = st_load_parts(st);
         if (rc < 0) return rc;
@@ -844,12 +858,17 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* window_out, float* m
     const bool graph = st->use_graph;
     st->use_graph = false;
     st->plain = 0;
-    static const int shapes[][2] = {{2, 4}, {2, 8}, {4, 4}, {4, 8}, {8, 4}, {8, 8}};
+    // warps, layout, stages (window 4: the 8-step window was never the fastest shape)
+    static const int shapes[][3] = {{2, 0, 1}, {4, 0, 1}, {8, 0, 1}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1},
+                                    {2, 0, 2}, {4, 0, 2}, {8, 0, 2}, {2, 1, 2}, {4, 1, 2}, {8, 1, 2}};
+    const int nshapes = sizeof(shapes) / sizeof(shapes[0]);
     int best = -1;
     float best_ms = 0.f;
-    for (int k = 0; k < 6; k++) {
+    for (int k = 0; k < nshapes; k++) {
         st->warps = shapes[k][0];
-        st->window = shapes[k][1];
+        st->layout = shapes[k][1];
+        st->stages = shapes[k][2];
+        st->window = 4;
         std::vector<float> t;
         for (int r = 0; r <= reps; r++) {
             int rc = st_resident(st);
@@ -870,12 +889,15 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* window_out, float* m
         }
     }
     st->warps = shapes[best][0];
-    st->window = shapes[best][1];
+    st->layout = shapes[best][1];
+    st->stages = shapes[best][2];
+    st->window = 4;
     st->use_graph = graph;
     const int rc = st_resident(st);           // leave the chosen shape's results resident
     if (rc < 0) return rc;
     if (warps_out) *warps_out = st->warps;
-    if (window_out) *window_out = st->window;
+    if (layout_out) *layout_out = st->layout;
+    if (stages_out) *stages_out = st->stages;
     if (ms_out) *ms_out = best_ms;
     return 0;
 }
@@ -928,6 +950,14 @@ extern "C" int engine_cuda_setwindow(struct engine* e, int window) {
     return 0;
 }
 
+extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2)) return engine_err_range;
+    state(e)->layout = layout;
+    state(e)->stages = stages;
+    return 0;
+}
+
 extern "C" int engine_cuda_graph(struct engine* e, int enable) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     NbState* st = state(e);
@@ -937,9 +967,9 @@ extern "C" int engine_cuda_graph(struct engine* e, int enable) {
     return 0;
 }
 
-extern "C" int engine_cuda_autotune(struct engine* e, int reps, int* warps, int* window, float* ms) {
+extern "C" int engine_cuda_autotune(struct engine* e, int reps, int* warps, int* layout, int* stages, float* ms) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    return st_autotune(state(e), reps, warps, window, ms);
+    return st_autotune(state(e), reps, warps, layout, stages, ms);
 }
 
 extern "C" int engine_cuda_load(struct engine* e) {
@@ -1106,9 +1136,20 @@ extern "C" int engine_batch_graph(struct engine_batch* b, int enable) {
     return 0;
 }
 
-extern "C" int engine_batch_autotune(struct engine_batch* b, int reps, int* warps, int* window, float* ms) {
+extern "C" int engine_batch_autotune(struct engine_batch* b, int reps, int* warps, int* layout, int* stages,
+                                     float* ms) {
     if (b == nullptr) return engine_err_null;
-    return st_autotune(bstate(b), reps, warps, window, ms);
+    return st_autotune(bstate(b), reps, warps, layout, stages, ms);
+}
+
+extern "C" int engine_batch_setlayout(struct engine_batch* b, int layout, int stages, int window) {
+    if (b == nullptr) return engine_err_null;
+    if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2) || (window != 4 && window != 8))
+        return engine_err_range;
+    bstate(b)->layout = layout;
+    bstate(b)->stages = stages;
+    bstate(b)->window = window;
+    return 0;
 }
 
 extern "C" int engine_batch_ntasks(struct engine_batch* b) {
@@ -1304,7 +1345,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     T.task_clock = nullptr;
     T.task_sm = nullptr;
     const int cap = cap4 + 8;
-    const size_t smem = warps_smem_bytes(cap, 4, st->ncoef, st->npots, st->max_type);
+    const size_t smem = warps_smem_bytes(cap, 4, st->ncoef, st->npots, st->max_type, 1);
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
                       __func__, __FILE__);
@@ -1314,7 +1355,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const bool cap_saved = st->capturing;
     st->stream = s;
     st->capturing = false;
-    const int rc = launch_tuned_w<4, 4>(st, T, cap, smem);
+    const int rc = launch_tuned_w<4, 4, 0, 1>(st, T, cap, smem);
     st->stream = saved;
     st->capturing = cap_saved;
     return rc;

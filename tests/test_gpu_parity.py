@@ -205,17 +205,35 @@ def test_graph_replay_bit_identical(fname):
     e.close()
 
 
+@pytest.mark.parametrize("stages", [1, 2])
+@pytest.mark.parametrize("layout", [0, 1], ids=["32i", "8x4"])
 @pytest.mark.parametrize("window", [4, 8])
 @pytest.mark.parametrize("warps", [2, 4, 8])
-def test_sweep_window_bit_identical(warps, window):
-    """The sweep window only changes how j partials are reduced across the warp, so every
-    launch shape gives the same pair set and forces within FP32 rounding."""
-    sysm, ref = load_golden("water_3000.npz")
+@pytest.mark.parametrize("fname", SYSTEMS)
+def test_persistent_launch_shapes(fname, warps, window, layout, stages):
+    """Lane layout and sweep window only change how pairs are spread over lanes and how j
+    partials are reduced across the warp: every launch shape gives the same pair set and
+    forces within FP32 rounding."""
+    sysm, ref = load_golden(fname)
     e = M.Engine.from_system(sysm)
     e.tune(warps)
     e.set_window(window)
+    e.set_layout(layout, stages)
     e.nonbond()
-    check_against_oracle(sysm, ref["tables"], e.forces(), e.stats(), f"warps={warps} window={window}")
+    check_against_oracle(sysm, ref["tables"], e.forces(), e.stats(),
+                         f"warps={warps} window={window} layout={layout} stages={stages}")
+    e.close()
+
+
+@pytest.mark.parametrize("make", [lambda: W.argon_fcc(20), lambda: W.water_spce(32), lambda: W.lj_slab()],
+                         ids=["argon-32000", "water-98304", "slab-1048576"])
+def test_full_size_tiled_layout_vs_oracle(make):
+    sysm = make()
+    tables = [M.create_potential(p).contents.table() for p in sysm.pots]
+    e = M.Engine.from_system(sysm)
+    e.set_layout(1, 2)
+    e.nonbond()
+    check_against_oracle(sysm, tables, e.forces(), e.stats(), sysm.name + " 8x4, 2 stages")
     e.close()
 
 
@@ -223,8 +241,8 @@ def test_autotune_keeps_results():
     sysm, ref = load_golden("water_3000.npz")
     e = M.Engine.from_system(sysm)
     e.load_parts()
-    warps, window, ms = e.autotune(reps=3)
-    assert warps in (2, 4, 8) and window in (4, 8) and ms > 0
+    warps, layout, stages, ms = e.autotune(reps=3)
+    assert warps in (2, 4, 8) and layout in (0, 1) and stages in (1, 2) and ms > 0
     e.unload_parts()
     check_against_oracle(sysm, ref["tables"], e.forces(), e.stats(), "autotuned")
     e.close()
