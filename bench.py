@@ -49,14 +49,14 @@ def ns_per_day(ms_per_step):
 WORKLOADS = {
     "water": ("rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, 9x9x9 cells, "
               "cutoff 1.0 nm, 98,304 exclusions, seeded", lambda W: W.water_spce(32),
-              "sweep_tuned_water98k_traffic.txt"),
+              "sweep_water98k_traffic.txt"),
     "slab": ("LJ liquid slab in vapour, 1,048,576 atoms (80/20 two types) in a 40x40x160 nm box, 40x40x160 cells, "
-             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab(), "sweep_tuned_slab1m_traffic.txt"),
+             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab(), "sweep_slab1m_traffic.txt"),
     "argon": ("LJ argon, 32,000 atoms on a jittered FCC lattice in an 11.5074 nm box, 11^3 cells, cutoff 1.0 nm, "
-              "seeded", lambda W: W.argon_fcc(20), "sweep_tuned_argon32k_traffic.txt"),
+              "seeded", lambda W: W.argon_fcc(20), "sweep_argon32k_traffic.txt"),
     "replicas": ("512 LJ argon replicas, N log-uniform 500-8,000 (1,451,403 atoms in all), density 18-24 "
                  "atoms/nm^3, cubic periodic boxes, cutoff 1.0 nm, seeded; one batch", lambda W: W.argon_replicas(),
-                 "sweep_tuned_replicas512_traffic.txt"),
+                 "sweep_replicas512_traffic.txt"),
 }
 SELECTED = "water"
 
@@ -268,9 +268,15 @@ def ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- launch shape by the autotuner, then CUDA-graph replay of every evaluation
+    # ---- launch shape by the autotuner (or --launch), then CUDA-graph replay of every evaluation
     tgt.load_parts()
-    warps, layout, stages, tune_ms = tgt.autotune(reps=3)
+    if args.launch:
+        warps, layout, stages = (int(v) for v in args.launch.split(","))
+        tgt.tune(warps)
+        tgt.set_layout(layout, stages)
+        tune_ms = None
+    else:
+        warps, layout, stages, tune_ms = tgt.autotune(reps=3)
     tgt.graph(True)
     for _ in range(3):                   # direct launch, capture, first replay
         tgt.resident()
@@ -379,7 +385,7 @@ def ours(args, rank, world, local_rank):
                     "host_ms": {k: round(v, 4) for k, v in host.items()}},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "sweep_tuned", "kernel_ms": ms_sweep,
+                         "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
             "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms,
@@ -401,8 +407,9 @@ def ours(args, rank, world, local_rank):
 
 
 def sched_ab(args, local_rank):
-    """Makespan of the sweep with the count-product order, the learned order and a random
-    order (same workload, device-resident, CUDA events, L2 flushed before every step)."""
+    """Makespan of the sweep with the count-product order, the learned order, a random order
+    and the cell-major order tasks are generated in (same workload, autotuned launch shape,
+    device-resident, CUDA events, L2 flushed before every step)."""
     import numpy as np
     import torch
     import mdcore_b200 as M
@@ -418,6 +425,7 @@ def sched_ab(args, local_rank):
     for _ in range(args.warmup):
         e.nonbond()
     e.load_parts()
+    warps, layout, stages, _ = e.autotune(reps=3)
     t0 = time.time()
     e.sched_record(args.record)
     X = e.sched_features()
@@ -443,10 +451,14 @@ def sched_ab(args, local_rank):
     res["learned"] = timed("mlp")
     e.set_order(np.random.default_rng(0).permutation(e.ntasks()))
     res["random"] = timed("random")
+    e.set_order(np.arange(e.ntasks()))           # tasks as generated: cell-major (L2 locality)
+    res["cell_order"] = timed("cells")
     e.tune(0, plain=True)
     res["plain_form"] = timed("plain")
     nz = y > 0
     print(json.dumps({"sched_ab": WORKLOADS[SELECTED][0], "sweep_ms_median": res, "tasks": e.ntasks(),
+                      "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
+                                 "staging_buffers": stages},
                       "record_steps": args.record, "epochs": args.epochs, "train_s": round(train_s, 3),
                       "train_mse": loss, "corr_pred_target": float(np.corrcoef(pred[nz], y[nz])[0, 1])}))
     e.close()
@@ -461,6 +473,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
     ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
                     help="water (default: the headline configuration), argon, slab or replicas")
+    ap.add_argument("--launch", default="",
+                    help="fixed persistent launch shape warps,layout,stages (e.g. 4,1,1) instead of the autotuner")
     ap.add_argument("--sched-ab", action="store_true",
                     help="train the task-cost model and compare sweep makespans of the queue orders")
     ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")

@@ -476,6 +476,8 @@ int engine_batch_load_parts(struct engine_batch *b);
 int engine_batch_resident(struct engine_batch *b);
 int engine_batch_unload_parts(struct engine_batch *b);
 int engine_batch_stats(struct engine_batch *b, struct nb_stats *out);
+/* engine_zero_forces for every engine of the batch. */
+int engine_batch_zero_forces(struct engine_batch *b);
 int engine_batch_setstream(struct engine_batch *b, void *stream);
 int engine_batch_kernel_times(struct engine_batch *b, float *total_ms, float *sweep_ms);
 int engine_batch_settune(struct engine_batch *b, int warps, int plain);

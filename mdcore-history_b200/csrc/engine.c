@@ -391,11 +391,7 @@ int engine_step(struct engine *e) {
     e->time += 1;
     if (space_shuffle(s) < 0) return engine_error(engine_err_space);
     s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
-    for (int c = 0; c < s->nr_cells; c++) {
-        struct cell *cl = &s->cells[c];
-        cl->epot = 0.0;
-        for (int k = 0; k < cl->count; k++) cl->parts[k].f[0] = cl->parts[k].f[1] = cl->parts[k].f[2] = 0.0f;
-    }
+    nb_zero_cells(s);
     if (engine_nonbond_cuda(e) < 0) return engine_error(engine_err_cuda);
     s->epot += s->epot_nonbond;
     if (engine_advance(e) < 0) return engine_error(engine_err);
@@ -434,10 +430,6 @@ int engine_zero_forces(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
     struct space *s = &e->s;
     s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
-    for (int c = 0; c < s->nr_cells; c++) {
-        struct cell *cl = &s->cells[c];
-        cl->epot = 0.0;
-        for (int k = 0; k < cl->count; k++) cl->parts[k].f[0] = cl->parts[k].f[1] = cl->parts[k].f[2] = 0.0f;
-    }
+    nb_zero_cells(s);
     return engine_err_ok;
 }

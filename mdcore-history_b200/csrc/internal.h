@@ -23,6 +23,8 @@ int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dns
 /* Device side (nonbond.cu, rigid.cu). */
 int nb_device_free(struct engine *e);
 int rigid_device_free(struct engine *e);
+/* Zeroes forces and energies of every cell of s (host threads over ranges of cells). */
+void nb_zero_cells(struct space *s);
 /* Launch stream of the engine's device state (NULL before engine_cuda_load). */
 void *nb_engine_stream(struct engine *e);
 

@@ -28,6 +28,7 @@
 #include "mdcore_b200.h"
 #include "internal.h"
 #include "nb_tuned.cuh"
+#include "host_pool.h"
 
 using namespace nb;
 
@@ -42,6 +43,7 @@ struct NbState {
     // engines served by this state and their offsets in the global cell / id numbering
     std::vector<struct engine*> engines;
     std::vector<int> cell_off, id_off;
+    std::vector<struct cell*> flat_cells;  // every engine's cells in global order
     struct nb_stats bstats = {};           // totals of the last evaluation over all engines
     // geometry
     int ncells = 0, ntasks = 0, ncap = 0, nid = 0;
@@ -183,30 +185,55 @@ double now_ms() {
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
-// Packs every engine's cells into the pinned staging buffers; returns the number of slots.
+// Cells per host-thread range: about 8,192 particles, at least 16 cells.
+int cell_grain(const NbState* st) {
+    long long n = 0;
+    for (const struct engine* e : st->engines) n += e->s.nr_parts;
+    const long long avg = st->ncells > 0 ? n / st->ncells + 1 : 1;
+    return (int)std::max(16LL, 8192 / avg);
+}
+
+// Packs every engine's cells into the pinned staging buffers (host threads over ranges of
+// cells: counts, then slot offsets, then positions and ids); returns the number of slots.
 int pack_cells(NbState* st) {
-    int total = 0, maxc = 0;
-    for (struct engine* e : st->engines)
-        for (int c = 0; c < e->s.nr_cells; c++) {
-            const int n = e->s.cells[c].count;
-            total += (n + 3) & ~3;
-            if (n > maxc) maxc = n;
+    HostPool& pool = HostPool::get();
+    const int nc = st->ncells;
+    int* cstart = st->h_cstart;
+    int* ccount = st->h_cstart + nc + 1;
+    const std::vector<struct cell*>& cells = st->flat_cells;
+    const int parts = pool.threads();
+    std::vector<int> part_slots(parts + 1, 0), part_max(parts, 0);
+    const int grain = cell_grain(st);
+    pool.run(nc, grain, [&](int part, int b, int e) {
+        int slots = 0, maxc = 0;
+        for (int c = b; c < e; c++) {
+            const int n = cells[c]->count;
+            ccount[c] = n;
+            slots += (n + 3) & ~3;
+            maxc = std::max(maxc, n);
         }
+        part_slots[part + 1] = slots;
+        part_max[part] = maxc;
+    });
+    int maxc = 0;
+    for (int k = 0; k < parts; k++) {
+        part_slots[k + 1] += part_slots[k];
+        maxc = std::max(maxc, part_max[k]);
+    }
+    const int total = part_slots[parts];
     if (maxc > kMaxPartsPerCell) {
         errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
     if (alloc_particles(st, total + 4) < 0) return engine_err_cuda;
-    int* cstart = st->h_cstart;
-    int* ccount = st->h_cstart + st->ncells + 1;
-    int slot = 0;
-    for (size_t k = 0; k < st->engines.size(); k++) {
-        struct space* s = &st->engines[k]->s;
-        const int c0 = st->cell_off[k], id0 = st->id_off[k];
-        for (int c = 0; c < s->nr_cells; c++) {
-            struct cell* cl = &s->cells[c];
-            cstart[c0 + c] = slot;
-            ccount[c0 + c] = cl->count;
+    pool.run(nc, grain, [&](int part, int b, int e) {
+        int slot = part_slots[part];
+        size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), b) - st->cell_off.begin() - 1;
+        for (int c = b; c < e; c++) {
+            while (c >= st->cell_off[k + 1]) k++;
+            const int id0 = st->id_off[k];
+            const struct cell* cl = cells[c];
+            cstart[c] = slot;
             for (int q = 0; q < cl->count; q++) {
                 const struct part* p = &cl->parts[q];
                 st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
@@ -219,10 +246,10 @@ int pack_cells(NbState* st) {
             }
             slot += pad;
         }
-    }
-    cstart[st->ncells] = slot;
+    });
+    cstart[nc] = total;
     st->maxcount = maxc;
-    return slot;
+    return total;
 }
 
 template <int NW>
@@ -551,6 +578,9 @@ int load_state(NbState* st) {
         st->id_off[k + 1] = st->id_off[k] + (e->s.size_parts > 0 ? e->s.size_parts : 1);
     }
     st->ncells = st->cell_off[ne];
+    st->flat_cells.clear();
+    for (struct engine* e : st->engines)
+        for (int c = 0; c < e->s.nr_cells; c++) st->flat_cells.push_back(&e->s.cells[c]);
     st->device = e0->device;
     CU(cudaSetDevice(st->device));
     CU(cudaStreamCreateWithFlags(&st->own_stream, cudaStreamNonBlocking));
@@ -777,18 +807,17 @@ int st_unload_parts(NbState* st) {
     else
         cudaGetLastError();
     const int rc = finish_stats(st);
-    for (size_t k = 0; k < st->engines.size(); k++) {
-        struct space* s = &st->engines[k]->s;
-        for (int c = 0; c < s->nr_cells; c++) {
-            struct cell* cl = &s->cells[c];
-            const float* f = hf + 3 * (size_t)st->h_cstart[st->cell_off[k] + c];
+    HostPool::get().run(st->ncells, cell_grain(st), [&](int, int b, int e) {
+        for (int c = b; c < e; c++) {
+            struct cell* cl = st->flat_cells[c];
+            const float* f = hf + 3 * (size_t)st->h_cstart[c];
             for (int q = 0; q < cl->count; q++) {
                 cl->parts[q].f[0] += f[3 * q];
                 cl->parts[q].f[1] += f[3 * q + 1];
                 cl->parts[q].f[2] += f[3 * q + 2];
             }
         }
-    }
+    });
     st->bstats.ms_device += (float)(t1 - t0);
     st->bstats.ms_unpack = (float)(now_ms() - t1);
     share_times(st);
@@ -905,6 +934,17 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
 }  // namespace
 
 // ---------------------------------------------------------------- single engine
+
+extern "C" void nb_zero_cells(struct space* s) {
+    const int grain = (int)std::max(16, 8192 / (s->nr_parts / std::max(1, s->nr_cells) + 1));
+    HostPool::get().run(s->nr_cells, grain, [&](int, int b, int e) {
+        for (int c = b; c < e; c++) {
+            struct cell* cl = &s->cells[c];
+            cl->epot = 0.0;
+            for (int q = 0; q < cl->count; q++) cl->parts[q].f[0] = cl->parts[q].f[1] = cl->parts[q].f[2] = 0.0f;
+        }
+    });
+}
 
 extern "C" void* nb_engine_stream(struct engine* e) {
     return (e != nullptr && e->cuda != nullptr) ? static_cast<void*>(state(e)->stream) : nullptr;
@@ -1094,8 +1134,8 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
     for (struct engine* e : st->engines) {
         e->time += 1;
         if (space_shuffle(&e->s) < 0) return engine_err = engine_err_space;
-        engine_zero_forces(e);
     }
+    engine_batch_zero_forces(b);
     const int rc = st_nonbond(st);
     if (rc < 0) return rc;
     for (struct engine* e : st->engines) {
@@ -1103,6 +1143,24 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
         if (engine_advance(e) < 0) return engine_err;
         if (e->nr_rigids > 0 && engine_rigid_eval(e) < 0) return engine_err = engine_err_rigid;
     }
+    return 0;
+}
+
+// engine_zero_forces for every engine of the batch (host threads over the cells).
+extern "C" int engine_batch_zero_forces(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    NbState* st = bstate(b);
+    for (struct engine* e : st->engines) {
+        struct space* s = &e->s;
+        s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
+    }
+    HostPool::get().run(st->ncells, cell_grain(st), [&](int, int cb, int ce) {
+        for (int c = cb; c < ce; c++) {
+            struct cell* cl = st->flat_cells[c];
+            cl->epot = 0.0;
+            for (int q = 0; q < cl->count; q++) cl->parts[q].f[0] = cl->parts[q].f[1] = cl->parts[q].f[2] = 0.0f;
+        }
+    });
     return 0;
 }
 

@@ -128,6 +128,7 @@ def lib() -> C.CDLL:
         "engine_batch_resident": (C.c_int, [vp]),
         "engine_batch_unload_parts": (C.c_int, [vp]),
         "engine_batch_stats": (C.c_int, [vp, P(NbStats)]),
+        "engine_batch_zero_forces": (C.c_int, [vp]),
         "engine_batch_setstream": (C.c_int, [vp, vp]),
         "engine_batch_kernel_times": (C.c_int, [vp, P(C.c_float), P(C.c_float)]),
         "engine_batch_settune": (C.c_int, [vp, C.c_int, C.c_int]),
@@ -456,8 +457,7 @@ class Batch:
         self.closed = False
 
     def _zero(self):
-        for e in self.engines:
-            _check(self.lib.engine_zero_forces(e.ptr), "engine_zero_forces")
+        _check(self.lib.engine_batch_zero_forces(self.ptr), "engine_batch_zero_forces")
 
     def nonbond(self):
         """One force evaluation of every engine (host buffers in and out)."""
