@@ -1,8 +1,8 @@
 // Sort and sorted-sweep kernels of the nonbonded engine (sm_100a).
 //
-// sort_cells   : runner_dosort (src/runner_dosort.c:97-161) -- one CTA per cell builds the
-//                13 projected-distance key lists the cell's pair tasks need and orders
-//                them by descending distance (a stable rank sort: ties keep storage order).
+// sort_cells   : runner_dosort (src/runner_dosort.c:97-161) -- builds every cell's 13
+//                projected-distance key lists its pair tasks need and orders them by
+//                descending distance (a stable rank sort: ties keep storage order).
 // sweep_tasks  : runner_dopair_vec / runner_doself_vec (src/runner_dopair.c:540-741,
 //                858-1029) with potential_eval (src/potential_eval.h:67-104) -- one CTA per
 //                cell-pair task; the two cells' particle blocks and sort keys are moved
@@ -22,12 +22,17 @@ namespace nb {
 __constant__ float c_axes[13][3];
 
 // ---------------------------------------------------------------- sort
-// One CTA per cell, one warp per sort direction (directions w, w+4, ... for warp w).  Keys
-// of a direction are ranked by a counting sort on the top bits of the 16-bit distance
-// (64 buckets in the warp's shared memory) and an exact rank inside the bucket:
-// position = (keys in farther buckets) + (keys of the same bucket with a larger distance,
-// or an equal distance and a smaller storage index).  The result is the stable descending
-// order, independent of the order in which lanes reach the atomics.
+// A block of kSortWarps warps sorts `cpc` consecutive cells (1 for systems of large cells,
+// 8 for systems of small ones).  Keys of a direction are ordered by descending distance,
+// ties by ascending storage index (a stable order, independent of the order in which lanes
+// run):
+//  * a cell of at most 32 particles is sorted by one warp in registers: each lane holds one
+//    particle and counts, with a shuffle loop, the keys that come before its own;
+//  * a larger cell is sorted by all warps of the block, one warp per direction (w, w+4, ..),
+//    with a counting sort on the top bits of the 16-bit distance (64 buckets in the warp's
+//    shared memory) and an exact rank inside the bucket: position = (keys in farther
+//    buckets) + (keys of the same bucket with a larger distance, or an equal distance and a
+//    smaller storage index).
 constexpr int kSortBuckets = 64;
 constexpr int kSortWarps = 4;
 
@@ -36,45 +41,50 @@ __host__ __device__ inline size_t sort_warp_bytes() {
 }
 __host__ inline size_t sort_smem_bytes() { return kSortWarps * sort_warp_bytes(); }
 
-__global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
-                                                              const int* __restrict__ ccount,
-                                                              const unsigned* __restrict__ cmask,
-                                                              unsigned* __restrict__ keys,
-                                                              const float2* __restrict__ cscale,
-                                                              unsigned long long* acc) {
-    extern __shared__ __align__(16) unsigned char sort_smem[];
+// dscale * (bias + x.n), evaluated left to right without contraction (src/runner_dosort.c:148-149).
+__device__ __forceinline__ unsigned sort_dist(float4 x, float nx, float ny, float nz, float dscale, float bias) {
+    float d = __fadd_rn(bias, __fmul_rn(x.x, nx));
+    d = __fadd_rn(d, __fmul_rn(x.y, ny));
+    d = __fadd_rn(d, __fmul_rn(x.z, nz));
+    return __float2uint_rz(__fmul_rn(dscale, d));
+}
+
+// One warp, a cell of n <= 32 particles, every direction of its mask.
+__device__ __forceinline__ void sort_small_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys, int start,
+                                                int n, unsigned mask, float dscale, float bias, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wp = sort_smem + (size_t)warp * sort_warp_bytes();
+    const int pad = (n + 3) & ~3;
+    const float4 x = lane < n ? xq[start + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int sid = 0; sid < 13; ++sid) {
+        if (!((mask >> sid) & 1u)) continue;
+        const unsigned md = sort_dist(x, c_axes[sid][0], c_axes[sid][1], c_axes[sid][2], dscale, bias);
+        int rank = 0;
+        for (int m = 0; m < n; ++m) {
+            const unsigned od = __shfl_sync(FULL, md, m);
+            rank += (od > md) | ((od == md) & (m < lane));
+        }
+        if (lane < n) keys[13 * (size_t)start + (size_t)sid * pad + rank] = ((unsigned)lane << 16) | md;
+    }
+}
+
+// The warp's share of the directions of a cell of more than 32 particles.
+__device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys,
+                                                unsigned char* wp, int start, int n, unsigned mask, float dscale,
+                                                float bias, int warp, int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
     unsigned* skey = reinterpret_cast<unsigned*>(wp);
     unsigned short* members = reinterpret_cast<unsigned short*>(wp + (size_t)kMaxPartsPerCell * 4);
     int* bcount = reinterpret_cast<int*>(wp + (size_t)kMaxPartsPerCell * 6);
     int* bstart = bcount + kSortBuckets;
     int* bfill = bstart + kSortBuckets;
-    const int c = blockIdx.x;
-    const int n = ccount[c];
-    if (n <= 0) return;
-    if (n > kMaxPartsPerCell) {
-        if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
-        return;
-    }
-    const int start = cstart[c];
     const int pad = (n + 3) & ~3;
-    const unsigned mask = cmask[c];
-    const float dscale = cscale[c].x, bias = cscale[c].y;     // 32767/(2|h|), |h| of the cell's box
     for (int sid = warp; sid < 13; sid += kSortWarps) {
         if (!((mask >> sid) & 1u)) continue;
         const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
         for (int b = lane; b < kSortBuckets; b += 32) { bcount[b] = 0; bfill[b] = 0; }
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const float4 x = xq[start + k];
-            // dscale * (bias + x.n), evaluated left to right without contraction.
-            float d = __fadd_rn(bias, __fmul_rn(x.x, nx));
-            d = __fadd_rn(d, __fmul_rn(x.y, ny));
-            d = __fadd_rn(d, __fmul_rn(x.z, nz));
-            d = __fmul_rn(dscale, d);
-            const unsigned key = ((unsigned)k << 16) | __float2uint_rz(d);
+            const unsigned key = ((unsigned)k << 16) | sort_dist(xq[start + k], nx, ny, nz, dscale, bias);
             skey[k] = key;
             atomicAdd(&bcount[min((int)((key & 0xffffu) >> 9), kSortBuckets - 1)], 1);
         }
@@ -113,6 +123,33 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
             out[rank] = mine;
         }
         __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+                                                              const int* __restrict__ ccount,
+                                                              const unsigned* __restrict__ cmask,
+                                                              unsigned* __restrict__ keys,
+                                                              const float2* __restrict__ cscale, int ncells, int cpc,
+                                                              unsigned long long* acc) {
+    extern __shared__ __align__(16) unsigned char sort_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c0 = blockIdx.x * cpc, c1 = min(c0 + cpc, ncells);
+    // cells of at most 32 particles: one warp each
+    for (int c = c0 + warp; c < c1; c += kSortWarps) {
+        const int n = ccount[c];
+        if (n > 0 && n <= 32) sort_small_cell(xq, keys, cstart[c], n, cmask[c], cscale[c].x, cscale[c].y, lane);
+    }
+    // larger cells: all warps, one direction each
+    for (int c = c0; c < c1; ++c) {
+        const int n = ccount[c];
+        if (n <= 32) continue;
+        if (n > kMaxPartsPerCell) {
+            if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
+            continue;
+        }
+        sort_large_cell(xq, keys, sort_smem + (size_t)warp * sort_warp_bytes(), cstart[c], n, cmask[c], cscale[c].x,
+                        cscale[c].y, warp, lane);
     }
 }
 

@@ -185,6 +185,10 @@ double now_ms() {
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
+// Cells per sort block: 8 when cells hold 32 particle slots or fewer on average (one warp
+// sorts a small cell alone), else 1 (the block's warps share a large cell's directions).
+int sort_cells_per_block(int slots, int ncells) { return slots <= 32 * (long long)ncells ? 8 : 1; }
+
 // Cells per host-thread range: about 8,192 particles, at least 16 cells.
 int cell_grain(const NbState* st) {
     long long n = 0;
@@ -382,8 +386,9 @@ int issue_kernels(NbState* st) {
     CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * 2 * st->ncells, st->stream));
     const int cap = (st->maxcount + 3) & ~3;
     if (cap == 0) return 0;
-    sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
-        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->d_cscale, st->d_acc);
+    const int cpc = sort_cells_per_block(st->h_cstart[st->ncells], st->ncells);
+    sort_cells<<<(st->ncells + cpc - 1) / cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
+        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->d_cscale, st->ncells, cpc, st->d_acc);
     CU(cudaGetLastError());
 
     Params P;
@@ -1365,8 +1370,9 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     CU(cudaMemsetAsync(counter, 0, sizeof(int), s));
     const int cap4 = (maxcount + 3) & ~3;
     if (cap4 == 0) return 0;
-    sort_cells<<<st->ncells, kSortWarps * 32, sort_smem_bytes(), s>>>(static_cast<const float4*>(xq), cstart, ccount,
-                                                                      st->d_cmask, keys, st->d_cscale, acc);
+    const int cpc = sort_cells_per_block(nslots, st->ncells);
+    sort_cells<<<(st->ncells + cpc - 1) / cpc, kSortWarps * 32, sort_smem_bytes(), s>>>(
+        static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale, st->ncells, cpc, acc);
     CU(cudaGetLastError());
 
     TunedParams T;
