@@ -271,12 +271,12 @@ def ours(args, rank, world, local_rank):
     # ---- launch shape by the autotuner (or --launch), then CUDA-graph replay of every evaluation
     tgt.load_parts()
     if args.launch:
-        warps, layout, stages = (int(v) for v in args.launch.split(","))
+        warps, layout, stages, occupancy = (int(v) for v in (args.launch + ",640").split(",")[:4])
         tgt.tune(warps)
-        tgt.set_layout(layout, stages)
+        tgt.set_layout(layout, stages, occupancy)
         tune_ms = None
     else:
-        warps, layout, stages, tune_ms = tgt.autotune(reps=3)
+        warps, layout, stages, occupancy, tune_ms = tgt.autotune(reps=3)
     tgt.graph(True)
     for _ in range(3):                   # direct launch, capture, first replay
         tgt.resident()
@@ -378,7 +378,8 @@ def ours(args, rank, world, local_rank):
                        "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
                        "tasks": tgt.ntasks(), "cells": ncells, "parallelism": f"replicas x{world}",
                        "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
-                                  "staging_buffers": stages, "autotune_ms": tune_ms, "cuda_graph": True},
+                                  "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
+                                  "cuda_graph": True},
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
             "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -425,7 +426,7 @@ def sched_ab(args, local_rank):
     for _ in range(args.warmup):
         e.nonbond()
     e.load_parts()
-    warps, layout, stages, _ = e.autotune(reps=3)
+    warps, layout, stages, occupancy, _ = e.autotune(reps=3)
     t0 = time.time()
     e.sched_record(args.record)
     X = e.sched_features()
@@ -458,7 +459,7 @@ def sched_ab(args, local_rank):
     nz = y > 0
     print(json.dumps({"sched_ab": WORKLOADS[SELECTED][0], "sweep_ms_median": res, "tasks": e.ntasks(),
                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
-                                 "staging_buffers": stages},
+                                 "staging_buffers": stages, "threads_per_sm": occupancy},
                       "record_steps": args.record, "epochs": args.epochs, "train_s": round(train_s, 3),
                       "train_mse": loss, "corr_pred_target": float(np.corrcoef(pred[nz], y[nz])[0, 1])}))
     e.close()
@@ -474,7 +475,8 @@ def main():
     ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
                     help="water (default: the headline configuration), argon, slab or replicas")
     ap.add_argument("--launch", default="",
-                    help="fixed persistent launch shape warps,layout,stages (e.g. 4,1,1) instead of the autotuner")
+                    help="fixed persistent launch shape warps,layout,stages[,threads per SM] (e.g. 4,1,1,640) "
+                         "instead of the autotuner")
     ap.add_argument("--sched-ab", action="store_true",
                     help="train the task-cost model and compare sweep makespans of the queue orders")
     ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")

@@ -439,7 +439,7 @@ int engine_rigid_get(struct engine *e, int g, struct rigid *out);
  * each) and cell index; any pointer may be NULL. */
 int engine_getparts(struct engine *e, float *x, float *v, float *f, int *cell, int N);
 /* Sweep steps each lane holds before the warp reduce-scatter of the persistent sweep: 4
- * (default) or 8.  Forces are identical either way. */
+ * (default) or 8 (used at 640 threads per SM).  Same pair set. */
 int engine_cuda_setwindow(struct engine *e, int window);
 /* CUDA-graph replay of each evaluation's launches (zeroing, sort, queue compaction,
  * sweep): enable = 1 captures the launches on the second evaluation of a launch
@@ -449,13 +449,16 @@ int engine_cuda_graph(struct engine *e, int enable);
 /* Persistent sweep shape: lane layout 0 = one i particle per lane (32 per warp, the
  * default), 1 = a tile of 8 i particles x 4 j columns per warp; stages = 1 or 2 staging
  * buffers per worker warp (2: the next task's bulk copies land while the warp sweeps the
- * current one).  Same pair set. */
-int engine_cuda_setlayout(struct engine *e, int layout, int stages);
+ * current one; only with occupancy 640); occupancy = resident threads per SM the kernel's
+ * registers are sized for: 640 (96 registers, the default), 768 (80) or 1024 (64).  Same
+ * pair set. */
+int engine_cuda_setlayout(struct engine *e, int layout, int stages, int occupancy);
 /* Times every persistent launch shape (2, 4, 8 worker warps per block x lane layout x
- * staging buffers, window 4) on the resident particles (uploaded first if none are) and
- * keeps the fastest; returns the chosen shape and its median device time (sort + sweep).
- * Results stay resident. */
-int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, int *stages, float *ms);
+ * staging buffers x occupancy, window 4) on the resident particles (uploaded first if none
+ * are) and keeps the fastest; returns the chosen shape and its median device time (sort +
+ * sweep).  Results stay resident. */
+int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, int *stages, int *occupancy,
+                         float *ms);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff
@@ -482,8 +485,9 @@ int engine_batch_setstream(struct engine_batch *b, void *stream);
 int engine_batch_kernel_times(struct engine_batch *b, float *total_ms, float *sweep_ms);
 int engine_batch_settune(struct engine_batch *b, int warps, int plain);
 int engine_batch_graph(struct engine_batch *b, int enable);
-int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *layout, int *stages, float *ms);
-int engine_batch_setlayout(struct engine_batch *b, int layout, int stages, int window);
+int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *layout, int *stages, int *occupancy,
+                          float *ms);
+int engine_batch_setlayout(struct engine_batch *b, int layout, int stages, int occupancy);
 int engine_batch_ntasks(struct engine_batch *b);
 
 #ifdef __cplusplus

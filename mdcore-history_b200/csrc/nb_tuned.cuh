@@ -22,11 +22,10 @@
 #pragma once
 #include "nb_kernels.cuh"
 
-// Resident threads per SM the register allocation of sweep_tuned is sized for (launch
-// bounds): 640 threads = 20 warps leaves ~100 registers per thread.
-#ifndef MDB_TUNED_THREADS_PER_SM
-#define MDB_TUNED_THREADS_PER_SM 640
-#endif
+// TPSM, a template parameter of both persistent sweeps: resident threads per SM their
+// register allocation is sized for (launch bounds).  640 threads leave 96 registers per
+// thread, 768 leave 80, 1024 leave 64: large cells (long sweeps) run best with 96,
+// small cells (short tasks, latency-bound) with more warps per SM.
 
 namespace nb {
 
@@ -623,8 +622,8 @@ __device__ __forceinline__ float reduce_scatter_rows(const float (&v)[WIN], int 
 //
 // WIN (4 or 8): sweep steps per reduce-scatter; 8 halves the shuffles per step but holds
 // twice the registers.  STAGES (1 or 2): staging buffers per warp.
-template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES>
-__global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
+template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES, int TPSM>
+__global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
@@ -740,8 +739,8 @@ __global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32))
 // contributions of WIN steps (4 WIN consecutive j) are summed over the 8 rows by one
 // reduce-scatter, after which the 32 (or 16) lanes write distinct j; the i forces are
 // summed over the 4 columns at the end of the strip.
-template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES>
-__global__ void __launch_bounds__(NW * 32, MDB_TUNED_THREADS_PER_SM / (NW * 32)) sweep_tiled(TunedParams T, int cap) {
+template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES, int TPSM>
+__global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;

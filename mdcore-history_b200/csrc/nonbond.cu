@@ -59,6 +59,7 @@ struct NbState {
     int window = 4;                // sweep steps per register reduce-scatter (4 or 8)
     int layout = 0;                // persistent sweep: 0 = 32 i per warp, 1 = 8 i x 4 j tile
     int stages = 1;                // staging buffers per worker warp (2: next task's copies in flight)
+    int occupancy = 640;           // resident threads per SM the sweep's registers are sized for
     bool has_excl = false;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
@@ -288,9 +289,9 @@ int launch_plain(NbState* st, const Params& P, int cap) {
 // Persistent launch: as many CTAs as fit on every SM at once.  Under stream capture the
 // function attribute and occupancy query are skipped and the grid of the preceding direct
 // launch of the same configuration is reused.
-template <int NW, bool EX, bool ONE, int WIN, int LAY, int STG>
+template <int NW, bool EX, bool ONE, int WIN, int LAY, int STG, int TPSM>
 int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    auto kern = LAY ? sweep_tiled<NW, EX, ONE, WIN, STG> : sweep_tuned<NW, EX, ONE, WIN, STG>;
+    auto kern = LAY ? sweep_tiled<NW, EX, ONE, WIN, STG, TPSM> : sweep_tuned<NW, EX, ONE, WIN, STG, TPSM>;
     int grid = st->last_grid;
     if (!st->capturing) {
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -305,33 +306,35 @@ int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
     return 0;
 }
 
-template <int NW, int WIN, int LAY, int STG>
+template <int NW, int WIN, int LAY, int STG, int TPSM>
 int launch_tuned_w(NbState* st, const TunedParams& T, int cap, size_t smem) {
     const bool one = st->one_pot;
     if (st->has_excl)
-        return one ? launch_tuned_nw<NW, true, true, WIN, LAY, STG>(st, T, cap, smem)
-                   : launch_tuned_nw<NW, true, false, WIN, LAY, STG>(st, T, cap, smem);
-    return one ? launch_tuned_nw<NW, false, true, WIN, LAY, STG>(st, T, cap, smem)
-               : launch_tuned_nw<NW, false, false, WIN, LAY, STG>(st, T, cap, smem);
+        return one ? launch_tuned_nw<NW, true, true, WIN, LAY, STG, TPSM>(st, T, cap, smem)
+                   : launch_tuned_nw<NW, true, false, WIN, LAY, STG, TPSM>(st, T, cap, smem);
+    return one ? launch_tuned_nw<NW, false, true, WIN, LAY, STG, TPSM>(st, T, cap, smem)
+               : launch_tuned_nw<NW, false, false, WIN, LAY, STG, TPSM>(st, T, cap, smem);
 }
 
 // Worker warps per block: 2, 4 or 8 (two warps fit even the largest cells).
-template <int WIN, int LAY, int STG>
+template <int WIN, int LAY, int STG, int TPSM>
 int launch_tuned_win(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
     switch (nw) {
-        case 2: return launch_tuned_w<2, WIN, LAY, STG>(st, T, cap, smem);
-        case 8: return launch_tuned_w<8, WIN, LAY, STG>(st, T, cap, smem);
-        default: return launch_tuned_w<4, WIN, LAY, STG>(st, T, cap, smem);
+        case 2: return launch_tuned_w<2, WIN, LAY, STG, TPSM>(st, T, cap, smem);
+        case 8: return launch_tuned_w<8, WIN, LAY, STG, TPSM>(st, T, cap, smem);
+        default: return launch_tuned_w<4, WIN, LAY, STG, TPSM>(st, T, cap, smem);
     }
 }
 
-template <int STG>
-int launch_tuned_stg(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
-    if (st->layout)
-        return st->window == 8 ? launch_tuned_win<8, 1, STG>(st, T, cap, smem, nw)
-                               : launch_tuned_win<4, 1, STG>(st, T, cap, smem, nw);
-    return st->window == 8 ? launch_tuned_win<8, 0, STG>(st, T, cap, smem, nw)
-                           : launch_tuned_win<4, 0, STG>(st, T, cap, smem, nw);
+// Instantiated shapes: at 640 threads per SM every window and staging choice; at 768 and
+// 1024 (fewer registers per thread) the 4-step window with one staging buffer.
+template <int LAY>
+int launch_tuned_lay(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
+    if (st->occupancy == 1024) return launch_tuned_win<4, LAY, 1, 1024>(st, T, cap, smem, nw);
+    if (st->occupancy == 768) return launch_tuned_win<4, LAY, 1, 768>(st, T, cap, smem, nw);
+    if (st->stages == 2) return launch_tuned_win<4, LAY, 2, 640>(st, T, cap, smem, nw);
+    if (st->window == 8) return launch_tuned_win<8, LAY, 1, 640>(st, T, cap, smem, nw);
+    return launch_tuned_win<4, LAY, 1, 640>(st, T, cap, smem, nw);
 }
 
 int launch_tuned(NbState* st, const Params& P, int cap4) {
@@ -365,7 +368,7 @@ int launch_tuned(NbState* st, const Params& P, int cap4) {
                       __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
-    return st->stages == 2 ? launch_tuned_stg<2>(st, T, cap, smem, nw) : launch_tuned_stg<1>(st, T, cap, smem, nw);
+    return st->layout ? launch_tuned_lay<1>(st, T, cap, smem, nw) : launch_tuned_lay<0>(st, T, cap, smem, nw);
 }
 
 // Records an event; inside a stream capture as an external record node, so that replaying
@@ -442,6 +445,7 @@ long long launch_key(const NbState* st) {
     k = k * 17 + st->window;
     k = k * 3 + st->layout;
     k = k * 3 + st->stages;
+    k = k * 3 + (st->occupancy == 640 ? 0 : st->occupancy == 768 ? 1 : 2);
     k = k * 3 + st->plain;
     k = k * 3 + st->record_clock;
     return k;
@@ -879,10 +883,11 @@ int st_settune(NbState* st, int warps, int plain) {
 }
 
 // Times every persistent launch shape (worker warps per block x lane layout x staging
-// buffers per warp) on the resident particles, `reps` evaluations each after one warm-up,
-// and keeps the fastest (median device time of sort + sweep).  Every shape computes the
-// same pair set and forces within FP32 rounding.
-int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* stages_out, float* ms_out) {
+// buffers per warp x resident threads per SM) on the resident particles, `reps`
+// evaluations each after one warm-up, and keeps the fastest (median device time of sort +
+// sweep).  Every shape computes the same pair set and forces within FP32 rounding.
+int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* stages_out, int* occupancy_out,
+                float* ms_out) {
     if (!st->resident_valid) {
         const int rc = st_load_parts(st);
         if (rc < 0) return rc;
@@ -892,9 +897,13 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
     const bool graph = st->use_graph;
     st->use_graph = false;
     st->plain = 0;
-    // warps, layout, stages (window 4: the 8-step window was never the fastest shape)
-    static const int shapes[][3] = {{2, 0, 1}, {4, 0, 1}, {8, 0, 1}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1},
-                                    {2, 0, 2}, {4, 0, 2}, {8, 0, 2}, {2, 1, 2}, {4, 1, 2}, {8, 1, 2}};
+    // warps, layout, stages, threads per SM (window 4: the 8-step window was never the
+    // fastest shape)
+    static const int shapes[][4] = {
+        {2, 0, 1, 640}, {4, 0, 1, 640}, {8, 0, 1, 640}, {2, 1, 1, 640}, {4, 1, 1, 640}, {8, 1, 1, 640},
+        {2, 0, 2, 640}, {4, 0, 2, 640}, {8, 0, 2, 640}, {2, 1, 2, 640}, {4, 1, 2, 640}, {8, 1, 2, 640},
+        {2, 0, 1, 768}, {4, 0, 1, 768}, {8, 0, 1, 768}, {2, 1, 1, 768}, {4, 1, 1, 768}, {8, 1, 1, 768},
+        {2, 0, 1, 1024}, {4, 0, 1, 1024}, {8, 0, 1, 1024}, {2, 1, 1, 1024}, {4, 1, 1, 1024}, {8, 1, 1, 1024}};
     const int nshapes = sizeof(shapes) / sizeof(shapes[0]);
     int best = -1;
     float best_ms = 0.f;
@@ -902,6 +911,7 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
         st->warps = shapes[k][0];
         st->layout = shapes[k][1];
         st->stages = shapes[k][2];
+        st->occupancy = shapes[k][3];
         st->window = 4;
         std::vector<float> t;
         for (int r = 0; r <= reps; r++) {
@@ -925,6 +935,7 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
     st->warps = shapes[best][0];
     st->layout = shapes[best][1];
     st->stages = shapes[best][2];
+    st->occupancy = shapes[best][3];
     st->window = 4;
     st->use_graph = graph;
     const int rc = st_resident(st);           // leave the chosen shape's results resident
@@ -932,6 +943,7 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
     if (warps_out) *warps_out = st->warps;
     if (layout_out) *layout_out = st->layout;
     if (stages_out) *stages_out = st->stages;
+    if (occupancy_out) *occupancy_out = st->occupancy;
     if (ms_out) *ms_out = best_ms;
     return 0;
 }
@@ -995,12 +1007,19 @@ extern "C" int engine_cuda_setwindow(struct engine* e, int window) {
     return 0;
 }
 
-extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages) {
-    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2)) return engine_err_range;
-    state(e)->layout = layout;
-    state(e)->stages = stages;
+static int st_setlayout(NbState* st, int layout, int stages, int occupancy) {
+    if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2) ||
+        (occupancy != 640 && occupancy != 768 && occupancy != 1024) || (stages == 2 && occupancy != 640))
+        return engine_err_range;
+    st->layout = layout;
+    st->stages = stages;
+    st->occupancy = occupancy;
     return 0;
+}
+
+extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages, int occupancy) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_setlayout(state(e), layout, stages, occupancy);
 }
 
 extern "C" int engine_cuda_graph(struct engine* e, int enable) {
@@ -1012,9 +1031,10 @@ extern "C" int engine_cuda_graph(struct engine* e, int enable) {
     return 0;
 }
 
-extern "C" int engine_cuda_autotune(struct engine* e, int reps, int* warps, int* layout, int* stages, float* ms) {
+extern "C" int engine_cuda_autotune(struct engine* e, int reps, int* warps, int* layout, int* stages, int* occupancy,
+                                    float* ms) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    return st_autotune(state(e), reps, warps, layout, stages, ms);
+    return st_autotune(state(e), reps, warps, layout, stages, occupancy, ms);
 }
 
 extern "C" int engine_cuda_load(struct engine* e) {
@@ -1200,19 +1220,14 @@ extern "C" int engine_batch_graph(struct engine_batch* b, int enable) {
 }
 
 extern "C" int engine_batch_autotune(struct engine_batch* b, int reps, int* warps, int* layout, int* stages,
-                                     float* ms) {
+                                     int* occupancy, float* ms) {
     if (b == nullptr) return engine_err_null;
-    return st_autotune(bstate(b), reps, warps, layout, stages, ms);
+    return st_autotune(bstate(b), reps, warps, layout, stages, occupancy, ms);
 }
 
-extern "C" int engine_batch_setlayout(struct engine_batch* b, int layout, int stages, int window) {
+extern "C" int engine_batch_setlayout(struct engine_batch* b, int layout, int stages, int occupancy) {
     if (b == nullptr) return engine_err_null;
-    if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2) || (window != 4 && window != 8))
-        return engine_err_range;
-    bstate(b)->layout = layout;
-    bstate(b)->stages = stages;
-    bstate(b)->window = window;
-    return 0;
+    return st_setlayout(bstate(b), layout, stages, occupancy);
 }
 
 extern "C" int engine_batch_ntasks(struct engine_batch* b) {
@@ -1419,7 +1434,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const bool cap_saved = st->capturing;
     st->stream = s;
     st->capturing = false;
-    const int rc = launch_tuned_w<4, 4, 0, 1>(st, T, cap, smem);
+    const int rc = launch_tuned_w<4, 4, 0, 1, 640>(st, T, cap, smem);
     st->stream = saved;
     st->capturing = cap_saved;
     return rc;

@@ -117,8 +117,8 @@ def lib() -> C.CDLL:
         "engine_rigid_get": (C.c_int, [vp, C.c_int, vp]),
         "engine_getparts": (C.c_int, [vp, vp, vp, vp, vp, C.c_int]),
         "engine_cuda_graph": (C.c_int, [vp, C.c_int]),
-        "engine_cuda_autotune": (C.c_int, [vp, C.c_int, ip, ip, ip, P(C.c_float)]),
-        "engine_cuda_setlayout": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_cuda_autotune": (C.c_int, [vp, C.c_int, ip, ip, ip, ip, P(C.c_float)]),
+        "engine_cuda_setlayout": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "engine_batch_setlayout": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "engine_batch_create": (C.c_int, [P(vp), C.c_int, P(vp)]),
         "engine_batch_free": (C.c_int, [vp]),
@@ -133,7 +133,7 @@ def lib() -> C.CDLL:
         "engine_batch_kernel_times": (C.c_int, [vp, P(C.c_float), P(C.c_float)]),
         "engine_batch_settune": (C.c_int, [vp, C.c_int, C.c_int]),
         "engine_batch_graph": (C.c_int, [vp, C.c_int]),
-        "engine_batch_autotune": (C.c_int, [vp, C.c_int, ip, ip, ip, P(C.c_float)]),
+        "engine_batch_autotune": (C.c_int, [vp, C.c_int, ip, ip, ip, ip, P(C.c_float)]),
         "engine_batch_ntasks": (C.c_int, [vp]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -329,17 +329,19 @@ class Engine:
         """CUDA-graph replay of each evaluation's launches."""
         _check(self.lib.engine_cuda_graph(self.ptr, int(enable)), "engine_cuda_graph")
 
-    def set_layout(self, layout: int, stages: int = 1):
+    def set_layout(self, layout: int, stages: int = 1, occupancy: int = 640):
         """Persistent sweep shape: lane layout 0 = 32 i per warp, 1 = 8 i x 4 j tile;
-        stages = staging buffers per worker warp (1 or 2)."""
-        _check(self.lib.engine_cuda_setlayout(self.ptr, layout, stages), "engine_cuda_setlayout")
+        stages = staging buffers per worker warp (1 or 2); occupancy = resident threads per
+        SM the registers are sized for (640, 768, 1024)."""
+        _check(self.lib.engine_cuda_setlayout(self.ptr, layout, stages, occupancy), "engine_cuda_setlayout")
 
     def autotune(self, reps: int = 5):
-        """Keeps the fastest persistent launch shape; returns (warps, layout, stages, ms)."""
-        w, lay, win, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
-        _check(self.lib.engine_cuda_autotune(self.ptr, reps, C.byref(w), C.byref(lay), C.byref(win), C.byref(ms)),
-               "engine_cuda_autotune")
-        return w.value, lay.value, win.value, ms.value
+        """Keeps the fastest persistent launch shape; returns (warps, layout, stages,
+        occupancy, ms)."""
+        w, lay, stg, occ, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.engine_cuda_autotune(self.ptr, reps, C.byref(w), C.byref(lay), C.byref(stg), C.byref(occ),
+                                             C.byref(ms)), "engine_cuda_autotune")
+        return w.value, lay.value, stg.value, occ.value, ms.value
 
     def ntasks(self) -> int:
         return _check(self.lib.engine_cuda_ntasks(self.ptr), "engine_cuda_ntasks")
@@ -498,15 +500,16 @@ class Batch:
     def graph(self, enable: bool = True):
         _check(self.lib.engine_batch_graph(self.ptr, int(enable)), "engine_batch_graph")
 
-    def set_layout(self, layout: int, stages: int = 1, window: int = 4):
-        _check(self.lib.engine_batch_setlayout(self.ptr, layout, stages, window), "engine_batch_setlayout")
+    def set_layout(self, layout: int, stages: int = 1, occupancy: int = 640):
+        _check(self.lib.engine_batch_setlayout(self.ptr, layout, stages, occupancy), "engine_batch_setlayout")
 
     def autotune(self, reps: int = 5):
-        """Keeps the fastest persistent launch shape; returns (warps, layout, stages, ms)."""
-        w, lay, win, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
-        _check(self.lib.engine_batch_autotune(self.ptr, reps, C.byref(w), C.byref(lay), C.byref(win), C.byref(ms)),
-               "engine_batch_autotune")
-        return w.value, lay.value, win.value, ms.value
+        """Keeps the fastest persistent launch shape; returns (warps, layout, stages,
+        occupancy, ms)."""
+        w, lay, stg, occ, ms = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.engine_batch_autotune(self.ptr, reps, C.byref(w), C.byref(lay), C.byref(stg), C.byref(occ),
+                                              C.byref(ms)), "engine_batch_autotune")
+        return w.value, lay.value, stg.value, occ.value, ms.value
 
     def ntasks(self) -> int:
         return _check(self.lib.engine_batch_ntasks(self.ptr), "engine_batch_ntasks")

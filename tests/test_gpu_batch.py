@@ -150,8 +150,8 @@ def test_batch_graph_and_autotune_keep_results():
     engines = engines_of(systems)
     b = M.Batch(engines)
     b.nonbond()
-    warps, layout, stages, ms = b.autotune(reps=2)
-    assert warps in (2, 4, 8) and layout in (0, 1) and stages in (1, 2) and ms > 0
+    warps, layout, stages, occ, ms = b.autotune(reps=2)
+    assert warps in (2, 4, 8) and layout in (0, 1) and stages in (1, 2) and occ in (640, 768, 1024) and ms > 0
     b.nonbond()
     ref = [e.forces() for e in engines]
     e_ref = [e.stats().epot for e in engines]

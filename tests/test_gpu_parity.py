@@ -205,12 +205,12 @@ def test_graph_replay_bit_identical(fname):
     e.close()
 
 
-@pytest.mark.parametrize("stages", [1, 2])
+@pytest.mark.parametrize("stages,occupancy", [(1, 640), (2, 640), (1, 768), (1, 1024)])
 @pytest.mark.parametrize("layout", [0, 1], ids=["32i", "8x4"])
 @pytest.mark.parametrize("window", [4, 8])
 @pytest.mark.parametrize("warps", [2, 4, 8])
 @pytest.mark.parametrize("fname", SYSTEMS)
-def test_persistent_launch_shapes(fname, warps, window, layout, stages):
+def test_persistent_launch_shapes(fname, warps, window, layout, stages, occupancy):
     """Lane layout and sweep window only change how pairs are spread over lanes and how j
     partials are reduced across the warp: every launch shape gives the same pair set and
     forces within FP32 rounding."""
@@ -218,10 +218,10 @@ def test_persistent_launch_shapes(fname, warps, window, layout, stages):
     e = M.Engine.from_system(sysm)
     e.tune(warps)
     e.set_window(window)
-    e.set_layout(layout, stages)
+    e.set_layout(layout, stages, occupancy)
     e.nonbond()
     check_against_oracle(sysm, ref["tables"], e.forces(), e.stats(),
-                         f"warps={warps} window={window} layout={layout} stages={stages}")
+                         f"warps={warps} window={window} layout={layout} stages={stages} occupancy={occupancy}")
     e.close()
 
 
@@ -241,8 +241,8 @@ def test_autotune_keeps_results():
     sysm, ref = load_golden("water_3000.npz")
     e = M.Engine.from_system(sysm)
     e.load_parts()
-    warps, layout, stages, ms = e.autotune(reps=3)
-    assert warps in (2, 4, 8) and layout in (0, 1) and stages in (1, 2) and ms > 0
+    warps, layout, stages, occ, ms = e.autotune(reps=3)
+    assert warps in (2, 4, 8) and layout in (0, 1) and stages in (1, 2) and occ in (640, 768, 1024) and ms > 0
     e.unload_parts()
     check_against_oracle(sysm, ref["tables"], e.forces(), e.stats(), "autotuned")
     e.close()
