@@ -361,6 +361,9 @@ int engine_nonbond_cuda_resident(struct engine *e);
 int engine_set_dt(struct engine *e, double dt);
 /* Zeroes forces and energies ahead of a stand-alone engine_nonbond_cuda call. */
 int engine_zero_forces(struct engine *e);
+/* engine_zero_forces + engine_nonbond_cuda in one pass over the particles: the cells'
+ * forces and energies become those of this evaluation (engine_step uses it). */
+int engine_nonbond_cuda_fresh(struct engine *e);
 /* Makes later launches use this cudaStream_t (e.g. the caller framework's stream). */
 int engine_cuda_setstream(struct engine *e, void *stream);
 /* Device time (ms) of the last evaluation: sort + sweep, and the sweep kernel alone. */
@@ -473,6 +476,8 @@ int engine_batch_create(struct engine **engines, int n, struct engine_batch **ou
 int engine_batch_free(struct engine_batch *b);
 /* engine_nonbond_cuda for every engine: upload, sort + sweep, download. */
 int engine_batch_nonbond(struct engine_batch *b);
+/* engine_nonbond_cuda_fresh for every engine. */
+int engine_batch_nonbond_fresh(struct engine_batch *b);
 /* engine_step for every engine with the forces of one batch evaluation. */
 int engine_batch_step(struct engine_batch *b);
 int engine_batch_load_parts(struct engine_batch *b);

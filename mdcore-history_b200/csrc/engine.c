@@ -390,9 +390,8 @@ int engine_step(struct engine *e) {
     struct space *s = &e->s;
     e->time += 1;
     if (space_shuffle(s) < 0) return engine_error(engine_err_space);
-    s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
-    nb_zero_cells(s);
-    if (engine_nonbond_cuda(e) < 0) return engine_error(engine_err_cuda);
+    /* space_prepare's zeroing and the force evaluation in one pass over the particles */
+    if (engine_nonbond_cuda_fresh(e) < 0) return engine_error(engine_err_cuda);
     s->epot += s->epot_nonbond;
     if (engine_advance(e) < 0) return engine_error(engine_err);
     /* Resolve the rigid constraints (src/engine.c:2196-2231). */

@@ -44,6 +44,7 @@ struct NbState {
     std::vector<struct engine*> engines;
     std::vector<int> cell_off, id_off;
     std::vector<struct cell*> flat_cells;  // every engine's cells in global order
+    std::vector<cudaEvent_t> chunk_ev;     // one per download chunk
     struct nb_stats bstats = {};           // totals of the last evaluation over all engines
     // geometry
     int ncells = 0, ntasks = 0, ncap = 0, nid = 0;
@@ -163,8 +164,10 @@ int alloc_particles(NbState* st, int ncap) {
     if (dev_alloc(&st->d_xq, ncap) || dev_alloc(&st->d_pid, ncap) || dev_alloc(&st->d_keys, 13 * (size_t)ncap) ||
         dev_alloc(&st->d_force, 3 * (size_t)ncap))
         return engine_err_cuda;
-    CU(cudaMallocHost(&st->h_xq, sizeof(float4) * ncap));
-    CU(cudaMallocHost(&st->h_pid, sizeof(int) * ncap));
+    // Upload buffers are only written by the host: write-combined pages take the writes
+    // without reading the lines first and stream faster over PCIe.
+    CU(cudaHostAlloc(&st->h_xq, sizeof(float4) * ncap, cudaHostAllocWriteCombined));
+    CU(cudaHostAlloc(&st->h_pid, sizeof(int) * ncap, cudaHostAllocWriteCombined));
     CU(cudaMallocHost(&st->h_force, sizeof(unsigned long long) * 3 * ncap));
     cudaFree(st->d_forcef);
     if (dev_alloc(&st->d_forcef, 3 * (size_t)ncap)) return engine_err_cuda;
@@ -198,9 +201,9 @@ int cell_grain(const NbState* st) {
     return (int)std::max(16LL, 8192 / avg);
 }
 
-// Packs every engine's cells into the pinned staging buffers (host threads over ranges of
-// cells: counts, then slot offsets, then positions and ids); returns the number of slots.
-int pack_cells(NbState* st) {
+// Slot layout of this evaluation (host threads over ranges of cells): counts, padded slot
+// offsets, the largest cell; grows the buffers.  Returns the number of slots.
+int prepare_slots(NbState* st) {
     HostPool& pool = HostPool::get();
     const int nc = st->ncells;
     int* cstart = st->h_cstart;
@@ -233,28 +236,61 @@ int pack_cells(NbState* st) {
     if (alloc_particles(st, total + 4) < 0) return engine_err_cuda;
     pool.run(nc, grain, [&](int part, int b, int e) {
         int slot = part_slots[part];
-        size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), b) - st->cell_off.begin() - 1;
         for (int c = b; c < e; c++) {
-            while (c >= st->cell_off[k + 1]) k++;
-            const int id0 = st->id_off[k];
-            const struct cell* cl = cells[c];
             cstart[c] = slot;
-            for (int q = 0; q < cl->count; q++) {
-                const struct part* p = &cl->parts[q];
-                st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
-                st->h_pid[slot + q] = id0 + p->id;
-            }
-            const int pad = (cl->count + 3) & ~3;
-            for (int q = cl->count; q < pad; q++) {
-                st->h_xq[slot + q] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
-                st->h_pid[slot + q] = 0;
-            }
-            slot += pad;
+            slot += (ccount[c] + 3) & ~3;
         }
     });
     cstart[nc] = total;
     st->maxcount = maxc;
     return total;
+}
+
+// Packs cells [cb, ce) into the pinned upload buffers (host threads over ranges of cells):
+// positions and types, and particle ids when the system has exclusions.
+void pack_range(NbState* st, int cb, int ce) {
+    const int* cstart = st->h_cstart;
+    HostPool::get().run(ce - cb, cell_grain(st), [&](int, int b, int e) {
+        size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), cb + b) - st->cell_off.begin() - 1;
+        for (int c = cb + b; c < cb + e; c++) {
+            while (c >= st->cell_off[k + 1]) k++;
+            const int id0 = st->id_off[k];
+            const struct cell* cl = st->flat_cells[c];
+            const int slot = cstart[c];
+            const int pad = (cl->count + 3) & ~3;
+            for (int q = 0; q < cl->count; q++) {
+                const struct part* p = &cl->parts[q];
+                st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
+            }
+            for (int q = cl->count; q < pad; q++) st->h_xq[slot + q] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
+            if (st->has_excl) {          // ids are read by the sweep for exclusion tests only
+                for (int q = 0; q < cl->count; q++) st->h_pid[slot + q] = id0 + cl->parts[q].id;
+                for (int q = cl->count; q < pad; q++) st->h_pid[slot + q] = 0;
+            }
+        }
+    });
+}
+
+// Cell ranges of the host<->device pipeline: large systems move in up to 8 chunks of about
+// 256k slots, so that packing (unpacking) one chunk overlaps the copy of another.
+std::vector<int> chunk_bounds(const NbState* st, int total) {
+    const int k = std::max(1, std::min(8, total / 262144));
+    std::vector<int> bounds(k + 1, st->ncells);
+    bounds[0] = 0;
+    for (int q = 1; q < k; q++) {
+        const long long target = (long long)total * q / k;
+        bounds[q] = (int)(std::lower_bound(st->h_cstart, st->h_cstart + st->ncells, (int)target) - st->h_cstart);
+    }
+    return bounds;
+}
+
+int chunk_events(NbState* st, size_t n) {
+    while (st->chunk_ev.size() < n) {
+        cudaEvent_t ev;
+        CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        st->chunk_ev.push_back(ev);
+    }
+    return 0;
 }
 
 template <int NW>
@@ -549,6 +585,7 @@ void state_free(NbState* st) {
     if (st->ev1) cudaEventDestroy(st->ev1);
     if (st->evs0) cudaEventDestroy(st->evs0);
     if (st->evs1) cudaEventDestroy(st->evs1);
+    for (cudaEvent_t ev : st->chunk_ev) cudaEventDestroy(ev);
     if (st->own_stream) cudaStreamDestroy(st->own_stream);
     sched_free(st->sched);
     delete st;
@@ -772,16 +809,28 @@ void share_times(NbState* st) {
     }
 }
 
+// Packs and uploads the particles: slot layout, then chunk by chunk (pack on host threads,
+// one asynchronous copy per array), so that the copy of a chunk overlaps the packing of the
+// next.
 int st_load_parts(NbState* st) {
     CU(cudaSetDevice(st->device));
     const double t0 = now_ms();
-    const int slots = pack_cells(st);
+    const int slots = prepare_slots(st);
     if (slots < 0) return slots;
+    const std::vector<int> bounds = chunk_bounds(st, slots);
+    for (size_t q = 0; q + 1 < bounds.size(); q++) {
+        const int cb = bounds[q], ce = bounds[q + 1];
+        if (ce <= cb) continue;
+        pack_range(st, cb, ce);
+        const int s0 = st->h_cstart[cb], n = st->h_cstart[ce] - s0;
+        if (n <= 0) continue;
+        CU(cudaMemcpyAsync(st->d_xq + s0, st->h_xq + s0, sizeof(float4) * n, cudaMemcpyHostToDevice, st->stream));
+        if (st->has_excl)
+            CU(cudaMemcpyAsync(st->d_pid + s0, st->h_pid + s0, sizeof(int) * n, cudaMemcpyHostToDevice, st->stream));
+    }
     const double t1 = now_ms();
     st->bstats.ms_pack = (float)(t1 - t0);
     st->bstats.ms_device = 0.f;
-    CU(cudaMemcpyAsync(st->d_xq, st->h_xq, sizeof(float4) * slots, cudaMemcpyHostToDevice, st->stream));
-    CU(cudaMemcpyAsync(st->d_pid, st->h_pid, sizeof(int) * slots, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->d_cstart, st->h_cstart, sizeof(int) * (st->ncells + 1), cudaMemcpyHostToDevice,
                        st->stream));
     CU(cudaMemcpyAsync(st->d_ccount, st->h_cstart + st->ncells + 1, sizeof(int) * st->ncells,
@@ -792,7 +841,32 @@ int st_load_parts(NbState* st) {
 }
 
 // Copies forces and energies of the last evaluation back into the engines' cells.
-int st_unload_parts(NbState* st) {
+// Forces of cells [cb, ce) from the download buffer into the cells (host threads): added,
+// or, when fresh, replacing the cells' forces.
+void unpack_range(NbState* st, const float* hf, int cb, int ce, bool fresh) {
+    HostPool::get().run(ce - cb, cell_grain(st), [&](int, int b, int e) {
+        for (int c = cb + b; c < cb + e; c++) {
+            struct cell* cl = st->flat_cells[c];
+            const float* f = hf + 3 * (size_t)st->h_cstart[c];
+            if (fresh)
+                for (int q = 0; q < cl->count; q++) {
+                    cl->parts[q].f[0] = f[3 * q];
+                    cl->parts[q].f[1] = f[3 * q + 1];
+                    cl->parts[q].f[2] = f[3 * q + 2];
+                }
+            else
+                for (int q = 0; q < cl->count; q++) {
+                    cl->parts[q].f[0] += f[3 * q];
+                    cl->parts[q].f[1] += f[3 * q + 1];
+                    cl->parts[q].f[2] += f[3 * q + 2];
+                }
+        }
+    });
+}
+
+// fresh: the evaluation's forces and energies replace those of the cells (one pass over
+// the particles instead of zeroing them first); otherwise they are added.
+int st_unload_parts(NbState* st, bool fresh = false) {
     CU(cudaSetDevice(st->device));
     const int slots = st->h_cstart[st->ncells];
     const double t0 = now_ms();
@@ -801,11 +875,28 @@ int st_unload_parts(NbState* st) {
         CU(cudaGetLastError());
     }
     float* hf = reinterpret_cast<float*>(st->h_force);
-    CU(cudaMemcpyAsync(hf, st->d_forcef, sizeof(float) * 3 * (size_t)slots, cudaMemcpyDeviceToHost, st->stream));
+    const std::vector<int> bounds = chunk_bounds(st, slots);
+    const size_t nch = bounds.size() - 1;
+    if (chunk_events(st, nch) < 0) return engine_err_cuda;
+    for (size_t q = 0; q < nch; q++) {
+        const int s0 = st->h_cstart[bounds[q]], n = st->h_cstart[bounds[q + 1]] - s0;
+        if (n > 0)
+            CU(cudaMemcpyAsync(hf + 3 * (size_t)s0, st->d_forcef + 3 * (size_t)s0, sizeof(float) * 3 * (size_t)n,
+                               cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaEventRecord(st->chunk_ev[q], st->stream));
+    }
     CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
+    // Forces chunk by chunk as they arrive (the unpacking of one overlaps the copy of the next).
+    double t_unpack = 0.0;
+    for (size_t q = 0; q < nch; q++) {
+        CU(cudaEventSynchronize(st->chunk_ev[q]));
+        const double u0 = now_ms();
+        unpack_range(st, hf, bounds[q], bounds[q + 1], fresh);
+        t_unpack += now_ms() - u0;
+    }
     CU(cudaStreamSynchronize(st->stream));
     const double t1 = now_ms();
     float ms = 0.f;
@@ -815,20 +906,14 @@ int st_unload_parts(NbState* st) {
         st->bstats.ms_kernels = ms;
     else
         cudaGetLastError();
-    const int rc = finish_stats(st);
-    HostPool::get().run(st->ncells, cell_grain(st), [&](int, int b, int e) {
-        for (int c = b; c < e; c++) {
-            struct cell* cl = st->flat_cells[c];
-            const float* f = hf + 3 * (size_t)st->h_cstart[c];
-            for (int q = 0; q < cl->count; q++) {
-                cl->parts[q].f[0] += f[3 * q];
-                cl->parts[q].f[1] += f[3 * q + 1];
-                cl->parts[q].f[2] += f[3 * q + 2];
-            }
+    if (fresh)
+        for (struct engine* e : st->engines) {
+            struct space* s = &e->s;
+            s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
         }
-    });
-    st->bstats.ms_device += (float)(t1 - t0);
-    st->bstats.ms_unpack = (float)(now_ms() - t1);
+    const int rc = finish_stats(st);
+    st->bstats.ms_device += (float)(t1 - t0 - t_unpack);
+    st->bstats.ms_unpack = (float)(t_unpack + (now_ms() - t1));
     share_times(st);
     return rc;
 }
@@ -847,12 +932,12 @@ int st_resident(NbState* st) {
     return 0;
 }
 
-int st_nonbond(NbState* st) {
+int st_nonbond(NbState* st, bool fresh = false) {
     int rc = st_load_parts(st);
     if (rc < 0) return rc;
     rc = st_resident(st);
     if (rc < 0) return rc;
-    return st_unload_parts(st);
+    return st_unload_parts(st, fresh);
 }
 
 int st_setstream(NbState* st, void* stream) {
@@ -1062,6 +1147,13 @@ extern "C" int engine_nonbond_cuda(struct engine* e) {
     return st_nonbond(state(e));
 }
 
+// engine_zero_forces + engine_nonbond_cuda in one pass over the particles.
+extern "C" int engine_nonbond_cuda_fresh(struct engine* e) {
+    if (e == nullptr) return engine_err_null;
+    if (e->cuda == nullptr && engine_cuda_load(e) < 0) return engine_err_cuda;
+    return st_nonbond(state(e), true);
+}
+
 // Sort + sweep on the particles already resident on the device (no host copies, no
 // synchronisation); results stay on the device until engine_cuda_unload_parts.
 extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
@@ -1151,6 +1243,11 @@ extern "C" int engine_batch_nonbond(struct engine_batch* b) {
     return st_nonbond(bstate(b));
 }
 
+extern "C" int engine_batch_nonbond_fresh(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_nonbond(bstate(b), true);
+}
+
 // One time step of every engine: re-binning, force evaluation in one batch, symplectic
 // Euler update (engine_step for each engine, with the forces computed together).
 extern "C" int engine_batch_step(struct engine_batch* b) {
@@ -1160,8 +1257,7 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
         e->time += 1;
         if (space_shuffle(&e->s) < 0) return engine_err = engine_err_space;
     }
-    engine_batch_zero_forces(b);
-    const int rc = st_nonbond(st);
+    const int rc = st_nonbond(st, true);
     if (rc < 0) return rc;
     for (struct engine* e : st->engines) {
         e->s.epot += e->s.epot_nonbond;

@@ -94,6 +94,8 @@ def lib() -> C.CDLL:
         "engine_cuda_setdevice": (C.c_int, [vp, C.c_int]),
         "engine_cuda_load": (C.c_int, [vp]),
         "engine_nonbond_cuda": (C.c_int, [vp]),
+        "engine_nonbond_cuda_fresh": (C.c_int, [vp]),
+        "engine_batch_nonbond_fresh": (C.c_int, [vp]),
         "engine_cuda_load_parts": (C.c_int, [vp]),
         "engine_cuda_unload_parts": (C.c_int, [vp]),
         "engine_nonbond_cuda_resident": (C.c_int, [vp]),
@@ -257,9 +259,9 @@ class Engine:
 
     # -- force evaluation ----------------------------------------------------------
     def nonbond(self):
-        """One force evaluation at the current positions (host buffers in and out)."""
-        _check(self.lib.engine_zero_forces(self.ptr), "engine_zero_forces")
-        _check(self.lib.engine_nonbond_cuda(self.ptr), "engine_nonbond_cuda")
+        """One force evaluation at the current positions (host buffers in and out): the
+        cells' forces and energies become this evaluation's (engine_nonbond_cuda_fresh)."""
+        _check(self.lib.engine_nonbond_cuda_fresh(self.ptr), "engine_nonbond_cuda_fresh")
         return self
 
     def step(self):
@@ -463,8 +465,7 @@ class Batch:
 
     def nonbond(self):
         """One force evaluation of every engine (host buffers in and out)."""
-        self._zero()
-        _check(self.lib.engine_batch_nonbond(self.ptr), "engine_batch_nonbond")
+        _check(self.lib.engine_batch_nonbond_fresh(self.ptr), "engine_batch_nonbond_fresh")
         return self
 
     def step(self):
