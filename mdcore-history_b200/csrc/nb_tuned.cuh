@@ -467,30 +467,81 @@ __device__ __forceinline__ int sorted_prefix(const int* __restrict__ jdist, int 
 // exactly rounded r^2, potential lookup, exclusion test, table evaluation.  Returns the
 // force contribution on j (w) and adds -w to the i force; counts candidates, pairs and
 // excluded pairs.
+// The exclusions of lane's particle i, for the sweep: its bit mask of partners at id
+// offsets -16..16, the range [lo, lo + span] of offsets the mask covers (an empty range
+// when the mask is empty), and its CSR list of farther partners.
+struct IExcl {
+    int pid;
+    unsigned emask;
+    int lo, span;
+    int exlo, exhi;
+};
+
+__device__ __forceinline__ IExcl load_iexcl(const Params& P, int pid) {
+    IExcl x;
+    x.pid = pid;
+    x.emask = P.emask[pid];
+    x.exlo = P.exoff[pid];
+    x.exhi = P.exoff[pid + 1];
+    if (x.emask) {                     // bit b <-> offset b - 16 (b < 16) or b - 15 (b >= 16)
+        const int bl = __ffs(x.emask) - 1, bh = 31 - __clz(x.emask);
+        x.lo = bl < 16 ? bl - 16 : bl - 15;
+        x.span = (bh < 16 ? bh - 16 : bh - 15) - x.lo;
+    } else {
+        x.lo = 0x40000000;             // no offset d satisfies 0 <= d - lo <= span
+        x.span = 0;
+    }
+    return x;
+}
+
+__device__ __forceinline__ IExcl no_iexcl() {
+    IExcl x;
+    x.pid = 0; x.emask = 0u; x.lo = 0x40000000; x.span = 0; x.exlo = 0; x.exhi = 0;
+    return x;
+}
+
+// 1/sqrt(x) from the hardware approximation (x is never denormal here: r^2 of two
+// particles is at least ~1e-3 nm^2), refined by the caller.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Candidates a lane examines in a strip: the sweep positions k < len of its column
+// (stride = lanes per row of j: 4 in the 8 x 4 tile, 1 with 32 i per warp).
+__device__ __forceinline__ unsigned strip_candidates(int len, int col, int stride) {
+    return len > col ? (unsigned)((len - col + stride - 1) / stride) : 0u;
+}
+
 template <bool HAS_EXCL, bool ONE_POT>
 __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& S, const float4 xj,
                                            const int* __restrict__ jids, int k, bool act,
-                                           float pix, float piy, float piz, int prow, int pidi, unsigned emask,
-                                           int exlo, int exhi, float cut2, float& fix, float& fiy, float& fiz,
+                                           float pix, float piy, float piz, int prow, const IExcl& ix,
+                                           float cut2, float& fix, float& fiy, float& fiz,
                                            float& wx, float& wy, float& wz, double& e_task, unsigned& npairs,
-                                           unsigned& nexcl, unsigned& ncand, bool& any_acc) {
+                                           unsigned& nexcl, bool& any_acc) {
     constexpr unsigned FULL = 0xffffffffu;
     const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     int pot = 0;
     if (!ONE_POT) pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
     bool acc = act && pot >= 0 && r2 <= cut2;
-    ncand += act;
-    if (HAS_EXCL && acc) {
-        const int d = jids[k] - pidi;
-        bool ex;
-        if ((unsigned)(d + 16) <= 32u)
-            ex = (emask >> (d + 16 - (d > 0))) & (d != 0);
-        else {
-            ex = false;
-            for (int qx = exlo; qx < exhi; ++qx) ex |= (P.exlist[qx] == pidi + d);
+    if (HAS_EXCL) {
+        // One window test per candidate; the mask bit or the list is looked at only for
+        // ids inside the particle's exclusion window (or when it has far partners).
+        const int d = jids[k] - ix.pid;
+        const bool inwin = (unsigned)(d - ix.lo) <= (unsigned)ix.span;
+        if (acc && (inwin || ix.exhi > ix.exlo)) {
+            bool ex;
+            if (inwin)
+                ex = (ix.emask >> (d + 16 - (d > 0))) & 1u;
+            else {
+                ex = false;
+                for (int qx = ix.exlo; qx < ix.exhi; ++qx) ex |= (P.exlist[qx] == ix.pid + d);
+            }
+            if (ex) { acc = false; ++nexcl; }
         }
-        if (ex) { acc = false; ++nexcl; }
     }
     wx = 0.f; wy = 0.f; wz = 0.f;
     if (__any_sync(FULL, acc)) {
@@ -500,7 +551,7 @@ __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& 
             // which gives the correctly rounded square root (the water energy is ~250x
             // smaller than the sum of |pair energies|, so unbiased 1-ulp errors in r would
             // show at 1e-6).
-            float rinv = rsqrtf(r2);
+            float rinv = rsqrt_approx(r2);
             rinv = fmaf(-0.5f * rinv, fmaf(r2 * rinv, rinv, -1.0f), rinv);
             float r = r2 * rinv;
             r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
@@ -667,19 +718,14 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-            int pidi = 0, exlo = 0, exhi = 0;
-            unsigned emask = 0u;
+            IExcl ix = no_iexcl();
             if (valid) {
                 xi = self ? W.js[loc] : P.xq[si + loc];
-                if (HAS_EXCL) {
-                    pidi = self ? W.pidraw[loc] : P.pid[si + loc];
-                    emask = P.emask[pidi];
-                    exlo = P.exoff[pidi];
-                    exhi = P.exoff[pidi + 1];
-                }
+                if (HAS_EXCL) ix = load_iexcl(P, self ? W.pidraw[loc] : P.pid[si + loc]);
             }
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
+            ncand += strip_candidates(len, 0, 1);
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
             for (int k0 = 0; k0 < kmax; k0 += WIN) {
                 float vx[WIN], vy[WIN], vz[WIN];
@@ -687,9 +733,9 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
 #pragma unroll
                 for (int m = 0; m < WIN; ++m) {
                     const int k = k0 + m;
-                    pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, pidi, emask,
-                                                  exlo, exhi, cut2, fix, fiy, fiz, vx[m], vy[m], vz[m], e_task,
-                                                  npairs, nexcl, ncand, any_acc);
+                    pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, ix, cut2,
+                                                  fix, fiy, fiz, vx[m], vy[m], vz[m], e_task, npairs, nexcl,
+                                                  any_acc);
                 }
                 if (any_acc) {
                     float tx, ty, tz;
@@ -785,19 +831,14 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-            int pidi = 0, exlo = 0, exhi = 0;
-            unsigned emask = 0u;
+            IExcl ix = no_iexcl();
             if (valid) {
                 xi = self ? W.js[loc] : P.xq[si + loc];
-                if (HAS_EXCL) {
-                    pidi = self ? W.pidraw[loc] : P.pid[si + loc];
-                    emask = P.emask[pidi];
-                    exlo = P.exoff[pidi];
-                    exhi = P.exoff[pidi + 1];
-                }
+                if (HAS_EXCL) ix = load_iexcl(P, self ? W.pidraw[loc] : P.pid[si + loc]);
             }
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
+            ncand += strip_candidates(len, col, 4);
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
             for (int k0 = 0; k0 < kmax; k0 += 4 * WIN) {
                 float vx[WIN], vy[WIN], vz[WIN];
@@ -806,9 +847,9 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
                 for (int m = 0; m < WIN; ++m) {
                     if (k0 + 4 * m < kmax) {                 // warp-uniform
                         const int k = k0 + 4 * m + col;
-                        pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, pidi,
-                                                      emask, exlo, exhi, cut2, fix, fiy, fiz, vx[m], vy[m], vz[m],
-                                                      e_task, npairs, nexcl, ncand, any_acc);
+                        pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, ix,
+                                                      cut2, fix, fiy, fiz, vx[m], vy[m], vz[m], e_task, npairs,
+                                                      nexcl, any_acc);
                     } else {
                         vx[m] = 0.f; vy[m] = 0.f; vz[m] = 0.f;
                     }
