@@ -122,6 +122,25 @@ def run_reference_driver(sysm, threads, warmup, steps):
     return json.loads(line)
 
 
+def run_reference_md(threads, warmup, steps):
+    """The reference's engine_step on rigid SPC/E water (P-SHAKE, dt = 2 fs), all runners."""
+    import workloads as W
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    sysm = W.with_rigid_water(W.water_spce(32), 300.0, seed=1)
+    with tempfile.TemporaryDirectory() as tmp:
+        sysf, rigf = os.path.join(tmp, "water.sys"), os.path.join(tmp, "water.rig")
+        W.write_sysfile(sysm, sysf)
+        W.write_rigidfile(sysm, rigf, shake=False)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
+        r = subprocess.run([exe, "mdbench", sysf, rigf, str(threads), str(warmup), str(steps)], capture_output=True,
+                           text=True, env=env, check=True)
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    return {"ms_per_step": d["ms_per_step"], "ns_per_day": ns_per_day(d["ms_per_step"]), "steps": steps,
+            "cores": threads, "what": "reference engine_step of rigid SPC/E water (P-SHAKE), pthreads runners"}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -164,6 +183,12 @@ def reference_arm(args, rank):
     ms = cb.pop("ms_per_step")
     v = cb["value"]
     pairs = sum(pair_count(s) for s in systems)
+    md = None
+    if SELECTED == "water":
+        try:
+            md = run_reference_md(threads, 2, max(2, min(args.steps, 10)))
+        except (FileNotFoundError, subprocess.CalledProcessError) as exc:
+            md = {"unavailable": str(exc)}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 1, "ms_per_step": pairs / v * 1e3,
@@ -173,6 +198,7 @@ def reference_arm(args, rank):
                    "sample_ms_per_step": ms},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        **({"md_step": md} if md is not None else {}),
     }))
 
 
@@ -315,6 +341,37 @@ def ours(args, rank, world, local_rank):
     if tgt.stats().status != 0:
         raise SystemExit("bench.py: device status after e2e region")
 
+    # ---- water: full MD steps (engine_step: rebin, forces, integration, P-SHAKE on the
+    # device) of the rigid SPC/E system, dt = 2 fs
+    md = None
+    if SELECTED == "water":
+        import workloads as W
+        rig = M.Engine.from_system(W.with_rigid_water(W.water_spce(32), 300.0, seed=1), device=local_rank)
+        rig.set_stream(stream.cuda_stream)
+        rig.load_parts()
+        rig.tune(warps)
+        rig.set_layout(layout, stages, occupancy)
+        rig.graph(True)
+        for _ in range(max(args.warmup, 25)):        # past the 20 P-SHAKE refinement steps
+            rig.step()
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rig.step()
+        ev1.record(stream)
+        ev1.synchronize()
+        md_ms = ev0.elapsed_time(ev1) / args.steps
+        itmax, bad = rig.rigid_stats()
+        if rig.stats().status != 0 or bad != 0:
+            raise SystemExit("bench.py: rigid water steps failed")
+        md = {"ms_per_step": md_ms, "ns_per_day": ns_per_day(md_ms), "dt_fs": DT_FS,
+              "what": "engine_step of rigid SPC/E water (32,768 molecules, 98,304 constraints): rebin, "
+                      "forces with host buffers, symplectic Euler, P-SHAKE on the device (FP64)",
+              "shake_max_iterations": itmax}
+        rig.close()
+
     # ---- the plain form (one CTA per task, IEEE sqrt/div, no graph), same protocol
     tgt.graph(False)
     tgt.tune(0, plain=True)
@@ -397,8 +454,15 @@ def ours(args, rank, world, local_rank):
         }
         if seq is not None:
             line["sequential_plain"] = seq
+        if md is not None:
+            line["md_step"] = md
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_sample(systems, host_threads())
+            if md is not None:
+                try:
+                    line["cpu_baseline"]["md_step"] = run_reference_md(host_threads(), 2, 5)
+                except (FileNotFoundError, subprocess.CalledProcessError) as exc:
+                    line["cpu_baseline"]["md_step"] = {"unavailable": str(exc)}
         print(json.dumps(line))
     tgt.close()
     for e in engines:

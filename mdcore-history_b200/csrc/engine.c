@@ -363,15 +363,15 @@ int engine_start(struct engine *e, int nr_runners, int nr_queues) {
 }
 
 /* Symplectic Euler update v += f/m dt, x += v dt, as src/engine.c:1945-2052; particles
- * that leave their cell are moved at the start of the next step. */
-int engine_advance(struct engine *e) {
-    if (e == NULL) return engine_error(engine_err_null);
+ * that leave their cell are moved at the start of the next step.  Host threads over
+ * ranges of cells. */
+static void advance_cells(void *ctx, int part, int begin, int end) {
+    struct engine *e = ctx;
     struct space *s = &e->s;
     float dt = e->dt;
-    double epot = 0.0;
-    for (int c = 0; c < s->nr_cells; c++) {
+    (void)part;
+    for (int c = begin; c < end; c++) {
         struct cell *cl = &s->cells[c];
-        epot += cl->epot;
         for (int k = 0; k < cl->count; k++) {
             struct part *p = &cl->parts[k];
             float w = dt * e->types[p->type].imass;
@@ -381,7 +381,13 @@ int engine_advance(struct engine *e) {
             }
         }
     }
-    (void)epot;
+}
+
+int engine_advance(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    struct space *s = &e->s;
+    int grain = 8192 / (s->nr_parts / (s->nr_cells > 0 ? s->nr_cells : 1) + 1);
+    nb_parallel_for(s->nr_cells, grain < 16 ? 16 : grain, advance_cells, e);
     return engine_err_ok;
 }
 

@@ -25,6 +25,11 @@ int nb_device_free(struct engine *e);
 int rigid_device_free(struct engine *e);
 /* Zeroes forces and energies of every cell of s (host threads over ranges of cells). */
 void nb_zero_cells(struct space *s);
+/* Calls fn(ctx, part, begin, end) over contiguous ranges of [0, n) of at least `grain`
+ * items on the engine's host threads and returns when all are done; nb_host_parts() is
+ * the largest number of ranges (parts are numbered from 0). */
+void nb_parallel_for(int n, int grain, void (*fn)(void *ctx, int part, int begin, int end), void *ctx);
+int nb_host_parts(void);
 /* Launch stream of the engine's device state (NULL before engine_cuda_load). */
 void *nb_engine_stream(struct engine *e);
 

@@ -1037,6 +1037,12 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
 
 // ---------------------------------------------------------------- single engine
 
+extern "C" void nb_parallel_for(int n, int grain, void (*fn)(void*, int, int, int), void* ctx) {
+    HostPool::get().run(n, grain, [&](int part, int b, int e) { fn(ctx, part, b, e); });
+}
+
+extern "C" int nb_host_parts(void) { return HostPool::get().threads(); }
+
 extern "C" void nb_zero_cells(struct space* s) {
     const int grain = (int)std::max(16, 8192 / (s->nr_parts / std::max(1, s->nr_cells) + 1));
     HostPool::get().run(s->nr_cells, grain, [&](int, int b, int e) {

@@ -20,6 +20,9 @@
 #include <cuda_runtime.h>
 #include "mdcore_b200.h"
 #include "internal.h"
+#include "host_pool.h"
+
+using nb::HostPool;
 
 namespace {
 
@@ -351,8 +354,10 @@ extern "C" int engine_rigid_eval(struct engine* e) {
     struct space* s = &e->s;
     const bool pshake = !(e->flags & engine_flag_shake);
 
-    // Pack: cell-relative positions, velocities and shift codes of every group's particles.
-    for (int g = 0; g < rd->nrig; g++) {
+    // Pack: cell-relative positions, velocities and shift codes of every group's particles
+    // (host threads over ranges of groups).
+    HostPool::get().run(rd->nrig, 1024, [&](int, int gb, int ge) {
+    for (int g = gb; g < ge; g++) {
         const struct rigid* r = &e->rigids[g];
         const int p0 = rd->roff[g];
         bool local = true;
@@ -376,6 +381,7 @@ extern "C" int engine_rigid_eval(struct engine* e) {
             rd->h_v[p0 + k] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
         }
     }
+    });
     const size_t ns = (size_t)rd->nslots;
     CU(cudaMemcpyAsync(rd->d_x, rd->h_x, sizeof(float4) * ns, cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(rd->d_v, rd->h_v, sizeof(float4) * ns, cudaMemcpyHostToDevice, stream));
@@ -413,7 +419,8 @@ extern "C" int engine_rigid_eval(struct engine* e) {
 
     // Corrections, src/rigid.c:236-262 (SHAKE) and src/rigid.c:486-511 (P-SHAKE).
     const double idt = 1.0 / e->dt;
-    for (int g = 0; g < rd->nrig; g++) {
+    HostPool::get().run(rd->nrig, 1024, [&](int, int gb, int ge) {
+    for (int g = gb; g < ge; g++) {
         const struct rigid* r = &e->rigids[g];
         const int p0 = rd->roff[g];
         if (rd->skip[g]) continue;
@@ -431,6 +438,7 @@ extern "C" int engine_rigid_eval(struct engine* e) {
             }
         }
     }
+    });
     return 0;
 }
 

@@ -239,13 +239,31 @@ void space_relink(struct space *s, struct cell *c) {
     }
 }
 
-/* Move particles that left their cell into the neighbour cell (periodic wrap), as
- * src/space.c:307-364 does after each integration step. */
-int space_shuffle(struct space *s) {
+/* Particles that left their cell move into the neighbour cell (periodic wrap), as
+ * src/space.c:307-364 does after each integration step: like the reference's incoming
+ * buffers, arrivals are appended after every cell has been scanned.  A parallel scan in
+ * which every host thread takes the leavers out of its own range of cells; the arrivals in
+ * cell and particle order (independent of the number of threads); then the
+ * partlist/celllist entries of the cells that changed. */
+struct shuffle_mover {
+    struct part p;
+    int dst;
+};
+
+struct shuffle_ctx {
+    struct space *s;
+    struct shuffle_mover **lists;
+    int *count, *size;
+    unsigned char *touched;
+    int fail;
+};
+
+static void shuffle_scan(void *vctx, int part, int begin, int end) {
+    struct shuffle_ctx *ctx = vctx;
+    struct space *s = ctx->s;
     float h[3];
     for (int k = 0; k < 3; k++) h[k] = s->h[k];
-    int moved = 0;
-    for (int cid = 0; cid < s->nr_cells; cid++) {
+    for (int cid = begin; cid < end; cid++) {
         struct cell *c = &s->cells[cid];
         int pid = 0;
         while (pid < c->count) {
@@ -253,22 +271,72 @@ int space_shuffle(struct space *s) {
             int delta[3];
             for (int k = 0; k < 3; k++) delta[k] = (p->x[k] >= h[k]) - (p->x[k] < 0.0f);
             if (delta[0] || delta[1] || delta[2]) {
-                struct part tmp = *p;
-                for (int k = 0; k < 3; k++) tmp.x[k] -= delta[k] * h[k];
+                if (ctx->count[part] == ctx->size[part]) {
+                    int nsize = ctx->size[part] * 2 + 64;
+                    struct shuffle_mover *nl = realloc(ctx->lists[part], sizeof(struct shuffle_mover) * nsize);
+                    if (nl == NULL) {
+                        ctx->fail = 1;
+                        return;
+                    }
+                    ctx->lists[part] = nl;
+                    ctx->size[part] = nsize;
+                }
+                struct shuffle_mover *m = &ctx->lists[part][ctx->count[part]++];
+                m->p = *p;
+                for (int k = 0; k < 3; k++) m->p.x[k] -= delta[k] * h[k];
                 int nl[3];
                 for (int k = 0; k < 3; k++) nl[k] = (c->loc[k] + delta[k] + s->cdim[k]) % s->cdim[k];
-                struct cell *dst = &s->cells[space_cellid(s, nl[0], nl[1], nl[2])];
+                m->dst = space_cellid(s, nl[0], nl[1], nl[2]);
                 c->count -= 1;
                 if (pid < c->count) c->parts[pid] = c->parts[c->count];
-                if (cell_add(dst, &tmp) == NULL) return space_error(space_err_malloc);
-                moved = 1;
+                ctx->touched[cid] = 1;
             } else
                 pid += 1;
         }
     }
-    if (moved)
-        for (int cid = 0; cid < s->nr_cells; cid++) space_relink(s, &s->cells[cid]);
-    return moved;
+}
+
+static void shuffle_relink(void *vctx, int part, int begin, int end) {
+    struct shuffle_ctx *ctx = vctx;
+    (void)part;
+    for (int cid = begin; cid < end; cid++)
+        if (ctx->touched[cid]) space_relink(ctx->s, &ctx->s->cells[cid]);
+}
+
+int space_shuffle(struct space *s) {
+    const int parts = nb_host_parts();
+    struct shuffle_ctx ctx;
+    ctx.s = s;
+    ctx.fail = 0;
+    ctx.lists = calloc(parts, sizeof(struct shuffle_mover *));
+    ctx.count = calloc(parts, sizeof(int));
+    ctx.size = calloc(parts, sizeof(int));
+    ctx.touched = calloc(s->nr_cells > 0 ? s->nr_cells : 1, 1);
+    if (ctx.lists == NULL || ctx.count == NULL || ctx.size == NULL || ctx.touched == NULL) {
+        free(ctx.lists); free(ctx.count); free(ctx.size); free(ctx.touched);
+        return space_error(space_err_malloc);
+    }
+    const int avg = s->nr_parts / (s->nr_cells > 0 ? s->nr_cells : 1) + 1;
+    const int grain = 8192 / avg < 16 ? 16 : 8192 / avg;
+    nb_parallel_for(s->nr_cells, grain, shuffle_scan, &ctx);
+    int moved = 0, rc = 0;
+    for (int q = 0; q < parts && !ctx.fail; q++)
+        for (int k = 0; k < ctx.count[q]; k++) {
+            const struct shuffle_mover *m = &ctx.lists[q][k];
+            if (cell_add(&s->cells[m->dst], &m->p) == NULL) {
+                ctx.fail = 1;
+                break;
+            }
+            ctx.touched[m->dst] = 1;
+            moved = 1;
+        }
+    if (ctx.fail)
+        rc = space_error(space_err_malloc);
+    else if (moved)
+        nb_parallel_for(s->nr_cells, grain, shuffle_relink, &ctx);
+    for (int q = 0; q < parts; q++) free(ctx.lists[q]);
+    free(ctx.lists); free(ctx.count); free(ctx.size); free(ctx.touched);
+    return rc < 0 ? rc : moved;
 }
 
 /* Sort-key scale and sweep bound, computed with the reference's float arithmetic

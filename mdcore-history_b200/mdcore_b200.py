@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
         "engine_rigid_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]),
         "engine_start": (C.c_int, [vp, C.c_int, C.c_int]),
         "engine_step": (C.c_int, [vp]),
+        "engine_advance": (C.c_int, [vp]),
         "engine_finalize": (C.c_int, [vp]),
         "engine_cuda_setdevice": (C.c_int, [vp, C.c_int]),
         "engine_cuda_load": (C.c_int, [vp]),

@@ -16,6 +16,10 @@
  *       cell-relative positions, velocities and forces by particle id and every group's
  *       P-SHAKE matrix.  Rigid file (little-endian): "MDB2RIG1", int32 ncon, shake, pad,
  *       double dt, double v[3N], ncon x {int32 i, j; double d}.
+ *   ref_driver mdbench <sysfile> <rigidfile> <nr_runners> <warmup> <steps>
+ *       Loads the system with velocities and rigid constraints, sets dt from the rigid file,
+ *       starts nr_runners runners and times full engine_step calls (sort + sweep +
+ *       exclusions + integration + P-SHAKE, src/engine.c:2070-2240); one JSON line.
  *   ref_driver bench <sysfile> <nr_runners> <warmup> <steps>
  *       Times engine_step (dt = 0: sort + pair/self sweep + exclusion subtraction +
  *       bookkeeping, src/engine.c:2070-2240) with clock_gettime and prints one JSON line.
@@ -163,6 +167,47 @@ static int do_rigid(const char *sysf, const char *rigf, const char *outf, int ne
     return 0;
 }
 
+static double now_s(void);
+
+static int do_mdbench(const char *sysf, const char *rigf, int runners, int warmup, int steps) {
+    struct sys_desc sd;
+    static struct engine e;
+    struct potential **pots;
+    char magic[8];
+    int hdr[3], k;
+    double dt, t0, t1;
+    FILE *f;
+    if (sys_read(sysf, &sd) != 0) { fprintf(stderr, "ref_driver: bad system file %s\n", sysf); return 1; }
+    f = fopen(rigf, "rb");
+    if (f == NULL || fread(magic, 1, 8, f) != 8 || memcmp(magic, "MDB2RIG1", 8) != 0 ||
+        fread(hdr, sizeof(int), 3, f) != 3 || fread(&dt, sizeof(double), 1, f) != 1) {
+        fprintf(stderr, "ref_driver: bad rigid file %s\n", rigf);
+        return 1;
+    }
+    double *v = malloc(sizeof(double) * 3 * sd.N);
+    if (fread(v, sizeof(double), 3 * (size_t)sd.N, f) != 3 * (size_t)sd.N) return 1;
+    omp_set_num_threads(runners);
+    if (build_v(&e, &sd, &pots, runners, v, hdr[1] ? engine_flag_shake : 0, 0) != 0) return 1;
+    for (k = 0; k < hdr[0]; k++) {
+        int ij[2];
+        double d;
+        if (fread(ij, sizeof(int), 2, f) != 2 || fread(&d, sizeof(double), 1, f) != 1) return 1;
+        if (engine_rigid_add(&e, ij[0], ij[1], d) < 0) { errs_dump(stderr); return 1; }
+    }
+    fclose(f);
+    if (engine_start(&e, runners, runners) < 0) { errs_dump(stderr); return 1; }
+    e.dt = dt;
+    for (k = 0; k < warmup; k++)
+        if (engine_step(&e) != 0) { errs_dump(stderr); return 1; }
+    t0 = now_s();
+    for (k = 0; k < steps; k++)
+        if (engine_step(&e) != 0) { errs_dump(stderr); return 1; }
+    t1 = now_s();
+    printf("{\"ms_per_step\": %.6f, \"steps\": %i, \"runners\": %i, \"epot\": %.17g}\n",
+           1e3 * (t1 - t0) / steps, steps, runners, e.s.epot);
+    return 0;
+}
+
 static int do_forces(const char *sysf, const char *outf, int runners) {
     struct sys_desc sd;
     static struct engine e;
@@ -246,6 +291,8 @@ static int do_bench(const char *sysf, int runners, int warmup, int steps) {
 int main(int argc, char *argv[]) {
     if (argc >= 5 && strcmp(argv[1], "forces") == 0)
         return do_forces(argv[2], argv[3], atoi(argv[4]));
+    if (argc >= 7 && strcmp(argv[1], "mdbench") == 0)
+        return do_mdbench(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), atoi(argv[6]));
     if (argc >= 6 && strcmp(argv[1], "rigid") == 0)
         return do_rigid(argv[2], argv[3], argv[4], atoi(argv[5]));
     if (argc >= 6 && strcmp(argv[1], "bench") == 0)
