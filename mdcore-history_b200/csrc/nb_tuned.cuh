@@ -566,9 +566,20 @@ __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& 
     }
 }
 
+// Exact warp sum of 64-bit fixed-point values: three 32-bit reductions (the low and middle
+// 16 bits, the signed high 32 bits) and a recombination; the same total in any lane order.
+// Per-lane values stay far below 2^62, so the high words sum without overflow.
+__device__ __forceinline__ long long warp_sum_fixed(long long v) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned lo = __reduce_add_sync(FULL, (unsigned)(v & 0xffff));
+    const unsigned mid = __reduce_add_sync(FULL, (unsigned)((v >> 16) & 0xffff));
+    const int hi = __reduce_add_sync(FULL, (int)(v >> 32));
+    return ((long long)hi << 32) + ((long long)mid << 16) + (long long)lo;
+}
+
 // End of a task: the j partial forces (and, for self tasks, the i forces) go to the
 // fixed-point accumulators, the j side of the virial is added, the warp sums energy and
-// virial in a fixed order and lane 0 adds them to the i cell (per-task clock64 record).
+// virial exactly in fixed point and lane 0 adds them to the i cell (per-task clock64 record).
 __device__ __forceinline__ void finish_task(const Params& P, const TunedParams& T, const WarpSlice& W,
                                             const TaskDesc& d, double e_task, double v_task, long long t_start,
                                             unsigned& status, int lane) {
@@ -585,15 +596,12 @@ __device__ __forceinline__ void finish_task(const Params& P, const TunedParams& 
         atomic_add_fixed(fp + 1, to_fixed(a.y, status));
         atomic_add_fixed(fp + 2, to_fixed(a.z, status));
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        e_task += __shfl_xor_sync(FULL, e_task, o);
-        v_task += __shfl_xor_sync(FULL, v_task, o);
-    }
+    // Energy and virial: each lane's FP64 partial to fixed point, summed exactly.
+    const long long e_fix = warp_sum_fixed(__double2ll_rn(e_task * kEnergyScale));
+    const long long v_fix = warp_sum_fixed(__double2ll_rn(-v_task * kEnergyScale));
     if (lane == 0) {
-        atomicAdd(&P.cell_epot[d.tr.ci], (unsigned long long)__double2ll_rn(e_task * kEnergyScale));
-        atomicAdd(P.cell_vir ? &P.cell_vir[d.tr.ci] : &P.acc[kAccVirial],
-                  (unsigned long long)__double2ll_rn(-v_task * kEnergyScale));
+        atomicAdd(&P.cell_epot[d.tr.ci], (unsigned long long)e_fix);
+        atomicAdd(P.cell_vir ? &P.cell_vir[d.tr.ci] : &P.acc[kAccVirial], (unsigned long long)v_fix);
         if (T.task_clock) {
             T.task_clock[2 * d.t] = t_start;
             T.task_clock[2 * d.t + 1] = clock64();
