@@ -452,7 +452,7 @@ int engine_cuda_graph(struct engine *e, int enable);
 /* Persistent sweep shape: lane layout 0 = one i particle per lane (32 per warp, the
  * default), 1 = a tile of 8 i particles x 4 j columns per warp; stages = 1 or 2 staging
  * buffers per worker warp (2: the next task's bulk copies land while the warp sweeps the
- * current one; only with occupancy 640); occupancy = resident threads per SM the kernel's
+ * current one; not with occupancy 768); occupancy = resident threads per SM the kernel's
  * registers are sized for: 640 (96 registers, the default), 768 (80) or 1024 (64).  Same
  * pair set. */
 int engine_cuda_setlayout(struct engine *e, int layout, int stages, int occupancy);

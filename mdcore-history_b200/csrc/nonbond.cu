@@ -362,11 +362,13 @@ int launch_tuned_win(NbState* st, const TunedParams& T, int cap, size_t smem, in
     }
 }
 
-// Instantiated shapes: at 640 threads per SM every window and staging choice; at 768 and
-// 1024 (fewer registers per thread) the 4-step window with one staging buffer.
+// Instantiated shapes: at 640 threads per SM every window and staging choice; at 768 the
+// 4-step window with one staging buffer; at 1024 (small cells) one or two buffers.
 template <int LAY>
 int launch_tuned_lay(NbState* st, const TunedParams& T, int cap, size_t smem, int nw) {
-    if (st->occupancy == 1024) return launch_tuned_win<4, LAY, 1, 1024>(st, T, cap, smem, nw);
+    if (st->occupancy == 1024)
+        return st->stages == 2 ? launch_tuned_win<4, LAY, 2, 1024>(st, T, cap, smem, nw)
+                               : launch_tuned_win<4, LAY, 1, 1024>(st, T, cap, smem, nw);
     if (st->occupancy == 768) return launch_tuned_win<4, LAY, 1, 768>(st, T, cap, smem, nw);
     if (st->stages == 2) return launch_tuned_win<4, LAY, 2, 640>(st, T, cap, smem, nw);
     if (st->window == 8) return launch_tuned_win<8, LAY, 1, 640>(st, T, cap, smem, nw);
@@ -988,7 +990,8 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
         {2, 0, 1, 640}, {4, 0, 1, 640}, {8, 0, 1, 640}, {2, 1, 1, 640}, {4, 1, 1, 640}, {8, 1, 1, 640},
         {2, 0, 2, 640}, {4, 0, 2, 640}, {8, 0, 2, 640}, {2, 1, 2, 640}, {4, 1, 2, 640}, {8, 1, 2, 640},
         {2, 0, 1, 768}, {4, 0, 1, 768}, {8, 0, 1, 768}, {2, 1, 1, 768}, {4, 1, 1, 768}, {8, 1, 1, 768},
-        {2, 0, 1, 1024}, {4, 0, 1, 1024}, {8, 0, 1, 1024}, {2, 1, 1, 1024}, {4, 1, 1, 1024}, {8, 1, 1, 1024}};
+        {2, 0, 1, 1024}, {4, 0, 1, 1024}, {8, 0, 1, 1024}, {2, 1, 1, 1024}, {4, 1, 1, 1024}, {8, 1, 1, 1024},
+        {2, 1, 2, 1024}, {4, 1, 2, 1024}, {8, 1, 2, 1024}};
     const int nshapes = sizeof(shapes) / sizeof(shapes[0]);
     int best = -1;
     float best_ms = 0.f;
@@ -1100,7 +1103,7 @@ extern "C" int engine_cuda_setwindow(struct engine* e, int window) {
 
 static int st_setlayout(NbState* st, int layout, int stages, int occupancy) {
     if ((layout != 0 && layout != 1) || (stages != 1 && stages != 2) ||
-        (occupancy != 640 && occupancy != 768 && occupancy != 1024) || (stages == 2 && occupancy != 640))
+        (occupancy != 640 && occupancy != 768 && occupancy != 1024) || (stages == 2 && occupancy == 768))
         return engine_err_range;
     st->layout = layout;
     st->stages = stages;

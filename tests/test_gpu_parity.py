@@ -205,7 +205,7 @@ def test_graph_replay_bit_identical(fname):
     e.close()
 
 
-@pytest.mark.parametrize("stages,occupancy", [(1, 640), (2, 640), (1, 768), (1, 1024)])
+@pytest.mark.parametrize("stages,occupancy", [(1, 640), (2, 640), (1, 768), (1, 1024), (2, 1024)])
 @pytest.mark.parametrize("layout", [0, 1], ids=["32i", "8x4"])
 @pytest.mark.parametrize("window", [4, 8])
 @pytest.mark.parametrize("warps", [2, 4, 8])
