@@ -370,6 +370,25 @@ def ours(args, rank, world, local_rank):
               "what": "engine_step of rigid SPC/E water (32,768 molecules, 98,304 constraints): rebin, "
                       "forces with host buffers, symplectic Euler, P-SHAKE on the device (FP64)",
               "shake_max_iterations": itmax}
+        # the same MD steps with the particles resident on the device: re-binning,
+        # forces, integration and P-SHAKE as one CUDA graph per step, no host copies
+        rig.resident_begin()
+        rig.resident_steps(max(args.warmup, 3))
+        barrier()
+        ev0.record(stream)
+        rig.resident_steps(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        res_ms = ev0.elapsed_time(ev1) / args.steps
+        rig.resident_sync()
+        itmax, bad = rig.rigid_stats()
+        if rig.stats().status != 0 or bad != 0:
+            raise SystemExit("bench.py: resident rigid water steps failed")
+        md["resident"] = {"ms_per_step": res_ms, "ns_per_day": ns_per_day(res_ms),
+                          "what": "engine_cuda_resident_steps: the same steps with the particles resident "
+                                  "in HBM, one CUDA graph per step",
+                          "shake_max_iterations": itmax}
+        rig.resident_end()
         rig.close()
 
     # ---- the plain form (one CTA per task, IEEE sqrt/div, no graph), same protocol

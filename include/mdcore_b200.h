@@ -463,6 +463,26 @@ int engine_cuda_setlayout(struct engine *e, int layout, int stages, int occupanc
 int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, int *stages, int *occupancy,
                          float *ms);
 
+/* ---- device-resident time steps (replace engine_step, src/engine.c:2070-2240, while
+ * the particles stay on the device) ----
+ * engine_cuda_resident_begin uploads every particle into fixed blocks of slots per cell
+ * (the largest cell plus `margin` spare slots, rounded up to 4; margin < 0: half the
+ * largest cell plus 8).  engine_cuda_resident_steps runs nsteps time steps of
+ * engine_step -- space_shuffle, the nonbonded forces, engine_advance, the rigid
+ * constraints -- as device launches only (with engine_cuda_graph, one CUDA graph per
+ * step); e->time advances, the host's particles do not.  A cell that outgrows its block
+ * (or more than 16 particles leaving one cell in a step) returns engine_err_maxparts.
+ * engine_cuda_resident_sync rebuilds the host cells (the device's particles in the
+ * device's order: positions, velocities, the last step's forces before the constraint
+ * corrections; zero before the first resident step), cell and engine energies, stats and
+ * the rigid iteration statistics; engine_cuda_resident_end syncs and frees the blocks.
+ * Host and device re-binning keep the same particle order, so the trajectories are
+ * engine_step's bit for bit, and engine_step may carry on after a sync. */
+int engine_cuda_resident_begin(struct engine *e, int margin);
+int engine_cuda_resident_steps(struct engine *e, int nsteps);
+int engine_cuda_resident_sync(struct engine *e);
+int engine_cuda_resident_end(struct engine *e);
+
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff
  * and flags; their own particles, boxes and cell sizes).  Each evaluation sorts every
@@ -494,6 +514,12 @@ int engine_batch_autotune(struct engine_batch *b, int reps, int *warps, int *lay
                           float *ms);
 int engine_batch_setlayout(struct engine_batch *b, int layout, int stages, int occupancy);
 int engine_batch_ntasks(struct engine_batch *b);
+/* Device-resident steps of every engine of the batch (engine_cuda_resident_*): one
+ * re-binning, sort, sweep, integration and constraint launch sequence for all engines. */
+int engine_batch_resident_begin(struct engine_batch *b, int margin);
+int engine_batch_resident_steps(struct engine_batch *b, int nsteps);
+int engine_batch_resident_sync(struct engine_batch *b);
+int engine_batch_resident_end(struct engine_batch *b);
 
 #ifdef __cplusplus
 }

@@ -30,6 +30,16 @@ void nb_zero_cells(struct space *s);
  * the largest number of ranges (parts are numbered from 0). */
 void nb_parallel_for(int n, int grain, void (*fn)(void *ctx, int part, int begin, int end), void *ctx);
 int nb_host_parts(void);
+/* Rigid constraints inside a device-resident step (rigid.cu): where the engine's
+ * particles live on the device. */
+struct rigid_resident_view {
+    const int *slot_of;     /* global particle id -> device slot */
+    int id0;                /* the engine's first global id */
+    void *xq, *v;           /* float4 device cells: position (w = type), velocity */
+    int capc, cell0;        /* slots per cell, the engine's first global cell */
+};
+int rigid_eval_resident(struct engine *e, const struct rigid_resident_view *view, void *stream);
+int rigid_resident_stats(struct engine *e, void *stream);
 /* Launch stream of the engine's device state (NULL before engine_cuda_load). */
 void *nb_engine_stream(struct engine *e);
 

@@ -1,0 +1,190 @@
+// Device-resident time steps (sm_100a): the particles stay in HBM between steps and the
+// whole step -- re-binning, sort, sweep, integration, rigid constraints -- runs as device
+// launches (one CUDA graph per step), the host state being brought up to date only on
+// request.
+//
+// Layout: every cell owns a fixed block of `capc` slots (cell c: slots c*capc ..
+// c*capc + count[c]), so slot offsets never change and every launch has a fixed size.
+// Re-binning (the device form of space_shuffle, src/space.c:235-291) keeps each cell's
+// remaining particles in their order and appends the arrivals from the 26 neighbours in a
+// fixed direction order, each neighbour's leavers in their order: the result does not depend
+// on thread scheduling.  A cell that would exceed its capacity, or more than kMoversPerCell
+// leavers of one cell in one step, sets a status bit (the particles concerned are dropped
+// from the device copy, never written out of bounds) and the host reports the error.
+#pragma once
+#include "nb_device.cuh"
+
+namespace nb {
+
+constexpr int kMoversPerCell = 16;
+constexpr unsigned kStatusResidentOverflow = 1u << 4;
+
+struct Mover {
+    float4 x;        // position relative to the destination cell, w = type bits
+    float4 v;        // velocity, w = direction index (bits)
+    int pid;
+    int pad[3];
+};
+
+struct ResidentCells {
+    int ncells, capc;
+    const int* nbr;          // 27 per cell: global index of the neighbour in direction d (13 = self)
+    const float4* cell_h;    // per cell: edge lengths (float, as the host keeps them)
+};
+
+// Direction index of a cell offset (dx, dy, dz) in {-1, 0, 1}^3.
+__device__ __forceinline__ int dir_index(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
+
+// Phase 1, one warp per cell: particles still inside [0, h) keep their order and are
+// written to the same cell of the output side; leavers go to the cell's mover list,
+// shifted into their destination cell's frame (src/space.c: x -= delta*h).
+__global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float4* __restrict__ xq,
+                                                   const float4* __restrict__ v, const int* __restrict__ pid,
+                                                   const int* __restrict__ count, float4* __restrict__ xq_out,
+                                                   float4* __restrict__ v_out, int* __restrict__ pid_out,
+                                                   int* __restrict__ nstay, int* __restrict__ nmove,
+                                                   Mover* __restrict__ movers, unsigned long long* status) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    const float4 h = RC.cell_h[c];
+    int stays = 0, moves = 0;
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        const int k = k0 + lane;
+        const bool active = k < n;
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f), vv = x;
+        int id = 0;
+        if (active) {
+            x = xq[base + k];
+            vv = v[base + k];
+            id = pid[base + k];
+        }
+        const int dx = (x.x >= h.x) - (x.x < 0.0f), dy = (x.y >= h.y) - (x.y < 0.0f), dz = (x.z >= h.z) - (x.z < 0.0f);
+        const bool stay = active && dx == 0 && dy == 0 && dz == 0;
+        const bool move = active && !stay;
+        const unsigned bs = __ballot_sync(FULL, stay), bm = __ballot_sync(FULL, move);
+        const unsigned below = (1u << lane) - 1u;
+        if (stay) {
+            const int o = stays + __popc(bs & below);
+            xq_out[base + o] = x;
+            v_out[base + o] = vv;
+            pid_out[base + o] = id;
+        }
+        if (move) {
+            const int m = moves + __popc(bm & below);
+            if (m < kMoversPerCell) {
+                Mover mv;
+                mv.x = make_float4(__fsub_rn(x.x, __fmul_rn((float)dx, h.x)), __fsub_rn(x.y, __fmul_rn((float)dy, h.y)),
+                                   __fsub_rn(x.z, __fmul_rn((float)dz, h.z)), x.w);
+                mv.v = make_float4(vv.x, vv.y, vv.z, __int_as_float(dir_index(dx, dy, dz)));
+                mv.pid = id;
+                mv.pad[0] = mv.pad[1] = mv.pad[2] = 0;
+                movers[(size_t)c * kMoversPerCell + m] = mv;
+            } else {
+                atomicOr(status, (unsigned long long)kStatusResidentOverflow);
+            }
+        }
+        stays += __popc(bs);
+        moves += __popc(bm);
+    }
+    if (lane == 0) {
+        nstay[c] = stays;
+        nmove[c] = min(moves, kMoversPerCell);
+    }
+}
+
+// Phase 2, one warp per destination cell: after its stayers, the arrivals from the
+// neighbours in direction order 0..26 (a particle that moved by d arrives from the
+// neighbour at -d), each neighbour's leavers in their order.
+__global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Mover* __restrict__ movers,
+                                                    const int* __restrict__ nstay, const int* __restrict__ nmove,
+                                                    float4* __restrict__ xq_out, float4* __restrict__ v_out,
+                                                    int* __restrict__ pid_out, int* __restrict__ count,
+                                                    unsigned long long* status) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const size_t base = (size_t)c * RC.capc;
+    int off = nstay[c];
+    bool over = false;
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        const int src = RC.nbr[(size_t)c * 27 + (26 - d)];
+        const int nm = nmove[src];
+        for (int m0 = 0; m0 < nm; m0 += 32) {
+            const int m = m0 + lane;
+            Mover mv;
+            bool match = false;
+            if (m < nm) {
+                mv = movers[(size_t)src * kMoversPerCell + m];
+                match = __float_as_int(mv.v.w) == d;
+            }
+            const unsigned bmatch = __ballot_sync(FULL, match);
+            if (match) {
+                const int o = off + __popc(bmatch & ((1u << lane) - 1u));
+                if (o < RC.capc) {
+                    xq_out[base + o] = mv.x;
+                    v_out[base + o] = make_float4(mv.v.x, mv.v.y, mv.v.z, 0.f);
+                    pid_out[base + o] = mv.pid;
+                } else {
+                    over = true;
+                }
+            }
+            off += __popc(bmatch);
+        }
+    }
+    if (__any_sync(FULL, over) && lane == 0) atomicOr(status, (unsigned long long)kStatusResidentOverflow);
+    if (lane == 0) count[c] = min(off, RC.capc);
+}
+
+// Slot of every particle id after re-binning (for the rigid constraints).
+__global__ void __launch_bounds__(256) slot_of_ids(ResidentCells RC, const int* __restrict__ pid,
+                                                   const int* __restrict__ count, int* __restrict__ slot_of) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    for (int k = lane; k < n; k += 32) slot_of[pid[base + k]] = (int)(base + k);
+}
+
+// Symplectic Euler update of every particle (engine_advance, src/engine.c:1975-1979), with
+// the float expressions the host integrator evaluates: w = (float)(dt * 1/m),
+// v += f*w, x += dt*v; forces from the fixed-point accumulators of the sweep.
+__global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const int* __restrict__ count,
+                                                       const unsigned long long* __restrict__ force,
+                                                       const int* __restrict__ cell_engine,
+                                                       const float* __restrict__ engine_dt,
+                                                       const double* __restrict__ engine_imass, int max_type,
+                                                       float4* __restrict__ xq, float4* __restrict__ v) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    const int k_eng = cell_engine[c];
+    const float dt = engine_dt[k_eng];
+    for (int k = lane; k < n; k += 32) {
+        const size_t s = base + k;
+        float4 x = xq[s], vv = v[s];
+        const int type = __float_as_int(x.w);
+        const float w = (float)((double)dt * engine_imass[(size_t)k_eng * max_type + type]);
+        const float fx = (float)((double)(long long)force[3 * s + 0] * (1.0 / (double)kForceScale));
+        const float fy = (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale));
+        const float fz = (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale));
+        vv.x = __fadd_rn(vv.x, __fmul_rn(fx, w));
+        vv.y = __fadd_rn(vv.y, __fmul_rn(fy, w));
+        vv.z = __fadd_rn(vv.z, __fmul_rn(fz, w));
+        x.x = __fadd_rn(x.x, __fmul_rn(dt, vv.x));
+        x.y = __fadd_rn(x.y, __fmul_rn(dt, vv.y));
+        x.z = __fadd_rn(x.z, __fmul_rn(dt, vv.z));
+        xq[s] = x;
+        v[s] = vv;
+    }
+}
+
+}  // namespace nb

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <atomic>
 #include <utility>
 #include <cmath>
 #include <ctime>
@@ -28,6 +29,7 @@
 #include "mdcore_b200.h"
 #include "internal.h"
 #include "nb_tuned.cuh"
+#include "nb_resident.cuh"
 #include "host_pool.h"
 
 using namespace nb;
@@ -111,6 +113,34 @@ struct NbState {
     unsigned long long* h_cell_epot = nullptr;   // 2 * ncells
     unsigned long long* h_acc = nullptr;
     bool resident_valid = false;
+    // Device-resident steps (nb_resident.cuh): fixed blocks of capc slots per cell, two
+    // sides (re-binning writes the other side), static per-id fields for the host copy.
+    bool res_active = false;
+    int capc = 0, rside = 0;
+    long long res_nparts = 0;
+    float4* r_xq[2] = {nullptr, nullptr};
+    float4* r_v[2] = {nullptr, nullptr};
+    int* r_pid[2] = {nullptr, nullptr};
+    int *r_count = nullptr, *r_cstart = nullptr, *r_nstay = nullptr, *r_nmove = nullptr, *r_slot_of = nullptr;
+    int *r_nbr = nullptr, *r_cell_engine = nullptr;
+    float4* r_cell_h = nullptr;
+    float* r_engine_dt = nullptr;
+    double* r_engine_imass = nullptr;
+    Mover* r_movers = nullptr;
+    unsigned* r_keys = nullptr;
+    unsigned long long* r_force = nullptr;
+    unsigned long long* r_status = nullptr;
+    float4* r_dense = nullptr;         // 3 per particle, cell order: position+type, velocity, force
+    float4* h_dense = nullptr;
+    int *r_dpid = nullptr, *h_dpid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
+    std::vector<long long> res_engine_n;   // particles of each engine on the device
+    std::vector<float> id_q;
+    std::vector<int> id_vid;
+    std::vector<unsigned short> id_flags;
+    std::vector<unsigned char> id_present;
+    cudaGraph_t rgraph[2] = {nullptr, nullptr};
+    cudaGraphExec_t rgraph_exec[2] = {nullptr, nullptr};
+    long long rgraph_key[2] = {-1, -1}, rprepared[2] = {-1, -1};
     void* sched = nullptr;             // learned-scheduler state (SchedState)
     std::vector<int> heur_order;       // count-product order built at load
 };
@@ -419,26 +449,52 @@ int record_event(NbState* st, cudaEvent_t ev) {
     return 0;
 }
 
+// Where the particles of an evaluation live on the device: the per-evaluation slots of the
+// host-buffer path, or the fixed per-cell blocks of resident steps.
+struct DevView {
+    const float4* xq;
+    const int* pid;
+    unsigned* keys;
+    unsigned long long* force;
+    const int* cstart;
+    const int* ccount;
+    size_t slots;            // slots of the force accumulators
+    int cap4;                // largest cell (or cell capacity), rounded up to 4
+    int cpc;                 // cells per sort block
+};
+
+DevView host_view(const NbState* st) {
+    DevView V;
+    V.xq = st->d_xq;
+    V.pid = st->d_pid;
+    V.keys = st->d_keys;
+    V.force = st->d_force;
+    V.cstart = st->d_cstart;
+    V.ccount = st->d_ccount;
+    V.slots = (size_t)st->h_cstart[st->ncells];
+    V.cap4 = (st->maxcount + 3) & ~3;
+    V.cpc = sort_cells_per_block(st->h_cstart[st->ncells], st->ncells);
+    return V;
+}
+
 // The launches of one evaluation: zero the accumulators, sort, (compact the queue,) sweep.
-int issue_kernels(NbState* st) {
-    CU(cudaMemsetAsync(st->d_force, 0, sizeof(unsigned long long) * 3 * (size_t)st->h_cstart[st->ncells],
-                       st->stream));
+int issue_kernels(NbState* st, const DevView& V) {
+    CU(cudaMemsetAsync(V.force, 0, sizeof(unsigned long long) * 3 * V.slots, st->stream));
     CU(cudaMemsetAsync(st->d_acc, 0, sizeof(unsigned long long) * kAccCount, st->stream));
     CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * 2 * st->ncells, st->stream));
-    const int cap = (st->maxcount + 3) & ~3;
+    const int cap = V.cap4;
     if (cap == 0) return 0;
-    const int cpc = sort_cells_per_block(st->h_cstart[st->ncells], st->ncells);
-    sort_cells<<<(st->ncells + cpc - 1) / cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
-        st->d_xq, st->d_cstart, st->d_ccount, st->d_cmask, st->d_keys, st->d_cscale, st->ncells, cpc, st->d_acc);
+    sort_cells<<<(st->ncells + V.cpc - 1) / V.cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
+        V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, st->d_acc);
     CU(cudaGetLastError());
 
     Params P;
-    P.xq = st->d_xq;
-    P.pid = st->d_pid;
-    P.keys = st->d_keys;
-    P.cstart = st->d_cstart;
-    P.ccount = st->d_ccount;
-    P.force = st->d_force;
+    P.xq = V.xq;
+    P.pid = V.pid;
+    P.keys = V.keys;
+    P.cstart = V.cstart;
+    P.ccount = V.ccount;
+    P.force = V.force;
     P.acc = st->d_acc;
     P.cell_epot = st->d_cell_epot;
     P.cell_vir = st->d_cell_epot + st->ncells;
@@ -465,6 +521,8 @@ int issue_kernels(NbState* st) {
     if (rc < 0) return rc;
     return record_event(st, st->evs1);
 }
+
+int issue_kernels(NbState* st) { return issue_kernels(st, host_view(st)); }
 
 void drop_graph(NbState* st) {
     if (st->graph_exec) cudaGraphExecDestroy(st->graph_exec);
@@ -571,10 +629,13 @@ int finish_stats(NbState* st) {
     return 0;
 }
 
+void res_free(NbState* st);
+
 void state_free(NbState* st) {
     if (st == nullptr) return;
     cudaSetDevice(st->device);
     drop_graph(st);
+    res_free(st);
     void* dev[] = {st->d_xq, st->d_pid, st->d_keys, st->d_force, st->d_cstart, st->d_ccount, st->d_cmask,
                    st->d_cscale, st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
@@ -1036,6 +1097,451 @@ int st_autotune(NbState* st, int reps, int* warps_out, int* layout_out, int* sta
     return 0;
 }
 
+
+// ---------------------------------------------------------------- device-resident steps
+
+void res_free(NbState* st) {
+    for (int q = 0; q < 2; q++) {
+        if (st->rgraph_exec[q]) cudaGraphExecDestroy(st->rgraph_exec[q]);
+        if (st->rgraph[q]) cudaGraphDestroy(st->rgraph[q]);
+        st->rgraph_exec[q] = nullptr;
+        st->rgraph[q] = nullptr;
+        st->rgraph_key[q] = st->rprepared[q] = -1;
+    }
+    void* dev[] = {st->r_xq[0], st->r_xq[1], st->r_v[0], st->r_v[1], st->r_pid[0], st->r_pid[1], st->r_count,
+                   st->r_cstart, st->r_nstay, st->r_nmove, st->r_slot_of, st->r_nbr, st->r_cell_engine,
+                   st->r_cell_h, st->r_engine_dt, st->r_engine_imass, st->r_movers, st->r_keys, st->r_force,
+                   st->r_status, st->r_dense, st->r_dpid, st->r_doff};
+    for (void* p : dev) cudaFree(p);
+    if (st->h_dense) cudaFreeHost(st->h_dense);
+    if (st->h_dpid) cudaFreeHost(st->h_dpid);
+    if (st->h_rcount) cudaFreeHost(st->h_rcount);
+    st->r_dpid = st->h_dpid = st->r_doff = st->h_rcount = nullptr;
+    st->r_xq[0] = st->r_xq[1] = nullptr;
+    st->r_v[0] = st->r_v[1] = nullptr;
+    st->r_pid[0] = st->r_pid[1] = nullptr;
+    st->r_count = st->r_cstart = st->r_nstay = st->r_nmove = st->r_slot_of = nullptr;
+    st->r_nbr = st->r_cell_engine = nullptr;
+    st->r_cell_h = nullptr;
+    st->r_engine_dt = nullptr;
+    st->r_engine_imass = nullptr;
+    st->r_movers = nullptr;
+    st->r_keys = nullptr;
+    st->r_force = nullptr;
+    st->r_status = nullptr;
+    st->r_dense = nullptr;
+    st->h_dense = nullptr;
+    st->res_active = false;
+}
+
+// Places the dense upload (cell order, per-cell offsets) into the cells' blocks.
+__global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float4* __restrict__ dxq,
+                                                   const float4* __restrict__ dv, const int* __restrict__ dpid,
+                                                   const int* __restrict__ doff, const int* __restrict__ count,
+                                                   float4* __restrict__ xq, float4* __restrict__ v,
+                                                   int* __restrict__ pid) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    for (int k = lane; k < n; k += 32) {
+        xq[base + k] = dxq[doff[c] + k];
+        v[base + k] = dv[doff[c] + k];
+        pid[base + k] = dpid[doff[c] + k];
+    }
+}
+
+// Every particle in cell order for the host copy (cell c from offset doff[c]): position
+// (w = type), velocity and the last evaluation's force, and its id.
+__global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const float4* __restrict__ xq,
+                                                     const float4* __restrict__ v, const int* __restrict__ pid,
+                                                     const int* __restrict__ count, const int* __restrict__ doff,
+                                                     const unsigned long long* __restrict__ force,
+                                                     float4* __restrict__ dense, int* __restrict__ dpid) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    for (int k = lane; k < n; k += 32) {
+        const size_t s = base + k, o = (size_t)doff[c] + k;
+        dense[3 * o] = xq[s];
+        dense[3 * o + 1] = v[s];
+        dense[3 * o + 2] =
+            make_float4((float)((double)(long long)force[3 * s] * (1.0 / (double)kForceScale)),
+                        (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale)),
+                        (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale)), 0.f);
+        dpid[o] = pid[s];
+    }
+}
+
+ResidentCells res_cells(const NbState* st) {
+    ResidentCells RC;
+    RC.ncells = st->ncells;
+    RC.capc = st->capc;
+    RC.nbr = st->r_nbr;
+    RC.cell_h = st->r_cell_h;
+    return RC;
+}
+
+int res_grid(const NbState* st) { return (st->ncells + 7) / 8; }      // 8 warps (cells) per block
+
+// Uploads the engines' particles into the device cells.  margin: spare slots per cell
+// (negative: half the largest cell plus 8).
+int st_resident_begin(NbState* st, int margin) {
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    res_free(st);
+    const int nc = st->ncells, ne = (int)st->engines.size(), mt = st->max_type, nid = st->nid;
+    int maxc = 0;
+    long long n = 0;
+    std::vector<int> count(nc), doff(nc + 1, 0);
+    for (int c = 0; c < nc; c++) {
+        count[c] = st->flat_cells[c]->count;
+        maxc = std::max(maxc, count[c]);
+        doff[c + 1] = doff[c] + count[c];
+    }
+    n = doff[nc];
+    if (maxc > kMaxPartsPerCell) {
+        errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    if (margin < 0) margin = maxc / 2 + 8;
+    st->capc = std::min(kMaxPartsPerCell, (maxc + std::max(margin, 4) + 3) & ~3);
+    const size_t slots = (size_t)nc * st->capc;
+    for (int q = 0; q < 2; q++) {
+        CU(cudaMalloc(&st->r_xq[q], sizeof(float4) * slots));
+        CU(cudaMalloc(&st->r_v[q], sizeof(float4) * slots));
+        CU(cudaMalloc(&st->r_pid[q], sizeof(int) * slots));
+    }
+    CU(cudaMalloc(&st->r_keys, sizeof(unsigned) * 13 * slots));
+    CU(cudaMalloc(&st->r_force, sizeof(unsigned long long) * 3 * slots));
+    CU(cudaMalloc(&st->r_count, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_cstart, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_nstay, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_nmove, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_movers, sizeof(Mover) * (size_t)nc * kMoversPerCell));
+    CU(cudaMalloc(&st->r_slot_of, sizeof(int) * (nid + 1)));
+    CU(cudaMalloc(&st->r_nbr, sizeof(int) * 27 * (size_t)nc));
+    CU(cudaMalloc(&st->r_cell_h, sizeof(float4) * (nc + 1)));
+    CU(cudaMalloc(&st->r_cell_engine, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_engine_dt, sizeof(float) * ne));
+    CU(cudaMalloc(&st->r_engine_imass, sizeof(double) * (size_t)ne * mt));
+    CU(cudaMalloc(&st->r_status, sizeof(unsigned long long)));
+    CU(cudaMalloc(&st->r_dense, sizeof(float4) * 3 * (size_t)(n + 1)));
+    CU(cudaMallocHost(&st->h_dense, sizeof(float4) * 3 * (size_t)(n + 1)));
+    CU(cudaMalloc(&st->r_dpid, sizeof(int) * (size_t)(n + 1)));
+    CU(cudaMallocHost(&st->h_dpid, sizeof(int) * (size_t)(n + 1)));
+    CU(cudaMalloc(&st->r_doff, sizeof(int) * (nc + 1)));
+    CU(cudaMallocHost(&st->h_rcount, sizeof(int) * (2 * nc + 2)));
+    CU(cudaMemset(st->r_status, 0, sizeof(unsigned long long)));
+    CU(cudaMemset(st->r_force, 0, sizeof(unsigned long long) * 3 * slots));
+    // Slots past a cell's count hold zeros or an earlier occupant (finite positions, ids in range).
+    for (int q = 0; q < 2; q++) {
+        CU(cudaMemset(st->r_xq[q], 0, sizeof(float4) * slots));
+        CU(cudaMemset(st->r_v[q], 0, sizeof(float4) * slots));
+        CU(cudaMemset(st->r_pid[q], 0, sizeof(int) * slots));
+    }
+
+    // Static cell data: block offsets, neighbours (periodic), edges, engine of each cell.
+    std::vector<int> cstart(nc + 1), nbr(27 * (size_t)nc), cell_engine(nc);
+    std::vector<float4> cell_h(nc);
+    std::vector<float> edt(ne);
+    std::vector<double> imass((size_t)ne * mt, 0.0);
+    for (int c = 0; c <= nc; c++) cstart[c] = (int)((size_t)c * st->capc);
+    for (int k = 0; k < ne; k++) {
+        struct engine* e = st->engines[k];
+        struct space* sp = &e->s;
+        edt[k] = (float)e->dt;
+        for (int t = 0; t < mt && t < e->max_type; t++) imass[(size_t)k * mt + t] = e->types[t].imass;
+        for (int c = 0; c < sp->nr_cells; c++) {
+            const int g = st->cell_off[k] + c;
+            const int* loc = sp->cells[c].loc;
+            cell_engine[g] = k;
+            cell_h[g] = make_float4((float)sp->h[0], (float)sp->h[1], (float)sp->h[2], 0.f);
+            for (int d = 0; d < 27; d++) {
+                const int dl[3] = {d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1};
+                int nl[3];
+                for (int j = 0; j < 3; j++) nl[j] = (loc[j] + dl[j] + sp->cdim[j]) % sp->cdim[j];
+                nbr[(size_t)g * 27 + d] = st->cell_off[k] + space_cellid(sp, nl[0], nl[1], nl[2]);
+            }
+        }
+    }
+    CU(cudaMemcpy(st->r_cstart, cstart.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_cell_engine, cell_engine.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_cell_h, cell_h.data(), sizeof(float4) * nc, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_engine_dt, edt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_engine_imass, imass.data(), sizeof(double) * imass.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_count, count.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+
+    // Particles in cell order (dense), then into the cells' blocks on the device.
+    std::vector<float4> dxq(n + 1), dv(n + 1);
+    std::vector<int> dpid(n + 1);
+    st->id_q.assign(nid, 0.f);
+    st->id_vid.assign(nid, 0);
+    st->id_flags.assign(nid, 0);
+    st->id_present.assign(nid, 0);
+    for (int c = 0; c < nc; c++) {
+        const struct cell* cl = st->flat_cells[c];
+        const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
+        for (int q = 0; q < cl->count; q++) {
+            const struct part* p = &cl->parts[q];
+            const int gid = st->id_off[k] + p->id;
+            dxq[doff[c] + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
+            dv[doff[c] + q] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
+            dpid[doff[c] + q] = gid;
+            st->id_q[gid] = p->q;
+            st->id_vid[gid] = p->vid;
+            st->id_flags[gid] = p->flags;
+            st->id_present[gid] = 1;
+        }
+    }
+    float4 *t_xq = nullptr, *t_v = nullptr;
+    int *t_pid = nullptr, *t_off = nullptr;
+    CU(cudaMalloc(&t_xq, sizeof(float4) * (n + 1)));
+    CU(cudaMalloc(&t_v, sizeof(float4) * (n + 1)));
+    CU(cudaMalloc(&t_pid, sizeof(int) * (n + 1)));
+    CU(cudaMalloc(&t_off, sizeof(int) * (nc + 1)));
+    CU(cudaMemcpy(t_xq, dxq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(t_v, dv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(t_pid, dpid.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(t_off, doff.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
+    const ResidentCells RC = res_cells(st);
+    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, t_xq, t_v, t_pid, t_off, st->r_count, st->r_xq[0],
+                                                      st->r_v[0], st->r_pid[0]);
+    CU(cudaGetLastError());
+    slot_of_ids<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_pid[0], st->r_count, st->r_slot_of);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st->stream));
+    cudaFree(t_xq);
+    cudaFree(t_v);
+    cudaFree(t_pid);
+    cudaFree(t_off);
+    st->res_nparts = n;
+    st->res_engine_n.assign(ne, 0);
+    for (int k = 0; k < ne; k++)
+        for (int c = 0; c < st->engines[k]->s.nr_cells; c++) st->res_engine_n[k] += count[st->cell_off[k] + c];
+    st->rside = 0;
+    st->res_active = true;
+    return 0;
+}
+
+// The launches of one resident step: re-binning into the other side, the force evaluation,
+// the integration, the rigid constraints.
+int res_issue_step(NbState* st) {
+    const int r = st->rside, o = 1 - r;
+    const ResidentCells RC = res_cells(st);
+    const int grid = res_grid(st);
+    rebin_split<<<grid, 256, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_count, st->r_xq[o],
+                                              st->r_v[o], st->r_pid[o], st->r_nstay, st->r_nmove, st->r_movers,
+                                              st->r_status);
+    rebin_gather<<<grid, 256, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
+                                               st->r_pid[o], st->r_count, st->r_status);
+    CU(cudaGetLastError());
+    bool rigid = false;
+    for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
+    if (rigid) {
+        slot_of_ids<<<grid, 256, 0, st->stream>>>(RC, st->r_pid[o], st->r_count, st->r_slot_of);
+        CU(cudaGetLastError());
+    }
+    DevView V;
+    V.xq = st->r_xq[o];
+    V.pid = st->r_pid[o];
+    V.keys = st->r_keys;
+    V.force = st->r_force;
+    V.cstart = st->r_cstart;
+    V.ccount = st->r_count;
+    V.slots = (size_t)st->ncells * st->capc;
+    V.cap4 = st->capc;
+    V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
+    int rc = issue_kernels(st, V);
+    if (rc < 0) return rc;
+    integrate_cells<<<grid, 256, 0, st->stream>>>(RC, st->r_count, st->r_force, st->r_cell_engine, st->r_engine_dt,
+                                                  st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o]);
+    CU(cudaGetLastError());
+    for (size_t k = 0; k < st->engines.size(); k++) {
+        struct engine* e = st->engines[k];
+        if (e->nr_rigids == 0) continue;
+        struct rigid_resident_view view;
+        view.slot_of = st->r_slot_of;
+        view.id0 = st->id_off[k];
+        view.xq = st->r_xq[o];
+        view.v = st->r_v[o];
+        view.capc = st->capc;
+        view.cell0 = st->cell_off[k];
+        rc = rigid_eval_resident(e, &view, st->stream);
+        if (rc < 0) return rc;
+    }
+    return 0;
+}
+
+// Everything a captured resident step depends on besides the device buffers' contents.
+long long res_key(const NbState* st) {
+    long long k = st->capc;
+    k = k * 131 + st->buf_gen;
+    k = k * 17 + st->warps;
+    k = k * 17 + st->window;
+    k = k * 3 + st->layout;
+    k = k * 3 + st->stages;
+    k = k * 3 + (st->occupancy == 640 ? 0 : st->occupancy == 768 ? 1 : 2);
+    k = k * 3 + st->plain;
+    k = k * 3 + st->record_clock;
+    return k;
+}
+
+// nsteps device-resident time steps.  Steps run as direct launches until every engine with
+// rigid groups is past the P-SHAKE refinement steps; then, with graphs enabled, the first
+// step from each side sets up, the second is captured, later ones replay.
+int st_resident_steps(NbState* st, int nsteps) {
+    if (!st->res_active) {
+        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
+    CU(cudaSetDevice(st->device));
+    CU(cudaEventRecord(st->ev0, st->stream));
+    for (int k = 0; k < nsteps; k++) {
+        bool refine = false;
+        for (struct engine* e : st->engines) {
+            e->time += 1;
+            refine = refine || (e->nr_rigids > 0 && e->time < engine_pshake_steps);
+        }
+        const int side = st->rside;
+        const long long key = res_key(st);
+        if (!st->use_graph || refine) {
+            const int rc = res_issue_step(st);
+            if (rc < 0) return rc;
+        } else if (st->rgraph_exec[side] != nullptr && st->rgraph_key[side] == key) {
+            CU(cudaGraphLaunch(st->rgraph_exec[side], st->stream));
+        } else if (st->rprepared[side] != key) {
+            const int rc = res_issue_step(st);
+            if (rc < 0) return rc;
+            st->rprepared[side] = key;
+        } else {
+            if (st->rgraph_exec[side]) cudaGraphExecDestroy(st->rgraph_exec[side]);
+            if (st->rgraph[side]) cudaGraphDestroy(st->rgraph[side]);
+            st->rgraph_exec[side] = nullptr;
+            st->rgraph[side] = nullptr;
+            CU(cudaStreamBeginCapture(st->stream, cudaStreamCaptureModeThreadLocal));
+            st->capturing = true;
+            const int rc = res_issue_step(st);
+            st->capturing = false;
+            cudaGraph_t g = nullptr;
+            const cudaError_t end = cudaStreamEndCapture(st->stream, &g);
+            if (rc < 0) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CU(end);
+            st->rgraph[side] = g;
+            CU(cudaGraphInstantiate(&st->rgraph_exec[side], g, 0));
+            st->rgraph_key[side] = key;
+            CU(cudaGraphLaunch(st->rgraph_exec[side], st->stream));
+        }
+        st->rside = 1 - side;
+    }
+    CU(cudaEventRecord(st->ev1, st->stream));
+    // Re-binning overflow is reported once per call.
+    unsigned long long status = 0;
+    CU(cudaMemcpyAsync(&status, st->r_status, sizeof(status), cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaStreamSynchronize(st->stream));
+    if (status) {
+        errs_register(engine_err_maxparts, "Device cell capacity exceeded during resident steps.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    return 0;
+}
+
+// Brings the engines' host cells up to date: positions, velocities and the last
+// evaluation's forces of every particle, in the cells the device holds them in (by id
+// within a cell), energies and statistics of the last step.
+int st_resident_sync(NbState* st) {
+    if (!st->res_active) {
+        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
+    CU(cudaSetDevice(st->device));
+    const int nc = st->ncells, ne = (int)st->engines.size();
+    const ResidentCells RC = res_cells(st);
+    int* cnt = st->h_rcount;                     // counts, then offsets
+    int* off = st->h_rcount + nc + 1;
+    CU(cudaMemcpyAsync(cnt, st->r_count, sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaStreamSynchronize(st->stream));
+    // Every particle must still be in one of its engine's cells; else the host keeps its copy.
+    off[0] = 0;
+    for (int c = 0; c < nc; c++) off[c + 1] = off[c] + std::min(cnt[c], st->capc);
+    for (int k = 0; k < ne; k++)
+        if (off[st->cell_off[k + 1]] - off[st->cell_off[k]] != st->res_engine_n[k]) {
+            errs_register(engine_err_maxparts, "Particles missing from the device cells.", __LINE__, __func__,
+                          __FILE__);
+            return engine_err = engine_err_maxparts;
+        }
+    const long long n = off[nc];
+    CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
+    compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[st->rside], st->r_v[st->rside],
+                                                        st->r_pid[st->rside], st->r_count, st->r_doff, st->r_force,
+                                                        st->r_dense, st->r_dpid);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
+                       st->stream));
+    CU(cudaMemcpyAsync(st->h_dpid, st->r_dpid, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
+                       cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
+                       st->stream));
+    CU(cudaStreamSynchronize(st->stream));
+    // The host cells take the device's particles in the device's order.
+    std::atomic<int> fail(0);
+    HostPool::get().run(nc, cell_grain(st), [&](int, int cb, int ce) {
+        for (int c = cb; c < ce; c++) {
+            const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
+            const int lo = st->id_off[k];
+            struct space* sp = &st->engines[k]->s;
+            struct cell* cl = st->flat_cells[c];
+            cl->count = 0;
+            for (int q = off[c]; q < off[c + 1]; q++) {
+                const float4 x = st->h_dense[3 * (size_t)q], v = st->h_dense[3 * (size_t)q + 1];
+                const float4 f = st->h_dense[3 * (size_t)q + 2];
+                const int gid = st->h_dpid[q];
+                int type;
+                std::memcpy(&type, &x.w, sizeof(int));
+                struct part p;
+                std::memset(&p, 0, sizeof(p));
+                p.x[0] = x.x; p.x[1] = x.y; p.x[2] = x.z;
+                p.v[0] = v.x; p.v[1] = v.y; p.v[2] = v.z;
+                p.f[0] = f.x; p.f[1] = f.y; p.f[2] = f.z;
+                p.q = st->id_q[gid];
+                p.id = gid - lo;
+                p.vid = st->id_vid[gid];
+                p.type = (short)type;
+                p.flags = st->id_flags[gid];
+                if (cell_add(cl, &p) == nullptr) {
+                    fail = 1;
+                    return;
+                }
+            }
+            space_relink(sp, cl);
+        }
+    });
+    if (fail) {
+        errs_register(engine_err_malloc, "Could not grow a host cell.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_malloc;
+    }
+    for (int k = 0; k < ne; k++) {
+        struct engine* e = st->engines[k];
+        struct space* sp = &e->s;
+        sp->epot = sp->epot_nonbond = sp->epot_bond = sp->epot_angle = sp->epot_dihedral = sp->epot_exclusion = 0.0;
+        if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream);
+    }
+    const int rc = finish_stats(st);
+    for (struct engine* e : st->engines) e->s.epot += e->s.epot_nonbond;
+    return rc;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- single engine
@@ -1171,6 +1677,29 @@ extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
 }
 
 // Runs further launches on a caller-provided stream (e.g. the framework's current stream).
+extern "C" int engine_cuda_resident_begin(struct engine* e, int margin) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident_begin(state(e), margin);
+}
+
+extern "C" int engine_cuda_resident_steps(struct engine* e, int nsteps) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident_steps(state(e), nsteps);
+}
+
+extern "C" int engine_cuda_resident_sync(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident_sync(state(e));
+}
+
+extern "C" int engine_cuda_resident_end(struct engine* e) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    int rc = st->res_active ? st_resident_sync(st) : 0;
+    res_free(st);
+    return rc;
+}
+
 extern "C" int engine_cuda_setstream(struct engine* e, void* stream) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     return st_setstream(state(e), stream);
@@ -1277,6 +1806,29 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
 }
 
 // engine_zero_forces for every engine of the batch (host threads over the cells).
+extern "C" int engine_batch_resident_begin(struct engine_batch* b, int margin) {
+    if (b == nullptr) return engine_err_null;
+    return st_resident_begin(bstate(b), margin);
+}
+
+extern "C" int engine_batch_resident_steps(struct engine_batch* b, int nsteps) {
+    if (b == nullptr) return engine_err_null;
+    return st_resident_steps(bstate(b), nsteps);
+}
+
+extern "C" int engine_batch_resident_sync(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    return st_resident_sync(bstate(b));
+}
+
+extern "C" int engine_batch_resident_end(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
+    NbState* st = bstate(b);
+    int rc = st->res_active ? st_resident_sync(st) : 0;
+    res_free(st);
+    return rc;
+}
+
 extern "C" int engine_batch_zero_forces(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
     NbState* st = bstate(b);

@@ -42,14 +42,61 @@ struct RigidArgs {
     double h0, h1, h2;          // cell edge
     double dt, tol;
     int a_update;               // P-SHAKE: refine the matrices this step
+    // Resident steps (RES kernels): particles read and written in place in the device
+    // cells instead of the packed slots above.
+    const int* rpid;            // per group slot: particle id
+    const int* slot_of;         // global particle id -> device slot
+    int id0;                    // this engine's first global id
+    float4* rxq;                // device cells: cell-relative position, w = type
+    float4* rv;                 // device cells: velocity
+    int capc, cell0;            // slots per cell, this engine's first global cell
+    int cd0, cd1, cd2;          // cell grid
 };
 
-// Shift code of a slot: (sx+1) + 3 (sy+1) + 9 (sz+1), or -1 for a group to skip.
-__device__ __forceinline__ void load_group(const RigidArgs& A, int p0, int np, double* xp, double* xo, double* m) {
+// Cell grid coordinates of a resident slot.
+__device__ __forceinline__ void slot_loc(const RigidArgs& A, int slot, int* loc) {
+    const int c = slot / A.capc - A.cell0;
+    loc[0] = c / (A.cd1 * A.cd2);
+    loc[1] = (c / A.cd2) % A.cd1;
+    loc[2] = c % A.cd2;
+}
+
+// Periodic cell offset -1/0/+1 of loc relative to loc0 per dimension (src/rigid.c:133-141).
+__device__ __forceinline__ int shift_dim(int a, int b) {
+    int s = a - b;
+    if (s > 1) s = -1;
+    else if (s < -1) s = 1;
+    return s;
+}
+
+// Position (relative to the group's first cell), position before the step and mass of every
+// particle of a group; packed slots carry the shift code (sx+1) + 3 (sy+1) + 9 (sz+1) in w
+// (-1: a group to skip), resident ones derive it from the cells.  Returns the shifts.
+template <bool RES>
+__device__ __forceinline__ void load_group(const RigidArgs& A, int p0, int np, double* xp, double* xo, double* m,
+                                           int* shifts) {
+    int loc0[3] = {0, 0, 0};
+    if (RES) slot_loc(A, A.slot_of[A.id0 + A.rpid[p0]], loc0);
     for (int k = 0; k < np; k++) {
-        const float4 x = A.x[p0 + k], v = A.v[p0 + k];
-        const int code = __float_as_int(x.w);
-        const double s[3] = {(double)(code % 3 - 1), (double)((code / 3) % 3 - 1), (double)(code / 9 - 1)};
+        float4 x, v;
+        int sh[3];
+        if (RES) {
+            const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
+            x = A.rxq[slot];
+            v = A.rv[slot];
+            int loc[3];
+            slot_loc(A, slot, loc);
+            for (int j = 0; j < 3; j++) sh[j] = shift_dim(loc[j], loc0[j]);
+        } else {
+            x = A.x[p0 + k];
+            v = A.v[p0 + k];
+            const int code = __float_as_int(x.w);
+            sh[0] = code % 3 - 1;
+            sh[1] = (code / 3) % 3 - 1;
+            sh[2] = code / 9 - 1;
+        }
+        for (int j = 0; j < 3; j++) shifts[3 * k + j] = sh[j];
+        const double s[3] = {(double)sh[0], (double)sh[1], (double)sh[2]};
         const double h[3] = {A.h0, A.h1, A.h2};
         const float xv[3] = {x.x, x.y, x.z}, vv[3] = {v.x, v.y, v.z};
         for (int j = 0; j < 3; j++) {
@@ -61,16 +108,44 @@ __device__ __forceinline__ void load_group(const RigidArgs& A, int p0, int np, d
     }
 }
 
+// The corrected positions: packed, to the FP64 output slots (the host applies them);
+// resident, applied in place with the host's expressions (src/rigid.c:236-262):
+// xn = xp - h*shift, v += (xn - x)/dt, x = xn.  The P-SHAKE constraint forces, which no
+// later step reads, are not kept on the device.
+template <bool RES>
+__device__ __forceinline__ void store_group(const RigidArgs& A, int p0, int np, const double* xp, const int* shifts) {
+    if (!RES) {
+        for (int k = 0; k < 3 * np; k++) A.xp[3 * (size_t)p0 + k] = xp[k];
+        return;
+    }
+    const double h[3] = {A.h0, A.h1, A.h2};
+    const double idt = 1.0 / A.dt;
+    for (int k = 0; k < np; k++) {
+        const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
+        float4 x = A.rxq[slot], v = A.rv[slot];
+        float* xs = &x.x;
+        float* vs = &v.x;
+        for (int j = 0; j < 3; j++) {
+            const double xn = xp[3 * k + j] - h[j] * shifts[3 * k + j];
+            vs[j] = (float)((double)vs[j] + idt * (xn - (double)xs[j]));
+            xs[j] = (float)xn;
+        }
+        A.rxq[slot] = x;
+        A.rv[slot] = v;
+    }
+}
+
 // SHAKE, src/rigid.c:148-213, with every quantity in FP64.
-template <int MP, int MC>
+template <int MP, int MC, bool RES>
 __global__ void __launch_bounds__(128) rigid_shake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
-    if (np > MP || nc > MC || __float_as_int(A.x[p0].w) < 0) return;
+    if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
     double xp[3 * MP], xo[3 * MP], m[MP], vc[3 * MC], wvc[3 * MC], res[MC];
-    load_group(A, p0, np, xp, xo, m);
+    int shifts[3 * MP];
+    load_group<RES>(A, p0, np, xp, xo, m, shifts);
     for (int k = 0; k < nc; k++) {
         const int2 c = A.cij[c0 + k];
         for (int j = 0; j < 3; j++) {
@@ -104,21 +179,22 @@ __global__ void __launch_bounds__(128) rigid_shake(RigidArgs A) {
     }
     atomicMax(&A.stat[0], iter);
     if (iter == rigid_maxiter) atomicAdd(&A.stat[1], 1);
-    for (int k = 0; k < 3 * np; k++) A.xp[3 * (size_t)p0 + k] = xp[k];
+    store_group<RES>(A, p0, np, xp, shifts);
 }
 
 // P-SHAKE, src/rigid.c:336-475: FP64 iterations over mixed constraint directions, the
 // float mixing matrix refined as the reference does.
-template <int MP, int MC>
+template <int MP, int MC, bool RES>
 __global__ void __launch_bounds__(128) rigid_pshake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
-    if (np > MP || nc > MC || __float_as_int(A.x[p0].w) < 0) return;
+    if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
     float* a = A.a + A.aoff[r];
     double xp[3 * MP], xo[3 * MP], m[MP], vc[3 * MC * MP];
-    load_group(A, p0, np, xp, xo, m);
+    int shifts[3 * MP];
+    load_group<RES>(A, p0, np, xp, xo, m, shifts);
     const int rowlen = 3 * np;
     for (int k = 0; k < nc * rowlen; k++) vc[k] = 0.0;
     for (int k = 0; k < nc; k++) {
@@ -188,14 +264,14 @@ __global__ void __launch_bounds__(128) rigid_pshake(RigidArgs A) {
                 for (int i = 0; i < nc; i++) tmp[j * nc + i] += a[k * nc + i] * a_new[j * nc + k];
         for (int i = 0; i < nc * nc; i++) a[i] = tmp[i];
     }
-    for (int k = 0; k < 3 * np; k++) A.xp[3 * (size_t)p0 + k] = xp[k];
+    store_group<RES>(A, p0, np, xp, shifts);
 }
 
 struct RigidDev {
     int device = 0;
     int gen = -1, nrig = 0, nslots = 0, ncon = 0, namat = 0, maxp = 0, maxc = 0;
     cudaStream_t own_stream = nullptr;
-    int *d_roff = nullptr, *d_coff = nullptr, *d_aoff = nullptr, *d_stat = nullptr;
+    int *d_roff = nullptr, *d_coff = nullptr, *d_aoff = nullptr, *d_stat = nullptr, *d_rpid = nullptr;
     int2* d_cij = nullptr;
     double *d_d2 = nullptr, *d_mass = nullptr, *d_xp = nullptr;
     float* d_a = nullptr;
@@ -221,11 +297,11 @@ int rigid_fail(cudaError_t err, int line, const char* func) {
 
 void free_buffers(RigidDev* rd) {
     void* dev[] = {rd->d_roff, rd->d_coff, rd->d_aoff, rd->d_stat, rd->d_cij, rd->d_d2,
-                   rd->d_mass, rd->d_xp, rd->d_a, rd->d_x, rd->d_v};
+                   rd->d_mass, rd->d_xp, rd->d_a, rd->d_x, rd->d_v, rd->d_rpid};
     for (void* p : dev) cudaFree(p);
     void* host[] = {rd->h_x, rd->h_v, rd->h_xp, rd->h_stat};
     for (void* p : host) cudaFreeHost(p);
-    rd->d_roff = rd->d_coff = rd->d_aoff = rd->d_stat = nullptr;
+    rd->d_roff = rd->d_coff = rd->d_aoff = rd->d_stat = rd->d_rpid = nullptr;
     rd->d_cij = nullptr;
     rd->d_d2 = rd->d_mass = rd->d_xp = nullptr;
     rd->d_a = nullptr;
@@ -245,7 +321,7 @@ int upload(T** d, const std::vector<T>& h) {
 // (Re)builds the static description of the groups after engine_rigid_add changed them.
 int build(struct engine* e, RigidDev* rd) {
     free_buffers(rd);
-    std::vector<int> roff(1, 0), coff(1, 0), aoff(1, 0);
+    std::vector<int> roff(1, 0), coff(1, 0), aoff(1, 0), rpid;
     std::vector<int2> cij;
     std::vector<double> d2, mass;
     std::vector<float> amat;
@@ -256,6 +332,7 @@ int build(struct engine* e, RigidDev* rd) {
             const int id = r->parts[k];
             const struct part* p = (id >= 0 && id < e->s.size_parts) ? e->s.partlist[id] : nullptr;
             mass.push_back(p ? e->types[p->type].mass : 1.0);
+            rpid.push_back(id);
         }
         for (int k = 0; k < r->nr_constr; k++) {
             cij.push_back(make_int2(r->constr[k].i, r->constr[k].j));
@@ -275,7 +352,8 @@ int build(struct engine* e, RigidDev* rd) {
     rd->roff = roff;
     rd->skip.assign(rd->nrig + 1, 0);
     if (upload(&rd->d_roff, roff) || upload(&rd->d_coff, coff) || upload(&rd->d_aoff, aoff) ||
-        upload(&rd->d_cij, cij) || upload(&rd->d_d2, d2) || upload(&rd->d_mass, mass) || upload(&rd->d_a, amat))
+        upload(&rd->d_cij, cij) || upload(&rd->d_d2, d2) || upload(&rd->d_mass, mass) || upload(&rd->d_a, amat) ||
+        upload(&rd->d_rpid, rpid))
         return engine_err_cuda;
     const size_t ns = (size_t)rd->nslots + 1;
     CU(cudaMalloc(&rd->d_x, sizeof(float4) * ns));
@@ -306,13 +384,23 @@ float bits_float(int v) {
     return f;
 }
 
-template <int MP, int MC>
+template <int MP, int MC, bool RES>
 void launch(bool pshake, const RigidArgs& A, cudaStream_t s) {
     const int grid = (A.nrig + 127) / 128;
     if (pshake)
-        rigid_pshake<MP, MC><<<grid, 128, 0, s>>>(A);
+        rigid_pshake<MP, MC, RES><<<grid, 128, 0, s>>>(A);
     else
-        rigid_shake<MP, MC><<<grid, 128, 0, s>>>(A);
+        rigid_shake<MP, MC, RES><<<grid, 128, 0, s>>>(A);
+}
+
+template <bool RES>
+void launch_sized(const RigidDev* rd, bool pshake, const RigidArgs& A, cudaStream_t s) {
+    if (rd->maxp <= 3 && rd->maxc <= 3)
+        launch<3, 3, RES>(pshake, A, s);
+    else if (rd->maxp <= 4 && rd->maxc <= 6)
+        launch<4, 6, RES>(pshake, A, s);
+    else
+        launch<rigid_maxparts, rigid_maxconstr, RES>(pshake, A, s);
 }
 
 }  // namespace
@@ -406,12 +494,7 @@ extern "C" int engine_rigid_eval(struct engine* e) {
     A.dt = e->dt;
     A.tol = e->tol_rigid;
     A.a_update = e->time < engine_pshake_steps;
-    if (rd->maxp <= 3 && rd->maxc <= 3)
-        launch<3, 3>(pshake, A, stream);
-    else if (rd->maxp <= 4 && rd->maxc <= 6)
-        launch<4, 6>(pshake, A, stream);
-    else
-        launch<rigid_maxparts, rigid_maxconstr>(pshake, A, stream);
+    launch_sized<false>(rd, pshake, A, stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(rd->h_xp, rd->d_xp, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, stream));
     CU(cudaMemcpyAsync(rd->h_stat, rd->d_stat, sizeof(int) * 2, cudaMemcpyDeviceToHost, stream));
@@ -465,5 +548,67 @@ extern "C" int engine_rigid_getmatrices(struct engine* e) {
         std::memcpy(r->a, amat.data() + off, sizeof(float) * n);
         off += n;
     }
+    return 0;
+}
+
+// Rigid constraints of a device-resident step: the groups' particles are read and
+// corrected in place in the device cells (see nb_resident.cuh) on `stream`; the iteration
+// statistics of the step stay on the device until rigid_resident_stats.  Capturable in a
+// CUDA graph: no host work, no allocation after the first call.
+extern "C" int rigid_eval_resident(struct engine* e, const struct rigid_resident_view* view, void* stream_v) {
+    if (e == nullptr || view == nullptr) return engine_err_null;
+    if (e->nr_rigids == 0) return 0;
+    RigidDev* rd = static_cast<RigidDev*>(e->cuda_rigid);
+    if (rd == nullptr) {
+        rd = new RigidDev();
+        rd->device = e->device;
+        e->cuda_rigid = rd;
+    }
+    CU(cudaSetDevice(rd->device));
+    if (rd->gen != e->rigids_gen || rd->nrig != e->nr_rigids) {
+        const int rc = build(e, rd);
+        if (rc < 0) return rc;
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    struct space* s = &e->s;
+    RigidArgs A = {};
+    A.nrig = rd->nrig;
+    A.roff = rd->d_roff;
+    A.coff = rd->d_coff;
+    A.aoff = rd->d_aoff;
+    A.cij = rd->d_cij;
+    A.d2 = rd->d_d2;
+    A.mass = rd->d_mass;
+    A.a = rd->d_a;
+    A.stat = rd->d_stat;
+    A.h0 = s->h[0];
+    A.h1 = s->h[1];
+    A.h2 = s->h[2];
+    A.dt = e->dt;
+    A.tol = e->tol_rigid;
+    A.a_update = e->time < engine_pshake_steps;
+    A.rpid = rd->d_rpid;
+    A.slot_of = view->slot_of;
+    A.id0 = view->id0;
+    A.rxq = static_cast<float4*>(view->xq);
+    A.rv = static_cast<float4*>(view->v);
+    A.capc = view->capc;
+    A.cell0 = view->cell0;
+    A.cd0 = s->cdim[0];
+    A.cd1 = s->cdim[1];
+    A.cd2 = s->cdim[2];
+    CU(cudaMemsetAsync(rd->d_stat, 0, sizeof(int) * 2, stream));
+    launch_sized<true>(rd, !(e->flags & engine_flag_shake), A, stream);
+    CU(cudaGetLastError());
+    return 0;
+}
+
+// Iteration statistics of the last resident step (device counters to the host copy).
+extern "C" int rigid_resident_stats(struct engine* e, void* stream_v) {
+    if (e == nullptr || e->cuda_rigid == nullptr) return 0;
+    RigidDev* rd = static_cast<RigidDev*>(e->cuda_rigid);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+    CU(cudaMemcpyAsync(rd->h_stat, rd->d_stat, sizeof(int) * 2, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
     return 0;
 }

@@ -240,20 +240,24 @@ void space_relink(struct space *s, struct cell *c) {
 }
 
 /* Particles that left their cell move into the neighbour cell (periodic wrap), as
- * src/space.c:307-364 does after each integration step: like the reference's incoming
- * buffers, arrivals are appended after every cell has been scanned.  A parallel scan in
- * which every host thread takes the leavers out of its own range of cells; the arrivals in
- * cell and particle order (independent of the number of threads); then the
+ * src/space.c:235-291 does after each integration step, in a fixed order that does not
+ * depend on threads: every cell keeps its remaining particles in their order, then
+ * appends the arrivals from its 26 neighbours by direction index (dx+1)*9 + (dy+1)*3 +
+ * (dz+1) of the move, each neighbour's leavers in their order.  (The reference's order
+ * depends on which runner thread takes its cell mutex first.)  The device-resident steps
+ * re-bin by the same rule, so host and device steps keep the same particle order.
+ * Two parallel passes: leavers out of every cell, then arrivals into every cell with the
  * partlist/celllist entries of the cells that changed. */
 struct shuffle_mover {
     struct part p;
-    int dst;
+    int dir;
 };
 
 struct shuffle_ctx {
     struct space *s;
-    struct shuffle_mover **lists;
+    struct shuffle_mover **lists;   /* per host thread */
     int *count, *size;
+    int *first, *nmove, *owner;     /* per cell: its leavers in lists[owner][first ..] */
     unsigned char *touched;
     int fail;
 };
@@ -265,9 +269,11 @@ static void shuffle_scan(void *vctx, int part, int begin, int end) {
     for (int k = 0; k < 3; k++) h[k] = s->h[k];
     for (int cid = begin; cid < end; cid++) {
         struct cell *c = &s->cells[cid];
-        int pid = 0;
-        while (pid < c->count) {
-            struct part *p = &c->parts[pid];
+        int keep = 0;
+        ctx->first[cid] = ctx->count[part];
+        ctx->owner[cid] = part;
+        for (int pid = 0; pid < c->count; pid++) {
+            const struct part *p = &c->parts[pid];
             int delta[3];
             for (int k = 0; k < 3; k++) delta[k] = (p->x[k] >= h[k]) - (p->x[k] < 0.0f);
             if (delta[0] || delta[1] || delta[2]) {
@@ -284,58 +290,73 @@ static void shuffle_scan(void *vctx, int part, int begin, int end) {
                 struct shuffle_mover *m = &ctx->lists[part][ctx->count[part]++];
                 m->p = *p;
                 for (int k = 0; k < 3; k++) m->p.x[k] -= delta[k] * h[k];
-                int nl[3];
-                for (int k = 0; k < 3; k++) nl[k] = (c->loc[k] + delta[k] + s->cdim[k]) % s->cdim[k];
-                m->dst = space_cellid(s, nl[0], nl[1], nl[2]);
-                c->count -= 1;
-                if (pid < c->count) c->parts[pid] = c->parts[c->count];
-                ctx->touched[cid] = 1;
-            } else
-                pid += 1;
+                m->dir = (delta[0] + 1) * 9 + (delta[1] + 1) * 3 + (delta[2] + 1);
+            } else {
+                if (keep < pid) c->parts[keep] = *p;
+                keep += 1;
+            }
         }
+        ctx->nmove[cid] = ctx->count[part] - ctx->first[cid];
+        if (keep < c->count) ctx->touched[cid] = 1;
+        c->count = keep;
     }
 }
 
-static void shuffle_relink(void *vctx, int part, int begin, int end) {
+static void shuffle_gather(void *vctx, int part, int begin, int end) {
     struct shuffle_ctx *ctx = vctx;
+    struct space *s = ctx->s;
     (void)part;
-    for (int cid = begin; cid < end; cid++)
-        if (ctx->touched[cid]) space_relink(ctx->s, &ctx->s->cells[cid]);
+    for (int cid = begin; cid < end && !ctx->fail; cid++) {
+        struct cell *c = &s->cells[cid];
+        for (int d = 0; d < 27; d++) {
+            if (d == 13) continue;
+            /* a particle that moved by delta(d) comes from the neighbour at -delta(d) */
+            const int delta[3] = {d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1};
+            int nl[3];
+            for (int k = 0; k < 3; k++) nl[k] = (c->loc[k] - delta[k] + s->cdim[k]) % s->cdim[k];
+            const int src = space_cellid(s, nl[0], nl[1], nl[2]);
+            const struct shuffle_mover *m = ctx->lists[ctx->owner[src]] + ctx->first[src];
+            for (int k = 0; k < ctx->nmove[src]; k++) {
+                if (m[k].dir != d) continue;
+                if (cell_add(c, &m[k].p) == NULL) {
+                    ctx->fail = 1;
+                    return;
+                }
+                ctx->touched[cid] = 1;
+            }
+        }
+        if (ctx->touched[cid]) space_relink(s, c);
+    }
 }
 
 int space_shuffle(struct space *s) {
     const int parts = nb_host_parts();
+    const int nc = s->nr_cells > 0 ? s->nr_cells : 1;
     struct shuffle_ctx ctx;
     ctx.s = s;
     ctx.fail = 0;
     ctx.lists = calloc(parts, sizeof(struct shuffle_mover *));
     ctx.count = calloc(parts, sizeof(int));
     ctx.size = calloc(parts, sizeof(int));
-    ctx.touched = calloc(s->nr_cells > 0 ? s->nr_cells : 1, 1);
-    if (ctx.lists == NULL || ctx.count == NULL || ctx.size == NULL || ctx.touched == NULL) {
-        free(ctx.lists); free(ctx.count); free(ctx.size); free(ctx.touched);
-        return space_error(space_err_malloc);
-    }
-    const int avg = s->nr_parts / (s->nr_cells > 0 ? s->nr_cells : 1) + 1;
-    const int grain = 8192 / avg < 16 ? 16 : 8192 / avg;
-    nb_parallel_for(s->nr_cells, grain, shuffle_scan, &ctx);
-    int moved = 0, rc = 0;
-    for (int q = 0; q < parts && !ctx.fail; q++)
-        for (int k = 0; k < ctx.count[q]; k++) {
-            const struct shuffle_mover *m = &ctx.lists[q][k];
-            if (cell_add(&s->cells[m->dst], &m->p) == NULL) {
-                ctx.fail = 1;
-                break;
-            }
-            ctx.touched[m->dst] = 1;
-            moved = 1;
-        }
-    if (ctx.fail)
+    ctx.first = calloc(nc, sizeof(int));
+    ctx.nmove = calloc(nc, sizeof(int));
+    ctx.owner = calloc(nc, sizeof(int));
+    ctx.touched = calloc(nc, 1);
+    int rc = 0, moved = 0;
+    if (ctx.lists == NULL || ctx.count == NULL || ctx.size == NULL || ctx.first == NULL || ctx.nmove == NULL ||
+        ctx.owner == NULL || ctx.touched == NULL) {
         rc = space_error(space_err_malloc);
-    else if (moved)
-        nb_parallel_for(s->nr_cells, grain, shuffle_relink, &ctx);
-    for (int q = 0; q < parts; q++) free(ctx.lists[q]);
-    free(ctx.lists); free(ctx.count); free(ctx.size); free(ctx.touched);
+    } else {
+        const int avg = s->nr_parts / nc + 1;
+        const int grain = 8192 / avg < 16 ? 16 : 8192 / avg;
+        nb_parallel_for(s->nr_cells, grain, shuffle_scan, &ctx);
+        for (int q = 0; q < parts; q++) moved = moved || ctx.count[q] > 0;
+        if (!ctx.fail && moved) nb_parallel_for(s->nr_cells, grain, shuffle_gather, &ctx);
+        if (ctx.fail) rc = space_error(space_err_malloc);
+        for (int q = 0; q < parts; q++) free(ctx.lists[q]);
+    }
+    free(ctx.lists); free(ctx.count); free(ctx.size); free(ctx.first); free(ctx.nmove); free(ctx.owner);
+    free(ctx.touched);
     return rc < 0 ? rc : moved;
 }
 

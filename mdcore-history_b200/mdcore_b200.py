@@ -138,6 +138,14 @@ def lib() -> C.CDLL:
         "engine_batch_graph": (C.c_int, [vp, C.c_int]),
         "engine_batch_autotune": (C.c_int, [vp, C.c_int, ip, ip, ip, ip, P(C.c_float)]),
         "engine_batch_ntasks": (C.c_int, [vp]),
+        "engine_cuda_resident_begin": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_resident_steps": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_resident_sync": (C.c_int, [vp]),
+        "engine_cuda_resident_end": (C.c_int, [vp]),
+        "engine_batch_resident_begin": (C.c_int, [vp, C.c_int]),
+        "engine_batch_resident_steps": (C.c_int, [vp, C.c_int]),
+        "engine_batch_resident_sync": (C.c_int, [vp]),
+        "engine_batch_resident_end": (C.c_int, [vp]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -267,6 +275,26 @@ class Engine:
 
     def step(self):
         _check(self.lib.engine_step(self.ptr), "engine_step")
+        return self
+
+    # -- device-resident time steps --------------------------------------------------
+    def resident_begin(self, margin: int = -1):
+        """Uploads the particles into per-cell device blocks (engine_cuda_resident_begin)."""
+        _check(self.lib.engine_cuda_resident_begin(self.ptr, margin), "engine_cuda_resident_begin")
+        return self
+
+    def resident_steps(self, nsteps: int = 1):
+        """nsteps engine_step equivalents entirely on the device."""
+        _check(self.lib.engine_cuda_resident_steps(self.ptr, nsteps), "engine_cuda_resident_steps")
+        return self
+
+    def resident_sync(self):
+        """Host cells, energies and stats as of the last resident step."""
+        _check(self.lib.engine_cuda_resident_sync(self.ptr), "engine_cuda_resident_sync")
+        return self
+
+    def resident_end(self):
+        _check(self.lib.engine_cuda_resident_end(self.ptr), "engine_cuda_resident_end")
         return self
 
     def load_parts(self):
@@ -471,6 +499,22 @@ class Batch:
 
     def step(self):
         _check(self.lib.engine_batch_step(self.ptr), "engine_batch_step")
+        return self
+
+    def resident_begin(self, margin: int = -1):
+        _check(self.lib.engine_batch_resident_begin(self.ptr, margin), "engine_batch_resident_begin")
+        return self
+
+    def resident_steps(self, nsteps: int = 1):
+        _check(self.lib.engine_batch_resident_steps(self.ptr, nsteps), "engine_batch_resident_steps")
+        return self
+
+    def resident_sync(self):
+        _check(self.lib.engine_batch_resident_sync(self.ptr), "engine_batch_resident_sync")
+        return self
+
+    def resident_end(self):
+        _check(self.lib.engine_batch_resident_end(self.ptr), "engine_batch_resident_end")
         return self
 
     def load_parts(self):
