@@ -466,12 +466,16 @@ int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, in
 /* ---- device-resident time steps (replace engine_step, src/engine.c:2070-2240, while
  * the particles stay on the device) ----
  * engine_cuda_resident_begin uploads every particle into fixed blocks of slots per cell
- * (the largest cell plus `margin` spare slots, rounded up to 4; margin < 0: half the
- * largest cell plus 8).  engine_cuda_resident_steps runs nsteps time steps of
+ * (the largest cell plus `margin` spare slots, rounded up to 4; margin < 0: an eighth of
+ * the largest cell plus 8).  engine_cuda_resident_steps runs nsteps time steps of
  * engine_step -- space_shuffle, the nonbonded forces, engine_advance, the rigid
  * constraints -- as device launches only (with engine_cuda_graph, one CUDA graph per
- * step); e->time advances, the host's particles do not.  A cell that outgrows its block
- * (or more than 16 particles leaving one cell in a step) returns engine_err_maxparts.
+ * step); e->time advances, the host's particles do not.  A step in which a cell outgrows
+ * its block (or more than 16 particles, doubled on each such event, leave one cell) is
+ * aborted on the device together with the steps after it; the call then re-blocks the
+ * particles of the last completed step with twice the spare room and runs the remaining
+ * steps, at most 8 times per call, and returns engine_err_maxparts only when a cell
+ * would exceed 1,024 particles (the device then still holds the last completed step).
  * engine_cuda_resident_sync rebuilds the host cells (the device's particles in the
  * device's order: positions, velocities, the last step's forces before the constraint
  * corrections; zero before the first resident step), cell and engine energies, stats and
@@ -482,6 +486,9 @@ int engine_cuda_resident_begin(struct engine *e, int margin);
 int engine_cuda_resident_steps(struct engine *e, int nsteps);
 int engine_cuda_resident_sync(struct engine *e);
 int engine_cuda_resident_end(struct engine *e);
+/* Slots per cell, leavers per cell and step, completed resident steps and automatic
+ * re-blockings since engine_cuda_resident_begin; any pointer may be NULL. */
+int engine_cuda_resident_info(struct engine *e, int *capc, int *mcap, long long *steps, int *regrows);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff
@@ -520,6 +527,7 @@ int engine_batch_resident_begin(struct engine_batch *b, int margin);
 int engine_batch_resident_steps(struct engine_batch *b, int nsteps);
 int engine_batch_resident_sync(struct engine_batch *b);
 int engine_batch_resident_end(struct engine_batch *b);
+int engine_batch_resident_info(struct engine_batch *b, int *capc, int *mcap, long long *steps, int *regrows);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,7 @@ struct rigid_resident_view {
     int id0;                /* the engine's first global id */
     void *xq, *v;           /* float4 device cells: position (w = type), velocity */
     int capc, cell0;        /* slots per cell, the engine's first global cell */
+    const unsigned long long *abort;   /* nonzero: the step was aborted, launch nothing */
 };
 int rigid_eval_resident(struct engine *e, const struct rigid_resident_view *view, void *stream);
 int rigid_resident_stats(struct engine *e, void *stream);

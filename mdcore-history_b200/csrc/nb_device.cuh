@@ -70,7 +70,13 @@ struct Params {
     float cutoff2;              // pair tasks: float(cutoff)^2 in float (src/runner_dopair.c:578-579)
     float cutoff2s;             // self tasks: float(cutoff^2) (src/runner_dopair.c:896)
     int unsorted;               // 1: sweep every candidate (engine_flag_unsorted)
+    const unsigned long long* abort;   // device-resident steps: nonzero = skip this launch
 };
+
+// A device-resident step that was aborted (see nb_resident.cuh) launches nothing more.
+__device__ __forceinline__ bool step_aborted(const unsigned long long* abort) {
+    return abort != nullptr && *(const volatile unsigned long long*)abort != 0;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

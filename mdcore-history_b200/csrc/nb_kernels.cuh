@@ -131,8 +131,10 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
                                                               const unsigned* __restrict__ cmask,
                                                               unsigned* __restrict__ keys,
                                                               const float2* __restrict__ cscale, int ncells, int cpc,
-                                                              unsigned long long* acc) {
+                                                              unsigned long long* acc,
+                                                              const unsigned long long* abort) {
     extern __shared__ __align__(16) unsigned char sort_smem[];
+    if (step_aborted(abort)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c0 = blockIdx.x * cpc, c1 = min(c0 + cpc, ncells);
     // cells of at most 32 particles: one warp each
@@ -246,6 +248,7 @@ template <int NW>
 __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
+    if (step_aborted(P.abort)) return;
     const int t = blockIdx.x;
     const TaskRec tr = P.tasks[t];
     const bool self = tr.sid < 0;

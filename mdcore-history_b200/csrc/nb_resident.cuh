@@ -8,16 +8,21 @@
 // Re-binning (the device form of space_shuffle, src/space.c:235-291) keeps each cell's
 // remaining particles in their order and appends the arrivals from the 26 neighbours in a
 // fixed direction order, each neighbour's leavers in their order: the result does not depend
-// on thread scheduling.  A cell that would exceed its capacity, or more than kMoversPerCell
-// leavers of one cell in one step, sets a status bit (the particles concerned are dropped
-// from the device copy, never written out of bounds) and the host reports the error.
+// on thread scheduling.
+//
+// Overflow: a cell that would exceed its capacity, or more than `mcap` leavers of one cell
+// in one step, sets a sticky abort word.  Every later kernel of that step and of the steps
+// after it returns at once, so the side the step read from keeps the last completed step
+// intact; integrate_cells counts the completed steps, from which the host finds that side,
+// re-blocks the particles with more room and runs the remaining steps again.  Nothing is
+// written out of bounds.
 #pragma once
 #include "nb_device.cuh"
 
 namespace nb {
 
-constexpr int kMoversPerCell = 16;
-constexpr unsigned kStatusResidentOverflow = 1u << 4;
+constexpr unsigned kStatusResidentOverflow = 1u << 4;   // a cell outgrew its block
+constexpr unsigned kStatusMoverOverflow = 1u << 5;      // too many leavers of one cell
 
 struct Mover {
     float4 x;        // position relative to the destination cell, w = type bits
@@ -27,7 +32,7 @@ struct Mover {
 };
 
 struct ResidentCells {
-    int ncells, capc;
+    int ncells, capc, mcap;  // cells, slots per cell, leavers per cell and step
     const int* nbr;          // 27 per cell: global index of the neighbour in direction d (13 = self)
     const float4* cell_h;    // per cell: edge lengths (float, as the host keeps them)
 };
@@ -47,7 +52,7 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (c >= RC.ncells) return;
+    if (c >= RC.ncells || *(volatile unsigned long long*)status != 0) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;
     const float4 h = RC.cell_h[c];
@@ -75,16 +80,16 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
         }
         if (move) {
             const int m = moves + __popc(bm & below);
-            if (m < kMoversPerCell) {
+            if (m < RC.mcap) {
                 Mover mv;
                 mv.x = make_float4(__fsub_rn(x.x, __fmul_rn((float)dx, h.x)), __fsub_rn(x.y, __fmul_rn((float)dy, h.y)),
                                    __fsub_rn(x.z, __fmul_rn((float)dz, h.z)), x.w);
                 mv.v = make_float4(vv.x, vv.y, vv.z, __int_as_float(dir_index(dx, dy, dz)));
                 mv.pid = id;
                 mv.pad[0] = mv.pad[1] = mv.pad[2] = 0;
-                movers[(size_t)c * kMoversPerCell + m] = mv;
+                movers[(size_t)c * RC.mcap + m] = mv;
             } else {
-                atomicOr(status, (unsigned long long)kStatusResidentOverflow);
+                atomicOr(status, (unsigned long long)kStatusMoverOverflow);
             }
         }
         stays += __popc(bs);
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
     }
     if (lane == 0) {
         nstay[c] = stays;
-        nmove[c] = min(moves, kMoversPerCell);
+        nmove[c] = min(moves, RC.mcap);
     }
 }
 
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (c >= RC.ncells) return;
+    if (c >= RC.ncells || *(volatile unsigned long long*)status != 0) return;
     const size_t base = (size_t)c * RC.capc;
     int off = nstay[c];
     bool over = false;
@@ -120,7 +125,7 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
             Mover mv;
             bool match = false;
             if (m < nm) {
-                mv = movers[(size_t)src * kMoversPerCell + m];
+                mv = movers[(size_t)src * RC.mcap + m];
                 match = __float_as_int(mv.v.w) == d;
             }
             const unsigned bmatch = __ballot_sync(FULL, match);
@@ -143,10 +148,11 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
 
 // Slot of every particle id after re-binning (for the rigid constraints).
 __global__ void __launch_bounds__(256) slot_of_ids(ResidentCells RC, const int* __restrict__ pid,
-                                                   const int* __restrict__ count, int* __restrict__ slot_of) {
+                                                   const int* __restrict__ count, int* __restrict__ slot_of,
+                                                   const unsigned long long* __restrict__ status) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (c >= RC.ncells) return;
+    if (c >= RC.ncells || (status != nullptr && *status != 0)) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) slot_of[pid[base + k]] = (int)(base + k);
@@ -160,9 +166,13 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
                                                        const int* __restrict__ cell_engine,
                                                        const float* __restrict__ engine_dt,
                                                        const double* __restrict__ engine_imass, int max_type,
-                                                       float4* __restrict__ xq, float4* __restrict__ v) {
+                                                       float4* __restrict__ xq, float4* __restrict__ v,
+                                                       const unsigned long long* __restrict__ status,
+                                                       unsigned long long* __restrict__ steps_done) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (*status != 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(steps_done, 1ull);
     if (c >= RC.ncells) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;

@@ -687,6 +687,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const Params& P = T.p;
+    if (step_aborted(P.abort)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = P.max_type;
     const SharedTables S = stage_tables<NW, STAGES>(P, smem_raw, cap);
@@ -799,6 +800,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr unsigned FULL = 0xffffffffu;
     const Params& P = T.p;
+    if (step_aborted(P.abort)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = lane >> 2, col = lane & 3;
     const int mt = P.max_type;

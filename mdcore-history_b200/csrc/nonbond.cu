@@ -116,12 +116,15 @@ struct NbState {
     // Device-resident steps (nb_resident.cuh): fixed blocks of capc slots per cell, two
     // sides (re-binning writes the other side), static per-id fields for the host copy.
     bool res_active = false;
-    int capc = 0, rside = 0;
-    long long res_nparts = 0;
+    int capc = 0, rside = 0, mcap = 16, res_margin = 8;
+    long long res_nparts = 0, res_done = 0, res_done_total = 0;
+    int res_regrows = 0;
+    int* r_cnt[2] = {nullptr, nullptr};      // particles per cell of each side
+    unsigned long long* r_done = nullptr;    // completed resident steps (device counter)
     float4* r_xq[2] = {nullptr, nullptr};
     float4* r_v[2] = {nullptr, nullptr};
     int* r_pid[2] = {nullptr, nullptr};
-    int *r_count = nullptr, *r_cstart = nullptr, *r_nstay = nullptr, *r_nmove = nullptr, *r_slot_of = nullptr;
+    int *r_cstart = nullptr, *r_nstay = nullptr, *r_nmove = nullptr, *r_slot_of = nullptr;
     int *r_nbr = nullptr, *r_cell_engine = nullptr;
     float4* r_cell_h = nullptr;
     float* r_engine_dt = nullptr;
@@ -461,6 +464,7 @@ struct DevView {
     size_t slots;            // slots of the force accumulators
     int cap4;                // largest cell (or cell capacity), rounded up to 4
     int cpc;                 // cells per sort block
+    const unsigned long long* abort = nullptr;   // resident steps: the step's abort word
 };
 
 DevView host_view(const NbState* st) {
@@ -485,7 +489,7 @@ int issue_kernels(NbState* st, const DevView& V) {
     const int cap = V.cap4;
     if (cap == 0) return 0;
     sort_cells<<<(st->ncells + V.cpc - 1) / V.cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
-        V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, st->d_acc);
+        V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, st->d_acc, V.abort);
     CU(cudaGetLastError());
 
     Params P;
@@ -514,6 +518,7 @@ int issue_kernels(NbState* st, const DevView& V) {
     P.cutoff2 = st->cut2p;
     P.cutoff2s = st->cut2s;
     P.unsorted = st->unsorted;
+    P.abort = V.abort;
 
     int rc = record_event(st, st->evs0);
     if (rc < 0) return rc;
@@ -1108,8 +1113,8 @@ void res_free(NbState* st) {
         st->rgraph[q] = nullptr;
         st->rgraph_key[q] = st->rprepared[q] = -1;
     }
-    void* dev[] = {st->r_xq[0], st->r_xq[1], st->r_v[0], st->r_v[1], st->r_pid[0], st->r_pid[1], st->r_count,
-                   st->r_cstart, st->r_nstay, st->r_nmove, st->r_slot_of, st->r_nbr, st->r_cell_engine,
+    void* dev[] = {st->r_xq[0], st->r_xq[1], st->r_v[0], st->r_v[1], st->r_pid[0], st->r_pid[1], st->r_cnt[0],
+                   st->r_cnt[1], st->r_done, st->r_cstart, st->r_nstay, st->r_nmove, st->r_slot_of, st->r_nbr, st->r_cell_engine,
                    st->r_cell_h, st->r_engine_dt, st->r_engine_imass, st->r_movers, st->r_keys, st->r_force,
                    st->r_status, st->r_dense, st->r_dpid, st->r_doff};
     for (void* p : dev) cudaFree(p);
@@ -1120,7 +1125,9 @@ void res_free(NbState* st) {
     st->r_xq[0] = st->r_xq[1] = nullptr;
     st->r_v[0] = st->r_v[1] = nullptr;
     st->r_pid[0] = st->r_pid[1] = nullptr;
-    st->r_count = st->r_cstart = st->r_nstay = st->r_nmove = st->r_slot_of = nullptr;
+    st->r_cnt[0] = st->r_cnt[1] = nullptr;
+    st->r_done = nullptr;
+    st->r_cstart = st->r_nstay = st->r_nmove = st->r_slot_of = nullptr;
     st->r_nbr = st->r_cell_engine = nullptr;
     st->r_cell_h = nullptr;
     st->r_engine_dt = nullptr;
@@ -1180,6 +1187,7 @@ ResidentCells res_cells(const NbState* st) {
     ResidentCells RC;
     RC.ncells = st->ncells;
     RC.capc = st->capc;
+    RC.mcap = st->mcap;
     RC.nbr = st->r_nbr;
     RC.cell_h = st->r_cell_h;
     return RC;
@@ -1188,8 +1196,9 @@ ResidentCells res_cells(const NbState* st) {
 int res_grid(const NbState* st) { return (st->ncells + 7) / 8; }      // 8 warps (cells) per block
 
 // Uploads the engines' particles into the device cells.  margin: spare slots per cell
-// (negative: half the largest cell plus 8).
-int st_resident_begin(NbState* st, int margin) {
+// beyond the largest (negative: an eighth of the largest cell plus 8); mcap: leavers per
+// cell and step.
+int st_resident_begin(NbState* st, int margin, int mcap) {
     CU(cudaSetDevice(st->device));
     CU(cudaStreamSynchronize(st->stream));
     res_free(st);
@@ -1207,8 +1216,10 @@ int st_resident_begin(NbState* st, int margin) {
         errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_maxparts;
     }
-    if (margin < 0) margin = maxc / 2 + 8;
-    st->capc = std::min(kMaxPartsPerCell, (maxc + std::max(margin, 4) + 3) & ~3);
+    if (margin < 0) margin = maxc / 8 + 8;
+    st->res_margin = std::max(margin, 4);
+    st->mcap = std::max(mcap, 16);
+    st->capc = std::min(kMaxPartsPerCell, (maxc + st->res_margin + 3) & ~3);
     const size_t slots = (size_t)nc * st->capc;
     for (int q = 0; q < 2; q++) {
         CU(cudaMalloc(&st->r_xq[q], sizeof(float4) * slots));
@@ -1217,11 +1228,15 @@ int st_resident_begin(NbState* st, int margin) {
     }
     CU(cudaMalloc(&st->r_keys, sizeof(unsigned) * 13 * slots));
     CU(cudaMalloc(&st->r_force, sizeof(unsigned long long) * 3 * slots));
-    CU(cudaMalloc(&st->r_count, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_cnt[0], sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_cnt[1], sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_done, sizeof(unsigned long long)));
+    CU(cudaMemset(st->r_done, 0, sizeof(unsigned long long)));
+    CU(cudaMemset(st->r_cnt[1], 0, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_cstart, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_nstay, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_nmove, sizeof(int) * (nc + 1)));
-    CU(cudaMalloc(&st->r_movers, sizeof(Mover) * (size_t)nc * kMoversPerCell));
+    CU(cudaMalloc(&st->r_movers, sizeof(Mover) * (size_t)nc * st->mcap));
     CU(cudaMalloc(&st->r_slot_of, sizeof(int) * (nid + 1)));
     CU(cudaMalloc(&st->r_nbr, sizeof(int) * 27 * (size_t)nc));
     CU(cudaMalloc(&st->r_cell_h, sizeof(float4) * (nc + 1)));
@@ -1274,7 +1289,7 @@ int st_resident_begin(NbState* st, int margin) {
     CU(cudaMemcpy(st->r_cell_h, cell_h.data(), sizeof(float4) * nc, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_dt, edt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_imass, imass.data(), sizeof(double) * imass.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_count, count.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_cnt[0], count.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
 
     // Particles in cell order (dense), then into the cells' blocks on the device.
     std::vector<float4> dxq(n + 1), dv(n + 1);
@@ -1309,10 +1324,10 @@ int st_resident_begin(NbState* st, int margin) {
     CU(cudaMemcpy(t_pid, dpid.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(t_off, doff.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
     const ResidentCells RC = res_cells(st);
-    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, t_xq, t_v, t_pid, t_off, st->r_count, st->r_xq[0],
+    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, t_xq, t_v, t_pid, t_off, st->r_cnt[0], st->r_xq[0],
                                                       st->r_v[0], st->r_pid[0]);
     CU(cudaGetLastError());
-    slot_of_ids<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_pid[0], st->r_count, st->r_slot_of);
+    slot_of_ids<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_pid[0], st->r_cnt[0], st->r_slot_of, nullptr);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(st->stream));
     cudaFree(t_xq);
@@ -1320,6 +1335,8 @@ int st_resident_begin(NbState* st, int margin) {
     cudaFree(t_pid);
     cudaFree(t_off);
     st->res_nparts = n;
+    st->res_done = st->res_done_total = 0;
+    st->res_regrows = 0;
     st->res_engine_n.assign(ne, 0);
     for (int k = 0; k < ne; k++)
         for (int c = 0; c < st->engines[k]->s.nr_cells; c++) st->res_engine_n[k] += count[st->cell_off[k] + c];
@@ -1334,16 +1351,16 @@ int res_issue_step(NbState* st) {
     const int r = st->rside, o = 1 - r;
     const ResidentCells RC = res_cells(st);
     const int grid = res_grid(st);
-    rebin_split<<<grid, 256, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_count, st->r_xq[o],
+    rebin_split<<<grid, 256, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_cnt[r], st->r_xq[o],
                                               st->r_v[o], st->r_pid[o], st->r_nstay, st->r_nmove, st->r_movers,
                                               st->r_status);
     rebin_gather<<<grid, 256, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
-                                               st->r_pid[o], st->r_count, st->r_status);
+                                               st->r_pid[o], st->r_cnt[o], st->r_status);
     CU(cudaGetLastError());
     bool rigid = false;
     for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
     if (rigid) {
-        slot_of_ids<<<grid, 256, 0, st->stream>>>(RC, st->r_pid[o], st->r_count, st->r_slot_of);
+        slot_of_ids<<<grid, 256, 0, st->stream>>>(RC, st->r_pid[o], st->r_cnt[o], st->r_slot_of, st->r_status);
         CU(cudaGetLastError());
     }
     DevView V;
@@ -1352,14 +1369,16 @@ int res_issue_step(NbState* st) {
     V.keys = st->r_keys;
     V.force = st->r_force;
     V.cstart = st->r_cstart;
-    V.ccount = st->r_count;
+    V.ccount = st->r_cnt[o];
+    V.abort = st->r_status;
     V.slots = (size_t)st->ncells * st->capc;
     V.cap4 = st->capc;
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
     int rc = issue_kernels(st, V);
     if (rc < 0) return rc;
-    integrate_cells<<<grid, 256, 0, st->stream>>>(RC, st->r_count, st->r_force, st->r_cell_engine, st->r_engine_dt,
-                                                  st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o]);
+    integrate_cells<<<grid, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
+                                                  st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o],
+                                                  st->r_status, st->r_done);
     CU(cudaGetLastError());
     for (size_t k = 0; k < st->engines.size(); k++) {
         struct engine* e = st->engines[k];
@@ -1371,6 +1390,7 @@ int res_issue_step(NbState* st) {
         view.v = st->r_v[o];
         view.capc = st->capc;
         view.cell0 = st->cell_off[k];
+        view.abort = st->r_status;
         rc = rigid_eval_resident(e, &view, st->stream);
         if (rc < 0) return rc;
     }
@@ -1391,17 +1411,11 @@ long long res_key(const NbState* st) {
     return k;
 }
 
-// nsteps device-resident time steps.  Steps run as direct launches until every engine with
-// rigid groups is past the P-SHAKE refinement steps; then, with graphs enabled, the first
-// step from each side sets up, the second is captured, later ones replay.
-int st_resident_steps(NbState* st, int nsteps) {
-    if (!st->res_active) {
-        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
-                      __func__, __FILE__);
-        return engine_err = engine_err_cuda;
-    }
-    CU(cudaSetDevice(st->device));
-    CU(cudaEventRecord(st->ev0, st->stream));
+// Issues nsteps resident steps (no host synchronisation).  Steps run as direct launches
+// until every engine with rigid groups is past the P-SHAKE refinement steps; then, with
+// graphs enabled, the first step from each side sets up, the second is captured, later
+// ones replay.
+int res_issue_steps(NbState* st, int nsteps) {
     for (int k = 0; k < nsteps; k++) {
         bool refine = false;
         for (struct engine* e : st->engines) {
@@ -1442,16 +1456,54 @@ int st_resident_steps(NbState* st, int nsteps) {
         }
         st->rside = 1 - side;
     }
-    CU(cudaEventRecord(st->ev1, st->stream));
-    // Re-binning overflow is reported once per call.
-    unsigned long long status = 0;
-    CU(cudaMemcpyAsync(&status, st->r_status, sizeof(status), cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaStreamSynchronize(st->stream));
-    if (status) {
-        errs_register(engine_err_maxparts, "Device cell capacity exceeded during resident steps.", __LINE__,
+    return 0;
+}
+
+int st_resident_sync(NbState* st);
+
+// nsteps device-resident time steps (e->time advances by nsteps).
+int st_resident_steps(NbState* st, int nsteps) {
+    if (!st->res_active) {
+        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
                       __func__, __FILE__);
-        return engine_err = engine_err_maxparts;
+        return engine_err = engine_err_cuda;
     }
+    CU(cudaSetDevice(st->device));
+    CU(cudaEventRecord(st->ev0, st->stream));
+    // A step that overflowed a cell block (or the leaver lists) was aborted with every step
+    // after it: the device still holds the last completed step.  Re-block with twice the
+    // room from there and run the remaining steps (at most 8 times per call).
+    int left = nsteps, regrows = 0;
+    while (left > 0) {
+        const int side0 = st->rside;
+        int rc = res_issue_steps(st, left);
+        if (rc < 0) return rc;
+        unsigned long long w[2] = {0, 0};
+        CU(cudaMemcpyAsync(&w[0], st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaMemcpyAsync(&w[1], st->r_done, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaStreamSynchronize(st->stream));
+        const long long completed = (long long)w[1] - st->res_done;
+        st->res_done = (long long)w[1];
+        if (w[0] == 0) break;
+        for (struct engine* e : st->engines) e->time -= (int)(left - completed);
+        st->rside = side0 ^ (int)(completed & 1);
+        left -= (int)completed;
+        const bool cells = (w[0] & kStatusResidentOverflow) != 0, movers = (w[0] & kStatusMoverOverflow) != 0;
+        if (++regrows > 8 || (cells && st->capc >= kMaxPartsPerCell)) {
+            errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded during resident steps.",
+                          __LINE__, __func__, __FILE__);
+            return engine_err = engine_err_maxparts;
+        }
+        rc = st_resident_sync(st);
+        if (rc < 0) return rc;
+        const long long done = st->res_done_total + st->res_done;
+        const int total_regrows = st->res_regrows + 1;
+        rc = st_resident_begin(st, cells ? 2 * st->res_margin : st->res_margin, movers ? 2 * st->mcap : st->mcap);
+        if (rc < 0) return rc;
+        st->res_done_total = done;
+        st->res_regrows = total_regrows;
+    }
+    CU(cudaEventRecord(st->ev1, st->stream));
     return 0;
 }
 
@@ -1469,7 +1521,7 @@ int st_resident_sync(NbState* st) {
     const ResidentCells RC = res_cells(st);
     int* cnt = st->h_rcount;                     // counts, then offsets
     int* off = st->h_rcount + nc + 1;
-    CU(cudaMemcpyAsync(cnt, st->r_count, sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(cnt, st->r_cnt[st->rside], sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
     CU(cudaStreamSynchronize(st->stream));
     // Every particle must still be in one of its engine's cells; else the host keeps its copy.
     off[0] = 0;
@@ -1483,7 +1535,8 @@ int st_resident_sync(NbState* st) {
     const long long n = off[nc];
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[st->rside], st->r_v[st->rside],
-                                                        st->r_pid[st->rside], st->r_count, st->r_doff, st->r_force,
+                                                        st->r_pid[st->rside], st->r_cnt[st->rside], st->r_doff,
+                                                        st->r_force,
                                                         st->r_dense, st->r_dpid);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
@@ -1679,7 +1732,7 @@ extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
 // Runs further launches on a caller-provided stream (e.g. the framework's current stream).
 extern "C" int engine_cuda_resident_begin(struct engine* e, int margin) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    return st_resident_begin(state(e), margin);
+    return st_resident_begin(state(e), margin, 16);
 }
 
 extern "C" int engine_cuda_resident_steps(struct engine* e, int nsteps) {
@@ -1690,6 +1743,24 @@ extern "C" int engine_cuda_resident_steps(struct engine* e, int nsteps) {
 extern "C" int engine_cuda_resident_sync(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     return st_resident_sync(state(e));
+}
+
+int st_resident_info(const NbState* st, int* capc, int* mcap, long long* steps, int* regrows) {
+    if (!st->res_active) {
+        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
+    if (capc) *capc = st->capc;
+    if (mcap) *mcap = st->mcap;
+    if (steps) *steps = st->res_done_total + st->res_done;
+    if (regrows) *regrows = st->res_regrows;
+    return 0;
+}
+
+extern "C" int engine_cuda_resident_info(struct engine* e, int* capc, int* mcap, long long* steps, int* regrows) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident_info(state(e), capc, mcap, steps, regrows);
 }
 
 extern "C" int engine_cuda_resident_end(struct engine* e) {
@@ -1808,7 +1879,7 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
 // engine_zero_forces for every engine of the batch (host threads over the cells).
 extern "C" int engine_batch_resident_begin(struct engine_batch* b, int margin) {
     if (b == nullptr) return engine_err_null;
-    return st_resident_begin(bstate(b), margin);
+    return st_resident_begin(bstate(b), margin, 16);
 }
 
 extern "C" int engine_batch_resident_steps(struct engine_batch* b, int nsteps) {
@@ -1819,6 +1890,12 @@ extern "C" int engine_batch_resident_steps(struct engine_batch* b, int nsteps) {
 extern "C" int engine_batch_resident_sync(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
     return st_resident_sync(bstate(b));
+}
+
+extern "C" int engine_batch_resident_info(struct engine_batch* b, int* capc, int* mcap, long long* steps,
+                                          int* regrows) {
+    if (b == nullptr) return engine_err_null;
+    return st_resident_info(bstate(b), capc, mcap, steps, regrows);
 }
 
 extern "C" int engine_batch_resident_end(struct engine_batch* b) {
@@ -2044,7 +2121,8 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     if (cap4 == 0) return 0;
     const int cpc = sort_cells_per_block(nslots, st->ncells);
     sort_cells<<<(st->ncells + cpc - 1) / cpc, kSortWarps * 32, sort_smem_bytes(), s>>>(
-        static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale, st->ncells, cpc, acc);
+        static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale, st->ncells, cpc, acc,
+        nullptr);
     CU(cudaGetLastError());
 
     TunedParams T;
@@ -2075,6 +2153,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     P.cutoff2 = cutf * cutf;
     P.cutoff2s = (float)e->s.cutoff2;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
+    P.abort = nullptr;
     T.order = st->d_order;
     T.qcount = nullptr;
     T.counter = counter;

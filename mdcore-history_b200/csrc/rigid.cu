@@ -51,6 +51,7 @@ struct RigidArgs {
     float4* rv;                 // device cells: velocity
     int capc, cell0;            // slots per cell, this engine's first global cell
     int cd0, cd1, cd2;          // cell grid
+    const unsigned long long* abort;   // resident: nonzero = the step was aborted
 };
 
 // Cell grid coordinates of a resident slot.
@@ -140,6 +141,7 @@ template <int MP, int MC, bool RES>
 __global__ void __launch_bounds__(128) rigid_shake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
+    if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -188,6 +190,7 @@ template <int MP, int MC, bool RES>
 __global__ void __launch_bounds__(128) rigid_pshake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
+    if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -597,6 +600,7 @@ extern "C" int rigid_eval_resident(struct engine* e, const struct rigid_resident
     A.cd0 = s->cdim[0];
     A.cd1 = s->cdim[1];
     A.cd2 = s->cdim[2];
+    A.abort = view->abort;
     CU(cudaMemsetAsync(rd->d_stat, 0, sizeof(int) * 2, stream));
     launch_sized<true>(rd, !(e->flags & engine_flag_shake), A, stream);
     CU(cudaGetLastError());

@@ -146,6 +146,8 @@ def lib() -> C.CDLL:
         "engine_batch_resident_steps": (C.c_int, [vp, C.c_int]),
         "engine_batch_resident_sync": (C.c_int, [vp]),
         "engine_batch_resident_end": (C.c_int, [vp]),
+        "engine_cuda_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), ip]),
+        "engine_batch_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), ip]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -296,6 +298,13 @@ class Engine:
     def resident_end(self):
         _check(self.lib.engine_cuda_resident_end(self.ptr), "engine_cuda_resident_end")
         return self
+
+    def resident_info(self):
+        """(slots per cell, leavers per cell and step, completed steps, re-blockings)."""
+        a, b, c, d = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
+        _check(self.lib.engine_cuda_resident_info(self.ptr, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "engine_cuda_resident_info")
+        return a.value, b.value, c.value, d.value
 
     def load_parts(self):
         _check(self.lib.engine_cuda_load_parts(self.ptr), "engine_cuda_load_parts")
@@ -516,6 +525,12 @@ class Batch:
     def resident_end(self):
         _check(self.lib.engine_batch_resident_end(self.ptr), "engine_batch_resident_end")
         return self
+
+    def resident_info(self):
+        a, b, c, d = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
+        _check(self.lib.engine_batch_resident_info(self.ptr, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "engine_batch_resident_info")
+        return a.value, b.value, c.value, d.value
 
     def load_parts(self):
         _check(self.lib.engine_batch_load_parts(self.ptr), "engine_batch_load_parts")

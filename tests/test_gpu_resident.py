@@ -154,21 +154,41 @@ def crowding_system():
                     x=x, type=np.zeros(len(x), np.int32), excl=np.zeros((0, 2), np.int32), dt=0.005, v=v)
 
 
-def test_block_overflow_is_an_error_not_a_fault():
+def test_block_overflow_regrows_and_matches_engine_step():
+    """Twelve slots per cell: the second step's re-binning would put 16 particles into one
+    block.  The step is aborted on the device, the particles of step 1 are re-blocked with
+    more room and step 2 runs again: the same result as engine_step."""
     sysm = crowding_system()
+    ref, _ = host_run(sysm, 3)
     e = M.Engine.from_system(sysm)
-    before = e.parts()
     e.resident_begin(margin=0)
-    with pytest.raises(M.MdcoreError, match="-24"):
-        e.resident_steps(2)
-    M.lib().errs_clear()
-    with pytest.raises(M.MdcoreError, match="-24"):
-        e.resident_sync()                             # dropped particles: host copy kept
-    M.lib().errs_clear()
-    x, v, _, c = e.parts()
-    assert np.array_equal(c, before[3]) and np.array_equal(bits(x), bits(before[0]))
-    # with room to spare the same steps run and match engine_step
-    e.resident_begin(margin=16).resident_steps(2).resident_sync()
-    ref, _ = host_run(sysm, 2)
+    assert e.resident_info()[0] == 12
+    e.resident_steps(3).resident_sync()
+    capc, mcap, steps, regrows = e.resident_info()
+    assert regrows == 1 and steps == 3 and capc >= 16
+    same_state(ref, (e.parts(), e.stats()))
+    e.close()
+
+
+def test_many_leavers_regrow_the_lists():
+    """The whole box drifts by 0.6 nm per step: two layers of nine particles leave every
+    cell in the same step (more than 16), the leaver lists double and the steps match
+    engine_step."""
+    rng = np.random.default_rng(11)
+    A, B = W.lj_AB(0.996, 0.3405)
+    g = np.stack(np.meshgrid(*[np.arange(3)] * 3, indexing="ij"), -1).reshape(-1, 3).astype(float)
+    sub = np.stack(np.meshgrid(*[[0.1, 0.4, 0.7]] * 3, indexing="ij"), -1).reshape(-1, 3)
+    x = (g[:, None, :] + sub[None, :, :]).reshape(-1, 3) + rng.uniform(0, 0.02, size=(27 * 27, 3))
+    v = np.tile([[120.0, 0.0, 0.0]], (len(x), 1))         # 0.6 nm per step of 0.005 ps: 18 leave a cell
+    sysm = W.System(name="drift", origin=np.zeros(3), dim=np.full(3, 3.0), L=np.full(3, 1.0), cutoff=1.0,
+                    masses=[39.948], charges=[0.0],
+                    pots=[W.PotSpec(W.KIND_LJ126, 0, 0, 0.25, 1.0, 1e-4, (A * 1e-6, B * 1e-6, 0.0, 0.0))],
+                    x=x, type=np.zeros(len(x), np.int32), excl=np.zeros((0, 2), np.int32), dt=0.005, v=v)
+    ref, _ = host_run(sysm, 8)
+    e = M.Engine.from_system(sysm)
+    e.graph(True)
+    e.resident_begin().resident_steps(8).resident_sync()
+    capc, mcap, steps, regrows = e.resident_info()
+    assert mcap > 16 and regrows >= 1 and steps == 8
     same_state(ref, (e.parts(), e.stats()))
     e.close()
