@@ -1,24 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark of the nonbonded hot path: pair interactions per second on rigid SPC/E water
-(98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions per molecule) by default; also LJ
-argon (32,000 atoms), the 1,048,576-atom LJ slab and the 512-replica argon ensemble
+"""Benchmark of the nonbonded hot path inside the MD step: pair interactions per second and
+ns/day on rigid SPC/E water (98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions and 3
+constraints per molecule, 300 K, dt 2 fs) by default; also LJ argon (32,000 atoms, 100 K),
+the 1,048,576-atom LJ slab (90 K) and the 512-replica argon ensemble (80-140 K)
 (--workload argon|slab|replicas).
 
-One step = one nonbonded force evaluation of the whole system (of every replica): sort every
-cell along the 13 pair directions, sweep all cell-pair/self tasks, fixed-point force
-accumulation, FP64 energy and virial.  The launch shape comes from the autotuner and every
-evaluation replays a CUDA graph of its launches.
+One step = one engine_step of the whole system (of every replica): re-binning, sort of
+every cell along the 13 pair directions, the cell-pair/self sweep with fixed-point force
+accumulation and FP64 energy/virial, the symplectic Euler update, the rigid constraints
+(P-SHAKE, FP64).  Pairs per step = accepted pairs within the cutoff (excluded pairs not
+counted), counted on the device every step.  The sweep's launch shape comes from the
+autotuner.
 
-  value   device-resident: positions already in HBM, kernels only (CUDA events around each
-          step on the launching stream; L2 flushed with a 256 MiB write before every step,
-          outside the events).
-  e2e     the C-ABI call engine_nonbond_cuda (engine_batch_nonbond for the replicas) with
-          host buffers: packing the cells, one host->device copy of positions/ids/cell
-          offsets, sort + sweep, one device->host copy of forces and energies, unpacking.
-  plain   the plain form (one block per task) on the same protocol; for the replicas also
-          the ensemble evaluated as 512 sequential single-engine plain runs.
+  value   device-resident steps (engine_cuda_resident_steps / engine_batch_resident_steps):
+          particles in HBM, one CUDA graph per step; CUDA events recorded on the launching
+          stream inside the graph around each step's launches, L2 flushed with a 256 MiB
+          write before every step (outside the events).
+  e2e     engine_step (engine_batch_step) through the C ABI with host buffers: every step
+          the host cells' positions, velocities and ids go up, one device step runs, and
+          positions, velocities, forces, ids, energies and statistics come back into the
+          host cells.
+  plain   the same resident steps with the plain sweep (one block per task, IEEE sqrt/div):
+          "tuned vs plain".
+  force_eval  the force evaluation alone (sort + sweep) on the same particles, resident
+          and through engine_nonbond_cuda with host buffers.
+  roofline    the sweep kernel inside the timed resident steps (its own CUDA events).
 
-Multi-GPU: the path is not partitioned here ("replicas only"): each rank evaluates its own
+Multi-GPU: the path is not partitioned here ("replicas only"): each rank steps its own
 copy of the workload and value = ranks * pairs / max-over-ranks time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
@@ -30,7 +38,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -39,24 +46,48 @@ sys.path.insert(0, os.path.join(ROOT, "mdcore-history_b200"))
 METRIC = "pair interactions/s + ns/day, 1 B200: tuned vs plain at ≤1e-5 rel force err"
 UNIT = "pair interactions/s"
 FLOPS_PER_PAIR = 45          # per accepted pair, FMA = 2 (roofline)
-DT_FS = 2.0
 
 
-def ns_per_day(ms_per_step):
-    return DT_FS * 1e-6 * 86400.0 / (ms_per_step * 1e-3)
+def ns_per_day(ms_per_step, dt_fs):
+    return dt_fs * 1e-6 * 86400.0 / (ms_per_step * 1e-3)
+
+
+def _water(W):
+    return W.with_rigid_water(W.water_spce(32), 300.0, seed=1)
+
+
+def _argon(W):
+    s = W.argon_fcc(20)
+    s.v = W.maxwell_velocities(s, 100.0, seed=1)
+    return s
+
+
+def _slab(W):
+    s = W.lj_slab()
+    s.v = W.maxwell_velocities(s, 90.0, seed=1)
+    return s
+
+
+def _replicas(W):
+    import numpy as np
+    out = W.argon_replicas()
+    temps = np.random.default_rng(7).uniform(80.0, 140.0, size=len(out))
+    for k, s in enumerate(out):
+        s.v = W.maxwell_velocities(s, float(temps[k]), seed=100 + k)
+    return out
 
 
 WORKLOADS = {
-    "water": ("rigid SPC/E water, 98,304 atoms (32,768 molecules) in a 9.9365 nm periodic box, 9x9x9 cells, "
-              "cutoff 1.0 nm, 98,304 exclusions, seeded", lambda W: W.water_spce(32),
+    "water": ("rigid SPC/E water, 98,304 atoms (32,768 molecules, 98,304 constraints, P-SHAKE) in a 9.9365 nm "
+              "periodic box, 9x9x9 cells, cutoff 1.0 nm, 98,304 exclusions, 300 K, dt 2 fs, seeded", _water,
               "sweep_water98k_traffic.txt"),
     "slab": ("LJ liquid slab in vapour, 1,048,576 atoms (80/20 two types) in a 40x40x160 nm box, 40x40x160 cells, "
-             "cutoff 1.0 nm, seeded", lambda W: W.lj_slab(), "sweep_slab1m_traffic.txt"),
+             "cutoff 1.0 nm, 90 K, dt 5 fs, seeded", _slab, "sweep_slab1m_traffic.txt"),
     "argon": ("LJ argon, 32,000 atoms on a jittered FCC lattice in an 11.5074 nm box, 11^3 cells, cutoff 1.0 nm, "
-              "seeded", lambda W: W.argon_fcc(20), "sweep_argon32k_traffic.txt"),
+              "100 K, dt 5 fs, seeded", _argon, "sweep_argon32k_traffic.txt"),
     "replicas": ("512 LJ argon replicas, N log-uniform 500-8,000 (1,451,403 atoms in all), density 18-24 "
-                 "atoms/nm^3, cubic periodic boxes, cutoff 1.0 nm, seeded; one batch", lambda W: W.argon_replicas(),
-                 "sweep_replicas512_traffic.txt"),
+                 "atoms/nm^3, cubic periodic boxes, cutoff 1.0 nm, 80-140 K, dt 5 fs, seeded; one batch",
+                 _replicas, "sweep_replicas512_traffic.txt"),
 }
 SELECTED = "water"
 
@@ -107,38 +138,38 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_reference_driver(sysm, threads, warmup, steps):
+# ---------------------------------------------------------------- the reference on the host
+
+def run_reference_md(sysm, threads, warmup, steps):
+    """The reference's engine_step (oracle/_ref/ref_driver mdbench: its pthreads runners,
+    integration, P-SHAKE for rigid systems) on one system; ms per step."""
     import workloads as W
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     with tempfile.TemporaryDirectory() as tmp:
-        sysf = os.path.join(tmp, "system.sys")
-        W.write_sysfile(sysm, sysf)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
-        r = subprocess.run([exe, "bench", sysf, str(threads), str(warmup), str(steps)], capture_output=True,
-                           text=True, env=env, check=True)
-    line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
-    return json.loads(line)
-
-
-def run_reference_md(threads, warmup, steps):
-    """The reference's engine_step on rigid SPC/E water (P-SHAKE, dt = 2 fs), all runners."""
-    import workloads as W
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
-    if not os.path.exists(exe):
-        raise FileNotFoundError(exe)
-    sysm = W.with_rigid_water(W.water_spce(32), 300.0, seed=1)
-    with tempfile.TemporaryDirectory() as tmp:
-        sysf, rigf = os.path.join(tmp, "water.sys"), os.path.join(tmp, "water.rig")
+        sysf, rigf = os.path.join(tmp, "system.sys"), os.path.join(tmp, "system.rig")
         W.write_sysfile(sysm, sysf)
         W.write_rigidfile(sysm, rigf, shake=False)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_WAIT_POLICY="PASSIVE")
         r = subprocess.run([exe, "mdbench", sysf, rigf, str(threads), str(warmup), str(steps)], capture_output=True,
                            text=True, env=env, check=True)
-    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
-    return {"ms_per_step": d["ms_per_step"], "ns_per_day": ns_per_day(d["ms_per_step"]), "steps": steps,
-            "cores": threads, "what": "reference engine_step of rigid SPC/E water (P-SHAKE), pthreads runners"}
+    return json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])["ms_per_step"]
+
+
+_PAIRS = {}
+
+
+def pair_count(sysm):
+    """Accepted pairs of the system's initial configuration (the reference's pair set,
+    counted by the oracle)."""
+    if sysm.name not in _PAIRS:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import mdcore_b200 as M
+        import oracle as O
+        tables = [M.create_potential(p).contents.table() for p in sysm.pots]
+        _PAIRS[sysm.name] = O.nonbond(sysm, tables)["pairs"]
+    return _PAIRS[sysm.name]
 
 
 def host_threads():
@@ -149,72 +180,54 @@ def host_threads():
 
 
 def cpu_sample(systems, threads, steps=5, every=16):
-    """The reference's pthreads CPU runner on a bounded sample of the workload: the whole
-    system, or every `every`-th replica of an ensemble; pairs per second over the sample."""
+    """The reference's engine_step with its pthreads runners on a bounded sample of the
+    workload (the whole system, or every `every`-th replica of an ensemble): pairs per
+    second over the sample, pairs of the initial configurations."""
     sample = systems if len(systems) == 1 else systems[::every]
     try:
         ms = pairs = 0.0
         for s in sample:
-            r = run_reference_driver(s, threads, 1, steps)
-            ms += r["ms_per_step"]
+            ms += run_reference_md(s, threads, 1, steps)
             pairs += pair_count(s)
     except (FileNotFoundError, subprocess.CalledProcessError) as exc:
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
     what = ("the full system" if len(systems) == 1 else
             f"{len(sample)} of the {len(systems)} replicas (every {every}th, {int(sum(s.n for s in sample))} atoms)")
     return {"value": pairs / (ms * 1e-3), "unit": UNIT, "cores": threads, "kind": "reference",
-            "ms_per_step": ms, "sample": f"{steps} engine_step calls (dt=0) of {what} on {threads} pthreads runners, "
-                                        f"reference build in oracle/_ref"}
+            "ms_per_step": ms, "sample": f"{steps} engine_step calls of {what} on {threads} pthreads runners "
+                                        f"(reference build in oracle/_ref, P-SHAKE where the system is rigid)"}
 
 
 def reference_arm(args, rank):
-    """The reference's own pthreads CPU runner (oracle/_ref, built from the reference
-    sources) on the same workload, all host threads."""
+    """The reference's own engine_step with its pthreads CPU runners (oracle/_ref, built from
+    the reference sources) on the same workload, all host threads."""
     if rank != 0:
         return
     built = build_system()
     systems = built if isinstance(built, list) else [built]
     threads = host_threads()
-    steps = max(1, min(args.steps, 20 if len(systems) == 1 else 3))
+    steps = max(1, min(args.steps, 10 if len(systems) == 1 else 3))
     cb = cpu_sample(systems, threads, steps=steps)
     if cb["value"] is None:
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {cb['sample']}"}))
         return
-    ms = cb.pop("ms_per_step")
+    sample_ms = cb.pop("ms_per_step")
     v = cb["value"]
     pairs = sum(pair_count(s) for s in systems)
-    md = None
-    if SELECTED == "water":
-        try:
-            md = run_reference_md(threads, 2, max(2, min(args.steps, 10)))
-        except (FileNotFoundError, subprocess.CalledProcessError) as exc:
-            md = {"unavailable": str(exc)}
+    ms = pairs / v * 1e3
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": pairs / v * 1e3,
+        "steps": steps, "warmup": 1, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "ns_per_day": ns_per_day(pairs / v * 1e3),
+        "data": "synthetic", "ns_per_day": ns_per_day(ms, systems[0].dt * 1e3),
         "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "parallelism": "pthreads runners",
-                   "sample_ms_per_step": ms},
+                   "sample_ms_per_step": sample_ms},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        **({"md_step": md} if md is not None else {}),
     }))
 
 
-_PAIRS = {}
-
-
-def pair_count(sysm):
-    """Pairs per step of the workload (the reference's pair set, counted by the oracle)."""
-    if sysm.name not in _PAIRS:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import mdcore_b200 as M
-        import oracle as O
-        tables = [M.create_potential(p).contents.table() for p in sysm.pots]
-        _PAIRS[sysm.name] = O.nonbond(sysm, tables)["pairs"]
-    return _PAIRS[sysm.name]
-
+# ---------------------------------------------------------------- this library on the GPU
 
 def cell_counts(sysm, e):
     """Particles per cell of one engine (cells as space_init lays them out)."""
@@ -224,33 +237,59 @@ def cell_counts(sysm, e):
 
 
 def transfer_bytes(systems, engines):
-    """Bytes copied per host-buffer evaluation: positions+types and ids per padded slot and
-    the cell offsets/counts up; float forces per slot, cell energies and virials and the
-    counters down."""
-    slots = ncells = 0
+    """Bytes copied per engine_step (device step with the host cells as input and output):
+    up, positions+types and velocities (32 B) and ids (4 B) per particle, counts and offsets
+    (8 B) per cell; down, the step's status and counters (24 B), counts (4 B) per cell,
+    positions, velocities and forces (48 B) and ids (4 B) per particle, offsets up (4 B per
+    cell), cell energies and virials (16 B per cell), the 64-byte accumulator block and the
+    constraint statistics (8 B per rigid engine).  Also the cell count and whether any cell
+    is empty (the queue-compaction launches run then)."""
+    n = ncells = nrigid = 0
+    empty = False
     for s, e in zip(systems, engines):
         c = cell_counts(s, e)
-        slots += int((((c + 3) // 4) * 4).sum())
+        n += int(c.sum())
         ncells += len(c)
-    return 20 * slots + 4 * (2 * ncells + 1), 12 * slots + 16 * ncells + 64, ncells, \
-        any((cell_counts(s, e) == 0).any() for s, e in zip(systems, engines))
+        empty = empty or bool((c == 0).any())
+        nrigid += int(s.rigid is not None and len(s.rigid) > 0)
+    h2d = 36 * n + 8 * ncells + 4 + 4 * (ncells + 1)
+    d2h = 24 + 4 * ncells + 52 * n + 16 * ncells + 64 + 8 * nrigid
+    return h2d, d2h, ncells, empty
 
 
-def timed_resident(tgt, stream, flush, steps, torch):
-    """Mean device time (ms) of `steps` device-resident evaluations, L2 flushed before
-    each (outside the events), and the mean sweep-kernel time."""
+def timed_force_evals(tgt, stream, flush, steps, torch):
+    """Mean device time (ms) of `steps` device-resident force evaluations (zeroing, sort,
+    sweep: CUDA events recorded on the launching stream inside the evaluation's graph), L2
+    flushed before each (outside the events), and the mean sweep-kernel time."""
     tot = sweep = 0.0
     for _ in range(steps):
         flush.zero_()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
+        torch.cuda.synchronize()
         tgt.resident()
-        ev1.record(stream)
-        ev1.synchronize()
-        tot += ev0.elapsed_time(ev1)
-        sweep += tgt.kernel_times()[1]
+        t, s = tgt.kernel_times()
+        tot += t
+        sweep += s
     return tot / steps, sweep / steps
+
+
+def timed_resident_steps(tgt, stream, flush, steps, torch):
+    """`steps` device-resident MD steps, one call each, L2 flushed before each (outside the
+    events): mean step time (ms, CUDA events recorded on the launching stream inside the
+    step's graph, first to last launch), mean sweep-kernel time (the sweep's own events),
+    accepted pairs summed over the steps."""
+    p0 = tgt.resident_info().pairs
+    tot = sweep = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        tgt.resident_steps(1)
+        t, s = tgt.kernel_times()
+        tot += t
+        sweep += s
+    info = tgt.resident_info()
+    if info.regrows:
+        raise SystemExit("bench.py: device cells were re-blocked inside the timed region")
+    return tot / steps, sweep / steps, info.pairs - p0
 
 
 def ours(args, rank, world, local_rank):
@@ -270,6 +309,8 @@ def ours(args, rank, world, local_rank):
     built = build_system()
     replicas = isinstance(built, list)
     systems = built if replicas else [built]
+    dt_fs = systems[0].dt * 1e3
+    rigid = any(s.rigid is not None and len(s.rigid) for s in systems)
     if replicas:
         engines = [M.Engine.from_system(s, start=False) for s in systems]
         tgt = M.Batch(engines, device=local_rank)
@@ -280,21 +321,22 @@ def ours(args, rank, world, local_rank):
     torch.cuda.set_stream(stream)
     tgt.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    # warm-up (host-buffer path, which also uploads the particles)
-    for _ in range(args.warmup):
-        tgt.nonbond()
-    st = tgt.stats()
-    if st.status != 0:
-        raise SystemExit(f"bench.py: device status {st.status}")
-    pairs = int(st.pairs)
+    h2d, d2h, ncells, compact = transfer_bytes(systems, engines)
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- launch shape by the autotuner (or --launch), then CUDA-graph replay of every evaluation
+    # ---- warm-up of the host-buffer force evaluation (uploads the particles)
+    for _ in range(args.warmup):
+        tgt.nonbond()
+    st = tgt.stats()
+    if st.status != 0:
+        raise SystemExit(f"bench.py: device status {st.status}")
+    fe_pairs = int(st.pairs)
+
+    # ---- launch shape by the autotuner (or --launch), CUDA-graph replay from here on
     tgt.load_parts()
     if args.launch:
         warps, layout, stages, occupancy = (int(v) for v in (args.launch + ",640").split(",")[:4])
@@ -310,18 +352,12 @@ def ours(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
 
-    # ---- device-resident timed region
+    # ---- force evaluation alone (sort + sweep), resident and with host buffers
     barrier()
-    ms, ms_sweep = timed_resident(tgt, stream, flush, args.steps, torch)
+    fe_ms, fe_sweep = timed_force_evals(tgt, stream, flush, args.steps, torch)
     barrier()
     tgt.unload_parts()
-    if tgt.stats().status != 0:
-        raise SystemExit("bench.py: device status after timed region")
-
-    # ---- end-to-end timed region (host buffers through the C ABI, graph replay)
-    barrier()
-    e2e_ms = 0.0
-    host = {"pack": 0.0, "device": 0.0, "unpack": 0.0}
+    fe_e2e = 0.0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -331,112 +367,75 @@ def ours(args, rank, world, local_rank):
         tgt.nonbond()
         ev1.record(stream)
         ev1.synchronize()
-        e2e_ms += ev0.elapsed_time(ev1)
-        hs = tgt.stats()
-        host["pack"] += hs.ms_pack / args.steps
-        host["device"] += hs.ms_device / args.steps
-        host["unpack"] += hs.ms_unpack / args.steps
+        fe_e2e += ev0.elapsed_time(ev1) / args.steps
     barrier()
-    clk = clocks.stop()
-    if tgt.stats().status != 0:
-        raise SystemExit("bench.py: device status after e2e region")
 
-    # ---- water: full MD steps (engine_step: rebin, forces, integration, P-SHAKE on the
-    # device) of the rigid SPC/E system, dt = 2 fs
-    md = None
-    if SELECTED == "water":
-        import workloads as W
-        rig = M.Engine.from_system(W.with_rigid_water(W.water_spce(32), 300.0, seed=1), device=local_rank)
-        rig.set_stream(stream.cuda_stream)
-        rig.load_parts()
-        rig.tune(warps)
-        rig.set_layout(layout, stages, occupancy)
-        rig.graph(True)
-        for _ in range(max(args.warmup, 25)):        # past the 20 P-SHAKE refinement steps
-            rig.step()
-        barrier()
+    # ---- MD steps resident in HBM: the headline value
+    tgt.resident_begin()
+    tgt.resident_steps(max(args.warmup, 25 if rigid else 3))     # past the P-SHAKE refinement steps
+    barrier()
+    ms, ms_sweep, pairs_timed = timed_resident_steps(tgt, stream, flush, args.steps, torch)
+    barrier()
+    pairs = pairs_timed / args.steps
+    tgt.resident_sync()
+    if tgt.stats().status != 0:
+        raise SystemExit("bench.py: device status after the resident steps")
+    shake = None
+    if rigid:
+        itmax, bad = engines[0].rigid_stats()
+        if bad:
+            raise SystemExit("bench.py: rigid groups did not converge")
+        shake = itmax
+
+    # ---- the plain sweep in the same resident steps ("tuned vs plain")
+    tgt.graph(False)
+    tgt.tune(0, plain=True)
+    tgt.resident_steps(2)
+    barrier()
+    plain_ms, plain_sweep, plain_pairs = timed_resident_steps(tgt, stream, flush, args.steps, torch)
+    barrier()
+    tgt.tune(warps, plain=False)
+    tgt.set_layout(layout, stages, occupancy)
+    tgt.graph(True)
+    tgt.resident_end()
+
+    # ---- engine_step with host buffers through the C ABI (e2e)
+    for _ in range(2):
+        tgt.step()
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        for _ in range(args.steps):
-            rig.step()
+        tgt.step()
         ev1.record(stream)
         ev1.synchronize()
-        md_ms = ev0.elapsed_time(ev1) / args.steps
-        itmax, bad = rig.rigid_stats()
-        if rig.stats().status != 0 or bad != 0:
-            raise SystemExit("bench.py: rigid water steps failed")
-        md = {"ms_per_step": md_ms, "ns_per_day": ns_per_day(md_ms), "dt_fs": DT_FS,
-              "what": "engine_step of rigid SPC/E water (32,768 molecules, 98,304 constraints): rebin, "
-                      "forces with host buffers, symplectic Euler, P-SHAKE on the device (FP64)",
-              "shake_max_iterations": itmax}
-        # the same MD steps with the particles resident on the device: re-binning,
-        # forces, integration and P-SHAKE as one CUDA graph per step, no host copies
-        rig.resident_begin()
-        rig.resident_steps(max(args.warmup, 3))
-        barrier()
+        e2e_ms += ev0.elapsed_time(ev1) / args.steps
+    barrier()
+    host_ms = 0.0                       # the host-threaded step, for comparison
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        rig.resident_steps(args.steps)
+        tgt.step_host()
         ev1.record(stream)
         ev1.synchronize()
-        res_ms = ev0.elapsed_time(ev1) / args.steps
-        rig.resident_sync()
-        itmax, bad = rig.rigid_stats()
-        if rig.stats().status != 0 or bad != 0:
-            raise SystemExit("bench.py: resident rigid water steps failed")
-        md["resident"] = {"ms_per_step": res_ms, "ns_per_day": ns_per_day(res_ms),
-                          "what": "engine_cuda_resident_steps: the same steps with the particles resident "
-                                  "in HBM, one CUDA graph per step",
-                          "shake_max_iterations": itmax}
-        rig.resident_end()
-        rig.close()
-
-    # ---- the plain form (one CTA per task, IEEE sqrt/div, no graph), same protocol
-    tgt.graph(False)
-    tgt.tune(0, plain=True)
-    tgt.load_parts()
-    tgt.resident()
+        host_ms += ev0.elapsed_time(ev1) / args.steps
     barrier()
-    plain_ms, plain_sweep = timed_resident(tgt, stream, flush, args.steps, torch)
-    barrier()
-    tgt.tune(warps, plain=False)
-
-    # ---- replicas: the same ensemble as sequential single-engine runs of the plain form
-    seq = None
-    if replicas:
-        singles = [M.Engine.from_system(s, device=local_rank) for s in systems]
-        for e in singles:
-            e.set_stream(stream.cuda_stream)
-            e.tune(0, plain=True)
-            e.load_parts()
-            e.resident()
-        barrier()
-        seq_ms = 0.0
-        for _ in range(args.steps):
-            flush.zero_()
-            ev0 = torch.cuda.Event(enable_timing=True)
-            ev1 = torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
-            for e in singles:
-                e.resident()
-            ev1.record(stream)
-            ev1.synchronize()
-            seq_ms += ev0.elapsed_time(ev1)
-        barrier()
-        seq_ms /= args.steps
-        seq = {"value": world * pairs / (seq_ms * 1e-3), "ms_per_step": seq_ms,
-               "what": f"{len(singles)} sequential single-engine evaluations of the plain form, device-resident"}
-        for e in singles:
-            e.close()
+    clk = clocks.stop()
+    if tgt.stats().status != 0:
+        raise SystemExit("bench.py: device status after the host-buffer steps")
 
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms / args.steps, ms_sweep], device="cuda", dtype=torch.float64)
+        t = torch.tensor([ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e, ms_sweep = [float(v) for v in t.tolist()]
-    else:
-        ms_e2e = e2e_ms / args.steps
+        ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e = [float(v) for v in t.tolist()]
     if rank == 0:
-        h2d, d2h, ncells, compact = transfer_bytes(systems, engines)
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
         traffic = None
@@ -445,43 +444,50 @@ def ours(args, rank, world, local_rank):
             for ln in open(prof):
                 if ln.startswith("dram_bytes_per_launch"):
                     traffic = int(ln.split()[1])
+        # kernels of one resident step: re-binning (2), id -> slot (rigid), sort, queue
+        # compaction (3, systems with empty cells), sweep, integration, constraints (rigid)
+        per_step = 2 + int(rigid) + 1 + 3 * int(compact) + 1 + 1 + int(rigid) * len(engines)
         line = {
             "metric": METRIC, "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "ns_per_day": ns_per_day(ms),
+            "ns_per_day": ns_per_day(ms, dt_fs),
             "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
                        "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
                        "tasks": tgt.ntasks(), "cells": ncells, "parallelism": f"replicas x{world}",
+                       "step": "engine_step on the device: re-binning, sort, sweep, integration"
+                               + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step",
                        "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
                                   "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
                                   "cuda_graph": True},
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
-            "e2e": {"value": world * pairs / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "host_ms": {k: round(v, 4) for k, v in host.items()}},
+            "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                    "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "what": "engine_step (engine_batch_step for the replicas) with the host cells as input "
+                            "and output every step"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+            "plain": {"value": world * (plain_pairs / args.steps) / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                       "sweep_ms": plain_sweep,
-                      "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
-            "gpu_launches": (2 + 3 * int(compact)) * args.steps,
+                      "what": "the same resident steps with the plain sweep: one block per task, IEEE sqrt/div, "
+                              "per-step warp reductions, no graph"},
+            "step_host": {"value": world * pairs / (host_ms * 1e-3), "ms_per_step": host_ms,
+                          "what": "engine_step_host: re-binning and integration on the host threads, forces "
+                                  "and constraints through host buffers"},
+            "force_eval": {"value": world * fe_pairs / (fe_ms * 1e-3), "ms_per_step": fe_ms, "sweep_ms": fe_sweep,
+                           "e2e": {"value": world * fe_pairs / (fe_e2e * 1e-3), "ms_per_step": fe_e2e},
+                           "what": "sort + sweep alone at the initial positions (engine_nonbond_cuda_resident; "
+                                   "e2e: engine_nonbond_cuda with host buffers)"},
+            "gpu_launches": per_step * args.steps,
             "clocks": clk,
         }
-        if seq is not None:
-            line["sequential_plain"] = seq
-        if md is not None:
-            line["md_step"] = md
+        if shake is not None:
+            line["shake_max_iterations"] = shake
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_sample(systems, host_threads())
-            if md is not None:
-                try:
-                    line["cpu_baseline"]["md_step"] = run_reference_md(host_threads(), 2, 5)
-                except (FileNotFoundError, subprocess.CalledProcessError) as exc:
-                    line["cpu_baseline"]["md_step"] = {"unavailable": str(exc)}
         print(json.dumps(line))
     tgt.close()
     for e in engines:

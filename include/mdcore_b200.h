@@ -317,8 +317,17 @@ int engine_exclusion_shrink(struct engine *e);
 int engine_rigid_add(struct engine *e, int pid, int pjd, double d);
 /* src/engine.c:1674-1826 */
 int engine_start(struct engine *e, int nr_runners, int nr_queues);
-/* src/engine.c:2070-2240 */
+/* src/engine.c:2070-2240.  One time step (re-binning, forces, symplectic Euler, rigid
+ * constraints) run on the device with the host cells as input and output: the particles
+ * go up, one device-resident step runs (engine_cuda_resident_*), particles (in the
+ * device's cell order), forces, energies and statistics come back. */
 int engine_step(struct engine *e);
+/* engine_step with re-binning and integration on the host threads and the force evaluation
+ * (engine_nonbond_cuda_fresh) and the constraints (engine_rigid_eval) through host buffers.
+ * Same positions, velocities and energies as engine_step, bit for bit. */
+int engine_step_host(struct engine *e);
+/* The device part of engine_step (no error stack entry of its own). */
+int engine_cuda_step(struct engine *e);
 /* src/engine.c:1945-2052 */
 int engine_advance(struct engine *e);
 /* src/engine.c:2338-2430 */
@@ -366,7 +375,10 @@ int engine_zero_forces(struct engine *e);
 int engine_nonbond_cuda_fresh(struct engine *e);
 /* Makes later launches use this cudaStream_t (e.g. the caller framework's stream). */
 int engine_cuda_setstream(struct engine *e, void *stream);
-/* Device time (ms) of the last evaluation: sort + sweep, and the sweep kernel alone. */
+/* Device time (ms) of the last evaluation: its launches from the first to the last (the
+ * zeroing, sort and sweep; after resident steps the whole last step), and the sweep kernel
+ * alone.  Events recorded on the launch stream, inside the CUDA graph when one is replayed,
+ * so host launch latency is not counted. */
 int engine_cuda_kernel_times(struct engine *e, float *total_ms, float *sweep_ms);
 /* Measured FP32 FMA throughput of a device in TFLOP/s (a register-only FMA loop). */
 int engine_cuda_fp32_peak(int device, float *tflops);
@@ -466,8 +478,7 @@ int engine_cuda_autotune(struct engine *e, int reps, int *warps, int *layout, in
 /* ---- device-resident time steps (replace engine_step, src/engine.c:2070-2240, while
  * the particles stay on the device) ----
  * engine_cuda_resident_begin uploads every particle into fixed blocks of slots per cell
- * (the largest cell plus `margin` spare slots, rounded up to 4; margin < 0: an eighth of
- * the largest cell plus 8).  engine_cuda_resident_steps runs nsteps time steps of
+ * (the largest cell plus `margin` spare slots, rounded up to 4; margin < 0: 8).  engine_cuda_resident_steps runs nsteps time steps of
  * engine_step -- space_shuffle, the nonbonded forces, engine_advance, the rigid
  * constraints -- as device launches only (with engine_cuda_graph, one CUDA graph per
  * step); e->time advances, the host's particles do not.  A step in which a cell outgrows
@@ -486,9 +497,11 @@ int engine_cuda_resident_begin(struct engine *e, int margin);
 int engine_cuda_resident_steps(struct engine *e, int nsteps);
 int engine_cuda_resident_sync(struct engine *e);
 int engine_cuda_resident_end(struct engine *e);
-/* Slots per cell, leavers per cell and step, completed resident steps and automatic
- * re-blockings since engine_cuda_resident_begin; any pointer may be NULL. */
-int engine_cuda_resident_info(struct engine *e, int *capc, int *mcap, long long *steps, int *regrows);
+/* Slots per cell, leavers per cell and step, completed resident steps, the accepted pairs
+ * summed over them, and automatic re-blockings since engine_cuda_resident_begin; any
+ * pointer may be NULL. */
+int engine_cuda_resident_info(struct engine *e, int *capc, int *mcap, long long *steps, long long *pairs,
+                              int *regrows);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff
@@ -505,8 +518,11 @@ int engine_batch_free(struct engine_batch *b);
 int engine_batch_nonbond(struct engine_batch *b);
 /* engine_nonbond_cuda_fresh for every engine. */
 int engine_batch_nonbond_fresh(struct engine_batch *b);
-/* engine_step for every engine with the forces of one batch evaluation. */
+/* engine_step for every engine: one device step of the whole batch, the engines' host
+ * cells as input and output. */
 int engine_batch_step(struct engine_batch *b);
+/* engine_step_host for every engine with the forces of one batch evaluation. */
+int engine_batch_step_host(struct engine_batch *b);
 int engine_batch_load_parts(struct engine_batch *b);
 int engine_batch_resident(struct engine_batch *b);
 int engine_batch_unload_parts(struct engine_batch *b);
@@ -527,7 +543,8 @@ int engine_batch_resident_begin(struct engine_batch *b, int margin);
 int engine_batch_resident_steps(struct engine_batch *b, int nsteps);
 int engine_batch_resident_sync(struct engine_batch *b);
 int engine_batch_resident_end(struct engine_batch *b);
-int engine_batch_resident_info(struct engine_batch *b, int *capc, int *mcap, long long *steps, int *regrows);
+int engine_batch_resident_info(struct engine_batch *b, int *capc, int *mcap, long long *steps, long long *pairs,
+                               int *regrows);
 
 #ifdef __cplusplus
 }

@@ -391,7 +391,18 @@ int engine_advance(struct engine *e) {
     return engine_err_ok;
 }
 
+/* One time step on the device with the host's particles as input and output: upload,
+ * re-binning, forces, integration and constraints as device launches, download
+ * (engine_cuda_step).  The same trajectory as engine_step_host, bit for bit. */
 int engine_step(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (engine_cuda_step(e) < 0) return engine_error(engine_err_cuda);
+    return engine_err_ok;
+}
+
+/* engine_step with re-binning and integration on the host threads and the force
+ * evaluation and constraints through host buffers. */
+int engine_step_host(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
     struct space *s = &e->s;
     e->time += 1;

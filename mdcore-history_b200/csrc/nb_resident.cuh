@@ -13,7 +13,8 @@
 // Overflow: a cell that would exceed its capacity, or more than `mcap` leavers of one cell
 // in one step, sets a sticky abort word.  Every later kernel of that step and of the steps
 // after it returns at once, so the side the step read from keeps the last completed step
-// intact; integrate_cells counts the completed steps, from which the host finds that side,
+// intact; integrate_cells counts the completed steps (and their accepted pairs), from which
+// the host finds that side,
 // re-blocks the particles with more room and runs the remaining steps again.  Nothing is
 // written out of bounds.
 #pragma once
@@ -168,11 +169,15 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
                                                        const double* __restrict__ engine_imass, int max_type,
                                                        float4* __restrict__ xq, float4* __restrict__ v,
                                                        const unsigned long long* __restrict__ status,
-                                                       unsigned long long* __restrict__ steps_done) {
+                                                       const unsigned long long* __restrict__ acc,
+                                                       unsigned long long* __restrict__ done) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (*status != 0) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(steps_done, 1ull);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {          // completed steps, accepted pairs
+        done[0] += 1ull;
+        done[1] += acc[kAccPairs];
+    }
     if (c >= RC.ncells) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;

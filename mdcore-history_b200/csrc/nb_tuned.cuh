@@ -209,11 +209,13 @@ __global__ void __launch_bounds__(kQueueBlock) queue_scatter(const int* __restri
 
 // Shared memory of one worker warp (cap = largest cell rounded up to 4, plus 8 spare rows
 // that the sweep windows may read past the end of the j list): two mbarriers, the j list
-// in sweep order (js, jid, jloc, jdist: 28 B per row) and STAGES staging buffers for the
-// raw bulk copies of a task (xraw, pidraw, keyj, keyi: 28 B per row).  With two stages the
-// copies of the next task land while the warp sweeps the current one.
+// in sweep order (js, jid: 20 B per row) and STAGES staging buffers for the raw bulk copies
+// of a task (xraw, pidraw, keyj, keyi: 28 B per row).  The j list's slots and sort
+// distances are read from the copied keys (keyj, in descending distance order), which stay
+// in place while the task is swept.  With two stages the copies of the next task land
+// while the warp sweeps the current one.
 __host__ __device__ inline size_t warp_slice_bytes(int cap, int stages) {
-    return 16 + (size_t)cap * 28 * (size_t)(stages + 1);
+    return 16 + (size_t)cap * (20 + 28 * (size_t)stages);
 }
 
 __host__ __device__ inline size_t warps_smem_bytes(int cap, int nw, int ncoef, int npots, int mt, int stages) {
@@ -258,9 +260,14 @@ struct WarpSlice {
     unsigned* keyj;
     unsigned* keyi;
     int* jid;
-    int* jloc;
-    int* jdist;
 };
+
+// Slot in cell j and sort distance of the j list's k-th entry (sweep order: ascending
+// distance, the reverse of the copied keys).
+__device__ __forceinline__ int jlist_loc(const WarpSlice& W, int nj, int k) { return W.keyj[nj - 1 - k] >> 16; }
+__device__ __forceinline__ int jlist_dist(const WarpSlice& W, int nj, int k) {
+    return W.keyj[nj - 1 - k] & 0xffff;
+}
 
 __device__ __forceinline__ WarpSlice warp_slice(unsigned char* smem_raw, int cap, int warp, int stages, int stage) {
     unsigned char* wp = smem_raw + (size_t)warp * warp_slice_bytes(cap, stages);
@@ -269,8 +276,6 @@ __device__ __forceinline__ WarpSlice warp_slice(unsigned char* smem_raw, int cap
     wp += 16;
     W.js = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;
     W.jid = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
-    W.jloc = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
-    W.jdist = reinterpret_cast<int*>(wp); wp += (size_t)cap * 4;
     wp += (size_t)stage * cap * 28;
     W.xraw = reinterpret_cast<float4*>(wp); wp += (size_t)cap * 16;
     W.fj = W.xraw;
@@ -374,8 +379,6 @@ __device__ __forceinline__ void build_jlist(const TaskDesc& d, const WarpSlice& 
             const int loc = key >> 16;
             W.js[k] = W.xraw[loc];
             W.jid[k] = W.pidraw[loc];
-            W.jloc[k] = loc;
-            W.jdist[k] = key & 0xffff;
         }
     } else {
         for (int k = lane; k < nj; k += 32) W.js[k] = W.xraw[k];
@@ -453,14 +456,15 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
 }
 
 // Length of the sorted j prefix lane's particle i (sort distance di) interacts with: j
-// whose distance is below dmaxdist - dnshift + di (src/runner_dopair.c:606-612).
-__device__ __forceinline__ int sorted_prefix(const int* __restrict__ jdist, int nj, int lim) {
-    int lo = 0, hi = nj;
+// whose distance is below dmaxdist - dnshift + di (src/runner_dopair.c:606-612).  keyj
+// holds cell j's keys in descending distance order; the prefix is its tail.
+__device__ __forceinline__ int sorted_prefix(const unsigned* __restrict__ keyj, int nj, int lim) {
+    int lo = 0, hi = nj;          // first key (descending) whose distance is below lim
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (jdist[mid] < lim) lo = mid + 1; else hi = mid;
+        if ((int)(keyj[mid] & 0xffff) >= lim) lo = mid + 1; else hi = mid;
     }
-    return lo;
+    return nj - lo;
 }
 
 // The pair interaction of lane's particle i with j at sweep position k: cutoff test on the
@@ -591,7 +595,7 @@ __device__ __forceinline__ void finish_task(const Params& P, const TunedParams& 
         const float4 a = W.fj[k];
         const float4 xk = W.js[k];
         v_task += (double)xk.x * a.x + (double)xk.y * a.y + (double)xk.z * a.z;
-        unsigned long long* fp = P.force + 3 * (size_t)(self ? (d.si + k) : (d.sj + W.jloc[k]));
+        unsigned long long* fp = P.force + 3 * (size_t)(self ? (d.si + k) : (d.sj + jlist_loc(W, d.nj, k)));
         atomic_add_fixed(fp + 0, to_fixed(a.x, status));
         atomic_add_fixed(fp + 1, to_fixed(a.y, status));
         atomic_add_fixed(fp + 2, to_fixed(a.z, status));
@@ -709,7 +713,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
         const int dmaxdist = task_dmax(d.tr);
         double e_task = 0.0, v_task = 0.0;
         const int nchunks = (ni + 31) >> 5;
-        const int jd0 = self ? 0 : W.jdist[0];
+        const int jd0 = self ? 0 : jlist_dist(W, nj, 0);
 
         for (int ch = 0; ch < nchunks; ++ch) {
             const int ii = ch * 32 + lane;
@@ -723,7 +727,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
                 const int di = key & 0xffff;
                 if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
                 if (!__any_sync(FULL, valid)) break;        // later chunks lie farther from cell j
-                if (valid) len = P.unsorted ? nj : sorted_prefix(W.jdist, nj, dmaxdist - dnshift + di);
+                if (valid) len = P.unsorted ? nj : sorted_prefix(W.keyj, nj, dmaxdist - dnshift + di);
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -823,7 +827,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
         const int dmaxdist = task_dmax(d.tr);
         double e_task = 0.0, v_task = 0.0;
         const int nstrips = (ni + 7) >> 3;
-        const int jd0 = self ? 0 : W.jdist[0];
+        const int jd0 = self ? 0 : jlist_dist(W, nj, 0);
 
         for (int st = 0; st < nstrips; ++st) {
             const int ii = st * 8 + row;
@@ -837,7 +841,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
                 const int di = key & 0xffff;
                 if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
                 if (!__any_sync(FULL, valid)) break;        // later strips lie farther from cell j
-                if (valid) len = P.unsorted ? nj : sorted_prefix(W.jdist, nj, dmaxdist - dnshift + di);
+                if (valid) len = P.unsorted ? nj : sorted_prefix(W.keyj, nj, dmaxdist - dnshift + di);
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -22,6 +22,10 @@
 #include <vector>
 #include <algorithm>
 #include <atomic>
+#include <cstdint>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 #include <utility>
 #include <cmath>
 #include <ctime>
@@ -116,11 +120,12 @@ struct NbState {
     // Device-resident steps (nb_resident.cuh): fixed blocks of capc slots per cell, two
     // sides (re-binning writes the other side), static per-id fields for the host copy.
     bool res_active = false;
+    bool res_dirty = false;            // the device holds steps the host cells do not
     int capc = 0, rside = 0, mcap = 16, res_margin = 8;
-    long long res_nparts = 0, res_done = 0, res_done_total = 0;
+    long long res_nparts = 0, res_done = 0, res_done_total = 0, res_pairs = 0, res_pairs_total = 0;
     int res_regrows = 0;
     int* r_cnt[2] = {nullptr, nullptr};      // particles per cell of each side
-    unsigned long long* r_done = nullptr;    // completed resident steps (device counter)
+    unsigned long long* r_done = nullptr;    // completed resident steps, their accepted pairs
     float4* r_xq[2] = {nullptr, nullptr};
     float4* r_v[2] = {nullptr, nullptr};
     int* r_pid[2] = {nullptr, nullptr};
@@ -134,8 +139,9 @@ struct NbState {
     unsigned long long* r_force = nullptr;
     unsigned long long* r_status = nullptr;
     float4* r_dense = nullptr;         // 3 per particle, cell order: position+type, velocity, force
-    float4* h_dense = nullptr;
-    int *r_dpid = nullptr, *h_dpid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
+    float4* h_dense = nullptr;         // downloads (cached host memory)
+    float4* h_up = nullptr;            // uploads: positions, velocities
+    int *r_dpid = nullptr, *h_dpid = nullptr, *h_uppid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
     std::vector<long long> res_engine_n;   // particles of each engine on the device
     std::vector<float> id_q;
     std::vector<int> id_vid;
@@ -199,8 +205,8 @@ int alloc_particles(NbState* st, int ncap) {
         return engine_err_cuda;
     // Upload buffers are only written by the host: write-combined pages take the writes
     // without reading the lines first and stream faster over PCIe.
-    CU(cudaHostAlloc(&st->h_xq, sizeof(float4) * ncap, cudaHostAllocWriteCombined));
-    CU(cudaHostAlloc(&st->h_pid, sizeof(int) * ncap, cudaHostAllocWriteCombined));
+    CU(cudaMallocHost(&st->h_xq, sizeof(float4) * ncap));
+    CU(cudaMallocHost(&st->h_pid, sizeof(int) * ncap));
     CU(cudaMallocHost(&st->h_force, sizeof(unsigned long long) * 3 * ncap));
     cudaFree(st->d_forcef);
     if (dev_alloc(&st->d_forcef, 3 * (size_t)ncap)) return engine_err_cuda;
@@ -214,6 +220,34 @@ int alloc_particles(NbState* st, int ncap) {
 __global__ void fixed_to_float(const unsigned long long* __restrict__ f, float* __restrict__ out, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (float)((double)(long long)f[i] * (1.0 / (double)kForceScale));
+}
+
+// Evicts [p, p + bytes) from the host caches (writing dirty lines back).  The pinned upload
+// and download buffers are written or read by many host threads; lines left in their caches
+// make the copy engine snoop every core (measured: uploads of 3 MB at 6 GB/s instead of
+// 50 GB/s), so each thread evicts what it has written or read.
+#if defined(__x86_64__)
+__attribute__((target("clflushopt"))) static void evict_lines_opt(const void* p, size_t bytes) {
+    const char* c = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(63));
+    const char* e = static_cast<const char*>(p) + bytes;
+    for (; c < e; c += 64) _mm_clflushopt(const_cast<char*>(c));
+}
+#endif
+
+void evict_lines(const void* p, size_t bytes) {
+#if defined(__x86_64__)
+    static const bool opt = __builtin_cpu_supports("clflushopt");
+    if (opt) {
+        evict_lines_opt(p, bytes);
+        return;
+    }
+    const char* c = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(63));
+    const char* e = static_cast<const char*>(p) + bytes;
+    for (; c < e; c += 64) _mm_clflush(c);
+#else
+    (void)p;
+    (void)bytes;
+#endif
 }
 
 double now_ms() {
@@ -301,6 +335,9 @@ void pack_range(NbState* st, int cb, int ce) {
                 for (int q = cl->count; q < pad; q++) st->h_pid[slot + q] = 0;
             }
         }
+        const size_t s0 = (size_t)cstart[cb + b], s1 = (size_t)cstart[cb + e];
+        evict_lines(st->h_xq + s0, sizeof(float4) * (s1 - s0));
+        if (st->has_excl) evict_lines(st->h_pid + s0, sizeof(int) * (s1 - s0));
     });
 }
 
@@ -482,12 +519,23 @@ DevView host_view(const NbState* st) {
 }
 
 // The launches of one evaluation: zero the accumulators, sort, (compact the queue,) sweep.
-int issue_kernels(NbState* st, const DevView& V) {
+// span: record ev0/ev1 around them (inside a captured graph as event nodes, so that they
+// time the device work and not the host's launch).
+int issue_kernels(NbState* st, const DevView& V, bool span = true) {
+    if (span) {
+        const int rc = record_event(st, st->ev0);
+        if (rc < 0) return rc;
+    }
     CU(cudaMemsetAsync(V.force, 0, sizeof(unsigned long long) * 3 * V.slots, st->stream));
     CU(cudaMemsetAsync(st->d_acc, 0, sizeof(unsigned long long) * kAccCount, st->stream));
     CU(cudaMemsetAsync(st->d_cell_epot, 0, sizeof(unsigned long long) * 2 * st->ncells, st->stream));
     const int cap = V.cap4;
-    if (cap == 0) return 0;
+    if (cap == 0) {                   // no particles: nothing to launch
+        int rc = record_event(st, st->evs0);
+        if (rc == 0) rc = record_event(st, st->evs1);
+        if (rc == 0 && span) rc = record_event(st, st->ev1);
+        return rc;
+    }
     sort_cells<<<(st->ncells + V.cpc - 1) / V.cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
         V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, st->d_acc, V.abort);
     CU(cudaGetLastError());
@@ -524,7 +572,9 @@ int issue_kernels(NbState* st, const DevView& V) {
     if (rc < 0) return rc;
     rc = st->plain ? launch_plain(st, P, cap) : launch_tuned(st, P, cap);
     if (rc < 0) return rc;
-    return record_event(st, st->evs1);
+    rc = record_event(st, st->evs1);
+    if (rc < 0 || !span) return rc;
+    return record_event(st, st->ev1);
 }
 
 int issue_kernels(NbState* st) { return issue_kernels(st, host_view(st)); }
@@ -929,6 +979,8 @@ void unpack_range(NbState* st, const float* hf, int cb, int ce, bool fresh) {
                     cl->parts[q].f[2] += f[3 * q + 2];
                 }
         }
+        const size_t s0 = (size_t)st->h_cstart[cb + b], s1 = (size_t)st->h_cstart[cb + e];
+        evict_lines(hf + 3 * s0, sizeof(float) * 3 * (s1 - s0));
     });
 }
 
@@ -993,11 +1045,7 @@ int st_resident(NbState* st) {
         return engine_err = engine_err_cuda;
     }
     CU(cudaSetDevice(st->device));
-    CU(cudaEventRecord(st->ev0, st->stream));
-    const int rc = launch_kernels(st);
-    if (rc < 0) return rc;
-    CU(cudaEventRecord(st->ev1, st->stream));
-    return 0;
+    return launch_kernels(st);
 }
 
 int st_nonbond(NbState* st, bool fresh = false) {
@@ -1121,7 +1169,10 @@ void res_free(NbState* st) {
     if (st->h_dense) cudaFreeHost(st->h_dense);
     if (st->h_dpid) cudaFreeHost(st->h_dpid);
     if (st->h_rcount) cudaFreeHost(st->h_rcount);
-    st->r_dpid = st->h_dpid = st->r_doff = st->h_rcount = nullptr;
+    if (st->h_up) cudaFreeHost(st->h_up);
+    if (st->h_uppid) cudaFreeHost(st->h_uppid);
+    st->r_dpid = st->h_dpid = st->h_uppid = st->r_doff = st->h_rcount = nullptr;
+    st->h_up = nullptr;
     st->r_xq[0] = st->r_xq[1] = nullptr;
     st->r_v[0] = st->r_v[1] = nullptr;
     st->r_pid[0] = st->r_pid[1] = nullptr;
@@ -1159,12 +1210,13 @@ __global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float
     }
 }
 
-// Every particle in cell order for the host copy (cell c from offset doff[c]): position
-// (w = type), velocity and the last evaluation's force, and its id.
+// Every particle in cell order for the host copy (cell c from offset doff[c]): positions
+// (w = type), velocities and the last evaluation's forces as three arrays of np entries,
+// and the ids.
 __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const float4* __restrict__ xq,
                                                      const float4* __restrict__ v, const int* __restrict__ pid,
                                                      const int* __restrict__ count, const int* __restrict__ doff,
-                                                     const unsigned long long* __restrict__ force,
+                                                     const unsigned long long* __restrict__ force, size_t np,
                                                      float4* __restrict__ dense, int* __restrict__ dpid) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -1173,9 +1225,9 @@ __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const flo
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) {
         const size_t s = base + k, o = (size_t)doff[c] + k;
-        dense[3 * o] = xq[s];
-        dense[3 * o + 1] = v[s];
-        dense[3 * o + 2] =
+        dense[o] = xq[s];
+        dense[np + o] = v[s];
+        dense[2 * np + o] =
             make_float4((float)((double)(long long)force[3 * s] * (1.0 / (double)kForceScale)),
                         (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale)),
                         (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale)), 0.f);
@@ -1195,44 +1247,42 @@ ResidentCells res_cells(const NbState* st) {
 
 int res_grid(const NbState* st) { return (st->ncells + 7) / 8; }      // 8 warps (cells) per block
 
-// Uploads the engines' particles into the device cells.  margin: spare slots per cell
-// beyond the largest (negative: an eighth of the largest cell plus 8); mcap: leavers per
-// cell and step.
-int st_resident_begin(NbState* st, int margin, int mcap) {
-    CU(cudaSetDevice(st->device));
-    CU(cudaStreamSynchronize(st->stream));
-    res_free(st);
-    const int nc = st->ncells, ne = (int)st->engines.size(), mt = st->max_type, nid = st->nid;
+// Largest cell of the engines' host cells and the particle count.
+int res_host_counts(const NbState* st, long long* n) {
     int maxc = 0;
-    long long n = 0;
-    std::vector<int> count(nc), doff(nc + 1, 0);
-    for (int c = 0; c < nc; c++) {
-        count[c] = st->flat_cells[c]->count;
-        maxc = std::max(maxc, count[c]);
-        doff[c + 1] = doff[c] + count[c];
+    long long tot = 0;
+    for (int c = 0; c < st->ncells; c++) {
+        maxc = std::max(maxc, st->flat_cells[c]->count);
+        tot += st->flat_cells[c]->count;
     }
-    n = doff[nc];
-    if (maxc > kMaxPartsPerCell) {
-        errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_maxparts;
-    }
-    if (margin < 0) margin = maxc / 8 + 8;
-    st->res_margin = std::max(margin, 4);
-    st->mcap = std::max(mcap, 16);
-    st->capc = std::min(kMaxPartsPerCell, (maxc + st->res_margin + 3) & ~3);
+    *n = tot;
+    return maxc;
+}
+
+// Device blocks of capc slots per cell for n particles, with the static cell data
+// (block offsets, periodic neighbours, edges, engine of each cell, dt and 1/m).
+int res_alloc(NbState* st, int capc, int mcap, long long n) {
+    const int nc = st->ncells, ne = (int)st->engines.size(), mt = st->max_type, nid = st->nid;
+    st->capc = capc;
+    st->mcap = mcap;
+    st->res_nparts = n;
     const size_t slots = (size_t)nc * st->capc;
     for (int q = 0; q < 2; q++) {
         CU(cudaMalloc(&st->r_xq[q], sizeof(float4) * slots));
         CU(cudaMalloc(&st->r_v[q], sizeof(float4) * slots));
         CU(cudaMalloc(&st->r_pid[q], sizeof(int) * slots));
+        // Slots past a cell's count hold zeros or an earlier occupant (finite, ids in range).
+        CU(cudaMemset(st->r_xq[q], 0, sizeof(float4) * slots));
+        CU(cudaMemset(st->r_v[q], 0, sizeof(float4) * slots));
+        CU(cudaMemset(st->r_pid[q], 0, sizeof(int) * slots));
     }
     CU(cudaMalloc(&st->r_keys, sizeof(unsigned) * 13 * slots));
     CU(cudaMalloc(&st->r_force, sizeof(unsigned long long) * 3 * slots));
+    CU(cudaMemset(st->r_force, 0, sizeof(unsigned long long) * 3 * slots));
     CU(cudaMalloc(&st->r_cnt[0], sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_cnt[1], sizeof(int) * (nc + 1)));
-    CU(cudaMalloc(&st->r_done, sizeof(unsigned long long)));
-    CU(cudaMemset(st->r_done, 0, sizeof(unsigned long long)));
     CU(cudaMemset(st->r_cnt[1], 0, sizeof(int) * (nc + 1)));
+    CU(cudaMalloc(&st->r_done, 2 * sizeof(unsigned long long)));
     CU(cudaMalloc(&st->r_cstart, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_nstay, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_nmove, sizeof(int) * (nc + 1)));
@@ -1248,18 +1298,11 @@ int st_resident_begin(NbState* st, int margin, int mcap) {
     CU(cudaMallocHost(&st->h_dense, sizeof(float4) * 3 * (size_t)(n + 1)));
     CU(cudaMalloc(&st->r_dpid, sizeof(int) * (size_t)(n + 1)));
     CU(cudaMallocHost(&st->h_dpid, sizeof(int) * (size_t)(n + 1)));
+    CU(cudaMallocHost(&st->h_up, sizeof(float4) * 2 * (size_t)(n + 1)));
+    CU(cudaMallocHost(&st->h_uppid, sizeof(int) * (size_t)(n + 1)));
     CU(cudaMalloc(&st->r_doff, sizeof(int) * (nc + 1)));
     CU(cudaMallocHost(&st->h_rcount, sizeof(int) * (2 * nc + 2)));
-    CU(cudaMemset(st->r_status, 0, sizeof(unsigned long long)));
-    CU(cudaMemset(st->r_force, 0, sizeof(unsigned long long) * 3 * slots));
-    // Slots past a cell's count hold zeros or an earlier occupant (finite positions, ids in range).
-    for (int q = 0; q < 2; q++) {
-        CU(cudaMemset(st->r_xq[q], 0, sizeof(float4) * slots));
-        CU(cudaMemset(st->r_v[q], 0, sizeof(float4) * slots));
-        CU(cudaMemset(st->r_pid[q], 0, sizeof(int) * slots));
-    }
 
-    // Static cell data: block offsets, neighbours (periodic), edges, engine of each cell.
     std::vector<int> cstart(nc + 1), nbr(27 * (size_t)nc), cell_engine(nc);
     std::vector<float4> cell_h(nc);
     std::vector<float> edt(ne);
@@ -1289,59 +1332,98 @@ int st_resident_begin(NbState* st, int margin, int mcap) {
     CU(cudaMemcpy(st->r_cell_h, cell_h.data(), sizeof(float4) * nc, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_dt, edt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_imass, imass.data(), sizeof(double) * imass.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_cnt[0], count.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
-
-    // Particles in cell order (dense), then into the cells' blocks on the device.
-    std::vector<float4> dxq(n + 1), dv(n + 1);
-    std::vector<int> dpid(n + 1);
     st->id_q.assign(nid, 0.f);
     st->id_vid.assign(nid, 0);
     st->id_flags.assign(nid, 0);
     st->id_present.assign(nid, 0);
+    st->res_active = true;
+    return 0;
+}
+
+// The engines' host cells into side 0 of the device blocks (the caller has checked that
+// every cell fits): positions, velocities and ids packed in cell order by the host threads,
+// one copy each, then placed into the blocks on the device.
+int res_upload(NbState* st) {
+    const int nc = st->ncells, ne = (int)st->engines.size();
+    int* cnt = st->h_rcount;
+    int* off = st->h_rcount + nc + 1;
+    off[0] = 0;
     for (int c = 0; c < nc; c++) {
-        const struct cell* cl = st->flat_cells[c];
-        const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
-        for (int q = 0; q < cl->count; q++) {
-            const struct part* p = &cl->parts[q];
-            const int gid = st->id_off[k] + p->id;
-            dxq[doff[c] + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
-            dv[doff[c] + q] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
-            dpid[doff[c] + q] = gid;
-            st->id_q[gid] = p->q;
-            st->id_vid[gid] = p->vid;
-            st->id_flags[gid] = p->flags;
-            st->id_present[gid] = 1;
-        }
+        cnt[c] = st->flat_cells[c]->count;
+        off[c + 1] = off[c] + cnt[c];
     }
-    float4 *t_xq = nullptr, *t_v = nullptr;
-    int *t_pid = nullptr, *t_off = nullptr;
-    CU(cudaMalloc(&t_xq, sizeof(float4) * (n + 1)));
-    CU(cudaMalloc(&t_v, sizeof(float4) * (n + 1)));
-    CU(cudaMalloc(&t_pid, sizeof(int) * (n + 1)));
-    CU(cudaMalloc(&t_off, sizeof(int) * (nc + 1)));
-    CU(cudaMemcpy(t_xq, dxq.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(t_v, dv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(t_pid, dpid.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(t_off, doff.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
+    const size_t np = (size_t)st->res_nparts;
+    float4* hx = st->h_up;
+    float4* hv = st->h_up + np;
+    const double t0 = now_ms();
+    HostPool::get().run(nc, cell_grain(st), [&](int, int cb, int ce) {
+        for (int c = cb; c < ce; c++) {
+            const struct cell* cl = st->flat_cells[c];
+            const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
+            for (int q = 0; q < cl->count; q++) {
+                const struct part* p = &cl->parts[q];
+                const int gid = st->id_off[k] + p->id;
+                const size_t o = (size_t)off[c] + q;
+                hx[o] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
+                hv[o] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
+                st->h_uppid[o] = gid;
+                st->id_q[gid] = p->q;
+                st->id_vid[gid] = p->vid;
+                st->id_flags[gid] = p->flags;
+                st->id_present[gid] = 1;
+            }
+        }
+        const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
+        evict_lines(hx + q0, sizeof(float4) * (q1 - q0));
+        evict_lines(hv + q0, sizeof(float4) * (q1 - q0));
+        evict_lines(st->h_uppid + q0, sizeof(int) * (q1 - q0));
+    });
+    st->bstats.ms_pack = (float)(now_ms() - t0);
+    st->res_engine_n.assign(ne, 0);
+    for (int k = 0; k < ne; k++) st->res_engine_n[k] = off[st->cell_off[k + 1]] - off[st->cell_off[k]];
+    CU(cudaMemcpyAsync(st->r_dense, st->h_up, sizeof(float4) * 2 * np, cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemcpyAsync(st->r_dpid, st->h_uppid, sizeof(int) * np, cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemcpyAsync(st->r_cnt[0], cnt, sizeof(int) * nc, cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
+    CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
+    CU(cudaMemsetAsync(st->r_done, 0, 2 * sizeof(unsigned long long), st->stream));
     const ResidentCells RC = res_cells(st);
-    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, t_xq, t_v, t_pid, t_off, st->r_cnt[0], st->r_xq[0],
-                                                      st->r_v[0], st->r_pid[0]);
+    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid, st->r_doff,
+                                                      st->r_cnt[0], st->r_xq[0], st->r_v[0], st->r_pid[0]);
     CU(cudaGetLastError());
     slot_of_ids<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_pid[0], st->r_cnt[0], st->r_slot_of, nullptr);
     CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(st->stream));
-    cudaFree(t_xq);
-    cudaFree(t_v);
-    cudaFree(t_pid);
-    cudaFree(t_off);
-    st->res_nparts = n;
-    st->res_done = st->res_done_total = 0;
-    st->res_regrows = 0;
-    st->res_engine_n.assign(ne, 0);
-    for (int k = 0; k < ne; k++)
-        for (int c = 0; c < st->engines[k]->s.nr_cells; c++) st->res_engine_n[k] += count[st->cell_off[k] + c];
+    st->res_done = st->res_pairs = 0;
     st->rside = 0;
-    st->res_active = true;
+    st->res_dirty = false;
+    return 0;
+}
+
+// Uploads the engines' particles into the device cells.  margin: spare slots per cell
+// beyond the largest (negative: 8; the sweep's shared-memory slices are sized by the block,
+// so a small margin keeps its occupancy, and an overflow re-blocks with twice the margin);
+// mcap: leavers per cell and step.
+int st_resident_begin(NbState* st, int margin, int mcap) {
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    long long n = 0;
+    const int maxc = res_host_counts(st, &n);
+    if (maxc > kMaxPartsPerCell) {
+        errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    if (margin < 0) margin = 8;
+    margin = std::max(margin, 4);
+    const int capc = std::min(kMaxPartsPerCell, (maxc + margin + 3) & ~3);
+    res_free(st);
+    int rc = res_alloc(st, capc, std::max(mcap, 16), n);
+    if (rc < 0) return rc;
+    st->res_margin = margin;
+    rc = res_upload(st);
+    if (rc < 0) return rc;
+    CU(cudaStreamSynchronize(st->stream));
+    st->res_done_total = st->res_pairs_total = 0;
+    st->res_regrows = 0;
     return 0;
 }
 
@@ -1349,6 +1431,8 @@ int st_resident_begin(NbState* st, int margin, int mcap) {
 // the integration, the rigid constraints.
 int res_issue_step(NbState* st) {
     const int r = st->rside, o = 1 - r;
+    int rc = record_event(st, st->ev0);
+    if (rc < 0) return rc;
     const ResidentCells RC = res_cells(st);
     const int grid = res_grid(st);
     rebin_split<<<grid, 256, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_cnt[r], st->r_xq[o],
@@ -1374,11 +1458,11 @@ int res_issue_step(NbState* st) {
     V.slots = (size_t)st->ncells * st->capc;
     V.cap4 = st->capc;
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
-    int rc = issue_kernels(st, V);
+    rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
     integrate_cells<<<grid, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
                                                   st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o],
-                                                  st->r_status, st->r_done);
+                                                  st->r_status, st->d_acc, st->r_done);
     CU(cudaGetLastError());
     for (size_t k = 0; k < st->engines.size(); k++) {
         struct engine* e = st->engines[k];
@@ -1394,7 +1478,7 @@ int res_issue_step(NbState* st) {
         rc = rigid_eval_resident(e, &view, st->stream);
         if (rc < 0) return rc;
     }
-    return 0;
+    return record_event(st, st->ev1);
 }
 
 // Everything a captured resident step depends on besides the device buffers' contents.
@@ -1469,21 +1553,22 @@ int st_resident_steps(NbState* st, int nsteps) {
         return engine_err = engine_err_cuda;
     }
     CU(cudaSetDevice(st->device));
-    CU(cudaEventRecord(st->ev0, st->stream));
     // A step that overflowed a cell block (or the leaver lists) was aborted with every step
     // after it: the device still holds the last completed step.  Re-block with twice the
     // room from there and run the remaining steps (at most 8 times per call).
     int left = nsteps, regrows = 0;
+    st->res_dirty = st->res_dirty || nsteps > 0;
     while (left > 0) {
         const int side0 = st->rside;
         int rc = res_issue_steps(st, left);
         if (rc < 0) return rc;
-        unsigned long long w[2] = {0, 0};
+        unsigned long long w[3] = {0, 0, 0};
         CU(cudaMemcpyAsync(&w[0], st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
-        CU(cudaMemcpyAsync(&w[1], st->r_done, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaMemcpyAsync(&w[1], st->r_done, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
         CU(cudaStreamSynchronize(st->stream));
         const long long completed = (long long)w[1] - st->res_done;
         st->res_done = (long long)w[1];
+        st->res_pairs = (long long)w[2];
         if (w[0] == 0) break;
         for (struct engine* e : st->engines) e->time -= (int)(left - completed);
         st->rside = side0 ^ (int)(completed & 1);
@@ -1497,13 +1582,14 @@ int st_resident_steps(NbState* st, int nsteps) {
         rc = st_resident_sync(st);
         if (rc < 0) return rc;
         const long long done = st->res_done_total + st->res_done;
+        const long long pairs = st->res_pairs_total + st->res_pairs;
         const int total_regrows = st->res_regrows + 1;
         rc = st_resident_begin(st, cells ? 2 * st->res_margin : st->res_margin, movers ? 2 * st->mcap : st->mcap);
         if (rc < 0) return rc;
         st->res_done_total = done;
+        st->res_pairs_total = pairs;
         st->res_regrows = total_regrows;
     }
-    CU(cudaEventRecord(st->ev1, st->stream));
     return 0;
 }
 
@@ -1536,11 +1622,11 @@ int st_resident_sync(NbState* st) {
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[st->rside], st->r_v[st->rside],
                                                         st->r_pid[st->rside], st->r_cnt[st->rside], st->r_doff,
-                                                        st->r_force,
+                                                        st->r_force, (size_t)st->res_nparts,
                                                         st->r_dense, st->r_dpid);
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
-                       st->stream));
+    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * (size_t)st->res_nparts,
+                       cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_dpid, st->r_dpid, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
@@ -1548,6 +1634,8 @@ int st_resident_sync(NbState* st) {
                        st->stream));
     CU(cudaStreamSynchronize(st->stream));
     // The host cells take the device's particles in the device's order.
+    const size_t np = (size_t)st->res_nparts;
+    const double t_rebuild = now_ms();
     std::atomic<int> fail(0);
     HostPool::get().run(nc, cell_grain(st), [&](int, int cb, int ce) {
         for (int c = cb; c < ce; c++) {
@@ -1557,8 +1645,7 @@ int st_resident_sync(NbState* st) {
             struct cell* cl = st->flat_cells[c];
             cl->count = 0;
             for (int q = off[c]; q < off[c + 1]; q++) {
-                const float4 x = st->h_dense[3 * (size_t)q], v = st->h_dense[3 * (size_t)q + 1];
-                const float4 f = st->h_dense[3 * (size_t)q + 2];
+                const float4 x = st->h_dense[q], v = st->h_dense[np + q], f = st->h_dense[2 * np + q];
                 const int gid = st->h_dpid[q];
                 int type;
                 std::memcpy(&type, &x.w, sizeof(int));
@@ -1579,7 +1666,11 @@ int st_resident_sync(NbState* st) {
             }
             space_relink(sp, cl);
         }
+        const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
+        for (int a = 0; a < 3; a++) evict_lines(st->h_dense + a * np + q0, sizeof(float4) * (q1 - q0));
+        evict_lines(st->h_dpid + q0, sizeof(int) * (q1 - q0));
     });
+    st->bstats.ms_unpack = (float)(now_ms() - t_rebuild);
     if (fail) {
         errs_register(engine_err_malloc, "Could not grow a host cell.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_malloc;
@@ -1590,6 +1681,7 @@ int st_resident_sync(NbState* st) {
         sp->epot = sp->epot_nonbond = sp->epot_bond = sp->epot_angle = sp->epot_dihedral = sp->epot_exclusion = 0.0;
         if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream);
     }
+    st->res_dirty = false;
     const int rc = finish_stats(st);
     for (struct engine* e : st->engines) e->s.epot += e->s.epot_nonbond;
     return rc;
@@ -1745,7 +1837,7 @@ extern "C" int engine_cuda_resident_sync(struct engine* e) {
     return st_resident_sync(state(e));
 }
 
-int st_resident_info(const NbState* st, int* capc, int* mcap, long long* steps, int* regrows) {
+int st_resident_info(const NbState* st, int* capc, int* mcap, long long* steps, long long* pairs, int* regrows) {
     if (!st->res_active) {
         errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
                       __func__, __FILE__);
@@ -1754,13 +1846,48 @@ int st_resident_info(const NbState* st, int* capc, int* mcap, long long* steps, 
     if (capc) *capc = st->capc;
     if (mcap) *mcap = st->mcap;
     if (steps) *steps = st->res_done_total + st->res_done;
+    if (pairs) *pairs = st->res_pairs_total + st->res_pairs;
     if (regrows) *regrows = st->res_regrows;
     return 0;
 }
 
-extern "C" int engine_cuda_resident_info(struct engine* e, int* capc, int* mcap, long long* steps, int* regrows) {
+// One engine_step of every engine on the device with the host cells as input and output:
+// the particles go up, one resident step runs (re-binning, sort, sweep, integration, rigid
+// constraints), the particles, forces, energies and statistics come back.  The device
+// blocks are kept between calls and re-made only when a cell has outgrown them.  If
+// resident steps left the device ahead of the host, the step continues from the device.
+int st_step_device(NbState* st) {
+    CU(cudaSetDevice(st->device));
+    const double t0 = now_ms();
+    st->bstats.ms_pack = st->bstats.ms_unpack = 0.f;
+    int rc = 0;
+    if (!(st->res_active && st->res_dirty)) {
+        long long n = 0;
+        const int maxc = res_host_counts(st, &n);
+        if (st->res_active && n == st->res_nparts && maxc + 4 <= st->capc) {
+            rc = res_upload(st);
+        } else {
+            rc = st_resident_begin(st, -1, st->res_active ? st->mcap : 16);
+        }
+        if (rc < 0) return rc;
+    }
+    rc = st_resident_steps(st, 1);
+    if (rc < 0) return rc;
+    rc = st_resident_sync(st);
+    st->bstats.ms_device = (float)(now_ms() - t0) - st->bstats.ms_pack - st->bstats.ms_unpack;
+    share_times(st);
+    return rc;
+}
+
+extern "C" int engine_cuda_step(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    return st_resident_info(state(e), capc, mcap, steps, regrows);
+    return st_step_device(state(e));
+}
+
+extern "C" int engine_cuda_resident_info(struct engine* e, int* capc, int* mcap, long long* steps, long long* pairs,
+                                         int* regrows) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    return st_resident_info(state(e), capc, mcap, steps, pairs, regrows);
 }
 
 extern "C" int engine_cuda_resident_end(struct engine* e) {
@@ -1861,6 +1988,11 @@ extern "C" int engine_batch_nonbond_fresh(struct engine_batch* b) {
 // Euler update (engine_step for each engine, with the forces computed together).
 extern "C" int engine_batch_step(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
+    return st_step_device(bstate(b));
+}
+
+extern "C" int engine_batch_step_host(struct engine_batch* b) {
+    if (b == nullptr) return engine_err_null;
     NbState* st = bstate(b);
     for (struct engine* e : st->engines) {
         e->time += 1;
@@ -1893,9 +2025,9 @@ extern "C" int engine_batch_resident_sync(struct engine_batch* b) {
 }
 
 extern "C" int engine_batch_resident_info(struct engine_batch* b, int* capc, int* mcap, long long* steps,
-                                          int* regrows) {
+                                          long long* pairs, int* regrows) {
     if (b == nullptr) return engine_err_null;
-    return st_resident_info(bstate(b), capc, mcap, steps, regrows);
+    return st_resident_info(bstate(b), capc, mcap, steps, pairs, regrows);
 }
 
 extern "C" int engine_batch_resident_end(struct engine_batch* b) {

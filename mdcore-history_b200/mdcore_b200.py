@@ -7,6 +7,7 @@ loudly when it cannot: there is no CPU fallback.
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import os
 from typing import Optional
@@ -90,6 +91,8 @@ def lib() -> C.CDLL:
         "engine_rigid_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_double]),
         "engine_start": (C.c_int, [vp, C.c_int, C.c_int]),
         "engine_step": (C.c_int, [vp]),
+        "engine_step_host": (C.c_int, [vp]),
+        "engine_batch_step_host": (C.c_int, [vp]),
         "engine_advance": (C.c_int, [vp]),
         "engine_finalize": (C.c_int, [vp]),
         "engine_cuda_setdevice": (C.c_int, [vp, C.c_int]),
@@ -146,8 +149,8 @@ def lib() -> C.CDLL:
         "engine_batch_resident_steps": (C.c_int, [vp, C.c_int]),
         "engine_batch_resident_sync": (C.c_int, [vp]),
         "engine_batch_resident_end": (C.c_int, [vp]),
-        "engine_cuda_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), ip]),
-        "engine_batch_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), ip]),
+        "engine_cuda_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), P(C.c_longlong), ip]),
+        "engine_batch_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), P(C.c_longlong), ip]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -276,7 +279,14 @@ class Engine:
         return self
 
     def step(self):
+        """engine_step: one time step on the device, host particles in and out."""
         _check(self.lib.engine_step(self.ptr), "engine_step")
+        return self
+
+    def step_host(self):
+        """engine_step_host: re-binning and integration on the host, forces and constraints
+        through host buffers."""
+        _check(self.lib.engine_step_host(self.ptr), "engine_step_host")
         return self
 
     # -- device-resident time steps --------------------------------------------------
@@ -300,11 +310,9 @@ class Engine:
         return self
 
     def resident_info(self):
-        """(slots per cell, leavers per cell and step, completed steps, re-blockings)."""
-        a, b, c, d = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
-        _check(self.lib.engine_cuda_resident_info(self.ptr, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
-               "engine_cuda_resident_info")
-        return a.value, b.value, c.value, d.value
+        """ResidentInfo(capc, mcap, steps, pairs, regrows): slots per cell, leavers per cell
+        and step, completed steps and their accepted pairs, re-blockings."""
+        return _resident_info(self.lib.engine_cuda_resident_info, self.ptr)
 
     def load_parts(self):
         _check(self.lib.engine_cuda_load_parts(self.ptr), "engine_cuda_load_parts")
@@ -480,6 +488,15 @@ def fp32_peak_tflops(device: int = 0) -> float:
     return v.value
 
 
+ResidentInfo = collections.namedtuple("ResidentInfo", "capc mcap steps pairs regrows")
+
+
+def _resident_info(fn, ptr):
+    a, b, c, d, g = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong(), C.c_int()
+    _check(fn(ptr, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(g)), fn.__name__)
+    return ResidentInfo(a.value, b.value, c.value, d.value, g.value)
+
+
 class Batch:
     """Many engines (replicas) evaluated together: one sort and one persistent sweep
     launch over all of them (engine_batch_*).  The engines need no device state of their
@@ -510,6 +527,10 @@ class Batch:
         _check(self.lib.engine_batch_step(self.ptr), "engine_batch_step")
         return self
 
+    def step_host(self):
+        _check(self.lib.engine_batch_step_host(self.ptr), "engine_batch_step_host")
+        return self
+
     def resident_begin(self, margin: int = -1):
         _check(self.lib.engine_batch_resident_begin(self.ptr, margin), "engine_batch_resident_begin")
         return self
@@ -527,10 +548,7 @@ class Batch:
         return self
 
     def resident_info(self):
-        a, b, c, d = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
-        _check(self.lib.engine_batch_resident_info(self.ptr, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
-               "engine_batch_resident_info")
-        return a.value, b.value, c.value, d.value
+        return _resident_info(self.lib.engine_batch_resident_info, self.ptr)
 
     def load_parts(self):
         _check(self.lib.engine_batch_load_parts(self.ptr), "engine_batch_load_parts")

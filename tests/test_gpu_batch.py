@@ -123,7 +123,7 @@ def test_batch_steps_equal_single_steps():
     for s in systems:
         e = M.Engine.from_system(s)
         for _ in range(5):
-            e.step()
+            e.step_host()
         single.append(e.unload())
         e.close()
     engines = engines_of(systems)

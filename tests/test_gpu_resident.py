@@ -28,12 +28,17 @@ def warm_argon(ncell=8, temperature=1200.0, seed=4):
     return sysm
 
 
-def host_run(sysm, nsteps, flags=M.engine_flag_cuda, layout=None):
+def host_run(sysm, nsteps, flags=M.engine_flag_cuda, layout=None, device_steps=False):
+    """nsteps of engine_step_host (re-binning and integration on the host), or of
+    engine_step (one device step per call, host particles in and out)."""
     e = M.Engine.from_system(sysm, flags=flags)
     if layout is not None:
         e.set_layout(layout)
     for _ in range(nsteps):
-        e.step()
+        if device_steps:
+            e.step()
+        else:
+            e.step_host()
     out = e.parts(), e.stats()
     rig = e.rigid_stats() if sysm.rigid is not None else None
     e.close()
@@ -63,6 +68,9 @@ def test_resident_steps_equal_engine_step(graph, layout):
     e.resident_begin()
     e.resident_steps(10).resident_steps(nsteps - 10).resident_sync()
     assert e.stats().status == 0
+    info = e.resident_info()
+    assert info.steps == nsteps and info.regrows == 0
+    assert info.pairs > nsteps * 0.9 * e.stats().pairs
     got = e.parts(), e.stats()
     # particles did cross cell faces
     e0 = M.Engine.from_system(sysm)
@@ -86,17 +94,40 @@ def test_resident_sync_without_steps_keeps_the_host_state():
 
 
 def test_host_steps_continue_after_resident_steps():
-    """resident_end hands the particles back: engine_step carries on from the device state."""
+    """resident_end hands the particles back: host and device steps carry on from the device
+    state."""
     sysm = warm_argon(6)
     ref, _ = host_run(sysm, 12)
     e = M.Engine.from_system(sysm)
     for _ in range(4):
-        e.step()
+        e.step_host()
     e.resident_begin().resident_steps(5).resident_end()
-    for _ in range(3):
+    e.step()
+    e.step_host()
+    e.step()
+    same_state(ref, (e.parts(), e.stats()))
+    e.close()
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["direct", "graph"])
+def test_engine_step_on_the_device_equals_host_steps(graph):
+    """engine_step (upload, one device step, download per call) against engine_step_host."""
+    sysm = warm_argon(7)
+    ref, _ = host_run(sysm, 15)
+    e = M.Engine.from_system(sysm)
+    e.graph(graph)
+    for _ in range(15):
         e.step()
     same_state(ref, (e.parts(), e.stats()))
     e.close()
+
+
+def test_engine_step_on_the_device_rigid_water():
+    sysm = W.with_rigid_water(W.water_spce(10), 300.0, seed=4)
+    ref, rig_ref = host_run(sysm, 24)
+    got, rig = host_run(sysm, 24, device_steps=True)
+    same_state(ref, got, forces=False)
+    assert got[1].epot == ref[1].epot and rig == rig_ref
 
 
 @pytest.mark.parametrize("flags", [M.engine_flag_cuda, M.engine_flag_cuda | M.engine_flag_shake],
@@ -137,6 +168,24 @@ def test_batch_resident_steps_equal_engine_step():
         e.close()
 
 
+def test_batch_step_on_the_device_equals_host_steps():
+    systems = W.argon_replicas(nrep=5, seed=9)
+    for k, s in enumerate(systems):
+        s.v = W.maxwell_velocities(s, 900.0, seed=k)
+    out = []
+    for device in (False, True):
+        engines = [M.Engine.from_system(s, start=False) for s in systems]
+        b = M.Batch(engines)
+        for _ in range(6):
+            b.step() if device else b.step_host()
+        out.append([(e.parts(), e.stats()) for e in engines])
+        b.close()
+        for e in engines:
+            e.close()
+    for ref, got in zip(*out):
+        same_state(ref, got)
+
+
 def crowding_system():
     """Eight particles of cell (0,0,0) heading into cell (1,0,0), which holds eight of its
     own: the second step's re-binning puts 16 into a block of 12 slots."""
@@ -164,8 +213,8 @@ def test_block_overflow_regrows_and_matches_engine_step():
     e.resident_begin(margin=0)
     assert e.resident_info()[0] == 12
     e.resident_steps(3).resident_sync()
-    capc, mcap, steps, regrows = e.resident_info()
-    assert regrows == 1 and steps == 3 and capc >= 16
+    info = e.resident_info()
+    assert info.regrows == 1 and info.steps == 3 and info.capc >= 16
     same_state(ref, (e.parts(), e.stats()))
     e.close()
 
@@ -188,7 +237,7 @@ def test_many_leavers_regrow_the_lists():
     e = M.Engine.from_system(sysm)
     e.graph(True)
     e.resident_begin().resident_steps(8).resident_sync()
-    capc, mcap, steps, regrows = e.resident_info()
-    assert mcap > 16 and regrows >= 1 and steps == 8
+    info = e.resident_info()
+    assert info.mcap > 16 and info.regrows >= 1 and info.steps == 8
     same_state(ref, (e.parts(), e.stats()))
     e.close()

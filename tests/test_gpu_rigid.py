@@ -4,8 +4,8 @@
                      constraint forces and refined mixing matrices, three evaluations.
   SHAKE              device == oracle bit for bit (both FP64); the reference's single
                      build (float multiplier) agrees to a float ulp in position.
-  steps              engine_step with rigid water keeps every constraint within the
-                     tolerance, no group fails to converge.
+  steps              engine_step (device) and engine_step_host with rigid water keep every
+                     constraint within the tolerance, no group fails to converge.
 """
 import dataclasses
 
@@ -73,13 +73,17 @@ def constraint_residuals(e, sysm):
     return np.abs((dx ** 2).sum(1) - d ** 2)
 
 
+@pytest.mark.parametrize("device_steps", [True, False], ids=["engine_step", "engine_step_host"])
 @pytest.mark.parametrize("flags", [M.engine_flag_cuda, M.engine_flag_cuda | M.engine_flag_shake],
                          ids=["pshake", "shake"])
-def test_rigid_water_steps_keep_constraints(flags):
+def test_rigid_water_steps_keep_constraints(flags, device_steps):
     sysm = W.with_rigid_water(W.water_spce(10), 300.0, seed=2)
     e = M.Engine.from_system(sysm, flags=flags)
     for _ in range(25):                      # crosses the 20 matrix-refinement steps
-        e.step()
+        if device_steps:
+            e.step()
+        else:
+            e.step_host()
         assert e.stats().status == 0
         itmax, bad = e.rigid_stats()
         assert bad == 0 and 0 < itmax < 100
