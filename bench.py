@@ -404,6 +404,7 @@ def ours(args, rank, world, local_rank):
         tgt.step()
     barrier()
     e2e_ms = 0.0
+    host = {"pack": 0.0, "device_and_copies": 0.0, "unpack": 0.0}
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -414,6 +415,10 @@ def ours(args, rank, world, local_rank):
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms += ev0.elapsed_time(ev1) / args.steps
+        hs = tgt.stats()
+        host["pack"] += hs.ms_pack / args.steps
+        host["device_and_copies"] += hs.ms_device / args.steps
+        host["unpack"] += hs.ms_unpack / args.steps
     barrier()
     host_ms = 0.0                       # the host-threaded step, for comparison
     for _ in range(args.steps):
@@ -463,6 +468,7 @@ def ours(args, rank, world, local_rank):
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
             "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
                     "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "host_ms": {k: round(v, 4) for k, v in host.items()},
                     "what": "engine_step (engine_batch_step for the replicas) with the host cells as input "
                             "and output every step"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

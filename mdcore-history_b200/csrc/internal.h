@@ -40,7 +40,9 @@ struct rigid_resident_view {
     const unsigned long long *abort;   /* nonzero: the step was aborted, launch nothing */
 };
 int rigid_eval_resident(struct engine *e, const struct rigid_resident_view *view, void *stream);
-int rigid_resident_stats(struct engine *e, void *stream);
+/* Copies the iteration statistics of the last resident step to the host copy (wait = 0:
+ * only enqueues the copy on `stream`). */
+int rigid_resident_stats(struct engine *e, void *stream, int wait);
 /* Launch stream of the engine's device state (NULL before engine_cuda_load). */
 void *nb_engine_stream(struct engine *e);
 

@@ -202,4 +202,68 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
     }
 }
 
+// Cell offsets of the compacted download: an exclusive scan of min(count, capc) over the
+// cells in three launches of kScanBlock-thread blocks (block sums, their scan, the scan).
+constexpr int kScanBlock = 1024;
+
+__device__ __forceinline__ int block_scan_int(int v, int& excl, int* warp_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        warp_tot[lane] = wi - w;
+        if (lane == 31) warp_tot[32] = wi;
+    }
+    __syncthreads();
+    excl = warp_tot[warp] + incl - v;
+    const int total = warp_tot[32];
+    __syncthreads();
+    return total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_counts_sums(const int* __restrict__ count, int n, int capc,
+                                                              int* __restrict__ bsum) {
+    __shared__ int warp_tot[33];
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    int excl;
+    const int total = block_scan_int(i < n ? min(count[i], capc) : 0, excl, warp_tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_counts_blocks(int* __restrict__ bsum, int nblocks) {
+    __shared__ int warp_tot[33];
+    int run = 0;
+    for (int base = 0; base < nblocks; base += kScanBlock) {
+        const int b = base + threadIdx.x;
+        const int v = b < nblocks ? bsum[b] : 0;
+        int excl;
+        const int total = block_scan_int(v, excl, warp_tot);
+        if (b < nblocks) bsum[b] = run + excl;
+        run += total;
+    }
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_counts_apply(const int* __restrict__ count, int n, int capc,
+                                                               const int* __restrict__ bsum, int* __restrict__ off) {
+    __shared__ int warp_tot[33];
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    const int v = i < n ? min(count[i], capc) : 0;
+    int excl;
+    block_scan_int(v, excl, warp_tot);
+    if (i < n) off[i] = bsum[blockIdx.x] + excl;
+}
+
 }  // namespace nb

@@ -142,6 +142,8 @@ struct NbState {
     float4* h_dense = nullptr;         // downloads (cached host memory)
     float4* h_up = nullptr;            // uploads: positions, velocities
     int *r_dpid = nullptr, *h_dpid = nullptr, *h_uppid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
+    int* r_bsum = nullptr;                   // block sums of the count scan
+    unsigned long long* h_words = nullptr;   // status, completed steps, their pairs (pinned)
     std::vector<long long> res_engine_n;   // particles of each engine on the device
     std::vector<float> id_q;
     std::vector<int> id_vid;
@@ -1170,6 +1172,10 @@ void res_free(NbState* st) {
     if (st->h_dpid) cudaFreeHost(st->h_dpid);
     if (st->h_rcount) cudaFreeHost(st->h_rcount);
     if (st->h_up) cudaFreeHost(st->h_up);
+    if (st->h_words) cudaFreeHost(st->h_words);
+    if (st->r_bsum) cudaFree(st->r_bsum);
+    st->h_words = nullptr;
+    st->r_bsum = nullptr;
     if (st->h_uppid) cudaFreeHost(st->h_uppid);
     st->r_dpid = st->h_dpid = st->h_uppid = st->r_doff = st->h_rcount = nullptr;
     st->h_up = nullptr;
@@ -1225,6 +1231,7 @@ __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const flo
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) {
         const size_t s = base + k, o = (size_t)doff[c] + k;
+        if (o >= np) break;            // counts of an aborted step: nothing past the buffers
         dense[o] = xq[s];
         dense[np + o] = v[s];
         dense[2 * np + o] =
@@ -1302,6 +1309,8 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMallocHost(&st->h_uppid, sizeof(int) * (size_t)(n + 1)));
     CU(cudaMalloc(&st->r_doff, sizeof(int) * (nc + 1)));
     CU(cudaMallocHost(&st->h_rcount, sizeof(int) * (2 * nc + 2)));
+    CU(cudaMalloc(&st->r_bsum, sizeof(int) * ((nc + kScanBlock - 1) / kScanBlock + 1)));
+    CU(cudaMallocHost(&st->h_words, 4 * sizeof(unsigned long long)));
 
     std::vector<int> cstart(nc + 1), nbr(27 * (size_t)nc), cell_engine(nc);
     std::vector<float4> cell_h(nc);
@@ -1593,22 +1602,44 @@ int st_resident_steps(NbState* st, int nsteps) {
     return 0;
 }
 
-// Brings the engines' host cells up to date: positions, velocities and the last
-// evaluation's forces of every particle, in the cells the device holds them in (by id
-// within a cell), energies and statistics of the last step.
-int st_resident_sync(NbState* st) {
-    if (!st->res_active) {
-        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
-                      __func__, __FILE__);
-        return engine_err = engine_err_cuda;
-    }
-    CU(cudaSetDevice(st->device));
-    const int nc = st->ncells, ne = (int)st->engines.size();
+// Enqueues the download of the current side: cell offsets scanned on the device, the
+// particles compacted in cell order, the counts, cell energies, counters, the status and
+// completed-step words and the constraint statistics.  Nothing waits.
+int res_download_enqueue(NbState* st) {
+    const int nc = st->ncells, side = st->rside;
+    const size_t np = (size_t)st->res_nparts;
     const ResidentCells RC = res_cells(st);
+    const int nb = (nc + kScanBlock - 1) / kScanBlock;
+    if (nc > 0) {
+        scan_counts_sums<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum);
+        scan_counts_blocks<<<1, kScanBlock, 0, st->stream>>>(st->r_bsum, nb);
+        scan_counts_apply<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum, st->r_doff);
+        compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side], st->r_pid[side],
+                                                            st->r_cnt[side], st->r_doff, st->r_force, np,
+                                                            st->r_dense, st->r_dpid);
+        CU(cudaGetLastError());
+    }
+    CU(cudaMemcpyAsync(st->h_rcount, st->r_cnt[side], sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * np, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_dpid, st->r_dpid, sizeof(int) * np, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
+                       cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
+                       st->stream));
+    CU(cudaMemcpyAsync(st->h_words, st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_words + 1, st->r_done, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       st->stream));
+    for (struct engine* e : st->engines)
+        if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream, 0);
+    return 0;
+}
+
+// After a completed download: the host cells take the device's particles in the device's
+// order (each particle's id, charge and flags from the upload), energies and statistics.
+int res_rebuild(NbState* st) {
+    const int nc = st->ncells, ne = (int)st->engines.size();
     int* cnt = st->h_rcount;                     // counts, then offsets
     int* off = st->h_rcount + nc + 1;
-    CU(cudaMemcpyAsync(cnt, st->r_cnt[st->rside], sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaStreamSynchronize(st->stream));
     // Every particle must still be in one of its engine's cells; else the host keeps its copy.
     off[0] = 0;
     for (int c = 0; c < nc; c++) off[c + 1] = off[c] + std::min(cnt[c], st->capc);
@@ -1618,22 +1649,6 @@ int st_resident_sync(NbState* st) {
                           __FILE__);
             return engine_err = engine_err_maxparts;
         }
-    const long long n = off[nc];
-    CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
-    compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[st->rside], st->r_v[st->rside],
-                                                        st->r_pid[st->rside], st->r_cnt[st->rside], st->r_doff,
-                                                        st->r_force, (size_t)st->res_nparts,
-                                                        st->r_dense, st->r_dpid);
-    CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * (size_t)st->res_nparts,
-                       cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_dpid, st->r_dpid, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
-                       cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
-                       st->stream));
-    CU(cudaStreamSynchronize(st->stream));
-    // The host cells take the device's particles in the device's order.
     const size_t np = (size_t)st->res_nparts;
     const double t_rebuild = now_ms();
     std::atomic<int> fail(0);
@@ -1676,15 +1691,29 @@ int st_resident_sync(NbState* st) {
         return engine_err = engine_err_malloc;
     }
     for (int k = 0; k < ne; k++) {
-        struct engine* e = st->engines[k];
-        struct space* sp = &e->s;
+        struct space* sp = &st->engines[k]->s;
         sp->epot = sp->epot_nonbond = sp->epot_bond = sp->epot_angle = sp->epot_dihedral = sp->epot_exclusion = 0.0;
-        if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream);
     }
     st->res_dirty = false;
     const int rc = finish_stats(st);
     for (struct engine* e : st->engines) e->s.epot += e->s.epot_nonbond;
     return rc;
+}
+
+// Brings the engines' host cells up to date: positions, velocities and the last
+// evaluation's forces of every particle, in the device's cell order, energies and
+// statistics of the last step.
+int st_resident_sync(NbState* st) {
+    if (!st->res_active) {
+        errs_register(engine_err_cuda, "No device-resident particles (engine_cuda_resident_begin).", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
+    CU(cudaSetDevice(st->device));
+    int rc = res_download_enqueue(st);
+    if (rc < 0) return rc;
+    CU(cudaStreamSynchronize(st->stream));
+    return res_rebuild(st);
 }
 
 }  // namespace
@@ -1853,27 +1882,54 @@ int st_resident_info(const NbState* st, int* capc, int* mcap, long long* steps, 
 
 // One engine_step of every engine on the device with the host cells as input and output:
 // the particles go up, one resident step runs (re-binning, sort, sweep, integration, rigid
-// constraints), the particles, forces, energies and statistics come back.  The device
-// blocks are kept between calls and re-made only when a cell has outgrown them.  If
+// constraints), the particles, forces, energies and statistics come back, with a single
+// host synchronisation.  The device blocks are kept between calls and re-made only when a
+// cell has outgrown them (before the step, or when the step itself overflowed and was
+// aborted: the host copy is then unchanged and the step runs again in larger blocks).  If
 // resident steps left the device ahead of the host, the step continues from the device.
 int st_step_device(NbState* st) {
     CU(cudaSetDevice(st->device));
     const double t0 = now_ms();
     st->bstats.ms_pack = st->bstats.ms_unpack = 0.f;
     int rc = 0;
-    if (!(st->res_active && st->res_dirty)) {
-        long long n = 0;
-        const int maxc = res_host_counts(st, &n);
-        if (st->res_active && n == st->res_nparts && maxc + 4 <= st->capc) {
-            rc = res_upload(st);
-        } else {
-            rc = st_resident_begin(st, -1, st->res_active ? st->mcap : 16);
-        }
+    if (st->res_active && st->res_dirty) {
+        rc = st_resident_sync(st);
         if (rc < 0) return rc;
     }
-    rc = st_resident_steps(st, 1);
-    if (rc < 0) return rc;
-    rc = st_resident_sync(st);
+    int margin = 8, mcap = st->res_active ? st->mcap : 16;
+    for (int attempt = 0;; attempt++) {
+        long long n = 0;
+        const int maxc = res_host_counts(st, &n);
+        if (st->res_active && n == st->res_nparts && maxc + 4 <= st->capc && st->mcap >= mcap) {
+            rc = res_upload(st);
+        } else {
+            rc = st_resident_begin(st, margin, mcap);
+        }
+        if (rc < 0) return rc;
+        rc = res_issue_steps(st, 1);
+        if (rc < 0) return rc;
+        rc = res_download_enqueue(st);
+        if (rc < 0) return rc;
+        CU(cudaStreamSynchronize(st->stream));
+        const unsigned long long status = st->h_words[0];
+        if (status == 0) {
+            st->res_done = (long long)st->h_words[1];
+            st->res_pairs = (long long)st->h_words[2];
+            break;
+        }
+        // Aborted on the device: the host cells still hold the step's input.
+        for (struct engine* e : st->engines) e->time -= 1;
+        const bool cells = (status & kStatusResidentOverflow) != 0;
+        if (attempt >= 8 || (cells && st->capc >= kMaxPartsPerCell)) {
+            errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded.", __LINE__, __func__,
+                          __FILE__);
+            return engine_err = engine_err_maxparts;
+        }
+        margin = cells ? 2 * std::max(st->res_margin, 8) : st->res_margin;
+        if (status & kStatusMoverOverflow) mcap = 2 * st->mcap;
+        res_free(st);
+    }
+    rc = res_rebuild(st);
     st->bstats.ms_device = (float)(now_ms() - t0) - st->bstats.ms_pack - st->bstats.ms_unpack;
     share_times(st);
     return rc;

@@ -608,11 +608,11 @@ extern "C" int rigid_eval_resident(struct engine* e, const struct rigid_resident
 }
 
 // Iteration statistics of the last resident step (device counters to the host copy).
-extern "C" int rigid_resident_stats(struct engine* e, void* stream_v) {
+extern "C" int rigid_resident_stats(struct engine* e, void* stream_v, int wait) {
     if (e == nullptr || e->cuda_rigid == nullptr) return 0;
     RigidDev* rd = static_cast<RigidDev*>(e->cuda_rigid);
     cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
     CU(cudaMemcpyAsync(rd->h_stat, rd->d_stat, sizeof(int) * 2, cudaMemcpyDeviceToHost, stream));
-    CU(cudaStreamSynchronize(stream));
+    if (wait) CU(cudaStreamSynchronize(stream));
     return 0;
 }

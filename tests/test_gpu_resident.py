@@ -241,3 +241,22 @@ def test_many_leavers_regrow_the_lists():
     assert info.mcap > 16 and info.regrows >= 1 and info.steps == 8
     same_state(ref, (e.parts(), e.stats()))
     e.close()
+
+
+def test_engine_step_retries_an_aborted_step():
+    """engine_step with more than 16 leavers per cell: the device step is aborted, the host
+    cells are untouched, the step runs again with longer leaver lists; same trajectory as
+    engine_step_host."""
+    rng = np.random.default_rng(11)
+    A, B = W.lj_AB(0.996, 0.3405)
+    g = np.stack(np.meshgrid(*[np.arange(3)] * 3, indexing="ij"), -1).reshape(-1, 3).astype(float)
+    sub = np.stack(np.meshgrid(*[[0.1, 0.4, 0.7]] * 3, indexing="ij"), -1).reshape(-1, 3)
+    x = (g[:, None, :] + sub[None, :, :]).reshape(-1, 3) + rng.uniform(0, 0.02, size=(27 * 27, 3))
+    v = np.tile([[120.0, 0.0, 0.0]], (len(x), 1))
+    sysm = W.System(name="drift", origin=np.zeros(3), dim=np.full(3, 3.0), L=np.full(3, 1.0), cutoff=1.0,
+                    masses=[39.948], charges=[0.0],
+                    pots=[W.PotSpec(W.KIND_LJ126, 0, 0, 0.25, 1.0, 1e-4, (A * 1e-6, B * 1e-6, 0.0, 0.0))],
+                    x=x, type=np.zeros(len(x), np.int32), excl=np.zeros((0, 2), np.int32), dt=0.005, v=v)
+    ref, _ = host_run(sysm, 8)
+    got, _ = host_run(sysm, 8, device_steps=True)
+    same_state(ref, got)
