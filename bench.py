@@ -449,9 +449,9 @@ def ours(args, rank, world, local_rank):
             for ln in open(prof):
                 if ln.startswith("dram_bytes_per_launch"):
                     traffic = int(ln.split()[1])
-        # kernels of one resident step: re-binning (2), id -> slot (rigid), sort, queue
-        # compaction (3, systems with empty cells), sweep, integration, constraints (rigid)
-        per_step = 2 + int(rigid) + 1 + 3 * int(compact) + 1 + 1 + int(rigid) * len(engines)
+        # kernels of one resident step: re-binning (2), sort, queue compaction (3, systems
+        # with empty cells), sweep, integration, constraints (rigid, one per engine)
+        per_step = 2 + 1 + 3 * int(compact) + 1 + 1 + int(rigid) * len(engines)
         line = {
             "metric": METRIC, "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

@@ -104,12 +104,13 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
 
 // Phase 2, one warp per destination cell: after its stayers, the arrivals from the
 // neighbours in direction order 0..26 (a particle that moved by d arrives from the
-// neighbour at -d), each neighbour's leavers in their order.
+// neighbour at -d), each neighbour's leavers in their order; with slot_of, the slot of
+// every particle id of the cell.
 __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Mover* __restrict__ movers,
                                                     const int* __restrict__ nstay, const int* __restrict__ nmove,
                                                     float4* __restrict__ xq_out, float4* __restrict__ v_out,
                                                     int* __restrict__ pid_out, int* __restrict__ count,
-                                                    unsigned long long* status) {
+                                                    unsigned long long* status, int* __restrict__ slot_of) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -144,7 +145,12 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
         }
     }
     if (__any_sync(FULL, over) && lane == 0) atomicOr(status, (unsigned long long)kStatusResidentOverflow);
-    if (lane == 0) count[c] = min(off, RC.capc);
+    const int n = min(off, RC.capc);
+    if (lane == 0) count[c] = n;
+    if (slot_of != nullptr) {          // rigid systems: the slot of every particle id in this cell
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) slot_of[pid_out[base + k]] = (int)(base + k);
+    }
 }
 
 // Slot of every particle id after re-binning (for the rigid constraints).

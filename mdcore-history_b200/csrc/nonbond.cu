@@ -1252,7 +1252,11 @@ ResidentCells res_cells(const NbState* st) {
     return RC;
 }
 
-int res_grid(const NbState* st) { return (st->ncells + 7) / 8; }      // 8 warps (cells) per block
+// Per-cell kernels of the resident steps: one warp per cell, two cells per block (small
+// blocks spread a few hundred cells over all 148 SMs).
+constexpr int kCellWarps = 2;
+constexpr int kCellThreads = 32 * kCellWarps;
+int res_grid(const NbState* st) { return (st->ncells + kCellWarps - 1) / kCellWarps; }
 
 // Largest cell of the engines' host cells and the particle count.
 int res_host_counts(const NbState* st, long long* n) {
@@ -1397,10 +1401,10 @@ int res_upload(NbState* st) {
     CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
     CU(cudaMemsetAsync(st->r_done, 0, 2 * sizeof(unsigned long long), st->stream));
     const ResidentCells RC = res_cells(st);
-    place_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid, st->r_doff,
+    place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid, st->r_doff,
                                                       st->r_cnt[0], st->r_xq[0], st->r_v[0], st->r_pid[0]);
     CU(cudaGetLastError());
-    slot_of_ids<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_pid[0], st->r_cnt[0], st->r_slot_of, nullptr);
+    slot_of_ids<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_pid[0], st->r_cnt[0], st->r_slot_of, nullptr);
     CU(cudaGetLastError());
     st->res_done = st->res_pairs = 0;
     st->rside = 0;
@@ -1444,18 +1448,15 @@ int res_issue_step(NbState* st) {
     if (rc < 0) return rc;
     const ResidentCells RC = res_cells(st);
     const int grid = res_grid(st);
-    rebin_split<<<grid, 256, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_cnt[r], st->r_xq[o],
+    rebin_split<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_cnt[r], st->r_xq[o],
                                               st->r_v[o], st->r_pid[o], st->r_nstay, st->r_nmove, st->r_movers,
                                               st->r_status);
-    rebin_gather<<<grid, 256, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
-                                               st->r_pid[o], st->r_cnt[o], st->r_status);
-    CU(cudaGetLastError());
     bool rigid = false;
     for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
-    if (rigid) {
-        slot_of_ids<<<grid, 256, 0, st->stream>>>(RC, st->r_pid[o], st->r_cnt[o], st->r_slot_of, st->r_status);
-        CU(cudaGetLastError());
-    }
+    rebin_gather<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
+                                               st->r_pid[o], st->r_cnt[o], st->r_status,
+                                               rigid ? st->r_slot_of : nullptr);
+    CU(cudaGetLastError());
     DevView V;
     V.xq = st->r_xq[o];
     V.pid = st->r_pid[o];
@@ -1469,7 +1470,7 @@ int res_issue_step(NbState* st) {
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
     rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
-    integrate_cells<<<grid, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
+    integrate_cells<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
                                                   st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o],
                                                   st->r_status, st->d_acc, st->r_done);
     CU(cudaGetLastError());
@@ -1614,7 +1615,7 @@ int res_download_enqueue(NbState* st) {
         scan_counts_sums<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum);
         scan_counts_blocks<<<1, kScanBlock, 0, st->stream>>>(st->r_bsum, nb);
         scan_counts_apply<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum, st->r_doff);
-        compact_cells<<<res_grid(st), 256, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side], st->r_pid[side],
+        compact_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side], st->r_pid[side],
                                                             st->r_cnt[side], st->r_doff, st->r_force, np,
                                                             st->r_dense, st->r_dpid);
         CU(cudaGetLastError());

@@ -270,6 +270,309 @@ __global__ void __launch_bounds__(128) rigid_pshake(RigidArgs A) {
     store_group<RES>(A, p0, np, xp, shifts);
 }
 
+// ---- small groups (water: 3 particles, 3 constraints): the same iterations with every
+// per-group array in registers.  Particle indices come from the constraint list at run
+// time; each access compares them against the unrolled positions, so no array is indexed
+// dynamically and none spills to local memory.  The arithmetic and its order are those of
+// the kernels above.
+
+template <int MP>
+__device__ __forceinline__ void reg_get3(const double (&a)[MP][3], int p, double o[3]) {
+    o[0] = a[0][0];
+    o[1] = a[0][1];
+    o[2] = a[0][2];
+#pragma unroll
+    for (int q = 1; q < MP; q++)
+        if (p == q) {
+            o[0] = a[q][0];
+            o[1] = a[q][1];
+            o[2] = a[q][2];
+        }
+}
+
+template <int MP>
+__device__ __forceinline__ double reg_get(const double (&a)[MP], int p) {
+    double o = a[0];
+#pragma unroll
+    for (int q = 1; q < MP; q++)
+        if (p == q) o = a[q];
+    return o;
+}
+
+template <int MP, bool RES>
+__device__ __forceinline__ void load_group_reg(const RigidArgs& A, int p0, int np, double (&xp)[MP][3],
+                                               double (&xo)[MP][3], double (&m)[MP], int (&shifts)[MP][3]) {
+    int loc0[3] = {0, 0, 0};
+    if (RES) slot_loc(A, A.slot_of[A.id0 + A.rpid[p0]], loc0);
+#pragma unroll
+    for (int k = 0; k < MP; k++) {
+        xp[k][0] = xp[k][1] = xp[k][2] = 0.0;
+        xo[k][0] = xo[k][1] = xo[k][2] = 0.0;
+        m[k] = 0.0;
+        shifts[k][0] = shifts[k][1] = shifts[k][2] = 0;
+        if (k >= np) continue;
+        float4 x, v;
+        int sh[3];
+        if (RES) {
+            const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
+            x = A.rxq[slot];
+            v = A.rv[slot];
+            int loc[3];
+            slot_loc(A, slot, loc);
+#pragma unroll
+            for (int j = 0; j < 3; j++) sh[j] = shift_dim(loc[j], loc0[j]);
+        } else {
+            x = A.x[p0 + k];
+            v = A.v[p0 + k];
+            const int code = __float_as_int(x.w);
+            sh[0] = code % 3 - 1;
+            sh[1] = (code / 3) % 3 - 1;
+            sh[2] = code / 9 - 1;
+        }
+        const double h[3] = {A.h0, A.h1, A.h2};
+        const float xv[3] = {x.x, x.y, x.z}, vv[3] = {v.x, v.y, v.z};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            shifts[k][j] = sh[j];
+            xp[k][j] = (double)xv[j] + h[j] * (double)sh[j];
+            xo[k][j] = xp[k][j] - A.dt * (double)vv[j];
+        }
+        m[k] = A.mass[p0 + k];
+    }
+}
+
+template <int MP, bool RES>
+__device__ __forceinline__ void store_group_reg(const RigidArgs& A, int p0, int np, const double (&xp)[MP][3],
+                                                const int (&shifts)[MP][3]) {
+    const double h[3] = {A.h0, A.h1, A.h2};
+    const double idt = 1.0 / A.dt;
+#pragma unroll
+    for (int k = 0; k < MP; k++) {
+        if (k >= np) continue;
+        if (!RES) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) A.xp[3 * (size_t)p0 + 3 * k + j] = xp[k][j];
+            continue;
+        }
+        const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
+        float4 x = A.rxq[slot], v = A.rv[slot];
+        float xs[3] = {x.x, x.y, x.z}, vs[3] = {v.x, v.y, v.z};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const double xn = xp[k][j] - h[j] * shifts[k][j];
+            vs[j] = (float)((double)vs[j] + idt * (xn - (double)xs[j]));
+            xs[j] = (float)xn;
+        }
+        A.rxq[slot] = make_float4(xs[0], xs[1], xs[2], x.w);
+        A.rv[slot] = make_float4(vs[0], vs[1], vs[2], v.w);
+    }
+}
+
+template <int MP, int MC, bool RES>
+__global__ void __launch_bounds__(64) rigid_shake_reg(RigidArgs A) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.nrig) return;
+    if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
+    const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
+    if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
+    double xp[MP][3], xo[MP][3], m[MP], vc[MC][3], wvc[MC][3], res[MC];
+    int shifts[MP][3], cx[MC], cy[MC];
+    load_group_reg<MP, RES>(A, p0, np, xp, xo, m, shifts);
+#pragma unroll
+    for (int k = 0; k < MC; k++) {
+        cx[k] = cy[k] = 0;
+        if (k >= nc) continue;
+        const int2 c = A.cij[c0 + k];
+        cx[k] = c.x;
+        cy[k] = c.y;
+        double a[3], b[3];
+        reg_get3<MP>(xo, c.x, a);
+        reg_get3<MP>(xo, c.y, b);
+        const double mx = reg_get<MP>(m, c.x), my = reg_get<MP>(m, c.y);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            vc[k][j] = a[j] - b[j];
+            wvc[k][j] = 1.0 / (mx + my) * vc[k][j];
+        }
+    }
+    int iter;
+    for (iter = 0; iter < rigid_maxiter; iter++) {
+        double max_res = 0.0;
+#pragma unroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) continue;
+            double a[3], b[3];
+            reg_get3<MP>(xp, cx[k], a);
+            reg_get3<MP>(xp, cy[k], b);
+            res[k] = A.d2[c0 + k];
+#pragma unroll
+            for (int j = 0; j < 3; j++) res[k] -= (a[j] - b[j]) * (a[j] - b[j]);
+            if (fabs(res[k]) > max_res) max_res = fabs(res[k]);
+        }
+        if (max_res < A.tol) break;
+#pragma unroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) continue;
+            double a[3], b[3];
+            reg_get3<MP>(xp, cx[k], a);
+            reg_get3<MP>(xp, cy[k], b);
+            const double lambda =
+                0.5 * res[k] / ((a[0] - b[0]) * vc[k][0] + (a[1] - b[1]) * vc[k][1] + (a[2] - b[2]) * vc[k][2]);
+            const double mx = reg_get<MP>(m, cx[k]), my = reg_get<MP>(m, cy[k]);
+#pragma unroll
+            for (int q = 0; q < MP; q++) {
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    const double w = lambda * wvc[k][j];
+                    if (q == cx[k]) xp[q][j] += w * my;
+                    if (q == cy[k]) xp[q][j] -= w * mx;
+                }
+            }
+        }
+    }
+    atomicMax(&A.stat[0], iter);
+    if (iter == rigid_maxiter) atomicAdd(&A.stat[1], 1);
+    store_group_reg<MP, RES>(A, p0, np, xp, shifts);
+}
+
+template <int MP, int MC, bool RES>
+__global__ void __launch_bounds__(64) rigid_pshake_reg(RigidArgs A) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.nrig) return;
+    if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
+    const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
+    if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
+    float* a = A.a + A.aoff[r];
+    double xp[MP][3], xo[MP][3], m[MP], vc[MC][MP][3];
+    int shifts[MP][3], cx[MC], cy[MC];
+    load_group_reg<MP, RES>(A, p0, np, xp, xo, m, shifts);
+#pragma unroll
+    for (int i = 0; i < MC; i++)
+#pragma unroll
+        for (int q = 0; q < MP; q++) vc[i][q][0] = vc[i][q][1] = vc[i][q][2] = 0.0;
+#pragma unroll
+    for (int k = 0; k < MC; k++) {
+        cx[k] = cy[k] = 0;
+        if (k >= nc) continue;
+        const int2 c = A.cij[c0 + k];
+        cx[k] = c.x;
+        cy[k] = c.y;
+        double ox[3], oy[3], dv[3];
+        reg_get3<MP>(xo, c.x, ox);
+        reg_get3<MP>(xo, c.y, oy);
+        const double mx = reg_get<MP>(m, c.x), my = reg_get<MP>(m, c.y);
+#pragma unroll
+        for (int j = 0; j < 3; j++) dv[j] = (ox[j] - oy[j]) / (mx + my);
+#pragma unroll
+        for (int i = 0; i < MC; i++) {
+            if (i >= nc) continue;
+            const float aki = a[k * nc + i];
+            if (aki != 0.0f)
+#pragma unroll
+                for (int q = 0; q < MP; q++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        if (q == c.x) vc[i][q][j] += aki * dv[j] * my;
+                        if (q == c.y) vc[i][q][j] += -aki * dv[j] * mx;
+                    }
+        }
+    }
+    int iter;
+    for (iter = 0; iter < rigid_maxiter; iter++) {
+        double max_res = 0.0;
+#pragma unroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) continue;
+            double a1[3], b1[3], va[3], vb[3];
+            reg_get3<MP>(xp, cx[k], a1);
+            reg_get3<MP>(xp, cy[k], b1);
+            reg_get3<MP>(vc[k], cx[k], va);
+            reg_get3<MP>(vc[k], cy[k], vb);
+            double res = A.d2[c0 + k];
+#pragma unroll
+            for (int j = 0; j < 3; j++) res -= (a1[j] - b1[j]) * (a1[j] - b1[j]);
+            if (fabs(res) > max_res) max_res = fabs(res);
+            const double lambda = 0.5 * res /
+                                  ((a1[0] - b1[0]) * (va[0] - vb[0]) + (a1[1] - b1[1]) * (va[1] - vb[1]) +
+                                   (a1[2] - b1[2]) * (va[2] - vb[2]));
+#pragma unroll
+            for (int q = 0; q < MP; q++)
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    if (q < np) xp[q][j] += lambda * vc[k][q][j];
+        }
+        if (max_res < A.tol) break;
+    }
+    atomicMax(&A.stat[0], iter);
+    if (iter == rigid_maxiter) atomicAdd(&A.stat[1], 1);
+
+    // Matrix refinement, src/rigid.c:433-474.
+    if (nc > 1 && (A.a_update || iter > rigid_pshake_refine)) {
+        float a_new[MC][MC], tmp[MC][MC];
+        float max_alpha = 0.0f;
+#pragma unroll
+        for (int i = 0; i < MC; i++) {
+            if (i >= nc) continue;
+            double pa[3], pb[3], va[3], vb[3];
+            reg_get3<MP>(xp, cx[i], pa);
+            reg_get3<MP>(xp, cy[i], pb);
+            float dx[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) dx[j] = (float)(pa[j] - pb[j]);
+            reg_get3<MP>(vc[i], cx[i], va);
+            reg_get3<MP>(vc[i], cy[i], vb);
+            const float w = (float)(-1.0 / ((double)dx[0] * (va[0] - vb[0]) + (double)dx[1] * (va[1] - vb[1]) +
+                                            (double)dx[2] * (va[2] - vb[2])));
+#pragma unroll
+            for (int j = 0; j < MC; j++) {
+                if (j <= i || j >= nc) continue;
+                double ja[3], jb[3];
+                reg_get3<MP>(vc[j], cx[i], ja);
+                reg_get3<MP>(vc[j], cy[i], jb);
+                a_new[j][i] = (float)((double)w * ((double)dx[0] * (ja[0] - jb[0]) + (double)dx[1] * (ja[1] - jb[1]) +
+                                                   (double)dx[2] * (ja[2] - jb[2])));
+                a_new[i][j] = a_new[j][i];
+                max_alpha = fmaxf(max_alpha, fabsf(a_new[j][i]));
+            }
+            a_new[i][i] = 1.0f;
+        }
+        if (max_alpha > rigid_pshake_maxalpha) {
+            const float w = (float)(0.1 / (double)max_alpha);
+#pragma unroll
+            for (int i = 0; i < MC; i++)
+#pragma unroll
+                for (int j = 0; j < MC; j++)
+                    if (i < nc && j < nc) a_new[i][j] *= w;
+#pragma unroll
+            for (int i = 0; i < MC; i++)
+                if (i < nc) a_new[i][i] = 1.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < MC; j++)
+#pragma unroll
+            for (int i = 0; i < MC; i++) tmp[j][i] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < MC; j++) {
+            if (j >= nc) continue;
+#pragma unroll
+            for (int k = 0; k < MC; k++) {
+                if (k >= nc) continue;
+#pragma unroll
+                for (int i = 0; i < MC; i++)
+                    if (i < nc) tmp[j][i] += a[k * nc + i] * a_new[j][k];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MC; j++)
+#pragma unroll
+            for (int i = 0; i < MC; i++)
+                if (j < nc && i < nc) a[j * nc + i] = tmp[j][i];
+    }
+    store_group_reg<MP, RES>(A, p0, np, xp, shifts);
+}
+
 struct RigidDev {
     int device = 0;
     int gen = -1, nrig = 0, nslots = 0, ncon = 0, namat = 0, maxp = 0, maxc = 0;
@@ -389,19 +692,28 @@ float bits_float(int v) {
 
 template <int MP, int MC, bool RES>
 void launch(bool pshake, const RigidArgs& A, cudaStream_t s) {
-    const int grid = (A.nrig + 127) / 128;
+    const int grid = (A.nrig + 63) / 64;     // 64 groups per block: every SM gets work
     if (pshake)
-        rigid_pshake<MP, MC, RES><<<grid, 128, 0, s>>>(A);
+        rigid_pshake<MP, MC, RES><<<grid, 64, 0, s>>>(A);
     else
-        rigid_shake<MP, MC, RES><<<grid, 128, 0, s>>>(A);
+        rigid_shake<MP, MC, RES><<<grid, 64, 0, s>>>(A);
+}
+
+template <int MP, int MC, bool RES>
+void launch_reg(bool pshake, const RigidArgs& A, cudaStream_t s) {
+    const int grid = (A.nrig + 63) / 64;
+    if (pshake)
+        rigid_pshake_reg<MP, MC, RES><<<grid, 64, 0, s>>>(A);
+    else
+        rigid_shake_reg<MP, MC, RES><<<grid, 64, 0, s>>>(A);
 }
 
 template <bool RES>
 void launch_sized(const RigidDev* rd, bool pshake, const RigidArgs& A, cudaStream_t s) {
     if (rd->maxp <= 3 && rd->maxc <= 3)
-        launch<3, 3, RES>(pshake, A, s);
+        launch_reg<3, 3, RES>(pshake, A, s);
     else if (rd->maxp <= 4 && rd->maxc <= 6)
-        launch<4, 6, RES>(pshake, A, s);
+        launch_reg<4, 6, RES>(pshake, A, s);
     else
         launch<rigid_maxparts, rigid_maxconstr, RES>(pshake, A, s);
 }
