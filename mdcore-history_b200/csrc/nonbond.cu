@@ -1353,6 +1353,11 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     return 0;
 }
 
+// Pipeline chunks of a transfer of np particles: one per 256k particles, 1 to 8 (every
+// chunk costs a wake-up of the host threads, ~0.1 ms here, more than the copy it hides
+// for smaller chunks).
+int res_chunks(size_t np) { return (int)std::max<size_t>(1, std::min<size_t>(8, np / 262144)); }
+
 // The engines' host cells into side 0 of the device blocks (the caller has checked that
 // every cell fits): positions, velocities and ids packed in cell order by the host threads,
 // one copy each, then placed into the blocks on the device.
@@ -1369,7 +1374,17 @@ int res_upload(NbState* st) {
     float4* hx = st->h_up;
     float4* hv = st->h_up + np;
     const double t0 = now_ms();
-    HostPool::get().run(nc, cell_grain(st), [&](int, int cb, int ce) {
+    // Chunks of cells with about equal particle counts: each chunk's copies overlap the
+    // packing of the next.
+    const int K = res_chunks(np);
+    std::vector<int> bounds(K + 1, nc);
+    bounds[0] = 0;
+    for (int k = 1; k < K; k++)
+        bounds[k] = (int)(std::lower_bound(off, off + nc + 1, (int)(np * k / K)) - off);
+    for (int k = 0; k < K; k++) {
+    const int c0 = bounds[k], c1 = bounds[k + 1];
+    HostPool::get().run(c1 - c0, cell_grain(st), [&](int, int rb, int re) {
+        const int cb = c0 + rb, ce = c0 + re;
         for (int c = cb; c < ce; c++) {
             const struct cell* cl = st->flat_cells[c];
             const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
@@ -1391,11 +1406,19 @@ int res_upload(NbState* st) {
         evict_lines(hv + q0, sizeof(float4) * (q1 - q0));
         evict_lines(st->h_uppid + q0, sizeof(int) * (q1 - q0));
     });
+    const size_t q0 = (size_t)off[c0], q1 = (size_t)off[c1];
+    if (q1 > q0) {
+        CU(cudaMemcpyAsync(st->r_dense + q0, hx + q0, sizeof(float4) * (q1 - q0), cudaMemcpyHostToDevice,
+                           st->stream));
+        CU(cudaMemcpyAsync(st->r_dense + np + q0, hv + q0, sizeof(float4) * (q1 - q0), cudaMemcpyHostToDevice,
+                           st->stream));
+        CU(cudaMemcpyAsync(st->r_dpid + q0, st->h_uppid + q0, sizeof(int) * (q1 - q0), cudaMemcpyHostToDevice,
+                           st->stream));
+    }
+    }
     st->bstats.ms_pack = (float)(now_ms() - t0);
     st->res_engine_n.assign(ne, 0);
     for (int k = 0; k < ne; k++) st->res_engine_n[k] = off[st->cell_off[k + 1]] - off[st->cell_off[k]];
-    CU(cudaMemcpyAsync(st->r_dense, st->h_up, sizeof(float4) * 2 * np, cudaMemcpyHostToDevice, st->stream));
-    CU(cudaMemcpyAsync(st->r_dpid, st->h_uppid, sizeof(int) * np, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->r_cnt[0], cnt, sizeof(int) * nc, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
@@ -1589,6 +1612,8 @@ int st_resident_steps(NbState* st, int nsteps) {
                           __LINE__, __func__, __FILE__);
             return engine_err = engine_err_maxparts;
         }
+        // the abort word has served: the side it protected is the one to bring back
+        CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
         rc = st_resident_sync(st);
         if (rc < 0) return rc;
         const long long done = st->res_done_total + st->res_done;
@@ -1603,42 +1628,56 @@ int st_resident_steps(NbState* st, int nsteps) {
     return 0;
 }
 
-// Enqueues the download of the current side: cell offsets scanned on the device, the
-// particles compacted in cell order, the counts, cell energies, counters, the status and
-// completed-step words and the constraint statistics.  Nothing waits.
-int res_download_enqueue(NbState* st) {
-    const int nc = st->ncells, side = st->rside;
+// Downloads the current side into the host cells.  On the device: cell offsets by a scan
+// of the counts, the particles compacted in cell order.  Down: the status and completed-
+// step words and the counts first, then the particles in chunks, each chunk's cells rebuilt
+// on the host threads while the next one copies, then energies, counters and constraint
+// statistics.  *status receives the abort word; when it is set nothing is rebuilt (the
+// host cells keep what they held).
+int res_download(NbState* st, unsigned long long* status) {
+    const int nc = st->ncells, ne = (int)st->engines.size(), side = st->rside;
     const size_t np = (size_t)st->res_nparts;
     const ResidentCells RC = res_cells(st);
     const int nb = (nc + kScanBlock - 1) / kScanBlock;
+    const int K = res_chunks(np);
+    int rc = chunk_events(st, K + 1);
+    if (rc < 0) return rc;
     if (nc > 0) {
         scan_counts_sums<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum);
         scan_counts_blocks<<<1, kScanBlock, 0, st->stream>>>(st->r_bsum, nb);
         scan_counts_apply<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum, st->r_doff);
-        compact_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side], st->r_pid[side],
-                                                            st->r_cnt[side], st->r_doff, st->r_force, np,
-                                                            st->r_dense, st->r_dpid);
+        compact_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side],
+                                                                     st->r_pid[side], st->r_cnt[side], st->r_doff,
+                                                                     st->r_force, np, st->r_dense, st->r_dpid);
         CU(cudaGetLastError());
     }
+    CU(cudaMemcpyAsync(st->h_words, st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaMemcpyAsync(st->h_words + 1, st->r_done, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       st->stream));
     CU(cudaMemcpyAsync(st->h_rcount, st->r_cnt[side], sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_dense, st->r_dense, sizeof(float4) * 3 * np, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_dpid, st->r_dpid, sizeof(int) * np, cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaEventRecord(st->chunk_ev[0], st->stream));
+    for (int k = 0; k < K; k++) {
+        const size_t q0 = np * k / K, q1 = np * (k + 1) / K;
+        for (int a = 0; a < 3; a++)
+            CU(cudaMemcpyAsync(st->h_dense + a * np + q0, st->r_dense + a * np + q0, sizeof(float4) * (q1 - q0),
+                               cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaMemcpyAsync(st->h_dpid + q0, st->r_dpid + q0, sizeof(int) * (q1 - q0), cudaMemcpyDeviceToHost,
+                           st->stream));
+        CU(cudaEventRecord(st->chunk_ev[k + 1], st->stream));
+    }
     CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
-    CU(cudaMemcpyAsync(st->h_words, st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaMemcpyAsync(st->h_words + 1, st->r_done, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                       st->stream));
     for (struct engine* e : st->engines)
         if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream, 0);
-    return 0;
-}
 
-// After a completed download: the host cells take the device's particles in the device's
-// order (each particle's id, charge and flags from the upload), energies and statistics.
-int res_rebuild(NbState* st) {
-    const int nc = st->ncells, ne = (int)st->engines.size();
+    CU(cudaEventSynchronize(st->chunk_ev[0]));
+    *status = st->h_words[0];
+    if (*status != 0) {
+        CU(cudaStreamSynchronize(st->stream));
+        return 0;
+    }
     int* cnt = st->h_rcount;                     // counts, then offsets
     int* off = st->h_rcount + nc + 1;
     // Every particle must still be in one of its engine's cells; else the host keeps its copy.
@@ -1646,47 +1685,71 @@ int res_rebuild(NbState* st) {
     for (int c = 0; c < nc; c++) off[c + 1] = off[c] + std::min(cnt[c], st->capc);
     for (int k = 0; k < ne; k++)
         if (off[st->cell_off[k + 1]] - off[st->cell_off[k]] != st->res_engine_n[k]) {
+            CU(cudaStreamSynchronize(st->stream));
             errs_register(engine_err_maxparts, "Particles missing from the device cells.", __LINE__, __func__,
                           __FILE__);
             return engine_err = engine_err_maxparts;
         }
-    const size_t np = (size_t)st->res_nparts;
-    const double t_rebuild = now_ms();
+    // The host cells take the device's particles in the device's order (id, charge and
+    // flags of each particle from the upload).
     std::atomic<int> fail(0);
-    HostPool::get().run(nc, cell_grain(st), [&](int, int cb, int ce) {
-        for (int c = cb; c < ce; c++) {
-            const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
-            const int lo = st->id_off[k];
-            struct space* sp = &st->engines[k]->s;
-            struct cell* cl = st->flat_cells[c];
-            cl->count = 0;
-            for (int q = off[c]; q < off[c + 1]; q++) {
-                const float4 x = st->h_dense[q], v = st->h_dense[np + q], f = st->h_dense[2 * np + q];
-                const int gid = st->h_dpid[q];
-                int type;
-                std::memcpy(&type, &x.w, sizeof(int));
-                struct part p;
-                std::memset(&p, 0, sizeof(p));
-                p.x[0] = x.x; p.x[1] = x.y; p.x[2] = x.z;
-                p.v[0] = v.x; p.v[1] = v.y; p.v[2] = v.z;
-                p.f[0] = f.x; p.f[1] = f.y; p.f[2] = f.z;
-                p.q = st->id_q[gid];
-                p.id = gid - lo;
-                p.vid = st->id_vid[gid];
-                p.type = (short)type;
-                p.flags = st->id_flags[gid];
-                if (cell_add(cl, &p) == nullptr) {
-                    fail = 1;
-                    return;
+    double t_rebuild = 0.0;
+    int cdone = 0;
+    for (int k = 0; k < K; k++) {
+        const int pend = (int)(np * (k + 1) / K);
+        const int cend = k == K - 1 ? nc : (int)(std::upper_bound(off + 1, off + nc + 1, pend) - (off + 1));
+        CU(cudaEventSynchronize(st->chunk_ev[k + 1]));
+        const double t0 = now_ms();
+        const int c0 = cdone;
+        HostPool::get().run(cend - c0, cell_grain(st), [&](int, int rb, int re) {
+            const int cb = c0 + rb, ce = c0 + re;
+            for (int c = cb; c < ce; c++) {
+                const size_t ke =
+                    std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
+                const int lo = st->id_off[ke];
+                struct space* sp = &st->engines[ke]->s;
+                struct cell* cl = st->flat_cells[c];
+                const int n = off[c + 1] - off[c];
+                if (n > cl->size) {             // the old contents are replaced, not copied
+                    const int nsize = std::max(n, std::max(2 * cl->size, 16));
+                    struct part* fresh = nullptr;
+                    if (posix_memalign(reinterpret_cast<void**>(&fresh), 64, sizeof(struct part) * nsize) != 0) {
+                        fail = 1;
+                        return;
+                    }
+                    free(cl->parts);
+                    cl->parts = fresh;
+                    cl->size = nsize;
                 }
+                for (int q = 0; q < n; q++) {
+                    const size_t o = (size_t)off[c] + q;
+                    const float4 x = st->h_dense[o], v = st->h_dense[np + o], f = st->h_dense[2 * np + o];
+                    const int gid = st->h_dpid[o];
+                    struct part* p = &cl->parts[q];
+                    int type;
+                    std::memcpy(&type, &x.w, sizeof(int));
+                    p->x[0] = x.x; p->x[1] = x.y; p->x[2] = x.z; p->x[3] = 0.f;
+                    p->v[0] = v.x; p->v[1] = v.y; p->v[2] = v.z; p->v[3] = 0.f;
+                    p->f[0] = f.x; p->f[1] = f.y; p->f[2] = f.z; p->f[3] = 0.f;
+                    p->q = st->id_q[gid];
+                    p->id = gid - lo;
+                    p->vid = st->id_vid[gid];
+                    p->type = (short)type;
+                    p->flags = st->id_flags[gid];
+                    sp->partlist[p->id] = p;      // space_relink, inline
+                    sp->celllist[p->id] = cl;
+                }
+                cl->count = n;
             }
-            space_relink(sp, cl);
-        }
-        const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
-        for (int a = 0; a < 3; a++) evict_lines(st->h_dense + a * np + q0, sizeof(float4) * (q1 - q0));
-        evict_lines(st->h_dpid + q0, sizeof(int) * (q1 - q0));
-    });
-    st->bstats.ms_unpack = (float)(now_ms() - t_rebuild);
+            const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
+            for (int a = 0; a < 3; a++) evict_lines(st->h_dense + a * np + q0, sizeof(float4) * (q1 - q0));
+            evict_lines(st->h_dpid + q0, sizeof(int) * (q1 - q0));
+        });
+        t_rebuild += now_ms() - t0;
+        cdone = cend;
+    }
+    st->bstats.ms_unpack = (float)t_rebuild;
+    CU(cudaStreamSynchronize(st->stream));
     if (fail) {
         errs_register(engine_err_malloc, "Could not grow a host cell.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_malloc;
@@ -1696,7 +1759,7 @@ int res_rebuild(NbState* st) {
         sp->epot = sp->epot_nonbond = sp->epot_bond = sp->epot_angle = sp->epot_dihedral = sp->epot_exclusion = 0.0;
     }
     st->res_dirty = false;
-    const int rc = finish_stats(st);
+    rc = finish_stats(st);
     for (struct engine* e : st->engines) e->s.epot += e->s.epot_nonbond;
     return rc;
 }
@@ -1711,10 +1774,15 @@ int st_resident_sync(NbState* st) {
         return engine_err = engine_err_cuda;
     }
     CU(cudaSetDevice(st->device));
-    int rc = res_download_enqueue(st);
+    unsigned long long status = 0;
+    const int rc = res_download(st, &status);
     if (rc < 0) return rc;
-    CU(cudaStreamSynchronize(st->stream));
-    return res_rebuild(st);
+    if (status != 0) {
+        errs_register(engine_err_maxparts, "Device cell capacity exceeded during resident steps.", __LINE__,
+                      __func__, __FILE__);
+        return engine_err = engine_err_maxparts;
+    }
+    return 0;
 }
 
 }  // namespace
@@ -1909,10 +1977,9 @@ int st_step_device(NbState* st) {
         if (rc < 0) return rc;
         rc = res_issue_steps(st, 1);
         if (rc < 0) return rc;
-        rc = res_download_enqueue(st);
+        unsigned long long status = 0;
+        rc = res_download(st, &status);
         if (rc < 0) return rc;
-        CU(cudaStreamSynchronize(st->stream));
-        const unsigned long long status = st->h_words[0];
         if (status == 0) {
             st->res_done = (long long)st->h_words[1];
             st->res_pairs = (long long)st->h_words[2];
@@ -1930,7 +1997,6 @@ int st_step_device(NbState* st) {
         if (status & kStatusMoverOverflow) mcap = 2 * st->mcap;
         res_free(st);
     }
-    rc = res_rebuild(st);
     st->bstats.ms_device = (float)(now_ms() - t0) - st->bstats.ms_pack - st->bstats.ms_unpack;
     share_times(st);
     return rc;
