@@ -22,24 +22,26 @@ namespace nb {
 __constant__ float c_axes[13][3];
 
 // ---------------------------------------------------------------- sort
-// A block of kSortWarps warps sorts `cpc` consecutive cells (1 for systems of large cells,
-// 8 for systems of small ones).  Keys of a direction are ordered by descending distance,
+// A block of kSortWarps (13) warps sorts `cpc` consecutive cells (1 for systems of large
+// cells, 13 for systems of small ones).  Keys of a direction are ordered by descending distance,
 // ties by ascending storage index (a stable order, independent of the order in which lanes
 // run):
 //  * a cell of at most 32 particles is sorted by one warp in registers: each lane holds one
 //    particle and counts, with a shuffle loop, the keys that come before its own;
-//  * a larger cell is sorted by all warps of the block, one warp per direction (w, w+4, ..),
-//    with a counting sort on the top bits of the 16-bit distance (64 buckets in the warp's
+//  * a larger cell is sorted by all warps of the block, one warp per direction, with a
+//    counting sort on the top bits of the 16-bit distance (64 buckets in the warp's
 //    shared memory) and an exact rank inside the bucket: position = (keys in farther
 //    buckets) + (keys of the same bucket with a larger distance, or an equal distance and a
 //    smaller storage index).
 constexpr int kSortBuckets = 64;
-constexpr int kSortWarps = 4;
+constexpr int kSortWarps = 13;
 
-__host__ __device__ inline size_t sort_warp_bytes() {
-    return (size_t)kMaxPartsPerCell * 4 + (size_t)kMaxPartsPerCell * 2 + (size_t)3 * kSortBuckets * 4;
+// Shared memory of one sorting warp for cells of up to scap particles (a multiple of 4):
+// the keys, the bucket members, bucket counts, starts and fill levels.
+__host__ __device__ inline size_t sort_warp_bytes(int scap) {
+    return (size_t)scap * 4 + (size_t)scap * 2 + (size_t)3 * kSortBuckets * 4;
 }
-__host__ inline size_t sort_smem_bytes() { return kSortWarps * sort_warp_bytes(); }
+__host__ inline size_t sort_smem_bytes(int scap) { return kSortWarps * sort_warp_bytes(scap); }
 
 // dscale * (bias + x.n), evaluated left to right without contraction (src/runner_dosort.c:148-149).
 __device__ __forceinline__ unsigned sort_dist(float4 x, float nx, float ny, float nz, float dscale, float bias) {
@@ -69,12 +71,12 @@ __device__ __forceinline__ void sort_small_cell(const float4* __restrict__ xq, u
 
 // The warp's share of the directions of a cell of more than 32 particles.
 __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys,
-                                                unsigned char* wp, int start, int n, unsigned mask, float dscale,
-                                                float bias, int warp, int lane) {
+                                                unsigned char* wp, int scap, int start, int n, unsigned mask,
+                                                float dscale, float bias, int warp, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
     unsigned* skey = reinterpret_cast<unsigned*>(wp);
-    unsigned short* members = reinterpret_cast<unsigned short*>(wp + (size_t)kMaxPartsPerCell * 4);
-    int* bcount = reinterpret_cast<int*>(wp + (size_t)kMaxPartsPerCell * 6);
+    unsigned short* members = reinterpret_cast<unsigned short*>(wp + (size_t)scap * 4);
+    int* bcount = reinterpret_cast<int*>(wp + (size_t)scap * 6);
     int* bstart = bcount + kSortBuckets;
     int* bfill = bstart + kSortBuckets;
     const int pad = (n + 3) & ~3;
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
                                                               const unsigned* __restrict__ cmask,
                                                               unsigned* __restrict__ keys,
                                                               const float2* __restrict__ cscale, int ncells, int cpc,
-                                                              unsigned long long* acc,
+                                                              int scap, unsigned long long* acc,
                                                               const unsigned long long* abort) {
     extern __shared__ __align__(16) unsigned char sort_smem[];
     if (step_aborted(abort)) return;
@@ -146,12 +148,12 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
     for (int c = c0; c < c1; ++c) {
         const int n = ccount[c];
         if (n <= 32) continue;
-        if (n > kMaxPartsPerCell) {
+        if (n > scap) {
             if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
             continue;
         }
-        sort_large_cell(xq, keys, sort_smem + (size_t)warp * sort_warp_bytes(), cstart[c], n, cmask[c], cscale[c].x,
-                        cscale[c].y, warp, lane);
+        sort_large_cell(xq, keys, sort_smem + (size_t)warp * sort_warp_bytes(scap), scap, cstart[c], n, cmask[c],
+                        cscale[c].x, cscale[c].y, warp, lane);
     }
 }
 

@@ -260,7 +260,21 @@ double now_ms() {
 
 // Cells per sort block: 8 when cells hold 32 particle slots or fewer on average (one warp
 // sorts a small cell alone), else 1 (the block's warps share a large cell's directions).
-int sort_cells_per_block(int slots, int ncells) { return slots <= 32 * (long long)ncells ? 8 : 1; }
+int sort_cells_per_block(int slots, int ncells) { return slots <= 32 * (long long)ncells ? kSortWarps : 1; }
+
+// Launches sort_cells for cells of up to scap particles (its shared memory sized by scap).
+int launch_sort(const float4* xq, const int* cstart, const int* ccount, const unsigned* cmask, unsigned* keys,
+                const float2* cscale, int ncells, int cpc, int scap, unsigned long long* acc,
+                const unsigned long long* abort, bool capturing, cudaStream_t s) {
+    scap = std::max(4, std::min(kMaxPartsPerCell, (scap + 3) & ~3));
+    const size_t smem = sort_smem_bytes(scap);
+    if (!capturing)
+        CU(cudaFuncSetAttribute(sort_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sort_cells<<<(ncells + cpc - 1) / cpc, kSortWarps * 32, smem, s>>>(xq, cstart, ccount, cmask, keys, cscale,
+                                                                       ncells, cpc, scap, acc, abort);
+    CU(cudaGetLastError());
+    return 0;
+}
 
 // Cells per host-thread range: about 8,192 particles, at least 16 cells.
 int cell_grain(const NbState* st) {
@@ -538,9 +552,9 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
         if (rc == 0 && span) rc = record_event(st, st->ev1);
         return rc;
     }
-    sort_cells<<<(st->ncells + V.cpc - 1) / V.cpc, kSortWarps * 32, sort_smem_bytes(), st->stream>>>(
-        V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, st->d_acc, V.abort);
-    CU(cudaGetLastError());
+    int rc0 = launch_sort(V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, cap,
+                          st->d_acc, V.abort, st->capturing, st->stream);
+    if (rc0 < 0) return rc0;
 
     Params P;
     P.xq = V.xq;
@@ -2375,10 +2389,9 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     const int cap4 = (maxcount + 3) & ~3;
     if (cap4 == 0) return 0;
     const int cpc = sort_cells_per_block(nslots, st->ncells);
-    sort_cells<<<(st->ncells + cpc - 1) / cpc, kSortWarps * 32, sort_smem_bytes(), s>>>(
-        static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale, st->ncells, cpc, acc,
-        nullptr);
-    CU(cudaGetLastError());
+    const int rcs = launch_sort(static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale,
+                                st->ncells, cpc, cap4, acc, nullptr, false, s);
+    if (rcs < 0) return rcs;
 
     TunedParams T;
     Params& P = T.p;
