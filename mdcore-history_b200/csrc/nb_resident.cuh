@@ -118,10 +118,19 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
     const size_t base = (size_t)c * RC.capc;
     int off = nstay[c];
     bool over = false;
-    for (int d = 0; d < 27; ++d) {
-        if (d == 13) continue;
-        const int src = RC.nbr[(size_t)c * 27 + (26 - d)];
-        const int nm = nmove[src];
+    // lane d (< 27) looks up the neighbour a particle moving by direction d comes from and
+    // whether it has leavers; only those directions are walked, in order
+    int my_src = 0, my_nm = 0;
+    if (lane < 27 && lane != 13) {
+        my_src = RC.nbr[(size_t)c * 27 + (26 - lane)];
+        my_nm = nmove[my_src];
+    }
+    unsigned todo = __ballot_sync(FULL, my_nm > 0);
+    while (todo) {
+        const int d = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int src = __shfl_sync(FULL, my_src, d);
+        const int nm = __shfl_sync(FULL, my_nm, d);
         for (int m0 = 0; m0 < nm; m0 += 32) {
             const int m = m0 + lane;
             Mover mv;
@@ -167,7 +176,8 @@ __global__ void __launch_bounds__(256) slot_of_ids(ResidentCells RC, const int* 
 
 // Symplectic Euler update of every particle (engine_advance, src/engine.c:1975-1979), with
 // the float expressions the host integrator evaluates: w = (float)(dt * 1/m),
-// v += f*w, x += dt*v; forces from the fixed-point accumulators of the sweep.
+// v += f*w, x += dt*v; forces from the fixed-point accumulators of the sweep.  One thread
+// per slot (grid: ncells * capc threads).
 __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const int* __restrict__ count,
                                                        const unsigned long long* __restrict__ force,
                                                        const int* __restrict__ cell_engine,
@@ -177,20 +187,19 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
                                                        const unsigned long long* __restrict__ status,
                                                        const unsigned long long* __restrict__ acc,
                                                        unsigned long long* __restrict__ done) {
-    const int lane = threadIdx.x & 31;
-    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (*status != 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {          // completed steps, accepted pairs
         done[0] += 1ull;
         done[1] += acc[kAccPairs];
     }
-    if (c >= RC.ncells) return;
-    const int n = min(count[c], RC.capc);
-    const size_t base = (size_t)c * RC.capc;
+    // one thread per slot of every block (the slots past a cell's count do nothing)
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= (size_t)RC.ncells * RC.capc) return;
+    const int c = (int)(s / (unsigned)RC.capc);
+    if ((int)(s - (size_t)c * RC.capc) >= min(count[c], RC.capc)) return;
     const int k_eng = cell_engine[c];
     const float dt = engine_dt[k_eng];
-    for (int k = lane; k < n; k += 32) {
-        const size_t s = base + k;
+    {
         float4 x = xq[s], vv = v[s];
         const int type = __float_as_int(x.w);
         const float w = (float)((double)dt * engine_imass[(size_t)k_eng * max_type + type]);

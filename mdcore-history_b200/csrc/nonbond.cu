@@ -1507,7 +1507,8 @@ int res_issue_step(NbState* st) {
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
     rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
-    integrate_cells<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
+    const unsigned slot_blocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
+    integrate_cells<<<slot_blocks, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
                                                   st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o],
                                                   st->r_status, st->d_acc, st->r_done);
     CU(cudaGetLastError());
