@@ -295,6 +295,7 @@ struct engine {
     void *cuda_rigid;       /* device state of the rigid groups, owned by the engine */
     int part2rigid_size;    /* entries of part2rigid */
     int rigids_gen;         /* bumped by every engine_rigid_add */
+    struct potential *ep;   /* explicit electrostatics (engine_setexplepot), or NULL */
 };
 
 /* src/engine.c:2439-2591 */
@@ -315,6 +316,15 @@ int engine_exclusion_add(struct engine *e, int i, int j);
 int engine_exclusion_shrink(struct engine *e);
 /* src/engine_rigid.c:78-229 */
 int engine_rigid_add(struct engine *e, int pid, int pjd, double d);
+/* src/engine.c:1029-1053.  Sets the explicit electrostatic potential (engine_flag_explepot)
+ * or clears it (ep = NULL).  The reference stores ep but no runner reads it; here every
+ * pair within the cutoff that is not excluded also interacts through q_i q_j ep(r) with the
+ * particles' charges (engine_load's q), in addition to its type pair's potential, if any:
+ * a pair whose types have no potential still interacts through ep.  ep is normally
+ * potential_create_Coulomb(a, b, 1, tol) (prefactor 1/(4 pi) as the reference's tables),
+ * so that q in units of e * sqrt(4 pi * 138.935458) gives kJ/mol.  Call before
+ * engine_start. */
+int engine_setexplepot(struct engine *e, struct potential *ep);
 /* src/engine.c:1674-1826 */
 int engine_start(struct engine *e, int nr_runners, int nr_queues);
 /* src/engine.c:2070-2240.  One time step (re-binning, forces, symplectic Euler, rigid

@@ -51,7 +51,8 @@ static const char *engine_msg[] = {
 #define ENGINE_FLAGS_SUPPORTED                                                                 \
     (engine_flag_static | engine_flag_localparts | engine_flag_cuda | engine_flag_verlet |     \
      engine_flag_verlet_pairwise | engine_flag_affinity | engine_flag_prefetch |               \
-     engine_flag_verlet_pseudo | engine_flag_unsorted | engine_flag_shake | engine_flag_nullpart)
+     engine_flag_verlet_pseudo | engine_flag_unsorted | engine_flag_shake | engine_flag_nullpart |   \
+     engine_flag_explepot)
 
 size_t engine_sizeof(void) { return sizeof(struct engine); }
 
@@ -431,6 +432,18 @@ int engine_finalize(struct engine *e) {
     free(e->rigids);
     free(e->part2rigid);
     memset(e, 0, sizeof(struct engine));
+    return engine_err_ok;
+}
+
+int engine_setexplepot(struct engine *e, struct potential *ep) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (ep != NULL) {
+        e->flags |= engine_flag_explepot;
+        e->ep = ep;
+    } else {
+        e->flags &= ~engine_flag_explepot;
+        e->ep = NULL;
+    }
     return engine_err_ok;
 }
 

@@ -71,6 +71,13 @@ struct Params {
     float cutoff2s;             // self tasks: float(cutoff^2) (src/runner_dopair.c:896)
     int unsorted;               // 1: sweep every candidate (engine_flag_unsorted)
     const unsigned long long* abort;   // device-resident steps: nonzero = skip this launch
+    // Explicit electrostatics (engine_setexplepot): every pair within the cutoff that is not
+    // excluded also interacts through q_i q_j ep(r), ep being table ep_pot (-1: none), q by
+    // particle id.  tab_global: the tables are read from global memory (through L1) instead
+    // of being staged in shared memory (many type pairs).
+    const float* qid;
+    int ep_pot;
+    int tab_global;
 };
 
 // A device-resident step that was aborted (see nb_resident.cuh) launches nothing more.

@@ -44,11 +44,14 @@ __host__ __device__ inline size_t sort_warp_bytes(int scap) {
 __host__ inline size_t sort_smem_bytes(int scap) { return kSortWarps * sort_warp_bytes(scap); }
 
 // dscale * (bias + x.n), evaluated left to right without contraction (src/runner_dosort.c:148-149).
+// A particle inside its cell gives 0..32767; one that has left it by more than a cell (a
+// system blowing up) is held to 16 bits, so that the key's upper half, its slot in the
+// cell, stays intact and every access stays inside the cell.
 __device__ __forceinline__ unsigned sort_dist(float4 x, float nx, float ny, float nz, float dscale, float bias) {
     float d = __fadd_rn(bias, __fmul_rn(x.x, nx));
     d = __fadd_rn(d, __fmul_rn(x.y, ny));
     d = __fadd_rn(d, __fmul_rn(x.z, nz));
-    return __float2uint_rz(__fmul_rn(dscale, d));
+    return min(__float2uint_rz(__fmul_rn(dscale, d)), 0xffffu);
 }
 
 // One warp, a cell of n <= 32 particles, every direction of its mask.
@@ -264,7 +267,8 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     const int si = P.cstart[ci], sj = P.cstart[cj];
     const int padi = (ni + 3) & ~3, padj = (nj + 3) & ~3;
     const int mt = P.max_type;
-    SweepSmem S = carve(smem_raw, cap, NW, P.ncoef, P.npots, mt);
+    // tables in shared memory, or read from global memory when they do not fit
+    SweepSmem S = carve(smem_raw, cap, NW, P.tab_global ? 0 : P.ncoef, P.tab_global ? 0 : P.npots, mt);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // Stage the cells with TMA bulk copies; the tables with ordinary loads meanwhile.
@@ -285,11 +289,16 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             bulk_g2s(S.keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, S.bar);
         }
     }
-    for (int k = tid; k < P.ncoef; k += NW * 32) S.coef[k] = P.coef[k];
-    for (int k = tid; k < P.npots; k += NW * 32) {
-        S.potinfo[k] = P.potinfo[k];
-        S.potn[k] = P.potn[k];
+    if (!P.tab_global) {
+        for (int k = tid; k < P.ncoef; k += NW * 32) S.coef[k] = P.coef[k];
+        for (int k = tid; k < P.npots; k += NW * 32) {
+            S.potinfo[k] = P.potinfo[k];
+            S.potn[k] = P.potn[k];
+        }
     }
+    const float* __restrict__ tcoef = P.tab_global ? P.coef : S.coef;
+    const float4* __restrict__ tinfo = P.tab_global ? P.potinfo : S.potinfo;
+    const int* __restrict__ tn = P.tab_global ? P.potn : S.potn;
     for (int k = tid; k < mt * mt; k += NW * 32) S.potidx[k] = P.potidx[k];
     for (int k = tid; k < NW * cap; k += NW * 32) S.fj[k] = make_float4(0.f, 0.f, 0.f, 0.f);
     const bool arrived = mbar_wait_bounded(S.bar, 0);
@@ -340,12 +349,14 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
         int pidi = -1;
         unsigned emask = 0u;
         int exlo = 0, exhi = 0;
+        float qi = 0.f;
         if (valid) {
             xi = self ? S.xj[loc] : S.xi[loc];
             pidi = self ? S.pidj[loc] : S.pidi[loc];
             emask = P.emask[pidi];
             exlo = P.exoff[pidi];
             exhi = P.exoff[pidi + 1];
+            if (P.ep_pot >= 0) qi = P.qid[pidi];
         }
         const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
         const int prow = __float_as_int(xi.w) * mt;
@@ -364,7 +375,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
             const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
             const int pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
-            bool acc = act && pot >= 0 && r2 <= cut2;
+            bool acc = act && (pot >= 0 || P.ep_pot >= 0) && r2 <= cut2;
             ncand += act;
             if (acc && excluded_pair(pidi, jids[k], emask, exlo, exhi, P.exlist)) {
                 acc = false;
@@ -373,8 +384,15 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             if (__any_sync(FULL, acc)) {
                 float wx = 0.f, wy = 0.f, wz = 0.f;
                 if (acc) {
-                    float e, f;
-                    eval_table(S.coef, S.potinfo[pot], S.potn[pot], r2, e, f, status);
+                    float e = 0.f, f = 0.f;
+                    if (pot >= 0) eval_table(tcoef, tinfo[pot], tn[pot], r2, e, f, status);
+                    if (P.ep_pot >= 0) {        // + q_i q_j ep(r)
+                        const float qq = qi * P.qid[jids[k]];
+                        float ee, fe;
+                        eval_table(tcoef, tinfo[P.ep_pot], tn[P.ep_pot], r2, ee, fe, status);
+                        e = fmaf(qq, ee, e);
+                        f = fmaf(qq, fe, f);
+                    }
                     wx = f * dx; wy = f * dy; wz = f * dz;
                     fix -= wx; fiy -= wy; fiz -= wz;
                     epot += (double)e;

@@ -235,9 +235,22 @@ struct SharedTables {
     int* potidx;
 };
 
-template <int NW, int STAGES>
+// Table modes of the persistent sweeps: kTabShared (tables staged in shared memory, a lookup
+// per pair), kTabOne (one table for every type pair), kTabGlobal (tables read from global
+// memory through L1, for systems whose tables do not fit in shared memory, and explicit
+// electrostatics).
+constexpr int kTabShared = 0, kTabOne = 1, kTabGlobal = 2;
+
+template <int NW, int STAGES, int TAB>
 __device__ __forceinline__ SharedTables stage_tables(const Params& P, unsigned char* smem_raw, int cap) {
     SharedTables S;
+    if (TAB == kTabGlobal) {
+        S.potinfo = const_cast<float4*>(P.potinfo);
+        S.coef = const_cast<float*>(P.coef);
+        S.potn = const_cast<int*>(P.potn);
+        S.potidx = const_cast<int*>(P.potidx);
+        return S;
+    }
     unsigned char* sp = smem_raw + (size_t)NW * warp_slice_bytes(cap, STAGES);
     S.potinfo = reinterpret_cast<float4*>(sp); sp += (size_t)P.npots * 16;
     S.coef = reinterpret_cast<float*>(sp); sp += (size_t)((P.ncoef + 3) & ~3) * 4;
@@ -518,10 +531,10 @@ __device__ __forceinline__ unsigned strip_candidates(int len, int col, int strid
     return len > col ? (unsigned)((len - col + stride - 1) / stride) : 0u;
 }
 
-template <bool HAS_EXCL, bool ONE_POT>
+template <bool HAS_EXCL, int TAB>
 __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& S, const float4 xj,
                                            const int* __restrict__ jids, int k, bool act,
-                                           float pix, float piy, float piz, int prow, const IExcl& ix,
+                                           float pix, float piy, float piz, int prow, float qi, const IExcl& ix,
                                            float cut2, float& fix, float& fiy, float& fiz,
                                            float& wx, float& wy, float& wz, double& e_task, unsigned& npairs,
                                            unsigned& nexcl, bool& any_acc) {
@@ -529,8 +542,8 @@ __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& 
     const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
     const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     int pot = 0;
-    if (!ONE_POT) pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
-    bool acc = act && pot >= 0 && r2 <= cut2;
+    if (TAB != kTabOne) pot = act ? S.potidx[prow + __float_as_int(xj.w)] : -1;
+    bool acc = act && (pot >= 0 || (TAB == kTabGlobal && P.ep_pot >= 0)) && r2 <= cut2;
     if (HAS_EXCL) {
         // One window test per candidate; the mask bit or the list is looked at only for
         // ids inside the particle's exclusion window (or when it has far partners).
@@ -560,8 +573,25 @@ __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& 
             float r = r2 * rinv;
             r = fmaf(fmaf(-r, r, r2), 0.5f * rinv, r);
             float e, f;
-            const float4 info = S.potinfo[pot];
-            eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
+            if (TAB == kTabGlobal) {
+                e = 0.f;
+                f = 0.f;
+                if (pot >= 0) {
+                    const float4 info = S.potinfo[pot];
+                    eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
+                }
+                if (P.ep_pot >= 0) {            // + q_i q_j ep(r)
+                    const float qq = qi * P.qid[jids[k]];
+                    const float4 info = S.potinfo[P.ep_pot];
+                    float ee, fe;
+                    eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, ee, fe);
+                    e = fmaf(qq, ee, e);
+                    f = fmaf(qq, fe, f);
+                }
+            } else {
+                const float4 info = S.potinfo[pot];
+                eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
+            }
             wx = f * dx; wy = f * dy; wz = f * dz;
             fix -= wx; fiy -= wy; fiz -= wz;
             e_task += (double)e;
@@ -685,7 +715,7 @@ __device__ __forceinline__ float reduce_scatter_rows(const float (&v)[WIN], int 
 //
 // WIN (4 or 8): sweep steps per reduce-scatter; 8 halves the shuffles per step but holds
 // twice the registers.  STAGES (1 or 2): staging buffers per warp.
-template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES, int TPSM>
+template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM>
 __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -694,7 +724,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
     if (step_aborted(P.abort)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = P.max_type;
-    const SharedTables S = stage_tables<NW, STAGES>(P, smem_raw, cap);
+    const SharedTables S = stage_tables<NW, STAGES, TAB>(P, smem_raw, cap);
     if (lane < STAGES) {
         mbar_init(warp_slice(smem_raw, cap, warp, STAGES, lane).bar, 1);
         mbar_fence_init();
@@ -732,9 +762,11 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
             IExcl ix = no_iexcl();
+            float qi = 0.f;
             if (valid) {
                 xi = self ? W.js[loc] : P.xq[si + loc];
                 if (HAS_EXCL) ix = load_iexcl(P, self ? W.pidraw[loc] : P.pid[si + loc]);
+                if (TAB == kTabGlobal && P.ep_pot >= 0) qi = P.qid[self ? W.pidraw[loc] : P.pid[si + loc]];
             }
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
@@ -746,7 +778,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
 #pragma unroll
                 for (int m = 0; m < WIN; ++m) {
                     const int k = k0 + m;
-                    pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, ix, cut2,
+                    pair_force<HAS_EXCL, TAB>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, qi, ix, cut2,
                                                   fix, fiy, fiz, vx[m], vy[m], vz[m], e_task, npairs, nexcl,
                                                   any_acc);
                 }
@@ -798,7 +830,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
 // contributions of WIN steps (4 WIN consecutive j) are summed over the 8 rows by one
 // reduce-scatter, after which the 32 (or 16) lanes write distinct j; the i forces are
 // summed over the 4 columns at the end of the strip.
-template <int NW, bool HAS_EXCL, bool ONE_POT, int WIN, int STAGES, int TPSM>
+template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM>
 __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -808,7 +840,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = lane >> 2, col = lane & 3;
     const int mt = P.max_type;
-    const SharedTables S = stage_tables<NW, STAGES>(P, smem_raw, cap);
+    const SharedTables S = stage_tables<NW, STAGES, TAB>(P, smem_raw, cap);
     if (lane < STAGES) {
         mbar_init(warp_slice(smem_raw, cap, warp, STAGES, lane).bar, 1);
         mbar_fence_init();
@@ -846,9 +878,11 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
             IExcl ix = no_iexcl();
+            float qi = 0.f;
             if (valid) {
                 xi = self ? W.js[loc] : P.xq[si + loc];
                 if (HAS_EXCL) ix = load_iexcl(P, self ? W.pidraw[loc] : P.pid[si + loc]);
+                if (TAB == kTabGlobal && P.ep_pot >= 0) qi = P.qid[self ? W.pidraw[loc] : P.pid[si + loc]];
             }
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
@@ -861,7 +895,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
                 for (int m = 0; m < WIN; ++m) {
                     if (k0 + 4 * m < kmax) {                 // warp-uniform
                         const int k = k0 + 4 * m + col;
-                        pair_force<HAS_EXCL, ONE_POT>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, ix,
+                        pair_force<HAS_EXCL, TAB>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, qi, ix,
                                                       cut2, fix, fiy, fiz, vx[m], vy[m], vz[m], e_task, npairs,
                                                       nexcl, any_acc);
                     } else {

@@ -68,6 +68,11 @@ struct NbState {
     int stages = 1;                // staging buffers per worker warp (2: next task's copies in flight)
     int occupancy = 640;           // resident threads per SM the sweep's registers are sized for
     bool has_excl = false;
+    bool need_pid = false;         // ids uploaded: exclusions or explicit charges
+    int ep_pot = -1;               // table index of the explicit electrostatic potential
+    int tab_global = 0;            // tables read from global memory (too large for shared)
+    float* d_qid = nullptr;        // charges by global id (explicit electrostatics)
+    std::vector<float> h_qid;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
     int* d_order = nullptr;        // task queue order (scheduling order of all tasks)
@@ -346,14 +351,14 @@ void pack_range(NbState* st, int cb, int ce) {
                 st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
             }
             for (int q = cl->count; q < pad; q++) st->h_xq[slot + q] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
-            if (st->has_excl) {          // ids are read by the sweep for exclusion tests only
+            if (st->need_pid) {          // ids are read by the sweep for exclusions and charges only
                 for (int q = 0; q < cl->count; q++) st->h_pid[slot + q] = id0 + cl->parts[q].id;
                 for (int q = cl->count; q < pad; q++) st->h_pid[slot + q] = 0;
             }
         }
         const size_t s0 = (size_t)cstart[cb + b], s1 = (size_t)cstart[cb + e];
         evict_lines(st->h_xq + s0, sizeof(float4) * (s1 - s0));
-        if (st->has_excl) evict_lines(st->h_pid + s0, sizeof(int) * (s1 - s0));
+        if (st->need_pid) evict_lines(st->h_pid + s0, sizeof(int) * (s1 - s0));
     });
 }
 
@@ -390,10 +395,11 @@ int launch_plain_nw(NbState* st, const Params& P, int cap, size_t smem) {
 
 int launch_plain(NbState* st, const Params& P, int cap) {
     int nw = st->warps;
-    size_t smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+    const int tc = st->tab_global ? 0 : st->ncoef, tp = st->tab_global ? 0 : st->npots;
+    size_t smem = sweep_smem_bytes(cap, nw, tc, tp, st->max_type);
     while (smem > 200 * 1024 && nw > 1) {
         nw /= 2;
-        smem = sweep_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type);
+        smem = sweep_smem_bytes(cap, nw, tc, tp, st->max_type);
     }
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
@@ -411,9 +417,9 @@ int launch_plain(NbState* st, const Params& P, int cap) {
 // Persistent launch: as many CTAs as fit on every SM at once.  Under stream capture the
 // function attribute and occupancy query are skipped and the grid of the preceding direct
 // launch of the same configuration is reused.
-template <int NW, bool EX, bool ONE, int WIN, int LAY, int STG, int TPSM>
+template <int NW, bool EX, int TAB, int WIN, int LAY, int STG, int TPSM>
 int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    auto kern = LAY ? sweep_tiled<NW, EX, ONE, WIN, STG, TPSM> : sweep_tuned<NW, EX, ONE, WIN, STG, TPSM>;
+    auto kern = LAY ? sweep_tiled<NW, EX, TAB, WIN, STG, TPSM> : sweep_tuned<NW, EX, TAB, WIN, STG, TPSM>;
     int grid = st->last_grid;
     if (!st->capturing) {
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -430,12 +436,15 @@ int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
 
 template <int NW, int WIN, int LAY, int STG, int TPSM>
 int launch_tuned_w(NbState* st, const TunedParams& T, int cap, size_t smem) {
+    if (st->tab_global)
+        return st->has_excl ? launch_tuned_nw<NW, true, kTabGlobal, WIN, LAY, STG, TPSM>(st, T, cap, smem)
+                            : launch_tuned_nw<NW, false, kTabGlobal, WIN, LAY, STG, TPSM>(st, T, cap, smem);
     const bool one = st->one_pot;
     if (st->has_excl)
-        return one ? launch_tuned_nw<NW, true, true, WIN, LAY, STG, TPSM>(st, T, cap, smem)
-                   : launch_tuned_nw<NW, true, false, WIN, LAY, STG, TPSM>(st, T, cap, smem);
-    return one ? launch_tuned_nw<NW, false, true, WIN, LAY, STG, TPSM>(st, T, cap, smem)
-               : launch_tuned_nw<NW, false, false, WIN, LAY, STG, TPSM>(st, T, cap, smem);
+        return one ? launch_tuned_nw<NW, true, kTabOne, WIN, LAY, STG, TPSM>(st, T, cap, smem)
+                   : launch_tuned_nw<NW, true, kTabShared, WIN, LAY, STG, TPSM>(st, T, cap, smem);
+    return one ? launch_tuned_nw<NW, false, kTabOne, WIN, LAY, STG, TPSM>(st, T, cap, smem)
+               : launch_tuned_nw<NW, false, kTabShared, WIN, LAY, STG, TPSM>(st, T, cap, smem);
 }
 
 // Worker warps per block: 2, 4 or 8 (two warps fit even the largest cells).
@@ -482,10 +491,11 @@ int launch_tuned(NbState* st, const Params& P, int cap4) {
     T.task_sm = st->record_clock ? st->d_task_sm : nullptr;
     CU(cudaMemsetAsync(st->d_counter, 0, sizeof(int), st->stream));
     int nw = st->warps < 2 ? 2 : st->warps;
-    size_t smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type, st->stages);
+    const int tc = st->tab_global ? 0 : st->ncoef, tp = st->tab_global ? 0 : st->npots;
+    size_t smem = warps_smem_bytes(cap, nw, tc, tp, st->max_type, st->stages);
     while (smem > 200 * 1024 && nw > 2) {
         nw /= 2;
-        smem = warps_smem_bytes(cap, nw, st->ncoef, st->npots, st->max_type, st->stages);
+        smem = warps_smem_bytes(cap, nw, tc, tp, st->max_type, st->stages);
     }
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
@@ -583,6 +593,9 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
     P.cutoff2s = st->cut2s;
     P.unsorted = st->unsorted;
     P.abort = V.abort;
+    P.qid = st->d_qid;
+    P.ep_pot = st->ep_pot;
+    P.tab_global = st->tab_global;
 
     int rc = record_event(st, st->evs0);
     if (rc < 0) return rc;
@@ -701,6 +714,7 @@ int finish_stats(NbState* st) {
 }
 
 void res_free(NbState* st);
+int refresh_charges(NbState* st);
 
 void state_free(NbState* st) {
     if (st == nullptr) return;
@@ -711,7 +725,7 @@ void state_free(NbState* st) {
                    st->d_cscale, st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
                    st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef, st->d_queue,
-                   st->d_qcount, st->d_bsum};
+                   st->d_qcount, st->d_bsum, st->d_qid};
     for (void* p : dev) cudaFree(p);
     void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
     for (void* p : host) cudaFreeHost(p);
@@ -754,6 +768,11 @@ int load_state(NbState* st) {
                               __func__, __FILE__);
                 return engine_err = engine_err_potential;
             }
+        if (!same_table(e->ep, e0->ep)) {
+            errs_register(engine_err_potential, "Engines of a batch differ in their explicit electrostatics.",
+                          __LINE__, __func__, __FILE__);
+            return engine_err = engine_err_potential;
+        }
         st->cell_off[k + 1] = st->cell_off[k] + e->s.nr_cells;
         st->id_off[k + 1] = st->id_off[k] + (e->s.size_parts > 0 ? e->s.size_parts : 1);
     }
@@ -792,6 +811,14 @@ int load_state(NbState* st) {
             if (k == (int)uniq.size()) uniq.push_back(p);
             potidx[i * mt + j] = k;
         }
+    // The explicit electrostatic potential, if any, is one more table.
+    st->ep_pot = -1;
+    if (e0->ep != nullptr) {
+        int k = 0;
+        while (k < (int)uniq.size() && uniq[k] != e0->ep) k++;
+        if (k == (int)uniq.size()) uniq.push_back(e0->ep);
+        st->ep_pot = k;
+    }
     std::vector<float> coef;
     std::vector<float4> potinfo;
     std::vector<int> potn;
@@ -807,7 +834,11 @@ int load_state(NbState* st) {
         return engine_err = engine_err_potential;
     }
     st->npots = (int)uniq.size();
-    st->one_pot = (uniq.size() == 1) && std::all_of(potidx.begin(), potidx.end(), [](int v) { return v == 0; });
+    st->one_pot = (uniq.size() == 1) && std::all_of(potidx.begin(), potidx.end(), [](int v) { return v == 0; }) &&
+                  st->ep_pot < 0;
+    // Tables of more than 24 KB (many type pairs) would crowd the sweep's shared memory; they
+    // are read from global memory instead, as they are with explicit electrostatics.
+    st->tab_global = (st->ep_pot >= 0 || coef.size() * sizeof(float) > 24 * 1024) ? 1 : 0;
     st->ncoef = (int)coef.size();
     st->max_type = mt;
     if (coef.empty()) coef.push_back(0.f);
@@ -905,6 +936,9 @@ int load_state(NbState* st) {
         }
     }
     st->has_excl = !ex.empty();
+    st->need_pid = st->has_excl || st->ep_pot >= 0;
+    if (dev_alloc(&st->d_qid, nid + 1)) return engine_err_cuda;
+    refresh_charges(st);
     std::vector<unsigned> emask(nid, 0u);
     std::vector<int> cnt(nid + 1, 0);
     for (const auto& ab : ex) {
@@ -933,6 +967,25 @@ int load_state(NbState* st) {
     return 0;
 }
 
+// Charges by global particle id from the engines' host cells, to the device (explicit
+// electrostatics only; other systems never read them).
+int refresh_charges(NbState* st) {
+    if (st->ep_pot < 0) return 0;
+    st->h_qid.assign((size_t)st->nid + 1, 0.f);
+    for (size_t k = 0; k < st->engines.size(); k++) {
+        const struct space* sp = &st->engines[k]->s;
+        for (int c = 0; c < sp->nr_cells; c++)
+            for (int q = 0; q < sp->cells[c].count; q++) {
+                const struct part* p = &sp->cells[c].parts[q];
+                st->h_qid[(size_t)st->id_off[k] + p->id] = p->q;
+            }
+    }
+    CU(cudaMemcpyAsync(st->d_qid, st->h_qid.data(), sizeof(float) * st->h_qid.size(), cudaMemcpyHostToDevice,
+                       st->stream));
+    CU(cudaStreamSynchronize(st->stream));
+    return 0;
+}
+
 // Copies of the timing fields of the last evaluation into every engine's stats.
 void share_times(NbState* st) {
     for (struct engine* e : st->engines) {
@@ -949,6 +1002,10 @@ void share_times(NbState* st) {
 int st_load_parts(NbState* st) {
     CU(cudaSetDevice(st->device));
     const double t0 = now_ms();
+    if (st->ep_pot >= 0) {               // charges may have been changed on the host
+        const int rc = refresh_charges(st);
+        if (rc < 0) return rc;
+    }
     const int slots = prepare_slots(st);
     if (slots < 0) return slots;
     const std::vector<int> bounds = chunk_bounds(st, slots);
@@ -959,7 +1016,7 @@ int st_load_parts(NbState* st) {
         const int s0 = st->h_cstart[cb], n = st->h_cstart[ce] - s0;
         if (n <= 0) continue;
         CU(cudaMemcpyAsync(st->d_xq + s0, st->h_xq + s0, sizeof(float4) * n, cudaMemcpyHostToDevice, st->stream));
-        if (st->has_excl)
+        if (st->need_pid)
             CU(cudaMemcpyAsync(st->d_pid + s0, st->h_pid + s0, sizeof(int) * n, cudaMemcpyHostToDevice, st->stream));
     }
     const double t1 = now_ms();
@@ -1433,6 +1490,9 @@ int res_upload(NbState* st) {
     st->bstats.ms_pack = (float)(now_ms() - t0);
     st->res_engine_n.assign(ne, 0);
     for (int k = 0; k < ne; k++) st->res_engine_n[k] = off[st->cell_off[k + 1]] - off[st->cell_off[k]];
+    if (st->ep_pot >= 0)                 // charges by id, as packed above
+        CU(cudaMemcpyAsync(st->d_qid, st->id_q.data(), sizeof(float) * st->id_q.size(), cudaMemcpyHostToDevice,
+                           st->stream));
     CU(cudaMemcpyAsync(st->r_cnt[0], cnt, sizeof(int) * nc, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
@@ -2423,13 +2483,17 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     P.cutoff2s = (float)e->s.cutoff2;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
     P.abort = nullptr;
+    P.qid = st->d_qid;
+    P.ep_pot = st->ep_pot;
+    P.tab_global = st->tab_global;
     T.order = st->d_order;
     T.qcount = nullptr;
     T.counter = counter;
     T.task_clock = nullptr;
     T.task_sm = nullptr;
     const int cap = cap4 + 8;
-    const size_t smem = warps_smem_bytes(cap, 4, st->ncoef, st->npots, st->max_type, 1);
+    const size_t smem = warps_smem_bytes(cap, 4, st->tab_global ? 0 : st->ncoef, st->tab_global ? 0 : st->npots,
+                                         st->max_type, 1);
     if (smem > 220 * 1024) {
         errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
                       __func__, __FILE__);

@@ -374,13 +374,23 @@ void nb_sweep_scales(const struct space *s, float *bias, float *dscale, int *dma
 }
 
 /* Shift of cell j relative to cell i of task t and its discretised norm
- * (src/runner_dopair.c:586-597). */
+ * (src/runner_dopair.c:586-597).  The sweep takes dnshift as the distance of cell j from
+ * cell i along the task's sort axis.  For cubic cells the shift lies on that axis and its
+ * norm, which the reference uses, is that distance; for other cells the norm exceeds it and
+ * the reference's sweep skips pairs inside the cutoff, so the projection on the axis is
+ * used there (a lower bound, like the truncation to an integer). */
 int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dnshift, int *ci_out,
                   int *cj_out) {
     struct task *tk = &s->tasks[t];
     struct cell *ci = &s->cells[tk->i], *cj = &s->cells[tk->j];
     int sid = space_getsid(s, &ci, &cj, shift);
     float nshift = sqrt(shift[0] * shift[0] + shift[1] * shift[1] + shift[2] * shift[2]);
+    if (!(s->h[0] == s->h[1] && s->h[1] == s->h[2])) {
+        float n[3];
+        sort_axis(sid, n);
+        nshift = shift[0] * n[0] + shift[1] * n[1] + shift[2] * n[2];
+        if (nshift < 0.0f) nshift = 0.0f;
+    }
     *dnshift = dscale * nshift;
     *ci_out = (int)(ci - s->cells);
     *cj_out = (int)(cj - s->cells);

@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
         "engine_start": (C.c_int, [vp, C.c_int, C.c_int]),
         "engine_step": (C.c_int, [vp]),
         "engine_step_host": (C.c_int, [vp]),
+        "engine_setexplepot": (C.c_int, [vp, P(Potential)]),
         "engine_batch_step_host": (C.c_int, [vp]),
         "engine_advance": (C.c_int, [vp]),
         "engine_finalize": (C.c_int, [vp]),
@@ -255,8 +256,13 @@ class Engine:
         x = np.ascontiguousarray(sysm.x, np.float64)
         t = np.ascontiguousarray(sysm.type, np.int32)
         v = None if sysm.v is None else np.ascontiguousarray(sysm.v, np.float64)
-        _check(e.lib.engine_load(e.ptr, _dptr(x), None if v is None else _dptr(v), _iptr(t), None, None, None, None,
-                                 sysm.n), "engine_load")
+        q = None if getattr(sysm, "q", None) is None else np.ascontiguousarray(sysm.q, np.float64)
+        _check(e.lib.engine_load(e.ptr, _dptr(x), None if v is None else _dptr(v), _iptr(t), None, None,
+                                 None if q is None else _dptr(q), None, sysm.n), "engine_load")
+        if getattr(sysm, "ep", None) is not None:
+            ep = create_potential(sysm.ep)
+            e.pots.append(ep)
+            _check(e.lib.engine_setexplepot(e.ptr, ep), "engine_setexplepot")
         e.n = sysm.n
         if sysm.rigid is not None:
             for i, j, d in np.asarray(sysm.rigid):

@@ -57,6 +57,8 @@ class System:
     period: int = 7
     v: Optional[np.ndarray] = None          # (N,3) velocities, nm/ps (None: at rest)
     rigid: Optional[np.ndarray] = None      # (M,3) rigid constraints: id i, id j, length d (nm)
+    q: Optional[np.ndarray] = None          # (N,) per-particle charges (explicit electrostatics)
+    ep: Optional[PotSpec] = None            # explicit electrostatic potential (engine_setexplepot)
 
     @property
     def n(self) -> int:
@@ -318,3 +320,111 @@ def read_refout(path: str, sysm: System):
     return dict(N=int(N), nexcl=int(nexcl), epot=float(epot), epot_nonbond=float(epot_nb),
                 epot_exclusion=float(epot_ex), f=f.copy(), xrel=xr.copy(), cell=cell.copy(),
                 cells=cells, tables=tables)
+
+
+QSCALE = math.sqrt(Q_SCALE)     # e -> per-particle charge unit of tables with prefactor 1/(4 pi)
+
+
+def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box=(10.8, 10.8, 7.8), seed: int = 0,
+                 cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12) -> System:
+    """Heterogeneous solvated-chain system: `nchains` linear bead chains of `length` beads
+    (bond 0.15 nm, 20 LJ bead types with sigma U[0.25, 0.40] nm and epsilon U[0.1, 1.0]
+    kJ/mol, Lorentz-Berthelot mixing, charges N(0, 0.3) e neutralised per chain) and up to
+    `nwater` 3-site water molecules in the SPC/E geometry (O -0.8476 e, H +0.4238 e, O-O LJ
+    sigma 0.3166 nm, epsilon 0.650, the three intramolecular distances constrained) on a
+    jittered grid at 33.4 molecules/nm^3, waters whose oxygen is closer than `gap` to a bead
+    left out (0.12 nm: the 23,400 waters of the named system fit; the close contacts this
+    leaves make the unrelaxed system unfit for dynamics, 0.25 nm gives a calmer one).  Charges act through explicit electrostatics (ep: the shifted Coulomb table
+    with unit charge, cutoff 1.2 nm); the type tables are LJ only (none for H).  1-2 and 1-3
+    exclusions along the chains, the three intramolecular pairs of every water excluded.
+    Types: 0 O, 1 H, 2..21 beads.  Seeded.
+
+    Chains grow together as self-avoiding random walks (every new bead at least 0.25 nm
+    from the beads placed before it other than its two predecessors, bond angles >= 90
+    degrees, up to 20 tries per bead)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    dim = np.array(box, np.float64)
+    nbt = 20
+    sig_b = rng.uniform(0.25, 0.40, nbt)
+    eps_b = rng.uniform(0.1, 1.0, nbt)
+    pos = np.zeros((nchains, length, 3))
+    pos[:, 0] = rng.uniform(0, 1, (nchains, 3)) * dim
+    prev = rng.normal(size=(nchains, 3))
+    prev /= np.linalg.norm(prev, axis=1)[:, None]
+    for t in range(1, length):
+        placed = pos[:, :t].reshape(-1, 3) % dim
+        tree = cKDTree(placed, boxsize=dim)
+        todo = np.arange(nchains)
+        cand = np.zeros((nchains, 3))
+        for _try in range(20):
+            u = rng.normal(size=(len(todo), 3))
+            u /= np.linalg.norm(u, axis=1)[:, None]
+            flip = (u * prev[todo]).sum(1) < 0.0
+            u[flip] = -u[flip]
+            p = (pos[todo, t - 1] + bond * u) % dim
+            d, idx = tree.query(p, k=3)
+            # neighbours that are the chain's own last two beads do not count
+            own = (idx // t == todo[:, None]) & (idx % t >= t - 2)
+            dmin = np.where(own, np.inf, d).min(1)
+            ok = dmin >= 0.25
+            cand[todo[ok]] = p[ok]
+            prev[todo[ok]] = u[ok]
+            if _try == 19:
+                cand[todo[~ok]] = p[~ok]
+                prev[todo[~ok]] = u[~ok]
+            todo = todo[~ok]
+            if len(todo) == 0:
+                break
+        pos[:, t] = cand
+    xb = pos.reshape(-1, 3) % dim
+    tb = rng.integers(0, nbt, size=len(xb)).astype(np.int32) + 2
+    qb = rng.normal(0.0, 0.3, size=(nchains, length))
+    qb -= qb.mean(1, keepdims=True)
+    qb = qb.reshape(-1)
+    # --- water on a grid, away from the beads
+    spacing = (1.0 / 33.4) ** (1.0 / 3.0)
+    nsite = np.maximum(1, np.round(dim / spacing)).astype(int)
+    sites = np.stack(np.meshgrid(*[np.arange(n) for n in nsite], indexing="ij"), -1).reshape(-1, 3)
+    sites = (sites + 0.5) * (dim / nsite) + rng.normal(0.0, 0.01, (len(sites), 3))
+    sites = sites % dim
+    d, _ = cKDTree(xb, boxsize=dim).query(sites, k=1)
+    sites = sites[d >= gap]
+    sites = sites[rng.permutation(len(sites))[:nwater]]
+    nw = len(sites)
+    rot = _random_rotations(rng, nw)
+    hh = 0.1 * math.sin(math.radians(109.47) / 2.0)
+    hz = 0.1 * math.cos(math.radians(109.47) / 2.0)
+    h1 = np.einsum("mij,j->mi", rot, np.array([hh, 0.0, hz]))
+    h2 = np.einsum("mij,j->mi", rot, np.array([-hh, 0.0, hz]))
+    xw = np.stack([sites, sites + h1, sites + h2], 1).reshape(-1, 3)
+    tw = np.tile(np.array([0, 1, 1], np.int32), nw)
+    qw = np.tile(np.array([-0.8476, 0.4238, 0.4238]), nw)
+    x = np.concatenate([xw, xb])
+    typ = np.concatenate([tw, tb]).astype(np.int32)
+    q = np.concatenate([qw, qb]) * QSCALE
+    nwa = 3 * nw
+    # --- exclusions and constraints
+    k = np.arange(nw) * 3
+    ex = [np.stack([k, k + 1], 1), np.stack([k, k + 2], 1), np.stack([k + 1, k + 2], 1)]
+    b0 = nwa + np.arange(nchains)[:, None] * length
+    i1 = (b0 + np.arange(length - 1)[None, :]).reshape(-1)
+    i2 = (b0 + np.arange(length - 2)[None, :]).reshape(-1)
+    ex += [np.stack([i1, i1 + 1], 1), np.stack([i2, i2 + 2], 1)]
+    hhd = 2.0 * 0.1 * math.sin(math.radians(109.47) / 2.0)
+    rig = np.stack([np.stack([k, k + 1, np.full(nw, 0.1)], 1), np.stack([k, k + 2, np.full(nw, 0.1)], 1),
+                    np.stack([k + 1, k + 2, np.full(nw, hhd)], 1)], 1).reshape(-1, 3)
+    # --- potentials: LJ among O and the bead types (Lorentz-Berthelot), none for H
+    sig = np.concatenate([[0.3166], sig_b])
+    eps = np.concatenate([[0.650], eps_b])
+    lj_types = [0] + list(range(2, 2 + nbt))
+    pots = []
+    for a_i, ti in enumerate(lj_types):
+        for b_i in range(a_i, len(lj_types)):
+            e_ij, s_ij = lb_mix(eps[a_i], sig[a_i], eps[b_i], sig[b_i])
+            pots.append(PotSpec(KIND_LJ126, ti, lj_types[b_i], 0.2, cutoff, tol, (*lj_AB(e_ij, s_ij), 0.0, 0.0)))
+    ep = PotSpec(KIND_COULOMB, 0, 0, 0.05, cutoff, tol, (1.0, 0.0, 0.0, 0.0))
+    masses = [15.9994, 1.008] + list(rng.uniform(12.0, 44.0, nbt))
+    return System(name=f"chains-water-{len(x)}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
+                  masses=masses, charges=[0.0] * len(masses), pots=pots, x=_wrap(x, dim), type=typ,
+                  excl=np.concatenate(ex).astype(np.int32), dt=0.002, rigid=rig, q=q, ep=ep)

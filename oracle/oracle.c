@@ -13,8 +13,11 @@
  *     r2 = (dx0^2 + dx1^2) + dx2^2), is <= cutoff^2 with a potential for the two types
  *     (src/runner_dopair.c:640-642, 954-955).  The cut is the float cutoff squared in float
  *     for pair tasks (src/runner_dopair.c:578-579) and the float of the double square for
- *     self tasks (src/runner_dopair.c:896).  The sorted sweep of the reference is a pruned
- *     walk over exactly this set, so the oracle enumerates it by brute force;
+ *     self tasks (src/runner_dopair.c:896).  For cubic cells the sorted sweep of the
+ *     reference is a pruned walk over exactly this set, so the oracle enumerates it by brute
+ *     force.  (For non-cubic cells the reference's sweep bound, the norm of the cell shift
+ *     instead of its projection on the sort axis, src/runner_dopair.c:593-597, skips some
+ *     pairs of this set; the engine uses the projection there and keeps them);
  *   - exclusions: excluded pairs are removed from the set (src/exclusion.c:81-295 subtracts
  *     them after the sweep, which is the same sum) and counted;
  *   - potential evaluation: the interval index is computed in float exactly as
@@ -22,7 +25,11 @@
  *     polynomial, the distance, the force and all sums are then evaluated in double
  *     (src/potential_eval.h:84-103 restated in FP64);
  *   - sort keys: src/runner_dosort.c:140-153, ordered by descending distance with ties in
- *     storage order.
+ *     storage order;
+ *   - explicit electrostatics (the engine_setexplepot extension; the reference stores ep,
+ *     src/engine.c:1029-1053, but no runner evaluates it): with table ep, every pair within
+ *     the cutoff that is not excluded also contributes q_i q_j ep(r) to energy and force,
+ *     and a pair whose types have no potential is in the set when ep is given.
  *
  * Compile with -ffp-contract=off: the float steps must round like the reference build.
  */
@@ -96,7 +103,8 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                    unsigned period, int mt, const int *potidx, const float *coef, const float *alpha,
                    const int *coff, const int *potn, int nexcl, const int *excl,
                    double *f_out, double *epot_out, double *epot_abs_out, double *virial_out,
-                   double *virial_abs_out, long long *npairs_out, long long *nexcl_out) {
+                   double *virial_abs_out, long long *npairs_out, long long *nexcl_out, const double *q,
+                   int ep) {
     const int ncells = cdim[0] * cdim[1] * cdim[2];
     double h[3];
     int span[3];
@@ -180,15 +188,22 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
                                     float dxf[3] = {pix[0] - xj[0], pix[1] - xj[1], pix[2] - xj[2]};
                                     float r2f = dxf[0] * dxf[0] + dxf[1] * dxf[1] + dxf[2] * dxf[2];
                                     int pot = potidx[type[pi] * mt + type[pj]];
-                                    if (pot < 0 || r2f > cut2) continue;
+                                    if ((pot < 0 && ep < 0) || r2f > cut2) continue;
                                     if (nexcl > 0 && is_excluded(ekeys, nexcl, pi, pj)) { nex++; continue; }
                                     double dx[3], r2 = 0.0;
                                     for (int q = 0; q < 3; q++) {
                                         dx[q] = ((double)xi[q] - (double)shift[q]) - (double)xj[q];
                                         r2 += dx[q] * dx[q];
                                     }
-                                    double r = sqrt(r2), e, fs;
-                                    eval_fp64(coef + coff[pot], alpha + 4 * pot, potn[pot], r2f, r, &e, &fs);
+                                    double r = sqrt(r2), e = 0.0, fs = 0.0;
+                                    if (pot >= 0)
+                                        eval_fp64(coef + coff[pot], alpha + 4 * pot, potn[pot], r2f, r, &e, &fs);
+                                    if (ep >= 0) {
+                                        double ee, fe, qq = q[pi] * q[pj];
+                                        eval_fp64(coef + coff[ep], alpha + 4 * ep, potn[ep], r2f, r, &ee, &fe);
+                                        e += qq * ee;
+                                        fs += qq * fe;
+                                    }
                                     for (int q = 0; q < 3; q++) {
                                         double w = fs * dx[q];
                                         f_out[3 * pi + q] -= w;

@@ -33,7 +33,7 @@ def lib():
                                      P(C.c_int), C.c_double, C.c_uint, C.c_int, P(C.c_int), P(C.c_float),
                                      P(C.c_float), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int), P(C.c_double),
                                      P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_longlong),
-                                     P(C.c_longlong)]
+                                     P(C.c_longlong), P(C.c_double), C.c_int]
         L.oracle_rigid.restype = C.c_int
         L.oracle_rigid.argtypes = [C.c_int] + [C.c_void_p] * 14 + [C.c_double, C.c_double, C.c_int, C.c_int,
                                                                     C.c_void_p]
@@ -60,14 +60,17 @@ def bin_system(sysm):
 
 
 def pack_tables(sysm, tables):
-    """tables[k] = (n, alpha[4] float32, coef[(n+1)*8] float32) for sysm.pots[k]."""
+    """tables[k] = (n, alpha[4] float32, coef[(n+1)*8] float32) for sysm.pots[k], then, for a
+    system with explicit electrostatics (sysm.ep), the table of sysm.ep last."""
     mt = len(sysm.masses)
     potidx = -np.ones((mt, mt), np.int32)
     coef, alpha, coff, potn = [], [], [], []
     off = 0
-    for k, (spec, (n, a, c)) in enumerate(zip(sysm.pots, tables)):
-        potidx[spec.ti, spec.tj] = k
-        potidx[spec.tj, spec.ti] = k
+    for k, (n, a, c) in enumerate(tables):
+        if k < len(sysm.pots):
+            spec = sysm.pots[k]
+            potidx[spec.ti, spec.tj] = k
+            potidx[spec.tj, spec.ti] = k
         coef.append(np.asarray(c, np.float32))
         alpha.append(np.asarray(a, np.float32)[:4])
         coff.append(off)
@@ -94,13 +97,17 @@ def nonbond(sysm, tables, binned=None):
     dim = np.ascontiguousarray(sysm.dim, np.float64)
     cdim = np.ascontiguousarray(b["cdim"], np.int32)
     excl = np.ascontiguousarray(sysm.excl, np.int32).reshape(-1)
+    ep = len(sysm.pots) if getattr(sysm, "ep", None) is not None else -1
+    if ep >= 0 and len(tables) != len(sysm.pots) + 1:
+        raise ValueError("a system with explicit electrostatics needs the ep table after the type tables")
+    q = np.ascontiguousarray(sysm.q if getattr(sysm, "q", None) is not None else np.zeros(N), np.float64)
     rc = lib().oracle_nonbond(N, _p(xrel, C.c_float), _p(cell, C.c_int), _p(typ, C.c_int), _p(org, C.c_double),
                               _p(dim, C.c_double), _p(cdim, C.c_int), float(sysm.cutoff), sysm.period,
                               len(sysm.masses), _p(t["potidx"], C.c_int), _p(t["coef"], C.c_float),
                               _p(t["alpha"], C.c_float), _p(t["coff"], C.c_int), _p(t["potn"], C.c_int),
                               len(sysm.excl), _p(excl, C.c_int) if excl.size else None, _p(f, C.c_double),
                               C.byref(epot), C.byref(eabs), C.byref(vir), C.byref(vabs), C.byref(npairs),
-                              C.byref(nex))
+                              C.byref(nex), _p(q, C.c_double) if ep >= 0 else None, ep)
     if rc != 0:
         raise RuntimeError("oracle_nonbond failed")
     return dict(f=f, epot=epot.value, epot_abs=eabs.value, virial=vir.value, virial_abs=vabs.value,

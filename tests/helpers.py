@@ -22,6 +22,14 @@ def load_golden(fname):
     return sysm, ref
 
 
+def tables_of(sysm):
+    """The library's tables of a system's potentials, in oracle order (type tables, then the
+    explicit electrostatic potential's, if any)."""
+    import mdcore_b200 as M
+    specs = list(sysm.pots) + ([sysm.ep] if getattr(sysm, "ep", None) is not None else [])
+    return [M.create_potential(p).contents.table() for p in specs]
+
+
 def force_errors(f, f_ref):
     """Error metrics of forces f against f_ref (both N x 3, by particle id)."""
     d = np.linalg.norm(f - f_ref, axis=1)
