@@ -68,6 +68,10 @@ def _slab(W):
     return s
 
 
+def _chains(W):
+    return W.chains_water()
+
+
 def _replicas(W):
     import numpy as np
     out = W.argon_replicas()
@@ -88,7 +92,14 @@ WORKLOADS = {
     "replicas": ("512 LJ argon replicas, N log-uniform 500-8,000 (1,451,403 atoms in all), density 18-24 "
                  "atoms/nm^3, cubic periodic boxes, cutoff 1.0 nm, 80-140 K, dt 5 fs, seeded; one batch",
                  _replicas, "sweep_replicas512_traffic.txt"),
+    "chains": ("solvated chains, 92,200 atoms: 220 chains of 100 beads (20 LJ types, Lorentz-Berthelot, "
+               "charges N(0, 0.3) e neutralised per chain, 1-2 and 1-3 exclusions) and 23,400 3-site waters in "
+               "a 10.8 x 10.8 x 7.8 nm box (9 x 9 x 6 cells), cutoff 1.2 nm, 231 type tables and explicit "
+               "electrostatics, seeded; force evaluation only (the chains' bonded terms are not built)",
+               _chains, "sweep_chains92k_traffic.txt"),
 }
+# workloads whose bench step is a force evaluation (no trajectory can be run)
+FORCE_ONLY = {"chains"}
 SELECTED = "water"
 
 
@@ -203,6 +214,10 @@ def reference_arm(args, rank):
     the reference sources) on the same workload, all host threads."""
     if rank != 0:
         return
+    if SELECTED in FORCE_ONLY:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no per-particle charges "
+                          "(engine_setexplepot is stored but never evaluated), so it cannot run this system"}))
+        return
     built = build_system()
     systems = built if isinstance(built, list) else [built]
     threads = host_threads()
@@ -292,6 +307,75 @@ def timed_resident_steps(tgt, stream, flush, steps, torch):
     return tot / steps, sweep / steps, info.pairs - p0
 
 
+def force_only_line(args, rank, world, local_rank, M, tgt, engines, systems, st, pairs, fe_ms, fe_sweep, fe_e2e,
+                    h2d, d2h, ncells, compact, warps, layout, stages, occupancy, tune_ms, clocks, stream, flush,
+                    barrier, torch, dist):
+    """The JSON line of a workload whose step is one force evaluation (sort + sweep): value
+    device-resident, e2e engine_nonbond_cuda with host buffers, plain the plain form."""
+    tgt.graph(False)
+    tgt.tune(0, plain=True)
+    tgt.load_parts()
+    tgt.resident()
+    barrier()
+    plain_ms, plain_sweep = timed_force_evals(tgt, stream, flush, args.steps, torch)
+    barrier()
+    clk = clocks.stop()
+    if tgt.stats().status != 0:
+        raise SystemExit("bench.py: device status after the plain evaluations")
+    if dist is not None:
+        t = torch.tensor([fe_ms, fe_e2e, fe_sweep, plain_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fe_ms, fe_e2e, fe_sweep, plain_ms = [float(v) for v in t.tolist()]
+    if rank == 0:
+        peak = M.fp32_peak_tflops(local_rank)
+        achieved = FLOPS_PER_PAIR * pairs / (fe_sweep * 1e-3) / 1e12
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", WORKLOADS[SELECTED][2])
+        if os.path.exists(prof):
+            for ln in open(prof):
+                if ln.startswith("dram_bytes_per_launch"):
+                    traffic = int(ln.split()[1])
+        # engine_nonbond_cuda's copies: positions+types and ids per padded slot and the cell
+        # offsets/counts up; float forces per slot, cell energies/virials, counters down
+        slots = sum(int((((cell_counts(s, e) + 3) // 4) * 4).sum()) for s, e in zip(systems, engines))
+        fe_h2d, fe_d2h = 20 * slots + 4 * (2 * ncells + 1), 12 * slots + 16 * ncells + 64
+        line = {
+            "metric": METRIC, "value": world * pairs / (fe_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": fe_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "ns_per_day": None,
+            "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
+                       "pairs_per_step": pairs, "candidates_per_step": int(st.candidates), "tasks": tgt.ntasks(),
+                       "cells": ncells, "parallelism": f"replicas x{world}",
+                       "step": "one force evaluation: sort + sweep (engine_nonbond_cuda_resident)",
+                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
+                                  "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
+                                  "cuda_graph": True},
+                       "l2": "256 MiB write before every timed step (outside the timed events)"},
+            "e2e": {"value": world * pairs / (fe_e2e * 1e-3), "unit": UNIT, "ms_per_step": fe_e2e,
+                    "h2d_bytes_per_step": fe_h2d, "d2h_bytes_per_step": fe_d2h,
+                    "what": "engine_nonbond_cuda with host buffers: positions and ids up, forces and energies down"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": fe_sweep,
+                         "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
+                                        "MEASURED_PEAKS.json has no FP32 figure"},
+            "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms, "sweep_ms": plain_sweep,
+                      "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
+            "gpu_launches": (2 + 3 * int(compact)) * args.steps,
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": "not run: the reference has no per-particle charges (engine_setexplepot "
+                                              "is stored but never evaluated), so it cannot run this system"}
+        print(json.dumps(line))
+    tgt.close()
+    for e in engines:
+        e.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -369,6 +453,12 @@ def ours(args, rank, world, local_rank):
         ev1.synchronize()
         fe_e2e += ev0.elapsed_time(ev1) / args.steps
     barrier()
+
+    if SELECTED in FORCE_ONLY:
+        force_only_line(args, rank, world, local_rank, M, tgt, engines, systems, st, fe_pairs, fe_ms, fe_sweep,
+                        fe_e2e, h2d, d2h, ncells, compact, warps, layout, stages, occupancy, tune_ms, clocks, stream,
+                        flush, barrier, torch, dist)
+        return
 
     # ---- MD steps resident in HBM: the headline value
     tgt.resident_begin()
