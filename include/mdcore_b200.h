@@ -136,6 +136,11 @@ struct part {
     unsigned short int flags;
 } __attribute__((aligned(64)));
 
+/* src/bond.h:31-36: a bond between particles i and j (ids). */
+struct bond {
+    int i, j;
+};
+
 /* src/part.h:73-88 */
 struct part_type {
     int id;
@@ -182,6 +187,8 @@ struct potential *potential_create_LJ126_Ewald(double a, double b, double A, dou
 struct potential *potential_create_LJ126_Coulomb(double a, double b, double A, double B, double q, double tol);
 struct potential *potential_create_Ewald(double a, double b, double q, double kappa, double tol);
 struct potential *potential_create_Coulomb(double a, double b, double q, double tol);
+/* src/potential.c:301-322: harmonic bond K (r - r0)^2 on [a, b]. */
+struct potential *potential_create_harmonic(double a, double b, double K, double r0, double tol);
 void potential_clear(struct potential *p);
 /* Scalar host evaluation, src/potential_eval.h:67-104. */
 void potential_eval(struct potential *p, float r2, float *e, float *f);
@@ -296,6 +303,10 @@ struct engine {
     int part2rigid_size;    /* entries of part2rigid */
     int rigids_gen;         /* bumped by every engine_rigid_add */
     struct potential *ep;   /* explicit electrostatics (engine_setexplepot), or NULL */
+    struct bond *bonds;     /* engine_bond_add */
+    int nr_bonds, bonds_size;
+    struct potential **p_bond;   /* max_type x max_type bond potentials (engine_bond_addpot) */
+    int bonds_gen;          /* bumped by every engine_bond_add / engine_bond_addpot */
 };
 
 /* src/engine.c:2439-2591 */
@@ -325,6 +336,15 @@ int engine_rigid_add(struct engine *e, int pid, int pjd, double d);
  * so that q in units of e * sqrt(4 pi * 138.935458) gives kJ/mol.  Call before
  * engine_start. */
 int engine_setexplepot(struct engine *e, struct potential *ep);
+/* src/engine_bonded.c:2086-2102: the bond potential of type pair (i, j) (symmetric). */
+int engine_bond_addpot(struct engine *e, struct potential *p, int i, int j);
+/* src/engine_bonded.c:1447-1475: a bond between particles i and j.  Bonds are evaluated
+ * as bond_eval does (src/bond.c:81-250: the potential of the two particles' types, the
+ * distance from the cell-relative positions and the cells' periodic offset, r^2 held to
+ * the table's range [a^2, b^2]) by engine_step (the device step) and the device-resident
+ * steps, into the same fixed-point forces as the nonbonded sweep; their energy goes to
+ * e->s.epot_bond.  engine_step_host returns engine_err_nyi for an engine with bonds. */
+int engine_bond_add(struct engine *e, int i, int j);
 /* src/engine.c:1674-1826 */
 int engine_start(struct engine *e, int nr_runners, int nr_queues);
 /* src/engine.c:2070-2240.  One time step (re-binning, forces, symplectic Euler, rigid

@@ -405,6 +405,7 @@ int engine_step(struct engine *e) {
  * evaluation and constraints through host buffers. */
 int engine_step_host(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
+    if (e->nr_bonds > 0) return engine_error(engine_err_nyi);   /* bonds: device steps only */
     struct space *s = &e->s;
     e->time += 1;
     if (space_shuffle(s) < 0) return engine_error(engine_err_space);
@@ -431,6 +432,8 @@ int engine_finalize(struct engine *e) {
     free(e->exclusions);
     free(e->rigids);
     free(e->part2rigid);
+    free(e->bonds);
+    free(e->p_bond);
     memset(e, 0, sizeof(struct engine));
     return engine_err_ok;
 }
@@ -444,6 +447,35 @@ int engine_setexplepot(struct engine *e, struct potential *ep) {
         e->flags &= ~engine_flag_explepot;
         e->ep = NULL;
     }
+    return engine_err_ok;
+}
+
+int engine_bond_addpot(struct engine *e, struct potential *p, int i, int j) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (i < 0 || i >= e->max_type || j < 0 || j >= e->max_type) return engine_error(engine_err_range);
+    if (e->p_bond == NULL) {
+        e->p_bond = calloc((size_t)e->max_type * e->max_type, sizeof(struct potential *));
+        if (e->p_bond == NULL) return engine_error(engine_err_malloc);
+    }
+    e->p_bond[i * e->max_type + j] = p;
+    if (i != j) e->p_bond[j * e->max_type + i] = p;
+    e->bonds_gen++;
+    return engine_err_ok;
+}
+
+int engine_bond_add(struct engine *e, int i, int j) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (e->nr_bonds == e->bonds_size) {
+        int nsize = e->bonds_size ? 2 * e->bonds_size : 100;
+        struct bond *nb = realloc(e->bonds, sizeof(struct bond) * nsize);
+        if (nb == NULL) return engine_error(engine_err_malloc);
+        e->bonds = nb;
+        e->bonds_size = nsize;
+    }
+    e->bonds[e->nr_bonds].i = i;
+    e->bonds[e->nr_bonds].j = j;
+    e->nr_bonds += 1;
+    e->bonds_gen++;
     return engine_err_ok;
 }
 

@@ -19,6 +19,7 @@
 // written out of bounds.
 #pragma once
 #include "nb_device.cuh"
+#include "nb_kernels.cuh"
 
 namespace nb {
 
@@ -215,6 +216,68 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
         xq[s] = x;
         v[s] = vv;
     }
+}
+
+// Bonds (bond_eval, src/bond.c:81-250) of the particles in the device cells: one thread per
+// bond, the two particles found through slot_of, the distance from their cell-relative
+// positions and the periodic offset of their cells (held to -1..1), r^2 held to the table's
+// [a^2, b^2]; the pair force goes into the fixed-point accumulators like the sweep's, the
+// energy into a fixed-point sum per engine.
+struct BondArgs {
+    const int4* bonds;           // global id i, global id j, bond table, engine
+    int nbonds;
+    const float* coef;           // bond tables, the sweep's format
+    const float4* potinfo;
+    const int* potn;
+    const double2* ab2;          // per table: a^2, b^2
+    const int* slot_of;
+    const float4* xq;
+    unsigned long long* force;
+    const int* eng_cell0;        // per engine: first global cell, cell grid, cell edge
+    const int4* eng_cdim;
+    const double4* eng_h;
+    int capc;
+    unsigned long long* ebond;   // per engine, 2^32 units per kJ/mol
+    unsigned long long* acc;     // status bits
+    const unsigned long long* abort;
+};
+
+__global__ void __launch_bounds__(128) bond_forces(BondArgs B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B.nbonds || (B.abort != nullptr && *(const volatile unsigned long long*)B.abort != 0)) return;
+    const int4 b = B.bonds[t];
+    const int si = B.slot_of[b.x], sj = B.slot_of[b.y];
+    const float4 xi = B.xq[si], xj = B.xq[sj];
+    const int4 cd = B.eng_cdim[b.w];
+    const double4 h = B.eng_h[b.w];
+    const int ci = si / B.capc - B.eng_cell0[b.w], cj = sj / B.capc - B.eng_cell0[b.w];
+    const int li[3] = {ci / (cd.y * cd.z), (ci / cd.z) % cd.y, ci % cd.z};
+    const int lj[3] = {cj / (cd.y * cd.z), (cj / cd.z) % cd.y, cj % cd.z};
+    const double hh[3] = {h.x, h.y, h.z};
+    const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
+    float dx[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        int sh = li[k] - lj[k];
+        if (sh > 1) sh = -1;
+        else if (sh < -1) sh = 1;
+        const float pix = (float)((double)xiv[k] + hh[k] * sh);
+        dx[k] = __fsub_rn(pix, xjv[k]);
+    }
+    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx[0], dx[0]), __fmul_rn(dx[1], dx[1])), __fmul_rn(dx[2], dx[2]));
+    const double2 ab2 = B.ab2[b.z];
+    if ((double)r2 < ab2.x || (double)r2 > ab2.y) r2 = (float)fmax(ab2.x, fmin(ab2.y, (double)r2));
+    float e, f;
+    unsigned status = 0;
+    eval_table(B.coef, B.potinfo[b.z], B.potn[b.z], r2, e, f, status);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float w = f * dx[k];
+        atomic_add_fixed(B.force + 3 * (size_t)si + k, to_fixed(-w, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sj + k, to_fixed(w, status));
+    }
+    atomicAdd(&B.ebond[b.w], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
+    if (status) atomicOr(&B.acc[kAccStatus], (unsigned long long)status);
 }
 
 // Cell offsets of the compacted download: an exclusive scan of min(count, capc) over the

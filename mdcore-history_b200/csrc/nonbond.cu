@@ -148,6 +148,19 @@ struct NbState {
     float4* h_up = nullptr;            // uploads: positions, velocities
     int *r_dpid = nullptr, *h_dpid = nullptr, *h_uppid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
     int* r_bsum = nullptr;                   // block sums of the count scan
+    // Bonds of the resident steps (built with the device blocks).
+    int nbonds = 0;
+    long long bonds_key = -1;              // sum of the engines' bonds_gen the bonds were built from
+    int4* r_bonds = nullptr;
+    float* r_bcoef = nullptr;
+    float4* r_bpotinfo = nullptr;
+    int* r_bpotn = nullptr;
+    double2* r_bab2 = nullptr;
+    int* r_eng_cell0 = nullptr;
+    int4* r_eng_cdim = nullptr;
+    double4* r_eng_h = nullptr;
+    unsigned long long* r_ebond = nullptr;   // per engine
+    unsigned long long* h_ebond = nullptr;
     unsigned long long* h_words = nullptr;   // status, completed steps, their pairs (pinned)
     std::vector<long long> res_engine_n;   // particles of each engine on the device
     std::vector<float> id_q;
@@ -1244,6 +1257,23 @@ void res_free(NbState* st) {
     if (st->h_rcount) cudaFreeHost(st->h_rcount);
     if (st->h_up) cudaFreeHost(st->h_up);
     if (st->h_words) cudaFreeHost(st->h_words);
+    {
+        void* bdev[] = {st->r_bonds, st->r_bcoef, st->r_bpotinfo, st->r_bpotn, st->r_bab2, st->r_eng_cell0,
+                        st->r_eng_cdim, st->r_eng_h, st->r_ebond};
+        for (void* p : bdev) cudaFree(p);
+        if (st->h_ebond) cudaFreeHost(st->h_ebond);
+        st->r_bonds = nullptr;
+        st->r_bcoef = nullptr;
+        st->r_bpotinfo = nullptr;
+        st->r_bpotn = nullptr;
+        st->r_bab2 = nullptr;
+        st->r_eng_cell0 = nullptr;
+        st->r_eng_cdim = nullptr;
+        st->r_eng_h = nullptr;
+        st->r_ebond = nullptr;
+        st->h_ebond = nullptr;
+        st->nbonds = 0;
+    }
     if (st->r_bsum) cudaFree(st->r_bsum);
     st->h_words = nullptr;
     st->r_bsum = nullptr;
@@ -1328,6 +1358,81 @@ ResidentCells res_cells(const NbState* st) {
 constexpr int kCellWarps = 2;
 constexpr int kCellThreads = 32 * kCellWarps;
 int res_grid(const NbState* st) { return (st->ncells + kCellWarps - 1) / kCellWarps; }
+
+// The engines' bonds for the device: global ids, the bond table of the two particles' types
+// (bonds whose types have none are dropped, as bond_eval skips them), the engine; the
+// distinct bond tables; per engine its first cell, cell grid and cell edge.
+long long res_bonds_key(const NbState* st) {
+    long long k = 0;
+    for (struct engine* e : st->engines) k += e->bonds_gen;
+    return k;
+}
+
+int res_build_bonds(NbState* st) {
+    const int ne = (int)st->engines.size();
+    st->bonds_key = res_bonds_key(st);
+    std::vector<int4> bonds;
+    std::vector<struct potential*> uniq;
+    for (int k = 0; k < ne; k++) {
+        struct engine* e = st->engines[k];
+        if (e->nr_bonds == 0 || e->p_bond == nullptr) continue;
+        const int mt = e->max_type;
+        for (int b = 0; b < e->nr_bonds; b++) {
+            const int i = e->bonds[b].i, j = e->bonds[b].j;
+            if (i < 0 || j < 0 || i >= e->s.nr_parts || j >= e->s.nr_parts) continue;
+            const struct part *pi = e->s.partlist[i], *pj = e->s.partlist[j];
+            if (pi == nullptr || pj == nullptr) continue;
+            struct potential* pot = e->p_bond[pj->type * mt + pi->type];
+            if (pot == nullptr) continue;
+            int u = 0;
+            while (u < (int)uniq.size() && uniq[u] != pot) u++;
+            if (u == (int)uniq.size()) uniq.push_back(pot);
+            bonds.push_back(make_int4(st->id_off[k] + i, st->id_off[k] + j, u, k));
+        }
+    }
+    st->nbonds = (int)bonds.size();
+    if (st->nbonds == 0) return 0;
+    std::vector<float> coef;
+    std::vector<float4> info;
+    std::vector<int> potn;
+    std::vector<double2> ab2;
+    for (struct potential* p : uniq) {
+        const int off = (int)coef.size();
+        coef.insert(coef.end(), p->c, p->c + (size_t)(p->n + 1) * potential_chunk);
+        info.push_back(make_float4(p->alpha[0], p->alpha[1], p->alpha[2], bits_as_float(off | (p->n << 20))));
+        potn.push_back(p->n);
+        ab2.push_back(make_double2(p->a * p->a, p->b * p->b));
+    }
+    std::vector<int> cell0(ne);
+    std::vector<int4> cdim(ne);
+    std::vector<double4> h(ne);
+    for (int k = 0; k < ne; k++) {
+        const struct space* sp = &st->engines[k]->s;
+        cell0[k] = st->cell_off[k];
+        cdim[k] = make_int4(sp->cdim[0], sp->cdim[1], sp->cdim[2], 0);
+        h[k] = make_double4(sp->h[0], sp->h[1], sp->h[2], 0.0);
+    }
+    CU(cudaMalloc(&st->r_bonds, sizeof(int4) * bonds.size()));
+    CU(cudaMalloc(&st->r_bcoef, sizeof(float) * coef.size()));
+    CU(cudaMalloc(&st->r_bpotinfo, sizeof(float4) * info.size()));
+    CU(cudaMalloc(&st->r_bpotn, sizeof(int) * potn.size()));
+    CU(cudaMalloc(&st->r_bab2, sizeof(double2) * ab2.size()));
+    CU(cudaMalloc(&st->r_eng_cell0, sizeof(int) * ne));
+    CU(cudaMalloc(&st->r_eng_cdim, sizeof(int4) * ne));
+    CU(cudaMalloc(&st->r_eng_h, sizeof(double4) * ne));
+    CU(cudaMalloc(&st->r_ebond, sizeof(unsigned long long) * ne));
+    CU(cudaMallocHost(&st->h_ebond, sizeof(unsigned long long) * ne));
+    CU(cudaMemset(st->r_ebond, 0, sizeof(unsigned long long) * ne));
+    CU(cudaMemcpy(st->r_bonds, bonds.data(), sizeof(int4) * bonds.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_bcoef, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_bpotinfo, info.data(), sizeof(float4) * info.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_bpotn, potn.data(), sizeof(int) * potn.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_bab2, ab2.data(), sizeof(double2) * ab2.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_eng_cell0, cell0.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_eng_cdim, cdim.data(), sizeof(int4) * ne, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(st->r_eng_h, h.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
+    return 0;
+}
 
 // Largest cell of the engines' host cells and the particle count.
 int res_host_counts(const NbState* st, long long* n) {
@@ -1421,7 +1526,7 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     st->id_flags.assign(nid, 0);
     st->id_present.assign(nid, 0);
     st->res_active = true;
-    return 0;
+    return res_build_bonds(st);
 }
 
 // Pipeline chunks of a transfer of np particles: one per 256k particles, 1 to 8 (every
@@ -1552,7 +1657,7 @@ int res_issue_step(NbState* st) {
     for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
     rebin_gather<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
                                                st->r_pid[o], st->r_cnt[o], st->r_status,
-                                               rigid ? st->r_slot_of : nullptr);
+                                               (rigid || st->nbonds > 0) ? st->r_slot_of : nullptr);
     CU(cudaGetLastError());
     DevView V;
     V.xq = st->r_xq[o];
@@ -1567,6 +1672,28 @@ int res_issue_step(NbState* st) {
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
     rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
+    if (st->nbonds > 0) {              // the bonds' forces join the sweep's before the update
+        CU(cudaMemsetAsync(st->r_ebond, 0, sizeof(unsigned long long) * st->engines.size(), st->stream));
+        BondArgs B;
+        B.bonds = st->r_bonds;
+        B.nbonds = st->nbonds;
+        B.coef = st->r_bcoef;
+        B.potinfo = st->r_bpotinfo;
+        B.potn = st->r_bpotn;
+        B.ab2 = st->r_bab2;
+        B.slot_of = st->r_slot_of;
+        B.xq = st->r_xq[o];
+        B.force = st->r_force;
+        B.eng_cell0 = st->r_eng_cell0;
+        B.eng_cdim = st->r_eng_cdim;
+        B.eng_h = st->r_eng_h;
+        B.capc = st->capc;
+        B.ebond = st->r_ebond;
+        B.acc = st->d_acc;
+        B.abort = st->r_status;
+        bond_forces<<<(st->nbonds + 127) / 128, 128, 0, st->stream>>>(B);
+        CU(cudaGetLastError());
+    }
     const unsigned slot_blocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
     integrate_cells<<<slot_blocks, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine, st->r_engine_dt,
                                                   st->r_engine_imass, st->max_type, st->r_xq[o], st->r_v[o],
@@ -1744,6 +1871,9 @@ int res_download(NbState* st, unsigned long long* status) {
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
+    if (st->nbonds > 0)
+        CU(cudaMemcpyAsync(st->h_ebond, st->r_ebond, sizeof(unsigned long long) * ne, cudaMemcpyDeviceToHost,
+                           st->stream));
     for (struct engine* e : st->engines)
         if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream, 0);
 
@@ -1835,7 +1965,11 @@ int res_download(NbState* st, unsigned long long* status) {
     }
     st->res_dirty = false;
     rc = finish_stats(st);
-    for (struct engine* e : st->engines) e->s.epot += e->s.epot_nonbond;
+    for (int k = 0; k < ne; k++) {
+        struct space* sp = &st->engines[k]->s;
+        if (st->nbonds > 0) sp->epot_bond = (double)(long long)st->h_ebond[k] / kEnergyScale;
+        sp->epot += sp->epot_nonbond + sp->epot_bond;
+    }
     return rc;
 }
 
@@ -2044,7 +2178,8 @@ int st_step_device(NbState* st) {
     for (int attempt = 0;; attempt++) {
         long long n = 0;
         const int maxc = res_host_counts(st, &n);
-        if (st->res_active && n == st->res_nparts && maxc + 4 <= st->capc && st->mcap >= mcap) {
+        if (st->res_active && n == st->res_nparts && maxc + 4 <= st->capc && st->mcap >= mcap &&
+            st->bonds_key == res_bonds_key(st)) {
             rc = res_upload(st);
         } else {
             rc = st_resident_begin(st, margin, mcap);
@@ -2192,6 +2327,8 @@ extern "C" int engine_batch_step(struct engine_batch* b) {
 extern "C" int engine_batch_step_host(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
     NbState* st = bstate(b);
+    for (struct engine* e : st->engines)
+        if (e->nr_bonds > 0) return engine_err = engine_err_nyi;     // bonds: device steps only
     for (struct engine* e : st->engines) {
         e->time += 1;
         if (space_shuffle(&e->s) < 0) return engine_err = engine_err_space;

@@ -550,6 +550,19 @@ struct potential *potential_create_LJ126_switch(double a, double b, double A, do
     P.A = A; P.B = B; P.s = s; P.b = b;
     return create(f_ljsw, fp_ljsw, f6_ljsw, a, b, tol, potential_flag_LJ126);
 }
+static struct { double K, r0; } H;
+static double f_harm(double r) { return H.K * (r - H.r0) * (r - H.r0); }
+static double f6_harm(double r) {
+    (void)r;
+    return 0.0;
+}
+
+struct potential *potential_create_harmonic(double a, double b, double K, double r0, double tol) {
+    H.K = K;
+    H.r0 = r0;
+    return create(f_harm, NULL, f6_harm, a, b, tol, potential_flag_none);
+}
+
 struct potential *potential_create_Coulomb(double a, double b, double q, double tol) {
     P.q = q; P.b = b;
     return create(f_coul, fp_coul, f6_coul, a, b, tol, potential_flag_Coulomb);

@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
         "engine_step": (C.c_int, [vp]),
         "engine_step_host": (C.c_int, [vp]),
         "engine_setexplepot": (C.c_int, [vp, P(Potential)]),
+        "engine_bond_addpot": (C.c_int, [vp, P(Potential), C.c_int, C.c_int]),
+        "engine_bond_add": (C.c_int, [vp, C.c_int, C.c_int]),
         "engine_batch_step_host": (C.c_int, [vp]),
         "engine_advance": (C.c_int, [vp]),
         "engine_finalize": (C.c_int, [vp]),
@@ -164,6 +166,7 @@ def lib() -> C.CDLL:
         "potential_create_LJ126": (P(Potential), [C.c_double] * 5),
         "potential_create_LJ126_Coulomb": (P(Potential), [C.c_double] * 6),
         "potential_create_Coulomb": (P(Potential), [C.c_double] * 4),
+        "potential_create_harmonic": (P(Potential), [C.c_double] * 5),
         "potential_create_Ewald": (P(Potential), [C.c_double] * 5),
         "potential_create_LJ126_Ewald": (P(Potential), [C.c_double] * 7),
         "errs_dump": (C.c_int, [vp]),
@@ -219,6 +222,8 @@ def create_potential(spec):
         ptr = L.potential_create_Ewald(a, b, p[0], p[1], tol)
     elif k == 5:
         ptr = L.potential_create_LJ126_Ewald(a, b, p[0], p[1], p[2], p[3], tol)
+    elif k == 7:
+        ptr = L.potential_create_harmonic(a, b, p[0], p[1], tol)
     else:
         raise ValueError(f"potential kind {k} has no library constructor")
     if not ptr:
@@ -263,6 +268,14 @@ class Engine:
             ep = create_potential(sysm.ep)
             e.pots.append(ep)
             _check(e.lib.engine_setexplepot(e.ptr, ep), "engine_setexplepot")
+        if getattr(sysm, "bonds", None) is not None and len(sysm.bonds):
+            bp = create_potential(sysm.bond_pot)
+            e.pots.append(bp)
+            bt = np.asarray(sysm.type)[np.asarray(sysm.bonds)]
+            for ti, tj in {(int(min(a, b)), int(max(a, b))) for a, b in bt}:
+                _check(e.lib.engine_bond_addpot(e.ptr, bp, ti, tj), "engine_bond_addpot")
+            for i, j in np.asarray(sysm.bonds):
+                _check(e.lib.engine_bond_add(e.ptr, int(i), int(j)), "engine_bond_add")
         e.n = sysm.n
         if sysm.rigid is not None:
             for i, j, d in np.asarray(sysm.rigid):

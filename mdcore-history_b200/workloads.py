@@ -26,6 +26,7 @@ Q_SCALE = 4.0 * math.pi * COULOMB_K        # undoes potential_escale = 1/(4 pi)
 
 # Potential kinds shared with oracle/sysfile.h.
 KIND_LJ126, KIND_LJ126_COULOMB, KIND_COULOMB, KIND_EWALD, KIND_LJ126_EWALD, KIND_COUNTER = 1, 2, 3, 4, 5, 6
+KIND_HARMONIC = 7                            # p = (K, r0): K (r - r0)^2
 
 
 @dataclasses.dataclass
@@ -59,6 +60,8 @@ class System:
     rigid: Optional[np.ndarray] = None      # (M,3) rigid constraints: id i, id j, length d (nm)
     q: Optional[np.ndarray] = None          # (N,) per-particle charges (explicit electrostatics)
     ep: Optional[PotSpec] = None            # explicit electrostatic potential (engine_setexplepot)
+    bonds: Optional[np.ndarray] = None      # (M,2) bonded particle ids
+    bond_pot: Optional[PotSpec] = None      # the bond potential of every bonded type pair
 
     @property
     def n(self) -> int:
@@ -326,7 +329,8 @@ QSCALE = math.sqrt(Q_SCALE)     # e -> per-particle charge unit of tables with p
 
 
 def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box=(10.8, 10.8, 7.8), seed: int = 0,
-                 cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12) -> System:
+                 cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12,
+                 bond_k: float = 2.0e5) -> System:
     """Heterogeneous solvated-chain system: `nchains` linear bead chains of `length` beads
     (bond 0.15 nm, 20 LJ bead types with sigma U[0.25, 0.40] nm and epsilon U[0.1, 1.0]
     kJ/mol, Lorentz-Berthelot mixing, charges N(0, 0.3) e neutralised per chain) and up to
@@ -336,7 +340,8 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     left out (0.12 nm: the 23,400 waters of the named system fit; the close contacts this
     leaves make the unrelaxed system unfit for dynamics, 0.25 nm gives a calmer one).  Charges act through explicit electrostatics (ep: the shifted Coulomb table
     with unit charge, cutoff 1.2 nm); the type tables are LJ only (none for H).  1-2 and 1-3
-    exclusions along the chains, the three intramolecular pairs of every water excluded.
+    exclusions along the chains, the three intramolecular pairs of every water excluded;
+    chain bonds harmonic, bond_k (r - 0.15 nm)^2 (bond_pot, a table on [0.05, 0.3] nm).
     Types: 0 O, 1 H, 2..21 beads.  Seeded.
 
     Chains grow together as self-avoiding random walks (every new bead at least 0.25 nm
@@ -425,6 +430,9 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
             pots.append(PotSpec(KIND_LJ126, ti, lj_types[b_i], 0.2, cutoff, tol, (*lj_AB(e_ij, s_ij), 0.0, 0.0)))
     ep = PotSpec(KIND_COULOMB, 0, 0, 0.05, cutoff, tol, (1.0, 0.0, 0.0, 0.0))
     masses = [15.9994, 1.008] + list(rng.uniform(12.0, 44.0, nbt))
+    bonds = np.stack([i1, i1 + 1], 1).astype(np.int32)
+    bond_pot = PotSpec(KIND_HARMONIC, 2, 2, 0.05, 0.3, 1e-5, (bond_k, bond, 0.0, 0.0))
     return System(name=f"chains-water-{len(x)}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
                   masses=masses, charges=[0.0] * len(masses), pots=pots, x=_wrap(x, dim), type=typ,
-                  excl=np.concatenate(ex).astype(np.int32), dt=0.002, rigid=rig, q=q, ep=ep)
+                  excl=np.concatenate(ex).astype(np.int32), dt=0.002, rigid=rig, q=q, ep=ep,
+                  bonds=bonds, bond_pot=bond_pot)

@@ -232,6 +232,48 @@ int oracle_nonbond(int N, const float *xrel, const int *cell, const int *type,
     return 0;
 }
 
+/* Bonds (src/bond.c:81-250): for each bond (i, j) with table `tab`, the position of i shifted
+ * by the periodic offset of the two cells (held to -1..1), the distance, r^2 held to
+ * [a^2, b^2] (ab2), the table's energy and force, in double (the interval index from the
+ * float r^2 as the reference computes it).  Forces added into f_out (by id), energy into
+ * *e_out. */
+int oracle_bonds(int nb, const int *bij, const float *xrel, const int *cell, const int *cdim, const double *dim,
+                 const float *coef, const float *alpha, int potn, const double *ab2, double *f_out,
+                 double *e_out) {
+    double h[3];
+    for (int k = 0; k < 3; k++) h[k] = dim[k] / cdim[k];
+    double epot = 0.0;
+    for (int b = 0; b < nb; b++) {
+        const int i = bij[2 * b], j = bij[2 * b + 1];
+        int li[3], lj[3];
+        li[0] = cell[i] / (cdim[1] * cdim[2]); li[1] = (cell[i] / cdim[2]) % cdim[1]; li[2] = cell[i] % cdim[2];
+        lj[0] = cell[j] / (cdim[1] * cdim[2]); lj[1] = (cell[j] / cdim[2]) % cdim[1]; lj[2] = cell[j] % cdim[2];
+        double dx[3], r2 = 0.0;
+        float dxf[3];
+        for (int k = 0; k < 3; k++) {
+            int sh = li[k] - lj[k];
+            if (sh > 1) sh = -1;
+            else if (sh < -1) sh = 1;
+            float pix = (float)((double)xrel[3 * i + k] + h[k] * sh);
+            dxf[k] = pix - xrel[3 * j + k];
+            dx[k] = ((double)xrel[3 * i + k] + h[k] * sh) - (double)xrel[3 * j + k];
+            r2 += dx[k] * dx[k];
+        }
+        float r2f = dxf[0] * dxf[0] + dxf[1] * dxf[1] + dxf[2] * dxf[2];
+        if (r2f < ab2[0] || r2f > ab2[1]) r2f = (float)fmax(ab2[0], fmin(ab2[1], (double)r2f));
+        if (r2 < ab2[0] || r2 > ab2[1]) r2 = fmax(ab2[0], fmin(ab2[1], r2));
+        double e, fs;
+        eval_fp64(coef, alpha, potn, r2f, sqrt(r2), &e, &fs);
+        for (int k = 0; k < 3; k++) {
+            f_out[3 * i + k] -= fs * dx[k];
+            f_out[3 * j + k] += fs * dx[k];
+        }
+        epot += e;
+    }
+    *e_out = epot;
+    return 0;
+}
+
 /* Sort keys of one cell along direction sid (src/runner_dosort.c:118-153): key =
  * (k << 16) | (unsigned)(dscale*(bias + x.n)), dscale = 32767/(2 bias), bias = |h|; ordered
  * by descending distance, ties in storage order. */

@@ -34,6 +34,10 @@ def lib():
                                      P(C.c_float), P(C.c_int), P(C.c_int), C.c_int, P(C.c_int), P(C.c_double),
                                      P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_longlong),
                                      P(C.c_longlong), P(C.c_double), C.c_int]
+        L.oracle_bonds.restype = C.c_int
+        L.oracle_bonds.argtypes = [C.c_int, P(C.c_int), P(C.c_float), P(C.c_int), P(C.c_int), P(C.c_double),
+                                   P(C.c_float), P(C.c_float), C.c_int, P(C.c_double), P(C.c_double),
+                                   P(C.c_double)]
         L.oracle_rigid.restype = C.c_int
         L.oracle_rigid.argtypes = [C.c_int] + [C.c_void_p] * 14 + [C.c_double, C.c_double, C.c_int, C.c_int,
                                                                     C.c_void_p]
@@ -112,6 +116,29 @@ def nonbond(sysm, tables, binned=None):
         raise RuntimeError("oracle_nonbond failed")
     return dict(f=f, epot=epot.value, epot_abs=eabs.value, virial=vir.value, virial_abs=vabs.value,
                 pairs=npairs.value, excluded=nex.value)
+
+
+def bonds(sysm, table, binned=None):
+    """FP64 bond forces (by id) and energy of sysm.bonds with one bond table (n, alpha, coef)
+    of potential sysm.bond_pot (oracle_bonds)."""
+    b = binned or bin_system(sysm)
+    n, alpha, coef = table
+    N = sysm.n
+    f = np.zeros((N, 3), np.float64)
+    e = C.c_double()
+    bij = np.ascontiguousarray(sysm.bonds, np.int32).reshape(-1)
+    xrel = np.ascontiguousarray(b["xrel"], np.float32)
+    cell = np.ascontiguousarray(b["cell"], np.int32)
+    cdim = np.ascontiguousarray(b["cdim"], np.int32)
+    dim = np.ascontiguousarray(sysm.dim, np.float64)
+    coef = np.ascontiguousarray(coef, np.float32)
+    alpha = np.ascontiguousarray(alpha, np.float32)
+    spec = sysm.bond_pot
+    ab2 = np.array([spec.a * spec.a, spec.b * spec.b], np.float64)
+    lib().oracle_bonds(len(bij) // 2, _p(bij, C.c_int), _p(xrel, C.c_float), _p(cell, C.c_int), _p(cdim, C.c_int),
+                       _p(dim, C.c_double), _p(coef, C.c_float), _p(alpha, C.c_float), int(n), _p(ab2, C.c_double),
+                       _p(f, C.c_double), C.byref(e))
+    return dict(f=f, epot=e.value)
 
 
 def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:
