@@ -94,7 +94,7 @@ WORKLOADS = {
                  _replicas, "sweep_replicas512_traffic.txt"),
     "chains": ("solvated chains, 92,200 atoms: 220 chains of 100 beads (20 LJ types, Lorentz-Berthelot, "
                "charges N(0, 0.3) e neutralised per chain, 1-2 and 1-3 exclusions) and 23,400 3-site waters in "
-               "a 10.8 x 10.8 x 7.8 nm box (9 x 9 x 6 cells), cutoff 1.2 nm, 231 type tables and explicit "
+               "a 10.8 x 10.8 x 7.8 nm box (9 x 9 x 6 cells), cutoff 1.2 nm, 253 type tables and explicit "
                "electrostatics, seeded; force evaluation only (the chains' bonded terms are not built)",
                _chains, "sweep_chains92k_traffic.txt"),
 }

@@ -30,6 +30,7 @@ enum : unsigned {
     kStatusCellOverflow = 2u,
     kStatusTableIndex = 4u,
     kStatusForceOverflow = 8u,
+    kStatusNonFinite = 64u,        // a particle's position or velocity stopped being finite
 };
 
 // Accumulator slots (unsigned long long each).

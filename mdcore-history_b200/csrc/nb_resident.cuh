@@ -16,7 +16,8 @@
 // intact; integrate_cells counts the completed steps (and their accepted pairs), from which
 // the host finds that side,
 // re-blocks the particles with more room and runs the remaining steps again.  Nothing is
-// written out of bounds.
+// written out of bounds.  A position or velocity that is no longer finite (a system blowing
+// up) stops the steps after the step that produced it, and the host reports an error.
 #pragma once
 #include "nb_device.cuh"
 #include "nb_kernels.cuh"
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
                                                        const float* __restrict__ engine_dt,
                                                        const double* __restrict__ engine_imass, int max_type,
                                                        float4* __restrict__ xq, float4* __restrict__ v,
-                                                       const unsigned long long* __restrict__ status,
+                                                       unsigned long long* __restrict__ status,
                                                        const unsigned long long* __restrict__ acc,
                                                        unsigned long long* __restrict__ done) {
     if (*status != 0) return;
@@ -215,6 +216,8 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
         x.z = __fadd_rn(x.z, __fmul_rn(dt, vv.z));
         xq[s] = x;
         v[s] = vv;
+        if (!isfinite(x.x + x.y + x.z + vv.x + vv.y + vv.z))      // a system blowing up: stop
+            atomicOr(status, (unsigned long long)kStatusNonFinite);
     }
 }
 

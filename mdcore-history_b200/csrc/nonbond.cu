@@ -718,6 +718,7 @@ int finish_stats(NbState* st) {
         const char* msg = (a[kAccStatus] & kStatusCellOverflow)   ? "Max. number of parts per cell exceeded."
                           : (a[kAccStatus] & kStatusCopyTimeout)  ? "Bulk copy into shared memory timed out."
                           : (a[kAccStatus] & kStatusTableIndex)   ? "Pair distance beyond the potential table."
+                          : (a[kAccStatus] & kStatusNonFinite)    ? "Non-finite particle position or velocity."
                                                                    : "Fixed-point force overflow.";
         int code = (a[kAccStatus] & kStatusCellOverflow) ? engine_err_maxparts : engine_err_cuda;
         errs_register(code, msg, __LINE__, __func__, __FILE__);
@@ -1809,6 +1810,10 @@ int st_resident_steps(NbState* st, int nsteps) {
         st->rside = side0 ^ (int)(completed & 1);
         left -= (int)completed;
         const bool cells = (w[0] & kStatusResidentOverflow) != 0, movers = (w[0] & kStatusMoverOverflow) != 0;
+        if (w[0] & kStatusNonFinite) {
+            errs_register(engine_err_cuda, "Non-finite particle position or velocity.", __LINE__, __func__, __FILE__);
+            return engine_err = engine_err_cuda;
+        }
         if (++regrows > 8 || (cells && st->capc >= kMaxPartsPerCell)) {
             errs_register(engine_err_maxparts, "Max. number of parts per cell exceeded during resident steps.",
                           __LINE__, __func__, __FILE__);
@@ -2194,6 +2199,10 @@ int st_step_device(NbState* st) {
             st->res_done = (long long)st->h_words[1];
             st->res_pairs = (long long)st->h_words[2];
             break;
+        }
+        if (status & kStatusNonFinite) {
+            errs_register(engine_err_cuda, "Non-finite particle position or velocity.", __LINE__, __func__, __FILE__);
+            return engine_err = engine_err_cuda;
         }
         // Aborted on the device: the host cells still hold the step's input.
         for (struct engine* e : st->engines) e->time -= 1;

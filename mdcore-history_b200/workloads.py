@@ -330,7 +330,7 @@ QSCALE = math.sqrt(Q_SCALE)     # e -> per-particle charge unit of tables with p
 
 def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box=(10.8, 10.8, 7.8), seed: int = 0,
                  cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12,
-                 bond_k: float = 2.0e5) -> System:
+                 bond_k: float = 2.0e5, clearance: float = 0.25) -> System:
     """Heterogeneous solvated-chain system: `nchains` linear bead chains of `length` beads
     (bond 0.15 nm, 20 LJ bead types with sigma U[0.25, 0.40] nm and epsilon U[0.1, 1.0]
     kJ/mol, Lorentz-Berthelot mixing, charges N(0, 0.3) e neutralised per chain) and up to
@@ -344,7 +344,7 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     chain bonds harmonic, bond_k (r - 0.15 nm)^2 (bond_pot, a table on [0.05, 0.3] nm).
     Types: 0 O, 1 H, 2..21 beads.  Seeded.
 
-    Chains grow together as self-avoiding random walks (every new bead at least 0.25 nm
+    Chains grow together as self-avoiding random walks (every new bead at least `clearance`
     from the beads placed before it other than its two predecessors, bond angles >= 90
     degrees, up to 20 tries per bead)."""
     from scipy.spatial import cKDTree
@@ -372,7 +372,7 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
             # neighbours that are the chain's own last two beads do not count
             own = (idx // t == todo[:, None]) & (idx % t >= t - 2)
             dmin = np.where(own, np.inf, d).min(1)
-            ok = dmin >= 0.25
+            ok = dmin >= clearance
             cand[todo[ok]] = p[ok]
             prev[todo[ok]] = u[ok]
             if _try == 19:
@@ -419,10 +419,12 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     hhd = 2.0 * 0.1 * math.sin(math.radians(109.47) / 2.0)
     rig = np.stack([np.stack([k, k + 1, np.full(nw, 0.1)], 1), np.stack([k, k + 2, np.full(nw, 0.1)], 1),
                     np.stack([k + 1, k + 2, np.full(nw, hhd)], 1)], 1).reshape(-1, 3)
-    # --- potentials: LJ among O and the bead types (Lorentz-Berthelot), none for H
-    sig = np.concatenate([[0.3166], sig_b])
-    eps = np.concatenate([[0.650], eps_b])
-    lj_types = [0] + list(range(2, 2 + nbt))
+    # --- potentials: LJ among O, H and the bead types (Lorentz-Berthelot).  SPC/E gives H
+    # no LJ; with per-particle charges an H next to a negative bead would then meet no
+    # repulsion at all, so H carries a small one (sigma 0.1 nm, epsilon 0.1 kJ/mol).
+    sig = np.concatenate([[0.3166, 0.1], sig_b])
+    eps = np.concatenate([[0.650, 0.1], eps_b])
+    lj_types = [0, 1] + list(range(2, 2 + nbt))
     pots = []
     for a_i, ti in enumerate(lj_types):
         for b_i in range(a_i, len(lj_types)):

@@ -1,4 +1,4 @@
-"""GPU tests of the heterogeneous solvated-chain system (20 bead types + water, 231 type
+"""GPU tests of the heterogeneous solvated-chain system (20 bead types + water, 253 type
 tables read from global memory, explicit electrostatics q_i q_j ep(r) with per-particle
 charges, 1-2/1-3 chain exclusions, rigid water): forces, energy, virial and counts against
 the FP64 oracle, every launch shape, the plain form, and device steps against host steps."""

@@ -55,7 +55,7 @@ def test_pairs_without_type_potential_interact_through_charges():
 def test_chain_system_shape():
     s = W.chains_water(nchains=4, length=20, nwater=300, box=(3.6, 3.6, 3.6), seed=2)
     assert s.n == 80 + 900
-    assert len(s.pots) == 21 * 22 // 2 and s.ep is not None
+    assert len(s.pots) == 22 * 23 // 2 and s.ep is not None
     q = s.q[900:].reshape(4, 20)
     assert np.allclose(q.sum(1), 0.0, atol=1e-9)                 # neutral chains
     assert len(s.excl) == 3 * 300 + 4 * (19 + 18)
