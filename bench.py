@@ -244,6 +244,17 @@ def reference_arm(args, rank):
 
 # ---------------------------------------------------------------- this library on the GPU
 
+def reduce_max(values, dist, device):
+    """Every rank's timings -> their maxima over the ranks (the max-over-ranks rule for a
+    multi-GPU number); values unchanged when there is one rank (dist None)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def cell_counts(sysm, e):
     """Particles per cell of one engine (cells as space_init lays them out)."""
     import numpy as np
@@ -322,10 +333,7 @@ def force_only_line(args, rank, world, local_rank, M, tgt, engines, systems, st,
     clk = clocks.stop()
     if tgt.stats().status != 0:
         raise SystemExit("bench.py: device status after the plain evaluations")
-    if dist is not None:
-        t = torch.tensor([fe_ms, fe_e2e, fe_sweep, plain_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        fe_ms, fe_e2e, fe_sweep, plain_ms = [float(v) for v in t.tolist()]
+    fe_ms, fe_e2e, fe_sweep, plain_ms = reduce_max([fe_ms, fe_e2e, fe_sweep, plain_ms], dist, "cuda")
     if rank == 0:
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (fe_sweep * 1e-3) / 1e12
@@ -526,10 +534,8 @@ def ours(args, rank, world, local_rank):
     if tgt.stats().status != 0:
         raise SystemExit("bench.py: device status after the host-buffer steps")
 
-    if dist is not None:
-        t = torch.tensor([ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e = [float(v) for v in t.tolist()]
+    ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e = reduce_max([ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e],
+                                                              dist, "cuda")
     if rank == 0:
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
