@@ -26,9 +26,11 @@ __constant__ float c_axes[13][3];
 // cells, 13 for systems of small ones).  Keys of a direction are ordered by descending distance,
 // ties by ascending storage index (a stable order, independent of the order in which lanes
 // run):
-//  * a cell of at most 32 particles is sorted by one warp in registers: each lane holds one
-//    particle and counts, with a shuffle loop, the keys that come before its own;
-//  * a larger cell is sorted by all warps of the block, one warp per direction, with a
+//  * a cell of at most 32 particles is sorted by one warp in registers, with bitonic
+//    networks of shuffles over groups of lanes (several directions at once when it holds
+//    16 particles or fewer);
+//  * a larger cell's positions are staged once in shared memory, and it is sorted by all
+//    warps of the block, one warp per direction, with a
 //    counting sort on the top bits of the 16-bit distance (64 buckets in the warp's
 //    shared memory) and an exact rank inside the bucket: position = (keys in farther
 //    buckets) + (keys of the same bucket with a larger distance, or an equal distance and a
@@ -37,11 +39,14 @@ constexpr int kSortBuckets = 64;
 constexpr int kSortWarps = 13;
 
 // Shared memory of one sorting warp for cells of up to scap particles (a multiple of 4):
-// the keys, the bucket members, bucket counts, starts and fill levels.
+// the keys, the bucket members, bucket counts, starts and fill levels.  The block's
+// shared memory holds the staged positions of the cell (scap float4) and then one such
+// area per warp.
 __host__ __device__ inline size_t sort_warp_bytes(int scap) {
     return (size_t)scap * 4 + (size_t)scap * 2 + (size_t)3 * kSortBuckets * 4;
 }
-__host__ inline size_t sort_smem_bytes(int scap) { return kSortWarps * sort_warp_bytes(scap); }
+__host__ __device__ inline size_t sort_stage_bytes(int scap) { return (size_t)scap * 16; }
+__host__ inline size_t sort_smem_bytes(int scap) { return sort_stage_bytes(scap) + kSortWarps * sort_warp_bytes(scap); }
 
 // dscale * (bias + x.n), evaluated left to right without contraction (src/runner_dosort.c:148-149).
 // A particle inside its cell gives 0..32767; one that has left it by more than a cell (a
@@ -54,26 +59,62 @@ __device__ __forceinline__ unsigned sort_dist(float4 x, float nx, float ny, floa
     return min(__float2uint_rz(__fmul_rn(dscale, d)), 0xffffu);
 }
 
-// One warp, a cell of n <= 32 particles, every direction of its mask.
-__device__ __forceinline__ void sort_small_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys, int start,
-                                                int n, unsigned mask, float dscale, float bias, int lane) {
+// One warp, a cell of n <= 32 particles, every direction of its mask.  The warp is split
+// into 32/G groups of G lanes (G = n rounded up to a power of two), one direction per group
+// and one particle per lane, and each group sorts its values (distance << log2 G) |
+// (G-1 - index) -- unique, so the order is stable -- descending with a bitonic network
+// of shuffles inside the group.  Lanes past n carry 0, below every particle's value.
+template <int G>
+__device__ __forceinline__ void sort_small_group(const float4* __restrict__ xq, unsigned* __restrict__ keys, int start,
+                                                 int n, unsigned mask, float dscale, float bias, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
+    constexpr int D = 32 / G;
+    constexpr int SH = G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : G == 8 ? 3 : G == 16 ? 4 : 5;
     const int pad = (n + 3) & ~3;
-    const float4 x = lane < n ? xq[start + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int sid = 0; sid < 13; ++sid) {
-        if (!((mask >> sid) & 1u)) continue;
-        const unsigned md = sort_dist(x, c_axes[sid][0], c_axes[sid][1], c_axes[sid][2], dscale, bias);
-        int rank = 0;
-        for (int m = 0; m < n; ++m) {
-            const unsigned od = __shfl_sync(FULL, md, m);
-            rank += (od > md) | ((od == md) & (m < lane));
+    const int g = lane / G, idx = lane % G;
+    const float4 x = idx < n ? xq[start + idx] : make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned left = mask & 0x1fffu;
+    while (left) {
+        // this pass: the next D directions of the mask, the g-th of them for this group
+        int sid = -1;
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (left == 0) break;
+            const int b = __ffs(left) - 1;
+            left &= left - 1;
+            if (q == g) sid = b;
         }
-        if (lane < n) keys[13 * (size_t)start + (size_t)sid * pad + rank] = ((unsigned)lane << 16) | md;
+        const int sa = sid < 0 ? 0 : sid;
+        const unsigned md = sort_dist(x, c_axes[sa][0], c_axes[sa][1], c_axes[sa][2], dscale, bias);
+        unsigned v = idx < n ? (md << SH) | (unsigned)(G - 1 - idx) : 0u;
+#pragma unroll
+        for (int k = 2; k <= G; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const unsigned o = __shfl_xor_sync(FULL, v, j);
+                const bool keep_max = ((lane & j) == 0) == ((lane & k & (G - 1)) == 0);
+                v = keep_max ? max(v, o) : min(v, o);
+            }
+        }
+        if (sid >= 0 && idx < n)
+            keys[13 * (size_t)start + (size_t)sid * pad + idx] =
+                ((unsigned)(G - 1 - (int)(v & (G - 1))) << 16) | (v >> SH);
     }
 }
 
-// The warp's share of the directions of a cell of more than 32 particles.
-__device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys,
+__device__ __forceinline__ void sort_small_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys, int start,
+                                                int n, unsigned mask, float dscale, float bias, int lane) {
+    if (n <= 1) sort_small_group<1>(xq, keys, start, n, mask, dscale, bias, lane);
+    else if (n <= 2) sort_small_group<2>(xq, keys, start, n, mask, dscale, bias, lane);
+    else if (n <= 4) sort_small_group<4>(xq, keys, start, n, mask, dscale, bias, lane);
+    else if (n <= 8) sort_small_group<8>(xq, keys, start, n, mask, dscale, bias, lane);
+    else if (n <= 16) sort_small_group<16>(xq, keys, start, n, mask, dscale, bias, lane);
+    else sort_small_group<32>(xq, keys, start, n, mask, dscale, bias, lane);
+}
+
+// The warp's share of the directions of a cell of more than 32 particles, whose positions
+// xs[0..n) are staged in shared memory.
+__device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, unsigned* __restrict__ keys,
                                                 unsigned char* wp, int scap, int start, int n, unsigned mask,
                                                 float dscale, float bias, int warp, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
@@ -89,7 +130,7 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xq, u
         for (int b = lane; b < kSortBuckets; b += 32) { bcount[b] = 0; bfill[b] = 0; }
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const unsigned key = ((unsigned)k << 16) | sort_dist(xq[start + k], nx, ny, nz, dscale, bias);
+            const unsigned key = ((unsigned)k << 16) | sort_dist(xs[k], nx, ny, nz, dscale, bias);
             skey[k] = key;
             atomicAdd(&bcount[min((int)((key & 0xffffu) >> 9), kSortBuckets - 1)], 1);
         }
@@ -147,7 +188,9 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
         const int n = ccount[c];
         if (n > 0 && n <= 32) sort_small_cell(xq, keys, cstart[c], n, cmask[c], cscale[c].x, cscale[c].y, lane);
     }
-    // larger cells: all warps, one direction each
+    // larger cells: positions staged once, then all warps, one direction each
+    float4* xs = reinterpret_cast<float4*>(sort_smem);
+    unsigned char* warea = sort_smem + sort_stage_bytes(scap) + (size_t)warp * sort_warp_bytes(scap);
     for (int c = c0; c < c1; ++c) {
         const int n = ccount[c];
         if (n <= 32) continue;
@@ -155,8 +198,11 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __re
             if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
             continue;
         }
-        sort_large_cell(xq, keys, sort_smem + (size_t)warp * sort_warp_bytes(scap), scap, cstart[c], n, cmask[c],
-                        cscale[c].x, cscale[c].y, warp, lane);
+        const int start = cstart[c];
+        __syncthreads();  // the previous cell's readers are done with xs
+        for (int k = threadIdx.x; k < n; k += blockDim.x) xs[k] = xq[start + k];
+        __syncthreads();
+        sort_large_cell(xs, keys, warea, scap, start, n, cmask[c], cscale[c].x, cscale[c].y, warp, lane);
     }
 }
 

@@ -286,8 +286,11 @@ int launch_sort(const float4* xq, const int* cstart, const int* ccount, const un
                 const unsigned long long* abort, bool capturing, cudaStream_t s) {
     scap = std::max(4, std::min(kMaxPartsPerCell, (scap + 3) & ~3));
     const size_t smem = sort_smem_bytes(scap);
+    // the largest size any launch asks for, so that launches captured into a graph later
+    // (where the attribute is not set) are covered whatever their cells hold
     if (!capturing)
-        CU(cudaFuncSetAttribute(sort_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CU(cudaFuncSetAttribute(sort_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sort_smem_bytes(kMaxPartsPerCell)));
     sort_cells<<<(ncells + cpc - 1) / cpc, kSortWarps * 32, smem, s>>>(xq, cstart, ccount, cmask, keys, cscale,
                                                                        ncells, cpc, scap, acc, abort);
     CU(cudaGetLastError());

@@ -78,6 +78,46 @@ def test_sort_keys_bit_exact(fname):
     e.close()
 
 
+def cells_of_every_size(ncmax=40, seed=11):
+    """5 x 5 x 5 cells of 1 nm; cell c holds c % (ncmax + 1) particles, half of them sharing
+    their x and y with another particle of the cell (equal distances along some directions)."""
+    rng = np.random.default_rng(seed)
+    cd = 5
+    xs = []
+    for c in range(cd ** 3):
+        n = c % (ncmax + 1)
+        corner = np.array([c // (cd * cd), (c // cd) % cd, c % cd], np.float64)
+        p = rng.uniform(0.02, 0.98, size=(n, 3))
+        for k in range(1, n, 2):
+            p[k, :2] = p[k - 1, :2]
+        xs.append(corner + p)
+    x = np.concatenate(xs)
+    A, B = W.lj_AB(0.996, 0.3405)
+    s = W.System(name="cell-sizes", origin=np.zeros(3), dim=np.full(3, float(cd)), L=np.ones(3), cutoff=1.0,
+                 masses=[39.948], charges=[0.0],
+                 pots=[W.PotSpec(W.KIND_LJ126, 0, 0, 0.25, 1.0, 1e-4, (A, B, 0.0, 0.0))],
+                 x=x, type=np.zeros(len(x), np.int32), excl=np.zeros((0, 2), np.int32))
+    return s.counting()
+
+
+def test_sort_keys_every_cell_size():
+    """Cells of 0..40 particles (every lane-group width of the in-register sort, 1 to 32, and
+    the shared-memory sort above 32), with tied distances: keys equal the oracle's."""
+    sysm = cells_of_every_size()
+    e, _, st = evaluate(sysm)
+    assert st.status == 0
+    b = O.bin_system(sysm)
+    ncells = int(np.prod(b["cdim"]))
+    for cid in range(ncells):
+        ids = np.flatnonzero(b["cell"] == cid)
+        if len(ids) == 0:
+            continue
+        dev = e.sortkeys(cid, len(ids))
+        for sid in range(13):
+            assert np.array_equal(dev[sid], O.sortkeys(b["xrel"][ids], b["h"], sid)), (cid, len(ids), sid)
+    e.close()
+
+
 @pytest.mark.parametrize("plain", [False, True], ids=["tuned", "plain"])
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
 def test_launch_shapes_agree(warps, plain):
