@@ -3,17 +3,28 @@
 //
 // run(n, grain, fn) splits [0, n) into at most threads() contiguous ranges of at least
 // `grain` items, calls fn(part, begin, end) for each (the calling thread takes part 0) and
-// returns when every range is done.  Idle workers block on a
-// condition variable, so they take no CPU time between steps.  The thread count is
-// MDB_HOST_THREADS if set, else the number of CPUs this process may run on, at most 16.
+// returns when every range is done.  The thread count is MDB_HOST_THREADS if set, else the
+// number of CPUs this process may run on, at most 16.
+//
+// Waiting is spin-then-block: an idle worker polls for the next job for MDB_HOST_SPIN_US
+// microseconds (default 2000) after its last one, then blocks on a condition variable, so
+// that the several loops of one step (and of steps issued back to back) start without a
+// thread wake-up each, and an idle pool takes no CPU time.  The caller waits for the
+// workers the same way.  MDB_HOST_SPIN_US=0 blocks at once.
 #pragma once
 #include <sched.h>
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdlib>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
+#if defined(__x86_64__) || defined(__i386__)
+#include <immintrin.h>
+#endif
 
 namespace nb {
 
@@ -35,25 +46,28 @@ public:
             return;
         }
         {
-            std::unique_lock<std::mutex> lk(m_);
+            std::lock_guard<std::mutex> lk(m_);
             job_ = &fn;
             n_ = n;
             parts_ = parts;
-            pending_ = parts - 1;
-            ++generation_;
+            pending_.store(parts - 1, std::memory_order_relaxed);
+            gen_.fetch_add(1, std::memory_order_release);
         }
-        cv_.notify_all();
-        fn(0, 0, range_end(0));
-        std::unique_lock<std::mutex> lk(m_);
-        done_.wait(lk, [&] { return pending_ == 0; });
+        if (sleepers_.load(std::memory_order_acquire) > 0) cv_.notify_all();
+        fn(0, 0, range_end(0, n, parts));
+        if (!spin_until([&] { return pending_.load(std::memory_order_acquire) == 0; })) {
+            std::unique_lock<std::mutex> lk(m_);
+            done_.wait(lk, [&] { return pending_.load(std::memory_order_acquire) == 0; });
+        }
+        std::lock_guard<std::mutex> lk(m_);
         job_ = nullptr;
     }
 
     ~HostPool() {
         {
-            std::unique_lock<std::mutex> lk(m_);
+            std::lock_guard<std::mutex> lk(m_);
             stop_ = true;
-            ++generation_;
+            gen_.fetch_add(1, std::memory_order_release);
         }
         cv_.notify_all();
         for (std::thread& t : workers_) t.join();
@@ -73,36 +87,67 @@ private:
             if (n > 16) n = 16;
         }
         if (n < 1) n = 1;
+        if (const char* env = std::getenv("MDB_HOST_SPIN_US")) spin_us_ = std::max(0, std::atoi(env));
         for (int k = 1; k < n; k++) workers_.emplace_back([this, k] { loop(k); });
     }
 
-    int range_begin(int part) const { return (int)((long long)n_ * part / parts_); }
-    int range_end(int part) const { return (int)((long long)n_ * (part + 1) / parts_); }
+    static int range_end(int part, int n, int parts) { return (int)((long long)n * (part + 1) / parts); }
+
+    static void relax() {
+#if defined(__x86_64__) || defined(__i386__)
+        _mm_pause();
+#else
+        std::this_thread::yield();
+#endif
+    }
+
+    // Polls `ready` for at most spin_us_ microseconds; true once it holds.
+    template <class F>
+    bool spin_until(F ready) const {
+        if (ready()) return true;
+        if (spin_us_ <= 0) return false;
+        const auto t_end = std::chrono::steady_clock::now() + std::chrono::microseconds(spin_us_);
+        for (int it = 1;; ++it) {
+            relax();
+            if (ready()) return true;
+            if ((it & 63) == 0 && std::chrono::steady_clock::now() >= t_end) return ready();
+        }
+    }
 
     void loop(int id) {
         long long seen = 0;
         for (;;) {
+            spin_until([&] { return gen_.load(std::memory_order_acquire) != seen; });
             std::unique_lock<std::mutex> lk(m_);
-            cv_.wait(lk, [&] { return generation_ != seen; });
-            seen = generation_;
+            if (gen_.load(std::memory_order_acquire) == seen) {
+                sleepers_.fetch_add(1, std::memory_order_acq_rel);
+                cv_.wait(lk, [&] { return gen_.load(std::memory_order_acquire) != seen; });
+                sleepers_.fetch_sub(1, std::memory_order_acq_rel);
+            }
+            seen = gen_.load(std::memory_order_acquire);
             if (stop_) return;
             if (id >= parts_ || job_ == nullptr) continue;
             const std::function<void(int, int, int)>* job = job_;
-            const int b = range_begin(id), e = range_end(id);
+            const int b = range_end(id - 1, n_, parts_), e = range_end(id, n_, parts_);
             lk.unlock();
             (*job)(id, b, e);
-            lk.lock();
-            if (--pending_ == 0) done_.notify_one();
+            if (pending_.fetch_sub(1, std::memory_order_acq_rel) == 1) {
+                std::lock_guard<std::mutex> g(m_);
+                done_.notify_one();
+            }
         }
     }
 
     std::vector<std::thread> workers_;
     std::mutex m_;
     std::condition_variable cv_, done_;
-    const std::function<void(int, int, int)>* job_ = nullptr;
-    int n_ = 0, parts_ = 1, pending_ = 0;
-    long long generation_ = 0;
-    bool stop_ = false;
+    const std::function<void(int, int, int)>* job_ = nullptr;   // guarded by m_
+    int n_ = 0, parts_ = 1;                                       // guarded by m_
+    std::atomic<int> pending_{0};
+    std::atomic<long long> gen_{0};
+    std::atomic<int> sleepers_{0};
+    bool stop_ = false;                                           // guarded by m_
+    int spin_us_ = 2000;
 };
 
 }  // namespace nb

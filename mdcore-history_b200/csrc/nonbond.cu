@@ -163,10 +163,16 @@ struct NbState {
     unsigned long long* h_ebond = nullptr;
     unsigned long long* h_words = nullptr;   // status, completed steps, their pairs (pinned)
     std::vector<long long> res_engine_n;   // particles of each engine on the device
-    std::vector<float> id_q;
-    std::vector<int> id_vid;
-    std::vector<unsigned short> id_flags;
-    std::vector<unsigned char> id_present;
+    // What the device does not carry, by dense index of the last upload (cell order): the
+    // download returns each particle's upload index, so the host reads these (and the ids
+    // in h_uppid) nearly in order instead of scattering by particle id.
+    struct UpAux {
+        float q;
+        int vid;
+        unsigned short flags;
+    };
+    std::vector<UpAux> up_aux;
+    int* r_up_of = nullptr;            // device: global id -> dense index of the last upload
     cudaGraph_t rgraph[2] = {nullptr, nullptr};
     cudaGraphExec_t rgraph_exec[2] = {nullptr, nullptr};
     long long rgraph_key[2] = {-1, -1}, rprepared[2] = {-1, -1};
@@ -297,12 +303,30 @@ int launch_sort(const float4* xq, const int* cstart, const int* ccount, const un
     return 0;
 }
 
-// Cells per host-thread range: about 8,192 particles, at least 16 cells.
+// Particles per host-thread range of the per-step host loops (MDB_HOST_GRAIN, default
+// 2,048) and per pipelined chunk of the host<->device copies (MDB_COPY_CHUNK, default
+// 49,152): each chunk's copies overlap the host packing of the next one (upload) or the
+// host unpacking of the previous one (download).
+long long env_count(const char* name, long long dflt) {
+    const char* env = std::getenv(name);
+    const long long v = env ? std::atoll(env) : 0;
+    return v > 0 ? v : dflt;
+}
+long long host_grain_parts() {
+    static const long long v = env_count("MDB_HOST_GRAIN", 2048);
+    return v;
+}
+long long copy_chunk_parts() {
+    static const long long v = env_count("MDB_COPY_CHUNK", 49152);
+    return v;
+}
+
+// Cells per host-thread range: about host_grain_parts() particles, at least 16 cells.
 int cell_grain(const NbState* st) {
     long long n = 0;
     for (const struct engine* e : st->engines) n += e->s.nr_parts;
     const long long avg = st->ncells > 0 ? n / st->ncells + 1 : 1;
-    return (int)std::max(16LL, 8192 / avg);
+    return (int)std::max(16LL, host_grain_parts() / avg);
 }
 
 // Slot layout of this evaluation (host threads over ranges of cells): counts, padded slot
@@ -378,10 +402,10 @@ void pack_range(NbState* st, int cb, int ce) {
     });
 }
 
-// Cell ranges of the host<->device pipeline: large systems move in up to 8 chunks of about
-// 256k slots, so that packing (unpacking) one chunk overlaps the copy of another.
+// Cell ranges of the host<->device pipeline: up to 8 chunks of about copy_chunk_parts()
+// slots, so that packing (unpacking) one chunk overlaps the copy of another.
 std::vector<int> chunk_bounds(const NbState* st, int total) {
-    const int k = std::max(1, std::min(8, total / 262144));
+    const int k = (int)std::max(1LL, std::min(8LL, total / copy_chunk_parts()));
     std::vector<int> bounds(k + 1, st->ncells);
     bounds[0] = 0;
     for (int q = 1; q < k; q++) {
@@ -1254,7 +1278,7 @@ void res_free(NbState* st) {
     void* dev[] = {st->r_xq[0], st->r_xq[1], st->r_v[0], st->r_v[1], st->r_pid[0], st->r_pid[1], st->r_cnt[0],
                    st->r_cnt[1], st->r_done, st->r_cstart, st->r_nstay, st->r_nmove, st->r_slot_of, st->r_nbr, st->r_cell_engine,
                    st->r_cell_h, st->r_engine_dt, st->r_engine_imass, st->r_movers, st->r_keys, st->r_force,
-                   st->r_status, st->r_dense, st->r_dpid, st->r_doff};
+                   st->r_status, st->r_dense, st->r_dpid, st->r_doff, st->r_up_of};
     for (void* p : dev) cudaFree(p);
     if (st->h_dense) cudaFreeHost(st->h_dense);
     if (st->h_dpid) cudaFreeHost(st->h_dpid);
@@ -1289,7 +1313,7 @@ void res_free(NbState* st) {
     st->r_pid[0] = st->r_pid[1] = nullptr;
     st->r_cnt[0] = st->r_cnt[1] = nullptr;
     st->r_done = nullptr;
-    st->r_cstart = st->r_nstay = st->r_nmove = st->r_slot_of = nullptr;
+    st->r_cstart = st->r_nstay = st->r_nmove = st->r_slot_of = st->r_up_of = nullptr;
     st->r_nbr = st->r_cell_engine = nullptr;
     st->r_cell_h = nullptr;
     st->r_engine_dt = nullptr;
@@ -1303,32 +1327,40 @@ void res_free(NbState* st) {
     st->res_active = false;
 }
 
-// Places the dense upload (cell order, per-cell offsets) into the cells' blocks.
+// Places the dense upload (cell order, per-cell offsets) into the cells' blocks, records
+// each id's upload index (up_of) and, with explicit electrostatics, scatters the uploaded
+// charges by id (dq, qid; else nullptr).
 __global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float4* __restrict__ dxq,
                                                    const float4* __restrict__ dv, const int* __restrict__ dpid,
                                                    const int* __restrict__ doff, const int* __restrict__ count,
                                                    float4* __restrict__ xq, float4* __restrict__ v,
-                                                   int* __restrict__ pid) {
+                                                   int* __restrict__ pid, int* __restrict__ up_of,
+                                                   const float* __restrict__ dq, float* __restrict__ qid) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= RC.ncells) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) {
-        xq[base + k] = dxq[doff[c] + k];
-        v[base + k] = dv[doff[c] + k];
-        pid[base + k] = dpid[doff[c] + k];
+        const int o = doff[c] + k;
+        const int id = dpid[o];
+        xq[base + k] = dxq[o];
+        v[base + k] = dv[o];
+        pid[base + k] = id;
+        up_of[id] = o;
+        if (qid != nullptr) qid[id] = dq[o];
     }
 }
 
 // Every particle in cell order for the host copy (cell c from offset doff[c]): positions
 // (w = type), velocities and the last evaluation's forces as three arrays of np entries,
-// and the ids.
+// and each particle's index in the last upload (through up_of, by id).
 __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const float4* __restrict__ xq,
                                                      const float4* __restrict__ v, const int* __restrict__ pid,
                                                      const int* __restrict__ count, const int* __restrict__ doff,
                                                      const unsigned long long* __restrict__ force, size_t np,
-                                                     float4* __restrict__ dense, int* __restrict__ dpid) {
+                                                     const int* __restrict__ up_of, float4* __restrict__ dense,
+                                                     int* __restrict__ dpid) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= RC.ncells) return;
@@ -1343,7 +1375,7 @@ __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const flo
             make_float4((float)((double)(long long)force[3 * s] * (1.0 / (double)kForceScale)),
                         (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale)),
                         (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale)), 0.f);
-        dpid[o] = pid[s];
+        dpid[o] = up_of[pid[s]];
     }
 }
 
@@ -1479,6 +1511,8 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMalloc(&st->r_nmove, sizeof(int) * (nc + 1)));
     CU(cudaMalloc(&st->r_movers, sizeof(Mover) * (size_t)nc * st->mcap));
     CU(cudaMalloc(&st->r_slot_of, sizeof(int) * (nid + 1)));
+    CU(cudaMalloc(&st->r_up_of, sizeof(int) * (nid + 1)));
+    CU(cudaMemset(st->r_up_of, 0xff, sizeof(int) * (nid + 1)));     // -1: not uploaded
     CU(cudaMalloc(&st->r_nbr, sizeof(int) * 27 * (size_t)nc));
     CU(cudaMalloc(&st->r_cell_h, sizeof(float4) * (nc + 1)));
     CU(cudaMalloc(&st->r_cell_engine, sizeof(int) * (nc + 1)));
@@ -1525,18 +1559,15 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMemcpy(st->r_cell_h, cell_h.data(), sizeof(float4) * nc, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_dt, edt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_imass, imass.data(), sizeof(double) * imass.size(), cudaMemcpyHostToDevice));
-    st->id_q.assign(nid, 0.f);
-    st->id_vid.assign(nid, 0);
-    st->id_flags.assign(nid, 0);
-    st->id_present.assign(nid, 0);
+    st->up_aux.assign((size_t)n + 1, NbState::UpAux{0.f, 0, 0});
     st->res_active = true;
     return res_build_bonds(st);
 }
 
-// Pipeline chunks of a transfer of np particles: one per 256k particles, 1 to 8 (every
-// chunk costs a wake-up of the host threads, ~0.1 ms here, more than the copy it hides
-// for smaller chunks).
-int res_chunks(size_t np) { return (int)std::max<size_t>(1, std::min<size_t>(8, np / 262144)); }
+// Pipeline chunks of an engine_step transfer of np particles, 1 to 8.
+int res_chunks(size_t np) {
+    return (int)std::max(1LL, std::min(8LL, (long long)np / copy_chunk_parts()));
+}
 
 // The engines' host cells into side 0 of the device blocks (the caller has checked that
 // every cell fits): positions, velocities and ids packed in cell order by the host threads,
@@ -1553,6 +1584,10 @@ int res_upload(NbState* st) {
     const size_t np = (size_t)st->res_nparts;
     float4* hx = st->h_up;
     float4* hv = st->h_up + np;
+    // charges for explicit electrostatics: through the force section of the download
+    // buffers, free until the download (scattered by id on the device, in place_cells)
+    float* hq = st->ep_pot >= 0 ? reinterpret_cast<float*>(st->h_dense + 2 * np) : nullptr;
+    float* dq = reinterpret_cast<float*>(st->r_dense + 2 * np);
     const double t0 = now_ms();
     // Chunks of cells with about equal particle counts: each chunk's copies overlap the
     // packing of the next.
@@ -1575,16 +1610,15 @@ int res_upload(NbState* st) {
                 hx[o] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
                 hv[o] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
                 st->h_uppid[o] = gid;
-                st->id_q[gid] = p->q;
-                st->id_vid[gid] = p->vid;
-                st->id_flags[gid] = p->flags;
-                st->id_present[gid] = 1;
+                st->up_aux[o] = NbState::UpAux{p->q, p->vid, p->flags};
+                if (hq != nullptr) hq[o] = p->q;
             }
         }
         const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
         evict_lines(hx + q0, sizeof(float4) * (q1 - q0));
         evict_lines(hv + q0, sizeof(float4) * (q1 - q0));
         evict_lines(st->h_uppid + q0, sizeof(int) * (q1 - q0));
+        if (hq != nullptr) evict_lines(hq + q0, sizeof(float) * (q1 - q0));
     });
     const size_t q0 = (size_t)off[c0], q1 = (size_t)off[c1];
     if (q1 > q0) {
@@ -1594,21 +1628,22 @@ int res_upload(NbState* st) {
                            st->stream));
         CU(cudaMemcpyAsync(st->r_dpid + q0, st->h_uppid + q0, sizeof(int) * (q1 - q0), cudaMemcpyHostToDevice,
                            st->stream));
+        if (hq != nullptr)
+            CU(cudaMemcpyAsync(dq + q0, hq + q0, sizeof(float) * (q1 - q0), cudaMemcpyHostToDevice, st->stream));
     }
     }
     st->bstats.ms_pack = (float)(now_ms() - t0);
     st->res_engine_n.assign(ne, 0);
     for (int k = 0; k < ne; k++) st->res_engine_n[k] = off[st->cell_off[k + 1]] - off[st->cell_off[k]];
-    if (st->ep_pot >= 0)                 // charges by id, as packed above
-        CU(cudaMemcpyAsync(st->d_qid, st->id_q.data(), sizeof(float) * st->id_q.size(), cudaMemcpyHostToDevice,
-                           st->stream));
     CU(cudaMemcpyAsync(st->r_cnt[0], cnt, sizeof(int) * nc, cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
     CU(cudaMemsetAsync(st->r_done, 0, 2 * sizeof(unsigned long long), st->stream));
     const ResidentCells RC = res_cells(st);
-    place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid, st->r_doff,
-                                                      st->r_cnt[0], st->r_xq[0], st->r_v[0], st->r_pid[0]);
+    place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid,
+                                                               st->r_doff, st->r_cnt[0], st->r_xq[0], st->r_v[0],
+                                                               st->r_pid[0], st->r_up_of, dq,
+                                                               hq != nullptr ? st->d_qid : nullptr);
     CU(cudaGetLastError());
     slot_of_ids<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_pid[0], st->r_cnt[0], st->r_slot_of, nullptr);
     CU(cudaGetLastError());
@@ -1858,7 +1893,8 @@ int res_download(NbState* st, unsigned long long* status) {
         scan_counts_apply<<<nb, kScanBlock, 0, st->stream>>>(st->r_cnt[side], nc, st->capc, st->r_bsum, st->r_doff);
         compact_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side],
                                                                      st->r_pid[side], st->r_cnt[side], st->r_doff,
-                                                                     st->r_force, np, st->r_dense, st->r_dpid);
+                                                                     st->r_force, np, st->r_up_of, st->r_dense,
+                                                                     st->r_dpid);
         CU(cudaGetLastError());
     }
     CU(cudaMemcpyAsync(st->h_words, st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
@@ -1937,18 +1973,24 @@ int res_download(NbState* st, unsigned long long* status) {
                 for (int q = 0; q < n; q++) {
                     const size_t o = (size_t)off[c] + q;
                     const float4 x = st->h_dense[o], v = st->h_dense[np + o], f = st->h_dense[2 * np + o];
-                    const int gid = st->h_dpid[o];
+                    const int ou = st->h_dpid[o];           // the particle's upload index
+                    if (ou < 0 || (size_t)ou >= np) {
+                        fail = 2;
+                        return;
+                    }
+                    const int gid = st->h_uppid[ou];
+                    const NbState::UpAux& ax = st->up_aux[ou];
                     struct part* p = &cl->parts[q];
                     int type;
                     std::memcpy(&type, &x.w, sizeof(int));
                     p->x[0] = x.x; p->x[1] = x.y; p->x[2] = x.z; p->x[3] = 0.f;
                     p->v[0] = v.x; p->v[1] = v.y; p->v[2] = v.z; p->v[3] = 0.f;
                     p->f[0] = f.x; p->f[1] = f.y; p->f[2] = f.z; p->f[3] = 0.f;
-                    p->q = st->id_q[gid];
+                    p->q = ax.q;
                     p->id = gid - lo;
-                    p->vid = st->id_vid[gid];
+                    p->vid = ax.vid;
                     p->type = (short)type;
-                    p->flags = st->id_flags[gid];
+                    p->flags = ax.flags;
                     sp->partlist[p->id] = p;      // space_relink, inline
                     sp->celllist[p->id] = cl;
                 }
@@ -1963,6 +2005,10 @@ int res_download(NbState* st, unsigned long long* status) {
     }
     st->bstats.ms_unpack = (float)t_rebuild;
     CU(cudaStreamSynchronize(st->stream));
+    if (fail == 2) {
+        errs_register(engine_err_cuda, "A downloaded particle has no upload index.", __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_cuda;
+    }
     if (fail) {
         errs_register(engine_err_malloc, "Could not grow a host cell.", __LINE__, __func__, __FILE__);
         return engine_err = engine_err_malloc;
@@ -2013,7 +2059,7 @@ extern "C" void nb_parallel_for(int n, int grain, void (*fn)(void*, int, int, in
 extern "C" int nb_host_parts(void) { return HostPool::get().threads(); }
 
 extern "C" void nb_zero_cells(struct space* s) {
-    const int grain = (int)std::max(16, 8192 / (s->nr_parts / std::max(1, s->nr_cells) + 1));
+    const int grain = (int)std::max(16LL, host_grain_parts() / (s->nr_parts / std::max(1, s->nr_cells) + 1));
     HostPool::get().run(s->nr_cells, grain, [&](int, int b, int e) {
         for (int c = b; c < e; c++) {
             struct cell* cl = &s->cells[c];
