@@ -141,6 +141,18 @@ struct bond {
     int i, j;
 };
 
+/* src/angle.h:31-39: the angle i-j-k (ids, j the vertex) with angle potential pid. */
+struct angle {
+    int i, j, k;
+    int pid;
+};
+
+/* src/dihedral.h:31-39: the dihedral i-j-k-l (ids) with dihedral potential pid. */
+struct dihedral {
+    int i, j, k, l;
+    int pid;
+};
+
 /* src/part.h:73-88 */
 struct part_type {
     int id;
@@ -189,6 +201,12 @@ struct potential *potential_create_Ewald(double a, double b, double q, double ka
 struct potential *potential_create_Coulomb(double a, double b, double q, double tol);
 /* src/potential.c:301-322: harmonic bond K (r - r0)^2 on [a, b]. */
 struct potential *potential_create_harmonic(double a, double b, double K, double r0, double tol);
+/* src/potential.c:448-482: harmonic angle K (theta - theta0)^2 for theta in [a, b] (held to
+ * [0, pi]), tabulated over cos(theta) on [cos b, cos a]. */
+struct potential *potential_create_harmonic_angle(double a, double b, double K, double theta0, double tol);
+/* src/potential.c:382-411: harmonic dihedral K (1 + cos(n phi - delta)), tabulated over
+ * cos(phi) on [-1, 1]. */
+struct potential *potential_create_harmonic_dihedral(double K, int n, double delta, double tol);
 void potential_clear(struct potential *p);
 /* Scalar host evaluation, src/potential_eval.h:67-104. */
 void potential_eval(struct potential *p, float r2, float *e, float *f);
@@ -306,7 +324,13 @@ struct engine {
     struct bond *bonds;     /* engine_bond_add */
     int nr_bonds, bonds_size;
     struct potential **p_bond;   /* max_type x max_type bond potentials (engine_bond_addpot) */
-    int bonds_gen;          /* bumped by every engine_bond_add / engine_bond_addpot */
+    int bonds_gen;          /* bumped by every change of the bonds, angles or dihedrals */
+    struct angle *angles;   /* engine_angle_add */
+    int nr_angles, angles_size, nr_anglepots, anglepots_size;
+    struct potential **p_angle;      /* angle potentials by index (engine_angle_addpot) */
+    struct dihedral *dihedrals;      /* engine_dihedral_add */
+    int nr_dihedrals, dihedrals_size, nr_dihedralpots, dihedralpots_size;
+    struct potential **p_dihedral;   /* dihedral potentials by index (engine_dihedral_addpot) */
 };
 
 /* src/engine.c:2439-2591 */
@@ -345,6 +369,26 @@ int engine_bond_addpot(struct engine *e, struct potential *p, int i, int j);
  * steps, into the same fixed-point forces as the nonbonded sweep; their energy goes to
  * e->s.epot_bond.  engine_step_host returns engine_err_nyi for an engine with bonds. */
 int engine_bond_add(struct engine *e, int i, int j);
+/* Extension: the potential energies of the last step or force evaluation, out[6] = e->s.epot,
+ * epot_nonbond, epot_bond, epot_angle, epot_dihedral, epot_exclusion (engine_unload's epot
+ * sums the cells' nonbonded energies only, as the reference's does). */
+int engine_energies(struct engine *e, double *out);
+/* src/engine_bonded.c:2151-2177: adds an angle potential; returns its index. */
+int engine_angle_addpot(struct engine *e, struct potential *p);
+/* src/engine_bonded.c:1258-1290: the angle i-j-k with angle potential pid.  Evaluated as
+ * angle_eval does (src/angle.c:81-300: positions relative to j's cell, the cells' periodic
+ * offsets held to -1..1, cos(theta) held to [-1, 1] and then to the table's range, the
+ * table read at cos(theta), force = -dE/dcos * dcos/dx) on the device by engine_step and
+ * the device-resident steps; energy to e->s.epot_angle. */
+int engine_angle_add(struct engine *e, int i, int j, int k, int pid);
+/* src/engine_bonded.c:2114-2140: adds a dihedral potential; returns its index. */
+int engine_dihedral_addpot(struct engine *e, struct potential *p);
+/* src/engine_bonded.c:1210-1243: the dihedral i-j-k-l with dihedral potential pid.
+ * Evaluated as dihedral_eval does (src/dihedral.c:81-380: cos(phi) of the planes i-j-k and
+ * j-k-l, held to [-1, 1] and then to the table's range) on the device by engine_step and
+ * the device-resident steps; energy to e->s.epot_dihedral.  engine_step_host returns
+ * engine_err_nyi for an engine with angles or dihedrals. */
+int engine_dihedral_add(struct engine *e, int i, int j, int k, int l, int pid);
 /* src/engine.c:1674-1826 */
 int engine_start(struct engine *e, int nr_runners, int nr_queues);
 /* src/engine.c:2070-2240.  One time step (re-binning, forces, symplectic Euler, rigid

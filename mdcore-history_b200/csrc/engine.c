@@ -405,7 +405,8 @@ int engine_step(struct engine *e) {
  * evaluation and constraints through host buffers. */
 int engine_step_host(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
-    if (e->nr_bonds > 0) return engine_error(engine_err_nyi);   /* bonds: device steps only */
+    /* bonds, angles and dihedrals: device steps only */
+    if (e->nr_bonds > 0 || e->nr_angles > 0 || e->nr_dihedrals > 0) return engine_error(engine_err_nyi);
     struct space *s = &e->s;
     e->time += 1;
     if (space_shuffle(s) < 0) return engine_error(engine_err_space);
@@ -434,6 +435,10 @@ int engine_finalize(struct engine *e) {
     free(e->part2rigid);
     free(e->bonds);
     free(e->p_bond);
+    free(e->angles);
+    free(e->p_angle);
+    free(e->dihedrals);
+    free(e->p_dihedral);
     memset(e, 0, sizeof(struct engine));
     return engine_err_ok;
 }
@@ -476,6 +481,75 @@ int engine_bond_add(struct engine *e, int i, int j) {
     e->bonds[e->nr_bonds].j = j;
     e->nr_bonds += 1;
     e->bonds_gen++;
+    return engine_err_ok;
+}
+
+/* Grows an array of `size` elements of `elem` bytes holding `used` to at least used + 1. */
+static int grow(void **arr, int *size, int used, size_t elem, int first) {
+    if (used < *size) return 0;
+    const int nsize = *size ? 2 * *size : first;
+    void *na = realloc(*arr, elem * (size_t)nsize);
+    if (na == NULL) return -1;
+    *arr = na;
+    *size = nsize;
+    return 0;
+}
+
+int engine_angle_addpot(struct engine *e, struct potential *p) {
+    if (e == NULL || p == NULL) return engine_error(engine_err_null);
+    if (grow((void **)&e->p_angle, &e->anglepots_size, e->nr_anglepots, sizeof(struct potential *), 100) < 0)
+        return engine_error(engine_err_malloc);
+    e->p_angle[e->nr_anglepots] = p;
+    e->bonds_gen++;
+    return e->nr_anglepots++;
+}
+
+int engine_angle_add(struct engine *e, int i, int j, int k, int pid) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (grow((void **)&e->angles, &e->angles_size, e->nr_angles, sizeof(struct angle), 100) < 0)
+        return engine_error(engine_err_malloc);
+    struct angle *a = &e->angles[e->nr_angles++];
+    a->i = i;
+    a->j = j;
+    a->k = k;
+    a->pid = pid;
+    e->bonds_gen++;
+    return engine_err_ok;
+}
+
+int engine_dihedral_addpot(struct engine *e, struct potential *p) {
+    if (e == NULL || p == NULL) return engine_error(engine_err_null);
+    if (grow((void **)&e->p_dihedral, &e->dihedralpots_size, e->nr_dihedralpots, sizeof(struct potential *),
+             100) < 0)
+        return engine_error(engine_err_malloc);
+    e->p_dihedral[e->nr_dihedralpots] = p;
+    e->bonds_gen++;
+    return e->nr_dihedralpots++;
+}
+
+int engine_dihedral_add(struct engine *e, int i, int j, int k, int l, int pid) {
+    if (e == NULL) return engine_error(engine_err_null);
+    if (grow((void **)&e->dihedrals, &e->dihedrals_size, e->nr_dihedrals, sizeof(struct dihedral), 100) < 0)
+        return engine_error(engine_err_malloc);
+    struct dihedral *d = &e->dihedrals[e->nr_dihedrals++];
+    d->i = i;
+    d->j = j;
+    d->k = k;
+    d->l = l;
+    d->pid = pid;
+    e->bonds_gen++;
+    return engine_err_ok;
+}
+
+int engine_energies(struct engine *e, double *out) {
+    if (e == NULL || out == NULL) return engine_error(engine_err_null);
+    const struct space *s = &e->s;
+    out[0] = s->epot;
+    out[1] = s->epot_nonbond;
+    out[2] = s->epot_bond;
+    out[3] = s->epot_angle;
+    out[4] = s->epot_dihedral;
+    out[5] = s->epot_exclusion;
     return engine_err_ok;
 }
 

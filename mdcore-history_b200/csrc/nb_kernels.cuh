@@ -231,6 +231,30 @@ __device__ __forceinline__ void eval_table(const float* __restrict__ coef, float
     f = __fdiv_rn(eff * c0.y, r);
 }
 
+// The table read at r itself (potential_eval_r, src/potential_eval.h:122-148, used for the
+// cosines of angles and dihedrals): interval from the index polynomial at r, energy and
+// dE/dr (no division by r).
+__device__ __forceinline__ void eval_table_r(const float* __restrict__ coef, float4 info, int nmax, float r,
+                                             float& e, float& f, unsigned& status) {
+    float t = __fadd_rn(info.x, __fmul_rn(r, __fadd_rn(info.y, __fmul_rn(r, info.z))));
+    int ind = __float2int_rz(fmaxf(0.0f, t));
+    if (ind > nmax) {
+        status |= kStatusTableIndex;
+        ind = nmax;
+    }
+    const float4* c = reinterpret_cast<const float4*>(coef + (__float_as_int(info.w) & 0xfffff) + 8 * ind);
+    const float4 c0 = c[0], c1 = c[1];
+    const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
+    float ee = fmaf(c0.z, x, c0.w);
+    float eff = c0.z;
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.x);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.y);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.z);
+    eff = fmaf(eff, x, ee); ee = fmaf(ee, x, c1.w);
+    e = ee;
+    f = eff * c0.y;
+}
+
 __device__ __forceinline__ bool excluded_pair(int pi, int pj, unsigned emask, int exlo, int exhi,
                                               const int* __restrict__ exlist) {
     const int d = pj - pi;

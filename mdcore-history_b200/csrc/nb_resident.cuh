@@ -240,10 +240,58 @@ struct BondArgs {
     const int4* eng_cdim;
     const double4* eng_h;
     int capc;
-    unsigned long long* ebond;   // per engine, 2^32 units per kJ/mol
+    unsigned long long* ebond;   // bond, angle, dihedral energy per engine (3 x nengines), 2^32 units per kJ/mol
     unsigned long long* acc;     // status bits
     const unsigned long long* abort;
+    int nengines;
+    const int4* angles;          // global ids i, j, k; engine << 16 | table
+    int nangles;
+    const int4* dihedrals;       // global ids i, j, k, l
+    const int* dihedral_te;      // engine << 16 | table, by dihedral
+    int ndihedrals;
+    const double2* ab;           // per table: its range [a, b] (angles, dihedrals: of the cosine)
 };
+
+// Position of the particle in slot s relative to the cell of slot sref (both of engine eng):
+// its cell-relative position plus the cell edge times the cells' offset, the offset held to
+// -1..1 in each dimension (the periodic image next to sref's cell), as src/angle.c:141-158
+// and src/dihedral.c:146-171 place i, k (and l) relative to j's cell.
+__device__ __forceinline__ void pos_near(const BondArgs& B, int eng, int s, int sref, float out[3]) {
+    const int4 cd = B.eng_cdim[eng];
+    const double4 h = B.eng_h[eng];
+    const int c = s / B.capc - B.eng_cell0[eng], cr = sref / B.capc - B.eng_cell0[eng];
+    const int l[3] = {c / (cd.y * cd.z), (c / cd.z) % cd.y, c % cd.z};
+    const int lr[3] = {cr / (cd.y * cd.z), (cr / cd.z) % cd.y, cr % cd.z};
+    const double hh[3] = {h.x, h.y, h.z};
+    const float4 x = B.xq[s];
+    const float xv[3] = {x.x, x.y, x.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        int sh = l[k] - lr[k];
+        if (sh > 1) sh = -1;
+        else if (sh < -1) sh = 1;
+        out[k] = (float)((double)xv[k] + hh[k] * sh);
+    }
+}
+
+__device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a[0], b[0]), __fmul_rn(a[1], b[1])), __fmul_rn(a[2], b[2]));
+}
+
+__device__ __forceinline__ void cross3(const float a[3], const float b[3], float out[3]) {
+    out[0] = a[1] * b[2] - a[2] * b[1];
+    out[1] = a[2] * b[0] - a[0] * b[2];
+    out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// The cosine held to the table's range (the reference warns and clamps,
+// src/angle.c:183-187, src/dihedral.c:254-260), the table read at it.
+__device__ __forceinline__ void eval_cosine(const BondArgs& B, int tab, float c, float& e, float& f,
+                                            unsigned& status) {
+    const double2 ab = B.ab[tab];
+    if ((double)c < ab.x || (double)c > ab.y) c = (float)fmax(ab.x, fmin(ab.y, (double)c));
+    eval_table_r(B.coef, B.potinfo[tab], B.potn[tab], c, e, f, status);
+}
 
 __global__ void __launch_bounds__(128) bond_forces(BondArgs B) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -280,6 +328,108 @@ __global__ void __launch_bounds__(128) bond_forces(BondArgs B) {
         atomic_add_fixed(B.force + 3 * (size_t)sj + k, to_fixed(w, status));
     }
     atomicAdd(&B.ebond[b.w], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
+    if (status) atomicOr(&B.acc[kAccStatus], (unsigned long long)status);
+}
+
+// Angles (angle_eval, src/angle.c:81-300): one thread per angle i-j-k.  With u = x_i - x_j
+// and w = x_k - x_j (positions near j's cell), cos = u.w / (|u| |w|) held to [-1, 1], and
+// its gradients d cos/d x_i = (w/|w| - cos u/|u|) / |u|, d cos/d x_k = (u/|u| - cos w/|w|) / |w|,
+// d cos/d x_j = -(both); the force on each particle is -dE/dcos times its gradient.
+__global__ void __launch_bounds__(128) angle_forces(BondArgs B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B.nangles || (B.abort != nullptr && *(const volatile unsigned long long*)B.abort != 0)) return;
+    const int4 a = B.angles[t];
+    const int eng = a.w >> 16, tab = a.w & 0xffff;
+    const int si = B.slot_of[a.x], sj = B.slot_of[a.y], sk = B.slot_of[a.z];
+    float xi[3], xj[3], xk[3], u[3], w[3];
+    pos_near(B, eng, si, sj, xi);
+    pos_near(B, eng, sj, sj, xj);
+    pos_near(B, eng, sk, sj, xk);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        u[k] = __fsub_rn(xi[k], xj[k]);
+        w[k] = __fsub_rn(xk[k], xj[k]);
+    }
+    const float iu = __fdiv_rn(1.0f, __fsqrt_rn(dot3(u, u)));
+    const float iw = __fdiv_rn(1.0f, __fsqrt_rn(dot3(w, w)));
+    const float c = fminf(1.0f, fmaxf(-1.0f, dot3(u, w) * iu * iw));
+    float gi[3], gk[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float uh = u[k] * iu, wh = w[k] * iw;
+        gi[k] = (wh - c * uh) * iu;
+        gk[k] = (uh - c * wh) * iw;
+    }
+    float e, f;
+    unsigned status = 0;
+    eval_cosine(B, tab, c, e, f, status);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float wi = f * gi[k], wk = f * gk[k];
+        atomic_add_fixed(B.force + 3 * (size_t)si + k, to_fixed(-wi, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sk + k, to_fixed(-wk, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sj + k, to_fixed(wi + wk, status));
+    }
+    atomicAdd(&B.ebond[B.nengines + eng], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
+    if (status) atomicOr(&B.acc[kAccStatus], (unsigned long long)status);
+}
+
+// Dihedrals (dihedral_eval, src/dihedral.c:81-380): one thread per dihedral i-j-k-l.  With
+// b1 = x_j - x_i, b2 = x_k - x_j, b3 = x_l - x_k (positions near j's cell), the plane normals
+// n1 = b1 x b2 and n2 = b2 x b3, cos = n1.n2 / (|n1| |n2|) held to [-1, 1].  Gradients by the
+// chain rule through the normals: g1 = d cos/d n1 = (n2/|n2| - cos n1/|n1|) / |n1|,
+// g2 = (n1/|n1| - cos n2/|n2|) / |n2|; d cos/d b1 = b2 x g1, d cos/d b3 = g2 x b2,
+// d cos/d b2 = g1 x b1 + b3 x g2; then x_i: -d/db1, x_j: d/db1 - d/db2, x_l: d/db3, and x_k
+// takes minus the sum of the other three.
+__global__ void __launch_bounds__(128) dihedral_forces(BondArgs B) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B.ndihedrals || (B.abort != nullptr && *(const volatile unsigned long long*)B.abort != 0)) return;
+    const int4 d = B.dihedrals[t];
+    const int te = B.dihedral_te[t];
+    const int eng = te >> 16, tab = te & 0xffff;
+    const int si = B.slot_of[d.x], sj = B.slot_of[d.y], sk = B.slot_of[d.z], sl = B.slot_of[d.w];
+    float xi[3], xj[3], xk[3], xl[3], b1[3], b2[3], b3[3];
+    pos_near(B, eng, si, sj, xi);
+    pos_near(B, eng, sj, sj, xj);
+    pos_near(B, eng, sk, sj, xk);
+    pos_near(B, eng, sl, sj, xl);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        b1[k] = __fsub_rn(xj[k], xi[k]);
+        b2[k] = __fsub_rn(xk[k], xj[k]);
+        b3[k] = __fsub_rn(xl[k], xk[k]);
+    }
+    float n1[3], n2[3];
+    cross3(b1, b2, n1);
+    cross3(b2, b3, n2);
+    const float i1 = __fdiv_rn(1.0f, __fsqrt_rn(dot3(n1, n1)));
+    const float i2 = __fdiv_rn(1.0f, __fsqrt_rn(dot3(n2, n2)));
+    const float c = fminf(1.0f, fmaxf(-1.0f, dot3(n1, n2) * i1 * i2));
+    float g1[3], g2[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float h1 = n1[k] * i1, h2 = n2[k] * i2;
+        g1[k] = (h2 - c * h1) * i1;
+        g2[k] = (h1 - c * h2) * i2;
+    }
+    float db1[3], db2[3], db3[3], t1[3], t2[3];
+    cross3(b2, g1, db1);
+    cross3(g2, b2, db3);
+    cross3(g1, b1, t1);
+    cross3(b3, g2, t2);
+    float e, f;
+    unsigned status = 0;
+    eval_cosine(B, tab, c, e, f, status);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        db2[k] = t1[k] + t2[k];
+        const float wi = f * -db1[k], wj = f * (db1[k] - db2[k]), wl = f * db3[k];
+        atomic_add_fixed(B.force + 3 * (size_t)si + k, to_fixed(-wi, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sj + k, to_fixed(-wj, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sl + k, to_fixed(-wl, status));
+        atomic_add_fixed(B.force + 3 * (size_t)sk + k, to_fixed(wi + wj + wl, status));
+    }
+    atomicAdd(&B.ebond[2 * B.nengines + eng], (unsigned long long)__double2ll_rn((double)e * kEnergyScale));
     if (status) atomicOr(&B.acc[kAccStatus], (unsigned long long)status);
 }
 

@@ -159,8 +159,13 @@ struct NbState {
     int* r_eng_cell0 = nullptr;
     int4* r_eng_cdim = nullptr;
     double4* r_eng_h = nullptr;
-    unsigned long long* r_ebond = nullptr;   // per engine
+    unsigned long long* r_ebond = nullptr;   // bond, angle, dihedral energy per engine (3 x engines)
     unsigned long long* h_ebond = nullptr;
+    int nangles = 0, ndihedrals = 0;
+    int4* r_angles = nullptr;                // i, j, k, engine << 16 | table
+    int4* r_dihedrals = nullptr;             // i, j, k, l
+    int* r_dihedral_te = nullptr;            // engine << 16 | table
+    double2* r_bab = nullptr;                // per table: a, b
     unsigned long long* h_words = nullptr;   // status, completed steps, their pairs (pinned)
     std::vector<long long> res_engine_n;   // particles of each engine on the device
     // What the device does not carry, by dense index of the last upload (cell order): the
@@ -1287,7 +1292,8 @@ void res_free(NbState* st) {
     if (st->h_words) cudaFreeHost(st->h_words);
     {
         void* bdev[] = {st->r_bonds, st->r_bcoef, st->r_bpotinfo, st->r_bpotn, st->r_bab2, st->r_eng_cell0,
-                        st->r_eng_cdim, st->r_eng_h, st->r_ebond};
+                        st->r_eng_cdim, st->r_eng_h, st->r_ebond, st->r_angles, st->r_dihedrals,
+                        st->r_dihedral_te, st->r_bab};
         for (void* p : bdev) cudaFree(p);
         if (st->h_ebond) cudaFreeHost(st->h_ebond);
         st->r_bonds = nullptr;
@@ -1300,7 +1306,11 @@ void res_free(NbState* st) {
         st->r_eng_h = nullptr;
         st->r_ebond = nullptr;
         st->h_ebond = nullptr;
-        st->nbonds = 0;
+        st->r_angles = nullptr;
+        st->r_dihedrals = nullptr;
+        st->r_dihedral_te = nullptr;
+        st->r_bab = nullptr;
+        st->nbonds = st->nangles = st->ndihedrals = 0;
     }
     if (st->r_bsum) cudaFree(st->r_bsum);
     st->h_words = nullptr;
@@ -1398,46 +1408,80 @@ int res_grid(const NbState* st) { return (st->ncells + kCellWarps - 1) / kCellWa
 // The engines' bonds for the device: global ids, the bond table of the two particles' types
 // (bonds whose types have none are dropped, as bond_eval skips them), the engine; the
 // distinct bond tables; per engine its first cell, cell grid and cell edge.
+bool res_bonded(const NbState* st) { return st->nbonds + st->nangles + st->ndihedrals > 0; }
+
 long long res_bonds_key(const NbState* st) {
     long long k = 0;
     for (struct engine* e : st->engines) k += e->bonds_gen;
     return k;
 }
 
+// Bonded terms of the resident steps: bonds (potential by the two particles' types), angles
+// and dihedrals (potential by index), with global ids; the tables they use, each once.
 int res_build_bonds(NbState* st) {
     const int ne = (int)st->engines.size();
     st->bonds_key = res_bonds_key(st);
-    std::vector<int4> bonds;
+    std::vector<int4> bonds, angles, dihedrals;
+    std::vector<int> dihedral_te;
     std::vector<struct potential*> uniq;
+    auto table_of = [&](struct potential* pot) {
+        int u = 0;
+        while (u < (int)uniq.size() && uniq[u] != pot) u++;
+        if (u == (int)uniq.size()) uniq.push_back(pot);
+        return u;
+    };
     for (int k = 0; k < ne; k++) {
         struct engine* e = st->engines[k];
-        if (e->nr_bonds == 0 || e->p_bond == nullptr) continue;
-        const int mt = e->max_type;
-        for (int b = 0; b < e->nr_bonds; b++) {
-            const int i = e->bonds[b].i, j = e->bonds[b].j;
-            if (i < 0 || j < 0 || i >= e->s.nr_parts || j >= e->s.nr_parts) continue;
-            const struct part *pi = e->s.partlist[i], *pj = e->s.partlist[j];
-            if (pi == nullptr || pj == nullptr) continue;
-            struct potential* pot = e->p_bond[pj->type * mt + pi->type];
-            if (pot == nullptr) continue;
-            int u = 0;
-            while (u < (int)uniq.size() && uniq[u] != pot) u++;
-            if (u == (int)uniq.size()) uniq.push_back(pot);
-            bonds.push_back(make_int4(st->id_off[k] + i, st->id_off[k] + j, u, k));
+        const int np = e->s.nr_parts;
+        auto present = [&](int id) { return id >= 0 && id < np && e->s.partlist[id] != nullptr; };
+        if (e->nr_bonds > 0 && e->p_bond != nullptr) {
+            const int mt = e->max_type;
+            for (int b = 0; b < e->nr_bonds; b++) {
+                const int i = e->bonds[b].i, j = e->bonds[b].j;
+                if (!present(i) || !present(j)) continue;
+                const struct part *pi = e->s.partlist[i], *pj = e->s.partlist[j];
+                struct potential* pot = e->p_bond[pj->type * mt + pi->type];
+                if (pot == nullptr) continue;
+                bonds.push_back(make_int4(st->id_off[k] + i, st->id_off[k] + j, table_of(pot), k));
+            }
+        }
+        for (int a = 0; a < e->nr_angles; a++) {
+            const struct angle* an = &e->angles[a];
+            if (!present(an->i) || !present(an->j) || !present(an->k)) continue;
+            if (an->pid < 0 || an->pid >= e->nr_anglepots || e->p_angle[an->pid] == nullptr) continue;
+            angles.push_back(make_int4(st->id_off[k] + an->i, st->id_off[k] + an->j, st->id_off[k] + an->k,
+                                       (k << 16) | table_of(e->p_angle[an->pid])));
+        }
+        for (int d = 0; d < e->nr_dihedrals; d++) {
+            const struct dihedral* dh = &e->dihedrals[d];
+            if (!present(dh->i) || !present(dh->j) || !present(dh->k) || !present(dh->l)) continue;
+            if (dh->pid < 0 || dh->pid >= e->nr_dihedralpots || e->p_dihedral[dh->pid] == nullptr) continue;
+            dihedrals.push_back(
+                make_int4(st->id_off[k] + dh->i, st->id_off[k] + dh->j, st->id_off[k] + dh->k, st->id_off[k] + dh->l));
+            dihedral_te.push_back((k << 16) | table_of(e->p_dihedral[dh->pid]));
         }
     }
     st->nbonds = (int)bonds.size();
-    if (st->nbonds == 0) return 0;
+    st->nangles = (int)angles.size();
+    st->ndihedrals = (int)dihedrals.size();
+    if (st->nbonds + st->nangles + st->ndihedrals == 0) return 0;
+    if ((!angles.empty() || !dihedrals.empty()) && (ne > 32767 || uniq.size() > 65535)) {
+        st->nbonds = st->nangles = st->ndihedrals = 0;
+        errs_register(engine_err_range, "Too many engines or bonded tables for the angle/dihedral records.",
+                      __LINE__, __func__, __FILE__);
+        return engine_err = engine_err_range;
+    }
     std::vector<float> coef;
     std::vector<float4> info;
     std::vector<int> potn;
-    std::vector<double2> ab2;
+    std::vector<double2> ab2, ab;
     for (struct potential* p : uniq) {
         const int off = (int)coef.size();
         coef.insert(coef.end(), p->c, p->c + (size_t)(p->n + 1) * potential_chunk);
         info.push_back(make_float4(p->alpha[0], p->alpha[1], p->alpha[2], bits_as_float(off | (p->n << 20))));
         potn.push_back(p->n);
         ab2.push_back(make_double2(p->a * p->a, p->b * p->b));
+        ab.push_back(make_double2(p->a, p->b));
     }
     std::vector<int> cell0(ne);
     std::vector<int4> cdim(ne);
@@ -1448,25 +1492,20 @@ int res_build_bonds(NbState* st) {
         cdim[k] = make_int4(sp->cdim[0], sp->cdim[1], sp->cdim[2], 0);
         h[k] = make_double4(sp->h[0], sp->h[1], sp->h[2], 0.0);
     }
-    CU(cudaMalloc(&st->r_bonds, sizeof(int4) * bonds.size()));
-    CU(cudaMalloc(&st->r_bcoef, sizeof(float) * coef.size()));
-    CU(cudaMalloc(&st->r_bpotinfo, sizeof(float4) * info.size()));
-    CU(cudaMalloc(&st->r_bpotn, sizeof(int) * potn.size()));
-    CU(cudaMalloc(&st->r_bab2, sizeof(double2) * ab2.size()));
-    CU(cudaMalloc(&st->r_eng_cell0, sizeof(int) * ne));
-    CU(cudaMalloc(&st->r_eng_cdim, sizeof(int4) * ne));
-    CU(cudaMalloc(&st->r_eng_h, sizeof(double4) * ne));
-    CU(cudaMalloc(&st->r_ebond, sizeof(unsigned long long) * ne));
-    CU(cudaMallocHost(&st->h_ebond, sizeof(unsigned long long) * ne));
-    CU(cudaMemset(st->r_ebond, 0, sizeof(unsigned long long) * ne));
-    CU(cudaMemcpy(st->r_bonds, bonds.data(), sizeof(int4) * bonds.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_bcoef, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_bpotinfo, info.data(), sizeof(float4) * info.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_bpotn, potn.data(), sizeof(int) * potn.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_bab2, ab2.data(), sizeof(double2) * ab2.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_eng_cell0, cell0.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_eng_cdim, cdim.data(), sizeof(int4) * ne, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(st->r_eng_h, h.data(), sizeof(double4) * ne, cudaMemcpyHostToDevice));
+    auto up = [&](auto** dst, const auto& v) -> int {
+        using T = typename std::decay<decltype(v)>::type::value_type;
+        CU(cudaMalloc(dst, sizeof(T) * std::max<size_t>(1, v.size())));
+        if (!v.empty()) CU(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+        return 0;
+    };
+    if (up(&st->r_bonds, bonds) < 0 || up(&st->r_angles, angles) < 0 || up(&st->r_dihedrals, dihedrals) < 0 ||
+        up(&st->r_dihedral_te, dihedral_te) < 0 || up(&st->r_bcoef, coef) < 0 || up(&st->r_bpotinfo, info) < 0 ||
+        up(&st->r_bpotn, potn) < 0 || up(&st->r_bab2, ab2) < 0 || up(&st->r_bab, ab) < 0 ||
+        up(&st->r_eng_cell0, cell0) < 0 || up(&st->r_eng_cdim, cdim) < 0 || up(&st->r_eng_h, h) < 0)
+        return engine_err_cuda;
+    CU(cudaMalloc(&st->r_ebond, sizeof(unsigned long long) * 3 * ne));
+    CU(cudaMallocHost(&st->h_ebond, sizeof(unsigned long long) * 3 * ne));
+    CU(cudaMemset(st->r_ebond, 0, sizeof(unsigned long long) * 3 * ne));
     return 0;
 }
 
@@ -1696,7 +1735,7 @@ int res_issue_step(NbState* st) {
     for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
     rebin_gather<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
                                                st->r_pid[o], st->r_cnt[o], st->r_status,
-                                               (rigid || st->nbonds > 0) ? st->r_slot_of : nullptr);
+                                               (rigid || res_bonded(st)) ? st->r_slot_of : nullptr);
     CU(cudaGetLastError());
     DevView V;
     V.xq = st->r_xq[o];
@@ -1711,8 +1750,8 @@ int res_issue_step(NbState* st) {
     V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
     rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
-    if (st->nbonds > 0) {              // the bonds' forces join the sweep's before the update
-        CU(cudaMemsetAsync(st->r_ebond, 0, sizeof(unsigned long long) * st->engines.size(), st->stream));
+    if (res_bonded(st)) {              // the bonded forces join the sweep's before the update
+        CU(cudaMemsetAsync(st->r_ebond, 0, sizeof(unsigned long long) * 3 * st->engines.size(), st->stream));
         BondArgs B;
         B.bonds = st->r_bonds;
         B.nbonds = st->nbonds;
@@ -1730,7 +1769,16 @@ int res_issue_step(NbState* st) {
         B.ebond = st->r_ebond;
         B.acc = st->d_acc;
         B.abort = st->r_status;
-        bond_forces<<<(st->nbonds + 127) / 128, 128, 0, st->stream>>>(B);
+        B.nengines = (int)st->engines.size();
+        B.angles = st->r_angles;
+        B.nangles = st->nangles;
+        B.dihedrals = st->r_dihedrals;
+        B.dihedral_te = st->r_dihedral_te;
+        B.ndihedrals = st->ndihedrals;
+        B.ab = st->r_bab;
+        if (st->nbonds > 0) bond_forces<<<(st->nbonds + 127) / 128, 128, 0, st->stream>>>(B);
+        if (st->nangles > 0) angle_forces<<<(st->nangles + 127) / 128, 128, 0, st->stream>>>(B);
+        if (st->ndihedrals > 0) dihedral_forces<<<(st->ndihedrals + 127) / 128, 128, 0, st->stream>>>(B);
         CU(cudaGetLastError());
     }
     const unsigned slot_blocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
@@ -1915,8 +1963,8 @@ int res_download(NbState* st, unsigned long long* status) {
                        cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
-    if (st->nbonds > 0)
-        CU(cudaMemcpyAsync(st->h_ebond, st->r_ebond, sizeof(unsigned long long) * ne, cudaMemcpyDeviceToHost,
+    if (res_bonded(st))
+        CU(cudaMemcpyAsync(st->h_ebond, st->r_ebond, sizeof(unsigned long long) * 3 * ne, cudaMemcpyDeviceToHost,
                            st->stream));
     for (struct engine* e : st->engines)
         if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream, 0);
@@ -2021,8 +2069,12 @@ int res_download(NbState* st, unsigned long long* status) {
     rc = finish_stats(st);
     for (int k = 0; k < ne; k++) {
         struct space* sp = &st->engines[k]->s;
-        if (st->nbonds > 0) sp->epot_bond = (double)(long long)st->h_ebond[k] / kEnergyScale;
-        sp->epot += sp->epot_nonbond + sp->epot_bond;
+        if (res_bonded(st)) {
+            sp->epot_bond = (double)(long long)st->h_ebond[k] / kEnergyScale;
+            sp->epot_angle = (double)(long long)st->h_ebond[ne + k] / kEnergyScale;
+            sp->epot_dihedral = (double)(long long)st->h_ebond[2 * ne + k] / kEnergyScale;
+        }
+        sp->epot += sp->epot_nonbond + sp->epot_bond + sp->epot_angle + sp->epot_dihedral;
     }
     return rc;
 }
@@ -2386,7 +2438,8 @@ extern "C" int engine_batch_step_host(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
     NbState* st = bstate(b);
     for (struct engine* e : st->engines)
-        if (e->nr_bonds > 0) return engine_err = engine_err_nyi;     // bonds: device steps only
+        if (e->nr_bonds > 0 || e->nr_angles > 0 || e->nr_dihedrals > 0)   // bonded: device steps only
+            return engine_err = engine_err_nyi;
     for (struct engine* e : st->engines) {
         e->time += 1;
         if (space_shuffle(&e->s) < 0) return engine_err = engine_err_space;

@@ -563,6 +563,50 @@ struct potential *potential_create_harmonic(double a, double b, double K, double
     return create(f_harm, NULL, f6_harm, a, b, tol, potential_flag_none);
 }
 
+/* Harmonic angle K (theta - theta0)^2 as a table over r = cos(theta) on [cos b, cos a],
+ * the angle range held to [0, pi] (src/potential.c:414-482). */
+static struct { double K, theta0; } HA;
+static double f_hangle(double r) {
+    const double theta = acos(fmin(1.0, fmax(-1.0, r)));
+    return HA.K * (theta - HA.theta0) * (theta - HA.theta0);
+}
+
+struct potential *potential_create_harmonic_angle(double a, double b, double K, double theta0, double tol) {
+    if (a < 0.0) a = 0.0;
+    if (b > M_PI) b = M_PI;
+    HA.K = K;
+    HA.theta0 = theta0;
+    return create(f_hangle, NULL, NULL, cos(b), cos(a), tol, potential_flag_none);
+}
+
+/* Harmonic dihedral K (1 + cos(n phi - delta)) as a table over r = cos(phi) on [-1, 1]
+ * (src/potential.c:325-411).  With phi = acos(r): cos(n phi) = T_n(r) and
+ * sin(n phi) = U_{n-1}(r) sqrt(1 - r^2), the Chebyshev polynomials of the first and second
+ * kind from their three-term recurrences; delta = 0 and delta = pi exactly take the
+ * cos-only forms, and |r| >= 1 drops the sine term. */
+static struct { double K, delta; int n; } HD;
+static double f_hdihedral(double r) {
+    double t0 = 1.0, t1 = r, u0 = 1.0, u1 = 2 * r;      /* T_k, T_{k+1}; U_k, U_{k+1} */
+    for (int k = 2; k <= HD.n; k++) {
+        const double t2 = 2 * r * t1 - t0, u2 = 2 * r * u1 - u0;
+        t0 = t1; t1 = t2;
+        u0 = u1; u1 = u2;
+    }
+    /* now t1 = T_n and u0 = U_{n-1} (for n = 1: T_1 = r, U_0 = 1) */
+    const double tn = HD.n == 0 ? 1.0 : t1, un1 = HD.n == 0 ? 0.0 : u0;
+    if (HD.delta == 0.0) return HD.K * (1.0 + tn);
+    if (HD.delta == M_PI) return HD.K * (1.0 - tn);
+    if (fabs(r) < 1.0) return HD.K * (1.0 + tn * cos(HD.delta) + un1 * sqrt(1.0 - r * r) * sin(HD.delta));
+    return HD.K * (1.0 + tn * cos(HD.delta));
+}
+
+struct potential *potential_create_harmonic_dihedral(double K, int n, double delta, double tol) {
+    HD.K = K;
+    HD.n = n;
+    HD.delta = delta;
+    return create(f_hdihedral, NULL, NULL, -1.0, 1.0, tol, potential_flag_none);
+}
+
 struct potential *potential_create_Coulomb(double a, double b, double q, double tol) {
     P.q = q; P.b = b;
     return create(f_coul, fp_coul, f6_coul, a, b, tol, potential_flag_Coulomb);

@@ -95,6 +95,13 @@ def lib() -> C.CDLL:
         "engine_setexplepot": (C.c_int, [vp, P(Potential)]),
         "engine_bond_addpot": (C.c_int, [vp, P(Potential), C.c_int, C.c_int]),
         "engine_bond_add": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_energies": (C.c_int, [vp, dp]),
+        "engine_angle_addpot": (C.c_int, [vp, P(Potential)]),
+        "engine_angle_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "engine_dihedral_addpot": (C.c_int, [vp, P(Potential)]),
+        "engine_dihedral_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "potential_create_harmonic_angle": (P(Potential), [C.c_double] * 5),
+        "potential_create_harmonic_dihedral": (P(Potential), [C.c_double, C.c_int, C.c_double, C.c_double]),
         "engine_batch_step_host": (C.c_int, [vp]),
         "engine_advance": (C.c_int, [vp]),
         "engine_finalize": (C.c_int, [vp]),
@@ -231,6 +238,31 @@ def create_potential(spec):
     return ptr
 
 
+def create_angle_potential(a, b, K, theta0, tol):
+    """potential_create_harmonic_angle (one entry of workloads.System.angle_pots)."""
+    ptr = lib().potential_create_harmonic_angle(a, b, K, theta0, tol)
+    if not ptr:
+        _check(-17, "potential_create_harmonic_angle")
+    return ptr
+
+
+def create_dihedral_potential(K, n, delta, tol):
+    """potential_create_harmonic_dihedral (one entry of workloads.System.dihedral_pots)."""
+    ptr = lib().potential_create_harmonic_dihedral(K, int(n), delta, tol)
+    if not ptr:
+        _check(-17, "potential_create_harmonic_dihedral")
+    return ptr
+
+
+def bonded_tables(ptrs):
+    """(n, alpha, coef, a, b) of each potential: the oracle's table arguments."""
+    out = []
+    for p in ptrs:
+        n, alpha, c = p.contents.table()
+        out.append((n, alpha, c, p.contents.a, p.contents.b))
+    return out
+
+
 class Engine:
     """Owns one struct engine allocated in Python memory, as a C driver would on its stack."""
 
@@ -276,6 +308,22 @@ class Engine:
                 _check(e.lib.engine_bond_addpot(e.ptr, bp, ti, tj), "engine_bond_addpot")
             for i, j in np.asarray(sysm.bonds):
                 _check(e.lib.engine_bond_add(e.ptr, int(i), int(j)), "engine_bond_add")
+        e.angle_pots, e.dihedral_pots = [], []
+        if getattr(sysm, "angles", None) is not None and len(sysm.angles):
+            for spec in sysm.angle_pots:
+                ptr = create_angle_potential(*spec)
+                e.angle_pots.append(ptr)
+                _check(e.lib.engine_angle_addpot(e.ptr, ptr), "engine_angle_addpot")
+            for i, j, k, pid in np.asarray(sysm.angles):
+                _check(e.lib.engine_angle_add(e.ptr, int(i), int(j), int(k), int(pid)), "engine_angle_add")
+        if getattr(sysm, "dihedrals", None) is not None and len(sysm.dihedrals):
+            for spec in sysm.dihedral_pots:
+                ptr = create_dihedral_potential(*spec)
+                e.dihedral_pots.append(ptr)
+                _check(e.lib.engine_dihedral_addpot(e.ptr, ptr), "engine_dihedral_addpot")
+            for i, j, k, l, pid in np.asarray(sysm.dihedrals):
+                _check(e.lib.engine_dihedral_add(e.ptr, int(i), int(j), int(k), int(l), int(pid)),
+                       "engine_dihedral_add")
         e.n = sysm.n
         if sysm.rigid is not None:
             for i, j, d in np.asarray(sysm.rigid):
@@ -481,6 +529,12 @@ class Engine:
         _check(self.lib.engine_cuda_getsort(self.ptr, cid, buf.ctypes.data_as(C.POINTER(C.c_uint)), buf.size),
                "engine_cuda_getsort")
         return buf[:13 * count].reshape(13, count)
+
+    def energies(self):
+        """e->s.epot and its parts after the last step or evaluation (engine_energies)."""
+        out = np.zeros(6)
+        _check(self.lib.engine_energies(self.ptr, _dptr(out)), "engine_energies")
+        return dict(zip(("total", "nonbond", "bond", "angle", "dihedral", "exclusion"), (float(v) for v in out)))
 
     def unload(self):
         x = np.zeros((self.n, 3)); t = np.zeros(self.n, np.int32); pid = np.zeros(self.n, np.int32)

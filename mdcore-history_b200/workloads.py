@@ -62,6 +62,10 @@ class System:
     ep: Optional[PotSpec] = None            # explicit electrostatic potential (engine_setexplepot)
     bonds: Optional[np.ndarray] = None      # (M,2) bonded particle ids
     bond_pot: Optional[PotSpec] = None      # the bond potential of every bonded type pair
+    angles: Optional[np.ndarray] = None     # (M,4) ids i, j (vertex), k and angle potential index
+    angle_pots: Optional[list] = None       # (a, b, K, theta0, tol) of potential_create_harmonic_angle
+    dihedrals: Optional[np.ndarray] = None  # (M,5) ids i, j, k, l and dihedral potential index
+    dihedral_pots: Optional[list] = None    # (K, n, delta, tol) of potential_create_harmonic_dihedral
 
     @property
     def n(self) -> int:
@@ -330,7 +334,7 @@ QSCALE = math.sqrt(Q_SCALE)     # e -> per-particle charge unit of tables with p
 
 def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box=(10.8, 10.8, 7.8), seed: int = 0,
                  cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12,
-                 bond_k: float = 2.0e5, clearance: float = 0.25) -> System:
+                 bond_k: float = 2.0e5, clearance: float = 0.25, angles_dihedrals: bool = True) -> System:
     """Heterogeneous solvated-chain system: `nchains` linear bead chains of `length` beads
     (bond 0.15 nm, 20 LJ bead types with sigma U[0.25, 0.40] nm and epsilon U[0.1, 1.0]
     kJ/mol, Lorentz-Berthelot mixing, charges N(0, 0.3) e neutralised per chain) and up to
@@ -342,6 +346,9 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     with unit charge, cutoff 1.2 nm); the type tables are LJ only (none for H).  1-2 and 1-3
     exclusions along the chains, the three intramolecular pairs of every water excluded;
     chain bonds harmonic, bond_k (r - 0.15 nm)^2 (bond_pot, a table on [0.05, 0.3] nm).
+    With `angles_dihedrals`, every three consecutive beads also form a harmonic angle
+    (CHAINS_ANGLE_POTS, one of two at random) and every four a dihedral (CHAINS_DIHEDRAL_POTS,
+    one of three at random, drawn after everything else so the positions do not depend on it).
     Types: 0 O, 1 H, 2..21 beads.  Seeded.
 
     Chains grow together as self-avoiding random walks (every new bead at least `clearance`
@@ -434,7 +441,130 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     masses = [15.9994, 1.008] + list(rng.uniform(12.0, 44.0, nbt))
     bonds = np.stack([i1, i1 + 1], 1).astype(np.int32)
     bond_pot = PotSpec(KIND_HARMONIC, 2, 2, 0.05, 0.3, 1e-5, (bond_k, bond, 0.0, 0.0))
+    angles = angle_pots = dihedrals = dihedral_pots = None
+    if angles_dihedrals and length >= 3:
+        angles = np.stack([i2, i2 + 1, i2 + 2, rng.integers(0, len(CHAINS_ANGLE_POTS), len(i2))], 1)
+        angle_pots = list(CHAINS_ANGLE_POTS)
+        if length >= 4:
+            i3 = (b0 + np.arange(length - 3)[None, :]).reshape(-1)
+            dihedrals = np.stack([i3, i3 + 1, i3 + 2, i3 + 3, rng.integers(0, len(CHAINS_DIHEDRAL_POTS), len(i3))], 1)
+            dihedral_pots = list(CHAINS_DIHEDRAL_POTS)
     return System(name=f"chains-water-{len(x)}", origin=np.zeros(3), dim=dim, L=np.full(3, cutoff), cutoff=cutoff,
                   masses=masses, charges=[0.0] * len(masses), pots=pots, x=_wrap(x, dim), type=typ,
                   excl=np.concatenate(ex).astype(np.int32), dt=0.002, rigid=rig, q=q, ep=ep,
-                  bonds=bonds, bond_pot=bond_pot)
+                  bonds=bonds, bond_pot=bond_pot,
+                  angles=None if angles is None else angles.astype(np.int32), angle_pots=angle_pots,
+                  dihedrals=None if dihedrals is None else dihedrals.astype(np.int32), dihedral_pots=dihedral_pots)
+
+
+# Bonded potentials of the chains: harmonic angles (a, b, K, theta0, tol) and harmonic
+# dihedrals (K, n, delta, tol).  The table builder (the reference's) needs an angle range
+# that stops short of 180 degrees and a dihedral phase of 0 or pi: dE/dcos is unbounded at
+# cos = -1 for an angle, and at cos = +-1 for a dihedral of any other phase, and no
+# interval count meets the tolerance (potential_err_ivalsmax).  Angles of the random-walk
+# chains beyond the range are held to it, as the reference holds them.
+CHAINS_ANGLE_POTS = [
+    (math.radians(60.0), math.radians(175.0), 120.0, math.radians(120.0), 1e-4),
+    (math.radians(50.0), math.radians(170.0), 80.0, math.radians(110.0), 1e-4),
+]
+CHAINS_DIHEDRAL_POTS = [(5.0, 3, 0.0, 1e-4), (2.0, 1, math.pi, 1e-4), (1.5, 2, 0.0, 1e-4)]
+
+
+def bonded_chains(nchains: int = 12, length: int = 20, box=(3.6, 3.6, 3.6), seed: int = 0, bond: float = 0.15,
+                  theta=(100.0, 150.0), tol: float = 1e-4) -> System:
+    """Bead chains with every bond angle in `theta` degrees (each bead placed from its three
+    predecessors by bond length, bond angle and a uniform random torsion), bonds, angles and
+    dihedrals as chains_water's, one LJ type (sigma 0.25 nm, epsilon 0.2 kJ/mol) and 1-2/1-3
+    exclusions; no solvent.  Chains may overlap each other: meant for the bonded terms."""
+    rng = np.random.default_rng(seed)
+    dim = np.array(box, np.float64)
+    pos = np.zeros((nchains, length, 3))
+    pos[:, 0] = rng.uniform(0, 1, (nchains, 3)) * dim
+    for c in range(nchains):
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        pos[c, 1] = pos[c, 0] + bond * d
+        for t in range(2, length):
+            a = pos[c, t - 1] - pos[c, t - 2]
+            a /= np.linalg.norm(a)
+            ref = pos[c, t - 3] - pos[c, t - 2] if t >= 3 else rng.normal(size=3)
+            n = np.cross(a, ref)
+            n /= np.linalg.norm(n)
+            m = np.cross(n, a)
+            th = math.radians(rng.uniform(*theta))
+            ph = rng.uniform(-math.pi, math.pi)
+            # the new bond makes angle th with the previous one (bond angle at bead t-1)
+            step = -math.cos(th) * a + math.sin(th) * (math.cos(ph) * m + math.sin(ph) * n)
+            pos[c, t] = pos[c, t - 1] + bond * step
+    x = _wrap(pos.reshape(-1, 3), dim)
+    b0 = np.arange(nchains)[:, None] * length
+    i1 = (b0 + np.arange(length - 1)[None, :]).reshape(-1)
+    i2 = (b0 + np.arange(length - 2)[None, :]).reshape(-1)
+    i3 = (b0 + np.arange(length - 3)[None, :]).reshape(-1)
+    ex = np.concatenate([np.stack([i1, i1 + 1], 1), np.stack([i2, i2 + 2], 1)]).astype(np.int32)
+    A, B = lj_AB(0.2, 0.25)
+    return System(name=f"bonded-chains-{len(x)}", origin=np.zeros(3), dim=dim, L=np.full(3, 1.2), cutoff=1.2,
+                  masses=[14.0], charges=[0.0], pots=[PotSpec(KIND_LJ126, 0, 0, 0.1, 1.2, tol, (A, B, 0.0, 0.0))],
+                  x=x, type=np.zeros(len(x), np.int32), excl=ex, dt=0.002,
+                  bonds=np.stack([i1, i1 + 1], 1).astype(np.int32),
+                  bond_pot=PotSpec(KIND_HARMONIC, 0, 0, 0.05, 0.3, 1e-5, (2.0e5, bond, 0.0, 0.0)),
+                  angles=np.stack([i2, i2 + 1, i2 + 2, rng.integers(0, 2, len(i2))], 1).astype(np.int32),
+                  angle_pots=list(CHAINS_ANGLE_POTS),
+                  dihedrals=np.stack([i3, i3 + 1, i3 + 2, i3 + 3, rng.integers(0, 3, len(i3))], 1).astype(np.int32),
+                  dihedral_pots=list(CHAINS_DIHEDRAL_POTS))
+
+
+def write_bondedfile(sysm: System, path: str) -> None:
+    """The bonded terms of sysm in the format `ref_driver bonded` reads (oracle/ref_driver.c):
+    the bond potential for every type pair that a bond joins."""
+    bonds = np.zeros((0, 2), np.int32) if sysm.bonds is None else np.asarray(sysm.bonds, np.int32)
+    pairs = sorted({(int(min(a, b)), int(max(a, b))) for a, b in np.asarray(sysm.type)[bonds]}) if len(bonds) else []
+    angles = np.zeros((0, 4), np.int32) if sysm.angles is None else np.asarray(sysm.angles, np.int32)
+    dihedrals = np.zeros((0, 5), np.int32) if sysm.dihedrals is None else np.asarray(sysm.dihedrals, np.int32)
+    apots = sysm.angle_pots or []
+    dpots = sysm.dihedral_pots or []
+    with open(path, "wb") as f:
+        f.write(b"MDB2BND1")
+        f.write(struct.pack("<6i", len(pairs), len(apots), len(dpots), len(bonds), len(angles), len(dihedrals)))
+        bp = sysm.bond_pot
+        for ti, tj in pairs:
+            f.write(struct.pack("<2i5d", ti, tj, bp.a, bp.b, bp.p[0], bp.p[1], bp.tol))
+        for a, b, K, th0, tol in apots:
+            f.write(struct.pack("<5d", a, b, K, th0, tol))
+        for K, n, delta, tol in dpots:
+            f.write(struct.pack("<2i3d", n, 0, K, delta, tol))
+        f.write(np.ascontiguousarray(bonds, "<i4").tobytes())
+        f.write(np.ascontiguousarray(angles, "<i4").tobytes())
+        f.write(np.ascontiguousarray(dihedrals, "<i4").tobytes())
+
+
+def read_bondedout(path: str):
+    """Parse the output of `ref_driver bonded`: forces by id of the bonds, the angles and the
+    dihedrals (float), their energies, cell-relative positions, cells and the tables
+    (n, alpha, coef, a, b) of the bond, angle and dihedral potentials in that order."""
+    buf = open(path, "rb").read()
+    assert buf[:8] == b"MDB2BOU1"
+    off = 8
+
+    def take(dtype, count):
+        nonlocal off
+        a = np.frombuffer(buf, dtype=dtype, count=count, offset=off)
+        off += a.nbytes
+        return a
+
+    N, nb, na, nd = (int(v) for v in take("<i4", 4))
+    fb = take("<f4", 3 * N).reshape(N, 3).copy()
+    fa = take("<f4", 3 * N).reshape(N, 3).copy()
+    fd = take("<f4", 3 * N).reshape(N, 3).copy()
+    eb, ea, ed = (float(v) for v in take("<f8", 3))
+    xr = take("<f4", 3 * N).reshape(N, 3).copy()
+    cell = take("<i4", N).copy()
+    tables = []
+    for _ in range(nb + na + nd):
+        (n,) = take("<i4", 1)
+        alpha = take("<f4", 4).copy()
+        c = take("<f4", (int(n) + 1) * 8).copy()
+        a, b = take("<f8", 2)
+        tables.append((int(n), alpha, c, float(a), float(b)))
+    return dict(f_bond=fb, f_angle=fa, f_dihedral=fd, e_bond=eb, e_angle=ea, e_dihedral=ed, xrel=xr, cell=cell,
+                bond_tables=tables[:nb], angle_tables=tables[nb:nb + na], dihedral_tables=tables[nb + na:])

@@ -26,6 +26,13 @@
  *     (src/potential_eval.h:84-103 restated in FP64);
  *   - sort keys: src/runner_dosort.c:140-153, ordered by descending distance with ties in
  *     storage order;
+ *   - bonded terms in double on the same float cell-relative positions: bonds
+ *     (src/bond.c:81-250), angles (src/angle.c:81-300) and dihedrals (src/dihedral.c:81-380),
+ *     each position taken near the cell of the second particle as the reference does, the
+ *     table interval picked from a float copy of the distance or cosine; angle and
+ *     dihedral gradients are written here from the vector form of d cos/dx (pinned against
+ *     the reference's own bond_eval/angle_eval/dihedral_eval outputs in
+ *     tests/golden/bonded.npz);
  *   - explicit electrostatics (the engine_setexplepot extension; the reference stores ep,
  *     src/engine.c:1029-1053, but no runner evaluates it): with table ep, every pair within
  *     the cutoff that is not excluded also contributes q_i q_j ep(r) to energy and force,
@@ -267,6 +274,151 @@ int oracle_bonds(int nb, const int *bij, const float *xrel, const int *cell, con
         for (int k = 0; k < 3; k++) {
             f_out[3 * i + k] -= fs * dx[k];
             f_out[3 * j + k] += fs * dx[k];
+        }
+        epot += e;
+    }
+    *e_out = epot;
+    return 0;
+}
+
+/* The table read at r itself (src/potential_eval.h:122-148, potential_eval_r): interval
+ * index from the float rf as the reference computes it, polynomial in double at r; e and
+ * dE/dr. */
+static void eval_fp64_r(const float *coef, const float *alpha, int nmax, float rf, double r, double *e, double *f) {
+    int ind = (int)fmaxf(0.0f, alpha[0] + rf * (alpha[1] + rf * alpha[2]));
+    if (ind > nmax) ind = nmax;
+    const float *c = &coef[8 * ind];
+    double x = (r - (double)c[0]) * (double)c[1];
+    double ee = (double)c[2] * x + (double)c[3];
+    double eff = (double)c[2];
+    for (int k = 4; k < 8; k++) {
+        eff = eff * x + ee;
+        ee = ee * x + (double)c[k];
+    }
+    *e = ee;
+    *f = eff * (double)c[1];
+}
+
+/* Position of particle p near the cell of particle q (src/angle.c:141-158,
+ * src/dihedral.c:146-171): its cell-relative position plus the cell edge times the cells'
+ * offset, held to -1..1 per dimension; in double (xd) and rounded to float as the
+ * reference stores it (xf). */
+static void near_cell(int p, int q, const float *xrel, const int *cell, const int *cdim, const double *h,
+                      double xd[3], float xf[3]) {
+    int lp[3], lq[3];
+    lp[0] = cell[p] / (cdim[1] * cdim[2]); lp[1] = (cell[p] / cdim[2]) % cdim[1]; lp[2] = cell[p] % cdim[2];
+    lq[0] = cell[q] / (cdim[1] * cdim[2]); lq[1] = (cell[q] / cdim[2]) % cdim[1]; lq[2] = cell[q] % cdim[2];
+    for (int k = 0; k < 3; k++) {
+        int sh = lp[k] - lq[k];
+        if (sh > 1) sh = -1;
+        else if (sh < -1) sh = 1;
+        xd[k] = (double)xrel[3 * p + k] + h[k] * sh;
+        xf[k] = (float)xd[k];
+    }
+}
+
+static double dotd(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static float dotf(const float *a, const float *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static void crossd(const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static void crossf(const float *a, const float *b, float *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1]; o[1] = a[2] * b[0] - a[0] * b[2]; o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* A cosine held to [-1, 1] and then to the table's range [ab[0], ab[1]]
+ * (src/angle.c:168, 183-187; src/dihedral.c:234, 254-260); the float copy picks the
+ * interval. */
+static void eval_cos(const float *coef, const float *alpha, int n, const double *ab, double c, float cf,
+                     double *e, double *f) {
+    c = fmax(-1.0, fmin(1.0, c));
+    cf = fmaxf(-1.0f, fminf(1.0f, cf));
+    if (c < ab[0] || c > ab[1]) c = fmax(ab[0], fmin(ab[1], c));
+    if (cf < ab[0] || cf > ab[1]) cf = (float)fmax(ab[0], fmin(ab[1], (double)cf));
+    eval_fp64_r(coef, alpha, n, cf, c, e, f);
+}
+
+/* Angles (src/angle.c:81-300) in double: for each angle (i, j, k, table t) of aijk[4 * na],
+ * u = x_i - x_j and w = x_k - x_j near j's cell, cos = u.w / (|u| |w|), the table (coef at
+ * coff[t], alpha[4 t], potn[t], range ab[2 t]) read at cos, and the forces
+ * -dE/dcos * dcos/dx with dcos/dx_i = (w/|w| - cos u/|u|)/|u|, dcos/dx_k = (u/|u| - cos w/|w|)/|w|,
+ * dcos/dx_j = -(the two).  Forces added into f_out (by id), energy into *e_out. */
+int oracle_angles(int na, const int *aijk, const float *xrel, const int *cell, const int *cdim, const double *dim,
+                  const float *coef, const int *coff, const float *alpha, const int *potn, const double *ab,
+                  double *f_out, double *e_out) {
+    double h[3], epot = 0.0;
+    for (int k = 0; k < 3; k++) h[k] = dim[k] / cdim[k];
+    for (int a = 0; a < na; a++) {
+        const int i = aijk[4 * a], j = aijk[4 * a + 1], kk = aijk[4 * a + 2], t = aijk[4 * a + 3];
+        double xi[3], xj[3], xk[3], u[3], w[3];
+        float fi[3], fj[3], fk[3], uf[3], wf[3];
+        near_cell(i, j, xrel, cell, cdim, h, xi, fi);
+        near_cell(j, j, xrel, cell, cdim, h, xj, fj);
+        near_cell(kk, j, xrel, cell, cdim, h, xk, fk);
+        for (int k = 0; k < 3; k++) {
+            u[k] = xi[k] - xj[k]; w[k] = xk[k] - xj[k];
+            uf[k] = fi[k] - fj[k]; wf[k] = fk[k] - fj[k];
+        }
+        const double iu = 1.0 / sqrt(dotd(u, u)), iw = 1.0 / sqrt(dotd(w, w));
+        const double c = fmax(-1.0, fmin(1.0, dotd(u, w) * iu * iw));
+        const float cf = dotf(uf, wf) * (1.0f / sqrtf(dotf(uf, uf))) * (1.0f / sqrtf(dotf(wf, wf)));
+        double e, fs;
+        eval_cos(coef + coff[t], alpha + 4 * t, potn[t], ab + 2 * t, c, cf, &e, &fs);
+        for (int k = 0; k < 3; k++) {
+            const double gi = (w[k] * iw - c * u[k] * iu) * iu, gk = (u[k] * iu - c * w[k] * iw) * iw;
+            f_out[3 * i + k] -= fs * gi;
+            f_out[3 * kk + k] -= fs * gk;
+            f_out[3 * j + k] += fs * (gi + gk);
+        }
+        epot += e;
+    }
+    *e_out = epot;
+    return 0;
+}
+
+/* Dihedrals (src/dihedral.c:81-380) in double: for each dihedral (i, j, k, l, table t) of
+ * dijkl[5 * nd], b1 = x_j - x_i, b2 = x_k - x_j, b3 = x_l - x_k near j's cell, normals
+ * n1 = b1 x b2, n2 = b2 x b3, cos = n1.n2 / (|n1| |n2|), the table read at cos, and the
+ * forces -dE/dcos * dcos/dx from g1 = (n2/|n2| - cos n1/|n1|)/|n1|,
+ * g2 = (n1/|n1| - cos n2/|n2|)/|n2|: dcos/db1 = b2 x g1, dcos/db3 = g2 x b2,
+ * dcos/db2 = g1 x b1 + b3 x g2. */
+int oracle_dihedrals(int nd, const int *dijkl, const float *xrel, const int *cell, const int *cdim,
+                     const double *dim, const float *coef, const int *coff, const float *alpha, const int *potn,
+                     const double *ab, double *f_out, double *e_out) {
+    double h[3], epot = 0.0;
+    for (int k = 0; k < 3; k++) h[k] = dim[k] / cdim[k];
+    for (int d = 0; d < nd; d++) {
+        const int i = dijkl[5 * d], j = dijkl[5 * d + 1], kk = dijkl[5 * d + 2], l = dijkl[5 * d + 3];
+        const int t = dijkl[5 * d + 4];
+        double x[4][3], b1[3], b2[3], b3[3], n1[3], n2[3];
+        float xf[4][3], b1f[3], b2f[3], b3f[3], n1f[3], n2f[3];
+        near_cell(i, j, xrel, cell, cdim, h, x[0], xf[0]);
+        near_cell(j, j, xrel, cell, cdim, h, x[1], xf[1]);
+        near_cell(kk, j, xrel, cell, cdim, h, x[2], xf[2]);
+        near_cell(l, j, xrel, cell, cdim, h, x[3], xf[3]);
+        for (int k = 0; k < 3; k++) {
+            b1[k] = x[1][k] - x[0][k]; b2[k] = x[2][k] - x[1][k]; b3[k] = x[3][k] - x[2][k];
+            b1f[k] = xf[1][k] - xf[0][k]; b2f[k] = xf[2][k] - xf[1][k]; b3f[k] = xf[3][k] - xf[2][k];
+        }
+        crossd(b1, b2, n1); crossd(b2, b3, n2);
+        crossf(b1f, b2f, n1f); crossf(b2f, b3f, n2f);
+        const double i1 = 1.0 / sqrt(dotd(n1, n1)), i2 = 1.0 / sqrt(dotd(n2, n2));
+        const double c = fmax(-1.0, fmin(1.0, dotd(n1, n2) * i1 * i2));
+        const float cf = dotf(n1f, n2f) * (1.0f / sqrtf(dotf(n1f, n1f))) * (1.0f / sqrtf(dotf(n2f, n2f)));
+        double e, fs, g1[3], g2[3], db1[3], db2[3], db3[3], t1[3], t2[3];
+        eval_cos(coef + coff[t], alpha + 4 * t, potn[t], ab + 2 * t, c, cf, &e, &fs);
+        for (int k = 0; k < 3; k++) {
+            g1[k] = (n2[k] * i2 - c * n1[k] * i1) * i1;
+            g2[k] = (n1[k] * i1 - c * n2[k] * i2) * i2;
+        }
+        crossd(b2, g1, db1); crossd(g2, b2, db3); crossd(g1, b1, t1); crossd(b3, g2, t2);
+        for (int k = 0; k < 3; k++) {
+            db2[k] = t1[k] + t2[k];
+            const double di = -db1[k], dj = db1[k] - db2[k], dk = db2[k] - db3[k], dl = db3[k];
+            f_out[3 * i + k] -= fs * di;
+            f_out[3 * j + k] -= fs * dj;
+            f_out[3 * kk + k] -= fs * dk;
+            f_out[3 * l + k] -= fs * dl;
         }
         epot += e;
     }

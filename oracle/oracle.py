@@ -141,6 +141,44 @@ def bonds(sysm, table, binned=None):
     return dict(f=f, epot=e.value)
 
 
+def _bonded(fn, terms, width, sysm, tables, xrel, cell, cdim):
+    """Calls oracle_angles / oracle_dihedrals: terms (M, width) ids and table index; tables
+    [(n, alpha, coef, a, b)] by potential index."""
+    N = sysm.n
+    f = np.zeros((N, 3), np.float64)
+    e = C.c_double()
+    t = np.ascontiguousarray(np.asarray(terms, np.int32).reshape(-1, width))
+    coef = np.ascontiguousarray(np.concatenate([np.asarray(tb[2], np.float32) for tb in tables]), np.float32)
+    coff = np.ascontiguousarray(np.cumsum([0] + [len(tb[2]) for tb in tables[:-1]]), np.int32)
+    alpha = np.ascontiguousarray(np.concatenate([np.asarray(tb[1], np.float32) for tb in tables]), np.float32)
+    potn = np.ascontiguousarray([tb[0] for tb in tables], np.int32)
+    ab = np.ascontiguousarray([[tb[3], tb[4]] for tb in tables], np.float64).reshape(-1)
+    xrel = np.ascontiguousarray(xrel, np.float32)
+    cell = np.ascontiguousarray(cell, np.int32)
+    cdim = np.ascontiguousarray(cdim, np.int32)
+    dim = np.ascontiguousarray(sysm.dim, np.float64)
+    fn(len(t), _p(t, C.c_int), _p(xrel, C.c_float), _p(cell, C.c_int), _p(cdim, C.c_int), _p(dim, C.c_double),
+       _p(coef, C.c_float), _p(coff, C.c_int), _p(alpha, C.c_float), _p(potn, C.c_int), _p(ab, C.c_double),
+       _p(f, C.c_double), C.byref(e))
+    return dict(f=f, epot=e.value)
+
+
+def angles(sysm, tables, binned=None, xrel=None, cell=None):
+    """FP64 angle forces (by id) and energy of sysm.angles (oracle_angles); tables
+    [(n, alpha, coef, a, b)] of sysm.angle_pots.  Positions from bin_system(sysm) unless
+    xrel and cell are given."""
+    b = binned or bin_system(sysm)
+    return _bonded(lib().oracle_angles, sysm.angles, 4, sysm, tables, b["xrel"] if xrel is None else xrel,
+                   b["cell"] if cell is None else cell, b["cdim"])
+
+
+def dihedrals(sysm, tables, binned=None, xrel=None, cell=None):
+    """FP64 dihedral forces (by id) and energy of sysm.dihedrals (oracle_dihedrals)."""
+    b = binned or bin_system(sysm)
+    return _bonded(lib().oracle_dihedrals, sysm.dihedrals, 5, sysm, tables, b["xrel"] if xrel is None else xrel,
+                   b["cell"] if cell is None else cell, b["cdim"])
+
+
 def sortkeys(xrel_cell: np.ndarray, h, sid: int) -> np.ndarray:
     n = len(xrel_cell)
     keys = np.zeros(max(n, 1), np.uint32)

@@ -20,6 +20,18 @@
  *       Loads the system with velocities and rigid constraints, sets dt from the rigid file,
  *       starts nr_runners runners and times full engine_step calls (sort + sweep +
  *       exclusions + integration + P-SHAKE, src/engine.c:2070-2240); one JSON line.
+ *   ref_driver bonded <sysfile> <bondedfile> <outfile>
+ *       Loads the system (no runners), adds the bonded potentials and terms of the bonded
+ *       file (engine_bond_addpot/engine_bond_add, engine_angle_addpot/engine_angle_add,
+ *       engine_dihedral_addpot/engine_dihedral_add with potential_create_harmonic,
+ *       _harmonic_angle and _harmonic_dihedral), then calls the reference's bond_eval,
+ *       angle_eval and dihedral_eval (src/bond.c:81, src/angle.c:81, src/dihedral.c:81)
+ *       once each on zeroed forces and dumps each one's forces and energy, the
+ *       cell-relative positions and cells, and every bonded table.  Bonded file
+ *       (little-endian): "MDB2BND1", int32 nbondpot, nangpot, ndihpot, nbond, nang, ndih;
+ *       nbondpot x {int32 ti, tj; double a, b, K, r0, tol}; nangpot x {double a, b, K,
+ *       theta0, tol}; ndihpot x {int32 n, pad; double K, delta, tol}; nbond x {int32 i, j};
+ *       nang x {int32 i, j, k, pid}; ndih x {int32 i, j, k, l, pid}.
  *   ref_driver bench <sysfile> <nr_runners> <warmup> <steps>
  *       Times engine_step (dt = 0: sort + pair/self sweep + exclusion subtraction +
  *       bookkeeping, src/engine.c:2070-2240) with clock_gettime and prints one JSON line.
@@ -257,6 +269,111 @@ static int do_forces(const char *sysf, const char *outf, int runners) {
     return 0;
 }
 
+static void zero_forces(struct engine *e, int N) {
+    int id;
+    for (id = 0; id < N; id++) e->s.partlist[id]->f[0] = e->s.partlist[id]->f[1] = e->s.partlist[id]->f[2] = 0.0f;
+}
+
+static void dump_forces(struct engine *e, int N, FILE *out) {
+    int id;
+    for (id = 0; id < N; id++) fwrite(e->s.partlist[id]->f, sizeof(float), 3, out);
+}
+
+static void dump_table(const struct potential *p, FILE *out) {
+    int n = p->n;
+    double ab[2];
+    fwrite(&n, sizeof(int), 1, out);
+    fwrite(p->alpha, sizeof(float), 4, out);
+    fwrite(p->c, sizeof(float), (size_t)(n + 1) * potential_chunk, out);
+    ab[0] = p->a; ab[1] = p->b;
+    fwrite(ab, sizeof(double), 2, out);
+}
+
+static int do_bonded(const char *sysf, const char *bndf, const char *outf) {
+    struct sys_desc sd;
+    static struct engine e;
+    struct potential **pots, **bp, **ap, **dp;
+    char magic[8];
+    int hdr[6], k, id;
+    double en[3] = {0.0, 0.0, 0.0};
+    FILE *f, *out;
+    if (sys_read(sysf, &sd) != 0) { fprintf(stderr, "ref_driver: bad system file %s\n", sysf); return 1; }
+    if (build_v(&e, &sd, &pots, 1, NULL, 0, 0) != 0) return 1;
+    f = fopen(bndf, "rb");
+    if (f == NULL || fread(magic, 1, 8, f) != 8 || memcmp(magic, "MDB2BND1", 8) != 0 ||
+        fread(hdr, sizeof(int), 6, f) != 6) {
+        fprintf(stderr, "ref_driver: bad bonded file %s\n", bndf);
+        return 1;
+    }
+    bp = malloc(sizeof(struct potential *) * (hdr[0] + 1));
+    ap = malloc(sizeof(struct potential *) * (hdr[1] + 1));
+    dp = malloc(sizeof(struct potential *) * (hdr[2] + 1));
+    for (k = 0; k < hdr[0]; k++) {
+        int t[2];
+        double d[5];
+        if (fread(t, sizeof(int), 2, f) != 2 || fread(d, sizeof(double), 5, f) != 5) return 1;
+        if ((bp[k] = potential_create_harmonic(d[0], d[1], d[2], d[3], d[4])) == NULL) { errs_dump(stderr); return 1; }
+        if (engine_bond_addpot(&e, bp[k], t[0], t[1]) < 0) { errs_dump(stderr); return 1; }
+    }
+    for (k = 0; k < hdr[1]; k++) {
+        double d[5];
+        if (fread(d, sizeof(double), 5, f) != 5) return 1;
+        if ((ap[k] = potential_create_harmonic_angle(d[0], d[1], d[2], d[3], d[4])) == NULL) { errs_dump(stderr); return 1; }
+        if (engine_angle_addpot(&e, ap[k]) != k) { errs_dump(stderr); return 1; }
+    }
+    for (k = 0; k < hdr[2]; k++) {
+        int t[2];
+        double d[3];
+        if (fread(t, sizeof(int), 2, f) != 2 || fread(d, sizeof(double), 3, f) != 3) return 1;
+        if ((dp[k] = potential_create_harmonic_dihedral(d[0], t[0], d[1], d[2])) == NULL) { errs_dump(stderr); return 1; }
+        if (engine_dihedral_addpot(&e, dp[k]) != k) { errs_dump(stderr); return 1; }
+    }
+    for (k = 0; k < hdr[3]; k++) {
+        int t[2];
+        if (fread(t, sizeof(int), 2, f) != 2) return 1;
+        if (engine_bond_add(&e, t[0], t[1]) < 0) { errs_dump(stderr); return 1; }
+    }
+    for (k = 0; k < hdr[4]; k++) {
+        int t[4];
+        if (fread(t, sizeof(int), 4, f) != 4) return 1;
+        if (engine_angle_add(&e, t[0], t[1], t[2], t[3]) < 0) { errs_dump(stderr); return 1; }
+    }
+    for (k = 0; k < hdr[5]; k++) {
+        int t[5];
+        if (fread(t, sizeof(int), 5, f) != 5) return 1;
+        if (engine_dihedral_add(&e, t[0], t[1], t[2], t[3], t[4]) < 0) { errs_dump(stderr); return 1; }
+    }
+    fclose(f);
+    out = fopen(outf, "wb");
+    if (out == NULL) return 1;
+    fwrite("MDB2BOU1", 1, 8, out);
+    {
+        int oh[4];
+        oh[0] = sd.N; oh[1] = hdr[0]; oh[2] = hdr[1]; oh[3] = hdr[2];
+        fwrite(oh, sizeof(int), 4, out);
+    }
+    zero_forces(&e, sd.N);
+    if (bond_eval(e.bonds, e.nr_bonds, &e, &en[0]) < 0) { errs_dump(stderr); return 1; }
+    dump_forces(&e, sd.N, out);
+    zero_forces(&e, sd.N);
+    if (angle_eval(e.angles, e.nr_angles, &e, &en[1]) < 0) { errs_dump(stderr); return 1; }
+    dump_forces(&e, sd.N, out);
+    zero_forces(&e, sd.N);
+    if (dihedral_eval(e.dihedrals, e.nr_dihedrals, &e, &en[2]) < 0) { errs_dump(stderr); return 1; }
+    dump_forces(&e, sd.N, out);
+    fwrite(en, sizeof(double), 3, out);
+    for (id = 0; id < sd.N; id++) fwrite(e.s.partlist[id]->x, sizeof(float), 3, out);
+    for (id = 0; id < sd.N; id++) {
+        int c = (int)(e.s.celllist[id] - e.s.cells);
+        fwrite(&c, sizeof(int), 1, out);
+    }
+    for (k = 0; k < hdr[0]; k++) dump_table(bp[k], out);
+    for (k = 0; k < hdr[1]; k++) dump_table(ap[k], out);
+    for (k = 0; k < hdr[2]; k++) dump_table(dp[k], out);
+    fclose(out);
+    return 0;
+}
+
 static double now_s(void) {
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -295,6 +412,8 @@ int main(int argc, char *argv[]) {
         return do_mdbench(argv[2], argv[3], atoi(argv[4]), atoi(argv[5]), atoi(argv[6]));
     if (argc >= 6 && strcmp(argv[1], "rigid") == 0)
         return do_rigid(argv[2], argv[3], argv[4], atoi(argv[5]));
+    if (argc >= 5 && strcmp(argv[1], "bonded") == 0)
+        return do_bonded(argv[2], argv[3], argv[4]);
     if (argc >= 6 && strcmp(argv[1], "bench") == 0)
         return do_bench(argv[2], atoi(argv[3]), atoi(argv[4]), atoi(argv[5]));
     fprintf(stderr, "usage: ref_driver forces <sys> <out> <runners> | bench <sys> <runners> <warmup> <steps>\n");

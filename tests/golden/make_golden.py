@@ -12,6 +12,10 @@ Fixtures
   argon_1372.npz   jittered FCC LJ argon, 1,372 atoms, 4^3 cells, table tol 1e-4
   water_3000.npz   rigid SPC/E water, 1,000 molecules, 3^3 cells, 3,000 exclusions
   tables.npz       float tables of potential_create_* for a parameter sweep
+  bonded.npz       bead chains (W.bonded_chains: 12 chains of 20 beads, bond angles 100-150
+                   degrees) with harmonic bonds, angles and dihedrals: the reference's
+                   bond_eval, angle_eval and dihedral_eval forces (FP32, by id) and energies,
+                   each alone, the cell-relative positions and cells, and the bonded tables
   water_rigid.npz  the water_3000 system with its 3,000 distance constraints (O-H, O-H, H-H)
                    and Maxwell-Boltzmann velocities at 300 K: the reference's
                    engine_rigid_eval, P-SHAKE three times in a row (matrix refinement on)
@@ -171,6 +175,32 @@ def table_fixture(tmp):
     np.savez_compressed(os.path.join(HERE, "tables.npz"), ncases=len(TABLE_CASES), **out)
 
 
+def bonded_fixture(tmp):
+    sysm = W.bonded_chains()
+    sysf, bndf, outf = (os.path.join(tmp, n) for n in ("b.sys", "b.bnd", "b.out"))
+    W.write_sysfile(sysm, sysf)
+    W.write_bondedfile(sysm, bndf)
+    subprocess.run([DRIVER, "bonded", sysf, bndf, outf], check=True)
+    ref = W.read_bondedout(outf)
+    out = dict(x=sysm.x, dim=sysm.dim, L=sysm.L, cutoff=np.float64(sysm.cutoff), type=sysm.type, excl=sysm.excl,
+               mass=np.array(sysm.masses), lj=np.array([[p.a, p.b, p.tol, *p.p] for p in sysm.pots]),
+               bonds=sysm.bonds, bond_pot=np.array([sysm.bond_pot.a, sysm.bond_pot.b, sysm.bond_pot.tol,
+                                                    *sysm.bond_pot.p]),
+               angles=sysm.angles, angle_pots=np.array(sysm.angle_pots, np.float64),
+               dihedrals=sysm.dihedrals, dihedral_pots=np.array(sysm.dihedral_pots, np.float64))
+    for key in ("f_bond", "f_angle", "f_dihedral", "xrel", "cell"):
+        out[key] = ref[key]
+    out["energies"] = np.array([ref["e_bond"], ref["e_angle"], ref["e_dihedral"]])
+    for kind in ("bond", "angle", "dihedral"):
+        for k, (n, alpha, c, a, b) in enumerate(ref[f"{kind}_tables"]):
+            out[f"{kind}{k}_n"] = np.int32(n)
+            out[f"{kind}{k}_alpha"] = alpha
+            out[f"{kind}{k}_c"] = c
+            out[f"{kind}{k}_ab"] = np.array([a, b])
+    np.savez_compressed(os.path.join(HERE, "bonded.npz"), **out)
+    print("bonded", sysm.n, "beads,", len(sysm.angles), "angles,", len(sysm.dihedrals), "dihedrals")
+
+
 if __name__ == "__main__":
     if not os.path.exists(DRIVER):
         sys.exit("build the reference first: make -f oracle/Makefile.ref")
@@ -179,3 +209,4 @@ if __name__ == "__main__":
         system_fixture(W.water_spce(10), "water_3000.npz", tmp)
         table_fixture(tmp)
         rigid_fixture(tmp)
+        bonded_fixture(tmp)

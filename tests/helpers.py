@@ -22,6 +22,36 @@ def load_golden(fname):
     return sysm, ref
 
 
+def load_bonded_golden():
+    """The bonded-chains fixture: (System with bonds, angles and dihedrals; dict of the
+    reference's outputs with its tables as lists of (n, alpha, coef, a, b))."""
+    z = np.load(os.path.join(GOLDEN, "bonded.npz"))
+    lj = z["lj"]
+    bp = z["bond_pot"]
+    sysm = W.System(name="bonded-golden", origin=np.zeros(3), dim=z["dim"], L=z["L"], cutoff=float(z["cutoff"]),
+                    masses=list(z["mass"]), charges=[0.0] * len(z["mass"]),
+                    pots=[W.PotSpec(W.KIND_LJ126, 0, 0, float(r[0]), float(r[1]), float(r[2]),
+                                    tuple(float(v) for v in r[3:7])) for r in lj],
+                    x=z["x"], type=z["type"].astype(np.int32), excl=z["excl"].astype(np.int32).reshape(-1, 2),
+                    bonds=z["bonds"].astype(np.int32),
+                    bond_pot=W.PotSpec(W.KIND_HARMONIC, 0, 0, float(bp[0]), float(bp[1]), float(bp[2]),
+                                       tuple(float(v) for v in bp[3:7])),
+                    angles=z["angles"].astype(np.int32),
+                    angle_pots=[tuple(float(v) for v in r) for r in z["angle_pots"]],
+                    dihedrals=z["dihedrals"].astype(np.int32),
+                    dihedral_pots=[(float(r[0]), int(r[1]), float(r[2]), float(r[3])) for r in z["dihedral_pots"]])
+    ref = {k: z[k] for k in z.files}
+    for kind in ("bond", "angle", "dihedral"):
+        ref[f"{kind}_tables"] = []
+        k = 0
+        while f"{kind}{k}_n" in z.files:
+            ab = z[f"{kind}{k}_ab"]
+            ref[f"{kind}_tables"].append((int(z[f"{kind}{k}_n"]), z[f"{kind}{k}_alpha"], z[f"{kind}{k}_c"],
+                                          float(ab[0]), float(ab[1])))
+            k += 1
+    return sysm, ref
+
+
 def tables_of(sysm):
     """The library's tables of a system's potentials, in oracle order (type tables, then the
     explicit electrostatic potential's, if any)."""

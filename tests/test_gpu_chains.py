@@ -57,8 +57,9 @@ def test_full_size_chain_system_vs_oracle():
 def test_chain_device_steps_equal_host_steps():
     """Without the chain bonds (engine_step_host has no bonds): explicit electrostatics,
     global tables and rigid water, host steps against device steps bit for bit."""
-    sysm = dataclasses.replace(W.chains_water(nchains=4, length=20, nwater=300, box=(3.6, 3.6, 3.6), seed=2, gap=0.3),
-                               bonds=None, bond_pot=None)
+    sysm = W.chains_water(nchains=4, length=20, nwater=300, box=(3.6, 3.6, 3.6), seed=2, gap=0.3,
+                          angles_dihedrals=False)
+    sysm = dataclasses.replace(sysm, bonds=None, bond_pot=None)
     sysm.v = W.maxwell_velocities(sysm, 300.0, seed=3)
     out = []
     for device in (False, True):
@@ -79,7 +80,7 @@ def test_bond_forces_vs_oracle():
     """Chains alone (no water): one device step with dt = 0 leaves the particles in place and
     returns the forces of the sweep plus the harmonic chain bonds; against the oracle's
     nonbonded and bond forces.  The engine's potential energy is the sum of both."""
-    sysm = W.chains_water(nchains=12, length=40, nwater=0, box=(3.6, 3.6, 3.6), seed=5)
+    sysm = W.chains_water(nchains=12, length=40, nwater=0, box=(3.6, 3.6, 3.6), seed=5, angles_dihedrals=False)
     sysm.dt = 0.0
     e = M.Engine.from_system(sysm)
     e.step()
@@ -124,6 +125,129 @@ def test_bonded_chains_hold_together():
 
 def test_host_step_refuses_bonds():
     sysm = W.chains_water(nchains=2, length=10, nwater=0, box=(3.6, 3.6, 3.6), seed=1)
+    e = M.Engine.from_system(sysm)
+    with pytest.raises(M.MdcoreError, match="-30"):
+        e.step_host()
+    M.lib().errs_clear()
+    e.close()
+
+
+def bonded_oracle(sysm):
+    """Oracle nonbonded + bond + angle + dihedral forces (by id) and the energies."""
+    o = O.nonbond(sysm, tables_of(sysm))
+    ob = O.bonds(sysm, M.create_potential(sysm.bond_pot).contents.table())
+    oa = O.angles(sysm, M.bonded_tables([M.create_angle_potential(*p) for p in sysm.angle_pots]))
+    od = O.dihedrals(sysm, M.bonded_tables([M.create_dihedral_potential(*p) for p in sysm.dihedral_pots]))
+    return o, ob, oa, od
+
+
+def test_angle_dihedral_forces_vs_oracle():
+    """Chains with bonds, angles (bond angles 100-150 degrees) and dihedrals, no solvent:
+    one device step with dt = 0 returns the sweep's forces plus the three bonded terms',
+    against the oracle's (FP32 on the device, FP64 in the oracle); the potential energy is
+    the sum of the four.  The largest single-atom error comes from FP32 pair forces at the
+    close contacts of chains that cross one another (the nonbonded part), hence the F_rms
+    bound of 5e-5; the bonded terms alone are checked in the next test."""
+    sysm = W.bonded_chains(nchains=4, seed=3)
+    sysm.dt = 0.0
+    e = M.Engine.from_system(sysm)
+    e.step()
+    _, _, f, _ = e.parts()
+    o, ob, oa, od = bonded_oracle(sysm)
+    ftot = o["f"] + ob["f"] + oa["f"] + od["f"]
+    err = force_errors(f.astype(np.float64), ftot)
+    print("bonded chains", err)
+    assert err["global_rel"] <= 1e-5, err
+    assert err["max_over_frms"] <= 5e-5, err
+    en = e.energies()
+    print("energies", en, "oracle", o["epot"], ob["epot"], oa["epot"], od["epot"])
+    assert abs(en["nonbond"] - o["epot"]) <= 1e-6 * o["epot_abs"]
+    assert abs(en["bond"] - ob["epot"]) <= 1e-6 * abs(oa["epot"])
+    assert abs(en["angle"] - oa["epot"]) <= 1e-6 * abs(oa["epot"])
+    assert abs(en["dihedral"] - od["epot"]) <= 1e-6 * abs(od["epot"])
+    assert en["total"] == en["nonbond"] + en["bond"] + en["angle"] + en["dihedral"]
+    assert e.stats().status == 0
+    e.close()
+
+
+def test_angle_dihedral_forces_alone():
+    """The same step without the angles and dihedrals: the difference of the two steps'
+    forces (each a fixed-point sum, rounded once to float) is the angles' and dihedrals'
+    forces, against the oracle's."""
+    full = W.bonded_chains(nchains=4, seed=3)
+    full.dt = 0.0
+    bare = dataclasses.replace(full, angles=None, angle_pots=None, dihedrals=None, dihedral_pots=None)
+    out = []
+    for sysm in (full, bare):
+        e = M.Engine.from_system(sysm)
+        e.step()
+        _, _, f, _ = e.parts()
+        out.append(f.astype(np.float64))
+        e.close()
+    _, _, oa, od = bonded_oracle(full)
+    df = out[0] - out[1]
+    err = force_errors(df, oa["f"] + od["f"])
+    print("angles + dihedrals", err)
+    assert err["global_rel"] <= 1e-5, err
+    assert err["max_over_frms"] <= 3e-5, err
+
+
+def test_bonded_resident_steps_equal_engine_step():
+    """Twenty steps of bonded chains at 300 K (dt 1 fs): device-resident steps and
+    engine_step give the same trajectory bit for bit."""
+    sysm = W.bonded_chains(nchains=4, seed=3)
+    sysm.dt = 0.001
+    sysm.v = W.maxwell_velocities(sysm, 300.0, seed=4)
+    out = []
+    for resident in (False, True):
+        e = M.Engine.from_system(sysm)
+        if resident:
+            e.graph(True)
+            e.resident_begin().resident_steps(20).resident_end()
+        else:
+            for _ in range(20):
+                e.step()
+        x, t, pid, epot = e.unload()
+        pos = np.zeros((sysm.n, 3))
+        pos[pid] = x
+        out.append((pos, epot))
+        e.close()
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+def test_bonded_batch_equals_single_engines():
+    """Three bonded-chain systems stepped as one batch (engine_batch_step) and each alone
+    (engine_step): the same positions and energies bit for bit (the angle and dihedral
+    records carry their engine)."""
+    systems = [W.bonded_chains(nchains=4, seed=s) for s in (3, 4, 5)]
+    for k, s in enumerate(systems):
+        s.v = W.maxwell_velocities(s, 300.0, seed=10 + k)
+        s.dt = 0.001
+    single = []
+    for s in systems:
+        e = M.Engine.from_system(s)
+        for _ in range(4):
+            e.step()
+        single.append(e.unload())
+        e.close()
+    engines = [M.Engine.from_system(s, start=False) for s in systems]
+    b = M.Batch(engines)
+    for _ in range(4):
+        b.step()
+        assert b.stats().status == 0
+    for e, (x1, t1, p1, ep1) in zip(engines, single):
+        x2, t2, p2, ep2 = e.unload()
+        o1, o2 = np.argsort(p1), np.argsort(p2)
+        assert np.array_equal(p1[o1], p2[o2])
+        assert np.array_equal(x1[o1], x2[o2])
+        assert ep1 == ep2
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_host_step_refuses_angles():
+    sysm = dataclasses.replace(W.bonded_chains(nchains=2, seed=1), bonds=None, bond_pot=None)
     e = M.Engine.from_system(sysm)
     with pytest.raises(M.MdcoreError, match="-30"):
         e.step_host()
