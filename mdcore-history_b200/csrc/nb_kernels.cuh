@@ -30,12 +30,12 @@ __constant__ float c_axes[13][3];
 //    networks of shuffles over groups of lanes (several directions at once when it holds
 //    16 particles or fewer);
 //  * a larger cell's positions are staged once in shared memory, and it is sorted by all
-//    warps of the block, one warp per direction, with a
-//    counting sort on the top bits of the 16-bit distance (64 buckets in the warp's
-//    shared memory) and an exact rank inside the bucket: position = (keys in farther
-//    buckets) + (keys of the same bucket with a larger distance, or an equal distance and a
-//    smaller storage index).
-constexpr int kSortBuckets = 64;
+//    warps of the block, one warp per direction, with a counting sort into 128 buckets
+//    that split the direction's own distance range [min, max] evenly (a few keys per
+//    bucket) and an exact rank inside the bucket: position = (keys in farther buckets) +
+//    (keys of the same bucket with a larger distance, or an equal distance and a smaller
+//    storage index).
+constexpr int kSortBuckets = 128;
 constexpr int kSortWarps = 13;
 
 // Shared memory of one sorting warp for cells of up to scap particles (a multiple of 4):
@@ -128,29 +128,41 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
         if (!((mask >> sid) & 1u)) continue;
         const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
         for (int b = lane; b < kSortBuckets; b += 32) { bcount[b] = 0; bfill[b] = 0; }
-        __syncwarp();
+        unsigned dlo = 0xffffu, dhi = 0u;
         for (int k = lane; k < n; k += 32) {
-            const unsigned key = ((unsigned)k << 16) | sort_dist(xs[k], nx, ny, nz, dscale, bias);
-            skey[k] = key;
-            atomicAdd(&bcount[min((int)((key & 0xffffu) >> 9), kSortBuckets - 1)], 1);
+            const unsigned d = sort_dist(xs[k], nx, ny, nz, dscale, bias);
+            skey[k] = ((unsigned)k << 16) | d;
+            dlo = min(dlo, d);
+            dhi = max(dhi, d);
         }
+        // buckets spread over this direction's own distance range (monotonic in the distance)
+        dlo = __reduce_min_sync(FULL, dlo);
+        dhi = __reduce_max_sync(FULL, dhi);
+        const float bsc = (float)kSortBuckets / (float)(dhi - dlo + 1u);
+        auto bucket_of = [&](unsigned d) { return min((int)((float)(d - dlo) * bsc), kSortBuckets - 1); };
         __syncwarp();
-        {   // bucket starts in descending bucket order: lane l owns buckets 63-2l, 62-2l
-            const int bh = kSortBuckets - 1 - 2 * lane, bl = bh - 1;
-            const int ch = bcount[bh], cl = bcount[bl];
-            int incl = ch + cl;
+        for (int k = lane; k < n; k += 32) atomicAdd(&bcount[bucket_of(skey[k] & 0xffffu)], 1);
+        __syncwarp();
+        {   // bucket starts in descending bucket order: lane l owns the kPer buckets below
+            // kSortBuckets - kPer l
+            constexpr int kPer = kSortBuckets / 32;
+            const int btop = kSortBuckets - 1 - kPer * lane;
+            int c[kPer], tot = 0;
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) { c[q] = bcount[btop - q]; tot += c[q]; }
+            int incl = tot;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int t = __shfl_up_sync(FULL, incl, o);
                 if (lane >= o) incl += t;
             }
-            const int excl = incl - ch - cl;
-            bstart[bh] = excl;
-            bstart[bl] = excl + ch;
+            int run = incl - tot;
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) { bstart[btop - q] = run; run += c[q]; }
         }
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const int b = min((int)((skey[k] & 0xffffu) >> 9), kSortBuckets - 1);
+            const int b = bucket_of(skey[k] & 0xffffu);
             members[bstart[b] + atomicAdd(&bfill[b], 1)] = (unsigned short)k;
         }
         __syncwarp();
@@ -158,7 +170,7 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
         for (int k = lane; k < n; k += 32) {
             const unsigned mine = skey[k];
             const unsigned md = mine & 0xffffu;
-            const int b = min((int)(md >> 9), kSortBuckets - 1);
+            const int b = bucket_of(md);
             const int b0 = bstart[b], nb = bcount[b];
             int rank = b0;
             for (int m = 0; m < nb; ++m) {
@@ -172,7 +184,7 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
     }
 }
 
-__global__ void __launch_bounds__(kSortWarps * 32) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+__global__ void __launch_bounds__(kSortWarps * 32, 4) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
                                                               const int* __restrict__ ccount,
                                                               const unsigned* __restrict__ cmask,
                                                               unsigned* __restrict__ keys,
