@@ -590,6 +590,10 @@ def ours(args, rank, world, local_rank):
             line["shake_max_iterations"] = shake
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_sample(systems, host_threads())
+            if line["cpu_baseline"]["value"] is not None:     # the same sample on one runner
+                one = cpu_sample(systems, 1, steps=2)
+                line["cpu_baseline"]["one_core"] = {"value": one["value"], "ms_per_step": one.get("ms_per_step"),
+                                                    "sample": one["sample"]}
         print(json.dumps(line))
     tgt.close()
     for e in engines:
