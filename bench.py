@@ -26,8 +26,11 @@ autotuner.
           and through engine_nonbond_cuda with host buffers.
   roofline    the sweep kernel inside the timed resident steps (its own CUDA events).
 
-Multi-GPU: the path is not partitioned here ("replicas only"): each rank steps its own
-copy of the workload and value = ranks * pairs / max-over-ranks time.
+Multi-GPU: a single system is not partitioned here ("replicas only"): each rank steps its
+own copy of the workload and value = ranks * pairs / max-over-ranks time (weak scaling).
+The replica ensemble (--workload replicas) is dealt round-robin over the ranks instead
+(rank r steps replicas r, r + N, ...): value = the pairs of all ranks / max-over-ranks time
+(strong scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 """
@@ -255,6 +258,16 @@ def reduce_max(values, dist, device):
     return [float(v) for v in t.tolist()]
 
 
+def reduce_sum(values, dist, device):
+    """Every rank's counts -> their sums over the ranks; unchanged with one rank."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
 def cell_counts(sysm, e):
     """Particles per cell of one engine (cells as space_init lays them out)."""
     import numpy as np
@@ -400,7 +413,8 @@ def ours(args, rank, world, local_rank):
 
     built = build_system()
     replicas = isinstance(built, list)
-    systems = built if replicas else [built]
+    share = replicas and world > 1          # the ensemble dealt round-robin over the ranks
+    systems = (built[rank::world] if share else built) if replicas else [built]
     dt_fs = systems[0].dt * 1e3
     rigid = any(s.rigid is not None and len(s.rigid) for s in systems)
     if replicas:
@@ -536,6 +550,10 @@ def ours(args, rank, world, local_rank):
 
     ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e = reduce_max([ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e],
                                                               dist, "cuda")
+    if share:
+        pairs_all, plain_all, fe_all = reduce_sum([pairs, plain_pairs / args.steps, fe_pairs], dist, "cuda")
+    else:
+        pairs_all, plain_all, fe_all = world * pairs, world * (plain_pairs / args.steps), world * fe_pairs
     if rank == 0:
         peak = M.fp32_peak_tflops(local_rank)
         achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
@@ -549,20 +567,23 @@ def ours(args, rank, world, local_rank):
         # with empty cells), sweep, integration, constraints (rigid, one per engine)
         per_step = 2 + 1 + 3 * int(compact) + 1 + 1 + int(rigid) * len(engines)
         line = {
-            "metric": METRIC, "value": world * pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": pairs_all / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "strong" if share else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "ns_per_day": ns_per_day(ms, dt_fs),
-            "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
-                       "pairs_per_step": pairs, "candidates_per_step": int(st.candidates),
-                       "tasks": tgt.ntasks(), "cells": ncells, "parallelism": f"replicas x{world}",
+            "config": {"workload": WORKLOADS[SELECTED][0],
+                       "atoms": int(sum(s.n for s in (built if replicas else systems))),
+                       "pairs_per_step": pairs_all if share else pairs, "candidates_per_step": int(st.candidates),
+                       "tasks": tgt.ntasks(), "cells": ncells,
+                       "parallelism": (f"replicas round-robin over {world} GPUs ({len(systems)} on rank 0)"
+                                       if share else f"replicas x{world}"),
                        "step": "engine_step on the device: re-binning, sort, sweep, integration"
                                + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step",
                        "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
                                   "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
                                   "cuda_graph": True},
                        "l2": "256 MiB write before every timed step (outside the timed events)"},
-            "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+            "e2e": {"value": pairs_all / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
                     "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "host_ms": {k: round(v, 4) for k, v in host.items()},
                     "what": "engine_step (engine_batch_step for the replicas) with the host cells as input "
@@ -572,15 +593,15 @@ def ours(args, rank, world, local_rank):
                          "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": ms_sweep,
                          "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
                                         "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain": {"value": world * (plain_pairs / args.steps) / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+            "plain": {"value": plain_all / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                       "sweep_ms": plain_sweep,
                       "what": "the same resident steps with the plain sweep: one block per task, IEEE sqrt/div, "
                               "per-step warp reductions, no graph"},
-            "step_host": {"value": world * pairs / (host_ms * 1e-3), "ms_per_step": host_ms,
+            "step_host": {"value": pairs_all / (host_ms * 1e-3), "ms_per_step": host_ms,
                           "what": "engine_step_host: re-binning and integration on the host threads, forces "
                                   "and constraints through host buffers"},
-            "force_eval": {"value": world * fe_pairs / (fe_ms * 1e-3), "ms_per_step": fe_ms, "sweep_ms": fe_sweep,
-                           "e2e": {"value": world * fe_pairs / (fe_e2e * 1e-3), "ms_per_step": fe_e2e},
+            "force_eval": {"value": fe_all / (fe_ms * 1e-3), "ms_per_step": fe_ms, "sweep_ms": fe_sweep,
+                           "e2e": {"value": fe_all / (fe_e2e * 1e-3), "ms_per_step": fe_e2e},
                            "what": "sort + sweep alone at the initial positions (engine_nonbond_cuda_resident; "
                                    "e2e: engine_nonbond_cuda with host buffers)"},
             "gpu_launches": per_step * args.steps,

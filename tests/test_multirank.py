@@ -1,5 +1,6 @@
 """The multi-GPU paths of bench.py on the CPU, with two gloo ranks: the max-over-ranks timing
-rule, and a torchrun launch of the reference arm in which rank 0 alone runs and prints."""
+rule, the sum of the ranks' pair counts when the replica ensemble is dealt round-robin, and
+a torchrun launch of the reference arm in which rank 0 alone runs and prints."""
 import json
 import os
 import socket
@@ -25,7 +26,8 @@ def _rank(rank, port, out):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=2,
                             timeout=datetime.timedelta(seconds=60))
     try:
-        out.put((rank, bench.reduce_max([rank + 1.0, 10.0 - rank, 0.5], dist, "cpu")))
+        out.put((rank, bench.reduce_max([rank + 1.0, 10.0 - rank, 0.5], dist, "cpu")
+                 + bench.reduce_sum([100.0 * (rank + 1), 7.0], dist, "cpu")))
     finally:
         dist.destroy_process_group()
 
@@ -41,13 +43,24 @@ def test_reduce_max_over_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert got[0] == got[1] == [2.0, 10.0, 0.5]
+    assert got[0] == got[1] == [2.0, 10.0, 0.5, 300.0, 14.0]
 
 
 def test_reduce_max_single_rank_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.reduce_max([1, 2.5], None, "cpu") == [1.0, 2.5]
+    assert bench.reduce_sum([1, 2.5], None, "cpu") == [1.0, 2.5]
+
+
+def test_round_robin_deals_every_replica_once():
+    """rank r of N takes replicas r, r + N, ...: every replica on exactly one rank."""
+    sys.path.insert(0, os.path.join(ROOT, "mdcore-history_b200"))
+    import workloads as W
+    ens = W.argon_replicas(nrep=10, seed=1)
+    for world in (1, 2, 3, 4):
+        dealt = [s.name for r in range(world) for s in ens[r::world]]
+        assert sorted(dealt) == sorted(s.name for s in ens) and len(set(dealt)) == len(ens)
 
 
 def test_reference_arm_under_torchrun_prints_one_line():
