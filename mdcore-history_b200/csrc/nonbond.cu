@@ -281,6 +281,34 @@ void evict_lines(const void* p, size_t bytes) {
 #endif
 }
 
+// Stores into the pinned upload buffers that bypass the CPU caches (non-temporal): the copy
+// engine then reads the lines from memory without snooping the host threads' caches, and no
+// eviction pass is needed.  fence_nt() orders a thread's streamed stores before the copy.
+inline void store_nt(float4* dst, float4 v) {
+#if defined(__x86_64__)
+    _mm_stream_ps(reinterpret_cast<float*>(dst), _mm_set_ps(v.w, v.z, v.y, v.x));
+#else
+    *dst = v;
+#endif
+}
+inline void store_nt(int* dst, int v) {
+#if defined(__x86_64__)
+    _mm_stream_si32(dst, v);
+#else
+    *dst = v;
+#endif
+}
+inline void store_nt(float* dst, float v) {
+    int bits;
+    std::memcpy(&bits, &v, sizeof(int));
+    store_nt(reinterpret_cast<int*>(dst), bits);
+}
+inline void fence_nt() {
+#if defined(__x86_64__)
+    _mm_sfence();
+#endif
+}
+
 double now_ms() {
     timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -393,17 +421,16 @@ void pack_range(NbState* st, int cb, int ce) {
             const int pad = (cl->count + 3) & ~3;
             for (int q = 0; q < cl->count; q++) {
                 const struct part* p = &cl->parts[q];
-                st->h_xq[slot + q] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
+                store_nt(st->h_xq + slot + q, make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type)));
             }
-            for (int q = cl->count; q < pad; q++) st->h_xq[slot + q] = make_float4(0.f, 0.f, 0.f, bits_as_float(0));
+            for (int q = cl->count; q < pad; q++)
+                store_nt(st->h_xq + slot + q, make_float4(0.f, 0.f, 0.f, bits_as_float(0)));
             if (st->need_pid) {          // ids are read by the sweep for exclusions and charges only
-                for (int q = 0; q < cl->count; q++) st->h_pid[slot + q] = id0 + cl->parts[q].id;
-                for (int q = cl->count; q < pad; q++) st->h_pid[slot + q] = 0;
+                for (int q = 0; q < cl->count; q++) store_nt(st->h_pid + slot + q, id0 + cl->parts[q].id);
+                for (int q = cl->count; q < pad; q++) store_nt(st->h_pid + slot + q, 0);
             }
         }
-        const size_t s0 = (size_t)cstart[cb + b], s1 = (size_t)cstart[cb + e];
-        evict_lines(st->h_xq + s0, sizeof(float4) * (s1 - s0));
-        if (st->need_pid) evict_lines(st->h_pid + s0, sizeof(int) * (s1 - s0));
+        fence_nt();
     });
 }
 
@@ -1646,18 +1673,14 @@ int res_upload(NbState* st) {
                 const struct part* p = &cl->parts[q];
                 const int gid = st->id_off[k] + p->id;
                 const size_t o = (size_t)off[c] + q;
-                hx[o] = make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type));
-                hv[o] = make_float4(p->v[0], p->v[1], p->v[2], 0.f);
-                st->h_uppid[o] = gid;
+                store_nt(hx + o, make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type)));
+                store_nt(hv + o, make_float4(p->v[0], p->v[1], p->v[2], 0.f));
+                store_nt(st->h_uppid + o, gid);
                 st->up_aux[o] = NbState::UpAux{p->q, p->vid, p->flags};
-                if (hq != nullptr) hq[o] = p->q;
+                if (hq != nullptr) store_nt(hq + o, p->q);
             }
         }
-        const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
-        evict_lines(hx + q0, sizeof(float4) * (q1 - q0));
-        evict_lines(hv + q0, sizeof(float4) * (q1 - q0));
-        evict_lines(st->h_uppid + q0, sizeof(int) * (q1 - q0));
-        if (hq != nullptr) evict_lines(hq + q0, sizeof(float) * (q1 - q0));
+        fence_nt();
     });
     const size_t q0 = (size_t)off[c0], q1 = (size_t)off[c1];
     if (q1 > q0) {
