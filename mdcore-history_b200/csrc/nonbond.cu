@@ -1667,6 +1667,10 @@ int res_upload(NbState* st) {
     HostPool::get().run(c1 - c0, cell_grain(st), [&](int, int rb, int re) {
         const int cb = c0 + rb, ce = c0 + re;
         for (int c = cb; c < ce; c++) {
+            // many small cells (each its own parts array): fetch the cell records and the
+            // particles a few cells ahead
+            if (c + 8 < ce) __builtin_prefetch(st->flat_cells[c + 8]);
+            if (c + 4 < ce) __builtin_prefetch(st->flat_cells[c + 4]->parts);
             const struct cell* cl = st->flat_cells[c];
             const size_t k = std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
             for (int q = 0; q < cl->count; q++) {
@@ -2024,6 +2028,8 @@ int res_download(NbState* st, unsigned long long* status) {
         HostPool::get().run(cend - c0, cell_grain(st), [&](int, int rb, int re) {
             const int cb = c0 + rb, ce = c0 + re;
             for (int c = cb; c < ce; c++) {
+                if (c + 8 < ce) __builtin_prefetch(st->flat_cells[c + 8], 1);
+                if (c + 4 < ce) __builtin_prefetch(st->flat_cells[c + 4]->parts, 1);
                 const size_t ke =
                     std::upper_bound(st->cell_off.begin(), st->cell_off.end(), c) - st->cell_off.begin() - 1;
                 const int lo = st->id_off[ke];
