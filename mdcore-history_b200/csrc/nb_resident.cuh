@@ -60,15 +60,24 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
     const size_t base = (size_t)c * RC.capc;
     const float4 h = RC.cell_h[c];
     int stays = 0, moves = 0;
+    // the next 32 particles are loaded while these are written (latency of one load, not of
+    // one per 32 particles)
+    float4 xn = make_float4(0.f, 0.f, 0.f, 0.f), vn = xn;
+    int idn = 0;
+    if (lane < n) {
+        xn = xq[base + lane];
+        vn = v[base + lane];
+        idn = pid[base + lane];
+    }
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool active = k < n;
-        float4 x = make_float4(0.f, 0.f, 0.f, 0.f), vv = x;
-        int id = 0;
-        if (active) {
-            x = xq[base + k];
-            vv = v[base + k];
-            id = pid[base + k];
+        const float4 x = xn, vv = vn;
+        const int id = idn;
+        if (k + 32 < n) {
+            xn = xq[base + k + 32];
+            vn = v[base + k + 32];
+            idn = pid[base + k + 32];
         }
         const int dx = (x.x >= h.x) - (x.x < 0.0f), dy = (x.y >= h.y) - (x.y < 0.0f), dz = (x.z >= h.z) - (x.z < 0.0f);
         const bool stay = active && dx == 0 && dy == 0 && dz == 0;
@@ -127,33 +136,46 @@ __global__ void __launch_bounds__(256) rebin_gather(ResidentCells RC, const Move
         my_src = RC.nbr[(size_t)c * 27 + (26 - lane)];
         my_nm = nmove[my_src];
     }
-    unsigned todo = __ballot_sync(FULL, my_nm > 0);
-    while (todo) {
-        const int d = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int src = __shfl_sync(FULL, my_src, d);
-        const int nm = __shfl_sync(FULL, my_nm, d);
-        for (int m0 = 0; m0 < nm; m0 += 32) {
-            const int m = m0 + lane;
-            Mover mv;
-            bool match = false;
-            if (m < nm) {
-                mv = movers[(size_t)src * RC.mcap + m];
-                match = __float_as_int(mv.v.w) == d;
-            }
-            const unsigned bmatch = __ballot_sync(FULL, match);
-            if (match) {
-                const int o = off + __popc(bmatch & ((1u << lane) - 1u));
-                if (o < RC.capc) {
-                    xq_out[base + o] = mv.x;
-                    v_out[base + o] = make_float4(mv.v.x, mv.v.y, mv.v.z, 0.f);
-                    pid_out[base + o] = mv.pid;
-                } else {
-                    over = true;
-                }
-            }
-            off += __popc(bmatch);
+    // The candidates of all those directions as one list, direction-major: lane d's movers
+    // occupy [pre_d, pre_d + nm_d).  Each pass loads 32 of them at once (one load latency
+    // for many directions instead of one per direction) and keeps those that moved by d.
+    int incl = my_nm;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int my_pre = incl - my_nm;
+    const int total = __shfl_sync(FULL, incl, 31);
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const int t = t0 + lane;
+        // the direction holding candidate t: the last lane whose list starts at or before t
+        int d = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int pre = __shfl_sync(FULL, my_pre, d + step);
+            if (pre <= t) d += step;
         }
+        const int src = __shfl_sync(FULL, my_src, d);
+        const int m = t - __shfl_sync(FULL, my_pre, d);
+        Mover mv;
+        bool match = false;
+        if (t < total) {
+            mv = movers[(size_t)src * RC.mcap + m];
+            match = __float_as_int(mv.v.w) == d;
+        }
+        const unsigned bmatch = __ballot_sync(FULL, match);
+        if (match) {
+            const int o = off + __popc(bmatch & ((1u << lane) - 1u));
+            if (o < RC.capc) {
+                xq_out[base + o] = mv.x;
+                v_out[base + o] = make_float4(mv.v.x, mv.v.y, mv.v.z, 0.f);
+                pid_out[base + o] = mv.pid;
+            } else {
+                over = true;
+            }
+        }
+        off += __popc(bmatch);
     }
     if (__any_sync(FULL, over) && lane == 0) atomicOr(status, (unsigned long long)kStatusResidentOverflow);
     const int n = min(off, RC.capc);
