@@ -43,7 +43,7 @@ constexpr int kSortWarps = 13;
 // shared memory holds the staged positions of the cell (scap float4) and then one such
 // area per warp.
 __host__ __device__ inline size_t sort_warp_bytes(int scap) {
-    return (size_t)scap * 4 + (size_t)scap * 2 + (size_t)3 * kSortBuckets * 4;
+    return (size_t)scap * 4 + (size_t)scap * 4 + (size_t)3 * kSortBuckets * 4;
 }
 __host__ __device__ inline size_t sort_stage_bytes(int scap) { return (size_t)scap * 16; }
 __host__ inline size_t sort_smem_bytes(int scap) { return sort_stage_bytes(scap) + kSortWarps * sort_warp_bytes(scap); }
@@ -119,8 +119,8 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
                                                 float dscale, float bias, int warp, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
     unsigned* skey = reinterpret_cast<unsigned*>(wp);
-    unsigned short* members = reinterpret_cast<unsigned short*>(wp + (size_t)scap * 4);
-    int* bcount = reinterpret_cast<int*>(wp + (size_t)scap * 6);
+    unsigned* members = reinterpret_cast<unsigned*>(wp + (size_t)scap * 4);    // keys, by bucket
+    int* bcount = reinterpret_cast<int*>(wp + (size_t)scap * 8);
     int* bstart = bcount + kSortBuckets;
     int* bfill = bstart + kSortBuckets;
     const int pad = (n + 3) & ~3;
@@ -162,8 +162,9 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
         }
         __syncwarp();
         for (int k = lane; k < n; k += 32) {
-            const int b = bucket_of(skey[k] & 0xffffu);
-            members[bstart[b] + atomicAdd(&bfill[b], 1)] = (unsigned short)k;
+            const unsigned key = skey[k];
+            const int b = bucket_of(key & 0xffffu);
+            members[bstart[b] + atomicAdd(&bfill[b], 1)] = key;
         }
         __syncwarp();
         unsigned* out = keys + 13 * (size_t)start + (size_t)sid * pad;
@@ -174,9 +175,9 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
             const int b0 = bstart[b], nb = bcount[b];
             int rank = b0;
             for (int m = 0; m < nb; ++m) {
-                const int o = members[b0 + m];
-                const unsigned od = skey[o] & 0xffffu;
-                rank += (od > md) | ((od == md) & (o < k));
+                const unsigned ok = members[b0 + m];
+                const unsigned od = ok & 0xffffu;
+                rank += (od > md) | ((od == md) & ((int)(ok >> 16) < k));
             }
             out[rank] = mine;
         }
