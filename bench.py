@@ -565,7 +565,11 @@ def ours(args, rank, world, local_rank):
                     traffic = int(ln.split()[1])
         # kernels of one resident step: re-binning (2), sort, queue compaction (3, systems
         # with empty cells), sweep, integration, constraints (rigid, one per engine)
-        per_step = 2 + 1 + 3 * int(compact) + 1 + 1 + int(rigid) * len(engines)
+        # (the update runs inside the constraint kernel when every particle of a single
+        # system is in a rigid group)
+        fused = (rigid and len(systems) == 1 and
+                 len(set(np.asarray(systems[0].rigid)[:, :2].astype(int).ravel().tolist())) == systems[0].n)
+        per_step = 2 + 1 + 3 * int(compact) + 1 + int(not fused) + int(rigid) * len(engines)
         line = {
             "metric": METRIC, "value": pairs_all / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

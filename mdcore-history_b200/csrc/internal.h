@@ -38,6 +38,15 @@ struct rigid_resident_view {
     void *xq, *v;           /* float4 device cells: position (w = type), velocity */
     int capc, cell0;        /* slots per cell, the engine's first global cell */
     const unsigned long long *abort;   /* nonzero: the step was aborted, launch nothing */
+    /* fuse != 0: every particle of the engine is in a rigid group, and the constraint
+     * kernel also runs the update (v += f dt/m, x += dt v) of each group's particles and
+     * counts the completed step (done += {1, *pairs}); else all of these are unused. */
+    int fuse;
+    const unsigned long long *force;   /* fixed-point forces by slot */
+    const double *imass;               /* 1/mass by type */
+    float dtf;                         /* the time step as the update uses it */
+    unsigned long long *status, *done;
+    const unsigned long long *pairs;
 };
 int rigid_eval_resident(struct engine *e, const struct rigid_resident_view *view, void *stream);
 /* Copies the iteration statistics of the last resident step to the host copy (wait = 0:

@@ -52,6 +52,16 @@ struct RigidArgs {
     int capc, cell0;            // slots per cell, this engine's first global cell
     int cd0, cd1, cd2;          // cell grid
     const unsigned long long* abort;   // resident: nonzero = the step was aborted
+    // Resident steps of an engine whose every particle is in a rigid group: the update of
+    // engine_advance (integrate_cells' arithmetic) runs here on each group's particles
+    // before the constraints, and no separate update kernel is launched.
+    int fuse;
+    const unsigned long long* force;   // fixed-point forces by slot (2^24 per kJ/mol/nm)
+    const double* imass;               // 1/mass by type
+    float dtf;                         // the time step as the update uses it
+    unsigned long long* status;        // the step's status word (non-finite result: bit 64)
+    unsigned long long* done;          // completed steps, their accepted pairs
+    const unsigned long long* pairs;   // this step's accepted pairs
 };
 
 // Cell grid coordinates of a resident slot.
@@ -85,6 +95,21 @@ __device__ __forceinline__ void load_group(const RigidArgs& A, int p0, int np, d
             const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
             x = A.rxq[slot];
             v = A.rv[slot];
+            if (A.fuse) {   // symplectic Euler, as integrate_cells: v += f w, x += dt v
+                const float w = (float)((double)A.dtf * A.imass[__float_as_int(x.w)]);
+                const float f0 = (float)((double)(long long)A.force[3 * (size_t)slot + 0] * (1.0 / 16777216.0));
+                const float f1 = (float)((double)(long long)A.force[3 * (size_t)slot + 1] * (1.0 / 16777216.0));
+                const float f2 = (float)((double)(long long)A.force[3 * (size_t)slot + 2] * (1.0 / 16777216.0));
+                v.x = __fadd_rn(v.x, __fmul_rn(f0, w));
+                v.y = __fadd_rn(v.y, __fmul_rn(f1, w));
+                v.z = __fadd_rn(v.z, __fmul_rn(f2, w));
+                x.x = __fadd_rn(x.x, __fmul_rn(A.dtf, v.x));
+                x.y = __fadd_rn(x.y, __fmul_rn(A.dtf, v.y));
+                x.z = __fadd_rn(x.z, __fmul_rn(A.dtf, v.z));
+                A.rxq[slot] = x;
+                A.rv[slot] = v;
+                if (!isfinite(x.x + x.y + x.z + v.x + v.y + v.z)) atomicOr(A.status, 64ull);
+            }
             int loc[3];
             slot_loc(A, slot, loc);
             for (int j = 0; j < 3; j++) sh[j] = shift_dim(loc[j], loc0[j]);
@@ -142,6 +167,10 @@ __global__ void __launch_bounds__(128) rigid_shake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    if (RES && A.fuse && r == 0) {     // completed steps, accepted pairs (integrate_cells' job)
+        A.done[0] += 1ull;
+        A.done[1] += *A.pairs;
+    }
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -191,6 +220,10 @@ __global__ void __launch_bounds__(128) rigid_pshake(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    if (RES && A.fuse && r == 0) {     // completed steps, accepted pairs (integrate_cells' job)
+        A.done[0] += 1ull;
+        A.done[1] += *A.pairs;
+    }
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -317,6 +350,21 @@ __device__ __forceinline__ void load_group_reg(const RigidArgs& A, int p0, int n
             const int slot = A.slot_of[A.id0 + A.rpid[p0 + k]];
             x = A.rxq[slot];
             v = A.rv[slot];
+            if (A.fuse) {   // symplectic Euler, as integrate_cells: v += f w, x += dt v
+                const float w = (float)((double)A.dtf * A.imass[__float_as_int(x.w)]);
+                const float f0 = (float)((double)(long long)A.force[3 * (size_t)slot + 0] * (1.0 / 16777216.0));
+                const float f1 = (float)((double)(long long)A.force[3 * (size_t)slot + 1] * (1.0 / 16777216.0));
+                const float f2 = (float)((double)(long long)A.force[3 * (size_t)slot + 2] * (1.0 / 16777216.0));
+                v.x = __fadd_rn(v.x, __fmul_rn(f0, w));
+                v.y = __fadd_rn(v.y, __fmul_rn(f1, w));
+                v.z = __fadd_rn(v.z, __fmul_rn(f2, w));
+                x.x = __fadd_rn(x.x, __fmul_rn(A.dtf, v.x));
+                x.y = __fadd_rn(x.y, __fmul_rn(A.dtf, v.y));
+                x.z = __fadd_rn(x.z, __fmul_rn(A.dtf, v.z));
+                A.rxq[slot] = x;
+                A.rv[slot] = v;
+                if (!isfinite(x.x + x.y + x.z + v.x + v.y + v.z)) atomicOr(A.status, 64ull);
+            }
             int loc[3];
             slot_loc(A, slot, loc);
 #pragma unroll
@@ -373,6 +421,10 @@ __global__ void __launch_bounds__(64) rigid_shake_reg(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    if (RES && A.fuse && r == 0) {     // completed steps, accepted pairs (integrate_cells' job)
+        A.done[0] += 1ull;
+        A.done[1] += *A.pairs;
+    }
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -441,6 +493,10 @@ __global__ void __launch_bounds__(64) rigid_pshake_reg(RigidArgs A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.nrig) return;
     if (RES && A.abort != nullptr && *(const volatile unsigned long long*)A.abort != 0) return;
+    if (RES && A.fuse && r == 0) {     // completed steps, accepted pairs (integrate_cells' job)
+        A.done[0] += 1ull;
+        A.done[1] += *A.pairs;
+    }
     const int p0 = A.roff[r], np = A.roff[r + 1] - p0;
     const int c0 = A.coff[r], nc = A.coff[r + 1] - c0;
     if (np > MP || nc > MC || (!RES && __float_as_int(A.x[p0].w) < 0)) return;
@@ -913,6 +969,13 @@ extern "C" int rigid_eval_resident(struct engine* e, const struct rigid_resident
     A.cd1 = s->cdim[1];
     A.cd2 = s->cdim[2];
     A.abort = view->abort;
+    A.fuse = view->fuse;
+    A.force = view->force;
+    A.imass = view->imass;
+    A.dtf = view->dtf;
+    A.status = view->status;
+    A.done = view->done;
+    A.pairs = view->pairs;
     CU(cudaMemsetAsync(rd->d_stat, 0, sizeof(int) * 2, stream));
     launch_sized<true>(rd, !(e->flags & engine_flag_shake), A, stream);
     CU(cudaGetLastError());
