@@ -459,16 +459,21 @@ int engine_cuda_fp32_peak(int device, float *tflops);
 /* Allocation-free force evaluation.  No counterpart in the reference.  For callers that
  * cannot allocate device memory when they need forces (a fixed, pre-reserved device
  * budget; code between set-up and a stream capture): sort + persistent sweep on
- * caller-provided device buffers, with the only scratch (sort keys, queue head) in a
- * static device array of at most 65,536 particle slots, shared by all calls; calls that
- * overlap on the GPU race on it.  The first call on a device looks up that array's
- * address and should come before any stream capture.  Inputs use the device layout of
- * engine_cuda_load_parts (cell-major slots, cell starts multiples of 4): xq = float4
- * {x, y, z cell-local, type bits}, pid, cstart[ncells+1], ccount[ncells]; maxcount = the
- * largest cell count.  Outputs (zeroed by the call): force[3*nslots] int64 fixed point
+ * caller-provided device buffers, with the only scratch (sort keys, queue head, a
+ * layout-error word) in a static device array of at most 65,536 particle slots, shared by
+ * all calls; calls that overlap on the GPU race on it.  The first call on a device looks
+ * up that array's address and should come before any stream capture.  Inputs use the
+ * device layout of engine_cuda_load_parts (cell-major slots, cell starts multiples of 4):
+ * xq = float4 {x, y, z cell-local, type bits} and pid, both 16-byte aligned;
+ * cstart[ncells], ccount[ncells]; maxcount = the largest cell count (a larger cell is
+ * skipped and reported as status bit 2).  A cell whose start is not a multiple of 4 or
+ * whose 4-rounded block leaves [0, nslots) makes the call do nothing but set status bit
+ * 128.  Outputs (zeroed by the call, 8-byte aligned): force[3*nslots] int64 fixed point
  * 2^24/(kJ/mol/nm), cell_epot[ncells] int64 2^32/(kJ/mol), acc[8] {unused, virial*2^32
  * (negated), pairs, excluded, candidates, status}.  stream may be NULL (engine stream).
- * Tables, tasks and exclusions come from engine_cuda_load. */
+ * Tables, tasks and exclusions come from engine_cuda_load.  The call leaves the launch
+ * state of the engine's own evaluations (grids, graphs) alone and restores the caller's
+ * current device. */
 int engine_nonbond_cuda_noalloc(struct engine *e, const void *xq, const int *pid, const int *cstart,
                                 const int *ccount, int nslots, int maxcount, unsigned long long *force,
                                 unsigned long long *cell_epot, unsigned long long *acc, void *stream);

@@ -31,6 +31,7 @@ enum : unsigned {
     kStatusTableIndex = 4u,
     kStatusForceOverflow = 8u,
     kStatusNonFinite = 64u,        // a particle's position or velocity stopped being finite
+    kStatusLayout = 128u,          // a caller-given cell start or count breaks the slot layout
 };
 
 // Accumulator slots (unsigned long long each).
@@ -79,6 +80,10 @@ struct Params {
     const float* qid;
     int ep_pot;
     int tab_global;
+    // Plain form only: when set, each task's partial forces are added to these floats with
+    // float atomics (FP32 accumulation, order-dependent, as the reference's GPU runner adds
+    // them) instead of to the fixed-point accumulators.
+    float* force32 = nullptr;
 };
 
 // A device-resident step that was aborted (see nb_resident.cuh) launches nothing more.

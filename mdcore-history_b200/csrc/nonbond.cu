@@ -2689,15 +2689,22 @@ extern "C" int engine_cuda_ntasks(struct engine* e) {
 // device or is forbidden (real-time loops, code running between the engine's set-up and a
 // stream capture), or a plugin that must not grow the process's footprint.  For them,
 // engine_nonbond_cuda_noalloc runs the same sort + persistent sweep on caller-provided
-// device buffers and keeps its only scratch -- the sort key lists and the task-queue head
-// -- in the file-scope array below, sized for at most kNoAllocMaxSlots particle slots.
-// Every GPU that loads this library holds the array until the process exits.
+// device buffers and keeps its only scratch -- the sort key lists, the task-queue head and
+// a layout-error word -- in the file-scope array below, sized for at most
+// kNoAllocMaxSlots particle slots.  Every GPU that loads this library holds the array
+// until the process exits.
 //
 // The array's name is a host-side stand-in, not a device address; the first call on each
 // device (with that device current) looks the address up with cudaGetSymbolAddress.  That
 // first call should therefore come before any stream capture.  All calls share the one
-// array and it keeps the last call's contents: the queue head is cleared on every call,
-// and calls that overlap on the GPU (other streams, other host threads) race on it.
+// array and it keeps the last call's contents: the queue head and the layout-error word
+// are cleared on every call, and calls that overlap on the GPU (other streams, other host
+// threads) race on it.
+//
+// The call touches none of the launch state the engine's own evaluations keep (the
+// persistent grid of the last direct launch, the captured graphs): it sizes its own grid
+// and only ever raises the sweep kernel's shared-memory limit, so evaluations through
+// engine_nonbond_cuda before and after it, with or without graphs, are unaffected.
 
 namespace {
 constexpr int kNoAllocMaxSlots = 65536;
@@ -2706,30 +2713,86 @@ static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocKeyBytes 
 
 constexpr int kMaxDevices = 64;
 unsigned char* noalloc_addr[kMaxDevices] = {nullptr};
-}  // namespace
 
-extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, const int* pid, const int* cstart,
-                                           const int* ccount, int nslots, int maxcount,
-                                           unsigned long long* force, unsigned long long* cell_epot,
-                                           unsigned long long* acc, void* stream) {
-    if (e == nullptr || e->cuda == nullptr || xq == nullptr || pid == nullptr || cstart == nullptr ||
-        ccount == nullptr || force == nullptr || cell_epot == nullptr || acc == nullptr) {
-        errs_register(engine_err_null, "engine_nonbond_cuda_noalloc: NULL argument.", __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_null;
+// Checks every cell against the layout the bulk copies rely on: a start that is a multiple
+// of 4 slots and a 4-rounded block inside [0, nslots).  A bad cell sets the status bit and
+// the abort word, and the sort and sweep that follow return without touching memory.
+__global__ void noalloc_check_cells(const int* __restrict__ cstart, const int* __restrict__ ccount, int ncells,
+                                    int nslots, unsigned long long* __restrict__ acc,
+                                    unsigned long long* __restrict__ abort) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const long long s = cstart[c], n = ccount[c];
+    if ((s & 3) != 0 || s < 0 || n < 0 || s + ((n + 3) & ~3LL) > nslots) {
+        atomicOr(&acc[kAccStatus], (unsigned long long)kStatusLayout);
+        atomicExch(abort, 1ull);
     }
+}
+
+template <int NW, bool EX, int TAB>
+int noalloc_sweep_nw(const NbState* st, const TunedParams& T, int cap, size_t smem, cudaStream_t s) {
+    auto kern = sweep_tuned<NW, EX, TAB, 4, 1, 640>;
+    cudaFuncAttributes fa;
+    CU(cudaFuncGetAttributes(&fa, kern));
+    if (fa.maxDynamicSharedSizeBytes < (int)smem)
+        CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem));
+    kern<<<st->sm_count * std::max(1, per_sm), NW * 32, smem, s>>>(T, cap);
+    CU(cudaGetLastError());
+    return 0;
+}
+
+template <int NW>
+int noalloc_sweep(const NbState* st, const TunedParams& T, int cap, size_t smem, cudaStream_t s) {
+    if (st->tab_global)
+        return st->has_excl ? noalloc_sweep_nw<NW, true, kTabGlobal>(st, T, cap, smem, s)
+                            : noalloc_sweep_nw<NW, false, kTabGlobal>(st, T, cap, smem, s);
+    if (st->has_excl)
+        return st->one_pot ? noalloc_sweep_nw<NW, true, kTabOne>(st, T, cap, smem, s)
+                           : noalloc_sweep_nw<NW, true, kTabShared>(st, T, cap, smem, s);
+    return st->one_pot ? noalloc_sweep_nw<NW, false, kTabOne>(st, T, cap, smem, s)
+                       : noalloc_sweep_nw<NW, false, kTabShared>(st, T, cap, smem, s);
+}
+
+int noalloc_fail(int code, const char* msg, int line) {
+    errs_register(code, msg, line, "engine_nonbond_cuda_noalloc", __FILE__);
+    return engine_err = code;
+}
+
+int nonbond_noalloc(struct engine* e, const void* xq, const int* pid, const int* cstart, const int* ccount,
+                    int nslots, int maxcount, unsigned long long* force, unsigned long long* cell_epot,
+                    unsigned long long* acc, void* stream) {
     NbState* st = state(e);
-    if (nslots < 0 || nslots > kNoAllocMaxSlots) {
-        errs_register(engine_err_range, "engine_nonbond_cuda_noalloc: more particle slots than its 65536-slot scratch.",
-                      __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_range;
+    if (nslots < 0 || nslots > kNoAllocMaxSlots)
+        return noalloc_fail(engine_err_range, "engine_nonbond_cuda_noalloc: more particle slots than its 65536-slot scratch.",
+                            __LINE__);
+    if (maxcount < 0 || maxcount > kMaxPartsPerCell)
+        return noalloc_fail(engine_err_maxparts, "engine_nonbond_cuda_noalloc: cell larger than 1024 particles.", __LINE__);
+    if ((((uintptr_t)xq | (uintptr_t)pid) & 15) != 0 || (((uintptr_t)force | (uintptr_t)cell_epot | (uintptr_t)acc) & 7) != 0 ||
+        (((uintptr_t)cstart | (uintptr_t)ccount) & 3) != 0)
+        return noalloc_fail(engine_err_range,
+                            "engine_nonbond_cuda_noalloc: xq and pid must be 16-byte aligned, force, cell_epot and acc 8-byte "
+                            "aligned, cstart and ccount 4-byte aligned.",
+                            __LINE__);
+    if (st->device < 0 || st->device >= kMaxDevices)
+        return noalloc_fail(engine_err_range, "engine_nonbond_cuda_noalloc: device index out of range.", __LINE__);
+
+    // Launch shape, decided before any work is queued: 4 worker warps, 2 when the warps'
+    // staging slices of the largest cell would not leave room for a second block.
+    const int cap4 = (maxcount + 3) & ~3;
+    const int cap = cap4 + 8;
+    const int tc = st->tab_global ? 0 : st->ncoef, tp = st->tab_global ? 0 : st->npots;
+    int nw = 4;
+    size_t smem = warps_smem_bytes(cap, nw, tc, tp, st->max_type, 1);
+    if (smem > 200 * 1024) {
+        nw = 2;
+        smem = warps_smem_bytes(cap, nw, tc, tp, st->max_type, 1);
     }
-    if (maxcount < 0 || maxcount > kMaxPartsPerCell) {
-        errs_register(engine_err_maxparts, "engine_nonbond_cuda_noalloc: cell larger than 1024 particles.",
-                      __LINE__, __func__, __FILE__);
-        return engine_err = engine_err_maxparts;
-    }
+    if (smem > 220 * 1024)
+        return noalloc_fail(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__);
+
     CU(cudaSetDevice(st->device));
-    if (st->device < 0 || st->device >= kMaxDevices) return engine_err_range;
     if (noalloc_addr[st->device] == nullptr) {
         void* p = nullptr;
         CU(cudaGetSymbolAddress(&p, noalloc_scratch));
@@ -2737,17 +2800,19 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     }
     unsigned* keys = reinterpret_cast<unsigned*>(noalloc_addr[st->device]);
     int* counter = reinterpret_cast<int*>(noalloc_addr[st->device] + kNoAllocKeyBytes);
+    unsigned long long* abort = reinterpret_cast<unsigned long long*>(noalloc_addr[st->device] + kNoAllocKeyBytes + 8);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : st->stream;
 
     CU(cudaMemsetAsync(force, 0, sizeof(unsigned long long) * 3 * (size_t)nslots, s));
     CU(cudaMemsetAsync(cell_epot, 0, sizeof(unsigned long long) * st->ncells, s));
     CU(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * kAccCount, s));
-    CU(cudaMemsetAsync(counter, 0, sizeof(int), s));
-    const int cap4 = (maxcount + 3) & ~3;
-    if (cap4 == 0) return 0;
+    CU(cudaMemsetAsync(counter, 0, 16, s));                  // queue head and abort word
+    if (cap4 == 0 || st->ncells == 0) return 0;
+    noalloc_check_cells<<<(st->ncells + 255) / 256, 256, 0, s>>>(cstart, ccount, st->ncells, nslots, acc, abort);
+    CU(cudaGetLastError());
     const int cpc = sort_cells_per_block(nslots, st->ncells);
     const int rcs = launch_sort(static_cast<const float4*>(xq), cstart, ccount, st->d_cmask, keys, st->d_cscale,
-                                st->ncells, cpc, cap4, acc, nullptr, false, s);
+                                st->ncells, cpc, cap4, acc, abort, false, s);
     if (rcs < 0) return rcs;
 
     TunedParams T;
@@ -2778,7 +2843,7 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     P.cutoff2 = cutf * cutf;
     P.cutoff2s = (float)e->s.cutoff2;
     P.unsorted = (e->flags & engine_flag_unsorted) ? 1 : 0;
-    P.abort = nullptr;
+    P.abort = abort;
     P.qid = st->d_qid;
     P.ep_pot = st->ep_pot;
     P.tab_global = st->tab_global;
@@ -2787,21 +2852,22 @@ extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, con
     T.counter = counter;
     T.task_clock = nullptr;
     T.task_sm = nullptr;
-    const int cap = cap4 + 8;
-    const size_t smem = warps_smem_bytes(cap, 4, st->tab_global ? 0 : st->ncoef, st->tab_global ? 0 : st->npots,
-                                         st->max_type, 1);
-    if (smem > 220 * 1024) {
-        errs_register(engine_err_maxparts, "Cell too large for the sweep kernel's shared memory.", __LINE__,
-                      __func__, __FILE__);
-        return engine_err = engine_err_maxparts;
-    }
-    cudaStream_t saved = st->stream;
-    const bool cap_saved = st->capturing;
-    st->stream = s;
-    st->capturing = false;
-    const int rc = launch_tuned_w<4, 4, 0, 1, 640>(st, T, cap, smem);
-    st->stream = saved;
-    st->capturing = cap_saved;
+    return nw == 2 ? noalloc_sweep<2>(st, T, cap, smem, s) : noalloc_sweep<4>(st, T, cap, smem, s);
+}
+}  // namespace
+
+extern "C" int engine_nonbond_cuda_noalloc(struct engine* e, const void* xq, const int* pid, const int* cstart,
+                                           const int* ccount, int nslots, int maxcount,
+                                           unsigned long long* force, unsigned long long* cell_epot,
+                                           unsigned long long* acc, void* stream) {
+    if (e == nullptr || e->cuda == nullptr || xq == nullptr || pid == nullptr || cstart == nullptr ||
+        ccount == nullptr || force == nullptr || cell_epot == nullptr || acc == nullptr)
+        return noalloc_fail(engine_err_null, "engine_nonbond_cuda_noalloc: NULL argument.", __LINE__);
+    // The caller's current device is restored on return.
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    const int rc = nonbond_noalloc(e, xq, pid, cstart, ccount, nslots, maxcount, force, cell_epot, acc, stream);
+    if (prev >= 0) cudaSetDevice(prev);
     return rc;
 }
 
