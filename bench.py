@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Benchmark of the nonbonded hot path inside the MD step: pair interactions per second and
-ns/day on rigid SPC/E water (98,304 atoms, 9^3 cells, cutoff 1.0 nm, 3 exclusions and 3
-constraints per molecule, 300 K, dt 2 fs) by default; also LJ argon (32,000 atoms, 100 K),
-the 1,048,576-atom LJ slab (90 K) and the 512-replica argon ensemble (80-140 K)
-(--workload argon|slab|replicas).
+ns/day.  The headline line is the largest single-GPU configuration, the 512-replica LJ argon
+ensemble (1,451,403 atoms, N log-uniform 500-8,000 per replica, 80-140 K, dt 5 fs, one
+batch); by default the same line carries the 1,048,576-atom LJ slab (90 K) and rigid SPC/E
+water (98,304 atoms, 300 K, dt 2 fs) as sub-objects under "configs" (--sub), each measured
+the same way.  --workload water|argon|slab|chains|replicas picks another headline.
 
 One step = one engine_step of the whole system (of every replica): re-binning, sort of
 every cell along the 13 pair directions, the cell-pair/self sweep with fixed-point force
@@ -25,6 +26,9 @@ autotuner.
   force_eval  the force evaluation alone (sort + sweep) on the same particles, resident
           and through engine_nonbond_cuda with host buffers.
   roofline    the sweep kernel inside the timed resident steps (its own CUDA events).
+  force_error after the timed steps, one more force evaluation with the timed launch shape,
+          checked against the FP64 oracle on the same particles (per-atom relative error
+          distribution, max |dF|/F_rms, energy, exact pair counts); rank 0, one GPU.
 
 Multi-GPU: a single system is not partitioned here ("replicas only"): each rank steps its
 own copy of the workload and value = ranks * pairs / max-over-ranks time (weak scaling).
@@ -33,6 +37,7 @@ The replica ensemble (--workload replicas) is dealt round-robin over the ranks i
 (strong scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
+                  [--sub slab,water]
 """
 import argparse
 import json
@@ -48,7 +53,8 @@ sys.path.insert(0, os.path.join(ROOT, "mdcore-history_b200"))
 
 METRIC = "pair interactions/s + ns/day, 1 B200: tuned vs plain at ≤1e-5 rel force err"
 UNIT = "pair interactions/s"
-FLOPS_PER_PAIR = 45          # per accepted pair, FMA = 2 (roofline)
+FLOPS_PER_PAIR = 45          # FP32 flops per accepted pair (FMA = 2): dx and r^2 8, r 1, interval
+                             # index 4, x 2, Horner value+derivative 18, f 2, forces 9, energy 1
 
 
 def ns_per_day(ms_per_step, dt_fs):
@@ -98,17 +104,47 @@ WORKLOADS = {
     "chains": ("solvated chains, 92,200 atoms: 220 chains of 100 beads (20 LJ types, Lorentz-Berthelot, "
                "charges N(0, 0.3) e neutralised per chain, 1-2 and 1-3 exclusions) and 23,400 3-site waters in "
                "a 10.8 x 10.8 x 7.8 nm box (9 x 9 x 6 cells), cutoff 1.2 nm, 253 type tables and explicit "
-               "electrostatics, seeded; force evaluation only (the chains' bonded terms are not built)",
+               "electrostatics, seeded; force evaluation only",
                _chains, "sweep_chains92k_traffic.txt"),
 }
-# workloads whose bench step is a force evaluation (no trajectory can be run)
+# workloads whose bench step is a force evaluation
 FORCE_ONLY = {"chains"}
-SELECTED = "water"
+DEFAULT_WORKLOAD = "replicas"
+DEFAULT_SUB = "slab,water"
+L2_RULE = "GPU arm: 256 MiB write before every timed step (outside the timed events)"
 
 
-def build_system():
+def build_system(workload):
     import workloads as W
-    return WORKLOADS[SELECTED][1](W)
+    return WORKLOADS[workload][1](W)
+
+
+def config_of(workload, systems, pairs):
+    """The workload's config object, identical in both arms: what it is, its atoms, and the
+    accepted pairs of its initial configuration (the device's count in this arm, the
+    oracle's in the reference arm; the two are equal by construction)."""
+    return {"workload": WORKLOADS[workload][0], "atoms": int(sum(s.n for s in systems)),
+            "pairs_per_step": int(pairs), "l2": L2_RULE}
+
+
+def host_cpu():
+    """lscpu model, sockets and physical cores of this host."""
+    info = {"model": None, "sockets": None, "physical_cores": None, "logical_cpus": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, check=True).stdout
+        kv = {}
+        for ln in out.splitlines():
+            if ":" in ln:
+                k, v = ln.split(":", 1)
+                kv[k.strip()] = v.strip()
+        info["model"] = kv.get("Model name")
+        sockets = int(kv.get("Socket(s)", "0") or 0)
+        cores = int(kv.get("Core(s) per socket", "0") or 0)
+        info["sockets"] = sockets or None
+        info["physical_cores"] = sockets * cores or None
+    except (OSError, subprocess.CalledProcessError, ValueError):
+        pass
+    return info
 
 
 class ClockSampler:
@@ -193,39 +229,41 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def cpu_sample(systems, threads, steps=5, every=16):
+def cpu_sample(systems, threads, steps=20, warmup=1, every=16):
     """The reference's engine_step with its pthreads runners on a bounded sample of the
-    workload (the whole system, or every `every`-th replica of an ensemble): pairs per
-    second over the sample, pairs of the initial configurations."""
+    workload (the whole system, or every `every`-th replica of an ensemble): `warmup`
+    untimed steps, then `steps` timed ones; pairs per second over the sample, pairs of the
+    initial configurations."""
     sample = systems if len(systems) == 1 else systems[::every]
     try:
         ms = pairs = 0.0
         for s in sample:
-            ms += run_reference_md(s, threads, 1, steps)
+            ms += run_reference_md(s, threads, warmup, steps)
             pairs += pair_count(s)
     except (FileNotFoundError, subprocess.CalledProcessError) as exc:
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
     what = ("the full system" if len(systems) == 1 else
             f"{len(sample)} of the {len(systems)} replicas (every {every}th, {int(sum(s.n for s in sample))} atoms)")
     return {"value": pairs / (ms * 1e-3), "unit": UNIT, "cores": threads, "kind": "reference",
-            "ms_per_step": ms, "sample": f"{steps} engine_step calls of {what} on {threads} pthreads runners "
-                                        f"(reference build in oracle/_ref, P-SHAKE where the system is rigid)"}
+            "ms_per_step": ms, "steps": steps, "warmup": warmup, "host": host_cpu(),
+            "sample": f"{steps} timed engine_step calls after {warmup} warm-up of {what} on {threads} pthreads "
+                      f"runners (reference build in oracle/_ref, P-SHAKE where the system is rigid)"}
 
 
 def reference_arm(args, rank):
     """The reference's own engine_step with its pthreads CPU runners (oracle/_ref, built from
-    the reference sources) on the same workload, all host threads."""
+    the reference sources) on the same workload, all host threads, args.warmup untimed and
+    args.steps timed steps of the sample."""
     if rank != 0:
         return
-    if SELECTED in FORCE_ONLY:
+    if args.workload in FORCE_ONLY:
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no per-particle charges "
                           "(engine_setexplepot is stored but never evaluated), so it cannot run this system"}))
         return
-    built = build_system()
+    built = build_system(args.workload)
     systems = built if isinstance(built, list) else [built]
     threads = host_threads()
-    steps = max(1, min(args.steps, 10 if len(systems) == 1 else 3))
-    cb = cpu_sample(systems, threads, steps=steps)
+    cb = cpu_sample(systems, threads, steps=args.steps, warmup=args.warmup)
     if cb["value"] is None:
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {cb['sample']}"}))
         return
@@ -235,14 +273,54 @@ def reference_arm(args, rank):
     ms = pairs / v * 1e3
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": ms,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "ns_per_day": ns_per_day(ms, systems[0].dt * 1e3),
-        "config": {"workload": WORKLOADS[SELECTED][0], "pairs_per_step": pairs, "parallelism": "pthreads runners",
-                   "sample_ms_per_step": sample_ms},
+        "config": config_of(args.workload, systems, pairs),
+        "parallelism": f"pthreads runners x{threads}", "sample_ms_per_step": sample_ms,
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def checker_force_error(systems, engines, stats):
+    """Checker (outside every timed region; rank 0, one GPU): the forces, energy and pair
+    count of the engines' last force evaluation against the FP64 oracle on the same
+    particles (cell-relative float positions and cells as the engines hold them)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mdcore_b200 as M
+    import oracle as O
+    fs, fo = [], []
+    epot = pairs = excluded = eabs = 0.0
+    t0 = time.time()
+    for s, e in zip(systems, engines):
+        x, _, _, c = e.parts()
+        cdim = np.floor(np.asarray(s.dim) / np.asarray(s.L)).astype(np.int32)
+        binned = dict(cdim=cdim, h=np.asarray(s.dim) / cdim, cell=c, xrel=x)
+        specs = list(s.pots) + ([s.ep] if getattr(s, "ep", None) is not None else [])
+        o = O.nonbond(s, [M.create_potential(p).contents.table() for p in specs], binned=binned)
+        fs.append(e.forces())
+        fo.append(o["f"])
+        epot += o["epot"]
+        eabs += o["epot_abs"]
+        pairs += o["pairs"]
+        excluded += o["excluded"]
+    f, f_ref = np.concatenate(fs), np.concatenate(fo)
+    d = np.linalg.norm(f - f_ref, axis=1)
+    fn = np.linalg.norm(f_ref, axis=1)
+    rel = d / np.maximum(fn, 1e-30)
+    frms = np.sqrt((f_ref ** 2).sum(1).mean())
+    return {"global_rel": float(np.linalg.norm(f - f_ref) / np.linalg.norm(f_ref)),
+            "max_over_frms": float(d.max() / frms), "rel_max": float(rel.max()),
+            "rel_p99": float(np.percentile(rel, 99)), "rel_median": float(np.median(rel)),
+            "frac_over_1e-5": float((rel > 1e-5).mean()),
+            "epot_rel": float(abs(stats.epot - epot) / max(abs(epot), 1e-30)),
+            "epot_err_over_sum_abs": float(abs(stats.epot - epot) / max(eabs, 1e-30)),
+            "pairs_exact": bool(int(stats.pairs) == int(pairs) and int(stats.excluded) == int(excluded)),
+            "atoms": int(len(f)), "oracle_s": round(time.time() - t0, 2),
+            "what": "after the timed steps: one force evaluation with the timed launch shape vs the FP64 "
+                    "oracle (the same float tables, double arithmetic) on the same particles"}
 
 
 # ---------------------------------------------------------------- this library on the GPU
@@ -331,90 +409,43 @@ def timed_resident_steps(tgt, stream, flush, steps, torch):
     return tot / steps, sweep / steps, info.pairs - p0
 
 
-def force_only_line(args, rank, world, local_rank, M, tgt, engines, systems, st, pairs, fe_ms, fe_sweep, fe_e2e,
-                    h2d, d2h, ncells, compact, warps, layout, stages, occupancy, tune_ms, clocks, stream, flush,
-                    barrier, torch, dist):
-    """The JSON line of a workload whose step is one force evaluation (sort + sweep): value
-    device-resident, e2e engine_nonbond_cuda with host buffers, plain the plain form."""
-    tgt.graph(False)
-    tgt.tune(0, plain=True)
-    tgt.load_parts()
-    tgt.resident()
-    barrier()
-    plain_ms, plain_sweep = timed_force_evals(tgt, stream, flush, args.steps, torch)
-    barrier()
-    clk = clocks.stop()
-    if tgt.stats().status != 0:
-        raise SystemExit("bench.py: device status after the plain evaluations")
-    fe_ms, fe_e2e, fe_sweep, plain_ms = reduce_max([fe_ms, fe_e2e, fe_sweep, plain_ms], dist, "cuda")
-    if rank == 0:
-        peak = M.fp32_peak_tflops(local_rank)
-        achieved = FLOPS_PER_PAIR * pairs / (fe_sweep * 1e-3) / 1e12
-        traffic = None
-        prof = os.path.join(ROOT, "profiles", WORKLOADS[SELECTED][2])
-        if os.path.exists(prof):
-            for ln in open(prof):
-                if ln.startswith("dram_bytes_per_launch"):
-                    traffic = int(ln.split()[1])
-        # engine_nonbond_cuda's copies: positions+types and ids per padded slot and the cell
-        # offsets/counts up; float forces per slot, cell energies/virials, counters down
-        slots = sum(int((((cell_counts(s, e) + 3) // 4) * 4).sum()) for s, e in zip(systems, engines))
-        fe_h2d, fe_d2h = 20 * slots + 4 * (2 * ncells + 1), 12 * slots + 16 * ncells + 64
-        line = {
-            "metric": METRIC, "value": world * pairs / (fe_ms * 1e-3), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": fe_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "ns_per_day": None,
-            "config": {"workload": WORKLOADS[SELECTED][0], "atoms": int(sum(s.n for s in systems)),
-                       "pairs_per_step": pairs, "candidates_per_step": int(st.candidates), "tasks": tgt.ntasks(),
-                       "cells": ncells, "parallelism": f"replicas x{world}",
-                       "step": "one force evaluation: sort + sweep (engine_nonbond_cuda_resident)",
-                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
-                                  "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
-                                  "cuda_graph": True},
-                       "l2": "256 MiB write before every timed step (outside the timed events)"},
-            "e2e": {"value": world * pairs / (fe_e2e * 1e-3), "unit": UNIT, "ms_per_step": fe_e2e,
-                    "h2d_bytes_per_step": fe_h2d, "d2h_bytes_per_step": fe_d2h,
-                    "what": "engine_nonbond_cuda with host buffers: positions and ids up, forces and energies down"},
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": fe_sweep,
-                         "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
-                                        "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms, "sweep_ms": plain_sweep,
-                      "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
-            "gpu_launches": (2 + 3 * int(compact)) * args.steps,
-            "clocks": clk,
-        }
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                                    "sample": "not run: the reference has no per-particle charges (engine_setexplepot "
-                                              "is stored but never evaluated), so it cannot run this system"}
-        print(json.dumps(line))
-    tgt.close()
-    for e in engines:
-        e.close()
-    if dist is not None:
-        dist.destroy_process_group()
+def read_traffic(workload):
+    """dram read + write bytes of one sweep launch, from the committed ncu summary."""
+    prof = os.path.join(ROOT, "profiles", WORKLOADS[workload][2])
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("dram_bytes_per_launch"):
+                return int(ln.split()[1])
+    return None
 
 
-def ours(args, rank, world, local_rank):
+def launch_obj(warps, layout, stages, occupancy, tune_ms):
+    return {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i", "staging_buffers": stages,
+            "threads_per_sm": occupancy, "autotune_ms": tune_ms, "cuda_graph": True}
+
+
+def roofline_obj(M, local_rank, pairs, sweep_ms, layout, workload):
+    peak = M.fp32_peak_tflops(local_rank)
+    achieved = FLOPS_PER_PAIR * pairs / (sweep_ms * 1e-3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": read_traffic(workload), "kernel": "sweep_tiled" if layout else "sweep_tuned",
+            "kernel_ms": sweep_ms, "flops_per_pair": FLOPS_PER_PAIR,
+            "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
+                           "MEASURED_PEAKS.json has no FP32 figure"}
+
+
+def measure(workload, args, rank, world, local_rank, dist, with_cpu):
+    """Everything measured for one workload on this rank; returns the JSON object on rank 0
+    (None elsewhere)."""
     import numpy as np
     import torch
     import mdcore_b200 as M
 
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py: no CUDA device")
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    built = build_system()
+    built = build_system(workload)
     replicas = isinstance(built, list)
     share = replicas and world > 1          # the ensemble dealt round-robin over the ranks
     systems = (built[rank::world] if share else built) if replicas else [built]
+    all_systems = built if replicas else [built]
     dt_fs = systems[0].dt * 1e3
     rigid = any(s.rigid is not None and len(s.rigid) for s in systems)
     if replicas:
@@ -440,7 +471,7 @@ def ours(args, rank, world, local_rank):
     st = tgt.stats()
     if st.status != 0:
         raise SystemExit(f"bench.py: device status {st.status}")
-    fe_pairs = int(st.pairs)
+    fe_pairs = int(st.pairs)               # accepted pairs of the initial configuration
 
     # ---- launch shape by the autotuner (or --launch), CUDA-graph replay from here on
     tgt.load_parts()
@@ -457,7 +488,6 @@ def ours(args, rank, world, local_rank):
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-
     # ---- force evaluation alone (sort + sweep), resident and with host buffers
     barrier()
     fe_ms, fe_sweep = timed_force_evals(tgt, stream, flush, args.steps, torch)
@@ -476,153 +506,221 @@ def ours(args, rank, world, local_rank):
         fe_e2e += ev0.elapsed_time(ev1) / args.steps
     barrier()
 
-    if SELECTED in FORCE_ONLY:
-        force_only_line(args, rank, world, local_rank, M, tgt, engines, systems, st, fe_pairs, fe_ms, fe_sweep,
-                        fe_e2e, h2d, d2h, ncells, compact, warps, layout, stages, occupancy, tune_ms, clocks, stream,
-                        flush, barrier, torch, dist)
-        return
-
-    # ---- MD steps resident in HBM: the headline value
-    tgt.resident_begin()
-    tgt.resident_steps(max(args.warmup, 25 if rigid else 3))     # past the P-SHAKE refinement steps
-    barrier()
-    ms, ms_sweep, pairs_timed = timed_resident_steps(tgt, stream, flush, args.steps, torch)
-    barrier()
-    pairs = pairs_timed / args.steps
-    tgt.resident_sync()
-    if tgt.stats().status != 0:
-        raise SystemExit("bench.py: device status after the resident steps")
+    force_only = workload in FORCE_ONLY
+    pairs_all_init = reduce_sum([fe_pairs], dist, "cuda")[0] if share else fe_pairs
     shake = None
-    if rigid:
-        itmax, bad = engines[0].rigid_stats()
-        if bad:
-            raise SystemExit("bench.py: rigid groups did not converge")
-        shake = itmax
-
-    # ---- the plain sweep in the same resident steps ("tuned vs plain")
-    tgt.graph(False)
-    tgt.tune(0, plain=True)
-    tgt.resident_steps(2)
-    barrier()
-    plain_ms, plain_sweep, plain_pairs = timed_resident_steps(tgt, stream, flush, args.steps, torch)
-    barrier()
-    tgt.tune(warps, plain=False)
-    tgt.set_layout(layout, stages, occupancy)
-    tgt.graph(True)
-    tgt.resident_end()
-
-    # ---- engine_step with host buffers through the C ABI (e2e)
-    for _ in range(2):
-        tgt.step()
-    barrier()
-    e2e_ms = 0.0
-    host = {"pack": 0.0, "device_and_copies": 0.0, "unpack": 0.0}
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        tgt.step()
-        ev1.record(stream)
-        ev1.synchronize()
-        e2e_ms += ev0.elapsed_time(ev1) / args.steps
-        hs = tgt.stats()
-        host["pack"] += hs.ms_pack / args.steps
-        host["device_and_copies"] += hs.ms_device / args.steps
-        host["unpack"] += hs.ms_unpack / args.steps
-    barrier()
-    host_ms = 0.0                       # the host-threaded step, for comparison
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        tgt.step_host()
-        ev1.record(stream)
-        ev1.synchronize()
-        host_ms += ev0.elapsed_time(ev1) / args.steps
-    barrier()
-    clk = clocks.stop()
-    if tgt.stats().status != 0:
-        raise SystemExit("bench.py: device status after the host-buffer steps")
-
-    ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e = reduce_max([ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e],
-                                                              dist, "cuda")
-    if share:
-        pairs_all, plain_all, fe_all = reduce_sum([pairs, plain_pairs / args.steps, fe_pairs], dist, "cuda")
+    if force_only:
+        # the plain form of the same force evaluation
+        tgt.graph(False)
+        tgt.tune(0, plain=True)
+        tgt.load_parts()
+        tgt.resident()
+        barrier()
+        plain_ms, plain_sweep = timed_force_evals(tgt, stream, flush, args.steps, torch)
+        barrier()
+        tgt.tune(warps, plain=False)
+        tgt.set_layout(layout, stages, occupancy)
+        tgt.graph(True)
+        clk = clocks.stop()
+        if tgt.stats().status != 0:
+            raise SystemExit("bench.py: device status after the plain evaluations")
+        fe_ms, fe_e2e, fe_sweep, plain_ms = reduce_max([fe_ms, fe_e2e, fe_sweep, plain_ms], dist, "cuda")
+        ms, ms_sweep, pairs = fe_ms, fe_sweep, fe_pairs
+        pairs_all = world * pairs
+        plain_all = pairs_all
     else:
-        pairs_all, plain_all, fe_all = world * pairs, world * (plain_pairs / args.steps), world * fe_pairs
+        # ---- MD steps resident in HBM: the headline value
+        tgt.resident_begin()
+        tgt.resident_steps(max(args.warmup, 25 if rigid else 3))     # past the P-SHAKE refinement steps
+        barrier()
+        ms, ms_sweep, pairs_timed = timed_resident_steps(tgt, stream, flush, args.steps, torch)
+        barrier()
+        pairs = pairs_timed / args.steps
+        tgt.resident_sync()
+        if tgt.stats().status != 0:
+            raise SystemExit("bench.py: device status after the resident steps")
+        if rigid:
+            itmax, bad = engines[0].rigid_stats()
+            if bad:
+                raise SystemExit("bench.py: rigid groups did not converge")
+            shake = itmax
+
+        # ---- the plain sweep in the same resident steps ("tuned vs plain")
+        tgt.graph(False)
+        tgt.tune(0, plain=True)
+        tgt.resident_steps(2)
+        barrier()
+        plain_ms, plain_sweep, plain_pairs = timed_resident_steps(tgt, stream, flush, args.steps, torch)
+        barrier()
+        tgt.tune(warps, plain=False)
+        tgt.set_layout(layout, stages, occupancy)
+        tgt.graph(True)
+        tgt.resident_end()
+
+        # ---- engine_step with host buffers through the C ABI (e2e)
+        for _ in range(2):
+            tgt.step()
+        barrier()
+        e2e_ms = 0.0
+        host = {"pack": 0.0, "device_and_copies": 0.0, "unpack": 0.0}
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            tgt.step()
+            ev1.record(stream)
+            ev1.synchronize()
+            e2e_ms += ev0.elapsed_time(ev1) / args.steps
+            hs = tgt.stats()
+            host["pack"] += hs.ms_pack / args.steps
+            host["device_and_copies"] += hs.ms_device / args.steps
+            host["unpack"] += hs.ms_unpack / args.steps
+        barrier()
+        host_ms = 0.0                       # the host-threaded step, for comparison
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            tgt.step_host()
+            ev1.record(stream)
+            ev1.synchronize()
+            host_ms += ev0.elapsed_time(ev1) / args.steps
+        barrier()
+        clk = clocks.stop()
+        if tgt.stats().status != 0:
+            raise SystemExit("bench.py: device status after the host-buffer steps")
+        ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e, host_ms = reduce_max(
+            [ms, e2e_ms, ms_sweep, plain_ms, fe_ms, fe_e2e, host_ms], dist, "cuda")
+        if share:
+            pairs_all, plain_all = reduce_sum([pairs, plain_pairs / args.steps], dist, "cuda")
+        else:
+            pairs_all, plain_all = world * pairs, world * (plain_pairs / args.steps)
+    fe_all = pairs_all_init if share else world * fe_pairs
+
+    line = None
     if rank == 0:
-        peak = M.fp32_peak_tflops(local_rank)
-        achieved = FLOPS_PER_PAIR * pairs / (ms_sweep * 1e-3) / 1e12
-        traffic = None
-        prof = os.path.join(ROOT, "profiles", WORKLOADS[SELECTED][2])
-        if os.path.exists(prof):       # dram read + write bytes of one sweep launch, from ncu
-            for ln in open(prof):
-                if ln.startswith("dram_bytes_per_launch"):
-                    traffic = int(ln.split()[1])
-        # kernels of one resident step: re-binning (2), sort, queue compaction (3, systems
-        # with empty cells), sweep, integration, constraints (rigid, one per engine)
-        # (the update runs inside the constraint kernel when every particle of a single
-        # system is in a rigid group)
-        fused = (rigid and len(systems) == 1 and
-                 len(set(np.asarray(systems[0].rigid)[:, :2].astype(int).ravel().tolist())) == systems[0].n)
-        per_step = 2 + 1 + 3 * int(compact) + 1 + int(not fused) + int(rigid) * len(engines)
-        line = {
-            "metric": METRIC, "value": pairs_all / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong" if share else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "ns_per_day": ns_per_day(ms, dt_fs),
-            "config": {"workload": WORKLOADS[SELECTED][0],
-                       "atoms": int(sum(s.n for s in (built if replicas else systems))),
-                       "pairs_per_step": pairs_all if share else pairs, "candidates_per_step": int(st.candidates),
-                       "tasks": tgt.ntasks(), "cells": ncells,
-                       "parallelism": (f"replicas round-robin over {world} GPUs ({len(systems)} on rank 0)"
-                                       if share else f"replicas x{world}"),
-                       "step": "engine_step on the device: re-binning, sort, sweep, integration"
-                               + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step",
-                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
-                                  "staging_buffers": stages, "threads_per_sm": occupancy, "autotune_ms": tune_ms,
-                                  "cuda_graph": True},
-                       "l2": "256 MiB write before every timed step (outside the timed events)"},
-            "e2e": {"value": pairs_all / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
-                    "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "host_ms": {k: round(v, 4) for k, v in host.items()},
-                    "what": "engine_step (engine_batch_step for the replicas) with the host cells as input "
-                            "and output every step"},
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "sweep_tiled" if layout else "sweep_tuned", "kernel_ms": ms_sweep,
-                         "peak_source": "measured FP32 FMA loop on this GPU (engine_cuda_fp32_peak); "
-                                        "MEASURED_PEAKS.json has no FP32 figure"},
-            "plain": {"value": plain_all / (plain_ms * 1e-3), "ms_per_step": plain_ms,
-                      "sweep_ms": plain_sweep,
-                      "what": "the same resident steps with the plain sweep: one block per task, IEEE sqrt/div, "
-                              "per-step warp reductions, no graph"},
-            "step_host": {"value": pairs_all / (host_ms * 1e-3), "ms_per_step": host_ms,
-                          "what": "engine_step_host: re-binning and integration on the host threads, forces "
-                                  "and constraints through host buffers"},
-            "force_eval": {"value": fe_all / (fe_ms * 1e-3), "ms_per_step": fe_ms, "sweep_ms": fe_sweep,
-                           "e2e": {"value": fe_all / (fe_e2e * 1e-3), "ms_per_step": fe_e2e},
-                           "what": "sort + sweep alone at the initial positions (engine_nonbond_cuda_resident; "
-                                   "e2e: engine_nonbond_cuda with host buffers)"},
-            "gpu_launches": per_step * args.steps,
-            "clocks": clk,
-        }
-        if shake is not None:
-            line["shake_max_iterations"] = shake
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_sample(systems, host_threads())
-            if line["cpu_baseline"]["value"] is not None:     # the same sample on one runner
-                one = cpu_sample(systems, 1, steps=2)
-                line["cpu_baseline"]["one_core"] = {"value": one["value"], "ms_per_step": one.get("ms_per_step"),
-                                                    "sample": one["sample"]}
-        print(json.dumps(line))
+        config = config_of(workload, all_systems, pairs_all_init if share else fe_pairs)
+        parallelism = (f"replicas round-robin over {world} GPUs ({len(systems)} on rank 0)" if share
+                       else f"replicas x{world}")
+        setup = {"tasks": tgt.ntasks(), "cells": ncells, "candidates_per_step": int(st.candidates),
+                 "launch": launch_obj(warps, layout, stages, occupancy, tune_ms)}
+        if force_only:
+            slots = sum(int((((cell_counts(s, e) + 3) // 4) * 4).sum()) for s, e in zip(systems, engines))
+            fe_h2d, fe_d2h = 20 * slots + 4 * (2 * ncells + 1), 12 * slots + 16 * ncells + 64
+            line = {
+                "metric": METRIC, "value": world * pairs / (fe_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": fe_ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "ns_per_day": None,
+                "config": config, "parallelism": parallelism,
+                "step": "one force evaluation: sort + sweep (engine_nonbond_cuda_resident)", "setup": setup,
+                "e2e": {"value": world * pairs / (fe_e2e * 1e-3), "unit": UNIT, "ms_per_step": fe_e2e,
+                        "h2d_bytes_per_step": fe_h2d, "d2h_bytes_per_step": fe_d2h,
+                        "what": "engine_nonbond_cuda with host buffers: positions and ids up, forces and "
+                                "energies down"},
+                "roofline": roofline_obj(M, local_rank, pairs, fe_sweep, layout, workload),
+                "plain": {"value": world * pairs / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                          "sweep_ms": plain_sweep,
+                          "what": "plain form: one block per task, IEEE sqrt/div, per-step warp reductions"},
+                "gpu_launches": (2 + 3 * int(compact)) * args.steps,
+                "clocks": clk,
+            }
+        else:
+            # kernels of one resident step: re-binning (2), sort, queue compaction (3, systems
+            # with empty cells), sweep, integration, constraints (rigid, one per engine)
+            # (the update runs inside the constraint kernel when every particle of a single
+            # system is in a rigid group)
+            fused = (rigid and len(systems) == 1 and
+                     len(set(np.asarray(systems[0].rigid)[:, :2].astype(int).ravel().tolist())) == systems[0].n)
+            per_step = 2 + 1 + 3 * int(compact) + 1 + int(not fused) + int(rigid) * len(engines)
+            line = {
+                "metric": METRIC, "value": pairs_all / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "strong" if share else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "ns_per_day": ns_per_day(ms, dt_fs),
+                "config": config, "parallelism": parallelism,
+                "pairs_per_step_timed": pairs_all,
+                "step": "engine_step on the device: re-binning, sort, sweep, integration"
+                        + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step",
+                "setup": setup,
+                "e2e": {"value": pairs_all / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                        "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "host_ms": {k: round(v, 4) for k, v in host.items()},
+                        "what": "engine_step (engine_batch_step for the replicas) with the host cells as input "
+                                "and output every step"},
+                "roofline": roofline_obj(M, local_rank, pairs, ms_sweep, layout, workload),
+                "plain": {"value": plain_all / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                          "sweep_ms": plain_sweep,
+                          "what": "the same resident steps with the plain sweep: one block per task, IEEE "
+                                  "sqrt/div, per-step warp reductions, no graph"},
+                "step_host": {"value": pairs_all / (host_ms * 1e-3), "ms_per_step": host_ms,
+                              "what": "engine_step_host: re-binning and integration on the host threads, forces "
+                                      "and constraints through host buffers"},
+                "force_eval": {"value": fe_all / (fe_ms * 1e-3), "ms_per_step": fe_ms, "sweep_ms": fe_sweep,
+                               "e2e": {"value": fe_all / (fe_e2e * 1e-3), "ms_per_step": fe_e2e},
+                               "what": "sort + sweep alone at the initial positions (engine_nonbond_cuda_resident; "
+                                       "e2e: engine_nonbond_cuda with host buffers)"},
+                "gpu_launches": per_step * args.steps,
+                "clocks": clk,
+            }
+            if shake is not None:
+                line["shake_max_iterations"] = shake
+        if with_cpu:
+            # checker and CPU baseline, outside every timed region
+            tgt.nonbond()
+            line["force_error"] = checker_force_error(systems, engines, tgt.stats())
+            if force_only:
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                        "host": host_cpu(),
+                                        "sample": "not run: the reference has no per-particle charges "
+                                                  "(engine_setexplepot is stored but never evaluated), so it "
+                                                  "cannot run this system"}
+            else:
+                line["cpu_baseline"] = cpu_sample(systems, host_threads())
+                if line["cpu_baseline"]["value"] is not None:     # the same sample on one runner
+                    big = sum(s.n for s in systems) > 500_000
+                    one = cpu_sample(systems, 1, steps=1 if big else 2, warmup=0 if big else 1)
+                    line["cpu_baseline"]["one_core"] = {"value": one["value"], "ms_per_step": one.get("ms_per_step"),
+                                                        "sample": one["sample"]}
     tgt.close()
     for e in engines:
         e.close()
+    del flush
+    torch.cuda.empty_cache()
+    return line
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    with_cpu = world == 1 and not args.no_cpu_baseline
+    line = measure(args.workload, args, rank, world, local_rank, dist, with_cpu)
+    # the other large configurations as sub-objects of the same line (one GPU only)
+    subs = [w for w in args.sub.split(",") if w and w != args.workload] if world == 1 else []
+    if subs:
+        configs = {}
+        for w in subs:
+            sub = measure(w, args, rank, world, local_rank, dist, with_cpu)
+            if sub is not None:
+                for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "vs_baseline",
+                          "data", "dtype"):
+                    sub.pop(k, None)
+                configs[w] = sub
+        if line is not None:
+            line["configs"] = configs
+    if line is not None:
+        print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
 
@@ -635,7 +733,7 @@ def sched_ab(args, local_rank):
     import torch
     import mdcore_b200 as M
     torch.cuda.set_device(local_rank)
-    sysm = build_system()
+    sysm = build_system(args.workload)
     if isinstance(sysm, list):
         raise SystemExit("bench.py: --sched-ab takes a single system (water, argon or slab)")
     e = M.Engine.from_system(sysm, device=local_rank)
@@ -677,7 +775,7 @@ def sched_ab(args, local_rank):
     e.tune(0, plain=True)
     res["plain_form"] = timed("plain")
     nz = y > 0
-    print(json.dumps({"sched_ab": WORKLOADS[SELECTED][0], "sweep_ms_median": res, "tasks": e.ntasks(),
+    print(json.dumps({"sched_ab": WORKLOADS[args.workload][0], "sweep_ms_median": res, "tasks": e.ntasks(),
                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
                                  "staging_buffers": stages, "threads_per_sm": occupancy},
                       "record_steps": args.record, "epochs": args.epochs, "train_s": round(train_s, 3),
@@ -692,8 +790,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
-    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS),
-                    help="water (default: the headline configuration), argon, slab or replicas")
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS),
+                    help="headline workload: replicas (default, the largest single-GPU configuration), slab, "
+                         "water, argon or chains")
+    ap.add_argument("--sub", default=None,
+                    help="comma-separated workloads measured as sub-objects of the same line (one GPU only); "
+                         f"default {DEFAULT_SUB} with the default workload, none otherwise")
     ap.add_argument("--launch", default="",
                     help="fixed persistent launch shape warps,layout,stages[,threads per SM] (e.g. 4,1,1,640) "
                          "instead of the autotuner")
@@ -702,8 +804,8 @@ def main():
     ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")
     ap.add_argument("--epochs", type=int, default=150, help="--sched-ab: training epochs")
     args = ap.parse_args()
-    global SELECTED
-    SELECTED = args.workload
+    if args.sub is None:
+        args.sub = DEFAULT_SUB if args.workload == DEFAULT_WORKLOAD else ""
     if args.sched_ab:
         sched_ab(args, int(os.environ.get("LOCAL_RANK", 0)))
         return
