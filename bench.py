@@ -40,6 +40,7 @@ The replica ensemble (--workload replicas) is dealt round-robin over the ranks i
                   [--sub slab,water]
 """
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -725,6 +726,125 @@ def ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def drift(args, local_rank):
+    """The solvated-chain system over args.drift_steps MD steps (dt 2 fs, NVE) from a state
+    relaxed on the device (steepest descent, then Maxwell-Boltzmann velocities at 300 K):
+    the plain FP32 arm (the plain form, forces accumulated with float atomics) and the
+    fixed-point arm (the persistent sweep, 64-bit fixed-point accumulation), from the same
+    state; per-atom force errors of each against the FP64 oracle at steps 0, 1,000 and the
+    last, and the drift of the total energy."""
+    import numpy as np
+    import torch
+    import workloads as W
+    import mdcore_b200 as M
+    torch.cuda.set_device(local_rank)
+    sysm = build_system(args.workload)
+    if isinstance(sysm, list):
+        raise SystemExit("bench.py: --drift takes a single system")
+    dt_ps = sysm.dt
+    # ---- relaxation on the device: steepest descent (rigid water held by the constraints)
+    t0 = time.time()
+    e = M.Engine.from_system(sysm, device=local_rank)
+    e.graph(True)
+    e.energy_log(args.min_steps + 8)
+    e.resident_begin()
+    phases = [(args.min_steps // 4, 2e-6, 0.003), (args.min_steps - args.min_steps // 4, 1e-6, 0.001)]
+    for nst, gamma, dmax in phases:
+        e.minimize(gamma, dmax)
+        e.resident_steps(nst)
+    lg = e.energy_log_read(args.min_steps + 8)
+    u_start, u_relaxed = float(lg[0, 1]), float(lg[-1, 1])
+    e.minimize(0.0)
+    e.resident_end()
+    x, _, pid, _ = e.unload()
+    xr = np.zeros_like(x)
+    xr[pid] = x
+    e.close()
+    relaxed = dataclasses.replace(sysm, x=W.wrap_positions(xr, np.asarray(sysm.dim)))
+    relaxed.v = W.maxwell_velocities(relaxed, 300.0, seed=11)
+    relax_s = time.time() - t0
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    specs = list(sysm.pots) + ([sysm.ep] if getattr(sysm, "ep", None) is not None else [])
+    tables = [M.create_potential(p).contents.table() for p in specs]
+    cdim = np.floor(np.asarray(sysm.dim) / np.asarray(sysm.L)).astype(np.int32)
+
+    def errors(eng):
+        xrel, _, _, c = eng.parts()
+        o = O.nonbond(relaxed, tables, binned=dict(cdim=cdim, h=np.asarray(sysm.dim) / cdim, cell=c, xrel=xrel))
+        f, fo = eng.forces(), o["f"]
+        d = np.linalg.norm(f - fo, axis=1)
+        rel = d / np.maximum(np.linalg.norm(fo, axis=1), 1e-30)
+        frms = np.sqrt((fo ** 2).sum(1).mean())
+        st = eng.stats()
+        return {"global_rel": float(np.linalg.norm(f - fo) / np.linalg.norm(fo)),
+                "max_over_frms": float(d.max() / frms), "rel_max": float(rel.max()),
+                "rel_p99": float(np.percentile(rel, 99)), "rel_median": float(np.median(rel)),
+                "frac_over_1e-5": float((rel > 1e-5).mean()),
+                "epot_rel": float(abs(st.epot - o["epot"]) / abs(o["epot"])),
+                "pairs_exact": bool(int(st.pairs) == o["pairs"] and int(st.excluded) == o["excluded"])}
+
+    checkpoints = sorted({0, min(1000, args.drift_steps), args.drift_steps})
+    arms = {}
+    nat = relaxed.n
+    ndof = 3 * nat - (len(relaxed.rigid) if relaxed.rigid is not None else 0) - 3
+    for arm in ("fp32", "fixed"):
+        eng = M.Engine.from_system(relaxed, device=local_rank)
+        if arm == "fp32":
+            eng.tune(0, plain=True)
+            eng.set_accum(True)
+        eng.graph(True)
+        cap = max(args.drift_steps, 2) + 8
+        eng.energy_log(cap)
+        logs, errs, done = [], {}, 0
+        t_steps = 0.0
+        for cp in checkpoints:
+            if cp > done:
+                eng.resident_begin()
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                ev0.record()
+                eng.resident_steps(cp - done)
+                ev1.record()
+                ev1.synchronize()
+                t_steps += ev0.elapsed_time(ev1)
+                lg = eng.energy_log_read(cap)
+                if len(lg) != cp - done:
+                    raise SystemExit(f"bench.py: energy log holds {len(lg)} records, expected {cp - done}")
+                lg[:, 0] += done
+                logs.append(lg)
+                eng.resident_end()
+                done = cp
+            eng.nonbond()                      # forces at the positions of step `cp`
+            errs[str(cp)] = errors(eng)
+        log = np.concatenate(logs)
+        E, t_ns, slope = M.leapfrog_energy(log, dt_ps)
+        K = log[:, 2]
+        arms[arm] = {
+            "force_error": errs,
+            "energy": {"E_first": float(E[0]), "E_last": float(E[-1]), "E_mean": float(E.mean()),
+                       "E_std": float(E.std()), "drift_kJ_mol_ns": slope,
+                       "drift_per_atom_kJ_mol_ns": slope / nat,
+                       "drift_rel_to_K_per_ns": slope / float(abs(K.mean())),
+                       "T_mean_K": float(2.0 * K.mean() / (ndof * W.KB)),
+                       "U_first": float(log[0, 1]), "U_last": float(log[-1, 1])},
+            "ms_per_step": t_steps / max(1, args.drift_steps),
+            "what": ("plain form, FP32 float-atomic force accumulation, FP64 energy sums" if arm == "fp32" else
+                     "persistent sweep, 64-bit fixed-point force accumulation, FP64 energy sums"),
+        }
+        eng.close()
+    print(json.dumps({
+        "drift": WORKLOADS[args.workload][0], "atoms": nat, "dof": ndof, "steps": args.drift_steps,
+        "dt_fs": dt_ps * 1e3, "ensemble": "NVE after relaxation",
+        "relaxation": {"steepest_descent_steps": args.min_steps, "phases": phases, "U_first": u_start,
+                       "U_relaxed": u_relaxed,
+                       "velocities": "Maxwell-Boltzmann 300 K (seed 11), net momentum removed", "s": round(relax_s, 2)},
+        "checkpoints": checkpoints, "arms": arms,
+        "oracle": "FP64 restatement on the same float tables and positions (the checker)",
+    }))
+
+
 def sched_ab(args, local_rank):
     """Makespan of the sweep with the count-product order, the learned order, a random order
     and the cell-major order tasks are generated in (same workload, autotuned launch shape,
@@ -803,11 +923,21 @@ def main():
                     help="train the task-cost model and compare sweep makespans of the queue orders")
     ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")
     ap.add_argument("--epochs", type=int, default=150, help="--sched-ab: training epochs")
+    ap.add_argument("--drift", action="store_true",
+                    help="energy drift and force errors over an MD trajectory of --workload (default chains): "
+                         "plain FP32 accumulation vs fixed point, against the FP64 oracle")
+    ap.add_argument("--drift-steps", type=int, default=10000, help="--drift: MD steps")
+    ap.add_argument("--min-steps", type=int, default=2000, help="--drift: steepest-descent steps first")
     args = ap.parse_args()
     if args.sub is None:
         args.sub = DEFAULT_SUB if args.workload == DEFAULT_WORKLOAD else ""
     if args.sched_ab:
         sched_ab(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
+    if args.drift:
+        if "--workload" not in sys.argv:
+            args.workload = "chains"
+        drift(args, int(os.environ.get("LOCAL_RANK", 0)))
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -581,6 +581,27 @@ int engine_cuda_resident_end(struct engine *e);
  * pointer may be NULL. */
 int engine_cuda_resident_info(struct engine *e, int *capc, int *mcap, long long *steps, long long *pairs,
                               int *regrows);
+/* Energy minimisation, no counterpart in the reference (its drivers start from relaxed or
+ * lattice systems): with gamma > 0 the resident steps move every particle by gamma f,
+ * held to at most dmax nm, and zero its velocity (steepest descent; the rigid constraints
+ * still apply); gamma <= 0 restores the time step. */
+int engine_cuda_minimize(struct engine *e, double gamma, double dmax);
+/* Per-step energy log of the resident steps, no counterpart in the reference (its drivers
+ * sum energies on the host every step): engine_cuda_energylog keeps a ring of the last
+ * `cap` steps' records (0: off; setting it clears the log, and so does
+ * engine_cuda_resident_begin); engine_cuda_energylog_read copies up to max records in step
+ * order: out[4 k + 0..3] = resident step number (1 = the first step after
+ * engine_cuda_resident_begin), potential energy (nonbonded + bonded), kinetic energy
+ * sum m v^2 / 2 of the velocities after the step (FP64 sums in fixed point), and their sum,
+ * in kJ/mol.  Returns the number of records.  The records sum over every engine of a
+ * batch. */
+int engine_cuda_energylog(struct engine *e, int cap);
+int engine_cuda_energylog_read(struct engine *e, double *out, int max);
+/* Force accumulation of the plain form (engine_cuda_settune(e, 0, 1)): 1 = FP32, each
+ * task's partial forces added as floats with float atomics (order-dependent, the way of
+ * the reference's GPU runner, src/runner_cuda.cu); 0 = 64-bit fixed point (the default,
+ * order-independent).  The persistent sweeps always accumulate in fixed point. */
+int engine_cuda_setaccum(struct engine *e, int fp32);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff

@@ -13,7 +13,8 @@
 //                by shuffles and over the warps in a fixed order, so every task produces
 //                the same FP32 partial forces whatever order the tasks run in; partials are
 //                converted once per particle and task to 64-bit fixed point and added with
-//                integer atomics.
+//                integer atomics (or, with FP32 accumulation, added as floats with float
+//                atomics, the order-dependent way of the reference's GPU runner).
 #pragma once
 #include "nb_device.cuh"
 
@@ -331,6 +332,35 @@ __device__ inline SweepSmem carve(unsigned char* base, int cap, int nw, int ncoe
     return s;
 }
 
+// A task's partial force on one particle: into the fixed-point accumulators, or, when the
+// engine accumulates in FP32, into the float forces with float atomics.
+__device__ __forceinline__ void add_task_force(const Params& P, size_t slot, float fx, float fy, float fz,
+                                               unsigned& status) {
+    if (P.force32 != nullptr) {
+        float* fp = P.force32 + 3 * slot;
+        atomicAdd(fp + 0, fx);
+        atomicAdd(fp + 1, fy);
+        atomicAdd(fp + 2, fz);
+        return;
+    }
+    unsigned long long* fp = P.force + 3 * slot;
+    atomic_add_fixed(fp + 0, to_fixed(fx, status));
+    atomic_add_fixed(fp + 1, to_fixed(fy, status));
+    atomic_add_fixed(fp + 2, to_fixed(fz, status));
+}
+
+// FP32 accumulation: the float forces of every slot into the fixed-point forces (which hold
+// nothing else yet), for the update and the readback.
+__global__ void __launch_bounds__(256) force32_to_fixed(const float* __restrict__ f32, unsigned long long* __restrict__ force,
+                                                        size_t n, unsigned long long* __restrict__ acc,
+                                                        const unsigned long long* __restrict__ abort) {
+    if (step_aborted(abort)) return;
+    unsigned status = 0;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        force[k] = (unsigned long long)to_fixed(f32[k], status);
+    if (status) atomicOr(&acc[kAccStatus], (unsigned long long)status);
+}
+
 // ---------------------------------------------------------------- sweep
 template <int NW>
 __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
@@ -499,10 +529,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             if (self) {
                 S.fi[loc] = make_float4(fix, fiy, fiz, 0.f);
             } else {
-                unsigned long long* fp = P.force + 3 * (size_t)(si + loc);
-                atomic_add_fixed(fp + 0, to_fixed(fix, status));
-                atomic_add_fixed(fp + 1, to_fixed(fiy, status));
-                atomic_add_fixed(fp + 2, to_fixed(fiz, status));
+                add_task_force(P, (size_t)(si + loc), fix, fiy, fiz, status);
             }
         }
     }
@@ -538,10 +565,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
                 a.x += b.x; a.y += b.y; a.z += b.z;
             }
             unsigned st = 0;
-            unsigned long long* fp = P.force + 3 * (size_t)(si + k);
-            atomic_add_fixed(fp + 0, to_fixed(a.x, st));
-            atomic_add_fixed(fp + 1, to_fixed(a.y, st));
-            atomic_add_fixed(fp + 2, to_fixed(a.z, st));
+            add_task_force(P, (size_t)(si + k), a.x, a.y, a.z, st);
             if (st) atomicOr(&P.acc[kAccStatus], (unsigned long long)st);
         }
     } else {
@@ -553,10 +577,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
                 a.x += b.x; a.y += b.y; a.z += b.z;
             }
             unsigned st = 0;
-            unsigned long long* fp = P.force + 3 * (size_t)(sj + S.jloc[k]);
-            atomic_add_fixed(fp + 0, to_fixed(a.x, st));
-            atomic_add_fixed(fp + 1, to_fixed(a.y, st));
-            atomic_add_fixed(fp + 2, to_fixed(a.z, st));
+            add_task_force(P, (size_t)(sj + S.jloc[k]), a.x, a.y, a.z, st);
             if (st) atomicOr(&P.acc[kAccStatus], (unsigned long long)st);
         }
     }

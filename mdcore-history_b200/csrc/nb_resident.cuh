@@ -202,6 +202,10 @@ __global__ void __launch_bounds__(256) slot_of_ids(ResidentCells RC, const int* 
 // the float expressions the host integrator evaluates: w = (float)(dt * 1/m),
 // v += f*w, x += dt*v; forces from the fixed-point accumulators of the sweep.  One thread
 // per slot (grid: ncells * capc threads).
+//
+// With sd_gamma > 0 the update is a steepest-descent move instead (an energy minimiser for
+// unrelaxed starts; no counterpart in the reference's step): x += g f with g = sd_gamma,
+// held so that no particle moves farther than sd_dmax, and v = 0.
 __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const int* __restrict__ count,
                                                        const unsigned long long* __restrict__ force,
                                                        const int* __restrict__ cell_engine,
@@ -210,7 +214,8 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
                                                        float4* __restrict__ xq, float4* __restrict__ v,
                                                        unsigned long long* __restrict__ status,
                                                        const unsigned long long* __restrict__ acc,
-                                                       unsigned long long* __restrict__ done) {
+                                                       unsigned long long* __restrict__ done, float sd_gamma,
+                                                       float sd_dmax) {
     if (*status != 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {          // completed steps, accepted pairs
         done[0] += 1ull;
@@ -230,6 +235,17 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
         const float fx = (float)((double)(long long)force[3 * s + 0] * (1.0 / (double)kForceScale));
         const float fy = (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale));
         const float fz = (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale));
+        if (sd_gamma > 0.f) {
+            const float fn = sqrtf(fx * fx + fy * fy + fz * fz);
+            const float g = fn * sd_gamma > sd_dmax ? sd_dmax / fn : sd_gamma;
+            x.x += g * fx;
+            x.y += g * fy;
+            x.z += g * fz;
+            xq[s] = x;
+            v[s] = make_float4(0.f, 0.f, 0.f, vv.w);
+            if (!isfinite(x.x + x.y + x.z)) atomicOr(status, (unsigned long long)kStatusNonFinite);
+            return;
+        }
         vv.x = __fadd_rn(vv.x, __fmul_rn(fx, w));
         vv.y = __fadd_rn(vv.y, __fmul_rn(fy, w));
         vv.z = __fadd_rn(vv.z, __fmul_rn(fz, w));
@@ -240,6 +256,69 @@ __global__ void __launch_bounds__(256) integrate_cells(ResidentCells RC, const i
         v[s] = vv;
         if (!isfinite(x.x + x.y + x.z + vv.x + vv.y + vv.z))      // a system blowing up: stop
             atomicOr(status, (unsigned long long)kStatusNonFinite);
+    }
+}
+
+// Per-step energy log (no counterpart in the reference; drivers such as
+// examples/argon/argon.c sum the kinetic energy on the host every step): the kinetic
+// energy of every particle's velocity after the step, sum of m v^2 / 2 in FP64 per thread,
+// to 2^32 fixed point per block and one integer atomic; then one block sums the cells'
+// fixed-point energies and the bonded energies and writes the record of the step.
+__global__ void __launch_bounds__(256) kinetic_cells(ResidentCells RC, const int* __restrict__ count,
+                                                     const int* __restrict__ cell_engine,
+                                                     const double* __restrict__ engine_imass, int max_type,
+                                                     const float4* __restrict__ xq, const float4* __restrict__ v,
+                                                     const unsigned long long* __restrict__ status,
+                                                     unsigned long long* __restrict__ ekin) {
+    __shared__ long long part[8];
+    if (*status != 0) return;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (s < (size_t)RC.ncells * RC.capc) {
+        const int c = (int)(s / (unsigned)RC.capc);
+        if ((int)(s - (size_t)c * RC.capc) < min(count[c], RC.capc)) {
+            const float4 vv = v[s];
+            const double im = engine_imass[(size_t)cell_engine[c] * max_type + __float_as_int(xq[s].w)];
+            e = 0.5 * ((double)vv.x * vv.x + (double)vv.y * vv.y + (double)vv.z * vv.z) / im;
+        }
+    }
+    long long q = __double2ll_rn(e * kEnergyScale);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        if (t != 0) atomicAdd(ekin, (unsigned long long)t);
+    }
+}
+
+__global__ void __launch_bounds__(1024) energy_record(const unsigned long long* __restrict__ cell_epot, int ncells,
+                                                      const unsigned long long* __restrict__ ebond, int nbond,
+                                                      const unsigned long long* __restrict__ ekin,
+                                                      const unsigned long long* __restrict__ base,
+                                                      const unsigned long long* __restrict__ done,
+                                                      const unsigned long long* __restrict__ status,
+                                                      unsigned long long* __restrict__ log, int cap) {
+    __shared__ long long part[32];
+    if (*status != 0) return;
+    long long q = 0;
+    for (int c = threadIdx.x; c < ncells; c += blockDim.x) q += (long long)cell_epot[c];
+    for (int k = threadIdx.x; k < nbond; k += blockDim.x) q += (long long)ebond[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        const unsigned long long n = *base + done[0];
+        unsigned long long* r = log + 4 * (size_t)((n - 1) % (unsigned long long)cap);
+        r[0] = n;
+        r[1] = (unsigned long long)t;
+        r[2] = *ekin;
+        r[3] = 0ull;
     }
 }
 

@@ -75,6 +75,15 @@ struct NbState {
     std::vector<float> h_qid;
     bool one_pot = false;           // every type pair uses table 0 (no per-pair lookup)
     int plain = 0;                 // 1: one CTA per task (the plain form); 0: persistent queue
+    int fp32acc = 0;               // plain form: forces accumulated in FP32 (float atomics)
+    float* d_force32 = nullptr;    // float forces of FP32 accumulation (3 per slot)
+    size_t force32_slots = 0;
+    // Resident steps: steepest-descent update instead of the time step (sd_gamma > 0), and a
+    // per-step energy log (elog_cap records, 0 = off).
+    float sd_gamma = 0.f, sd_dmax = 0.f;
+    int elog_cap = 0;
+    unsigned long long* r_elog = nullptr;    // elog_cap x {step number, epot, ekin, 0}
+    unsigned long long* r_eacc = nullptr;    // the step's kinetic-energy accumulator, step-number base
     int* d_order = nullptr;        // task queue order (scheduling order of all tasks)
     int* d_queue = nullptr;        // compacted queue of the current step
     int* d_qcount = nullptr;
@@ -669,12 +678,37 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
     P.ep_pot = st->ep_pot;
     P.tab_global = st->tab_global;
 
+    const bool f32 = st->plain && st->fp32acc;
+    if (f32) {
+        if (st->force32_slots < V.slots) {           // grown on a direct launch, never in a capture
+            if (st->capturing) {
+                errs_register(engine_err_cuda, "FP32 force buffer too small inside a stream capture.", __LINE__,
+                              __func__, __FILE__);
+                return engine_err = engine_err_cuda;
+            }
+            if (st->d_force32) CU(cudaFree(st->d_force32));
+            st->d_force32 = nullptr;
+            st->force32_slots = 0;
+            CU(cudaMalloc(&st->d_force32, sizeof(float) * 3 * V.slots));
+            st->force32_slots = V.slots;
+            st->buf_gen++;                           // graphs holding the old buffer are re-made
+        }
+        CU(cudaMemsetAsync(st->d_force32, 0, sizeof(float) * 3 * V.slots, st->stream));
+        P.force32 = st->d_force32;
+    }
     int rc = record_event(st, st->evs0);
     if (rc < 0) return rc;
     rc = st->plain ? launch_plain(st, P, cap) : launch_tuned(st, P, cap);
     if (rc < 0) return rc;
     rc = record_event(st, st->evs1);
-    if (rc < 0 || !span) return rc;
+    if (rc < 0) return rc;
+    if (f32) {
+        const size_t n = 3 * V.slots;
+        const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)st->sm_count * 8);
+        force32_to_fixed<<<blocks, 256, 0, st->stream>>>(st->d_force32, V.force, n, st->d_acc, V.abort);
+        CU(cudaGetLastError());
+    }
+    if (!span) return 0;
     return record_event(st, st->ev1);
 }
 
@@ -700,6 +734,7 @@ long long launch_key(const NbState* st) {
     k = k * 3 + (st->occupancy == 640 ? 0 : st->occupancy == 768 ? 1 : 2);
     k = k * 3 + st->plain;
     k = k * 3 + st->record_clock;
+    k = k * 2 + st->fp32acc;
     return k;
 }
 
@@ -798,7 +833,7 @@ void state_free(NbState* st) {
                    st->d_cscale, st->d_acc, st->d_cell_epot, st->d_tasks, st->d_tshift, st->d_coef, st->d_potinfo,
                    st->d_potn, st->d_potidx, st->d_emask, st->d_exoff, st->d_exlist, st->d_order,
                    st->d_counter, st->d_task_clock, st->d_task_sm, st->d_forcef, st->d_queue,
-                   st->d_qcount, st->d_bsum, st->d_qid};
+                   st->d_qcount, st->d_bsum, st->d_qid, st->d_force32, st->r_elog, st->r_eacc};
     for (void* p : dev) cudaFree(p);
     void* host[] = {st->h_xq, st->h_pid, st->h_cstart, st->h_force, st->h_cell_epot, st->h_acc};
     for (void* p : host) cudaFreeHost(p);
@@ -1747,6 +1782,15 @@ int st_resident_begin(NbState* st, int margin, int mcap) {
     return 0;
 }
 
+// A fresh start of resident steps: the energy log's step numbers restart from 1.
+int elog_restart(NbState* st) {
+    if (st->elog_cap <= 0) return 0;
+    const unsigned long long zero = 0ull;
+    CU(cudaMemset(st->r_elog, 0, sizeof(unsigned long long) * 4 * (size_t)st->elog_cap));
+    CU(cudaMemcpy(st->r_eacc + 1, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    return 0;
+}
+
 // The launches of one resident step: re-binning into the other side, the force evaluation,
 // the integration, the rigid constraints.
 int res_issue_step(NbState* st) {
@@ -1811,7 +1855,7 @@ int res_issue_step(NbState* st) {
     // One engine whose every particle is in a rigid group (rigid water): the constraint
     // kernel runs the update too (same arithmetic), one launch less per step.
     bool fuse = false;
-    if (st->engines.size() == 1 && st->engines[0]->nr_rigids > 0) {
+    if (st->engines.size() == 1 && st->engines[0]->nr_rigids > 0 && st->sd_gamma <= 0.f) {
         const struct engine* e = st->engines[0];
         long long in_groups = 0;
         for (int g = 0; g < e->nr_rigids; g++) in_groups += e->rigids[g].nr_parts;
@@ -1822,7 +1866,7 @@ int res_issue_step(NbState* st) {
         integrate_cells<<<slot_blocks, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_force, st->r_cell_engine,
                                                              st->r_engine_dt, st->r_engine_imass, st->max_type,
                                                              st->r_xq[o], st->r_v[o], st->r_status, st->d_acc,
-                                                             st->r_done);
+                                                             st->r_done, st->sd_gamma, st->sd_dmax);
         CU(cudaGetLastError());
     }
     for (size_t k = 0; k < st->engines.size(); k++) {
@@ -1846,6 +1890,18 @@ int res_issue_step(NbState* st) {
         rc = rigid_eval_resident(e, &view, st->stream);
         if (rc < 0) return rc;
     }
+    if (st->elog_cap > 0) {            // the step's energies into the log
+        CU(cudaMemsetAsync(st->r_eacc, 0, sizeof(unsigned long long), st->stream));
+        const unsigned slot_blocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
+        kinetic_cells<<<slot_blocks, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_cell_engine, st->r_engine_imass,
+                                                           st->max_type, st->r_xq[o], st->r_v[o], st->r_status,
+                                                           st->r_eacc);
+        energy_record<<<1, 1024, 0, st->stream>>>(st->d_cell_epot, st->ncells, st->r_ebond,
+                                                  res_bonded(st) ? 3 * (int)st->engines.size() : 0, st->r_eacc,
+                                                  st->r_eacc + 1, st->r_done, st->r_status, st->r_elog,
+                                                  st->elog_cap);
+        CU(cudaGetLastError());
+    }
     return record_event(st, st->ev1);
 }
 
@@ -1860,6 +1916,9 @@ long long res_key(const NbState* st) {
     k = k * 3 + (st->occupancy == 640 ? 0 : st->occupancy == 768 ? 1 : 2);
     k = k * 3 + st->plain;
     k = k * 3 + st->record_clock;
+    k = k * 2 + st->fp32acc;
+    k = k * 2 + (st->sd_gamma > 0.f);
+    k = k * 2 + (st->elog_cap > 0);
     return k;
 }
 
@@ -1963,6 +2022,10 @@ int st_resident_steps(NbState* st, int nsteps) {
         st->res_done_total = done;
         st->res_pairs_total = pairs;
         st->res_regrows = total_regrows;
+        if (st->elog_cap > 0) {       // the log keeps counting from the steps already done
+            const unsigned long long base = (unsigned long long)done;
+            CU(cudaMemcpy(st->r_eacc + 1, &base, sizeof(base), cudaMemcpyHostToDevice));
+        }
     }
     return 0;
 }
@@ -2228,6 +2291,83 @@ extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages, i
     return st_setlayout(state(e), layout, stages, occupancy);
 }
 
+// FP32 force accumulation (fp32 = 1: the plain form adds each task's partial forces as
+// floats with float atomics) or 64-bit fixed point (0, the default).
+extern "C" int engine_cuda_setaccum(struct engine* e, int fp32) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (fp32 != 0 && fp32 != 1) return engine_err_range;
+    state(e)->fp32acc = fp32;
+    return 0;
+}
+
+// Steepest-descent resident steps: x += g f, |g f| <= dmax, v = 0 (gamma <= 0: time steps).
+extern "C" int engine_cuda_minimize(struct engine* e, double gamma, double dmax) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (gamma > 0.0 && !(dmax > 0.0)) return engine_err_range;
+    NbState* st = state(e);
+    st->sd_gamma = gamma > 0.0 ? (float)gamma : 0.f;
+    st->sd_dmax = gamma > 0.0 ? (float)dmax : 0.f;
+    return 0;
+}
+
+// Per-step energy log of the resident steps: a ring of `cap` records (0: off).  Setting it
+// (again) clears the log.
+extern "C" int engine_cuda_energylog(struct engine* e, int cap) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (cap < 0) return engine_err_range;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    if (cap != st->elog_cap) {
+        if (st->r_elog) CU(cudaFree(st->r_elog));
+        if (st->r_eacc) CU(cudaFree(st->r_eacc));
+        st->r_elog = nullptr;
+        st->r_eacc = nullptr;
+        st->elog_cap = 0;
+        st->buf_gen++;
+        if (cap > 0) {
+            CU(cudaMalloc(&st->r_elog, sizeof(unsigned long long) * 4 * (size_t)cap));
+            CU(cudaMalloc(&st->r_eacc, sizeof(unsigned long long) * 2));
+        }
+        st->elog_cap = cap;
+    }
+    if (cap > 0) {
+        CU(cudaMemset(st->r_elog, 0, sizeof(unsigned long long) * 4 * (size_t)cap));
+        const unsigned long long base =
+            st->res_active ? (unsigned long long)(st->res_done_total + st->res_done) : 0ull;
+        CU(cudaMemcpy(st->r_eacc + 1, &base, sizeof(base), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+// The records of the log in step order: out[4 k + 0..3] = resident step number (1 = the
+// first step after engine_cuda_resident_begin), potential energy (nonbonded + bonded),
+// kinetic energy of the velocities after the step, their sum (kJ/mol).  Returns the count.
+extern "C" int engine_cuda_energylog_read(struct engine* e, double* out, int max) {
+    if (e == nullptr || e->cuda == nullptr || (out == nullptr && max > 0)) return engine_err_null;
+    NbState* st = state(e);
+    if (st->elog_cap <= 0) return 0;
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    std::vector<unsigned long long> h(4 * (size_t)st->elog_cap);
+    CU(cudaMemcpy(h.data(), st->r_elog, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> idx;
+    for (int k = 0; k < st->elog_cap; k++)
+        if (h[4 * (size_t)k] != 0) idx.push_back(k);
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return h[4 * (size_t)a] < h[4 * (size_t)b]; });
+    const int n = std::min((int)idx.size(), std::max(max, 0));
+    const size_t skip = idx.size() - (size_t)n;      // the latest records when max is smaller
+    for (int q = 0; q < n; q++) {
+        const unsigned long long* r = &h[4 * (size_t)idx[skip + q]];
+        const double ep = (double)(long long)r[1] / kEnergyScale, ek = (double)(long long)r[2] / kEnergyScale;
+        out[4 * q + 0] = (double)r[0];
+        out[4 * q + 1] = ep;
+        out[4 * q + 2] = ek;
+        out[4 * q + 3] = ep + ek;
+    }
+    return n;
+}
+
 extern "C" int engine_cuda_graph(struct engine* e, int enable) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     NbState* st = state(e);
@@ -2285,7 +2425,8 @@ extern "C" int engine_nonbond_cuda_resident(struct engine* e) {
 // Runs further launches on a caller-provided stream (e.g. the framework's current stream).
 extern "C" int engine_cuda_resident_begin(struct engine* e, int margin) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
-    return st_resident_begin(state(e), margin, 16);
+    const int rc = st_resident_begin(state(e), margin, 16);
+    return rc < 0 ? rc : elog_restart(state(e));
 }
 
 extern "C" int engine_cuda_resident_steps(struct engine* e, int nsteps) {
@@ -2505,7 +2646,8 @@ extern "C" int engine_batch_step_host(struct engine_batch* b) {
 // engine_zero_forces for every engine of the batch (host threads over the cells).
 extern "C" int engine_batch_resident_begin(struct engine_batch* b, int margin) {
     if (b == nullptr) return engine_err_null;
-    return st_resident_begin(bstate(b), margin, 16);
+    const int rc = st_resident_begin(bstate(b), margin, 16);
+    return rc < 0 ? rc : elog_restart(bstate(b));
 }
 
 extern "C" int engine_batch_resident_steps(struct engine_batch* b, int nsteps) {

@@ -161,6 +161,10 @@ def lib() -> C.CDLL:
         "engine_batch_resident_end": (C.c_int, [vp]),
         "engine_cuda_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), P(C.c_longlong), ip]),
         "engine_batch_resident_info": (C.c_int, [vp, ip, ip, P(C.c_longlong), P(C.c_longlong), ip]),
+        "engine_cuda_minimize": (C.c_int, [vp, C.c_double, C.c_double]),
+        "engine_cuda_energylog": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_energylog_read": (C.c_int, [vp, dp, C.c_int]),
+        "engine_cuda_setaccum": (C.c_int, [vp, C.c_int]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -381,6 +385,28 @@ class Engine:
         and step, completed steps and their accepted pairs, re-blockings."""
         return _resident_info(self.lib.engine_cuda_resident_info, self.ptr)
 
+    def minimize(self, gamma: float, dmax: float = 0.01):
+        """Resident steps become steepest-descent moves x += gamma f (at most dmax nm per
+        particle, velocities zeroed); gamma <= 0 restores the time step."""
+        _check(self.lib.engine_cuda_minimize(self.ptr, gamma, dmax), "engine_cuda_minimize")
+        return self
+
+    def energy_log(self, cap: int):
+        """Per-step energy log of the resident steps, a ring of `cap` records (0: off)."""
+        _check(self.lib.engine_cuda_energylog(self.ptr, cap), "engine_cuda_energylog")
+        return self
+
+    def energy_log_read(self, cap: int) -> np.ndarray:
+        """Records in step order: (step, potential, kinetic, total) per row, kJ/mol."""
+        out = np.zeros((max(cap, 1), 4))
+        n = _check(self.lib.engine_cuda_energylog_read(self.ptr, _dptr(out), cap), "engine_cuda_energylog_read")
+        return out[:n]
+
+    def set_accum(self, fp32: bool):
+        """Force accumulation of the plain form: FP32 float atomics (True) or fixed point."""
+        _check(self.lib.engine_cuda_setaccum(self.ptr, int(fp32)), "engine_cuda_setaccum")
+        return self
+
     def load_parts(self):
         _check(self.lib.engine_cuda_load_parts(self.ptr), "engine_cuda_load_parts")
 
@@ -553,6 +579,16 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def leapfrog_energy(log: np.ndarray, dt_ps: float):
+    """Total energy of the leap-frog steps of an energy log (rows: step, U, K after the step,
+    U + K): E_t = U_t + (K(v_(t-1/2)) + K(v_(t+1/2))) / 2 for every record after the first,
+    the times in ns, and the least-squares drift of E (kJ/mol/ns)."""
+    E = log[1:, 1] + 0.5 * (log[:-1, 2] + log[1:, 2])
+    t_ns = log[1:, 0] * dt_ps * 1e-3
+    slope = float(np.polyfit(t_ns, E, 1)[0]) if len(E) > 2 else 0.0
+    return E, t_ns, slope
 
 
 def fp32_peak_tflops(device: int = 0) -> float:
