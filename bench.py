@@ -818,6 +818,10 @@ def drift(args, local_rank):
                 done = cp
             eng.nonbond()                      # forces at the positions of step `cp`
             errs[str(cp)] = errors(eng)
+            if cp > 0:
+                itmax, bad = eng.rigid_stats()
+                errs[str(cp)]["shake_max_iterations"] = itmax
+                errs[str(cp)]["shake_unconverged"] = bad
         log = np.concatenate(logs)
         E, t_ns, slope = M.leapfrog_energy(log, dt_ps)
         K = log[:, 2]
@@ -834,13 +838,53 @@ def drift(args, local_rank):
                      "persistent sweep, 64-bit fixed-point force accumulation, FP64 energy sums"),
         }
         eng.close()
+    # time-step scan of the fixed-point arm: the drift of a leap-frog integrator limited by
+    # its stiffest modes falls as dt^2
+    scan = []
+    nscan = min(2000, args.drift_steps)
+    for dt_fs in [float(v) for v in args.drift_dts.split(",") if v]:
+        eng = M.Engine.from_system(dataclasses.replace(relaxed, dt=dt_fs * 1e-3), device=local_rank)
+        eng.graph(True)
+        eng.energy_log(nscan + 8)
+        eng.resident_begin()
+        eng.resident_steps(nscan)
+        lg = eng.energy_log_read(nscan + 8)
+        eng.resident_end()
+        itmax, bad = eng.rigid_stats()
+        eng.close()
+        _, _, sl = M.leapfrog_energy(lg, dt_fs * 1e-3)
+        scan.append({"dt_fs": dt_fs, "steps": nscan, "drift_per_atom_kJ_mol_ns": sl / nat,
+                     "T_mean_K": float(2.0 * lg[:, 2].mean() / (ndof * W.KB)),
+                     "shake_max_iterations": itmax, "shake_unconverged": bad})
+    # run-to-run reproducibility: each arm twice over the same steps from the same state
+    nrep = min(1000, args.drift_steps)
+    for arm in ("fp32", "fixed"):
+        runs = []
+        for _ in range(2):
+            eng = M.Engine.from_system(relaxed, device=local_rank)
+            if arm == "fp32":
+                eng.tune(0, plain=True)
+                eng.set_accum(True)
+            eng.graph(True)
+            eng.resident_begin()
+            eng.resident_steps(nrep)
+            eng.resident_end()
+            xx, _, pp, _ = eng.unload()
+            xs = np.zeros_like(xx)
+            xs[pp] = xx
+            runs.append(xs)
+            eng.close()
+        d = runs[1] - runs[0]
+        d -= np.round(d / np.asarray(sysm.dim)) * np.asarray(sysm.dim)
+        arms[arm]["repeat"] = {"steps": nrep, "bit_identical": bool(np.array_equal(runs[0], runs[1])),
+                               "max_dx_nm": float(np.abs(d).max())}
     print(json.dumps({
-        "drift": WORKLOADS[args.workload][0], "atoms": nat, "dof": ndof, "steps": args.drift_steps,
+        "drift": WORKLOADS[args.workload][0].replace("; force evaluation only", ""), "atoms": nat, "dof": ndof, "steps": args.drift_steps,
         "dt_fs": dt_ps * 1e3, "ensemble": "NVE after relaxation",
         "relaxation": {"steepest_descent_steps": args.min_steps, "phases": phases, "U_first": u_start,
                        "U_relaxed": u_relaxed,
                        "velocities": "Maxwell-Boltzmann 300 K (seed 11), net momentum removed", "s": round(relax_s, 2)},
-        "checkpoints": checkpoints, "arms": arms,
+        "checkpoints": checkpoints, "arms": arms, "dt_scan_fixed_point": scan,
         "oracle": "FP64 restatement on the same float tables and positions (the checker)",
     }))
 
@@ -928,6 +972,7 @@ def main():
                          "plain FP32 accumulation vs fixed point, against the FP64 oracle")
     ap.add_argument("--drift-steps", type=int, default=10000, help="--drift: MD steps")
     ap.add_argument("--min-steps", type=int, default=2000, help="--drift: steepest-descent steps first")
+    ap.add_argument("--drift-dts", default="2,1,0.5", help="--drift: time steps (fs) of the fixed-point dt scan")
     args = ap.parse_args()
     if args.sub is None:
         args.sub = DEFAULT_SUB if args.workload == DEFAULT_WORKLOAD else ""

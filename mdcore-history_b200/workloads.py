@@ -334,7 +334,8 @@ QSCALE = math.sqrt(Q_SCALE)     # e -> per-particle charge unit of tables with p
 
 def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box=(10.8, 10.8, 7.8), seed: int = 0,
                  cutoff: float = 1.2, tol: float = 1e-4, bond: float = 0.15, gap: float = 0.12,
-                 bond_k: float = 2.0e5, clearance: float = 0.25, angles_dihedrals: bool = True) -> System:
+                 bond_k: float = 2.0e5, clearance: float = 0.25, angles_dihedrals: bool = True,
+                 h_sigma: float = 0.2) -> System:
     """Heterogeneous solvated-chain system: `nchains` linear bead chains of `length` beads
     (bond 0.15 nm, 20 LJ bead types with sigma U[0.25, 0.40] nm and epsilon U[0.1, 1.0]
     kJ/mol, Lorentz-Berthelot mixing, charges N(0, 0.3) e neutralised per chain) and up to
@@ -343,7 +344,7 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
     jittered grid at 33.4 molecules/nm^3, waters whose oxygen is closer than `gap` to a bead
     left out (0.12 nm: the 23,400 waters of the named system fit; the close contacts this
     leaves make the unrelaxed system unfit for dynamics, 0.25 nm gives a calmer one).  Charges act through explicit electrostatics (ep: the shifted Coulomb table
-    with unit charge, cutoff 1.2 nm); the type tables are LJ only (none for H).  1-2 and 1-3
+    with unit charge, cutoff 1.2 nm); the type tables are LJ only (H: sigma h_sigma, epsilon 0.1).  1-2 and 1-3
     exclusions along the chains, the three intramolecular pairs of every water excluded;
     chain bonds harmonic, bond_k (r - 0.15 nm)^2 (bond_pot, a table on [0.05, 0.3] nm).
     With `angles_dihedrals`, every three consecutive beads also form a harmonic angle
@@ -428,8 +429,10 @@ def chains_water(nchains: int = 220, length: int = 100, nwater: int = 23400, box
                     np.stack([k + 1, k + 2, np.full(nw, hhd)], 1)], 1).reshape(-1, 3)
     # --- potentials: LJ among O, H and the bead types (Lorentz-Berthelot).  SPC/E gives H
     # no LJ; with per-particle charges an H next to a negative bead would then meet no
-    # repulsion at all, so H carries a small one (sigma 0.1 nm, epsilon 0.1 kJ/mol).
-    sig = np.concatenate([[0.3166, 0.1], sig_b])
+    # repulsion at all, so H carries a small one (sigma `h_sigma`, epsilon 0.1 kJ/mol).
+    # With sigma 0.1 nm the H-bead contacts are stiff enough that 2 fs steps heat the
+    # system about twice as fast as with 0.2 nm (the drift of either falls as dt^2).
+    sig = np.concatenate([[0.3166, h_sigma], sig_b])
     eps = np.concatenate([[0.650, 0.1], eps_b])
     lj_types = [0, 1] + list(range(2, 2 + nbt))
     pots = []
