@@ -252,6 +252,9 @@ struct space {
     float maxdx;
     double epot, epot_nonbond, epot_bond, epot_angle, epot_dihedral, epot_exclusion;
     double ekin;
+    /* Queue statistics of the reference's CPU runners (src/space.h:118, reset per step by
+     * space_prepare): there are no CPU runner queues here, so both stay 0. */
+    int nr_swaps, nr_stalls;
 };
 
 /* src/space.c:530-783 and src/space.c:80-114. */
@@ -602,6 +605,16 @@ int engine_cuda_energylog_read(struct engine *e, double *out, int max);
  * the reference's GPU runner, src/runner_cuda.cu); 0 = 64-bit fixed point (the default,
  * order-independent).  The persistent sweeps always accumulate in fixed point. */
 int engine_cuda_setaccum(struct engine *e, int fp32);
+/* The failure path of the device waits, no counterpart in the reference: every wait of a
+ * sweep on its staging copies (an mbarrier) polls at most `polls` times (<= 0: the default,
+ * 2^22), after which the kernel records a copy timeout, waits once more for copies in
+ * flight and returns; the evaluation then fails with engine_err_cuda and "Bulk copy into
+ * shared memory timed out." in the error stack, and the device stays usable.
+ * engine_cuda_copytimeout_test(e, 1) makes every such wait run out (the barriers are armed,
+ * no copy is issued, so nothing is in flight), for testing that path; 0 turns it off.
+ * Both settings hold for every engine on the engine's device. */
+int engine_cuda_setspin(struct engine *e, int polls);
+int engine_cuda_copytimeout_test(struct engine *e, int enable);
 
 /* ---- batches of engines (no counterpart in the reference) ----
  * One device state for many independent engines (replicas: the same potentials, cutoff

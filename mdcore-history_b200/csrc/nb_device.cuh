@@ -21,7 +21,13 @@ namespace nb {
 constexpr float kForceScale = 16777216.0f;          // 2^24
 constexpr double kEnergyScale = 4294967296.0;       // 2^32
 constexpr int kMaxPartsPerCell = 1024;
-constexpr int kSpinLimit = 1 << 22;                 // bounded waits
+constexpr int kSpinLimit = 1 << 22;                 // bounded waits: default polls per wait
+// Polls per bounded wait of the sweeps (engine_cuda_setspin; kSpinLimit by default), and a
+// test hook (engine_cuda_copytimeout_test): when set, the sweeps arm their mbarriers for
+// the staging copies but issue no copy, so every such wait runs out and reports
+// kStatusCopyTimeout with nothing left in flight.
+__constant__ int c_spin_limit = kSpinLimit;
+__constant__ int c_skip_copies = 0;
 
 // Status bits of the device status word.
 enum : unsigned {
@@ -130,9 +136,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for phase `parity` of `bar` to complete, at most kSpinLimit polls.
+// Waits for phase `parity` of `bar` to complete, at most c_spin_limit polls.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (int it = 0; it < kSpinLimit; ++it)
+    const int limit = c_spin_limit;
+    for (int it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

@@ -393,6 +393,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     if (tid == 0) {
         const uint32_t bytes = self ? (uint32_t)padj * 20u : (uint32_t)(padi + padj) * 24u;
         mbar_arrive_expect_tx(S.bar, bytes);
+        if (!c_skip_copies) {          // the test hook leaves the wait to run out
         bulk_g2s(S.xj, P.xq + sj, padj * 16, S.bar);
         bulk_g2s(S.pidj, P.pid + sj, padj * 4, S.bar);
         if (!self) {
@@ -400,6 +401,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
             bulk_g2s(S.xi, P.xq + si, padi * 16, S.bar);
             bulk_g2s(S.pidi, P.pid + si, padi * 4, S.bar);
             bulk_g2s(S.keyi, P.keys + 13 * (size_t)si + (size_t)tr.sid * padi, padi * 4, S.bar);
+        }
         }
     }
     if (!P.tab_global) {

@@ -372,6 +372,7 @@ __device__ __forceinline__ void issue_copies(const Params& P, const TaskDesc& d,
         const int padi = (d.ni + 3) & ~3, padj = (d.nj + 3) & ~3;
         fence_proxy_async();
         mbar_arrive_expect_tx(W.bar, self ? (uint32_t)padj * 20u : (uint32_t)padj * 24u + (uint32_t)padi * 4u);
+        if (c_skip_copies) return;     // test hook: the wait on W.bar runs out
         bulk_g2s(W.xraw, P.xq + d.sj, padj * 16, W.bar);
         bulk_g2s(W.pidraw, P.pid + d.sj, padj * 4, W.bar);
         if (!self) {
@@ -439,8 +440,15 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
         }
         const WarpSlice W = warp_slice(smem_raw, cap, warp, STAGES, s);
         if (!__all_sync(0xffffffffu, mbar_wait_bounded(W.bar, (phases >> s) & 1))) {
+            // A copy that has not landed after a whole bounded wait: flag it, give the copies
+            // still in flight a second bounded wait (their destination is this warp's
+            // slice, which must outlive them), and stop popping tasks.  These are the only
+            // copies this warp can have in flight: with two staging buffers the next task's
+            // copies are issued only after the current task's have landed.  If even the
+            // second wait runs out, the block may exit with a copy outstanding; the status
+            // makes the evaluation fail.
             status |= kStatusCopyTimeout;
-            mbar_wait_bounded(W.bar, (phases >> s) & 1);   // second bounded chance for copies in flight
+            mbar_wait_bounded(W.bar, (phases >> s) & 1);
             return;
         }
         phases ^= 1u << s;

@@ -2293,6 +2293,32 @@ extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages, i
 
 // FP32 force accumulation (fp32 = 1: the plain form adds each task's partial forces as
 // floats with float atomics) or 64-bit fixed point (0, the default).
+// Polls per bounded wait of the sweeps on the engine's device (polls <= 0: the default,
+// kSpinLimit).  A wait that runs out makes the evaluation report a copy timeout.
+extern "C" int engine_cuda_setspin(struct engine* e, int polls) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    const int v = polls > 0 ? polls : kSpinLimit;
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    CU(cudaMemcpyToSymbol(c_spin_limit, &v, sizeof(v)));
+    return 0;
+}
+
+// Test hook of the failure path: with enable = 1 the sweeps on the engine's device arm
+// their mbarriers for the staging copies but issue none, so every wait runs out after the
+// spin limit, the evaluation fails with engine_err_cuda ("Bulk copy into shared memory
+// timed out.") and nothing is left in flight; 0 restores normal copies.
+extern "C" int engine_cuda_copytimeout_test(struct engine* e, int enable) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if (enable != 0 && enable != 1) return engine_err_range;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    CU(cudaMemcpyToSymbol(c_skip_copies, &enable, sizeof(enable)));
+    return 0;
+}
+
 extern "C" int engine_cuda_setaccum(struct engine* e, int fp32) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     if (fp32 != 0 && fp32 != 1) return engine_err_range;

@@ -165,6 +165,8 @@ def lib() -> C.CDLL:
         "engine_cuda_energylog": (C.c_int, [vp, C.c_int]),
         "engine_cuda_energylog_read": (C.c_int, [vp, dp, C.c_int]),
         "engine_cuda_setaccum": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_setspin": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_copytimeout_test": (C.c_int, [vp, C.c_int]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_targets": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -405,6 +407,16 @@ class Engine:
     def set_accum(self, fp32: bool):
         """Force accumulation of the plain form: FP32 float atomics (True) or fixed point."""
         _check(self.lib.engine_cuda_setaccum(self.ptr, int(fp32)), "engine_cuda_setaccum")
+        return self
+
+    def set_spin(self, polls: int):
+        """Polls per bounded wait of the sweeps on this engine's device (<= 0: default)."""
+        _check(self.lib.engine_cuda_setspin(self.ptr, polls), "engine_cuda_setspin")
+        return self
+
+    def copytimeout_test(self, enable: bool):
+        """Test hook: the sweeps' staging copies are not issued, so their waits run out."""
+        _check(self.lib.engine_cuda_copytimeout_test(self.ptr, int(enable)), "engine_cuda_copytimeout_test")
         return self
 
     def load_parts(self):
