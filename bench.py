@@ -450,10 +450,10 @@ def measure(workload, args, rank, world, local_rank, dist, with_cpu):
     dt_fs = systems[0].dt * 1e3
     rigid = any(s.rigid is not None and len(s.rigid) for s in systems)
     if replicas:
-        engines = [M.Engine.from_system(s, start=False) for s in systems]
+        engines = [M.Engine.from_system(s, flags=args.engine_flags, start=False) for s in systems]
         tgt = M.Batch(engines, device=local_rank)
     else:
-        engines = [M.Engine.from_system(built, device=local_rank)]
+        engines = [M.Engine.from_system(built, flags=args.engine_flags, device=local_rank)]
         tgt = engines[0]
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -645,7 +645,8 @@ def measure(workload, args, rank, world, local_rank, dist, with_cpu):
                 "config": config, "parallelism": parallelism,
                 "pairs_per_step_timed": pairs_all,
                 "step": "engine_step on the device: re-binning, sort, sweep, integration"
-                        + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step",
+                        + (", P-SHAKE" if rigid else "") + "; one CUDA graph per step"
+                        + ("; Verlet skin (re-binning and sort only on rebuild steps)" if args.verlet else ""),
                 "setup": setup,
                 "e2e": {"value": pairs_all / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
                         "ns_per_day": ns_per_day(e2e_ms, dt_fs), "h2d_bytes_per_step": h2d,
@@ -973,7 +974,12 @@ def main():
     ap.add_argument("--drift-steps", type=int, default=10000, help="--drift: MD steps")
     ap.add_argument("--min-steps", type=int, default=2000, help="--drift: steepest-descent steps first")
     ap.add_argument("--drift-dts", default="2,1,0.5", help="--drift: time steps (fs) of the fixed-point dt scan")
+    ap.add_argument("--verlet", action="store_true",
+                    help="engine_flag_verlet_pseudo: the resident steps re-bin and sort only when the largest "
+                         "displacement exceeds half the skin (min h - cutoff)")
     args = ap.parse_args()
+    import mdcore_b200 as M
+    args.engine_flags = M.engine_flag_cuda | (M.engine_flag_verlet_pseudo if args.verlet else 0)
     if args.sub is None:
         args.sub = DEFAULT_SUB if args.workload == DEFAULT_WORKLOAD else ""
     if args.sched_ab:

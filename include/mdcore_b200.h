@@ -93,8 +93,13 @@ extern int space_err;      /* src/space.h:60 */
 
 /* ---------------------------------------------------------------- engine flags
  * Same bits as src/engine.h:56-72.  Honoured: none, cuda, unsorted (sweep without the
- * projection cut), verlet_pseudo/verlet/verlet_pairwise (accepted; sorts are redone every
- * step), affinity (ignored), shake.  Others make engine_init fail with engine_err_nyi. */
+ * projection cut), verlet (implied by verlet_pairwise, which verlet_pseudo implies, as in
+ * src/engine.c:2458-2461: in the device-resident steps particles are re-binned and sorted
+ * only when twice the largest displacement since the last rebuild exceeds the skin
+ * min(h) - cutoff or it exceeds cutoff/4, src/engine.c:193-315, and the sweep bound carries
+ * both cells' displacements, src/runner_dopair.c:583; engine_step and the host-buffer
+ * evaluations re-sort every call), affinity (ignored), shake.  Others make engine_init fail
+ * with engine_err_nyi. */
 #define engine_flag_none             0
 #define engine_flag_static           1
 #define engine_flag_localparts       2
@@ -614,6 +619,9 @@ int engine_cuda_setaccum(struct engine *e, int fp32);
  * no copy is issued, so nothing is in flight), for testing that path; 0 turns it off.
  * Both settings hold for every engine on the engine's device. */
 int engine_cuda_setspin(struct engine *e, int polls);
+/* With engine_flag_verlet: the rebuilds (re-binning and sort) the resident steps did since
+ * the particles were uploaded; -1 without the flag or resident particles. */
+int engine_cuda_verlet_rebuilds(struct engine *e, int *rebuilds);
 int engine_cuda_copytimeout_test(struct engine *e, int enable);
 
 /* ---- batches of engines (no counterpart in the reference) ----

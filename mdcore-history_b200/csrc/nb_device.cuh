@@ -90,7 +90,20 @@ struct Params {
     // float atomics (FP32 accumulation, order-dependent, as the reference's GPU runner adds
     // them) instead of to the fixed-point accumulators.
     float* force32 = nullptr;
+    // Verlet skin (resident steps with engine_flag_verlet): the sort keys are those of the
+    // last rebuild, and each cell's particles have moved since by at most cell_mdx[c] key
+    // units; a pair task's projection bound widens by cell_mdx[ci] + cell_mdx[cj]
+    // (src/runner_dopair.c:583: cutoff + maxdx_i + maxdx_j).  nullptr: fresh keys.
+    const int* cell_mdx = nullptr;
 };
+
+// The projection bound of a pair task, widened by the cells' displacements since the keys
+// were made (Verlet skin).
+__device__ __forceinline__ int task_dmax_skin(const Params& P, const TaskRec& r) {
+    int d = task_dmax(r);
+    if (P.cell_mdx != nullptr && r.sid >= 0) d += P.cell_mdx[r.ci] + P.cell_mdx[r.cj];
+    return d;
+}
 
 // A device-resident step that was aborted (see nb_resident.cuh) launches nothing more.
 __device__ __forceinline__ bool step_aborted(const unsigned long long* abort) {

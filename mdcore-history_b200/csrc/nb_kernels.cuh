@@ -192,9 +192,11 @@ __global__ void __launch_bounds__(kSortWarps * 32, 4) sort_cells(const float4* _
                                                               unsigned* __restrict__ keys,
                                                               const float2* __restrict__ cscale, int ncells, int cpc,
                                                               int scap, unsigned long long* acc,
-                                                              const unsigned long long* abort) {
+                                                              const unsigned long long* abort,
+                                                              const int* __restrict__ rebuild) {
     extern __shared__ __align__(16) unsigned char sort_smem[];
     if (step_aborted(abort)) return;
+    if (rebuild != nullptr && *rebuild == 0) return;   // Verlet skin: the keys are still valid
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c0 = blockIdx.x * cpc, c1 = min(c0 + cpc, ncells);
     // cells of at most 32 particles: one warp each
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     const int* __restrict__ jids = self ? S.pidj : S.jid;
     const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[t];
     const int dnshift = task_dnshift(tr);
-    const int dmaxdist = task_dmax(tr);
+    const int dmaxdist = task_dmax_skin(P, tr);
     const float cut2 = self ? P.cutoff2s : P.cutoff2;
     float4* myfj = S.fj + warp * cap;
     double epot = 0.0, vir = 0.0;

@@ -51,14 +51,18 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
                                                    const int* __restrict__ count, float4* __restrict__ xq_out,
                                                    float4* __restrict__ v_out, int* __restrict__ pid_out,
                                                    int* __restrict__ nstay, int* __restrict__ nmove,
-                                                   Mover* __restrict__ movers, unsigned long long* status) {
+                                                   Mover* __restrict__ movers, unsigned long long* status,
+                                                   const int* __restrict__ rebuild) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= RC.ncells || *(volatile unsigned long long*)status != 0) return;
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;
-    const float4 h = RC.cell_h[c];
+    // Verlet skin between rebuilds: nobody leaves (particles stay in their cells, in their
+    // slots, up to half the skin outside the cell), the block is copied in order.
+    const bool moving = rebuild == nullptr || *rebuild != 0;
+    const float4 h = moving ? RC.cell_h[c] : make_float4(INFINITY, INFINITY, INFINITY, 0.f);
     int stays = 0, moves = 0;
     // the next 32 particles are loaded while these are written (latency of one load, not of
     // one per 32 particles)
@@ -79,7 +83,8 @@ __global__ void __launch_bounds__(256) rebin_split(ResidentCells RC, const float
             vn = v[base + k + 32];
             idn = pid[base + k + 32];
         }
-        const int dx = (x.x >= h.x) - (x.x < 0.0f), dy = (x.y >= h.y) - (x.y < 0.0f), dz = (x.z >= h.z) - (x.z < 0.0f);
+        const int dx = moving ? (x.x >= h.x) - (x.x < 0.0f) : 0, dy = moving ? (x.y >= h.y) - (x.y < 0.0f) : 0,
+                  dz = moving ? (x.z >= h.z) - (x.z < 0.0f) : 0;
         const bool stay = active && dx == 0 && dy == 0 && dz == 0;
         const bool move = active && !stay;
         const unsigned bs = __ballot_sync(FULL, stay), bm = __ballot_sync(FULL, move);
@@ -196,6 +201,68 @@ __global__ void __launch_bounds__(256) slot_of_ids(ResidentCells RC, const int* 
     const int n = min(count[c], RC.capc);
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) slot_of[pid[base + k]] = (int)(base + k);
+}
+
+// ---------------------------------------------------------------- Verlet skin
+// engine_verlet_update (src/engine.c:193-315) for the resident steps: the particles are
+// re-binned and sorted only when the largest displacement since the last rebuild exceeds
+// half the skin (min h - cutoff) or a quarter of the cutoff; in between, each pair task's
+// projection bound carries the two cells' displacements.  Device words (vw): [0] rebuild
+// this step (1) or not (0), [1] largest displacement of the step (float bits, >= 0),
+// [2] rebuilds so far.
+
+// After re-binning: on a rebuild step, the positions the keys are made from become the
+// reference positions and the displacements restart from zero.
+__global__ void __launch_bounds__(256) verlet_mark(ResidentCells RC, const int* __restrict__ count,
+                                                  const float4* __restrict__ xq, float4* __restrict__ oldx,
+                                                  int* __restrict__ cell_mdx, const int* __restrict__ vw,
+                                                  const unsigned long long* __restrict__ status) {
+    if (*status != 0 || vw[0] == 0) return;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < (size_t)RC.ncells && s < (size_t)RC.ncells * RC.capc) cell_mdx[s] = 0;
+    if (s >= (size_t)RC.ncells * RC.capc) return;
+    const int c = (int)(s / (unsigned)RC.capc);
+    if ((int)(s - (size_t)c * RC.capc) < min(count[c], RC.capc)) oldx[s] = xq[s];
+}
+
+// After the step: each cell's largest displacement from the reference positions (one warp
+// per cell), in key units of its engine's sort scale for the next step's bounds, and the
+// largest of all.
+__global__ void __launch_bounds__(256) verlet_check(ResidentCells RC, const int* __restrict__ count,
+                                                   const float4* __restrict__ xq, const float4* __restrict__ oldx,
+                                                   const float2* __restrict__ cscale, int* __restrict__ cell_mdx,
+                                                   int* __restrict__ vw, const unsigned long long* __restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (c >= RC.ncells || *status != 0) return;
+    const int n = min(count[c], RC.capc);
+    const size_t base = (size_t)c * RC.capc;
+    float d2 = 0.f;
+    for (int k = lane; k < n; k += 32) {
+        const float4 x = xq[base + k], o = oldx[base + k];
+        const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
+        d2 = fmaxf(d2, dx * dx + dy * dy + dz * dz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    if (lane == 0) {
+        // rounded up, plus one unit for the floor of either key
+        const float md = sqrtf(d2) * 1.0001f;
+        cell_mdx[c] = (int)ceilf(cscale[c].x * md) + 1;
+        atomicMax(&vw[1], __float_as_int(md));
+    }
+}
+
+// The rebuild decision for the next step (src/engine.c:262): 2 maxdx > skin or
+// maxdx > cutoff / 4 (engine_maxdxratio, src/engine.h:83).
+__global__ void verlet_decide(int* __restrict__ vw, float skin, float cutoff,
+                              const unsigned long long* __restrict__ status) {
+    if (*status != 0) return;
+    const float md = __int_as_float(vw[1]);
+    const int rebuild = (2.0f * md > skin) || (md > 0.25f * cutoff);
+    vw[0] = rebuild;
+    vw[1] = 0;
+    if (rebuild) vw[2] += 1;
 }
 
 // Symplectic Euler update of every particle (engine_advance, src/engine.c:1975-1979), with

@@ -748,7 +748,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
         const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
         const int dnshift = task_dnshift(d.tr);
-        const int dmaxdist = task_dmax(d.tr);
+        const int dmaxdist = task_dmax_skin(P, d.tr);
         double e_task = 0.0, v_task = 0.0;
         const int nchunks = (ni + 31) >> 5;
         const int jd0 = self ? 0 : jlist_dist(W, nj, 0);
@@ -864,7 +864,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
         const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
         const int dnshift = task_dnshift(d.tr);
-        const int dmaxdist = task_dmax(d.tr);
+        const int dmaxdist = task_dmax_skin(P, d.tr);
         double e_task = 0.0, v_task = 0.0;
         const int nstrips = (ni + 7) >> 3;
         const int jd0 = self ? 0 : jlist_dist(W, nj, 0);

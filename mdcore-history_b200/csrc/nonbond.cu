@@ -84,6 +84,13 @@ struct NbState {
     int elog_cap = 0;
     unsigned long long* r_elog = nullptr;    // elog_cap x {step number, epot, ekin, 0}
     unsigned long long* r_eacc = nullptr;    // the step's kinetic-energy accumulator, step-number base
+    // Verlet skin of the resident steps (engine_flag_verlet): rebuild flag and counters,
+    // reference positions by slot, per-cell displacement in key units.
+    bool verlet = false;
+    float verlet_skin = 0.f;
+    int* r_vw = nullptr;
+    float4* r_oldx = nullptr;
+    int* r_cell_mdx = nullptr;
     int* d_order = nullptr;        // task queue order (scheduling order of all tasks)
     int* d_queue = nullptr;        // compacted queue of the current step
     int* d_qcount = nullptr;
@@ -331,7 +338,7 @@ int sort_cells_per_block(int slots, int ncells) { return slots <= 32 * (long lon
 // Launches sort_cells for cells of up to scap particles (its shared memory sized by scap).
 int launch_sort(const float4* xq, const int* cstart, const int* ccount, const unsigned* cmask, unsigned* keys,
                 const float2* cscale, int ncells, int cpc, int scap, unsigned long long* acc,
-                const unsigned long long* abort, bool capturing, cudaStream_t s) {
+                const unsigned long long* abort, bool capturing, cudaStream_t s, const int* rebuild = nullptr) {
     scap = std::max(4, std::min(kMaxPartsPerCell, (scap + 3) & ~3));
     const size_t smem = sort_smem_bytes(scap);
     // the largest size any launch asks for, so that launches captured into a graph later
@@ -340,7 +347,7 @@ int launch_sort(const float4* xq, const int* cstart, const int* ccount, const un
         CU(cudaFuncSetAttribute(sort_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sort_smem_bytes(kMaxPartsPerCell)));
     sort_cells<<<(ncells + cpc - 1) / cpc, kSortWarps * 32, smem, s>>>(xq, cstart, ccount, cmask, keys, cscale,
-                                                                       ncells, cpc, scap, acc, abort);
+                                                                       ncells, cpc, scap, acc, abort, rebuild);
     CU(cudaGetLastError());
     return 0;
 }
@@ -609,6 +616,8 @@ struct DevView {
     int cap4;                // largest cell (or cell capacity), rounded up to 4
     int cpc;                 // cells per sort block
     const unsigned long long* abort = nullptr;   // resident steps: the step's abort word
+    const int* rebuild = nullptr;                // Verlet skin: sort only when *rebuild
+    const int* cell_mdx = nullptr;               // Verlet skin: displacements in key units
 };
 
 DevView host_view(const NbState* st) {
@@ -644,7 +653,7 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
         return rc;
     }
     int rc0 = launch_sort(V.xq, V.cstart, V.ccount, st->d_cmask, V.keys, st->d_cscale, st->ncells, V.cpc, cap,
-                          st->d_acc, V.abort, st->capturing, st->stream);
+                          st->d_acc, V.abort, st->capturing, st->stream, V.rebuild);
     if (rc0 < 0) return rc0;
 
     Params P;
@@ -677,6 +686,7 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
     P.qid = st->d_qid;
     P.ep_pot = st->ep_pot;
     P.tab_global = st->tab_global;
+    P.cell_mdx = V.cell_mdx;
 
     const bool f32 = st->plain && st->fp32acc;
     if (f32) {
@@ -1375,6 +1385,13 @@ void res_free(NbState* st) {
         st->nbonds = st->nangles = st->ndihedrals = 0;
     }
     if (st->r_bsum) cudaFree(st->r_bsum);
+    cudaFree(st->r_vw);
+    cudaFree(st->r_oldx);
+    cudaFree(st->r_cell_mdx);
+    st->r_vw = nullptr;
+    st->r_oldx = nullptr;
+    st->r_cell_mdx = nullptr;
+    st->verlet = false;
     st->h_words = nullptr;
     st->r_bsum = nullptr;
     if (st->h_uppid) cudaFreeHost(st->h_uppid);
@@ -1630,6 +1647,21 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMallocHost(&st->h_rcount, sizeof(int) * (2 * nc + 2)));
     CU(cudaMalloc(&st->r_bsum, sizeof(int) * ((nc + kScanBlock - 1) / kScanBlock + 1)));
     CU(cudaMallocHost(&st->h_words, 4 * sizeof(unsigned long long)));
+    st->verlet = true;
+    for (struct engine* e : st->engines) st->verlet = st->verlet && (e->flags & engine_flag_verlet);
+    if (st->verlet) {
+        // skin = min h - cutoff (src/engine.c:211), the smallest over the engines
+        float skin = INFINITY;
+        for (struct engine* e : st->engines)
+            skin = std::min(skin, (float)(std::min(e->s.h[0], std::min(e->s.h[1], e->s.h[2])) - e->s.cutoff));
+        st->verlet_skin = skin;
+        CU(cudaMalloc(&st->r_vw, 4 * sizeof(int)));
+        CU(cudaMemset(st->r_vw, 0, 4 * sizeof(int)));
+        CU(cudaMalloc(&st->r_oldx, sizeof(float4) * slots));
+        CU(cudaMemset(st->r_oldx, 0, sizeof(float4) * slots));
+        CU(cudaMalloc(&st->r_cell_mdx, sizeof(int) * (nc + 1)));
+        CU(cudaMemset(st->r_cell_mdx, 0, sizeof(int) * (nc + 1)));
+    }
 
     std::vector<int> cstart(nc + 1), nbr(27 * (size_t)nc), cell_engine(nc);
     std::vector<float4> cell_h(nc);
@@ -1740,6 +1772,10 @@ int res_upload(NbState* st) {
     CU(cudaMemcpyAsync(st->r_doff, off, sizeof(int) * (nc + 1), cudaMemcpyHostToDevice, st->stream));
     CU(cudaMemsetAsync(st->r_status, 0, sizeof(unsigned long long), st->stream));
     CU(cudaMemsetAsync(st->r_done, 0, 2 * sizeof(unsigned long long), st->stream));
+    if (st->verlet) {                  // fresh positions: the first step re-bins and sorts
+        static const int first[2] = {1, 0};
+        CU(cudaMemcpyAsync(st->r_vw, first, sizeof(first), cudaMemcpyHostToDevice, st->stream));
+    }
     const ResidentCells RC = res_cells(st);
     place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid,
                                                                st->r_doff, st->r_cnt[0], st->r_xq[0], st->r_v[0],
@@ -1801,14 +1837,22 @@ int res_issue_step(NbState* st) {
     const int grid = res_grid(st);
     rebin_split<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_xq[r], st->r_v[r], st->r_pid[r], st->r_cnt[r], st->r_xq[o],
                                               st->r_v[o], st->r_pid[o], st->r_nstay, st->r_nmove, st->r_movers,
-                                              st->r_status);
+                                              st->r_status, st->verlet ? st->r_vw : nullptr);
     bool rigid = false;
     for (struct engine* e : st->engines) rigid = rigid || e->nr_rigids > 0;
     rebin_gather<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_movers, st->r_nstay, st->r_nmove, st->r_xq[o], st->r_v[o],
                                                st->r_pid[o], st->r_cnt[o], st->r_status,
                                                (rigid || res_bonded(st)) ? st->r_slot_of : nullptr);
     CU(cudaGetLastError());
+    const unsigned vblocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
+    if (st->verlet) {
+        verlet_mark<<<vblocks, 256, 0, st->stream>>>(RC, st->r_cnt[o], st->r_xq[o], st->r_oldx, st->r_cell_mdx,
+                                                     st->r_vw, st->r_status);
+        CU(cudaGetLastError());
+    }
     DevView V;
+    V.rebuild = st->verlet ? st->r_vw : nullptr;
+    V.cell_mdx = st->verlet ? st->r_cell_mdx : nullptr;
     V.xq = st->r_xq[o];
     V.pid = st->r_pid[o];
     V.keys = st->r_keys;
@@ -1890,6 +1934,13 @@ int res_issue_step(NbState* st) {
         rc = rigid_eval_resident(e, &view, st->stream);
         if (rc < 0) return rc;
     }
+    if (st->verlet) {                  // displacements and the next step's rebuild decision
+        verlet_check<<<grid, kCellThreads, 0, st->stream>>>(RC, st->r_cnt[o], st->r_xq[o], st->r_oldx, st->d_cscale,
+                                                            st->r_cell_mdx, st->r_vw, st->r_status);
+        verlet_decide<<<1, 1, 0, st->stream>>>(st->r_vw, st->verlet_skin, (float)st->engines[0]->s.cutoff,
+                                               st->r_status);
+        CU(cudaGetLastError());
+    }
     if (st->elog_cap > 0) {            // the step's energies into the log
         CU(cudaMemsetAsync(st->r_eacc, 0, sizeof(unsigned long long), st->stream));
         const unsigned slot_blocks = (unsigned)(((size_t)st->ncells * st->capc + 255) / 256);
@@ -1919,6 +1970,7 @@ long long res_key(const NbState* st) {
     k = k * 2 + st->fp32acc;
     k = k * 2 + (st->sd_gamma > 0.f);
     k = k * 2 + (st->elog_cap > 0);
+    k = k * 2 + st->verlet;
     return k;
 }
 
@@ -2289,6 +2341,21 @@ static int st_setlayout(NbState* st, int layout, int stages, int occupancy) {
 extern "C" int engine_cuda_setlayout(struct engine* e, int layout, int stages, int occupancy) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     return st_setlayout(state(e), layout, stages, occupancy);
+}
+
+// Rebuilds (re-binning + sort) of the resident steps since the last upload, with
+// engine_flag_verlet; -1 without the flag or resident particles.
+extern "C" int engine_cuda_verlet_rebuilds(struct engine* e, int* rebuilds) {
+    if (e == nullptr || e->cuda == nullptr || rebuilds == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    *rebuilds = -1;
+    if (!st->res_active || !st->verlet) return 0;
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    int w[4];
+    CU(cudaMemcpy(w, st->r_vw, sizeof(w), cudaMemcpyDeviceToHost));
+    *rebuilds = w[2];
+    return 0;
 }
 
 // FP32 force accumulation (fp32 = 1: the plain form adds each task's partial forces as

@@ -25,6 +25,8 @@ CLASS_WEIGHT = (0.50004, 0.16176, 0.036213)
 
 engine_flag_none = 0
 engine_flag_cuda = 4
+engine_flag_verlet = 16
+engine_flag_verlet_pseudo = 256
 engine_flag_unsorted = 512
 engine_flag_shake = 1024
 space_periodic_full = 7
@@ -166,6 +168,7 @@ def lib() -> C.CDLL:
         "engine_cuda_energylog_read": (C.c_int, [vp, dp, C.c_int]),
         "engine_cuda_setaccum": (C.c_int, [vp, C.c_int]),
         "engine_cuda_setspin": (C.c_int, [vp, C.c_int]),
+        "engine_cuda_verlet_rebuilds": (C.c_int, [vp, ip]),
         "engine_cuda_copytimeout_test": (C.c_int, [vp, C.c_int]),
         "engine_sched_record": (C.c_int, [vp, C.c_int]),
         "engine_sched_features": (C.c_int, [vp, P(C.c_float), C.c_int]),
@@ -408,6 +411,12 @@ class Engine:
         """Force accumulation of the plain form: FP32 float atomics (True) or fixed point."""
         _check(self.lib.engine_cuda_setaccum(self.ptr, int(fp32)), "engine_cuda_setaccum")
         return self
+
+    def verlet_rebuilds(self) -> int:
+        """Re-binning + sort steps of the resident steps since the upload (engine_flag_verlet)."""
+        r = C.c_int()
+        _check(self.lib.engine_cuda_verlet_rebuilds(self.ptr, C.byref(r)), "engine_cuda_verlet_rebuilds")
+        return r.value
 
     def set_spin(self, polls: int):
         """Polls per bounded wait of the sweeps on this engine's device (<= 0: default)."""
