@@ -891,9 +891,13 @@ def drift(args, local_rank):
 
 
 def sched_ab(args, local_rank):
-    """Makespan of the sweep with the count-product order, the learned order, a random order
-    and the cell-major order tasks are generated in (same workload, autotuned launch shape,
-    device-resident, CUDA events, L2 flushed before every step)."""
+    """The learned scheduler's protocol on one system (default: the slab): clock64 task
+    timings recorded over the first args.record device-resident MD steps, the cost network
+    trained on them (its own GPU kernels), then args.sched_steps MD steps from the same state
+    with each queue order -- the count-product heuristic (the default), the network's
+    longest-first order, both orders in locality tiles (cost classes, cell-major within a
+    class), and the cell-major order tasks are generated in -- and, for scale, the plain form.
+    Makespan = device time of the steps (CUDA events around the whole run) / steps."""
     import numpy as np
     import torch
     import mdcore_b200 as M
@@ -901,50 +905,78 @@ def sched_ab(args, local_rank):
     sysm = build_system(args.workload)
     if isinstance(sysm, list):
         raise SystemExit("bench.py: --sched-ab takes a single system (water, argon or slab)")
-    e = M.Engine.from_system(sysm, device=local_rank)
+    e = M.Engine.from_system(sysm, flags=args.engine_flags, device=local_rank)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     e.set_stream(stream.cuda_stream)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
         e.nonbond()
     e.load_parts()
     warps, layout, stages, occupancy, _ = e.autotune(reps=3)
+    e.graph(True)
+    e.resident_begin()
     t0 = time.time()
-    e.sched_record(args.record)
+    e.sched_record(args.record)                  # the first MD steps, timed per task
     X = e.sched_features()
     y = e.sched_targets()
+    t1 = time.time()
     loss = e.sched_train(epochs=args.epochs, batch=512, lr=3e-3, seed=1)
-    train_s = time.time() - t0
+    train_s = time.time() - t1
     pred = e.sched_predict()
-
-    def timed(order_name):
-        e.resident()
-        torch.cuda.synchronize()
-        sweeps = []
-        for _ in range(args.steps):
-            flush.zero_()
-            e.resident()
-            sweeps.append(e.kernel_times()[1])
-        return float(np.median(sweeps))
-
+    # every order starts from the state after the recorded steps (host copy, re-uploaded)
+    e.resident_sync()
+    ntasks = e.ntasks()
+    # every order computed now, from the state after the recorded steps
+    orders = []
+    for name, make in [("count_product", lambda: e.sched_apply(False)),
+                       ("learned", lambda: e.sched_apply(True)),
+                       ("learned_tiled", lambda: e.sched_order(1, 0)),
+                       ("count_product_tiled", lambda: e.sched_order(0, 0)),
+                       ("cell_major", lambda: e.set_order(np.arange(ntasks)))]:
+        make()
+        orders.append((name, e.get_order()))
     res = {}
+
+    def run(nsteps):
+        e.resident_begin()
+        e.resident_steps(3)                      # direct launch, capture, replay
+        p0 = e.resident_info().pairs
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        e.resident_steps(nsteps)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / nsteps
+        pairs = (e.resident_info().pairs - p0) / nsteps
+        if e.stats().status != 0:
+            raise SystemExit("bench.py: device status in the scheduled steps")
+        return {"ms_per_step": ms, "pairs_per_s": pairs / (ms * 1e-3)}
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    for name, order in orders:
+        e.set_order(order)
+        res[name] = run(args.sched_steps)
     e.sched_apply(False)
-    res["count_product"] = timed("heuristic")
-    e.sched_apply(True)
-    res["learned"] = timed("mlp")
-    e.set_order(np.random.default_rng(0).permutation(e.ntasks()))
-    res["random"] = timed("random")
-    e.set_order(np.arange(e.ntasks()))           # tasks as generated: cell-major (L2 locality)
-    res["cell_order"] = timed("cells")
     e.tune(0, plain=True)
-    res["plain_form"] = timed("plain")
+    res["plain_form"] = run(max(1, args.sched_steps // 10))
+    clk = clocks.stop()
+    e.resident_end()
     nz = y > 0
-    print(json.dumps({"sched_ab": WORKLOADS[args.workload][0], "sweep_ms_median": res, "tasks": e.ntasks(),
+    best = min((k for k in res if k != "plain_form"), key=lambda k: res[k]["ms_per_step"])
+    print(json.dumps({"sched_ab": WORKLOADS[args.workload][0], "tasks": ntasks,
+                      "protocol": {"record_md_steps": args.record, "scheduled_md_steps": args.sched_steps,
+                                   "plain_form_steps": max(1, args.sched_steps // 10),
+                                   "start": "every order from the state after the recorded steps"},
+                      "makespan": res, "fastest": best,
+                      "learned_vs_count_product": res["count_product"]["ms_per_step"] / res["learned_tiled"]["ms_per_step"],
+                      "learned_tiled_vs_cell_major": res["cell_major"]["ms_per_step"] / res["learned_tiled"]["ms_per_step"],
                       "launch": {"warps_per_block": warps, "lanes": "8i x 4j" if layout else "32i",
                                  "staging_buffers": stages, "threads_per_sm": occupancy},
-                      "record_steps": args.record, "epochs": args.epochs, "train_s": round(train_s, 3),
-                      "train_mse": loss, "corr_pred_target": float(np.corrcoef(pred[nz], y[nz])[0, 1])}))
+                      "epochs": args.epochs, "train_s": round(train_s, 3), "record_s": round(t1 - t0, 3),
+                      "train_mse": loss, "corr_pred_target": float(np.corrcoef(pred[nz], y[nz])[0, 1]),
+                      "clocks": clk}))
     e.close()
 
 
@@ -966,7 +998,8 @@ def main():
                          "instead of the autotuner")
     ap.add_argument("--sched-ab", action="store_true",
                     help="train the task-cost model and compare sweep makespans of the queue orders")
-    ap.add_argument("--record", type=int, default=4, help="--sched-ab: steps of task timings to train on")
+    ap.add_argument("--record", type=int, default=200, help="--sched-ab: MD steps of task timings to train on")
+    ap.add_argument("--sched-steps", type=int, default=5000, help="--sched-ab: MD steps timed per queue order")
     ap.add_argument("--epochs", type=int, default=150, help="--sched-ab: training epochs")
     ap.add_argument("--drift", action="store_true",
                     help="energy drift and force errors over an MD trajectory of --workload (default chains): "
@@ -983,6 +1016,8 @@ def main():
     if args.sub is None:
         args.sub = DEFAULT_SUB if args.workload == DEFAULT_WORKLOAD else ""
     if args.sched_ab:
+        if "--workload" not in sys.argv:
+            args.workload = "slab"
         sched_ab(args, int(os.environ.get("LOCAL_RANK", 0)))
         return
     if args.drift:

@@ -502,15 +502,24 @@ int nb_mlp_grad(const float *X, const float *target, const int *idx, int n, cons
 int nb_mlp_adam(float *w_master, void *w_bf16, const float *grad, float *m, float *v, float lr,
                 float beta1, float beta2, float eps, int step, void *stream);
 int nb_mlp_round(const float *w_master, void *w_bf16, void *stream);
-/* Engine-level use: record per-task durations over nsteps device-resident evaluations,
- * compute features, train, and apply an order (use_mlp = 0 restores the count-product
- * heuristic order). */
+/* Engine-level use: record per-task durations over nsteps device-resident MD steps (when
+ * engine_cuda_resident_begin holds the particles; the trajectory advances) or else nsteps
+ * force evaluations of the uploaded particles, compute features (of the last step's
+ * particles and keys), train, and apply an order (use_mlp = 0 restores the count-product
+ * heuristic order; 1 = longest predicted first).  engine_sched_order orders with locality:
+ * tiles of `tile` consecutive tasks of the cell-major task list (0: an automatic size of
+ * about an eighth of the tasks per worker warp) in decreasing class of their summed cost
+ * (source 0: count-product weights, 1: the network's predictions; a class per factor
+ * 2^(1/4)), tiles of one class in cell-major order, each tile's tasks longest first. */
 int engine_sched_record(struct engine *e, int nsteps);
 int engine_sched_features(struct engine *e, float *features_out, int n);
 int engine_sched_targets(struct engine *e, float *targets_out, int n);
 int engine_sched_train(struct engine *e, int epochs, int batch, float lr, unsigned seed, float *loss_out);
 int engine_sched_predict(struct engine *e, float *pred_out, int n);
 int engine_sched_apply(struct engine *e, int use_mlp);
+int engine_sched_order(struct engine *e, int source, int tile);
+/* The current queue order (n = the task count). */
+int engine_cuda_getorder(struct engine *e, int *order, int n);
 /* Sweep kernel launch parameters: warps per block (0 = default) and plain = 1 for the
  * plain form (one block per task, IEEE sqrt/div) instead of the persistent queue. */
 int engine_cuda_settune(struct engine *e, int warps, int plain);

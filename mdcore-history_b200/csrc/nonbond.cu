@@ -2895,6 +2895,17 @@ extern "C" int engine_cuda_setorder(struct engine* e, const int* order, int n) {
     return 0;
 }
 
+// The current queue order (task indices in scheduling order).
+extern "C" int engine_cuda_getorder(struct engine* e, int* order, int n) {
+    if (e == nullptr || e->cuda == nullptr || order == nullptr) return engine_err_null;
+    NbState* st = state(e);
+    if (n != st->ntasks) return engine_err_range;
+    CU(cudaSetDevice(st->device));
+    CU(cudaStreamSynchronize(st->stream));
+    CU(cudaMemcpy(order, st->d_order, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
 // Switches per-task clock64 recording on or off; reads the last launch's records
 // (start, end, SM of every task) when the output pointers are given.
 extern "C" int engine_cuda_taskclocks(struct engine* e, int enable, long long* clocks, int* sms, int n) {
@@ -3238,7 +3249,7 @@ extern "C" int engine_sched_record(struct engine* e, int nsteps) {
     CU(cudaSetDevice(st->device));
     SchedState* ss = sched(e, st);
     if (ss == nullptr) return engine_err_cuda;
-    if (!st->resident_valid) {
+    if (!st->resident_valid && !st->res_active) {
         int rc = engine_cuda_load_parts(e);
         if (rc < 0) return rc;
     }
@@ -3246,8 +3257,13 @@ extern "C" int engine_sched_record(struct engine* e, int nsteps) {
     st->record_clock = 1;
     for (int k = 0; k < nsteps; k++) {
         CU(cudaMemsetAsync(st->d_task_clock, 0, sizeof(long long) * 2 * st->ntasks, st->stream));
-        int rc = launch_kernels(st);
-        if (rc < 0) return rc;
+        // device-resident particles: one MD step each (the trajectory advances); else one
+        // force evaluation of the uploaded particles
+        int rc = st->res_active ? st_resident_steps(st, 1) : launch_kernels(st);
+        if (rc < 0) {
+            st->record_clock = prev;
+            return rc;
+        }
         accumulate_durations<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_task_clock, st->ntasks,
                                                                              ss->d_dur, ss->d_nrec);
         CU(cudaGetLastError());
@@ -3264,11 +3280,16 @@ extern "C" int engine_sched_features(struct engine* e, float* features_out, int 
     CU(cudaSetDevice(st->device));
     SchedState* ss = sched(e, st);
     if (ss == nullptr) return engine_err_cuda;
-    cell_type0<<<(st->ncells + 255) / 256, 256, 0, st->stream>>>(st->d_xq, st->d_cstart, st->d_ccount, st->ncells,
-                                                                 ss->d_ctype0);
-    task_features<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_tasks, st->ntasks, st->d_ccount,
-                                                                    st->d_cstart, st->d_keys, ss->d_ctype0,
-                                                                    1.0f / 32.0f, ss->d_feat);
+    // the particles and sort keys of the last evaluation: the resident cells' current side
+    // during device-resident steps, else the uploaded particles
+    const bool res = st->res_active;
+    const float4* xq = res ? st->r_xq[st->rside] : st->d_xq;
+    const int* cstart = res ? st->r_cstart : st->d_cstart;
+    const int* ccount = res ? st->r_cnt[st->rside] : st->d_ccount;
+    const unsigned* keys = res ? st->r_keys : st->d_keys;
+    cell_type0<<<(st->ncells + 255) / 256, 256, 0, st->stream>>>(xq, cstart, ccount, st->ncells, ss->d_ctype0);
+    task_features<<<(st->ntasks + 255) / 256, 256, 0, st->stream>>>(st->d_tasks, st->ntasks, ccount, cstart, keys,
+                                                                    ss->d_ctype0, 1.0f / 32.0f, ss->d_feat);
     CU(cudaGetLastError());
     if (features_out != nullptr) {
         if (n != st->ntasks) return engine_err_range;
@@ -3376,7 +3397,73 @@ extern "C" int engine_sched_predict(struct engine* e, float* pred_out, int n) {
     return 0;
 }
 
+namespace {
+
+// Task costs of the current configuration: predicted by the network (source 1) or the
+// reference's count-product weights (source 0, src/engine.c:574-576, 643-699).
+int task_costs(struct engine* e, NbState* st, int source, std::vector<float>& cost) {
+    cost.assign(st->ntasks, 0.f);
+    if (source == 1) return engine_sched_predict(e, cost.data(), st->ntasks);
+    std::vector<int> cnt(st->ncells);
+    if (st->res_active) {
+        CU(cudaStreamSynchronize(st->stream));
+        CU(cudaMemcpy(cnt.data(), st->r_cnt[st->rside], sizeof(int) * st->ncells, cudaMemcpyDeviceToHost));
+    } else {
+        for (size_t k = 0; k < st->engines.size(); k++)
+            for (int c = 0; c < st->engines[k]->s.nr_cells; c++)
+                cnt[st->cell_off[k] + c] = st->engines[k]->s.cells[c].count;
+    }
+    std::vector<TaskRec> tasks(st->ntasks);
+    CU(cudaMemcpy(tasks.data(), st->d_tasks, sizeof(TaskRec) * st->ntasks, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < st->ntasks; t++) cost[t] = (float)task_weight(tasks[t].sid, cnt[tasks[t].ci], cnt[tasks[t].cj]);
+    return 0;
+}
+
+}  // namespace
+
+// Orders the queue from task costs with locality: the tasks, in the cell-major order they
+// were generated in, are cut into tiles of `tile` consecutive tasks (0: about an eighth of
+// the tasks per worker warp of the persistent sweep, so that every warp still takes several
+// tiles); each tile's cost is the sum of its tasks' costs, and the tiles go in decreasing
+// cost class (a factor of 2^(1/4) per class) and, within a class, in cell-major order, each
+// tile's tasks by decreasing cost.  Longest-first at tile granularity, so that the queue
+// ends with cheap work, while neighbouring cells are swept close together in time and their
+// particles are read from L2 rather than DRAM.  tile = 1 is plain longest-first.
+extern "C" int engine_sched_order(struct engine* e, int source, int tile) {
+    if (e == nullptr || e->cuda == nullptr) return engine_err_null;
+    if ((source != 0 && source != 1) || tile < 0) return engine_err_range;
+    NbState* st = state(e);
+    CU(cudaSetDevice(st->device));
+    std::vector<float> cost;
+    int rc = task_costs(e, st, source, cost);
+    if (rc < 0) return rc;
+    const int n = st->ntasks;
+    if (tile == 0) {
+        const long long workers = (long long)st->sm_count * (st->occupancy / 32);
+        tile = (int)std::max(1LL, n / std::max(1LL, 8 * workers));
+    }
+    const int ntiles = (n + tile - 1) / tile;
+    std::vector<double> tcost(ntiles, 0.0);
+    for (int t = 0; t < n; t++) tcost[t / tile] += std::max(0.f, cost[t]);
+    std::vector<int> cls(ntiles);
+    for (int b = 0; b < ntiles; b++)
+        cls[b] = tcost[b] > 0.0 ? (int)std::floor(4.0 * std::log2(tcost[b])) : INT_MIN;
+    std::vector<int> tiles(ntiles);
+    for (int b = 0; b < ntiles; b++) tiles[b] = b;
+    std::stable_sort(tiles.begin(), tiles.end(), [&](int a, int b) { return cls[a] > cls[b]; });
+    std::vector<int> order;
+    order.reserve(n);
+    for (int b : tiles) {
+        const int t0 = b * tile, t1 = std::min(n, t0 + tile);
+        const size_t first = order.size();
+        for (int t = t0; t < t1; t++) order.push_back(t);
+        std::stable_sort(order.begin() + first, order.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    }
+    return engine_cuda_setorder(e, order.data(), n);
+}
+
 // Orders the queue by decreasing predicted cost (use_mlp) or restores the count-product
+// heuristic order.// Orders the queue by decreasing predicted cost (use_mlp) or restores the count-product
 // heuristic order.
 extern "C" int engine_sched_apply(struct engine* e, int use_mlp) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;

@@ -176,6 +176,8 @@ def lib() -> C.CDLL:
         "engine_sched_train": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_uint, P(C.c_float)]),
         "engine_sched_predict": (C.c_int, [vp, P(C.c_float), C.c_int]),
         "engine_sched_apply": (C.c_int, [vp, C.c_int]),
+        "engine_sched_order": (C.c_int, [vp, C.c_int, C.c_int]),
+        "engine_cuda_getorder": (C.c_int, [vp, ip, C.c_int]),
         "nb_mlp_predict": (C.c_int, [vp, C.c_int, vp, vp, vp]),
         "nb_mlp_grad": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
         "nb_mlp_adam": (C.c_int, [vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, vp]),
@@ -476,6 +478,10 @@ class Engine:
                "engine_sched_predict")
         return p
 
+    def sched_order(self, source: int, tile: int = 0):
+        """Cost-class tiles in cell-major order (source 0: count-product, 1: the network)."""
+        _check(self.lib.engine_sched_order(self.ptr, source, tile), "engine_sched_order")
+
     def sched_apply(self, use_mlp: bool):
         _check(self.lib.engine_sched_apply(self.ptr, int(use_mlp)), "engine_sched_apply")
 
@@ -507,6 +513,11 @@ class Engine:
 
     def ntasks(self) -> int:
         return _check(self.lib.engine_cuda_ntasks(self.ptr), "engine_cuda_ntasks")
+
+    def get_order(self) -> np.ndarray:
+        o = np.zeros(self.ntasks(), np.int32)
+        _check(self.lib.engine_cuda_getorder(self.ptr, _iptr(o), len(o)), "engine_cuda_getorder")
+        return o
 
     def set_order(self, order):
         o = np.ascontiguousarray(order, np.int32)

@@ -124,3 +124,41 @@ def test_learned_cost_beats_count_product_and_keeps_forces():
     e.nonbond()
     assert np.array_equal(e.forces(), f0)
     e.close()
+
+
+def test_learned_order_shortens_the_water_sweep():
+    """Full-size SPC/E water (10,206 tasks of ~135-particle cells, a few per worker warp,
+    their costs shaped by exclusions and type mix as well as by the counts): the network's
+    longest-first order sweeps faster than the count-product order.  Median sweep time of
+    21 device-resident evaluations per order, L2 flushed before each."""
+    torch = pytest.importorskip("torch")
+    sysm = W.water_spce(32)
+    e = M.Engine.from_system(sysm)
+    e.nonbond()
+    e.load_parts()
+    e.autotune(reps=3)
+    e.graph(True)
+    e.sched_record(4)
+    e.sched_features()
+    e.sched_targets()
+    e.sched_train(epochs=150, batch=512, lr=3e-3, seed=1)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def median_sweep():
+        for _ in range(3):                      # direct launch, capture, replay
+            e.resident()
+        ts = []
+        for _ in range(21):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e.resident()
+            ts.append(e.kernel_times()[1])
+        return float(np.median(ts))
+
+    e.sched_apply(False)
+    t_heur = median_sweep()
+    e.sched_apply(True)
+    t_mlp = median_sweep()
+    print(f"sweep: count-product {t_heur:.4f} ms, learned {t_mlp:.4f} ms")
+    assert t_mlp < t_heur, (t_mlp, t_heur)
+    e.close()
