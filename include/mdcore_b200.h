@@ -202,6 +202,10 @@ struct potential *potential_create_LJ126(double a, double b, double A, double B,
 struct potential *potential_create_LJ126_switch(double a, double b, double A, double B, double s, double tol);
 struct potential *potential_create_LJ126_Ewald(double a, double b, double A, double B, double q, double kappa, double tol);
 struct potential *potential_create_LJ126_Coulomb(double a, double b, double A, double B, double q, double tol);
+/* src/potential.c:651-676: the LJ term switched off between s and b, plus the Ewald
+ * real-space term. */
+struct potential *potential_create_LJ126_Ewald_switch(double a, double b, double A, double B, double q, double kappa,
+                                                      double s, double tol);
 struct potential *potential_create_Ewald(double a, double b, double q, double kappa, double tol);
 struct potential *potential_create_Coulomb(double a, double b, double q, double tol);
 /* src/potential.c:301-322: harmonic bond K (r - r0)^2 on [a, b]. */
@@ -357,6 +361,24 @@ int engine_unload(struct engine *e, double *x, double *v, int *type, int *pid, i
 /* src/engine_bonded.c:1400-1440 and :1301-1390 */
 int engine_exclusion_add(struct engine *e, int i, int j);
 int engine_exclusion_shrink(struct engine *e);
+/* Type lookups by name and by name2 (src/engine.c:1473-1530): the index of the first type
+ * with that name, engine_err_range when there is none. */
+int engine_gettype(struct engine *e, char *name);
+int engine_gettype2(struct engine *e, char *name2);
+/* Topology and parameter readers (src/engine_io.c): engine_read_psf adds the atoms of a
+ * PSF file (one type per atom type and charge, named type + charge string in name2), its
+ * bonds, angles, dihedrals and impropers (angles and dihedrals without a potential yet:
+ * pid -1, impropers -2), and places them at the positions of the PDB file's ATOM records
+ * (Angstrom, wrapped into the box); engine_read_cpf (CHARMM) and engine_read_xplor (XPLOR)
+ * read a parameter file and add the bond, angle, dihedral and improper potentials of the
+ * matching terms, rigid constraints for bonds over a type whose name starts with 'H'
+ * (rigidH), and a pair table for every type pair with parameters: kappa < 0 LJ (with the
+ * switch at switchlen for CHARMM), kappa = 0 LJ + shifted Coulomb, kappa > 0 LJ + Ewald
+ * real space (switched LJ for CHARMM).  Files are given as open descriptors and read to
+ * their end. */
+int engine_read_psf(struct engine *e, int psf, int pdb);
+int engine_read_cpf(struct engine *e, int cpf, double kappa, double tol, int rigidH, double switchlen);
+int engine_read_xplor(struct engine *e, int xplor, double kappa, double tol, int rigidH);
 /* src/engine_rigid.c:78-229 */
 int engine_rigid_add(struct engine *e, int pid, int pjd, double d);
 /* src/engine.c:1029-1053.  Sets the explicit electrostatic potential (engine_flag_explepot)

@@ -20,6 +20,11 @@ void nb_sweep_scales(const struct space *s, float *bias, float *dscale, int *dma
 int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dnshift, int *ci_out,
                   int *cj_out);
 
+/* Analytic 12-6 Lennard-Jones A/r^12 - B/r^6 and Ewald real-space erfc(kappa r)/r (with the
+ * 1/(4 pi) prefactor) values (potential.c). */
+double nb_lj126(double r, double A, double B);
+double nb_ewald(double r, double kappa);
+
 /* Device side (nonbond.cu, rigid.cu). */
 int nb_device_free(struct engine *e);
 int rigid_device_free(struct engine *e);

@@ -550,6 +550,26 @@ struct potential *potential_create_LJ126_switch(double a, double b, double A, do
     P.A = A; P.B = B; P.s = s; P.b = b;
     return create(f_ljsw, fp_ljsw, f6_ljsw, a, b, tol, potential_flag_LJ126);
 }
+/* LJ with the switch plus the Ewald real-space term: the switch acts on the LJ part only
+ * (src/potential.c:607-676). */
+static double f_ljewsw(double r) { return lj(r, P.A, P.B) * smooth_switch(r, P.s, P.b) + P.q * ewald(r, P.kappa); }
+static double fp_ljewsw(double r) {
+    return lj_p(r, P.A, P.B) * smooth_switch(r, P.s, P.b) + lj(r, P.A, P.B) * smooth_switch_p(r, P.s, P.b) +
+           P.q * ewald_p(r, P.kappa);
+}
+static double f6_ljewsw(double r) { return lj_6p(r, P.A, P.B) + P.q * ewald_6p(r, P.kappa); }
+
+struct potential *potential_create_LJ126_Ewald_switch(double a, double b, double A, double B, double q, double kappa,
+                                                      double s, double tol) {
+    P.A = A; P.B = B; P.q = q; P.kappa = kappa; P.s = s; P.b = b;
+    return create(f_ljewsw, fp_ljewsw, f6_ljewsw, a, b, tol, potential_flag_LJ126 | potential_flag_Ewald);
+}
+
+/* The analytic 12-6 Lennard-Jones and Ewald real-space values, for callers that bound a
+ * table's inner radius by the potential's size (the parameter-file readers). */
+double nb_lj126(double r, double A, double B) { return lj(r, A, B); }
+double nb_ewald(double r, double kappa) { return ewald(r, kappa); }
+
 static struct { double K, r0; } H;
 static double f_harm(double r) { return H.K * (r - H.r0) * (r - H.r0); }
 static double f6_harm(double r) {
