@@ -356,11 +356,11 @@ def cell_counts(sysm, e):
 
 def transfer_bytes(systems, engines):
     """Bytes copied per engine_step (device step with the host cells as input and output):
-    up, positions+types and velocities (32 B) and ids (4 B) per particle, counts and offsets
-    (8 B) per cell; down, the step's status and counters (24 B), counts (4 B) per cell,
-    positions, velocities and forces (48 B) and ids (4 B) per particle, offsets up (4 B per
-    cell), cell energies and virials (16 B per cell), the 64-byte accumulator block and the
-    constraint statistics (8 B per rigid engine).  Also the cell count and whether any cell
+    up, position+type and velocity+id (32 B) per particle, counts and offsets (8 B) per
+    cell; down, the step's status and counters (24 B), counts (4 B) per cell, position+upload
+    index (16 B), velocity and force (24 B) per particle, offsets up (4 B per cell), cell
+    energies and virials (16 B per cell), the 64-byte accumulator block and the constraint
+    statistics (8 B per rigid engine).  Also the cell count and whether any cell
     is empty (the queue-compaction launches run then)."""
     n = ncells = nrigid = 0
     empty = False
@@ -370,8 +370,8 @@ def transfer_bytes(systems, engines):
         ncells += len(c)
         empty = empty or bool((c == 0).any())
         nrigid += int(s.rigid is not None and len(s.rigid) > 0)
-    h2d = 36 * n + 8 * ncells + 4 + 4 * (ncells + 1)
-    d2h = 24 + 4 * ncells + 52 * n + 16 * ncells + 64 + 8 * nrigid
+    h2d = 32 * n + 8 * ncells + 4 + 4 * (ncells + 1)
+    d2h = 24 + 4 * ncells + 40 * n + 16 * ncells + 64 + 8 * nrigid
     return h2d, d2h, ncells, empty
 
 

@@ -671,8 +671,15 @@ int engine_batch_nonbond(struct engine_batch *b);
 /* engine_nonbond_cuda_fresh for every engine. */
 int engine_batch_nonbond_fresh(struct engine_batch *b);
 /* engine_step for every engine: one device step of the whole batch, the engines' host
- * cells as input and output. */
+ * cells as input and output.  Large batches step in groups of engines (contiguous runs of
+ * about equal particle counts, each with its own device blocks and stream) so that the
+ * host packing and unpacking of one group overlap the device work of the others; the
+ * result of every engine is the same as in one group. */
 int engine_batch_step(struct engine_batch *b);
+/* Groups of engine_batch_step: 0 = automatic (one per 2^18 particles, at most 4), else 1 to
+ * 64 (never more than the engines).  A batch holding resident particles
+ * (engine_batch_resident_begin) steps as one group. */
+int engine_batch_setgroups(struct engine_batch *b, int groups);
 /* engine_step_host for every engine with the forces of one batch evaluation. */
 int engine_batch_step_host(struct engine_batch *b);
 int engine_batch_load_parts(struct engine_batch *b);

@@ -159,10 +159,14 @@ struct NbState {
     unsigned* r_keys = nullptr;
     unsigned long long* r_force = nullptr;
     unsigned long long* r_status = nullptr;
-    float4* r_dense = nullptr;         // 3 per particle, cell order: position+type, velocity, force
-    float4* h_dense = nullptr;         // downloads (cached host memory)
-    float4* h_up = nullptr;            // uploads: positions, velocities
-    int *r_dpid = nullptr, *h_dpid = nullptr, *h_uppid = nullptr, *r_doff = nullptr, *h_rcount = nullptr;
+    // Dense copies of the particles in cell order, 3 float4 per particle of room.  Upload:
+    // position + type bits, velocity + global id bits (float4 each), and with explicit
+    // electrostatics the charges from float 10 np.  Download: position + upload-index bits
+    // (float4), then velocities and forces as float triples (40 bytes per particle).
+    float4* r_dense = nullptr;
+    float4* h_dense = nullptr;         // downloads (pinned)
+    float4* h_up = nullptr;            // uploads (pinned): positions, velocities
+    int *r_doff = nullptr, *h_rcount = nullptr;
     int* r_bsum = nullptr;                   // block sums of the count scan
     // Bonds of the resident steps (built with the device blocks).
     int nbonds = 0;
@@ -184,12 +188,14 @@ struct NbState {
     double2* r_bab = nullptr;                // per table: a, b
     unsigned long long* h_words = nullptr;   // status, completed steps, their pairs (pinned)
     std::vector<long long> res_engine_n;   // particles of each engine on the device
-    // What the device does not carry, by dense index of the last upload (cell order): the
-    // download returns each particle's upload index, so the host reads these (and the ids
-    // in h_uppid) nearly in order instead of scattering by particle id.
-    struct UpAux {
+    // What the device does not carry, and the global id, by dense index of the last upload
+    // (cell order): the download returns each particle's upload index, so the host reads
+    // these nearly in order instead of scattering by particle id.
+    struct alignas(16) UpAux {
+        int gid;
         float q;
         int vid;
+        short type;
         unsigned short flags;
     };
     std::vector<UpAux> up_aux;
@@ -198,6 +204,12 @@ struct NbState {
     cudaGraphExec_t rgraph_exec[2] = {nullptr, nullptr};
     long long rgraph_key[2] = {-1, -1}, rprepared[2] = {-1, -1};
     void* sched = nullptr;             // learned-scheduler state (SchedState)
+    // engine_step of a batch in groups of engines (engine_batch_setgroups): one device state
+    // and stream per group, so that the host packing and unpacking of one group overlap the
+    // uploads, steps and downloads of the others.  Built at the first grouped step.
+    int groups_req = 0;                // 0: automatic
+    std::vector<NbState*> groups;
+    int max_chunks = 8;                // pipeline chunks of one engine_step transfer
     std::vector<int> heur_order;       // count-product order built at load
 };
 
@@ -371,6 +383,9 @@ long long copy_chunk_parts() {
 }
 
 // Cells per host-thread range: about host_grain_parts() particles, at least 16 cells.
+// Cells per range of the host threads' passes over the cell records.
+constexpr int kCellPassGrain = 4096;
+
 int cell_grain(const NbState* st) {
     long long n = 0;
     for (const struct engine* e : st->engines) n += e->s.nr_parts;
@@ -784,20 +799,53 @@ int launch_kernels(NbState* st) {
 
 // Reads back the accumulators: per-engine energies and virials into each engine's stats
 // and cells, totals into st->bstats.
-int finish_stats(NbState* st) {
+// sums: each engine's fixed-point energy and virial sums when the caller has set the
+// cells' energies already (the resident download does it while rebuilding the cells), else
+// nullptr.
+int finish_stats(NbState* st, const std::vector<long long>* sums = nullptr) {
     const unsigned long long* a = st->h_acc;
     const unsigned long long* cvir = st->h_cell_epot + st->ncells;
-    long long etot = 0, vtot = 0;
-    for (size_t k = 0; k < st->engines.size(); k++) {
-        struct engine* e = st->engines[k];
-        struct space* s = &e->s;
-        long long esum = 0, vsum = 0;
-        for (int c = 0; c < s->nr_cells; c++) {
+    const size_t ne = st->engines.size();
+    // The cells' energies and each engine's fixed-point sums (host threads over ranges of
+    // engines, or of one engine's cells; integer sums, so the same in any order).
+    std::vector<long long> esums(ne, 0), vsums(ne, 0);
+    if (sums != nullptr) {
+        for (size_t k = 0; k < ne; k++) {
+            esums[k] = (*sums)[2 * k];
+            vsums[k] = (*sums)[2 * k + 1];
+        }
+    }
+    auto cell_range = [&](size_t k, int b, int e, long long& es, long long& vs) {
+        struct space* s = &st->engines[k]->s;
+        for (int c = b; c < e; c++) {
             const long long v = (long long)st->h_cell_epot[st->cell_off[k] + c];
-            esum += v;
-            vsum += (long long)cvir[st->cell_off[k] + c];
+            es += v;
+            vs += (long long)cvir[st->cell_off[k] + c];
             s->cells[c].epot = (double)v / kEnergyScale;
         }
+    };
+    if (sums != nullptr) {
+    } else if (ne > 1) {
+        HostPool::get().run((int)ne, std::max(1, kCellPassGrain * (int)ne / std::max(1, st->ncells)),
+                            [&](int, int b, int e) {
+                                for (int k = b; k < e; k++)
+                                    cell_range(k, 0, st->engines[k]->s.nr_cells, esums[k], vsums[k]);
+                            });
+    } else if (ne == 1) {
+        const int parts = HostPool::get().threads();
+        std::vector<long long> ep(parts, 0), vp(parts, 0);
+        HostPool::get().run(st->engines[0]->s.nr_cells, kCellPassGrain,
+                            [&](int part, int b, int e) { cell_range(0, b, e, ep[part], vp[part]); });
+        for (int q = 0; q < parts; q++) {
+            esums[0] += ep[q];
+            vsums[0] += vp[q];
+        }
+    }
+    long long etot = 0, vtot = 0;
+    for (size_t k = 0; k < ne; k++) {
+        struct engine* e = st->engines[k];
+        struct space* s = &e->s;
+        const long long esum = esums[k], vsum = vsums[k];
         etot += esum;
         vtot += vsum;
         e->stats.epot = (double)esum / kEnergyScale;
@@ -836,6 +884,8 @@ int refresh_charges(NbState* st);
 
 void state_free(NbState* st) {
     if (st == nullptr) return;
+    for (NbState* g : st->groups) state_free(g);
+    st->groups.clear();
     cudaSetDevice(st->device);
     drop_graph(st);
     res_free(st);
@@ -1355,10 +1405,9 @@ void res_free(NbState* st) {
     void* dev[] = {st->r_xq[0], st->r_xq[1], st->r_v[0], st->r_v[1], st->r_pid[0], st->r_pid[1], st->r_cnt[0],
                    st->r_cnt[1], st->r_done, st->r_cstart, st->r_nstay, st->r_nmove, st->r_slot_of, st->r_nbr, st->r_cell_engine,
                    st->r_cell_h, st->r_engine_dt, st->r_engine_imass, st->r_movers, st->r_keys, st->r_force,
-                   st->r_status, st->r_dense, st->r_dpid, st->r_doff, st->r_up_of};
+                   st->r_status, st->r_dense, st->r_doff, st->r_up_of};
     for (void* p : dev) cudaFree(p);
     if (st->h_dense) cudaFreeHost(st->h_dense);
-    if (st->h_dpid) cudaFreeHost(st->h_dpid);
     if (st->h_rcount) cudaFreeHost(st->h_rcount);
     if (st->h_up) cudaFreeHost(st->h_up);
     if (st->h_words) cudaFreeHost(st->h_words);
@@ -1394,8 +1443,7 @@ void res_free(NbState* st) {
     st->verlet = false;
     st->h_words = nullptr;
     st->r_bsum = nullptr;
-    if (st->h_uppid) cudaFreeHost(st->h_uppid);
-    st->r_dpid = st->h_dpid = st->h_uppid = st->r_doff = st->h_rcount = nullptr;
+    st->r_doff = st->h_rcount = nullptr;
     st->h_up = nullptr;
     st->r_xq[0] = st->r_xq[1] = nullptr;
     st->r_v[0] = st->r_v[1] = nullptr;
@@ -1416,11 +1464,11 @@ void res_free(NbState* st) {
     st->res_active = false;
 }
 
-// Places the dense upload (cell order, per-cell offsets) into the cells' blocks, records
-// each id's upload index (up_of) and, with explicit electrostatics, scatters the uploaded
-// charges by id (dq, qid; else nullptr).
+// Places the dense upload (cell order, per-cell offsets; the global id in the velocity's w)
+// into the cells' blocks, records each id's upload index (up_of) and, with explicit
+// electrostatics, scatters the uploaded charges by id (dq, qid; else nullptr).
 __global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float4* __restrict__ dxq,
-                                                   const float4* __restrict__ dv, const int* __restrict__ dpid,
+                                                   const float4* __restrict__ dv,
                                                    const int* __restrict__ doff, const int* __restrict__ count,
                                                    float4* __restrict__ xq, float4* __restrict__ v,
                                                    int* __restrict__ pid, int* __restrict__ up_of,
@@ -1432,9 +1480,10 @@ __global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float
     const size_t base = (size_t)c * RC.capc;
     for (int k = lane; k < n; k += 32) {
         const int o = doff[c] + k;
-        const int id = dpid[o];
+        const float4 vo = dv[o];
+        const int id = __float_as_int(vo.w);
         xq[base + k] = dxq[o];
-        v[base + k] = dv[o];
+        v[base + k] = make_float4(vo.x, vo.y, vo.z, 0.f);
         pid[base + k] = id;
         up_of[id] = o;
         if (qid != nullptr) qid[id] = dq[o];
@@ -1442,14 +1491,14 @@ __global__ void __launch_bounds__(256) place_cells(ResidentCells RC, const float
 }
 
 // Every particle in cell order for the host copy (cell c from offset doff[c]): positions
-// (w = type), velocities and the last evaluation's forces as three arrays of np entries,
-// and each particle's index in the last upload (through up_of, by id).
+// with the particle's index in the last upload (through up_of, by id) in w, then the
+// velocities and the last evaluation's forces as float triples.
 __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const float4* __restrict__ xq,
                                                      const float4* __restrict__ v, const int* __restrict__ pid,
                                                      const int* __restrict__ count, const int* __restrict__ doff,
                                                      const unsigned long long* __restrict__ force, size_t np,
-                                                     const int* __restrict__ up_of, float4* __restrict__ dense,
-                                                     int* __restrict__ dpid) {
+                                                     const int* __restrict__ up_of, float4* __restrict__ dx,
+                                                     float* __restrict__ dv3, float* __restrict__ df3) {
     const int lane = threadIdx.x & 31;
     const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= RC.ncells) return;
@@ -1458,13 +1507,14 @@ __global__ void __launch_bounds__(256) compact_cells(ResidentCells RC, const flo
     for (int k = lane; k < n; k += 32) {
         const size_t s = base + k, o = (size_t)doff[c] + k;
         if (o >= np) break;            // counts of an aborted step: nothing past the buffers
-        dense[o] = xq[s];
-        dense[np + o] = v[s];
-        dense[2 * np + o] =
-            make_float4((float)((double)(long long)force[3 * s] * (1.0 / (double)kForceScale)),
-                        (float)((double)(long long)force[3 * s + 1] * (1.0 / (double)kForceScale)),
-                        (float)((double)(long long)force[3 * s + 2] * (1.0 / (double)kForceScale)), 0.f);
-        dpid[o] = up_of[pid[s]];
+        const float4 x = xq[s], vs = v[s];
+        dx[o] = make_float4(x.x, x.y, x.z, __int_as_float(up_of[pid[s]]));
+        dv3[3 * o] = vs.x;
+        dv3[3 * o + 1] = vs.y;
+        dv3[3 * o + 2] = vs.z;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            df3[3 * o + a] = (float)((double)(long long)force[3 * s + a] * (1.0 / (double)kForceScale));
     }
 }
 
@@ -1588,16 +1638,31 @@ int res_build_bonds(NbState* st) {
     return 0;
 }
 
-// Largest cell of the engines' host cells and the particle count.
+// Largest cell of the engines' host cells and the particle count (host threads over
+// ranges of cells).
 int res_host_counts(const NbState* st, long long* n) {
-    int maxc = 0;
-    long long tot = 0;
-    for (int c = 0; c < st->ncells; c++) {
-        maxc = std::max(maxc, st->flat_cells[c]->count);
-        tot += st->flat_cells[c]->count;
+    const int parts = HostPool::get().threads();
+    std::vector<long long> tot(parts, 0);
+    std::vector<int> mx(parts, 0);
+    HostPool::get().run(st->ncells, kCellPassGrain, [&](int part, int b, int e) {
+        long long t = 0;
+        int m = 0;
+        for (int c = b; c < e; c++) {
+            const int k = st->flat_cells[c]->count;
+            t += k;
+            m = std::max(m, k);
+        }
+        tot[part] = t;
+        mx[part] = m;
+    });
+    long long t = 0;
+    int m = 0;
+    for (int k = 0; k < parts; k++) {
+        t += tot[k];
+        m = std::max(m, mx[k]);
     }
-    *n = tot;
-    return maxc;
+    *n = t;
+    return m;
 }
 
 // Device blocks of capc slots per cell for n particles, with the static cell data
@@ -1639,10 +1704,7 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMalloc(&st->r_status, sizeof(unsigned long long)));
     CU(cudaMalloc(&st->r_dense, sizeof(float4) * 3 * (size_t)(n + 1)));
     CU(cudaMallocHost(&st->h_dense, sizeof(float4) * 3 * (size_t)(n + 1)));
-    CU(cudaMalloc(&st->r_dpid, sizeof(int) * (size_t)(n + 1)));
-    CU(cudaMallocHost(&st->h_dpid, sizeof(int) * (size_t)(n + 1)));
     CU(cudaMallocHost(&st->h_up, sizeof(float4) * 2 * (size_t)(n + 1)));
-    CU(cudaMallocHost(&st->h_uppid, sizeof(int) * (size_t)(n + 1)));
     CU(cudaMalloc(&st->r_doff, sizeof(int) * (nc + 1)));
     CU(cudaMallocHost(&st->h_rcount, sizeof(int) * (2 * nc + 2)));
     CU(cudaMalloc(&st->r_bsum, sizeof(int) * ((nc + kScanBlock - 1) / kScanBlock + 1)));
@@ -1692,14 +1754,15 @@ int res_alloc(NbState* st, int capc, int mcap, long long n) {
     CU(cudaMemcpy(st->r_cell_h, cell_h.data(), sizeof(float4) * nc, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_dt, edt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(st->r_engine_imass, imass.data(), sizeof(double) * imass.size(), cudaMemcpyHostToDevice));
-    st->up_aux.assign((size_t)n + 1, NbState::UpAux{0.f, 0, 0});
+    st->up_aux.assign((size_t)n + 1, NbState::UpAux{0, 0.f, 0, 0, 0});
     st->res_active = true;
     return res_build_bonds(st);
 }
 
-// Pipeline chunks of an engine_step transfer of np particles, 1 to 8.
-int res_chunks(size_t np) {
-    return (int)std::max(1LL, std::min(8LL, (long long)np / copy_chunk_parts()));
+// Pipeline chunks of an engine_step transfer of np particles, 1 to st->max_chunks (8; fewer
+// for the groups of a grouped batch step, whose groups already overlap one another).
+int res_chunks(const NbState* st, size_t np) {
+    return (int)std::max(1LL, std::min((long long)st->max_chunks, (long long)np / copy_chunk_parts()));
 }
 
 // The engines' host cells into side 0 of the device blocks (the caller has checked that
@@ -1709,22 +1772,22 @@ int res_upload(NbState* st) {
     const int nc = st->ncells, ne = (int)st->engines.size();
     int* cnt = st->h_rcount;
     int* off = st->h_rcount + nc + 1;
+    HostPool::get().run(nc, kCellPassGrain, [&](int, int b, int e) {
+        for (int c = b; c < e; c++) cnt[c] = st->flat_cells[c]->count;
+    });
     off[0] = 0;
-    for (int c = 0; c < nc; c++) {
-        cnt[c] = st->flat_cells[c]->count;
-        off[c + 1] = off[c] + cnt[c];
-    }
+    for (int c = 0; c < nc; c++) off[c + 1] = off[c] + cnt[c];
     const size_t np = (size_t)st->res_nparts;
     float4* hx = st->h_up;
     float4* hv = st->h_up + np;
-    // charges for explicit electrostatics: through the force section of the download
-    // buffers, free until the download (scattered by id on the device, in place_cells)
-    float* hq = st->ep_pot >= 0 ? reinterpret_cast<float*>(st->h_dense + 2 * np) : nullptr;
-    float* dq = reinterpret_cast<float*>(st->r_dense + 2 * np);
+    // charges for explicit electrostatics: through the download buffers past the 10 np
+    // floats a download uses (scattered by id on the device, in place_cells)
+    float* hq = st->ep_pot >= 0 ? reinterpret_cast<float*>(st->h_dense) + 10 * np : nullptr;
+    float* dq = reinterpret_cast<float*>(st->r_dense) + 10 * np;
     const double t0 = now_ms();
     // Chunks of cells with about equal particle counts: each chunk's copies overlap the
     // packing of the next.
-    const int K = res_chunks(np);
+    const int K = res_chunks(st, np);
     std::vector<int> bounds(K + 1, nc);
     bounds[0] = 0;
     for (int k = 1; k < K; k++)
@@ -1745,9 +1808,8 @@ int res_upload(NbState* st) {
                 const int gid = st->id_off[k] + p->id;
                 const size_t o = (size_t)off[c] + q;
                 store_nt(hx + o, make_float4(p->x[0], p->x[1], p->x[2], bits_as_float((int)p->type)));
-                store_nt(hv + o, make_float4(p->v[0], p->v[1], p->v[2], 0.f));
-                store_nt(st->h_uppid + o, gid);
-                st->up_aux[o] = NbState::UpAux{p->q, p->vid, p->flags};
+                store_nt(hv + o, make_float4(p->v[0], p->v[1], p->v[2], bits_as_float(gid)));
+                st->up_aux[o] = NbState::UpAux{gid, p->q, p->vid, p->type, p->flags};
                 if (hq != nullptr) store_nt(hq + o, p->q);
             }
         }
@@ -1758,8 +1820,6 @@ int res_upload(NbState* st) {
         CU(cudaMemcpyAsync(st->r_dense + q0, hx + q0, sizeof(float4) * (q1 - q0), cudaMemcpyHostToDevice,
                            st->stream));
         CU(cudaMemcpyAsync(st->r_dense + np + q0, hv + q0, sizeof(float4) * (q1 - q0), cudaMemcpyHostToDevice,
-                           st->stream));
-        CU(cudaMemcpyAsync(st->r_dpid + q0, st->h_uppid + q0, sizeof(int) * (q1 - q0), cudaMemcpyHostToDevice,
                            st->stream));
         if (hq != nullptr)
             CU(cudaMemcpyAsync(dq + q0, hq + q0, sizeof(float) * (q1 - q0), cudaMemcpyHostToDevice, st->stream));
@@ -1777,7 +1837,7 @@ int res_upload(NbState* st) {
         CU(cudaMemcpyAsync(st->r_vw, first, sizeof(first), cudaMemcpyHostToDevice, st->stream));
     }
     const ResidentCells RC = res_cells(st);
-    place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np, st->r_dpid,
+    place_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_dense, st->r_dense + np,
                                                                st->r_doff, st->r_cnt[0], st->r_xq[0], st->r_v[0],
                                                                st->r_pid[0], st->r_up_of, dq,
                                                                hq != nullptr ? st->d_qid : nullptr);
@@ -2082,18 +2142,16 @@ int st_resident_steps(NbState* st, int nsteps) {
     return 0;
 }
 
-// Downloads the current side into the host cells.  On the device: cell offsets by a scan
-// of the counts, the particles compacted in cell order.  Down: the status and completed-
-// step words and the counts first, then the particles in chunks, each chunk's cells rebuilt
-// on the host threads while the next one copies, then energies, counters and constraint
-// statistics.  *status receives the abort word; when it is set nothing is rebuilt (the
-// host cells keep what they held).
-int res_download(NbState* st, unsigned long long* status) {
+// The download of the current side, queued on the state's stream: cell offsets by a scan
+// of the counts, the particles compacted in cell order; down: the status and completed-
+// step words and the counts first, then the particles in chunks with an event after each,
+// then energies, counters and constraint statistics.
+int res_download_issue(NbState* st) {
     const int nc = st->ncells, ne = (int)st->engines.size(), side = st->rside;
     const size_t np = (size_t)st->res_nparts;
     const ResidentCells RC = res_cells(st);
     const int nb = (nc + kScanBlock - 1) / kScanBlock;
-    const int K = res_chunks(np);
+    const int K = res_chunks(st, np);
     int rc = chunk_events(st, K + 1);
     if (rc < 0) return rc;
     if (nc > 0) {
@@ -2103,25 +2161,30 @@ int res_download(NbState* st, unsigned long long* status) {
         compact_cells<<<res_grid(st), kCellThreads, 0, st->stream>>>(RC, st->r_xq[side], st->r_v[side],
                                                                      st->r_pid[side], st->r_cnt[side], st->r_doff,
                                                                      st->r_force, np, st->r_up_of, st->r_dense,
-                                                                     st->r_dpid);
+                                                                     reinterpret_cast<float*>(st->r_dense + np),
+                                                                     reinterpret_cast<float*>(st->r_dense + np) + 3 * np);
         CU(cudaGetLastError());
     }
     CU(cudaMemcpyAsync(st->h_words, st->r_status, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st->stream));
     CU(cudaMemcpyAsync(st->h_words + 1, st->r_done, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        st->stream));
     CU(cudaMemcpyAsync(st->h_rcount, st->r_cnt[side], sizeof(int) * nc, cudaMemcpyDeviceToHost, st->stream));
-    CU(cudaEventRecord(st->chunk_ev[0], st->stream));
-    for (int k = 0; k < K; k++) {
-        const size_t q0 = np * k / K, q1 = np * (k + 1) / K;
-        for (int a = 0; a < 3; a++)
-            CU(cudaMemcpyAsync(st->h_dense + a * np + q0, st->r_dense + a * np + q0, sizeof(float4) * (q1 - q0),
-                               cudaMemcpyDeviceToHost, st->stream));
-        CU(cudaMemcpyAsync(st->h_dpid + q0, st->r_dpid + q0, sizeof(int) * (q1 - q0), cudaMemcpyDeviceToHost,
-                           st->stream));
-        CU(cudaEventRecord(st->chunk_ev[k + 1], st->stream));
-    }
+    // the cells' energies and virials ahead of the particles: the host sets each cell's
+    // energy while it rebuilds the cell
     CU(cudaMemcpyAsync(st->h_cell_epot, st->d_cell_epot, sizeof(unsigned long long) * 2 * st->ncells,
                        cudaMemcpyDeviceToHost, st->stream));
+    CU(cudaEventRecord(st->chunk_ev[0], st->stream));
+    const float* dv3 = reinterpret_cast<const float*>(st->r_dense + np);
+    float* hv3 = reinterpret_cast<float*>(st->h_dense + np);
+    for (int k = 0; k < K; k++) {
+        const size_t q0 = np * k / K, q1 = np * (k + 1) / K;
+        CU(cudaMemcpyAsync(st->h_dense + q0, st->r_dense + q0, sizeof(float4) * (q1 - q0), cudaMemcpyDeviceToHost,
+                           st->stream));
+        for (int a = 0; a < 2; a++)          // velocities, forces
+            CU(cudaMemcpyAsync(hv3 + 3 * (a * np + q0), dv3 + 3 * (a * np + q0), 3 * sizeof(float) * (q1 - q0),
+                               cudaMemcpyDeviceToHost, st->stream));
+        CU(cudaEventRecord(st->chunk_ev[k + 1], st->stream));
+    }
     CU(cudaMemcpyAsync(st->h_acc, st->d_acc, sizeof(unsigned long long) * kAccCount, cudaMemcpyDeviceToHost,
                        st->stream));
     if (res_bonded(st))
@@ -2129,7 +2192,16 @@ int res_download(NbState* st, unsigned long long* status) {
                            st->stream));
     for (struct engine* e : st->engines)
         if (e->nr_rigids > 0) rigid_resident_stats(e, st->stream, 0);
+    return 0;
+}
 
+// Waits for the download queued by res_download_issue and rebuilds the host cells from it,
+// chunk by chunk as the copies land; energies and statistics.  *status: the device status
+// word (nonzero: the step was aborted and the host cells are unchanged).
+int res_download_finish(NbState* st, unsigned long long* status) {
+    const int nc = st->ncells, ne = (int)st->engines.size();
+    const size_t np = (size_t)st->res_nparts;
+    const int K = res_chunks(st, np);
     CU(cudaEventSynchronize(st->chunk_ev[0]));
     *status = st->h_words[0];
     if (*status != 0) {
@@ -2153,14 +2225,24 @@ int res_download(NbState* st, unsigned long long* status) {
     std::atomic<int> fail(0);
     double t_rebuild = 0.0;
     int cdone = 0;
+    const float* hv3 = reinterpret_cast<const float*>(st->h_dense + np);
+    const float* hf3 = hv3 + 3 * np;
+    // Each cell's energy is set by the thread that rebuilds the cell; the engines' energy
+    // and virial sums per host thread (own 64-byte lines), summed afterwards (integers).
+    const unsigned long long* cep = st->h_cell_epot;
+    const unsigned long long* cvir = st->h_cell_epot + nc;
+    const int nparts = HostPool::get().threads();
+    const size_t stride = ((size_t)2 * ne + 7) & ~(size_t)7;
+    std::vector<long long> psum((size_t)nparts * stride, 0);
     for (int k = 0; k < K; k++) {
         const int pend = (int)(np * (k + 1) / K);
         const int cend = k == K - 1 ? nc : (int)(std::upper_bound(off + 1, off + nc + 1, pend) - (off + 1));
         CU(cudaEventSynchronize(st->chunk_ev[k + 1]));
         const double t0 = now_ms();
         const int c0 = cdone;
-        HostPool::get().run(cend - c0, cell_grain(st), [&](int, int rb, int re) {
+        HostPool::get().run(cend - c0, cell_grain(st), [&](int part, int rb, int re) {
             const int cb = c0 + rb, ce = c0 + re;
+            long long* my = psum.data() + (size_t)part * stride;
             for (int c = cb; c < ce; c++) {
                 if (c + 8 < ce) __builtin_prefetch(st->flat_cells[c + 8], 1);
                 if (c + 4 < ce) __builtin_prefetch(st->flat_cells[c + 4]->parts, 1);
@@ -2170,6 +2252,10 @@ int res_download(NbState* st, unsigned long long* status) {
                 struct space* sp = &st->engines[ke]->s;
                 struct cell* cl = st->flat_cells[c];
                 const int n = off[c + 1] - off[c];
+                const long long ev = (long long)cep[c];
+                my[2 * ke] += ev;
+                my[2 * ke + 1] += (long long)cvir[c];
+                cl->epot = (double)ev / kEnergyScale;
                 if (n > cl->size) {             // the old contents are replaced, not copied
                     const int nsize = std::max(n, std::max(2 * cl->size, 16));
                     struct part* fresh = nullptr;
@@ -2183,33 +2269,35 @@ int res_download(NbState* st, unsigned long long* status) {
                 }
                 for (int q = 0; q < n; q++) {
                     const size_t o = (size_t)off[c] + q;
-                    const float4 x = st->h_dense[o], v = st->h_dense[np + o], f = st->h_dense[2 * np + o];
-                    const int ou = st->h_dpid[o];           // the particle's upload index
+                    const float4 x = st->h_dense[o];
+                    int ou;                                  // the particle's upload index
+                    std::memcpy(&ou, &x.w, sizeof(int));
                     if (ou < 0 || (size_t)ou >= np) {
                         fail = 2;
                         return;
                     }
-                    const int gid = st->h_uppid[ou];
                     const NbState::UpAux& ax = st->up_aux[ou];
+                    const float* v = hv3 + 3 * o;
+                    const float* f = hf3 + 3 * o;
+                    struct part t;
+                    t.x[0] = x.x; t.x[1] = x.y; t.x[2] = x.z; t.x[3] = 0.f;
+                    t.v[0] = v[0]; t.v[1] = v[1]; t.v[2] = v[2]; t.v[3] = 0.f;
+                    t.f[0] = f[0]; t.f[1] = f[1]; t.f[2] = f[2]; t.f[3] = 0.f;
+                    t.q = ax.q;
+                    t.id = ax.gid - lo;
+                    t.vid = ax.vid;
+                    t.type = ax.type;
+                    t.flags = ax.flags;
                     struct part* p = &cl->parts[q];
-                    int type;
-                    std::memcpy(&type, &x.w, sizeof(int));
-                    p->x[0] = x.x; p->x[1] = x.y; p->x[2] = x.z; p->x[3] = 0.f;
-                    p->v[0] = v.x; p->v[1] = v.y; p->v[2] = v.z; p->v[3] = 0.f;
-                    p->f[0] = f.x; p->f[1] = f.y; p->f[2] = f.z; p->f[3] = 0.f;
-                    p->q = ax.q;
-                    p->id = gid - lo;
-                    p->vid = ax.vid;
-                    p->type = (short)type;
-                    p->flags = ax.flags;
-                    sp->partlist[p->id] = p;      // space_relink, inline
-                    sp->celllist[p->id] = cl;
+                    *p = t;
+                    sp->partlist[t.id] = p;      // space_relink, inline
+                    sp->celllist[t.id] = cl;
                 }
                 cl->count = n;
             }
             const size_t q0 = (size_t)off[cb], q1 = (size_t)off[ce];
-            for (int a = 0; a < 3; a++) evict_lines(st->h_dense + a * np + q0, sizeof(float4) * (q1 - q0));
-            evict_lines(st->h_dpid + q0, sizeof(int) * (q1 - q0));
+            evict_lines(st->h_dense + q0, sizeof(float4) * (q1 - q0));
+            for (int a = 0; a < 2; a++) evict_lines(hv3 + 3 * (a * np + q0), 3 * sizeof(float) * (q1 - q0));
         });
         t_rebuild += now_ms() - t0;
         cdone = cend;
@@ -2229,7 +2317,10 @@ int res_download(NbState* st, unsigned long long* status) {
         sp->epot = sp->epot_nonbond = sp->epot_bond = sp->epot_angle = sp->epot_dihedral = sp->epot_exclusion = 0.0;
     }
     st->res_dirty = false;
-    rc = finish_stats(st);
+    std::vector<long long> sums((size_t)2 * ne, 0);
+    for (int q = 0; q < nparts; q++)
+        for (int k = 0; k < 2 * ne; k++) sums[k] += psum[(size_t)q * stride + k];
+    const int rc = finish_stats(st, &sums);
     for (int k = 0; k < ne; k++) {
         struct space* sp = &st->engines[k]->s;
         if (res_bonded(st)) {
@@ -2240,6 +2331,15 @@ int res_download(NbState* st, unsigned long long* status) {
         sp->epot += sp->epot_nonbond + sp->epot_bond + sp->epot_angle + sp->epot_dihedral;
     }
     return rc;
+}
+
+// Downloads the current side into the host cells, each chunk's cells rebuilt on the host
+// threads while the next one copies.  *status receives the abort word; when it is set
+// nothing is rebuilt (the host cells keep what they held).
+int res_download(NbState* st, unsigned long long* status) {
+    const int rc = res_download_issue(st);
+    if (rc < 0) return rc;
+    return res_download_finish(st, status);
 }
 
 // Brings the engines' host cells up to date: positions, velocities and the last
@@ -2604,6 +2704,144 @@ int st_step_device(NbState* st) {
     return rc;
 }
 
+// ---- engine_step of a batch in groups of engines
+//
+// The host packs a group's cells and queues its upload, step and download on the group's
+// stream, then packs the next group while the device works; afterwards it rebuilds each
+// group's cells as its download lands, while the later groups' downloads still run.  Each
+// group is a batch of its own (own device blocks, graphs and stream), so the step is the
+// same per engine as in one batch.
+
+namespace {
+
+// Groups of a batch's engine_step: as requested, else one per 2^18 particles (at most 4);
+// never more than the engines.  A batch that holds resident particles steps as one group.
+int step_groups(const NbState* st) {
+    if (st->res_active) return 1;
+    long long n = 0;
+    for (const struct cell* c : st->flat_cells) n += c->count;
+    const long long k = st->groups_req > 0 ? st->groups_req : std::min(4LL, std::max(1LL, n >> 18));
+    return (int)std::max(1LL, std::min(k, (long long)st->engines.size()));
+}
+
+// The batch's launch shape and step options, for a group.
+void copy_shape(NbState* c, const NbState* st) {
+    c->warps = st->warps;
+    c->window = st->window;
+    c->layout = st->layout;
+    c->stages = st->stages;
+    c->occupancy = st->occupancy;
+    c->use_graph = st->use_graph;
+    c->plain = st->plain;
+    c->fp32acc = st->fp32acc;
+    c->sd_gamma = st->sd_gamma;
+    c->sd_dmax = st->sd_dmax;
+    c->max_chunks = std::max(1, 8 / (int)st->groups.size());
+}
+
+// (Re)builds k group states over contiguous runs of engines of about equal particle counts.
+int make_groups(NbState* st, int k) {
+    for (NbState* g : st->groups) state_free(g);
+    st->groups.clear();
+    const size_t ne = st->engines.size();
+    std::vector<long long> cum(ne + 1, 0);
+    for (size_t i = 0; i < ne; i++) {
+        long long n = 0;
+        const struct space* sp = &st->engines[i]->s;
+        for (int c = 0; c < sp->nr_cells; c++) n += sp->cells[c].count;
+        cum[i + 1] = cum[i] + n;
+    }
+    size_t e0 = 0;
+    for (int g = 0; g < k; g++) {
+        size_t e1 = ne;
+        if (g < k - 1) {
+            e1 = (size_t)(std::lower_bound(cum.begin(), cum.end(), cum[ne] * (g + 1) / k) - cum.begin());
+            e1 = std::min(std::max(e1, e0 + 1), ne - (size_t)(k - 1 - g));
+        }
+        NbState* c = new NbState();
+        c->engines.assign(st->engines.begin() + e0, st->engines.begin() + e1);
+        const int rc = load_state(c);
+        if (rc < 0) {
+            state_free(c);
+            return rc;
+        }
+        st->groups.push_back(c);
+        e0 = e1;
+    }
+    return 0;
+}
+
+int st_step_grouped(NbState* st, int k) {
+    CU(cudaSetDevice(st->device));
+    const double t0 = now_ms();
+    if ((int)st->groups.size() != k) {
+        const int rc = make_groups(st, k);
+        if (rc < 0) return rc;
+    }
+    CU(cudaStreamSynchronize(st->stream));       // work the caller queued on the batch's stream
+    double pack = 0.0, unpack = 0.0;
+    std::vector<char> begun(k, 0);
+    for (int g = 0; g < k; g++) {
+        NbState* c = st->groups[g];
+        copy_shape(c, st);
+        long long n = 0;
+        const int maxc = res_host_counts(c, &n);
+        if (!(c->res_active && n == c->res_nparts && maxc + 4 <= c->capc && c->bonds_key == res_bonds_key(c)))
+            continue;                            // new or outgrown blocks: stepped on their own below
+        int rc = res_upload(c);
+        if (rc < 0) return rc;
+        pack += c->bstats.ms_pack;
+        rc = res_issue_steps(c, 1);
+        if (rc < 0) return rc;
+        rc = res_download_issue(c);
+        if (rc < 0) return rc;
+        begun[g] = 1;
+    }
+    struct nb_stats tot = {};
+    for (int g = 0; g < k; g++) {
+        NbState* c = st->groups[g];
+        unsigned long long status = 1;
+        if (begun[g]) {
+            const int rc = res_download_finish(c, &status);
+            if (rc < 0) return rc;
+            unpack += c->bstats.ms_unpack;
+        }
+        if (status == 0) {
+            c->res_done = (long long)c->h_words[1];
+            c->res_pairs = (long long)c->h_words[2];
+        } else {
+            // aborted on the device (the host cells still hold the input), or not begun
+            if (begun[g])
+                for (struct engine* e : c->engines) e->time -= 1;
+            const int rc = st_step_device(c);
+            if (rc < 0) return rc;
+            pack += c->bstats.ms_pack;
+            unpack += c->bstats.ms_unpack;
+        }
+        tot.epot += c->bstats.epot;
+        tot.virial += c->bstats.virial;
+        tot.pairs += c->bstats.pairs;
+        tot.excluded += c->bstats.excluded;
+        tot.candidates += c->bstats.candidates;
+        tot.status |= c->bstats.status;
+    }
+    st->bstats.epot = tot.epot;
+    st->bstats.virial = tot.virial;
+    st->bstats.pairs = tot.pairs;
+    st->bstats.excluded = tot.excluded;
+    st->bstats.candidates = tot.candidates;
+    st->bstats.status = tot.status;
+    if (st->engines.size() > 1)                  // counts are kept for the batch only
+        for (struct engine* e : st->engines) e->stats.pairs = e->stats.excluded = e->stats.candidates = -1;
+    st->bstats.ms_pack = (float)pack;
+    st->bstats.ms_unpack = (float)unpack;
+    st->bstats.ms_device = (float)(now_ms() - t0 - pack - unpack);
+    share_times(st);
+    return 0;
+}
+
+}  // namespace
+
 extern "C" int engine_cuda_step(struct engine* e) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     return st_step_device(state(e));
@@ -2713,7 +2951,17 @@ extern "C" int engine_batch_nonbond_fresh(struct engine_batch* b) {
 // Euler update (engine_step for each engine, with the forces computed together).
 extern "C" int engine_batch_step(struct engine_batch* b) {
     if (b == nullptr) return engine_err_null;
-    return st_step_device(bstate(b));
+    NbState* st = bstate(b);
+    const int k = step_groups(st);
+    return k > 1 ? st_step_grouped(st, k) : st_step_device(st);
+}
+
+// Groups of engines that engine_batch_step pipelines (0: automatic).
+extern "C" int engine_batch_setgroups(struct engine_batch* b, int groups) {
+    if (b == nullptr) return engine_err_null;
+    if (groups < 0 || groups > 64) return engine_err_range;
+    bstate(b)->groups_req = groups;
+    return 0;
 }
 
 extern "C" int engine_batch_step_host(struct engine_batch* b) {

@@ -142,6 +142,7 @@ def lib() -> C.CDLL:
         "engine_batch_free": (C.c_int, [vp]),
         "engine_batch_nonbond": (C.c_int, [vp]),
         "engine_batch_step": (C.c_int, [vp]),
+        "engine_batch_setgroups": (C.c_int, [vp, C.c_int]),
         "engine_batch_load_parts": (C.c_int, [vp]),
         "engine_batch_resident": (C.c_int, [vp]),
         "engine_batch_unload_parts": (C.c_int, [vp]),
@@ -666,6 +667,11 @@ class Batch:
 
     def step(self):
         _check(self.lib.engine_batch_step(self.ptr), "engine_batch_step")
+        return self
+
+    def set_groups(self, groups: int):
+        """Groups of engines engine_batch_step pipelines (0: automatic)."""
+        _check(self.lib.engine_batch_setgroups(self.ptr, groups), "engine_batch_setgroups")
         return self
 
     def step_host(self):

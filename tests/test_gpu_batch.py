@@ -167,3 +167,69 @@ def test_batch_graph_and_autotune_keep_results():
     b.close()
     for e in engines:
         e.close()
+
+
+def _state(e):
+    x, v, f, c = e.parts()                 # by particle id
+    return x, v, f, c, e.energies()["total"]
+
+
+@pytest.mark.parametrize("groups", [2, 3, 64])
+def test_grouped_batch_steps_equal_one_group(groups):
+    """engine_batch_step in groups of engines (own device blocks and stream per group,
+    pipelined packing and unpacking): every engine's trajectory equals the one-group step
+    bit for bit -- positions, velocities, forces, cells and energy -- over argon replicas
+    and rigid-water replicas (P-SHAKE); more groups than engines means one per engine."""
+    def systems():
+        argon = W.argon_replicas(nrep=7, seed=11)
+        water = [W.with_rigid_water(W.water_spce(10, seed=k), 300.0, seed=k) for k in range(2)]
+        return argon, water
+
+    out = {}
+    for k in (1, groups):
+        runs = []
+        for sset in systems():
+            engines = engines_of(sset)
+            b = M.Batch(engines)
+            b.set_groups(k)
+            for _ in range(6):
+                b.step()
+                assert b.stats().status == 0
+            runs.append(([_state(e) for e in engines], b.stats()))
+            b.close()
+            for e in engines:
+                e.close()
+        out[k] = runs
+    for (s1, b1), (s2, b2) in zip(out[1], out[groups]):
+        assert (b1.pairs, b1.excluded) == (b2.pairs, b2.excluded)
+        assert b1.epot == b2.epot or abs(b1.epot - b2.epot) <= 1e-12 * abs(b1.epot)
+        for a, b in zip(s1, s2):
+            for u, w in zip(a[:4], b[:4]):
+                assert np.array_equal(u, w)
+            assert a[4] == b[4]
+
+
+def test_grouped_steps_then_resident_steps():
+    """A batch that stepped in groups still starts resident steps from the host cells, and
+    while it holds resident particles its engine_batch_step runs as one group."""
+    systems = W.argon_replicas(nrep=5, seed=13)
+    ref_engines = engines_of(systems)
+    ref = M.Batch(ref_engines)
+    ref.set_groups(1)
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    b.set_groups(3)
+    for bb in (ref, b):
+        for _ in range(3):
+            bb.step()
+        bb.resident_begin()
+        bb.resident_steps(4)
+        bb.resident_end()
+        bb.step()
+    for e1, e2 in zip(ref_engines, engines):
+        for u, w in zip(_state(e1)[:4], _state(e2)[:4]):
+            assert np.array_equal(u, w)
+    for bb in (ref, b):
+        bb.close()
+    for e in ref_engines + engines:
+        e.close()
