@@ -646,8 +646,9 @@ int engine_cuda_setaccum(struct engine *e, int fp32);
  * 2^22), after which the kernel records a copy timeout, waits once more for copies in
  * flight and returns; the evaluation then fails with engine_err_cuda and "Bulk copy into
  * shared memory timed out." in the error stack, and the device stays usable.
- * engine_cuda_copytimeout_test(e, 1) makes every such wait run out (the barriers are armed,
- * no copy is issued, so nothing is in flight), for testing that path; 0 turns it off.
+ * engine_cuda_copytimeout_test(e, 1) makes every such wait run out (nothing arrives on the
+ * barriers and no copy is issued, so nothing is in flight), for testing that path; 0 turns
+ * it off.
  * Both settings hold for every engine on the engine's device. */
 int engine_cuda_setspin(struct engine *e, int polls);
 /* With engine_flag_verlet: the rebuilds (re-binning and sort) the resident steps did since

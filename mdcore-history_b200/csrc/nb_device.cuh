@@ -23,9 +23,10 @@ constexpr double kEnergyScale = 4294967296.0;       // 2^32
 constexpr int kMaxPartsPerCell = 1024;
 constexpr int kSpinLimit = 1 << 22;                 // bounded waits: default polls per wait
 // Polls per bounded wait of the sweeps (engine_cuda_setspin; kSpinLimit by default), and a
-// test hook (engine_cuda_copytimeout_test): when set, the sweeps arm their mbarriers for
-// the staging copies but issue no copy, so every such wait runs out and reports
-// kStatusCopyTimeout with nothing left in flight.
+// test hook (engine_cuda_copytimeout_test): when set, the sweeps neither arrive on their
+// staging mbarriers nor issue a copy, so every such wait (a phase that nothing completes)
+// runs out and reports kStatusCopyTimeout with nothing in flight and no transaction
+// pending on any barrier.
 __constant__ int c_spin_limit = kSpinLimit;
 __constant__ int c_skip_copies = 0;
 

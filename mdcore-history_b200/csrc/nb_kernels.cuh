@@ -394,8 +394,8 @@ __global__ void __launch_bounds__(NW * 32) sweep_tasks(Params P, int cap) {
     __syncthreads();
     if (tid == 0) {
         const uint32_t bytes = self ? (uint32_t)padj * 20u : (uint32_t)(padi + padj) * 24u;
+        if (!c_skip_copies) {          // the test hook (no arrival, no copy) leaves the wait to run out
         mbar_arrive_expect_tx(S.bar, bytes);
-        if (!c_skip_copies) {          // the test hook leaves the wait to run out
         bulk_g2s(S.xj, P.xq + sj, padj * 16, S.bar);
         bulk_g2s(S.pidj, P.pid + sj, padj * 4, S.bar);
         if (!self) {

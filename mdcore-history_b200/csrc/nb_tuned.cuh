@@ -370,9 +370,11 @@ __device__ __forceinline__ void issue_copies(const Params& P, const TaskDesc& d,
     if (lane == 0) {
         const bool self = d.tr.sid < 0;
         const int padi = (d.ni + 3) & ~3, padj = (d.nj + 3) & ~3;
+        // test hook: no arrival and no copy, so the wait on W.bar runs out with no
+        // transaction pending on the barrier
+        if (c_skip_copies) return;
         fence_proxy_async();
         mbar_arrive_expect_tx(W.bar, self ? (uint32_t)padj * 20u : (uint32_t)padj * 24u + (uint32_t)padi * 4u);
-        if (c_skip_copies) return;     // test hook: the wait on W.bar runs out
         bulk_g2s(W.xraw, P.xq + d.sj, padj * 16, W.bar);
         bulk_g2s(W.pidraw, P.pid + d.sj, padj * 4, W.bar);
         if (!self) {

@@ -2472,10 +2472,10 @@ extern "C" int engine_cuda_setspin(struct engine* e, int polls) {
     return 0;
 }
 
-// Test hook of the failure path: with enable = 1 the sweeps on the engine's device arm
-// their mbarriers for the staging copies but issue none, so every wait runs out after the
-// spin limit, the evaluation fails with engine_err_cuda ("Bulk copy into shared memory
-// timed out.") and nothing is left in flight; 0 restores normal copies.
+// Test hook of the failure path: with enable = 1 the sweeps on the engine's device neither
+// arrive on their staging mbarriers nor issue a copy, so every wait runs out after the spin
+// limit, the evaluation fails with engine_err_cuda ("Bulk copy into shared memory timed
+// out.") and nothing is in flight; 0 restores normal copies.
 extern "C" int engine_cuda_copytimeout_test(struct engine* e, int enable) {
     if (e == nullptr || e->cuda == nullptr) return engine_err_null;
     if (enable != 0 && enable != 1) return engine_err_range;

@@ -1,6 +1,6 @@
 """The failure path of the device waits, exercised without a GPU fault: with a short spin
-limit and the copy-timeout test hook (the sweeps arm their mbarriers but issue no copy, so
-nothing is in flight), every wait on the staging copies runs out, the evaluation fails with
+limit and the copy-timeout test hook (the sweeps neither arrive on their mbarriers nor issue
+a copy, so nothing is in flight), every wait on the staging copies runs out, the evaluation fails with
 engine_err_cuda and the copy-timeout message, and the device stays usable: the next
 evaluation with copies restored matches the FP64 oracle."""
 import time
