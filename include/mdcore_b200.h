@@ -271,6 +271,15 @@ int space_init(struct space *s, const double *origin, const double *dim, double 
                double cutoff, unsigned int period);
 int space_getsid(struct space *s, struct cell **ci, struct cell **cj, float *shift);
 int space_addpart(struct space *s, struct part *p, double *x);
+/* src/space.c:307-364 (space_shuffle_local): every particle that left its cell moves to
+ * the cell it is now in (periodic wrap), partlist/celllist relinked (host threads). */
+int space_shuffle(struct space *s);
+/* src/space.c:186-219: swap/stall counters and energies reset, cell energies and particle
+ * forces zeroed. */
+int space_prepare(struct space *s);
+/* src/space.c:447-466: global position of particle id (cell origin + relative position);
+ * space_err_range for an id past nr_parts. */
+int space_getpos(struct space *s, int id, double *x);
 
 /* ---------------------------------------------------------------- exclusions, rigids
  * src/exclusion.h:34-41 and src/rigid.h:31-52. */

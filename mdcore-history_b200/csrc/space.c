@@ -396,3 +396,24 @@ int nb_task_shift(struct space *s, int t, float dscale, float shift[3], int *dns
     *cj_out = (int)(cj - s->cells);
     return sid;
 }
+
+/* src/space.c:186-219: a space made ready for one time step -- the swap and stall
+ * counters and the energies reset, every cell's energy and every particle's force zeroed
+ * (there are no task waits to re-arm: no CPU runners). */
+int space_prepare(struct space *s) {
+    if (s == NULL) return space_error(space_err_null);
+    s->nr_swaps = 0;
+    s->nr_stalls = 0;
+    s->epot = s->epot_nonbond = s->epot_bond = s->epot_angle = s->epot_dihedral = s->epot_exclusion = 0.0;
+    nb_zero_cells(s);
+    return space_err_ok;
+}
+
+/* src/space.c:447-466: the position of particle id (local id), its cell's origin plus the
+ * cell-relative position. */
+int space_getpos(struct space *s, int id, double *x) {
+    if (s == NULL || x == NULL) return space_error(space_err_null);
+    if (id < 0 || id >= s->nr_parts || s->partlist[id] == NULL) return space_error(space_err_range);
+    for (int k = 0; k < 3; k++) x[k] = (double)s->partlist[id]->x[k] + s->celllist[id]->origin[k];
+    return space_err_ok;
+}

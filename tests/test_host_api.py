@@ -63,6 +63,32 @@ def test_engine_cell_assignment_matches_reference(fname):
     e.close()
 
 
+def test_space_getpos_and_prepare():
+    """space_getpos (src/space.c:447-466): cell origin + relative position of a local id,
+    the same doubles engine_unload returns; space_err_range past nr_parts.  space_prepare
+    (src/space.c:186-219) zeroes the energies and forces."""
+    import ctypes as C
+    sysm, _ = load_golden("argon_1372.npz")
+    e = M.Engine.from_system(sysm, start=False)
+    lib = M.lib()
+    lib.space_getpos.restype = C.c_int
+    lib.space_getpos.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    lib.space_prepare.restype = C.c_int
+    lib.space_prepare.argtypes = [C.c_void_p]
+    sp = e.ptr.value + 8                       # struct engine: unsigned flags, then struct space
+    x, _, pid, _ = e.unload()
+    out = (C.c_double * 3)()
+    for row in range(0, sysm.n, 97):
+        assert lib.space_getpos(sp, int(pid[row]), out) == 0
+        assert list(out) == list(x[row])
+    assert lib.space_getpos(sp, sysm.n, out) < 0
+    M.lib().errs_clear()
+    assert lib.space_prepare(sp) == 0
+    assert not e.forces().any()
+    assert e.energies()["total"] == 0.0
+    e.close()
+
+
 def test_engine_refuses_unimplemented_flags():
     with pytest.raises(M.MdcoreError):
         M.Engine(np.zeros(3), np.full(3, 4.0), np.ones(3), 1.0, flags=16384)   # engine_flag_dpd
