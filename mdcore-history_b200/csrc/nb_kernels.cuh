@@ -75,31 +75,47 @@ __device__ __forceinline__ void sort_small_group(const float4* __restrict__ xq, 
     const int g = lane / G, idx = lane % G;
     const float4 x = idx < n ? xq[start + idx] : make_float4(0.f, 0.f, 0.f, 0.f);
     unsigned left = mask & 0x1fffu;
+    // Groups of 16 or 32 lanes sort two passes' directions at once: the two networks'
+    // shuffles are independent, so each one's latency passes behind the other's.
+    constexpr int P = G >= 16 ? 2 : 1;
     while (left) {
-        // this pass: the next D directions of the mask, the g-th of them for this group
-        int sid = -1;
+        // these passes: the next D directions of the mask each, the g-th of them for this group
+        int sid[P];
 #pragma unroll
-        for (int q = 0; q < D; ++q) {
-            if (left == 0) break;
-            const int b = __ffs(left) - 1;
-            left &= left - 1;
-            if (q == g) sid = b;
+        for (int p = 0; p < P; ++p) {
+            sid[p] = -1;
+#pragma unroll
+            for (int q = 0; q < D; ++q) {
+                if (left == 0) break;
+                const int b = __ffs(left) - 1;
+                left &= left - 1;
+                if (q == g) sid[p] = b;
+            }
         }
-        const int sa = sid < 0 ? 0 : sid;
-        const unsigned md = sort_dist(x, c_axes[sa][0], c_axes[sa][1], c_axes[sa][2], dscale, bias);
-        unsigned v = idx < n ? (md << SH) | (unsigned)(G - 1 - idx) : 0u;
+        unsigned v[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int sa = sid[p] < 0 ? 0 : sid[p];
+            const unsigned md = sort_dist(x, c_axes[sa][0], c_axes[sa][1], c_axes[sa][2], dscale, bias);
+            v[p] = idx < n ? (md << SH) | (unsigned)(G - 1 - idx) : 0u;
+        }
 #pragma unroll
         for (int k = 2; k <= G; k <<= 1) {
 #pragma unroll
             for (int j = k >> 1; j > 0; j >>= 1) {
-                const unsigned o = __shfl_xor_sync(FULL, v, j);
                 const bool keep_max = ((lane & j) == 0) == ((lane & k & (G - 1)) == 0);
-                v = keep_max ? max(v, o) : min(v, o);
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const unsigned o = __shfl_xor_sync(FULL, v[p], j);
+                    v[p] = keep_max ? max(v[p], o) : min(v[p], o);
+                }
             }
         }
-        if (sid >= 0 && idx < n)
-            keys[13 * (size_t)start + (size_t)sid * pad + idx] =
-                ((unsigned)(G - 1 - (int)(v & (G - 1))) << 16) | (v >> SH);
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+            if (sid[p] >= 0 && idx < n)
+                keys[13 * (size_t)start + (size_t)sid[p] * pad + idx] =
+                    ((unsigned)(G - 1 - (int)(v[p] & (G - 1))) << 16) | (v[p] >> SH);
     }
 }
 

@@ -343,8 +343,9 @@ double now_ms() {
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
-// Cells per sort block: 8 when cells hold 32 particle slots or fewer on average (one warp
-// sorts a small cell alone), else 1 (the block's warps share a large cell's directions).
+// Cells per sort block: kSortWarps (one per warp) when cells hold 32 particle slots or fewer
+// on average (one warp sorts a small cell alone), else 1 (the block's warps share a large
+// cell's directions).
 int sort_cells_per_block(int slots, int ncells) { return slots <= 32 * (long long)ncells ? kSortWarps : 1; }
 
 // Launches sort_cells for cells of up to scap particles (its shared memory sized by scap).
@@ -1922,7 +1923,7 @@ int res_issue_step(NbState* st) {
     V.abort = st->r_status;
     V.slots = (size_t)st->ncells * st->capc;
     V.cap4 = st->capc;
-    V.cpc = st->res_nparts <= 32LL * st->ncells ? 8 : 1;
+    V.cpc = st->res_nparts <= 32LL * st->ncells ? kSortWarps : 1;   // one warp per small cell
     rc = issue_kernels(st, V, false);
     if (rc < 0) return rc;
     if (res_bonded(st)) {              // the bonded forces join the sweep's before the update
