@@ -29,9 +29,10 @@ __constant__ float c_axes[13][3];
 // run):
 //  * a cell of at most 32 particles is sorted by one warp in registers, with bitonic
 //    networks of shuffles over groups of lanes (several directions at once when it holds
-//    16 particles or fewer);
-//  * a larger cell's positions are staged once in shared memory, and it is sorted by all
-//    warps of the block, one warp per direction, with a counting sort into 128 buckets
+//    16 particles or fewer); one of 33 to 64 particles by one warp with two values per lane;
+//  * a cell of more than 64 particles has its positions staged once in shared memory, and
+//    it is sorted by all warps of the block, one warp per direction, with a counting sort
+//    into 128 buckets
 //    that split the direction's own distance range [min, max] evenly (a few keys per
 //    bucket) and an exact rank inside the bucket: position = (keys in farther buckets) +
 //    (keys of the same bucket with a larger distance, or an equal distance and a smaller
@@ -129,7 +130,51 @@ __device__ __forceinline__ void sort_small_cell(const float4* __restrict__ xq, u
     else sort_small_group<32>(xq, keys, start, n, mask, dscale, bias, lane);
 }
 
-// The warp's share of the directions of a cell of more than 32 particles, whose positions
+// One warp, a cell of 33 to 64 particles: two particles per lane (slots lane and lane + 32)
+// and, per direction of the mask, a bitonic network over the 64 values (distance << 6) |
+// (63 - index), descending -- the same order as the small cells' (ties by ascending index);
+// slots past n carry 0, below every particle's value.  The stage that pairs slot i with
+// i + 32 compares the lane's two values in registers, every other stage shuffles both.
+__device__ __forceinline__ void sort_mid_cell(const float4* __restrict__ xq, unsigned* __restrict__ keys, int start,
+                                              int n, unsigned mask, float dscale, float bias, int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int pad = (n + 3) & ~3;
+    const bool has1 = lane + 32 < n;
+    const float4 x0 = xq[start + lane];
+    const float4 x1 = has1 ? xq[start + lane + 32] : make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned* out = keys + 13 * (size_t)start;
+    unsigned left = mask & 0x1fffu;
+    while (left) {
+        const int sid = __ffs(left) - 1;
+        left &= left - 1;
+        const float nx = c_axes[sid][0], ny = c_axes[sid][1], nz = c_axes[sid][2];
+        unsigned a = (sort_dist(x0, nx, ny, nz, dscale, bias) << 6) | (unsigned)(63 - lane);
+        unsigned b = has1 ? (sort_dist(x1, nx, ny, nz, dscale, bias) << 6) | (unsigned)(31 - lane) : 0u;
+#pragma unroll
+        for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                if (j == 32) {                     // k = 64: slot lane keeps the larger
+                    const unsigned hi = max(a, b), lo = min(a, b);
+                    a = hi;
+                    b = lo;
+                } else {
+                    const unsigned oa = __shfl_xor_sync(FULL, a, j), ob = __shfl_xor_sync(FULL, b, j);
+                    const bool lower = (lane & j) == 0;
+                    const bool ka = lower == ((lane & k & 63) == 0);
+                    const bool kb = lower == (((lane + 32) & k & 63) == 0);
+                    a = ka ? max(a, oa) : min(a, oa);
+                    b = kb ? max(b, ob) : min(b, ob);
+                }
+            }
+        }
+        unsigned* o = out + (size_t)sid * pad;
+        o[lane] = ((unsigned)(63 - (int)(a & 63)) << 16) | (a >> 6);
+        if (has1) o[lane + 32] = ((unsigned)(63 - (int)(b & 63)) << 16) | (b >> 6);
+    }
+}
+
+// The warp's share of the directions of a cell of more than 64 particles, whose positions
 // xs[0..n) are staged in shared memory.
 __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, unsigned* __restrict__ keys,
                                                 unsigned char* wp, int scap, int start, int n, unsigned mask,
@@ -215,17 +260,19 @@ __global__ void __launch_bounds__(kSortWarps * 32, 4) sort_cells(const float4* _
     if (rebuild != nullptr && *rebuild == 0) return;   // Verlet skin: the keys are still valid
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c0 = blockIdx.x * cpc, c1 = min(c0 + cpc, ncells);
-    // cells of at most 32 particles: one warp each
+    // cells of at most 64 particles: one warp each
     for (int c = c0 + warp; c < c1; c += kSortWarps) {
         const int n = ccount[c];
         if (n > 0 && n <= 32) sort_small_cell(xq, keys, cstart[c], n, cmask[c], cscale[c].x, cscale[c].y, lane);
+        else if (n > 32 && n <= 64 && n <= scap)
+            sort_mid_cell(xq, keys, cstart[c], n, cmask[c], cscale[c].x, cscale[c].y, lane);
     }
     // larger cells: positions staged once, then all warps, one direction each
     float4* xs = reinterpret_cast<float4*>(sort_smem);
     unsigned char* warea = sort_smem + sort_stage_bytes(scap) + (size_t)warp * sort_warp_bytes(scap);
     for (int c = c0; c < c1; ++c) {
         const int n = ccount[c];
-        if (n <= 32) continue;
+        if (n <= 64 && n <= scap) continue;
         if (n > scap) {
             if (threadIdx.x == 0) atomicOr(&acc[kAccStatus], (unsigned long long)kStatusCellOverflow);
             continue;

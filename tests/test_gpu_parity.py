@@ -100,10 +100,39 @@ def cells_of_every_size(ncmax=40, seed=11):
     return s
 
 
-def test_sort_keys_every_cell_size():
-    """Cells of 0..40 particles (every lane-group width of the in-register sort, 1 to 32, and
-    the shared-memory sort above 32), with tied distances: keys equal the oracle's."""
-    sysm = cells_of_every_size()
+def cells_of_every_size_2nm(ncmax=90, seed=13):
+    """5 x 5 x 5 cells of 2 nm (cutoff 1 nm); cell c holds c % (ncmax + 1) particles on a
+    jittered 0.4 nm grid (at least 0.3 nm apart), in pairs that share their x and y (equal
+    distances along some directions)."""
+    rng = np.random.default_rng(seed)
+    cd, h = 5, 2.0
+    xs = []
+    for c in range(cd ** 3):
+        n = c % (ncmax + 1)
+        corner = h * np.array([c // (cd * cd), (c // cd) % cd, c % cd], np.float64)
+        slots = [(col, zp) for col in range(25) for zp in ((0, 1), (2, 3))]
+        order = rng.permutation(len(slots))
+        p = []
+        for q in order[:(n + 1) // 2]:
+            col, zp = slots[q]
+            xy = 0.2 + 0.4 * np.array([col // 5, col % 5]) + rng.uniform(-0.05, 0.05, 2)
+            for z in zp:
+                p.append([xy[0], xy[1], 0.2 + 0.4 * z + rng.uniform(-0.05, 0.05)])
+        xs.append(corner + np.array(p[:n]).reshape(-1, 3))
+    x = np.concatenate(xs)
+    A, B = W.lj_AB(0.996, 0.3405)
+    return W.System(name="cell-sizes-2nm", origin=np.zeros(3), dim=np.full(3, cd * h), L=np.full(3, h),
+                    cutoff=1.0, masses=[39.948], charges=[0.0],
+                    pots=[W.PotSpec(W.KIND_LJ126, 0, 0, 0.25, 1.0, 1e-4, (A, B, 0.0, 0.0))],
+                    x=x, type=np.zeros(len(x), np.int32), excl=np.zeros((0, 2), np.int32))
+
+
+@pytest.mark.parametrize("make", [cells_of_every_size, cells_of_every_size_2nm], ids=["0-40", "0-90"])
+def test_sort_keys_every_cell_size(make):
+    """Cells of 0..40 and 0..90 particles (every lane-group width of the in-register sort, 1
+    to 32, the two-values-per-lane sort of 33 to 64 and the shared-memory sort above 64),
+    with tied distances: keys equal the oracle's."""
+    sysm = make()
     e, _, _ = evaluate(sysm)
     b = O.bin_system(sysm)
     ncells = int(np.prod(b["cdim"]))
