@@ -980,6 +980,34 @@ def sched_ab(args, local_rank):
     e.close()
 
 
+def profile_steps(args):
+    """--profile-steps K: the workload's device-resident steps alone (upload, K steps,
+    download), so that an ncu launch list or a capture of one kernel sees only the step's
+    kernels."""
+    import mdcore_b200 as M
+    built = build_system(args.workload)
+    systems = built if isinstance(built, list) else [built]
+    if isinstance(built, list):
+        engines = [M.Engine.from_system(s, flags=args.engine_flags, start=False) for s in systems]
+        tgt = M.Batch(engines, device=0)
+    else:
+        engines = [M.Engine.from_system(built, flags=args.engine_flags, device=0)]
+        tgt = engines[0]
+    warps, layout, stages, occupancy = (int(v) for v in ((args.launch or "8,1,1") + ",1024").split(",")[:4])
+    tgt.tune(warps)
+    tgt.set_layout(layout, stages, occupancy)
+    tgt.graph(True)
+    tgt.resident_begin()
+    tgt.resident_steps(args.profile_steps)
+    tgt.resident_sync()
+    status = tgt.stats().status
+    tgt.resident_end()
+    if status != 0:
+        raise SystemExit(f"bench.py: device status {status}")
+    print(json.dumps({"profile_steps": args.profile_steps, "workload": args.workload,
+                      "launch": [warps, layout, stages, occupancy], "status": status}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1007,6 +1035,9 @@ def main():
     ap.add_argument("--drift-steps", type=int, default=10000, help="--drift: MD steps")
     ap.add_argument("--min-steps", type=int, default=2000, help="--drift: steepest-descent steps first")
     ap.add_argument("--drift-dts", default="2,1,0.5", help="--drift: time steps (fs) of the fixed-point dt scan")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only K device-resident steps of --workload with the --launch shape (default "
+                         "8,1,1,1024), nothing timed: the command for ncu captures of the step's kernels")
     ap.add_argument("--verlet", action="store_true",
                     help="engine_flag_verlet_pseudo: the resident steps re-bin and sort only when the largest "
                          "displacement exceeds half the skin (min h - cutoff)")
@@ -1024,6 +1055,9 @@ def main():
         if "--workload" not in sys.argv:
             args.workload = "chains"
         drift(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
+    if args.profile_steps > 0:
+        profile_steps(args)
         return
     if args.warmup < 3:
         args.warmup = 3
