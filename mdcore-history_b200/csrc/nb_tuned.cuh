@@ -233,6 +233,7 @@ struct SharedTables {
     float* coef;
     int* potn;
     int* potidx;
+    float4 one;         // kTabOne: the one table's interval transform and offsets, in registers
 };
 
 // Table modes of the persistent sweeps: kTabShared (tables staged in shared memory, a lookup
@@ -244,6 +245,7 @@ constexpr int kTabShared = 0, kTabOne = 1, kTabGlobal = 2;
 template <int NW, int STAGES, int TAB>
 __device__ __forceinline__ SharedTables stage_tables(const Params& P, unsigned char* smem_raw, int cap) {
     SharedTables S;
+    S.one = TAB == kTabOne ? P.potinfo[0] : make_float4(0.f, 0.f, 0.f, 0.f);
     if (TAB == kTabGlobal) {
         S.potinfo = const_cast<float4*>(P.potinfo);
         S.coef = const_cast<float*>(P.coef);
@@ -599,7 +601,7 @@ __device__ __forceinline__ void pair_force(const Params& P, const SharedTables& 
                     f = fmaf(qq, fe, f);
                 }
             } else {
-                const float4 info = S.potinfo[pot];
+                const float4 info = TAB == kTabOne ? S.one : S.potinfo[pot];
                 eval_table_fast(S.coef, info, __float_as_int(info.w) >> 20, r, rinv, e, f);
             }
             wx = f * dx; wy = f * dy; wz = f * dz;
