@@ -247,7 +247,7 @@ __device__ __forceinline__ void sort_large_cell(const float4* __restrict__ xs, u
     }
 }
 
-__global__ void __launch_bounds__(kSortWarps * 32, 4) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
+__global__ void __launch_bounds__(kSortWarps * 32, 3) sort_cells(const float4* __restrict__ xq, const int* __restrict__ cstart,
                                                               const int* __restrict__ ccount,
                                                               const unsigned* __restrict__ cmask,
                                                               unsigned* __restrict__ keys,
