@@ -2291,8 +2291,10 @@ int res_download_finish(NbState* st, unsigned long long* status) {
                     t.flags = ax.flags;
                     struct part* p = &cl->parts[q];
                     *p = t;
-                    sp->partlist[t.id] = p;      // space_relink, inline
-                    sp->celllist[t.id] = cl;
+                    // space_relink, inline; most particles keep their slot from one step to
+                    // the next, and an unchanged entry is not written (no dirty line)
+                    if (sp->partlist[t.id] != p) sp->partlist[t.id] = p;
+                    if (sp->celllist[t.id] != cl) sp->celllist[t.id] = cl;
                 }
                 cl->count = n;
             }
