@@ -215,10 +215,11 @@ def test_bonded_resident_steps_equal_engine_step():
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
 
 
-def test_bonded_batch_equals_single_engines():
-    """Three bonded-chain systems stepped as one batch (engine_batch_step) and each alone
-    (engine_step): the same positions and energies bit for bit (the angle and dihedral
-    records carry their engine)."""
+@pytest.mark.parametrize("groups", [1, 3])
+def test_bonded_batch_equals_single_engines(groups):
+    """Three bonded-chain systems stepped as one batch (engine_batch_step, in one group or
+    one group per engine) and each alone (engine_step): the same positions and energies bit
+    for bit (the angle and dihedral records carry their engine)."""
     systems = [W.bonded_chains(nchains=4, seed=s) for s in (3, 4, 5)]
     for k, s in enumerate(systems):
         s.v = W.maxwell_velocities(s, 300.0, seed=10 + k)
@@ -232,6 +233,7 @@ def test_bonded_batch_equals_single_engines():
         e.close()
     engines = [M.Engine.from_system(s, start=False) for s in systems]
     b = M.Batch(engines)
+    b.set_groups(groups)                 # 3: one group per engine (own device blocks and stream)
     for _ in range(4):
         b.step()
         assert b.stats().status == 0
