@@ -2784,7 +2784,10 @@ int st_step_grouped(NbState* st, int k) {
     CU(cudaStreamSynchronize(st->stream));       // work the caller queued on the batch's stream
     double pack = 0.0, unpack = 0.0;
     std::vector<char> begun(k, 0);
-    for (int g = 0; g < k; g++) {
+    // On an error the groups already queued are still finished (their host cells rebuilt),
+    // no further group is started, and the first error is returned.
+    int err = 0;
+    for (int g = 0; g < k && err == 0; g++) {
         NbState* c = st->groups[g];
         copy_shape(c, st);
         long long n = 0;
@@ -2792,12 +2795,16 @@ int st_step_grouped(NbState* st, int k) {
         if (!(c->res_active && n == c->res_nparts && maxc + 4 <= c->capc && c->bonds_key == res_bonds_key(c)))
             continue;                            // new or outgrown blocks: stepped on their own below
         int rc = res_upload(c);
-        if (rc < 0) return rc;
-        pack += c->bstats.ms_pack;
-        rc = res_issue_steps(c, 1);
-        if (rc < 0) return rc;
-        rc = res_download_issue(c);
-        if (rc < 0) return rc;
+        if (rc == 0) {
+            pack += c->bstats.ms_pack;
+            rc = res_issue_steps(c, 1);
+        }
+        if (rc == 0) rc = res_download_issue(c);
+        if (rc < 0) {
+            CU(cudaStreamSynchronize(c->stream));
+            err = rc;
+            break;
+        }
         begun[g] = 1;
     }
     struct nb_stats tot = {};
@@ -2806,9 +2813,13 @@ int st_step_grouped(NbState* st, int k) {
         unsigned long long status = 1;
         if (begun[g]) {
             const int rc = res_download_finish(c, &status);
-            if (rc < 0) return rc;
             unpack += c->bstats.ms_unpack;
+            if (rc < 0) {
+                if (err == 0) err = rc;
+                continue;
+            }
         }
+        if (err != 0) continue;
         if (status == 0) {
             c->res_done = (long long)c->h_words[1];
             c->res_pairs = (long long)c->h_words[2];
@@ -2817,7 +2828,10 @@ int st_step_grouped(NbState* st, int k) {
             if (begun[g])
                 for (struct engine* e : c->engines) e->time -= 1;
             const int rc = st_step_device(c);
-            if (rc < 0) return rc;
+            if (rc < 0) {
+                err = rc;
+                continue;
+            }
             pack += c->bstats.ms_pack;
             unpack += c->bstats.ms_unpack;
         }
@@ -2828,6 +2842,7 @@ int st_step_grouped(NbState* st, int k) {
         tot.candidates += c->bstats.candidates;
         tot.status |= c->bstats.status;
     }
+    if (err != 0) return err;
     st->bstats.epot = tot.epot;
     st->bstats.virial = tot.virial;
     st->bstats.pairs = tot.pairs;
