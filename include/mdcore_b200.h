@@ -264,6 +264,10 @@ struct space {
     /* Queue statistics of the reference's CPU runners (src/space.h:118, reset per step by
      * space_prepare): there are no CPU runner queues here, so both stay 0. */
     int nr_swaps, nr_stalls;
+    /* src/space.h:92-93: the real, ghost and marked cells by index.  There are no ghost
+     * cells here (one process holds the whole space): every cell is real and marked. */
+    int *cid_real, *cid_ghost, *cid_marked;
+    int nr_real, nr_ghost, nr_marked;
 };
 
 /* src/space.c:530-783 and src/space.c:80-114. */
@@ -319,6 +323,32 @@ struct nb_stats {
     float ms_unpack;        /* host: adding the forces into the cells */
 };
 
+/* src/engine.h:92-112: the phases engine_step times, in CPU ticks (cycle.h getticks).
+ * Here: step = the whole engine_step; cuda_load / cuda_dopairs / cuda_unload = packing and
+ * upload, the device step with its copies, rebuilding the cells; nonbond, advance and rigid
+ * are parts of the device step and stay 0; the others belong to paths not built here. */
+enum {
+    engine_timer_step = 0,
+    engine_timer_prepare,
+    engine_timer_verlet,
+    engine_timer_exchange1,
+    engine_timer_nonbond,
+    engine_timer_bonded,
+    engine_timer_bonded_sort,
+    engine_timer_bonds,
+    engine_timer_angles,
+    engine_timer_dihedrals,
+    engine_timer_exclusions,
+    engine_timer_advance,
+    engine_timer_rigid,
+    engine_timer_exchange2,
+    engine_timer_shuffle,
+    engine_timer_cuda_load,
+    engine_timer_cuda_unload,
+    engine_timer_cuda_dopairs,
+    engine_timer_last
+};
+
 struct engine {
     unsigned int flags;
     struct space s;
@@ -352,6 +382,7 @@ struct engine {
     struct dihedral *dihedrals;      /* engine_dihedral_add */
     int nr_dihedrals, dihedrals_size, nr_dihedralpots, dihedralpots_size;
     struct potential **p_dihedral;   /* dihedral potentials by index (engine_dihedral_addpot) */
+    unsigned long long timers[engine_timer_last];   /* src/engine.h:293, CPU ticks per phase */
 };
 
 /* src/engine.c:2439-2591 */
@@ -445,6 +476,8 @@ int engine_cuda_step(struct engine *e);
 int engine_advance(struct engine *e);
 /* src/engine.c:2338-2430 */
 int engine_finalize(struct engine *e);
+/* src/engine.c:167-183: all of e->timers back to 0. */
+int engine_timers_reset(struct engine *e);
 
 /* ---------------------------------------------------------------- GPU entry points
  * The two functions src/engine.c calls when engine_flag_cuda is set, plus the device
@@ -570,6 +603,12 @@ int engine_cuda_ntasks(struct engine *e);
  * for P-SHAKE the constraint forces) of the cells are corrected as in the reference.  The
  * P-SHAKE matrices live on the device once the first evaluation has uploaded them. */
 int engine_rigid_eval(struct engine *e);
+/* src/engine_rigid.c:266-345: splits the groups for MPI ranks; a single process holds all
+ * of them, so it only checks its argument. */
+int engine_rigid_sort(struct engine *e);
+/* src/engine_rigid.c:231-250: the groups in a random order (rand()); the device copy is
+ * rebuilt at the next step and the results do not depend on the order. */
+int engine_rigid_unsort(struct engine *e);
 /* Largest iteration count of any group in the last engine_rigid_eval and the number of
  * groups that did not converge within rigid_maxiter iterations. */
 int engine_rigid_stats(struct engine *e, int *max_iter, int *unconverged);

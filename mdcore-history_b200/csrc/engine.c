@@ -7,8 +7,10 @@
 #include <stdlib.h>
 #include <string.h>
 #include <math.h>
+#include <time.h>
 #include "mdcore_b200.h"
 #include "internal.h"
+#include "cycle.h"
 
 int engine_err = engine_err_ok;
 
@@ -397,7 +399,59 @@ int engine_advance(struct engine *e) {
  * (engine_cuda_step).  The same trajectory as engine_step_host, bit for bit. */
 int engine_step(struct engine *e) {
     if (e == NULL) return engine_error(engine_err_null);
+    struct timespec w0, w1;
+    clock_gettime(CLOCK_MONOTONIC, &w0);
+    const ticks tic = getticks();
     if (engine_cuda_step(e) < 0) return engine_error(engine_err_cuda);
+    const ticks toc = getticks();
+    clock_gettime(CLOCK_MONOTONIC, &w1);
+    /* the step's phases (host milliseconds) in ticks at the rate this step ran */
+    const double ms = (w1.tv_sec - w0.tv_sec) * 1e3 + (w1.tv_nsec - w0.tv_nsec) * 1e-6;
+    e->timers[engine_timer_step] += toc - tic;
+    if (ms > 0.0) {
+        const double tpms = (double)(toc - tic) / ms;
+        e->timers[engine_timer_cuda_load] += (ticks)(e->stats.ms_pack * tpms);
+        e->timers[engine_timer_cuda_dopairs] += (ticks)(e->stats.ms_device * tpms);
+        e->timers[engine_timer_cuda_unload] += (ticks)(e->stats.ms_unpack * tpms);
+    }
+    return engine_err_ok;
+}
+
+/* src/engine.c:167-183: every timer back to 0. */
+int engine_timers_reset(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    for (int k = 0; k < engine_timer_last; k++) e->timers[k] = 0;
+    return engine_err_ok;
+}
+
+/* src/engine_rigid.c:266-345 splits the rigid groups into local, semi-local and remote
+ * ones for the MPI ranks; one process holds every group here, so there is nothing to
+ * split. */
+int engine_rigid_sort(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    return engine_err_ok;
+}
+
+/* src/engine_rigid.c:231-250: the rigid groups in a random order (rand(): each group
+ * swapped with a random one); part2rigid follows, and the device copy of the groups is
+ * rebuilt at the next step.  The constraints' results do not depend on the order. */
+int engine_rigid_unsort(struct engine *e) {
+    if (e == NULL) return engine_error(engine_err_null);
+    const int n = e->nr_rigids;
+    if (n < 2) return engine_err_ok;
+    const double scale = (double)n / RAND_MAX;
+    for (int k = 0; k < n; k++) {
+        int j = (int)(rand() * scale);
+        if (j >= n) j = n - 1;
+        if (j != k) {
+            const struct rigid t = e->rigids[j];
+            e->rigids[j] = e->rigids[k];
+            e->rigids[k] = t;
+        }
+    }
+    for (int g = 0; g < n; g++)
+        for (int k = 0; k < e->rigids[g].nr_parts; k++) e->part2rigid[e->rigids[g].parts[k]] = g;
+    e->rigids_gen++;
     return engine_err_ok;
 }
 
@@ -425,6 +479,7 @@ int engine_finalize(struct engine *e) {
     rigid_device_free(e);
     for (int c = 0; c < e->s.nr_cells; c++) free(e->s.cells[c].parts);
     free(e->s.cells);
+    free(e->s.cid_real);                 /* cid_marked is the same array */
     free(e->s.tasks);
     free(e->s.partlist);
     free(e->s.celllist);

@@ -99,6 +99,14 @@ int space_init(struct space *s, const double *origin, const double *dim, double 
     s->nr_cells = s->cdim[0] * s->cdim[1] * s->cdim[2];
     s->cells = calloc(s->nr_cells, sizeof(struct cell));
     if (s->cells == NULL) return space_error(space_err_malloc);
+    /* every cell is real (and marked): one process holds the whole space, no ghosts */
+    s->cid_real = malloc(sizeof(int) * s->nr_cells);
+    if (s->cid_real == NULL) return space_error(space_err_malloc);
+    for (int c = 0; c < s->nr_cells; c++) s->cid_real[c] = c;
+    s->cid_marked = s->cid_real;
+    s->cid_ghost = NULL;
+    s->nr_real = s->nr_marked = s->nr_cells;
+    s->nr_ghost = 0;
     for (int k = 0; k < 3; k++) {
         s->h[k] = s->dim[k] / s->cdim[k];
         s->ih[k] = 1.0 / s->h[k];

@@ -107,3 +107,42 @@ def test_full_size_rigid_water_vs_oracle():
     assert ito.max() > 5 and e.rigid_stats() == (ito.max(), 0)
     assert np.array_equal(bits(x), bits(xo)) and np.array_equal(bits(v), bits(vo)) and np.array_equal(bits(f), bits(fo))
     e.close()
+
+
+def _timers(e):
+    """struct engine's last field: unsigned long long timers[engine_timer_last] (18)."""
+    import ctypes as C
+    n = 18
+    off = M.lib().engine_sizeof() - 8 * n
+    return np.array((C.c_ulonglong * n).from_address(e.ptr.value + off))
+
+
+def test_rigid_unsort_timers_and_reset():
+    """engine_rigid_unsort (the groups in a random order) leaves the trajectory bit for bit
+    unchanged -- each group's constraints are solved alone; engine_step fills the step and
+    transfer timers (CPU ticks) and engine_timers_reset zeroes them."""
+    import ctypes as C
+    sysm = W.with_rigid_water(W.water_spce(10), 300.0, seed=3)
+    lib = M.lib()
+    lib.engine_rigid_unsort.restype = C.c_int
+    lib.engine_rigid_unsort.argtypes = [C.c_void_p]
+    lib.engine_timers_reset.restype = C.c_int
+    lib.engine_timers_reset.argtypes = [C.c_void_p]
+    out = []
+    for unsort in (False, True):
+        e = M.Engine.from_system(sysm)
+        if unsort:
+            assert lib.engine_rigid_unsort(e.ptr) == 0
+        assert lib.engine_timers_reset(e.ptr) == 0
+        for _ in range(4):
+            e.step()
+        t = _timers(e)
+        assert t[0] > 0 and t[15] > 0 and t[16] > 0 and t[17] > 0     # step, cuda_load, unload, dopairs
+        assert t[0] >= max(t[15], t[16], t[17])
+        assert lib.engine_timers_reset(e.ptr) == 0
+        assert not _timers(e).any()
+        x, v, f, c = e.parts()
+        out.append((x, v, c, e.energies()["total"]))
+        e.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
