@@ -872,6 +872,11 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
         double e_task = 0.0, v_task = 0.0;
         const int nstrips = (ni + 7) >> 3;
         const int jd0 = self ? 0 : jlist_dist(W, nj, 0);
+        // Pair tasks: every fourth strip, each lane finds the slot, validity and sorted-prefix
+        // length of one i of the next 32 (one search per lane instead of one per row and
+        // strip, where the row's four lanes repeat it); the strips take their rows' values
+        // from those lanes.
+        int c_loc = 0, c_len = 0, c_valid = 0;
 
         for (int st = 0; st < nstrips; ++st) {
             const int ii = st * 8 + row;
@@ -880,12 +885,21 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
             if (self) {
                 len = valid ? ii : 0;                       // pairs j < i
             } else {
-                const unsigned key = valid ? W.keyi[ii] : 0u;
-                loc = key >> 16;
-                const int di = key & 0xffff;
-                if (!P.unsorted) valid = valid && (jd0 + dnshift - di <= dmaxdist);
+                if ((st & 3) == 0) {                        // warp-uniform
+                    const int ic = st * 8 + lane;
+                    bool v = ic < ni;
+                    const unsigned key = v ? W.keyi[ic] : 0u;
+                    c_loc = key >> 16;
+                    const int di = key & 0xffff;
+                    if (!P.unsorted) v = v && (jd0 + dnshift - di <= dmaxdist);
+                    c_valid = v;
+                    c_len = v ? (P.unsorted ? nj : sorted_prefix(W.keyj, nj, dmaxdist - dnshift + di)) : 0;
+                }
+                const int src = ((st & 3) << 3) + row;
+                valid = __shfl_sync(FULL, c_valid, src) != 0;
                 if (!__any_sync(FULL, valid)) break;        // later strips lie farther from cell j
-                if (valid) len = P.unsorted ? nj : sorted_prefix(W.keyj, nj, dmaxdist - dnshift + di);
+                loc = __shfl_sync(FULL, c_loc, src);
+                len = __shfl_sync(FULL, c_len, src);
             }
             const int kmax = (int)__reduce_max_sync(FULL, (unsigned)len);
             float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
