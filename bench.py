@@ -894,7 +894,7 @@ def sched_ab(args, local_rank):
     """The learned scheduler's protocol on one system (default: the slab): clock64 task
     timings recorded over the first args.record device-resident MD steps, the cost network
     trained on them (its own GPU kernels), then args.sched_steps MD steps from the same state
-    with each queue order -- the count-product heuristic (the default), the network's
+    with each queue order -- the count-product heuristic longest-first (the reference's), the network's
     longest-first order, both orders in locality tiles (cost classes, cell-major within a
     class), and the cell-major order tasks are generated in -- and, for scale, the plain form.
     Makespan = device time of the steps (CUDA events around the whole run) / steps."""

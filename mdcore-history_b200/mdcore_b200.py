@@ -143,6 +143,7 @@ def lib() -> C.CDLL:
         "engine_batch_nonbond": (C.c_int, [vp]),
         "engine_batch_step": (C.c_int, [vp]),
         "engine_batch_setgroups": (C.c_int, [vp, C.c_int]),
+        "engine_batch_sched_order": (C.c_int, [vp, C.c_int]),
         "engine_batch_load_parts": (C.c_int, [vp]),
         "engine_batch_resident": (C.c_int, [vp]),
         "engine_batch_unload_parts": (C.c_int, [vp]),
@@ -667,6 +668,11 @@ class Batch:
 
     def step(self):
         _check(self.lib.engine_batch_step(self.ptr), "engine_batch_step")
+        return self
+
+    def sched_order(self, tile: int = 0):
+        """Count-product costs in locality tiles (engine_batch_sched_order; 0: automatic)."""
+        _check(self.lib.engine_batch_sched_order(self.ptr, tile), "engine_batch_sched_order")
         return self
 
     def set_groups(self, groups: int):
