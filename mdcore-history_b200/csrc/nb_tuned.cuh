@@ -679,6 +679,20 @@ __device__ __forceinline__ void flush_counters(const Params& P, unsigned npairs,
 
 
 
+// Warp reduce-scatter of two window steps over the 8 i rows of the 8 x 4 lane tile: the
+// lane of row q holds, for its column, the sum over the 8 rows of step q & 1.  Fixed order
+// of additions.
+__device__ __forceinline__ float reduce_scatter_rows2(const float (&v)[2], int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool b2 = lane & 4;
+    const float send = b2 ? v[0] : v[1];
+    const float keep = b2 ? v[1] : v[0];
+    float a = keep + __shfl_xor_sync(FULL, send, 4);
+    a += __shfl_xor_sync(FULL, a, 8);
+    a += __shfl_xor_sync(FULL, a, 16);
+    return a;
+}
+
 // Warp reduce-scatter over the 8 i rows of the 8 x 4 lane tile (lane = 4 * row + column):
 // each lane holds WIN values (window steps m); afterwards the lane of row q holds, for its
 // column, the sum over the 8 rows of step m = q (WIN = 8) or m = q & 3 (WIN = 4).  Fixed
@@ -915,6 +929,36 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
             ncand += strip_candidates(len, col, 4);
             float fix = 0.f, fiy = 0.f, fiz = 0.f;
             for (int k0 = 0; k0 < kmax; k0 += 4 * WIN) {
+                if (WIN == 4 && kmax - k0 <= 8) {
+                    // The last window, with at most two live steps (the usual case on cells
+                    // of ~20 particles, where a strip sweeps ~10 j): two steps and a
+                    // reduce-scatter of two values instead of four.
+                    float vx[2], vy[2], vz[2];
+                    bool any_acc = false;
+#pragma unroll
+                    for (int m = 0; m < 2; ++m) {
+                        if (k0 + 4 * m < kmax) {             // warp-uniform
+                            const int k = k0 + 4 * m + col;
+                            pair_force<HAS_EXCL, TAB>(P, S, jpos[k], jids, k, k < len, pix, piy, piz, prow, qi,
+                                                          ix, cut2, fix, fiy, fiz, vx[m], vy[m], vz[m], e_task,
+                                                          npairs, nexcl, any_acc);
+                        } else {
+                            vx[m] = 0.f; vy[m] = 0.f; vz[m] = 0.f;
+                        }
+                    }
+                    if (any_acc) {
+                        const float tx = reduce_scatter_rows2(vx, lane);
+                        const float ty = reduce_scatter_rows2(vy, lane);
+                        const float tz = reduce_scatter_rows2(vz, lane);
+                        const int k = k0 + 4 * (row & 1) + col;
+                        if (row < 2 && k < kmax) {
+                            float4 a = W.fj[k];
+                            a.x += tx; a.y += ty; a.z += tz;
+                            W.fj[k] = a;
+                        }
+                    }
+                    break;
+                }
                 float vx[WIN], vy[WIN], vz[WIN];
                 bool any_acc = false;
 #pragma unroll
