@@ -582,9 +582,6 @@ int engine_sched_train(struct engine *e, int epochs, int batch, float lr, unsign
 int engine_sched_predict(struct engine *e, float *pred_out, int n);
 int engine_sched_apply(struct engine *e, int use_mlp);
 int engine_sched_order(struct engine *e, int source, int tile);
-/* engine_sched_order for a batch, from the count-product costs (each engine's tasks are
- * consecutive, so a tile stays inside one engine's box); tile = 0: automatic. */
-int engine_batch_sched_order(struct engine_batch *b, int tile);
 /* The current queue order (n = the task count). */
 int engine_cuda_getorder(struct engine *e, int *order, int n);
 /* Sweep kernel launch parameters: warps per block (0 = default) and plain = 1 for the
@@ -732,6 +729,9 @@ int engine_batch_step(struct engine_batch *b);
  * 64 (never more than the engines).  A batch holding resident particles
  * (engine_batch_resident_begin) steps as one group. */
 int engine_batch_setgroups(struct engine_batch *b, int groups);
+/* engine_sched_order for a batch, from the count-product costs (each engine's tasks are
+ * consecutive, so a tile stays inside one engine's box); tile = 0: automatic. */
+int engine_batch_sched_order(struct engine_batch *b, int tile);
 /* engine_step_host for every engine with the forces of one batch evaluation. */
 int engine_batch_step_host(struct engine_batch *b);
 int engine_batch_load_parts(struct engine_batch *b);

@@ -134,3 +134,19 @@ def test_replica_ensemble_shapes():
         assert (s.dim >= 3 * s.cutoff).all()
         assert (s.x >= 0).all() and (s.x < s.dim).all()
         assert len(np.unique(np.round(s.x / 1e-4))) > 0
+
+
+@pytest.mark.parametrize("std", ["gnu99", "c11"])
+def test_headers_compile_cleanly(std, tmp_path):
+    """include/mdcore.h (and through it mdcore_b200.h and cycle.h) compiles in C with every
+    warning an error, as a driver built with -Wall -Werror includes it."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    src = tmp_path / "inc.c"
+    src.write_text('#include "mdcore.h"\nint main(void) { struct engine e; (void)e; return engine_timer_last > 0 ? 0 : 1; }\n')
+    r = subprocess.run(["gcc", f"-std={std}", "-D_GNU_SOURCE", "-Wall", "-Wextra", "-Werror", "-c",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(tmp_path / "inc.o")],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
