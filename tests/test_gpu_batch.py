@@ -233,3 +233,25 @@ def test_grouped_steps_then_resident_steps():
         bb.close()
     for e in ref_engines + engines:
         e.close()
+
+
+def test_batch_sched_order_keeps_results():
+    """engine_batch_sched_order (locality tiles of the count-product costs, any tile size)
+    only reorders the queue: forces and energies bit-identical to the default order."""
+    systems = W.argon_replicas(nrep=9, seed=17)
+    engines = engines_of(systems)
+    b = M.Batch(engines)
+    b.nonbond()
+    ref = [(e.forces().copy(), e.stats().epot) for e in engines]
+    pairs = b.stats().pairs
+    for tile in (1, 7, 0, 100000):
+        b.sched_order(tile)
+        b.nonbond()
+        assert b.stats().status == 0 and b.stats().pairs == pairs
+        for e, (f, ep) in zip(engines, ref):
+            assert np.array_equal(e.forces(), f) and e.stats().epot == ep
+    with pytest.raises(M.MdcoreError):
+        b.sched_order(-1)
+    b.close()
+    for e in engines:
+        e.close()
