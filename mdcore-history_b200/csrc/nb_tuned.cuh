@@ -879,7 +879,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
         const int ni = d.ni, nj = d.nj, si = d.si;
         const float4* __restrict__ jpos = W.js;
         const int* __restrict__ jids = self ? W.pidraw : W.jid;
-        const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
+        const int tshift_t = d.t;        // the task's shift is read at each strip, not held
         const float cut2 = self ? P.cutoff2s : P.cutoff2;
         const int dnshift = task_dnshift(d.tr);
         const int dmaxdist = task_dmax_skin(P, d.tr);
@@ -924,6 +924,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
                 if (HAS_EXCL) ix = load_iexcl(P, self ? W.pidraw[loc] : P.pid[si + loc]);
                 if (TAB == kTabGlobal && P.ep_pot >= 0) qi = P.qid[self ? W.pidraw[loc] : P.pid[si + loc]];
             }
+            const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[tshift_t];
             const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
             const int prow = __float_as_int(xi.w) * mt;
             ncand += strip_candidates(len, col, 4);
