@@ -255,3 +255,28 @@ def test_batch_sched_order_keeps_results():
     b.close()
     for e in engines:
         e.close()
+
+
+def test_full_ensemble_grouped_steps_equal_one_group():
+    """The 512-replica ensemble (1,451,403 atoms): three engine_batch_step calls in the
+    automatic grouping (4 groups) and in one group give every replica the same particles
+    bit for bit, and the batch totals agree."""
+    systems = W.argon_replicas()
+    out = []
+    for groups in (1, 0):
+        engines = engines_of(systems)
+        b = M.Batch(engines)
+        b.set_groups(groups)
+        for _ in range(3):
+            b.step()
+            assert b.stats().status == 0
+        st = b.stats()
+        out.append(([e.parts()[:3] for e in engines[::37]], (st.pairs, st.excluded, st.epot)))
+        b.close()
+        for e in engines:
+            e.close()
+    (p1, t1), (p2, t2) = out
+    assert t1[0] == t2[0] and t1[1] == t2[1] and abs(t1[2] - t2[2]) <= 1e-12 * abs(t1[2])
+    for a, b in zip(p1, p2):
+        for u, w in zip(a, b):
+            assert np.array_equal(u, w)
