@@ -679,6 +679,16 @@ __device__ __forceinline__ void flush_counters(const Params& P, unsigned npairs,
 
 
 
+// Sum of (x, y, z) over the 4 columns of a row of the 8 x 4 lane tile, scattered: column 0
+// gets the x sum, 1 the y sum, 2 the z sum, each as (c0 + c1) + (c2 + c3).
+__device__ __forceinline__ float reduce_scatter_cols3(float x, float y, float z, int col) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool b0 = col & 1, b1 = col & 2;
+    const float a0 = (b0 ? y : x) + __shfl_xor_sync(FULL, b0 ? x : y, 1);
+    const float a1 = (b0 ? 0.f : z) + __shfl_xor_sync(FULL, b0 ? z : 0.f, 1);
+    return (b1 ? a1 : a0) + __shfl_xor_sync(FULL, b1 ? a0 : a1, 2);
+}
+
 // Warp reduce-scatter of two window steps over the 8 i rows of the 8 x 4 lane tile: the
 // lane of row q holds, for its column, the sum over the 8 rows of step q & 1.  Fixed order
 // of additions.
@@ -985,25 +995,18 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
                     }
                 }
             }
-            // i force: sum over the 4 columns
-            fix += __shfl_xor_sync(FULL, fix, 1);
-            fiy += __shfl_xor_sync(FULL, fiy, 1);
-            fiz += __shfl_xor_sync(FULL, fiz, 1);
-            fix += __shfl_xor_sync(FULL, fix, 2);
-            fiy += __shfl_xor_sync(FULL, fiy, 2);
-            fiz += __shfl_xor_sync(FULL, fiz, 2);
+            // i force: sum over the 4 columns, scattered so that column c holds component c
+            // ((c0 + c1) + (c2 + c3) for every component, the same float sums in any lane)
+            const float fi = reduce_scatter_cols3(fix, fiy, fiz, col);
             __syncwarp();
-            if (valid && col == 0) {
+            if (valid && col < 3) {
                 if (self) {
-                    float4 a = W.fj[loc];
-                    a.x += fix; a.y += fiy; a.z += fiz;
-                    W.fj[loc] = a;
+                    float* a = &W.fj[loc].x + col;
+                    *a += fi;
                 } else {
-                    v_task += (double)pix * fix + (double)piy * fiy + (double)piz * fiz;
-                    unsigned long long* fp = P.force + 3 * (size_t)(si + loc);
-                    atomic_add_fixed(fp + 0, to_fixed(fix, status));
-                    atomic_add_fixed(fp + 1, to_fixed(fiy, status));
-                    atomic_add_fixed(fp + 2, to_fixed(fiz, status));
+                    const float pc = col == 0 ? pix : (col == 1 ? piy : piz);
+                    v_task += (double)pc * fi;
+                    atomic_add_fixed(P.force + 3 * (size_t)(si + loc) + col, to_fixed(fi, status));
                 }
             }
             __syncwarp();
