@@ -87,6 +87,9 @@ struct Params {
     const float* qid;
     int ep_pot;
     int tab_global;
+    // 1: the persistent sweeps evaluate tasks of at most 32 candidate pairs one pair per lane
+    // without staging (systems of few particles per cell); 0: every task is staged.
+    int tiny = 0;
     // Plain form only: when set, each task's partial forces are added to these floats with
     // float atomics (FP32 accumulation, order-dependent, as the reference's GPU runner adds
     // them) instead of to the fixed-point accumulators.

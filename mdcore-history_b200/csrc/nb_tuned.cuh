@@ -18,6 +18,8 @@
 //  * energy is summed per pair in double (float partial sums of cancelling Coulomb terms
 //    would cost ~1e-6 of the total); the virial per particle and task from the partial
 //    forces: sum over pairs of r_ij.F_ij = sum_i (x_i - shift).F_i + sum_j x_j.F_j;
+//  * tasks of at most 32 candidate pairs (a few particles per cell, as in a vapour) are not
+//    staged: one pair per lane, each accepted pair's force added to both particles;
 //  * optional per-task clock64 records (start, end, SM) for the learned scheduler.
 #pragma once
 #include "nb_kernels.cuh"
@@ -365,6 +367,21 @@ __device__ __forceinline__ bool desc_oversized(const TaskDesc& d, int cap) {
     return d.ni + 8 > cap || d.nj + 8 > cap;
 }
 
+// A task of at most 32 candidate pairs (a self task of at most 8 particles, a pair task with
+// n_i n_j <= 32: the vapour of an inhomogeneous system), evaluated one pair per lane
+// without staging (tiny_task).
+__device__ __forceinline__ bool desc_tiny(const TaskDesc& d) {
+    return d.tr.sid < 0 ? d.ni <= 8 : d.ni * d.nj <= 32;
+}
+
+// A task that is staged in the warp's slice and swept: every runnable one, except the tiny
+// ones when the kernel has the tiny path (TINY) and the system asks for it (P.tiny).
+template <bool TINY>
+__device__ __forceinline__ bool desc_staged(const Params& P, const TaskDesc& d, int cap) {
+    if constexpr (TINY) return desc_runnable(d, cap) && !(P.tiny && desc_tiny(d));
+    return desc_runnable(d, cap);
+}
+
 // Lane 0 issues the bulk copies of task d into the staging buffer of W: the j cell's
 // positions and ids, and for pair tasks the sort keys of both cells along the task's axis.
 __device__ __forceinline__ void issue_copies(const Params& P, const TaskDesc& d, const WarpSlice& W, int lane) {
@@ -409,16 +426,17 @@ __device__ __forceinline__ void build_jlist(const TaskDesc& d, const WarpSlice& 
 
 // The task loop of a worker warp: pops tasks, stages them (STAGES = 2: the next task's
 // copies are issued before the current task is swept) and calls
-// sweep(task, slice, t_start) for every task with pairs to sweep.  Returns when the queue
-// is drained or a bulk copy timed out (status set).
+// sweep(task, slice, t_start) for every task with pairs to sweep, or tiny(task, slice,
+// t_start) for a task of at most 32 candidate pairs, which is not staged.  Returns when the
+// queue is drained or a bulk copy timed out (status set).
 //
 // With many tasks per worker warp (at least 16), or two stages, the next task is popped
 // and its description loaded while the current one is swept.  With few, large tasks the
 // warp pops only when it is done: a task reserved early would wait behind the current one
 // while other warps run dry at the end of the queue.
-template <int STAGES, typename Sweep>
+template <int STAGES, bool TINY, typename Sweep, typename Tiny>
 __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T, unsigned char* smem_raw, int cap,
-                                          int nw, unsigned& status, Sweep&& sweep) {
+                                          int nw, unsigned& status, Sweep&& sweep, Tiny&& tiny) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nq = T.qcount ? *T.qcount : P.ntasks;
     const int workers = (int)gridDim.x * nw;
@@ -428,17 +446,20 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
     unsigned phases = 0;               // bit s: parity of completed phases of stage s
     int s = 0;
     TaskDesc d = desc_get(desc_fetch(P, T, cur, nq, batch, lane));
-    bool issued = d.t >= 0 && desc_runnable(d, cap);
+    bool issued = d.t >= 0 && desc_staged<TINY>(P, d, cap);
     if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
     while (d.t >= 0) {
         long long t_start = 0;
         if (T.task_clock && lane == 0) t_start = clock64();
         int fnext = early ? desc_fetch(P, T, cur, nq, batch, lane) : 0;
-        if (!issued) {                 // empty, single-particle or oversized task
+        if (!issued) {                 // empty, single-particle, oversized or tiny task
             if (!early) fnext = desc_fetch(P, T, cur, nq, batch, lane);
+            // No copy of this warp is in flight here (only the task marked issued has
+            // copies), so the tiny path may use the slice's j arrays.
             if (desc_oversized(d, cap)) status |= kStatusCellOverflow;
+            else if (TINY && desc_runnable(d, cap)) tiny(d, warp_slice(smem_raw, cap, warp, STAGES, s), t_start);
             d = desc_get(fnext);
-            issued = d.t >= 0 && desc_runnable(d, cap);
+            issued = d.t >= 0 && desc_staged<TINY>(P, d, cap);
             if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
             continue;
         }
@@ -460,7 +481,7 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
         bool n_issued = false;
         if (STAGES == 2) {
             const TaskDesc n = desc_get(fnext);
-            if (n.t >= 0 && desc_runnable(n, cap)) {
+            if (n.t >= 0 && desc_staged<TINY>(P, n, cap)) {
                 issue_copies(P, n, warp_slice(smem_raw, cap, warp, STAGES, s ^ 1), lane);
                 n_issued = true;
             }
@@ -474,7 +495,7 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
             s ^= 1;
             issued = n_issued;
         } else {
-            issued = d.t >= 0 && desc_runnable(d, cap);
+            issued = d.t >= 0 && desc_staged<TINY>(P, d, cap);
             if (issued) issue_copies(P, d, warp_slice(smem_raw, cap, warp, STAGES, s), lane);
         }
     }
@@ -679,6 +700,85 @@ __device__ __forceinline__ void flush_counters(const Params& P, unsigned npairs,
 
 
 
+// A tiny task (desc_tiny): one candidate pair per lane, the two particles read from global
+// memory, no staging and no sort keys.  All n_i n_j pairs of a pair task are tested: the
+// sorted sweep's bound is conservative (a j past a particle's sorted prefix lies beyond the
+// cutoff), so the accepted pairs are the same.  Each accepted pair's force goes to both
+// particles in fixed point (-w on i, +w on j; order-independent like every other partial),
+// the pair energy and virial d.w into the task's FP64 sums as in finish_task.  Self tasks
+// map lane l to the pair (i, j), j < i, of the triangle's rows i = 1, 2, ...
+template <bool HAS_EXCL, int TAB>
+__device__ __forceinline__ void tiny_task(const Params& P, const TunedParams& T, const SharedTables& S,
+                                          const TaskDesc& d, const WarpSlice& W, long long t_start, int mt,
+                                          unsigned& npairs, unsigned& nexcl, unsigned& ncand, unsigned& status,
+                                          int lane) {
+    const bool self = d.tr.sid < 0;
+    const int ni = d.ni, nj = d.nj;
+    const int npair = self ? ni * (ni - 1) / 2 : ni * nj;
+    const bool act = lane < npair;
+    int i = 0, j = 0;
+    if (act) {
+        if (self) {
+            int l = lane;
+            i = 1;
+            while (l >= i) { l -= i; ++i; }
+            j = l;
+        } else {
+            i = lane / nj;
+            j = lane - i * nj;
+        }
+    }
+    const int slot_i = d.si + i, slot_j = (self ? d.si : d.sj) + j;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f), xj = xi;
+    IExcl ix = no_iexcl();
+    float qi = 0.f;
+    if (act) {
+        xi = P.xq[slot_i];
+        xj = P.xq[slot_j];
+        if (HAS_EXCL || TAB == kTabGlobal) {
+            const int pi = P.pid[slot_i];
+            if (HAS_EXCL) ix = load_iexcl(P, pi);
+            if (TAB == kTabGlobal && P.ep_pot >= 0) qi = P.qid[pi];
+            W.jid[lane] = P.pid[slot_j];
+        }
+    }
+    __syncwarp();
+    const float4 sh = self ? make_float4(0.f, 0.f, 0.f, 0.f) : P.tshift[d.t];
+    const float pix = __fsub_rn(xi.x, sh.x), piy = __fsub_rn(xi.y, sh.y), piz = __fsub_rn(xi.z, sh.z);
+    const int prow = __float_as_int(xi.w) * mt;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f, wx, wy, wz;
+    double e_task = 0.0;
+    bool any_acc = false;
+    pair_force<HAS_EXCL, TAB>(P, S, xj, W.jid, lane, act, pix, piy, piz, prow, qi, ix, self ? P.cutoff2s : P.cutoff2,
+                              fix, fiy, fiz, wx, wy, wz, e_task, npairs, nexcl, any_acc);
+    ncand += act ? 1u : 0u;
+    const float dx = __fsub_rn(pix, xj.x), dy = __fsub_rn(piy, xj.y), dz = __fsub_rn(piz, xj.z);
+    const double v_pair = (double)dx * wx + (double)dy * wy + (double)dz * wz;      // 0 unless accepted
+    if (act) {
+        const long long fx = to_fixed(wx, status), fy = to_fixed(wy, status), fz = to_fixed(wz, status);
+        unsigned long long* fpi = P.force + 3 * (size_t)slot_i;
+        unsigned long long* fpj = P.force + 3 * (size_t)slot_j;
+        atomic_add_fixed(fpi + 0, -fx);
+        atomic_add_fixed(fpi + 1, -fy);
+        atomic_add_fixed(fpi + 2, -fz);
+        atomic_add_fixed(fpj + 0, fx);
+        atomic_add_fixed(fpj + 1, fy);
+        atomic_add_fixed(fpj + 2, fz);
+    }
+    const long long e_fix = warp_sum_fixed(__double2ll_rn(e_task * kEnergyScale));
+    const long long v_fix = warp_sum_fixed(__double2ll_rn(v_pair * kEnergyScale));
+    if (lane == 0) {
+        atomicAdd(&P.cell_epot[d.tr.ci], (unsigned long long)e_fix);
+        atomicAdd(P.cell_vir ? &P.cell_vir[d.tr.ci] : &P.acc[kAccVirial], (unsigned long long)v_fix);
+        if (T.task_clock) {
+            T.task_clock[2 * d.t] = t_start;
+            T.task_clock[2 * d.t + 1] = clock64();
+            T.task_sm[d.t] = (int)smid();
+        }
+    }
+    __syncwarp();
+}
+
 // Sum of (x, y, z) over the 4 columns of a row of the 8 x 4 lane tile, scattered: column 0
 // gets the x sum, 1 the y sum, 2 the z sum, each as (c0 + c1) + (c2 + c3).
 __device__ __forceinline__ float reduce_scatter_cols3(float x, float y, float z, int col) {
@@ -751,7 +851,7 @@ __device__ __forceinline__ float reduce_scatter_rows(const float (&v)[WIN], int 
 //
 // WIN (4 or 8): sweep steps per reduce-scatter; 8 halves the shuffles per step but holds
 // twice the registers.  STAGES (1 or 2): staging buffers per warp.
-template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM>
+template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM, bool TINY>
 __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -768,7 +868,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
     __syncthreads();
 
     unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
-    run_tasks<STAGES>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+    run_tasks<STAGES, TINY>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
         const bool self = d.tr.sid < 0;
         const int ni = d.ni, nj = d.nj, si = d.si;
         const float4* __restrict__ jpos = W.js;
@@ -854,6 +954,8 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
             __syncwarp();
         }
         finish_task(P, T, W, d, e_task, v_task, t_start, status, lane);
+    }, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+        tiny_task<HAS_EXCL, TAB>(P, T, S, d, W, t_start, mt, npairs, nexcl, ncand, status, lane);
     });
     flush_counters(P, npairs, nexcl, ncand, status, lane);
 }
@@ -866,7 +968,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tuned(TunedPa
 // contributions of WIN steps (4 WIN consecutive j) are summed over the 8 rows by one
 // reduce-scatter, after which the 32 (or 16) lanes write distinct j; the i forces are
 // summed over the 4 columns at the end of the strip.
-template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM>
+template <int NW, bool HAS_EXCL, int TAB, int WIN, int STAGES, int TPSM, bool TINY>
 __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedParams T, int cap) {
     static_assert(WIN == 4 || WIN == 8, "sweep window of 4 or 8 steps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -884,7 +986,7 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
     __syncthreads();
 
     unsigned npairs = 0, nexcl = 0, ncand = 0, status = 0;
-    run_tasks<STAGES>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+    run_tasks<STAGES, TINY>(P, T, smem_raw, cap, NW, status, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
         const bool self = d.tr.sid < 0;
         const int ni = d.ni, nj = d.nj, si = d.si;
         const float4* __restrict__ jpos = W.js;
@@ -1012,6 +1114,8 @@ __global__ void __launch_bounds__(NW * 32, TPSM / (NW * 32)) sweep_tiled(TunedPa
             __syncwarp();
         }
         finish_task(P, T, W, d, e_task, v_task, t_start, status, lane);
+    }, [&](const TaskDesc& d, const WarpSlice& W, long long t_start) {
+        tiny_task<HAS_EXCL, TAB>(P, T, S, d, W, t_start, mt, npairs, nexcl, ncand, status, lane);
     });
     flush_counters(P, npairs, nexcl, ncand, status, lane);
 }

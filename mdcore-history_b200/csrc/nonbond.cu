@@ -210,6 +210,7 @@ struct NbState {
     int groups_req = 0;                // 0: automatic
     std::vector<NbState*> groups;
     int max_chunks = 8;                // pipeline chunks of one engine_step transfer
+    int tiny_inherited = -1;           // a group's Params::tiny, its batch's (-1: from its own counts)
     std::vector<int> heur_order;       // count-product order built at load
 };
 
@@ -406,6 +407,18 @@ long long env_count(const char* name, long long dflt) {
     const long long v = env ? std::atoll(env) : 0;
     return v > 0 ? v : dflt;
 }
+// The persistent sweeps' unstaged path for tasks of at most 32 candidate pairs (Params::tiny)
+// is on for systems of fewer than 8 particles per cell on average, where such tasks are
+// common (a vapour, a dilute gas); elsewhere the per-task test is left out.  A property of
+// the engines' particle and cell counts, so every entry point (engine_step, resident steps,
+// batches, the no-alloc call) takes the same path for the same system.
+int tiny_tasks_of(const NbState* st) {
+    if (st->tiny_inherited >= 0) return st->tiny_inherited;
+    long long n = 0;
+    for (const struct engine* e : st->engines) n += e->s.nr_parts;
+    return n < 8LL * st->ncells ? 1 : 0;
+}
+
 long long host_grain_parts() {
     static const long long v = env_count("MDB_HOST_GRAIN", 2048);
     return v;
@@ -553,9 +566,9 @@ int launch_plain(NbState* st, const Params& P, int cap) {
 // Persistent launch: as many CTAs as fit on every SM at once.  Under stream capture the
 // function attribute and occupancy query are skipped and the grid of the preceding direct
 // launch of the same configuration is reused.
-template <int NW, bool EX, int TAB, int WIN, int LAY, int STG, int TPSM>
-int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
-    auto kern = LAY ? sweep_tiled<NW, EX, TAB, WIN, STG, TPSM> : sweep_tuned<NW, EX, TAB, WIN, STG, TPSM>;
+template <int NW, bool EX, int TAB, int WIN, int LAY, int STG, int TPSM, bool TINY>
+int launch_tuned_k(NbState* st, const TunedParams& T, int cap, size_t smem) {
+    auto kern = LAY ? sweep_tiled<NW, EX, TAB, WIN, STG, TPSM, TINY> : sweep_tuned<NW, EX, TAB, WIN, STG, TPSM, TINY>;
     int grid = st->last_grid;
     if (!st->capturing) {
         CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -568,6 +581,15 @@ int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
     kern<<<grid, NW * 32, smem, st->stream>>>(T, cap);
     CU(cudaGetLastError());
     return 0;
+}
+
+// The tiny-task path (Params::tiny) is compiled into the shapes of 1024 threads per SM, those
+// of small cells; the other shapes, and systems that do not ask for it, run without it.
+template <int NW, bool EX, int TAB, int WIN, int LAY, int STG, int TPSM>
+int launch_tuned_nw(NbState* st, const TunedParams& T, int cap, size_t smem) {
+    if constexpr (TPSM == 1024)
+        if (T.p.tiny) return launch_tuned_k<NW, EX, TAB, WIN, LAY, STG, TPSM, true>(st, T, cap, smem);
+    return launch_tuned_k<NW, EX, TAB, WIN, LAY, STG, TPSM, false>(st, T, cap, smem);
 }
 
 template <int NW, int WIN, int LAY, int STG, int TPSM>
@@ -734,6 +756,7 @@ int issue_kernels(NbState* st, const DevView& V, bool span = true) {
     P.qid = st->d_qid;
     P.ep_pot = st->ep_pot;
     P.tab_global = st->tab_global;
+    P.tiny = tiny_tasks_of(st);
     P.cell_mdx = V.cell_mdx;
 
     const bool f32 = st->plain && st->fp32acc;
@@ -2783,6 +2806,7 @@ void copy_shape(NbState* c, const NbState* st) {
     c->sd_gamma = st->sd_gamma;
     c->sd_dmax = st->sd_dmax;
     c->max_chunks = std::max(1, 8 / (int)st->groups.size());
+    c->tiny_inherited = tiny_tasks_of(st);       // the same sweep path as the whole batch
 }
 
 // (Re)builds k group states over contiguous runs of engines of about equal particle counts.
@@ -3291,7 +3315,7 @@ __global__ void noalloc_check_cells(const int* __restrict__ cstart, const int* _
 
 template <int NW, bool EX, int TAB>
 int noalloc_sweep_nw(const NbState* st, const TunedParams& T, int cap, size_t smem, cudaStream_t s) {
-    auto kern = sweep_tuned<NW, EX, TAB, 4, 1, 640>;
+    auto kern = sweep_tuned<NW, EX, TAB, 4, 1, 640, false>;
     cudaFuncAttributes fa;
     CU(cudaFuncGetAttributes(&fa, kern));
     if (fa.maxDynamicSharedSizeBytes < (int)smem)
@@ -3407,6 +3431,7 @@ int nonbond_noalloc(struct engine* e, const void* xq, const int* pid, const int*
     P.qid = st->d_qid;
     P.ep_pot = st->ep_pot;
     P.tab_global = st->tab_global;
+    P.tiny = tiny_tasks_of(st);
     T.order = st->d_order;
     T.qcount = nullptr;
     T.counter = counter;
