@@ -5,8 +5,8 @@ per lane without staging or sort keys, beside the staged sorted sweep of the lar
 Systems with both kinds -- dilute rigid water (exclusions, type tables in shared memory), a
 liquid slab in its vapour (two types), dilute argon (one table), dilute solvated chains
 (global tables, per-particle charges, exclusions) -- against the FP64 oracle for both lane
-layouts and both staging depths; forces independent of the queue order; resident steps
-equal to engine_step."""
+layouts and both staging depths; the full-size slab; forces independent of the queue order;
+resident steps equal to engine_step."""
 import numpy as np
 import pytest
 
@@ -116,3 +116,25 @@ def test_tiny_tasks_resident_steps_equal_engine_step():
         out.append((pos, epot))
         e.close()
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_full_size_slab_with_tiny_path_vs_oracle(layout):
+    """The 1,048,576-atom slab (4.1 particles per cell: the tiny path is on) with the
+    1024-thread shapes that carry it, two staging buffers: counts bit-exact, energy, virial
+    and forces as the oracle's."""
+    sysm = W.lj_slab()
+    o = oracle_of("slab-1048576", sysm)
+    e = M.Engine.from_system(sysm)
+    e.set_layout(layout, 2, 1024)
+    e.nonbond()
+    f, st = e.forces(), e.stats()
+    err = force_errors(f, o["f"])
+    print("slab-1048576", layout, "pairs", st.pairs, err)
+    assert st.status == 0
+    assert st.pairs == o["pairs"] and st.excluded == o["excluded"]
+    assert abs(st.epot - o["epot"]) <= 1e-6 * abs(o["epot"])
+    assert abs(st.virial - o["virial"]) <= 1e-6 * o["virial_abs"]
+    assert err["global_rel"] <= 2e-6, err
+    assert err["max_over_frms"] <= 2e-5, err
+    e.close()
