@@ -739,6 +739,10 @@ __device__ __forceinline__ void tiny_task(const Params& P, const TunedParams& T,
             const int pi = P.pid[slot_i];
             if (HAS_EXCL) ix = load_iexcl(P, pi);
             if (TAB == kTabGlobal && P.ep_pot >= 0) qi = P.qid[pi];
+            // slot `lane` of the j-id list (pair_force reads the partner's id there); with
+            // cap < 32 it runs past the list into this warp's own staging area (32 ids need
+            // 4 cap + 28 cap >= 128 bytes there, cap >= 9), which has no copy in flight
+            // while a tiny task runs
             W.jid[lane] = P.pid[slot_j];
         }
     }
