@@ -440,7 +440,8 @@ __device__ __forceinline__ void run_tasks(const Params& P, const TunedParams& T,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nq = T.qcount ? *T.qcount : P.ntasks;
     const int workers = (int)gridDim.x * nw;
-    const int batch = max(1, min(16, nq / (8 * workers)));
+    // queue entries per pop: up to 8 (16 and more measured slower on small-cell systems)
+    const int batch = max(1, min(8, nq / (8 * workers)));
     const bool early = STAGES == 2 || nq >= 16 * workers;     // warp-uniform
     QueueCursor cur;
     unsigned phases = 0;               // bit s: parity of completed phases of stage s
